@@ -1,0 +1,138 @@
+"""cup3d_b200: B200-native time-step hot path of CubismUP_3D behind a C ABI.
+
+Python is only a thin host layer over include/cup3d_b200.h (ctypes).  The
+compute path is the sm_100a library cup3d_b200/libcup3d_b200.so; there is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import (ADV, BC, FIELD, FIELD_NCOMP, SOLVER, CupError, check, cup_config,
+                   cup_solve_stats, dptr, iptr, lib)
+
+__all__ = ["Context", "config", "CupError", "ADV", "BC", "SOLVER", "FIELD"]
+
+
+def config(flags: str = "", **kw) -> cup_config:
+    """Config with the reference's defaults, then `-key value` flags, then keywords."""
+    cfg = cup_config()
+    lib().cup_config_default(C.byref(cfg))
+    if flags:
+        check(lib().cup_config_parse(C.byref(cfg), flags.encode()))
+    for k, v in kw.items():
+        key = "lambda_" if k == "lambda" else k
+        if key in ("bpd", "bc", "uinf"):
+            arr = getattr(cfg, key)
+            for i in range(3):
+                arr[i] = v[i]
+        else:
+            setattr(cfg, key, v)
+    return cfg
+
+
+def _dev_ptr(t):
+    """Raw device pointer of a torch CUDA tensor (float64, contiguous)."""
+    import torch
+    assert isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+    return C.c_void_p(t.data_ptr())
+
+
+class Context:
+    """One simulation on one GPU (cup_ctx).  device=-1 gives a host-only
+    context (mesh construction and tables only)."""
+
+    def __init__(self, cfg: cup_config):
+        self.cfg = cfg
+        p = lib().cup_create(C.byref(cfg))
+        if not p:
+            raise CupError(-1, lib().cup_last_error(None).decode())
+        self._p = C.c_void_p(p)
+
+    def close(self):
+        if getattr(self, "_p", None):
+            lib().cup_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- mesh -------------------------------------------------------------
+    def set_mesh(self, level, index):
+        level = np.ascontiguousarray(level, dtype=np.int32)
+        index = np.ascontiguousarray(index, dtype=np.int32).reshape(-1)
+        check(lib().cup_set_mesh(self._p, len(level), iptr(level), iptr(index)), self._p)
+
+    def set_mesh_uniform(self):
+        check(lib().cup_set_mesh_uniform(self._p), self._p)
+
+    def set_mesh_sphere_wake(self, center, radius, flow_dir=-1, near_radius=0.3, wake_len=1.0,
+                             wake_radius=0.3):
+        c = np.ascontiguousarray(center, dtype=np.float64)
+        check(lib().cup_set_mesh_sphere_wake(self._p, dptr(c), radius, flow_dir, near_radius,
+                                             wake_len, wake_radius), self._p)
+
+    def set_mesh_random(self, seed, prob):
+        check(lib().cup_set_mesh_random(self._p, seed, prob), self._p)
+
+    @property
+    def nb(self) -> int:
+        return lib().cup_num_blocks(self._p)
+
+    def blocks(self):
+        nb = self.nb
+        level = np.zeros(nb, np.int32)
+        index = np.zeros(3 * nb, np.int32)
+        h = np.zeros(nb, np.float64)
+        check(lib().cup_get_blocks(self._p, iptr(level), iptr(index), dptr(h)), self._p)
+        return level, index.reshape(nb, 3), h
+
+    def faces(self):
+        nb = self.nb
+        kinds = np.zeros(6 * nb, np.int32)
+        nbrs = np.zeros(24 * nb, np.int32)
+        check(lib().cup_get_faces(self._p, iptr(kinds), iptr(nbrs)), self._p)
+        return kinds.reshape(nb, 6), nbrs.reshape(nb, 6, 4)
+
+    # ---- fields -----------------------------------------------------------
+    def upload(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(-1)
+        assert a.size == FIELD_NCOMP[name] * self.nb * 512
+        check(lib().cup_upload_field(self._p, FIELD[name], dptr(a)), self._p)
+
+    def download(self, name):
+        a = np.zeros(FIELD_NCOMP[name] * self.nb * 512, np.float64)
+        check(lib().cup_download_field(self._p, FIELD[name], dptr(a)), self._p)
+        return a
+
+    def field_ptr(self, name) -> int:
+        return lib().cup_field_device_ptr(self._p, FIELD[name])
+
+    # ---- raw device operators (torch CUDA float64 tensors) ----------------
+    def poisson_apply(self, x, y, mean_mode=-1):
+        check(lib().cup_poisson_apply_dev(self._p, _dev_ptr(x), _dev_ptr(y), mean_mode), self._p)
+
+    def block_inverse(self, x, y):
+        check(lib().cup_block_inverse_dev(self._p, _dev_ptr(x), _dev_ptr(y)), self._p)
+
+    def poisson_solve_dev(self, b, x):
+        st = cup_solve_stats()
+        rc = check(lib().cup_poisson_solve_dev(self._p, _dev_ptr(b), _dev_ptr(x), C.byref(st)), self._p)
+        return rc, st.as_dict()
+
+    def poisson_solve(self):
+        """PoissonSolverBase::solve(): RHS in 'lhs', guess/result in 'pres'."""
+        st = cup_solve_stats()
+        rc = check(lib().cup_poisson_solve(self._p, C.byref(st)), self._p)
+        return rc, st.as_dict()

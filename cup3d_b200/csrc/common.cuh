@@ -1,0 +1,118 @@
+// Shared device definitions: block geometry, mesh tables, reductions.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+
+namespace cup3d {
+
+constexpr int BS = 8;     // cells per block edge (CUP_BLOCK_SIZE)
+constexpr int BN = 512;   // cells per block
+constexpr int NT = 256;   // threads per CTA for block kernels
+
+enum : int { K_SAME = 0, K_BOUNDARY = 1, K_COARSER = 2, K_FINER = 3 };
+enum : int { BCK_FREESPACE = 0, BCK_PERIODIC = 1, BCK_WALL = 2 };
+
+// Mesh tables as uploaded by the host (see mesh.h for their meaning).
+struct DevMesh {
+  int nb;
+  int mean_block;               // block with index (0,0,0), -1 if none
+  const int* __restrict__ fkind;  // 6*nb
+  const int* __restrict__ fnbr;   // 24*nb
+  const int* __restrict__ index;  // 3*nb
+  const double* __restrict__ h;   // nb
+};
+
+#ifndef CUP3D_TAN_HELPERS
+#define CUP3D_TAN_HELPERS
+__host__ __device__ __forceinline__ int tan1(int d) { return d == 0 ? 1 : 0; }
+__host__ __device__ __forceinline__ int tan2(int d) { return d == 2 ? 1 : 2; }
+#endif
+
+// Cell of a block on its own face (d, side) at `layer` cells inward, at
+// tangential position (a along tan1, b along tan2).
+__device__ __forceinline__ int face_cell(int d, int side, int layer, int a, int b) {
+  const int c = side ? BS - 1 - layer : layer;
+  return d == 0 ? c + BS * a + BS * BS * b : (d == 1 ? a + BS * c + BS * BS * b : a + BS * b + BS * BS * c);
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions: every CTA writes NR partial sums, the last CTA to
+// arrive (ticket counter) sums all partials in CTA order and runs `fin`.
+// ---------------------------------------------------------------------------
+template <int NR>
+__device__ __forceinline__ void block_reduce(double (&v)[NR], double* sm /* >= 8*NR */) {
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_xor_sync(0xffffffffu, v[r], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) sm[w * NR + r] = v[r];
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      double s = l < nw ? sm[l * NR + r] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      v[r] = s;
+    }
+  }
+  __syncthreads();
+}
+
+struct GridReduce {
+  double* partial;        // gridDim.x * 8 doubles
+  unsigned int* counter;  // one per reduction site, zero between launches
+};
+
+// Returns true in the last CTA, with the grid totals in v (all threads of it).
+template <int NR>
+__device__ bool grid_reduce(double (&v)[NR], const GridReduce& g, double* sm) {
+  block_reduce<NR>(v, sm);
+  __shared__ unsigned int s_ticket;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) g.partial[blockIdx.x * 8 + r] = v[r];
+    __threadfence();
+    s_ticket = atomicAdd(g.counter, 1u);
+  }
+  __syncthreads();
+  if (s_ticket != gridDim.x - 1) return false;
+  __threadfence();
+  double acc[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] += __ldcg(&g.partial[i * 8 + r]);
+  block_reduce<NR>(acc, sm);
+  // broadcast lane-0 totals to the whole CTA
+  __shared__ double s_tot[NR];
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) s_tot[r] = acc[r];
+    *g.counter = 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NR; ++r) v[r] = s_tot[r];
+  return true;
+}
+
+}  // namespace cup3d
+
+#define CUP_CUDA_TRY(expr)                                                        \
+  do {                                                                            \
+    cudaError_t e_ = (expr);                                                      \
+    if (e_ != cudaSuccess) return ::cup3d::set_cuda_error(e_, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+namespace cup3d {
+int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+}

@@ -1,0 +1,425 @@
+// C-ABI implementation: context, mesh, fields, Poisson entry points.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
+
+#include "context.h"
+
+namespace cup3d {
+
+static thread_local std::string g_last_error;
+
+int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+  std::ostringstream os;
+  os << "CUDA error " << int(e) << " (" << cudaGetErrorString(e) << ") in " << what << " at "
+     << file << ":" << line;
+  g_last_error = os.str();
+  return CUP_ERR_CUDA;
+}
+
+int ctx_fail(cup_ctx* c, int code, const std::string& msg) {
+  g_last_error = msg;
+  if (c) c->err = msg;
+  return code;
+}
+
+size_t nbn(const cup_ctx* c) { return size_t(c->mesh.nb) * BN; }
+
+// Propagates the thread-local message of a failed internal call into ctx.
+static int keep(cup_ctx* c, int rc) {
+  if (rc < 0 && c) c->err = g_last_error;
+  return rc;
+}
+
+static int upload_mesh(cup_ctx* c) {
+  Mesh& m = c->mesh;
+  c->mesh_arena.release();
+  int *fk, *fn, *ix;
+  double* h;
+  if (int rc = c->mesh_arena.alloc(&fk, 6 * size_t(m.nb))) return rc;
+  if (int rc = c->mesh_arena.alloc(&fn, 24 * size_t(m.nb))) return rc;
+  if (int rc = c->mesh_arena.alloc(&ix, 3 * size_t(m.nb))) return rc;
+  if (int rc = c->mesh_arena.alloc(&h, size_t(m.nb))) return rc;
+  CUP_CUDA_TRY(cudaMemcpy(fk, m.face_kind.data(), 6 * size_t(m.nb) * 4, cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(fn, m.face_nbr.data(), 24 * size_t(m.nb) * 4, cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(ix, m.index.data(), 3 * size_t(m.nb) * 4, cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(h, m.h.data(), size_t(m.nb) * 8, cudaMemcpyHostToDevice));
+  c->dm.nb = m.nb;
+  c->dm.mean_block = m.mean_block;
+  c->dm.fkind = fk;
+  c->dm.fnbr = fn;
+  c->dm.index = ix;
+  c->dm.h = h;
+  return 0;
+}
+
+static int alloc_fields(cup_ctx* c) {
+  c->field_arena.release();
+  c->obst_arena.release();
+  c->ob = DevObstacle();
+  const size_t n = nbn(c);
+  DevArena& A = c->field_arena;
+  Fields& F = c->F;
+  F = Fields();
+  for (int i = 0; i < 2; ++i) {
+    if (int rc = A.alloc(&F.vel[i], 3 * n)) return rc;
+    if (int rc = A.alloc(&F.pres[i], n)) return rc;
+  }
+  if (int rc = A.alloc(&F.tmpV, 3 * n)) return rc;
+  if (int rc = A.alloc(&F.lhs, n)) return rc;
+  if (int rc = A.alloc(&F.chi, n)) return rc;
+  if (int rc = A.alloc(&F.phi, n)) return rc;
+  PoissonWork& W = c->W;
+  double** vecs[] = {&W.r, &W.rhat, &W.p, &W.nu, &W.t, &W.z1, &W.z2, &W.xs[1], &W.xs[2]};
+  for (double** v : vecs)
+    if (int rc = A.alloc(v, n)) return rc;
+  W.xs[0] = nullptr;
+  // grid: a few CTAs per SM, never more than blocks
+  W.grid = std::max(1, std::min(c->mesh.nb, c->num_sms * 8));
+  if (int rc = A.alloc(&W.partial, size_t(W.grid) * 8)) return rc;
+  if (int rc = A.alloc(&W.counters, 32)) return rc;
+  if (int rc = A.alloc(&W.st, 1)) return rc;
+  CUP_CUDA_TRY(cudaMemset(W.counters, 0, 32 * sizeof(unsigned int)));
+  for (int i = 0; i < 2; ++i) {
+    CUP_CUDA_TRY(cudaMemset(F.vel[i], 0, 3 * n * 8));
+    CUP_CUDA_TRY(cudaMemset(F.pres[i], 0, n * 8));
+  }
+  CUP_CUDA_TRY(cudaMemset(F.tmpV, 0, 3 * n * 8));
+  CUP_CUDA_TRY(cudaMemset(F.lhs, 0, n * 8));
+  CUP_CUDA_TRY(cudaMemset(F.chi, 0, n * 8));
+  CUP_CUDA_TRY(cudaMemset(F.phi, 0, n * 8));
+  return 0;
+}
+
+static int install_mesh(cup_ctx* c, const std::vector<std::array<int32_t, 4>>& leaves) {
+  MeshSpec spec;
+  for (int d = 0; d < 3; ++d) {
+    spec.bpd[d] = c->cfg.bpd[d];
+    spec.bc[d] = c->cfg.bc[d];
+  }
+  spec.level_max = c->cfg.level_max;
+  spec.extent = c->cfg.extent;
+  std::string err;
+  Mesh m;
+  if (!mesh_build(spec, leaves, m, err)) return ctx_fail(c, CUP_ERR_MESH, "mesh: " + err);
+  c->mesh = std::move(m);
+  if (c->host_only) return 0;
+  if (int rc = upload_mesh(c)) return keep(c, rc);
+  if (int rc = alloc_fields(c)) return keep(c, rc);
+  return 0;
+}
+
+static double* field_ptr(cup_ctx* c, int field, int* ncomp) {
+  *ncomp = 1;
+  if (c->host_only) return nullptr;
+  switch (field) {
+    case CUP_FIELD_VEL: *ncomp = 3; return c->F.vel[c->F.vcur];
+    case CUP_FIELD_PRES: return c->F.pres[c->F.pcur];
+    case CUP_FIELD_CHI: return c->F.chi;
+    case CUP_FIELD_LHS: return c->F.lhs;
+    case CUP_FIELD_TMPV: *ncomp = 3; return c->F.tmpV;
+    default: return nullptr;
+  }
+}
+
+}  // namespace cup3d
+
+using namespace cup3d;
+
+extern "C" {
+
+void cup_config_default(cup_config* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->bpd[0] = c->bpd[1] = c->bpd[2] = 1;
+  c->level_max = 1;
+  c->bc[0] = c->bc[1] = c->bc[2] = CUP_BC_FREESPACE;
+  c->extent = 1.0;
+  c->nu = 0.0;
+  c->cfl = 0.1;
+  c->rampup = 100;
+  c->lambda = 1e6;
+  c->implicit_penalization = 1;
+  c->advection = CUP_ADV_UPWIND5;
+  c->mean_constraint = 1;
+  c->poisson_tol = 1e-6;
+  c->poisson_tol_rel = 1e-4;
+  c->poisson_solver = CUP_POISSON_B200;
+  c->poisson_max_iter = 1000;
+  c->poisson_max_restarts = 100;
+  c->step_2nd_start = 2;
+  c->device = 0;
+}
+
+static int parse_bc(const std::string& v) {
+  if (v == "periodic") return CUP_BC_PERIODIC;
+  if (v == "wall") return CUP_BC_WALL;
+  if (v == "freespace") return CUP_BC_FREESPACE;
+  return -1;
+}
+
+int cup_config_parse(cup_config* c, const char* args) {
+  if (!c || !args) return ctx_fail(nullptr, CUP_ERR_ARG, "cup_config_parse: null argument");
+  std::istringstream is(args);
+  std::string k, v;
+  while (is >> k) {
+    if (!(is >> v)) return ctx_fail(nullptr, CUP_ERR_ARG, "missing value for " + k);
+    std::string key = k;
+    while (!key.empty() && key[0] == '-') key.erase(0, 1);
+    char* end = nullptr;
+    const double dv = std::strtod(v.c_str(), &end);
+    const bool num = end && *end == '\0';
+    auto need_num = [&]() { return num ? 0 : ctx_fail(nullptr, CUP_ERR_ARG, "bad number for " + k); };
+    if (key == "bpdx" || key == "bpdy" || key == "bpdz") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->bpd[key[3] - 'x'] = int(dv);
+    } else if (key == "levelMax") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->level_max = int(dv);
+    } else if (key == "BC_x" || key == "BC_y" || key == "BC_z") {
+      const int bc = parse_bc(v);
+      if (bc < 0) return ctx_fail(nullptr, CUP_ERR_ARG, "BC not recognized " + v);
+      c->bc[key[3] - 'x'] = bc;
+    } else if (key == "extent") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->extent = dv;
+    } else if (key == "nu") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->nu = dv;
+    } else if (key == "CFL") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->cfl = dv;
+    } else if (key == "rampup") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->rampup = int(dv);
+    } else if (key == "lambda") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->lambda = dv;
+    } else if (key == "implicitPenalization") {
+      c->implicit_penalization = (v == "1" || v == "true");
+    } else if (key == "uinfx" || key == "uinfy" || key == "uinfz") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->uinf[key[4] - 'x'] = dv;
+    } else if (key == "advection") {
+      if (v == "upwind5" || v == "upwind3") c->advection = CUP_ADV_UPWIND5;
+      else if (v == "weno5") c->advection = CUP_ADV_WENO5;
+      else return ctx_fail(nullptr, CUP_ERR_ARG, "unknown advection scheme " + v);
+    } else if (key == "bMeanConstraint") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->mean_constraint = int(dv);
+    } else if (key == "poissonTol") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->poisson_tol = dv;
+    } else if (key == "poissonTolRel") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->poisson_tol_rel = dv;
+    } else if (key == "poissonSolver") {
+      if (v == "b200") c->poisson_solver = CUP_POISSON_B200;
+      else if (v == "b200_mixed") c->poisson_solver = CUP_POISSON_B200_MIXED;
+      else if (v == "b200_learned") c->poisson_solver = CUP_POISSON_B200_LEARNED;
+      else return ctx_fail(nullptr, CUP_ERR_ARG, "Poisson solver: \"" + v + "\" unrecognized!");
+    } else if (key == "device") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->device = int(dv);
+    } else {
+      return ctx_fail(nullptr, CUP_ERR_ARG, "unknown flag " + k);
+    }
+  }
+  return 0;
+}
+
+cup_ctx* cup_create(const cup_config* cfg) {
+  if (!cfg) {
+    ctx_fail(nullptr, CUP_ERR_ARG, "cup_create: null config");
+    return nullptr;
+  }
+  if (cfg->level_max < 1 || cfg->bpd[0] < 1 || cfg->bpd[1] < 1 || cfg->bpd[2] < 1 ||
+      !(cfg->extent > 0)) {
+    ctx_fail(nullptr, CUP_ERR_ARG, "cup_create: invalid bpd/levelMax/extent");
+    return nullptr;
+  }
+  cup_ctx* c = new cup_ctx();
+  c->cfg = *cfg;
+  if (cfg->device < 0) {  // host-only context: mesh construction and tables, no device work
+    c->host_only = true;
+    return c;
+  }
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+  if (e == cudaSuccess) e = cudaMallocHost(&c->h_pinned, 4096);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_scalars, 64 * sizeof(double));
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, cfg->device);
+  if (e != cudaSuccess) {
+    set_cuda_error(e, "cup_create", __FILE__, __LINE__);
+    cup_destroy(c);
+    return nullptr;
+  }
+  poisson_init_constants();
+  return c;
+}
+
+void cup_destroy(cup_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->mesh_arena.release();
+  c->field_arena.release();
+  c->obst_arena.release();
+  if (c->d_scalars) cudaFree(c->d_scalars);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+const char* cup_last_error(const cup_ctx* c) {
+  if (c && !c->err.empty()) return c->err.c_str();
+  return g_last_error.c_str();
+}
+
+int cup_set_mesh(cup_ctx* c, int32_t nblocks, const int32_t* level, const int32_t* index) {
+  if (!c || nblocks <= 0 || !level || !index) return ctx_fail(c, CUP_ERR_ARG, "cup_set_mesh: bad arguments");
+  std::vector<std::array<int32_t, 4>> leaves(nblocks);
+  for (int i = 0; i < nblocks; ++i) leaves[i] = {level[i], index[3 * i], index[3 * i + 1], index[3 * i + 2]};
+  return install_mesh(c, leaves);
+}
+
+static MeshSpec spec_of(const cup_ctx* c) {
+  MeshSpec s;
+  for (int d = 0; d < 3; ++d) {
+    s.bpd[d] = c->cfg.bpd[d];
+    s.bc[d] = c->cfg.bc[d];
+  }
+  s.level_max = c->cfg.level_max;
+  s.extent = c->cfg.extent;
+  mesh_spec_finalize(s);
+  return s;
+}
+
+int cup_set_mesh_uniform(cup_ctx* c) {
+  if (!c) return ctx_fail(c, CUP_ERR_ARG, "null ctx");
+  std::vector<std::array<int32_t, 4>> leaves;
+  for (int k = 0; k < c->cfg.bpd[2]; ++k)
+    for (int j = 0; j < c->cfg.bpd[1]; ++j)
+      for (int i = 0; i < c->cfg.bpd[0]; ++i) leaves.push_back({0, i, j, k});
+  return install_mesh(c, leaves);
+}
+
+int cup_set_mesh_sphere_wake(cup_ctx* c, const double* ctr, double r, int32_t flow_dir,
+                             double near_radius, double wake_len, double wake_radius) {
+  if (!c || !ctr) return ctx_fail(c, CUP_ERR_ARG, "null argument");
+  return install_mesh(c, mesh_sphere_wake_leaves(spec_of(c), ctr, r, flow_dir, near_radius,
+                                                 wake_len, wake_radius));
+}
+
+int cup_set_mesh_random(cup_ctx* c, uint64_t seed, double p) {
+  if (!c) return ctx_fail(c, CUP_ERR_ARG, "null ctx");
+  return install_mesh(c, mesh_random_leaves(spec_of(c), seed, p));
+}
+
+int32_t cup_num_blocks(const cup_ctx* c) { return c ? c->mesh.nb : 0; }
+
+int cup_get_blocks(const cup_ctx* c, int32_t* level, int32_t* index, double* h) {
+  if (!c) return ctx_fail(nullptr, CUP_ERR_ARG, "null ctx");
+  const Mesh& m = c->mesh;
+  if (level) std::memcpy(level, m.level.data(), m.nb * sizeof(int32_t));
+  if (index) std::memcpy(index, m.index.data(), 3 * m.nb * sizeof(int32_t));
+  if (h) std::memcpy(h, m.h.data(), m.nb * sizeof(double));
+  return 0;
+}
+
+int cup_get_faces(const cup_ctx* c, int32_t* kinds, int32_t* nbrs) {
+  if (!c) return ctx_fail(nullptr, CUP_ERR_ARG, "null ctx");
+  const Mesh& m = c->mesh;
+  if (kinds) std::memcpy(kinds, m.face_kind.data(), 6 * m.nb * sizeof(int32_t));
+  if (nbrs) std::memcpy(nbrs, m.face_nbr.data(), 24 * m.nb * sizeof(int32_t));
+  return 0;
+}
+
+int cup_upload_field(cup_ctx* c, int32_t field, const double* host) {
+  if (!c || !host || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_upload_field: bad arguments or no mesh");
+  int nc;
+  double* d = field_ptr(c, field, &nc);
+  if (!d) return ctx_fail(c, CUP_ERR_ARG, "unknown field id");
+  cudaError_t e = cudaMemcpyAsync(d, host, nc * nbn(c) * 8, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "upload", __FILE__, __LINE__));
+  return 0;
+}
+
+int cup_download_field(cup_ctx* c, int32_t field, double* host) {
+  if (!c || !host || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_download_field: bad arguments or no mesh");
+  int nc;
+  double* d = field_ptr(c, field, &nc);
+  if (!d) return ctx_fail(c, CUP_ERR_ARG, "unknown field id");
+  cudaError_t e = cudaMemcpyAsync(host, d, nc * nbn(c) * 8, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "download", __FILE__, __LINE__));
+  return 0;
+}
+
+double* cup_field_device_ptr(cup_ctx* c, int32_t field) {
+  if (!c) return nullptr;
+  int nc;
+  return field_ptr(c, field, &nc);
+}
+
+int cup_poisson_apply_dev(cup_ctx* c, const double* x, double* y, int32_t mean_mode) {
+  if (!c || !x || !y || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_apply_dev: bad arguments");
+  const int mm = mean_mode >= 0 ? mean_mode : c->cfg.mean_constraint;
+  if (int rc = launch_poisson_apply(c->dm, x, y, mm, c->W, c->stream)) return keep(c, rc);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "poisson_apply", __FILE__, __LINE__));
+  return 0;
+}
+
+int cup_block_inverse_dev(cup_ctx* c, const double* in, double* out) {
+  if (!c || !in || !out || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_block_inverse_dev: bad arguments");
+  if (int rc = launch_block_inverse(c->dm, in, out, c->W, c->stream)) return keep(c, rc);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "block_inverse", __FILE__, __LINE__));
+  return 0;
+}
+
+static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats) {
+  SolveParams P;
+  P.tol_abs = c->cfg.poisson_tol;
+  P.tol_rel = c->cfg.poisson_tol_rel;
+  P.max_iter = c->cfg.poisson_max_iter;
+  P.max_restarts = c->cfg.poisson_max_restarts;
+  P.mean_mode = c->cfg.mean_constraint;
+  P.check_every = 8;
+  SolveStats S{};
+  CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  if (int rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned)) return keep(c, rc);
+  CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  CUP_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  float ms = 0;
+  CUP_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  if (stats) {
+    stats->iterations = S.iterations;
+    stats->restarts = S.restarts;
+    stats->status = S.status;
+    stats->fallback = 0;
+    stats->err_init = S.err_init;
+    stats->err_final = S.err_opt;
+    stats->true_rel = S.err_init > 0 ? S.err_opt / S.err_init : 0.0;
+    stats->milliseconds = ms;
+  }
+  if (S.status == SOLVE_NAN) return ctx_fail(c, CUP_ERR_NAN, "Poisson solve produced NaN");
+  return S.status == SOLVE_CONVERGED ? CUP_OK : CUP_SOFT_MAXITER;
+}
+
+int cup_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats) {
+  if (!c || !b || !x || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve_dev: bad arguments");
+  return solve_impl(c, b, x, stats);
+}
+
+int cup_poisson_solve(cup_ctx* c, cup_solve_stats* stats) {
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve: no mesh");
+  return solve_impl(c, c->F.lhs, c->F.pres[c->F.pcur], stats);
+}
+
+}  // extern "C"

@@ -1,0 +1,76 @@
+// Internal definition of cup_ctx (the C-ABI handle).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/cup3d_b200.h"
+#include "common.cuh"
+#include "mesh.h"
+#include "poisson.cuh"
+
+namespace cup3d {
+
+struct DevArena {
+  std::vector<void*> ptrs;
+  ~DevArena() { release(); }
+  void release() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+  template <class T>
+  int alloc(T** out, size_t n) {
+    void* p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+    ptrs.push_back(p);
+    *out = static_cast<T*>(p);
+    return 0;
+  }
+};
+
+// Obstacle data on the device: per-slot chi and udef blocks, and the rigid
+// body kinematics (ObstacleBlock.h:41-42, Obstacle.h getters).
+struct DevObstacle {
+  int nslots = 0;
+  int* slot_of_block = nullptr;   // nb, -1 when the block holds no obstacle cells
+  int* block_of_slot = nullptr;   // nslots
+  double* chi = nullptr;          // nslots*512
+  double* udef = nullptr;         // 3*nslots*512 (component-major)
+  double kin[9] = {0};            // CM[3], vel[3], omega[3]
+};
+
+struct Fields {
+  double* vel[2] = {nullptr, nullptr};  // ping-pong, 3*nb*512 each
+  int vcur = 0;
+  double* tmpV = nullptr;               // 3*nb*512
+  double* pres[2] = {nullptr, nullptr}; // ping-pong pressure
+  int pcur = 0;
+  double* lhs = nullptr;
+  double* chi = nullptr;
+  double* phi = nullptr;                // Poisson unknown (increment)
+};
+
+}  // namespace cup3d
+
+struct cup_ctx {
+  cup_config cfg;
+  cup3d::Mesh mesh;
+  cup3d::DevMesh dm{};
+  cup3d::DevArena mesh_arena, field_arena, obst_arena;
+  cup3d::Fields F;
+  cup3d::PoissonWork W{};
+  cup3d::DevObstacle ob;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int* h_pinned = nullptr;        // small pinned host buffer
+  double* d_scalars = nullptr;    // 64 device doubles for misc reductions
+  int num_sms = 148;
+  bool host_only = false;         // device < 0: mesh work only
+  std::string err;
+};
+
+namespace cup3d {
+int ctx_fail(cup_ctx* c, int code, const std::string& msg);
+size_t nbn(const cup_ctx* c);
+}  // namespace cup3d

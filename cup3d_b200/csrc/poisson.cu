@@ -1,0 +1,714 @@
+// Poisson operator, exact block preconditioner and fused BiCGSTAB (FP64).
+//
+// Reference behaviour restated here:
+//   * operator rows: PoissonSolverExp::getMat / makeFlux / interpolate
+//     (PoissonSolverExp.cpp:112-373; D1/D2/Dmixed in PoissonSolverExp.h:384-478),
+//     evaluated matrix-free instead of assembled into COO;
+//   * mean constraint: hd_cusparseSpMV (BiCGSTAB.cu:392-413) and ComputeLHS
+//     (PoissonSolverAMR.h:108-172);
+//   * preconditioner: z = (1/h) P_inv p with P_inv = -(L_D)^-1 of the 8^3
+//     Dirichlet Laplacian (PoissonSolverExp.cpp:17-111, BiCGSTAB.cu:526-527),
+//     applied by fast diagonalization (three DST-I mode products each way)
+//     rather than a 512x512 DGEMM: the same matrix, 96 instead of 1024 flop/cell;
+//   * solver: BiCGSTABSolver::main (BiCGSTAB.cu:416-628) with the same
+//     scalars, restart rule and best-iterate return, but five fused kernels
+//     per iteration and no host round trip inside an iteration.
+#include <cmath>
+#include <cstring>
+
+#include "poisson.cuh"
+
+namespace cup3d {
+
+// DST-I eigenvectors of tridiag(-1,2,-1) on 8 points and their eigenvalues.
+__constant__ double c_S[64];
+__constant__ double c_lam[8];
+static bool g_consts_ready = false;
+
+void poisson_init_constants() {
+  if (g_consts_ready) return;
+  double S[64], lam[8];
+  const double pi = 3.14159265358979323846;
+  for (int j = 0; j < 8; ++j) {
+    lam[j] = 2.0 - 2.0 * std::cos(pi * (j + 1) / 9.0);
+    for (int k = 0; k < 8; ++k) S[j * 8 + k] = std::sqrt(2.0 / 9.0) * std::sin(pi * (j + 1) * (k + 1) / 9.0);
+  }
+  cudaMemcpyToSymbol(c_S, S, sizeof(S));
+  cudaMemcpyToSymbol(c_lam, lam, sizeof(lam));
+  g_consts_ready = true;
+}
+
+// ---------------------------------------------------------------------------
+// Coarse-fine interpolation of PoissonSolverExp::interpolate: the Taylor part
+// p_c + s1 D1 + s2 D2' + D2(ds1) + D2(ds2) + s1 s2 Dmixed, evaluated on one
+// coarse face layer cl[t1 + 8 t2].  Faces normal to y use ds1 = z (tan2),
+// ds2 = x (tan1); the others ds1 = tan1, ds2 = tan2 (PoissonSolverExp.h:159-371).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double cf_taylor(const double* cl, int d, int c1, int c2, double sa, double sb) {
+  int u, v;
+  double su, sv;
+  if (d == 1) {
+    u = c2; v = c1; su = sb; sv = sa;
+  } else {
+    u = c1; v = c2; su = sa; sv = sb;
+  }
+  auto L = [&](int uu, int vv) -> double { return d == 1 ? cl[vv + 8 * uu] : cl[uu + 8 * vv]; };
+  const bool bdu = (u == 7 || u == 3), fdu = (u == 0 || u == 4);
+  const bool bdv = (v == 7 || v == 3), fdv = (v == 0 || v == 4);
+  const double c = L(u, v);
+  double d1u, d1v, d2u, d2v, dm;
+  if (bdu) {
+    d1u = 1. / 8. * L(u - 2, v) - 1. / 2. * L(u - 1, v) + 3. / 8. * c;
+    d2u = 1. / 32. * L(u - 2, v) - 1. / 16. * L(u - 1, v) + 1. / 32. * c;
+  } else if (fdu) {
+    d1u = -1. / 8. * L(u + 2, v) + 1. / 2. * L(u + 1, v) - 3. / 8. * c;
+    d2u = 1. / 32. * L(u + 2, v) - 1. / 16. * L(u + 1, v) + 1. / 32. * c;
+  } else {
+    d1u = -1. / 8. * L(u - 1, v) + 1. / 8. * L(u + 1, v);
+    d2u = 1. / 32. * L(u - 1, v) + 1. / 32. * L(u + 1, v) - 1. / 16. * c;
+  }
+  if (bdv) {
+    d1v = 1. / 8. * L(u, v - 2) - 1. / 2. * L(u, v - 1) + 3. / 8. * c;
+    d2v = 1. / 32. * L(u, v - 2) - 1. / 16. * L(u, v - 1) + 1. / 32. * c;
+  } else if (fdv) {
+    d1v = -1. / 8. * L(u, v + 2) + 1. / 2. * L(u, v + 1) - 3. / 8. * c;
+    d2v = 1. / 32. * L(u, v + 2) - 1. / 16. * L(u, v + 1) + 1. / 32. * c;
+  } else {
+    d1v = -1. / 8. * L(u, v - 1) + 1. / 8. * L(u, v + 1);
+    d2v = 1. / 32. * L(u, v - 1) + 1. / 32. * L(u, v + 1) - 1. / 16. * c;
+  }
+  auto N = [&](int a, int b) { return L(u + a, v + b); };
+  if (bdu && bdv)
+    dm = 1. / 16. * (N(0, 0) + N(-1, -1) - N(-1, 0) - N(0, -1));
+  else if (fdu && bdv)
+    dm = 1. / 16. * (N(1, 0) + N(0, -1) - N(1, -1) - N(0, 0));
+  else if (bdu && fdv)
+    dm = 1. / 16. * (N(0, 1) + N(-1, 0) - N(-1, 1) - N(0, 0));
+  else if (fdu && fdv)
+    dm = 1. / 16. * (N(1, 1) + N(0, 0) - N(1, 0) - N(0, 1));
+  else if (bdu)
+    dm = 1. / 32. * (N(0, 1) + N(-1, -1) - N(0, -1) - N(-1, 1));
+  else if (fdu)
+    dm = 1. / 32. * (N(1, 1) + N(0, -1) - N(1, -1) - N(0, 1));
+  else if (bdv)
+    dm = 1. / 32. * (N(1, 0) + N(-1, -1) - N(-1, 0) - N(1, -1));
+  else if (fdv)
+    dm = 1. / 32. * (N(1, 1) + N(-1, 0) - N(-1, 1) - N(1, 0));
+  else
+    dm = 1. / 64. * (N(1, 1) + N(-1, -1) - N(1, -1) - N(-1, 1));
+  return c + su * d1u + sv * d1v + d2u + d2v + su * sv * dm;
+}
+
+// ---------------------------------------------------------------------------
+// y = A x for one mesh block.  Thread t owns cells t and t+256.  Shared:
+// lab[1000] (block + 1 ghost layer), ys[512], cl[64].
+// ---------------------------------------------------------------------------
+struct SpmvSmem {
+  double lab[1000];
+  double ys[512];
+  double cl[64];
+};
+
+__device__ __forceinline__ int lab1(int x, int y, int z) { return (x + 1) + 10 * ((y + 1) + 10 * (z + 1)); }
+
+template <class T>
+__device__ void spmv_block(const DevMesh& M, int b, const T* __restrict__ x, double mean_sum,
+                           int mean_mode, SpmvSmem& sm, double out[2]) {
+  const int t = threadIdx.x;
+  const double h = M.h[b];
+  const T* xb = x + size_t(b) * BN;
+  // interior
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int c = t + q * NT;
+    sm.lab[lab1(c & 7, (c >> 3) & 7, c >> 6)] = double(xb[c]);
+  }
+  // ghosts: same-level neighbour values; zero-flux elsewhere (own value)
+  for (int g = t; g < 384; g += NT) {
+    const int f = g >> 6, a = g & 7, bb = (g >> 3) & 7;
+    const int d = f >> 1, s = f & 1;
+    const int kind = M.fkind[b * 6 + f];
+    double v;
+    if (kind == K_SAME) {
+      const int nbk = M.fnbr[b * 24 + 4 * f];
+      v = double(x[size_t(nbk) * BN + face_cell(d, 1 - s, 0, a, bb)]);
+    } else {
+      v = double(xb[face_cell(d, s, 0, a, bb)]);
+    }
+    int q[3];
+    q[d] = s ? BS : -1;
+    q[tan1(d)] = a;
+    q[tan2(d)] = bb;
+    sm.lab[lab1(q[0], q[1], q[2])] = v;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int c = t + q * NT;
+    const int X = c & 7, Y = (c >> 3) & 7, Z = c >> 6;
+    const double* L = sm.lab;
+    sm.ys[c] = h * (L[lab1(X - 1, Y, Z)] + L[lab1(X + 1, Y, Z)] + L[lab1(X, Y - 1, Z)] +
+                    L[lab1(X, Y + 1, Z)] + L[lab1(X, Y, Z - 1)] + L[lab1(X, Y, Z + 1)] -
+                    6.0 * L[lab1(X, Y, Z)]);
+  }
+  // coarse-fine faces
+  for (int f = 0; f < 6; ++f) {
+    const int kind = M.fkind[b * 6 + f];
+    if (kind != K_COARSER && kind != K_FINER) continue;
+    const int d = f >> 1, s = f & 1;
+    const int a = t & 7, bb = (t >> 3) & 7;
+    __syncthreads();
+    if (kind == K_COARSER) {
+      const int cb = M.fnbr[b * 24 + 4 * f];
+      if (t < 64) sm.cl[t] = double(x[size_t(cb) * BN + face_cell(d, 1 - s, 0, a, bb)]);
+      __syncthreads();
+      if (t < 64) {
+        const int h1 = M.index[b * 3 + tan1(d)] & 1, h2 = M.index[b * 3 + tan2(d)] & 1;
+        const int c1 = h1 * 4 + (a >> 1), c2 = h2 * 4 + (bb >> 1);
+        const double T = cf_taylor(sm.cl, d, c1, c2, (a & 1) ? 1.0 : -1.0, (bb & 1) ? 1.0 : -1.0);
+        const int cs = face_cell(d, s, 0, a, bb), ci = face_cell(d, s, 1, a, bb);
+        const double xs = double(xb[cs]), xi = double(xb[ci]);
+        sm.ys[cs] += h * (2. / 3. * xs - 1. / 5. * xi + 8. / 15. * T - xs);
+      }
+    } else {
+      if (t < 64) sm.cl[t] = double(xb[face_cell(d, s, 0, a, bb)]);
+      __syncthreads();
+      if (t < 64) {
+        const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
+        const double hf = M.h[ch];
+        const T* xc = x + size_t(ch) * BN;
+        double acc = 0.0;
+#pragma unroll
+        for (int q4 = 0; q4 < 4; ++q4) {
+          const int f1 = q4 & 1, f2 = q4 >> 1;
+          const int fa = 2 * (a & 3) + f1, fb = 2 * (bb & 3) + f2;
+          const double close = double(xc[face_cell(d, 1 - s, 0, fa, fb)]);
+          const double far = double(xc[face_cell(d, 1 - s, 1, fa, fb)]);
+          const double T = cf_taylor(sm.cl, d, a, bb, f1 ? 1.0 : -1.0, f2 ? 1.0 : -1.0);
+          acc += hf * (close - (2. / 3. * close - 1. / 5. * far + 8. / 15. * T));
+        }
+        sm.ys[face_cell(d, s, 0, a, bb)] += acc;
+      }
+    }
+  }
+  __syncthreads();
+  if (mean_mode == 1 && b == M.mean_block && t == 0) sm.ys[0] = mean_sum;
+  if (mean_mode == 3 && b == M.mean_block && t == 0) sm.ys[0] = h * double(xb[0]);
+  __syncthreads();
+  const double h3 = h * h * h;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    out[q] = sm.ys[t + q * NT];
+    if (mean_mode == 2) out[q] += mean_sum * h3;
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// z = (1/h) P_inv v = -(1/h) L_D^-1 v on one block by fast diagonalization.
+// Thread t owns mode index k = t&7 along the transformed axis and the two
+// transverse positions (t>>3) and (t>>3)+32.  buf holds the block on entry
+// and the result on exit.
+// ---------------------------------------------------------------------------
+struct FdSmem {
+  double a[512];
+  double b[512];
+  double inv_lam[512];
+};
+
+__device__ __forceinline__ void fd_load_scale(FdSmem& sm) {
+  for (int i = threadIdx.x; i < 512; i += NT) {
+    const int kx = i & 7, ky = (i >> 3) & 7, kz = i >> 6;
+    sm.inv_lam[i] = 1.0 / (c_lam[kx] + c_lam[ky] + c_lam[kz]);
+  }
+}
+
+// one mode product along axis `ax` (0=x,1=y,2=z): out = S x_ax in
+__device__ __forceinline__ void fd_pass(const double* in, double* out, int ax, const double Srow[8]) {
+  const int t = threadIdx.x, k = t & 7;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int o = (t >> 3) + 32 * q;  // transverse pair index 0..63
+    const int p0 = o & 7, p1 = o >> 3;
+    int base, stride;
+    if (ax == 0) { base = 8 * p0 + 64 * p1; stride = 1; }
+    else if (ax == 1) { base = p0 + 64 * p1; stride = 8; }
+    else { base = p0 + 8 * p1; stride = 64; }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s = fma(Srow[i], in[base + stride * i], s);
+    out[base + stride * k] = s;
+  }
+}
+
+// in: sm.a, result in sm.a.  scale = -1/h
+__device__ __forceinline__ void fd_apply(FdSmem& sm, double scale) {
+  const int t = threadIdx.x, k = t & 7;
+  double Srow[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) Srow[i] = c_S[k * 8 + i];
+  fd_pass(sm.a, sm.b, 0, Srow);
+  __syncthreads();
+  fd_pass(sm.b, sm.a, 1, Srow);
+  __syncthreads();
+  fd_pass(sm.a, sm.b, 2, Srow);
+  __syncthreads();
+  for (int i = t; i < 512; i += NT) sm.b[i] *= scale * sm.inv_lam[i];
+  __syncthreads();
+  fd_pass(sm.b, sm.a, 0, Srow);
+  __syncthreads();
+  fd_pass(sm.a, sm.b, 1, Srow);
+  __syncthreads();
+  fd_pass(sm.b, sm.a, 2, Srow);
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// Standalone kernels
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_weighted_sum(DevMesh M, const double* __restrict__ v,
+                                                     GridReduce G, double* out, double* tgt) {
+  __shared__ double red[64];
+  double acc[2] = {0.0, 0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    const double h = M.h[b], h3 = h * h * h;
+    double s = 0.0;
+    for (int c = threadIdx.x; c < BN; c += NT) s += v[size_t(b) * BN + c];
+    acc[0] += s * h3;
+    if (threadIdx.x == 0) acc[1] += 512.0 * h3;
+  }
+  if (grid_reduce<2>(acc, G, red) && threadIdx.x == 0) {
+    if (out) { out[0] = acc[0]; out[1] = acc[1]; }
+    if (tgt) *tgt = acc[0];
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_spmv(DevMesh M, const double* __restrict__ x,
+                                             double* __restrict__ y, const double* mean_sum,
+                                             int mean_mode) {
+  __shared__ SpmvSmem sm;
+  const double ms = mean_sum ? *mean_sum : 0.0;
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    double o[2];
+    spmv_block<double>(M, b, x, ms, mean_mode, sm, o);
+    y[size_t(b) * BN + threadIdx.x] = o[0];
+    y[size_t(b) * BN + threadIdx.x + NT] = o[1];
+  }
+}
+
+__global__ void __launch_bounds__(NT) k_block_inverse(DevMesh M, const double* __restrict__ in,
+                                                      double* __restrict__ out) {
+  __shared__ FdSmem sm;
+  fd_load_scale(sm);
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    __syncthreads();
+    for (int c = threadIdx.x; c < BN; c += NT) sm.a[c] = in[size_t(b) * BN + c];
+    __syncthreads();
+    fd_apply(sm, -1.0 / M.h[b]);
+    for (int c = threadIdx.x; c < BN; c += NT) out[size_t(b) * BN + c] = sm.a[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// BiCGSTAB kernels
+// ---------------------------------------------------------------------------
+struct KArgs {
+  DevMesh M;
+  const double* b;
+  double* r;
+  double* rhat;
+  double* p;
+  double* nu;
+  double* t;
+  double* z1;
+  double* z2;
+  double* xs0;
+  double* xs1;
+  double* xs2;
+  KrylovState* st;
+  GridReduce g;
+  int mean_mode;
+};
+
+__device__ __forceinline__ double* xslot(const KArgs& A, int i) {
+  return i == 0 ? A.xs0 : (i == 1 ? A.xs1 : A.xs2);
+}
+
+// x0[mean row] = 0 (getVec, PoissonSolverExp.cpp:402-410) and sum(x0 h^3)
+__global__ void __launch_bounds__(NT) k_bicg_prepare(KArgs A) {
+  __shared__ double red[64];
+  const DevMesh& M = A.M;
+  if ((A.mean_mode == 1 || A.mean_mode == 3) && M.mean_block >= 0 && blockIdx.x == 0 && threadIdx.x == 0)
+    A.xs0[size_t(M.mean_block) * BN] = 0.0;
+  __syncthreads();
+  double acc[1] = {0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    const double h = M.h[b], h3 = h * h * h;
+    double s = 0.0;
+    for (int c = threadIdx.x; c < BN; c += NT) {
+      const size_t i = size_t(b) * BN + c;
+      s += (b == M.mean_block && c == 0 && (A.mean_mode == 1 || A.mean_mode == 3)) ? 0.0 : A.xs0[i];
+    }
+    acc[0] += s * h3;
+  }
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) A.st->mean_sum = acc[0];
+}
+
+// r = b - A x0, rhat = r, p = nu = 0; err_init = ||r||
+__global__ void __launch_bounds__(NT) k_bicg_init(KArgs A) {
+  __shared__ SpmvSmem sm;
+  __shared__ double red[64];
+  const DevMesh& M = A.M;
+  const double ms = A.st->mean_sum;
+  double acc[1] = {0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    double o[2];
+    spmv_block<double>(M, b, A.xs0, ms, A.mean_mode, sm, o);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = threadIdx.x + q * NT;
+      const size_t i = size_t(b) * BN + c;
+      double bi = A.b[i];
+      if ((A.mean_mode == 1 || A.mean_mode == 3) && b == M.mean_block && c == 0) bi = 0.0;
+      const double ri = bi - o[q];
+      A.r[i] = ri;
+      A.rhat[i] = ri;
+      A.p[i] = 0.0;
+      A.nu[i] = 0.0;
+      acc[0] += ri * ri;
+    }
+  }
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
+    KrylovState& S = *A.st;
+    const double e = sqrt(acc[0]);
+    S.err = S.err_init = S.err_opt = e;
+    S.rr = S.rr_hat = acc[0];
+    S.rho = acc[0];  // (rhat, r) of iteration 0
+    S.rho_prev = 1.0;
+    S.alpha = 1.0;
+    S.omega = 1.0;
+    S.beta = (S.rho / (S.rho_prev + S.eps)) * (S.alpha / (S.omega + S.eps));
+    S.k = 0;
+    S.restarts = 0;
+    S.cur = 0;
+    S.best = 0;
+    S.nxt = 1;
+    S.restart_pending = 0;
+    S.converged = 0;
+    S.done = 0;
+    S.status = SOLVE_RUNNING;
+    if (!(e == e)) {
+      S.done = 1;
+      S.status = SOLVE_NAN;
+    } else if (e <= S.tol_abs) {  // nothing to do (also covers b = A x0)
+      S.done = 1;
+      S.converged = 1;
+      S.status = SOLVE_CONVERGED;
+    }
+  }
+}
+
+// KA: p = r + beta (p - omega nu) (or p = r, rhat = r after a restart);
+//     z1 = M^-1 p; sum(z1 h^3)
+__global__ void __launch_bounds__(NT) k_bicg_a(KArgs A) {
+  __shared__ FdSmem sm;
+  __shared__ double red[64];
+  const KrylovState& S = *A.st;
+  if (S.done) return;
+  const double beta = S.beta, omega = S.omega;
+  const bool restart = S.restart_pending != 0;
+  const DevMesh& M = A.M;
+  fd_load_scale(sm);
+  double acc[1] = {0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = threadIdx.x + q * NT;
+      const size_t i = size_t(b) * BN + c;
+      const double ri = A.r[i];
+      double pi;
+      if (restart) {
+        pi = ri;
+        A.rhat[i] = ri;
+      } else {
+        pi = ri + beta * (A.p[i] - omega * A.nu[i]);
+      }
+      A.p[i] = pi;
+      sm.a[c] = pi;
+    }
+    __syncthreads();
+    const double h = M.h[b];
+    fd_apply(sm, -1.0 / h);
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = threadIdx.x + q * NT;
+      const double zi = sm.a[c];
+      A.z1[size_t(b) * BN + c] = zi;
+      s += zi;
+    }
+    acc[0] += s * h * h * h;
+  }
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
+    KrylovState& W = *A.st;
+    W.mean_sum = acc[0];
+    if (restart) {
+      W.rho = W.rr;
+      W.rr_hat = W.rr;
+      W.restart_pending = 0;
+    }
+  }
+}
+
+// KB: nu = A z1; alpha = rho / ((rhat, nu) + eps)
+__global__ void __launch_bounds__(NT) k_bicg_b(KArgs A) {
+  __shared__ SpmvSmem sm;
+  __shared__ double red[64];
+  const KrylovState& S = *A.st;
+  if (S.done) return;
+  const DevMesh& M = A.M;
+  const double ms = S.mean_sum;
+  double acc[1] = {0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    double o[2];
+    spmv_block<double>(M, b, A.z1, ms, A.mean_mode, sm, o);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const size_t i = size_t(b) * BN + threadIdx.x + q * NT;
+      A.nu[i] = o[q];
+      acc[0] += A.rhat[i] * o[q];
+    }
+  }
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
+    KrylovState& W = *A.st;
+    W.alpha = W.rho / (acc[0] + W.eps);
+  }
+}
+
+// KC: s = r - alpha nu (in place in r); z2 = M^-1 s; sum(z2 h^3)
+__global__ void __launch_bounds__(NT) k_bicg_c(KArgs A) {
+  __shared__ FdSmem sm;
+  __shared__ double red[64];
+  const KrylovState& S = *A.st;
+  if (S.done) return;
+  const double alpha = S.alpha;
+  const DevMesh& M = A.M;
+  fd_load_scale(sm);
+  double acc[1] = {0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = threadIdx.x + q * NT;
+      const size_t i = size_t(b) * BN + c;
+      const double si = A.r[i] - alpha * A.nu[i];
+      A.r[i] = si;
+      sm.a[c] = si;
+    }
+    __syncthreads();
+    const double h = M.h[b];
+    fd_apply(sm, -1.0 / h);
+    double s = 0.0;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = threadIdx.x + q * NT;
+      const double zi = sm.a[c];
+      A.z2[size_t(b) * BN + c] = zi;
+      s += zi;
+    }
+    acc[0] += s * h * h * h;
+  }
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) A.st->mean_sum = acc[0];
+}
+
+// KD: t = A z2; omega = (t, s) / ((t, t) + eps)
+__global__ void __launch_bounds__(NT) k_bicg_d(KArgs A) {
+  __shared__ SpmvSmem sm;
+  __shared__ double red[64];
+  const KrylovState& S = *A.st;
+  if (S.done) return;
+  const DevMesh& M = A.M;
+  const double ms = S.mean_sum;
+  double acc[2] = {0.0, 0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    double o[2];
+    spmv_block<double>(M, b, A.z2, ms, A.mean_mode, sm, o);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const size_t i = size_t(b) * BN + threadIdx.x + q * NT;
+      A.t[i] = o[q];
+      acc[0] += o[q] * A.r[i];
+      acc[1] += o[q] * o[q];
+    }
+  }
+  if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
+    KrylovState& W = *A.st;
+    W.omega = acc[0] / (acc[1] + W.eps);
+  }
+}
+
+// KE: x_new = x + alpha z1 + omega z2; r = s - omega t; (rhat, r), (r, r);
+//     convergence, best iterate, restart decision, beta for the next KA.
+__global__ void __launch_bounds__(NT) k_bicg_e(KArgs A) {
+  __shared__ double red[64];
+  const KrylovState& S = *A.st;
+  if (S.done) return;
+  const double alpha = S.alpha, omega = S.omega;
+  const double* xc = xslot(A, S.cur);
+  double* xn = xslot(A, S.nxt);
+  const DevMesh& M = A.M;
+  double acc[2] = {0.0, 0.0};
+  const size_t n = size_t(M.nb) * BN;
+  for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n; i += size_t(gridDim.x) * NT) {
+    xn[i] = (xc[i] + alpha * A.z1[i]) + omega * A.z2[i];
+    const double ri = A.r[i] - omega * A.t[i];
+    A.r[i] = ri;
+    acc[0] += A.rhat[i] * ri;
+    acc[1] += ri * ri;
+  }
+  if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
+    KrylovState& W = *A.st;
+    const double err = sqrt(acc[1]);
+    W.err = err;
+    W.rr = acc[1];
+    W.k += 1;
+    W.cur = W.nxt;
+    if (!(err == err)) {
+      W.done = 1;
+      W.status = SOLVE_NAN;
+    } else if (err < W.err_opt) {
+      W.err_opt = err;
+      W.best = W.cur;
+      if (err <= W.tol_abs || err / W.err_init <= W.tol_rel) {
+        W.done = 1;
+        W.converged = 1;
+        W.status = SOLVE_CONVERGED;
+      }
+    }
+    // next free slot: neither the current nor the best iterate
+    int nx = 0;
+    while (nx == W.cur || nx == W.best) ++nx;
+    W.nxt = nx;
+    if (!W.done && W.k >= W.max_iter) {
+      W.done = 1;
+      W.status = SOLVE_MAXITER;
+    }
+    W.rho_prev = W.rho;
+    W.rho = acc[0];
+    if (!W.done) {
+      const bool breakdown = W.rho * W.rho < 1e-16 * W.rr * W.rr_hat;
+      if (breakdown && W.max_restarts > 0) {
+        W.restarts += 1;
+        if (W.restarts >= W.max_restarts) {
+          W.done = 1;
+          W.status = SOLVE_RESTARTS;
+        } else {
+          W.restart_pending = 1;
+        }
+      }
+      W.beta = (W.rho / (W.rho_prev + W.eps)) * (W.alpha / (W.omega + W.eps));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static KArgs make_args(const DevMesh& M, const double* b, double* x, PoissonWork& W, int mean_mode,
+                       int site) {
+  KArgs A;
+  A.M = M;
+  A.b = b;
+  A.r = W.r;
+  A.rhat = W.rhat;
+  A.p = W.p;
+  A.nu = W.nu;
+  A.t = W.t;
+  A.z1 = W.z1;
+  A.z2 = W.z2;
+  A.xs0 = x;
+  A.xs1 = W.xs[1];
+  A.xs2 = W.xs[2];
+  A.st = W.st;
+  A.g.partial = W.partial;
+  A.g.counter = W.counters + site;
+  A.mean_mode = mean_mode;
+  return A;
+}
+
+int launch_weighted_sum(const DevMesh& M, const double* v, double* d_out, PoissonWork& W,
+                        cudaStream_t s) {
+  GridReduce g{W.partial, W.counters + 8};
+  k_weighted_sum<<<W.grid, NT, 0, s>>>(M, v, g, d_out, nullptr);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_mode,
+                         PoissonWork& W, cudaStream_t s) {
+  poisson_init_constants();
+  GridReduce g{W.partial, W.counters + 9};
+  double* ms = &W.st->mean_sum;
+  if (mean_mode == 1 || mean_mode == 2) {
+    k_weighted_sum<<<W.grid, NT, 0, s>>>(M, x, g, nullptr, ms);
+    CUP_CUDA_TRY(cudaGetLastError());
+  }
+  k_spmv<<<W.grid, NT, 0, s>>>(M, x, y, ms, mean_mode);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_block_inverse(const DevMesh& M, const double* in, double* out, PoissonWork& W,
+                         cudaStream_t s) {
+  poisson_init_constants();
+  k_block_inverse<<<W.grid, NT, 0, s>>>(M, in, out);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
+                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done) {
+  poisson_init_constants();
+  KrylovState init{};
+  init.tol_abs = P.tol_abs;
+  init.tol_rel = P.tol_rel;
+  init.max_iter = P.max_iter;
+  init.max_restarts = P.max_restarts;
+  init.eps = 1e-21;
+  CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  KArgs A = make_args(M, b, x, W, P.mean_mode, 0);
+  k_bicg_prepare<<<W.grid, NT, 0, s>>>(A);
+  k_bicg_init<<<W.grid, NT, 0, s>>>(A);
+  CUP_CUDA_TRY(cudaGetLastError());
+  const int chunk = P.check_every > 0 ? P.check_every : 8;
+  for (int it = 0; it < P.max_iter; it += chunk) {
+    for (int j = 0; j < chunk; ++j) {
+      k_bicg_a<<<W.grid, NT, 0, s>>>(A);
+      k_bicg_b<<<W.grid, NT, 0, s>>>(A);
+      k_bicg_c<<<W.grid, NT, 0, s>>>(A);
+      k_bicg_d<<<W.grid, NT, 0, s>>>(A);
+      k_bicg_e<<<W.grid, NT, 0, s>>>(A);
+    }
+    CUP_CUDA_TRY(cudaGetLastError());
+    CUP_CUDA_TRY(cudaMemcpyAsync(h_done, &W.st->done, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (*h_done) break;
+  }
+  KrylovState fin;
+  CUP_CUDA_TRY(cudaMemcpyAsync(&fin, W.st, sizeof(fin), cudaMemcpyDeviceToHost, s));
+  CUP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (fin.best != 0) {
+    double* src = fin.best == 1 ? W.xs[1] : W.xs[2];
+    CUP_CUDA_TRY(cudaMemcpyAsync(x, src, size_t(M.nb) * BN * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, s));
+  }
+  out.iterations = fin.k;
+  out.restarts = fin.restarts;
+  out.status = fin.done ? fin.status : SOLVE_MAXITER;
+  out.err_init = fin.err_init;
+  out.err_opt = fin.err_opt;
+  return 0;
+}
+
+}  // namespace cup3d

@@ -1,0 +1,65 @@
+// Poisson operator, block preconditioner and BiCGSTAB solver on the device.
+#pragma once
+#include "common.cuh"
+
+namespace cup3d {
+
+// Device-resident Krylov state.  Written only by the last CTA of a reduction
+// ("finalizer"), read by the kernels that follow on the same stream.
+struct KrylovState {
+  double rho, rho_prev, alpha, omega, beta;
+  double rr, rr_hat;                 // (r,r) and (rhat,rhat)
+  double err, err_init, err_opt;     // ||r||_2 now, initially, best so far
+  double tol_abs, tol_rel;
+  double mean_sum;                   // sum(v h^3) of the vector the next SpMV reads
+  double eps;
+  int k, restarts, max_restarts, max_iter;
+  int done, converged, restart_pending, status;
+  int cur, best, nxt;                // x buffer rotation (x_opt without copies)
+  int pad;
+};
+
+enum SolveStatus : int {
+  SOLVE_RUNNING = 0,
+  SOLVE_CONVERGED = 1,
+  SOLVE_MAXITER = 2,
+  SOLVE_RESTARTS = 3,
+  SOLVE_NAN = 4
+};
+
+struct PoissonWork {
+  // vectors, nb*512 each
+  double *r, *rhat, *p, *nu, *t, *z1, *z2, *xs[3];
+  KrylovState* st;
+  double* partial;          // grid * 8
+  unsigned int* counters;   // 16
+  int grid;                 // CTAs for block kernels
+};
+
+struct SolveParams {
+  double tol_abs, tol_rel;
+  int max_iter, max_restarts, mean_mode;
+  int check_every;  // host checks convergence every this many iterations
+};
+
+struct SolveStats {
+  int iterations, restarts, status;
+  double err_init, err_opt;
+};
+
+// Standalone operators (parity tests and the mixed/learned solvers).
+int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_mode,
+                         PoissonWork& W, cudaStream_t s);
+int launch_block_inverse(const DevMesh& M, const double* in, double* out, PoissonWork& W,
+                         cudaStream_t s);
+// Solves A x = b; x holds the initial guess on entry and x_opt on exit.
+int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
+                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done_pinned);
+
+// sum over cells of v*h^3 and of h^3 (zero-mean projection), into d_out[2]
+int launch_weighted_sum(const DevMesh& M, const double* v, double* d_out, PoissonWork& W,
+                        cudaStream_t s);
+
+void poisson_init_constants();
+
+}  // namespace cup3d

@@ -1,0 +1,139 @@
+/* cup3d_b200 — C ABI of the B200-native CUP3D time-step hot path.
+ *
+ * One context holds one simulation's mesh and fields on one GPU.  Every call
+ * returns an int status: 0 OK, > 0 soft (solver stopped without reaching the
+ * tolerance, fallback used), < 0 hard error (CUDA failure, bad argument, bad
+ * mesh, NaN).  cup_last_error() gives the message.  No C++ exception crosses
+ * this boundary.  A context is used by one host thread at a time.
+ *
+ * Field layout on the host side of this ABI: structure-of-arrays, component c
+ * of block b, cell (ix,iy,iz) at f[c*nb*512 + b*512 + iz*64 + iy*8 + ix], blocks
+ * in the order cup_get_blocks() reports (the space-filling-curve order set by
+ * cup_set_mesh).  cup_*_cubism variants take the reference's block layout
+ * instead (one pointer per block, VectorBlock = 512 x {u,v,w}, ScalarBlock =
+ * 512 x s, [iz][iy][ix]; Definitions.h:528-539).
+ */
+#ifndef CUP3D_B200_H
+#define CUP3D_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUP_OK 0
+#define CUP_SOFT_MAXITER 1      /* Poisson solve stopped at the iteration/restart cap */
+#define CUP_SOFT_FALLBACK 2     /* learned preconditioner stalled; block-Jacobi used */
+#define CUP_ERR_CUDA (-1)
+#define CUP_ERR_ARG (-2)
+#define CUP_ERR_MESH (-3)
+#define CUP_ERR_NAN (-4)
+#define CUP_ERR_STATE (-5)
+
+/* boundary conditions (BCflag, Definitions.h:38) */
+#define CUP_BC_FREESPACE 0
+#define CUP_BC_PERIODIC 1
+#define CUP_BC_WALL 2
+
+/* advection schemes (AdvectionDiffusion.cpp:32-103) */
+#define CUP_ADV_UPWIND5 0
+#define CUP_ADV_WENO5 1
+
+/* Poisson solvers selectable by -poissonSolver (PoissonSolverBase.cpp:30-52) */
+#define CUP_POISSON_B200 0          /* "b200": FP64 BiCGSTAB, exact block inverse */
+#define CUP_POISSON_B200_MIXED 1    /* "b200_mixed": FP32 inner, FP64 refinement */
+#define CUP_POISSON_B200_LEARNED 2  /* "b200_learned": CNN preconditioner, flexible */
+
+/* field ids */
+#define CUP_FIELD_VEL 0   /* 3 components */
+#define CUP_FIELD_PRES 1
+#define CUP_FIELD_CHI 2
+#define CUP_FIELD_LHS 3   /* Poisson right-hand side (sim.lhs) */
+#define CUP_FIELD_TMPV 4  /* 3 components */
+
+typedef struct cup_ctx cup_ctx;
+
+/* Run parameters; names follow the reference's command-line flags
+ * (SimulationData.cpp:21-132). */
+typedef struct cup_config {
+  int32_t bpd[3];              /* -bpdx -bpdy -bpdz */
+  int32_t level_max;           /* -levelMax */
+  int32_t bc[3];               /* -BC_x -BC_y -BC_z */
+  double extent;               /* -extent (largest side) */
+  double nu;                   /* -nu */
+  double cfl;                  /* -CFL */
+  int32_t rampup;              /* -rampup */
+  double lambda;               /* -lambda */
+  int32_t implicit_penalization; /* -implicitPenalization */
+  double uinf[3];              /* frame velocity sim.uinf */
+  int32_t advection;           /* CUP_ADV_* */
+  int32_t mean_constraint;     /* -bMeanConstraint */
+  double poisson_tol;          /* -poissonTol (absolute, on ||r||_2) */
+  double poisson_tol_rel;      /* -poissonTolRel */
+  int32_t poisson_solver;      /* CUP_POISSON_* */
+  int32_t poisson_max_iter;    /* 1000 in the reference */
+  int32_t poisson_max_restarts;/* 100 in the reference */
+  int32_t step_2nd_start;      /* 2 in the reference */
+  int32_t device;              /* CUDA device ordinal */
+} cup_config;
+
+typedef struct cup_solve_stats {
+  int32_t iterations;
+  int32_t restarts;
+  int32_t status;      /* 1 converged, 2 iteration cap, 3 restart cap, 4 NaN */
+  int32_t fallback;    /* learned solver fell back to block-Jacobi */
+  double err_init;     /* ||b - A x0||_2 */
+  double err_final;    /* best ||r||_2 (the iterate returned) */
+  double true_rel;     /* FP64 ||b - A x||_2 / ||b - A x0||_2 of the returned x */
+  double milliseconds; /* device time of the solve */
+} cup_solve_stats;
+
+/* Defaults of the reference (SimulationData.cpp:21-132) and the "b200" solver. */
+void cup_config_default(cup_config* cfg);
+/* ParseArguments-style: "-key value" pairs, e.g. "-bpdx 4 -levelMax 2 -nu 0.01". */
+int cup_config_parse(cup_config* cfg, const char* args);
+
+cup_ctx* cup_create(const cup_config* cfg);      /* NULL on failure: cup_last_error(NULL) */
+void cup_destroy(cup_ctx* ctx);
+const char* cup_last_error(const cup_ctx* ctx);  /* ctx may be NULL */
+
+/* ---- mesh (host C++: ordering, neighbour tables; Cubism's role) ---- */
+/* Leaf blocks in any order: level[n], index[3n].  Reordered along the
+ * space-filling curve; fields are reallocated and zeroed. */
+int cup_set_mesh(cup_ctx* ctx, int32_t nblocks, const int32_t* level, const int32_t* index);
+/* Uniform mesh at level 0 of cfg->bpd. */
+int cup_set_mesh_uniform(cup_ctx* ctx);
+/* Refined around a sphere (centre c, radius r) and its wake along flow_dir
+ * (+1/-1 in x), refined to level_max-1, 2:1 balanced. */
+int cup_set_mesh_sphere_wake(cup_ctx* ctx, const double* c, double r, int32_t flow_dir,
+                             double near_radius, double wake_len, double wake_radius);
+/* Random 2:1-balanced refinement (tests). */
+int cup_set_mesh_random(cup_ctx* ctx, uint64_t seed, double refine_prob);
+int32_t cup_num_blocks(const cup_ctx* ctx);
+/* level[n], index[3n], h[n] in device order; any pointer may be NULL */
+int cup_get_blocks(const cup_ctx* ctx, int32_t* level, int32_t* index, double* h);
+/* face tables: kinds[6n] (0 same, 1 boundary, 2 coarser, 3 finer), nbrs[24n] */
+int cup_get_faces(const cup_ctx* ctx, int32_t* kinds, int32_t* nbrs);
+
+/* ---- fields ---- */
+int cup_upload_field(cup_ctx* ctx, int32_t field, const double* host);
+int cup_download_field(cup_ctx* ctx, int32_t field, double* host);
+/* Device pointer of a field (SoA), for zero-copy use by device-resident callers. */
+double* cup_field_device_ptr(cup_ctx* ctx, int32_t field);
+
+/* ---- raw device-side operators on caller device buffers (nb*512 doubles) ---- */
+/* y = A x: the AMR Poisson operator of PoissonSolverExp::getMat with the
+ * mean constraint of the config (or mean_mode >= 0 to override). */
+int cup_poisson_apply_dev(cup_ctx* ctx, const double* d_x, double* d_y, int32_t mean_mode);
+/* out = (1/h) P_inv in per block (the preconditioner of BiCGSTAB.cu:526-527). */
+int cup_block_inverse_dev(cup_ctx* ctx, const double* d_in, double* d_out);
+/* Solves A x = b on device buffers; x: initial guess in, solution out. */
+int cup_poisson_solve_dev(cup_ctx* ctx, const double* d_b, double* d_x, cup_solve_stats* stats);
+
+/* ---- PoissonSolverBase::solve(): RHS in CUP_FIELD_LHS, guess and result in CUP_FIELD_PRES ---- */
+int cup_poisson_solve(cup_ctx* ctx, cup_solve_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

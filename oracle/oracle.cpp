@@ -1,0 +1,1489 @@
+// CPU FP64 oracle (test infrastructure only; see oracle.h for the contract).
+// Every function names the reference file:line it restates.
+#include "oracle.h"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+constexpr int BS = 8;
+constexpr int BN = 512;
+
+enum { K_SAME = 0, K_BOUNDARY = 1, K_COARSER = 2, K_FINER = 3 };
+enum { BC_FREESPACE = 0, BC_PERIODIC = 1, BC_WALL = 2 };
+
+inline int tan1(int d) { return d == 0 ? 1 : 0; }
+inline int tan2(int d) { return d == 2 ? 1 : 2; }
+inline int cell(int x, int y, int z) { return x + BS * y + BS * BS * z; }
+
+}  // namespace
+
+struct orc_mesh {
+  int nb = 0;
+  int bpd[3] = {1, 1, 1};
+  int level_max = 1;
+  int bc[3] = {0, 0, 0};
+  double h0 = 0, hmin = 0;
+  std::vector<int> level;
+  std::vector<std::array<int, 3>> idx;
+  std::vector<double> h;
+  std::vector<std::array<int, 6>> kind;
+  std::vector<std::array<std::array<int, 4>, 6>> nbr;
+  int mean_block = -1;
+  std::map<std::array<int, 4>, int> lookup;  // independent of the product's hash table
+  struct CSR {
+    std::vector<int64_t> rowptr, col;
+    std::vector<double> val;
+  };
+  CSR csr[4];  // assembled operator per mean-constraint mode (filled on first use)
+
+  int find(int l, int i, int j, int k) const {
+    auto it = lookup.find({l, i, j, k});
+    return it == lookup.end() ? -1 : it->second;
+  }
+  // Znei lookup with periodic wrap (Cubism BlockInfo::Znei semantics).
+  bool nei_index(int b, int d, int side, int n[3]) const {
+    const int l = level[b];
+    for (int e = 0; e < 3; ++e) n[e] = idx[b][e];
+    n[d] += side ? 1 : -1;
+    const int N = bpd[d] << l;
+    if (n[d] < 0 || n[d] >= N) {
+      if (bc[d] != BC_PERIODIC) return false;
+      n[d] = (n[d] + N) % N;
+    }
+    return true;
+  }
+};
+
+extern "C" orc_mesh* orc_mesh_create(int nb, const int32_t* level, const int32_t* index,
+                                     const int32_t* bpd, int level_max, const int32_t* bc,
+                                     double extent) {
+  orc_mesh* m = new orc_mesh();
+  m->nb = nb;
+  for (int d = 0; d < 3; ++d) {
+    m->bpd[d] = bpd[d];
+    m->bc[d] = bc[d];
+  }
+  m->level_max = level_max;
+  // SimulationData.cpp:141-165
+  const int aux = 1 << (level_max - 1);
+  const double nfe[3] = {double(bpd[0]) * aux * BS, double(bpd[1]) * aux * BS,
+                         double(bpd[2]) * aux * BS};
+  const double maxbpd = std::max({nfe[0], nfe[1], nfe[2]});
+  const double ex0 = (nfe[0] / maxbpd) * extent;
+  m->hmin = ex0 / nfe[0];
+  m->h0 = ex0 * aux / nfe[0];
+  m->level.resize(nb);
+  m->idx.resize(nb);
+  m->h.resize(nb);
+  for (int b = 0; b < nb; ++b) {
+    m->level[b] = level[b];
+    m->idx[b] = {index[3 * b], index[3 * b + 1], index[3 * b + 2]};
+    m->h[b] = std::ldexp(m->h0, -level[b]);
+    if (!m->lookup.emplace(std::array<int, 4>{level[b], index[3 * b], index[3 * b + 1],
+                                              index[3 * b + 2]},
+                           b)
+             .second) {
+      delete m;
+      return nullptr;
+    }
+    if (index[3 * b] == 0 && index[3 * b + 1] == 0 && index[3 * b + 2] == 0) m->mean_block = b;
+  }
+  m->kind.resize(nb);
+  m->nbr.resize(nb);
+  for (int b = 0; b < nb; ++b) {
+    const int l = m->level[b];
+    for (int d = 0; d < 3; ++d)
+      for (int side = 0; side < 2; ++side) {
+        const int f = 2 * d + side;
+        m->nbr[b][f] = {-1, -1, -1, -1};
+        int n[3];
+        if (!m->nei_index(b, d, side, n)) {
+          m->kind[b][f] = K_BOUNDARY;
+          m->nbr[b][f][0] = m->bc[d];
+          continue;
+        }
+        int id = m->find(l, n[0], n[1], n[2]);
+        if (id >= 0) {
+          m->kind[b][f] = K_SAME;
+          m->nbr[b][f][0] = id;
+          continue;
+        }
+        id = l > 0 ? m->find(l - 1, n[0] / 2, n[1] / 2, n[2] / 2) : -1;
+        if (id >= 0) {
+          m->kind[b][f] = K_COARSER;
+          m->nbr[b][f][0] = id;
+          continue;
+        }
+        m->kind[b][f] = K_FINER;
+        const int t1 = tan1(d), t2 = tan2(d);
+        for (int bb = 0; bb < 2; ++bb)
+          for (int aa = 0; aa < 2; ++aa) {
+            int c[3];
+            c[d] = 2 * n[d] + (side == 0 ? 1 : 0);
+            c[t1] = 2 * n[t1] + aa;
+            c[t2] = 2 * n[t2] + bb;
+            const int ch = m->find(l + 1, c[0], c[1], c[2]);
+            if (ch < 0) {
+              delete m;
+              return nullptr;
+            }
+            m->nbr[b][f][aa + 2 * bb] = ch;
+          }
+      }
+  }
+  return m;
+}
+
+extern "C" void orc_mesh_destroy(orc_mesh* m) { delete m; }
+extern "C" int orc_mesh_nb(const orc_mesh* m) { return m->nb; }
+extern "C" double orc_mesh_h(const orc_mesh* m, int b) { return m->h[b]; }
+extern "C" double orc_mesh_hmin(const orc_mesh* m) { return m->hmin; }
+extern "C" void orc_mesh_faces(const orc_mesh* m, int32_t* kinds, int32_t* nbrs) {
+  for (int b = 0; b < m->nb; ++b)
+    for (int f = 0; f < 6; ++f) {
+      kinds[6 * b + f] = m->kind[b][f];
+      for (int q = 0; q < 4; ++q) nbrs[24 * b + 4 * f + q] = m->nbr[b][f][q];
+    }
+}
+
+// ============================================================================
+// Poisson matrix rows, PoissonSolverExp.cpp:112-373 and PoissonSolverExp.h:63-478
+// ============================================================================
+namespace {
+
+using Row = std::map<int64_t, double>;  // SpRowInfo::mapColVal accumulates per column
+
+struct FaceIdx {
+  // Indexer for the face normal to d on side `side` of a block (the reference's
+  // [XYZ]{min,max}Indexer), plus the Taylor-direction convention
+  // X: ds1=y, ds2=z; Y: ds1=z, ds2=x; Z: ds1=x, ds2=y.
+  int d, side;
+  int ds(int which) const {  // dimension of ds1 (which=1) or ds2 (which=2)
+    if (d == 0) return which == 1 ? 1 : 2;
+    if (d == 1) return which == 1 ? 2 : 0;
+    return which == 1 ? 0 : 1;
+  }
+};
+
+inline int64_t gidx(int b, int x, int y, int z) { return int64_t(b) * BN + cell(x, y, z); }
+
+// taylorSign: parity of the fine cell index along ds (XbaseIndexer etc.)
+inline double taylor_sign(const FaceIdx& F, const int c[3], int which) {
+  return (c[F.ds(which)] % 2 == 0) ? -1.0 : 1.0;
+}
+inline bool isBD(const FaceIdx& F, const int c[3], int which) {
+  const int v = c[F.ds(which)];
+  return v == BS - 1 || v == BS / 2 - 1;
+}
+inline bool isFD(const FaceIdx& F, const int c[3], int which) {
+  const int v = c[F.ds(which)];
+  return v == 0 || v == BS / 2;
+}
+// Nei(info, ix, iy, iz, dist1, dist2)
+inline int64_t nei(int b, const FaceIdx& F, const int c[3], int d1, int d2) {
+  int q[3] = {c[0], c[1], c[2]};
+  q[F.ds(1)] += d1;
+  q[F.ds(2)] += d2;
+  return gidx(b, q[0], q[1], q[2]);
+}
+
+struct Coef {
+  int64_t idx;
+  double v;
+};
+
+// D1 (PoissonSolverExp.h:384-405), scaled by h/4
+std::array<Coef, 3> D1(int b, const FaceIdx& F, const int c[3], int which) {
+  const int s1 = which == 1, s2 = which == 2;
+  auto N = [&](int k) { return nei(b, F, c, s1 * k, s2 * k); };
+  const int64_t self = gidx(b, c[0], c[1], c[2]);
+  if (isBD(F, c, which)) return {{{N(-2), 1. / 8.}, {N(-1), -1. / 2.}, {self, 3. / 8.}}};
+  if (isFD(F, c, which)) return {{{N(2), -1. / 8.}, {N(1), 1. / 2.}, {self, -3. / 8.}}};
+  return {{{N(-1), -1. / 8.}, {N(1), 1. / 8.}, {self, 0.}}};
+}
+// D2 (PoissonSolverExp.h:407-428), scaled by 0.5*(h/4)^2
+std::array<Coef, 3> D2(int b, const FaceIdx& F, const int c[3], int which) {
+  const int s1 = which == 1, s2 = which == 2;
+  auto N = [&](int k) { return nei(b, F, c, s1 * k, s2 * k); };
+  const int64_t self = gidx(b, c[0], c[1], c[2]);
+  if (isBD(F, c, which)) return {{{N(-2), 1. / 32.}, {N(-1), -1. / 16.}, {self, 1. / 32.}}};
+  if (isFD(F, c, which)) return {{{N(2), 1. / 32.}, {N(1), -1. / 16.}, {self, 1. / 32.}}};
+  return {{{N(-1), 1. / 32.}, {N(1), 1. / 32.}, {self, -1. / 16.}}};
+}
+// Dmixed (PoissonSolverExp.h:430-478), scaled by (h/4)^2
+std::array<Coef, 4> Dm(int b, const FaceIdx& F, const int c[3]) {
+  auto N = [&](int a, int bb) { return nei(b, F, c, a, bb); };
+  const bool bd1 = isBD(F, c, 1), bd2 = isBD(F, c, 2), fd1 = isFD(F, c, 1), fd2 = isFD(F, c, 2);
+  if (bd1 && bd2)
+    return {{{N(0, 0), 1. / 16.}, {N(-1, -1), 1. / 16.}, {N(-1, 0), -1. / 16.}, {N(0, -1), -1. / 16.}}};
+  if (fd1 && bd2)
+    return {{{N(1, 0), 1. / 16.}, {N(0, -1), 1. / 16.}, {N(1, -1), -1. / 16.}, {N(0, 0), -1. / 16.}}};
+  if (bd1 && fd2)
+    return {{{N(0, 1), 1. / 16.}, {N(-1, 0), 1. / 16.}, {N(-1, 1), -1. / 16.}, {N(0, 0), -1. / 16.}}};
+  if (fd1 && fd2)
+    return {{{N(1, 1), 1. / 16.}, {N(0, 0), 1. / 16.}, {N(1, 0), -1. / 16.}, {N(0, 1), -1. / 16.}}};
+  if (bd1)
+    return {{{N(0, 1), 1. / 32.}, {N(-1, -1), 1. / 32.}, {N(0, -1), -1. / 32.}, {N(-1, 1), -1. / 32.}}};
+  if (fd1)
+    return {{{N(1, 1), 1. / 32.}, {N(0, -1), 1. / 32.}, {N(1, -1), -1. / 32.}, {N(0, 1), -1. / 32.}}};
+  if (bd2)
+    return {{{N(1, 0), 1. / 32.}, {N(-1, -1), 1. / 32.}, {N(-1, 0), -1. / 32.}, {N(1, -1), -1. / 32.}}};
+  if (fd2)
+    return {{{N(1, 1), 1. / 32.}, {N(-1, 0), 1. / 32.}, {N(-1, 1), -1. / 32.}, {N(1, 0), -1. / 32.}}};
+  return {{{N(1, 1), 1. / 64.}, {N(-1, -1), 1. / 64.}, {N(1, -1), -1. / 64.}, {N(-1, 1), -1. / 64.}}};
+}
+
+// PoissonSolverExp::interpolate (PoissonSolverExp.cpp:112-155)
+void interpolate(int bc_, const int cc[3], double hf, int64_t fine_close, int64_t fine_far,
+                 double sign, double sds1, double sds2, const FaceIdx& F, Row& row) {
+  row[fine_close] += sign * hf * 2. / 3.;
+  row[fine_far] += -sign * hf * 1. / 5.;
+  const double tf = sign * hf * 8. / 15.;
+  row[gidx(bc_, cc[0], cc[1], cc[2])] += tf;
+  for (const auto& e : D1(bc_, F, cc, 1)) row[e.idx] += sds1 * tf * e.v;
+  for (const auto& e : D1(bc_, F, cc, 2)) row[e.idx] += sds2 * tf * e.v;
+  for (const auto& e : D2(bc_, F, cc, 1)) row[e.idx] += tf * e.v;
+  for (const auto& e : D2(bc_, F, cc, 2)) row[e.idx] += tf * e.v;
+  for (const auto& e : Dm(bc_, F, cc)) row[e.idx] += sds1 * sds2 * tf * e.v;
+}
+
+// PoissonSolverExp::makeFlux (PoissonSolverExp.cpp:157-219)
+void make_flux(const orc_mesh& m, int b, const int c[3], int d, int side, Row& row) {
+  const FaceIdx F{d, side};
+  const int f = 2 * d + side;
+  const int64_t self = gidx(b, c[0], c[1], c[2]);
+  const int k = m.kind[b][f];
+  if (k == K_SAME) {
+    const int nb_ = m.nbr[b][f][0];
+    int q[3] = {c[0], c[1], c[2]};
+    q[d] = side ? 0 : BS - 1;  // neiUnif: Xmax of the minus neighbour, Xmin of the plus one
+    const double h = m.h[nb_];
+    row[gidx(nb_, q[0], q[1], q[2])] += h;
+    row[self] += -h;
+  } else if (k == K_COARSER) {
+    const int bc_ = m.nbr[b][f][0];
+    int cc[3];
+    for (int e = 0; e < 3; ++e)
+      cc[e] = (m.idx[b][e] % 2 == 0) ? (c[e] / 2) : (c[e] / 2 + BS / 2);
+    cc[d] = side ? 0 : BS - 1;  // ix_c override of XminIndexer / XmaxIndexer
+    int q[3] = {c[0], c[1], c[2]};
+    q[d] += side ? -1 : 1;  // neiInward
+    const double sds1 = taylor_sign(F, c, 1), sds2 = taylor_sign(F, c, 2);
+    const double h = m.h[b];
+    interpolate(bc_, cc, h, self, gidx(b, q[0], q[1], q[2]), 1., sds1, sds2, F, row);
+    row[self] += -h;
+  } else if (k == K_FINER) {
+    const int t1 = F.ds(1), t2 = F.ds(2);
+    // Zchild: the child touching us; its tangential halves follow our cell index
+    const int a1 = c[tan1(d)] >= BS / 2, a2 = c[tan2(d)] >= BS / 2;
+    const int ch = m.nbr[b][f][a1 + 2 * a2];
+    const double h = m.h[ch];
+    // neiFine1..4 with (sign_ds1, sign_ds2) = (-,-), (+,-), (-,+), (+,+)
+    for (int q4 = 0; q4 < 4; ++q4) {
+      const int e1 = q4 & 1, e2 = q4 >> 1;
+      int fc[3], ff[3];
+      for (int e = 0; e < 3; ++e) fc[e] = (c[e] % (BS / 2)) * 2;
+      fc[t1] += e1;
+      fc[t2] += e2;
+      fc[d] = side ? 0 : BS - 1;  // Xmin / Xmax of the child, offset 0
+      for (int e = 0; e < 3; ++e) ff[e] = fc[e];
+      ff[d] = side ? 1 : BS - 2;  // offset 1
+      const int64_t close = gidx(ch, fc[0], fc[1], fc[2]);
+      const int64_t far = gidx(ch, ff[0], ff[1], ff[2]);
+      row[close] += h;
+      interpolate(b, c, h, close, far, -1., e1 ? 1. : -1., e2 ? 1. : -1., F, row);
+    }
+  }
+}
+
+// getMat (PoissonSolverExp.cpp:221-373): row `r` of block b
+void poisson_row(const orc_mesh& m, int mean_constraint, int b, int x, int y, int z, Row& row) {
+  const double h = m.h[b];
+  const int64_t self = gidx(b, x, y, z);
+  if (mean_constraint == 3 && b == m.mean_block && x == 0 && y == 0 && z == 0) {
+    row[self] += h;
+    return;
+  }
+  const int c[3] = {x, y, z};
+  for (int d = 0; d < 3; ++d)
+    for (int side = 0; side < 2; ++side) {
+      const bool valid = side ? c[d] < BS - 1 : c[d] > 0;
+      if (valid) {
+        int q[3] = {x, y, z};
+        q[d] += side ? 1 : -1;
+        row[gidx(b, q[0], q[1], q[2])] += h;
+        row[self] += -h;
+      } else if (m.kind[b][2 * d + side] != K_BOUNDARY) {
+        make_flux(m, b, c, d, side, row);
+      }
+    }
+}
+
+}  // namespace
+
+extern "C" int64_t orc_poisson_nnz(orc_mesh* m, int mean_constraint) {
+  int64_t nnz = 0;
+#pragma omp parallel for reduction(+ : nnz) schedule(dynamic, 4)
+  for (int b = 0; b < m->nb; ++b)
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) {
+          Row row;
+          poisson_row(*m, mean_constraint, b, x, y, z, row);
+          nnz += int64_t(row.size());
+        }
+  return nnz;
+}
+
+extern "C" void orc_poisson_csr(orc_mesh* m, int mean_constraint, int64_t* rowptr, int64_t* col,
+                                double* val) {
+  int64_t p = 0;
+  rowptr[0] = 0;
+  for (int b = 0; b < m->nb; ++b)
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) {
+          Row row;
+          poisson_row(*m, mean_constraint, b, x, y, z, row);
+          for (const auto& e : row) {
+            col[p] = e.first;
+            val[p] = e.second;
+            ++p;
+          }
+          rowptr[int64_t(b) * BN + cell(x, y, z) + 1] = p;
+        }
+}
+
+namespace {
+// CSR of the operator, cached inside the mesh per mean_constraint mode.
+const orc_mesh::CSR& get_csr(orc_mesh* m, int mc) {
+  orc_mesh::CSR* c = &m->csr[mc & 3];
+  if (c->rowptr.empty()) {
+    const int64_t n = int64_t(m->nb) * BN;
+    const int64_t nnz = orc_poisson_nnz(m, mc);
+    c->rowptr.resize(n + 1);
+    c->col.resize(nnz);
+    c->val.resize(nnz);
+    orc_poisson_csr(m, mc, c->rowptr.data(), c->col.data(), c->val.data());
+  }
+  return *c;
+}
+
+// A x with the mean constraint of ComputeLHS (PoissonSolverAMR.h:108-172) /
+// hd_cusparseSpMV (BiCGSTAB.cu:392-413): mode 1 replaces row (0,0,0) of the
+// index-(0,0,0) block by sum(x h^3), mode 2 adds sum(x h^3) h^3 to every row.
+void apply_A(orc_mesh* m, int mc, const double* x, double* y) {
+  const orc_mesh::CSR& A = get_csr(m, mc);
+  const int64_t n = int64_t(m->nb) * BN;
+#pragma omp parallel for schedule(static)
+  for (int64_t r = 0; r < n; ++r) {
+    double s = 0;
+    for (int64_t p = A.rowptr[r]; p < A.rowptr[r + 1]; ++p) s += A.val[p] * x[A.col[p]];
+    y[r] = s;
+  }
+  if (mc == 1 || mc == 2) {
+    double avg = 0;
+#pragma omp parallel for reduction(+ : avg) schedule(static)
+    for (int b = 0; b < m->nb; ++b) {
+      const double h3 = m->h[b] * m->h[b] * m->h[b];
+      for (int i = 0; i < BN; ++i) avg += x[int64_t(b) * BN + i] * h3;
+    }
+    if (mc == 1) {
+      if (m->mean_block >= 0) y[int64_t(m->mean_block) * BN] = avg;
+    } else {
+#pragma omp parallel for schedule(static)
+      for (int b = 0; b < m->nb; ++b) {
+        const double h3 = m->h[b] * m->h[b] * m->h[b];
+        for (int i = 0; i < BN; ++i) y[int64_t(b) * BN + i] += avg * h3;
+      }
+    }
+  }
+}
+}  // namespace
+
+extern "C" void orc_poisson_apply(orc_mesh* m, int mean_constraint, const double* x, double* y) {
+  apply_A(m, mean_constraint, x, y);
+}
+
+// ============================================================================
+// Block preconditioners
+// ============================================================================
+
+// PoissonSolverExp ctor (PoissonSolverExp.cpp:17-111): P_inv = -(L_D)^-1 for the
+// 8^3 Dirichlet 7-point operator L_D (6 on the diagonal, -1 per face neighbour),
+// via Cholesky-Crout and a Gauss-Jordan inverse of the factor.
+extern "C" void orc_pinv(double* P) {
+  const int n = BN;
+  auto A = [](int i, int j) -> double {
+    if (i == j) return 6.;
+    const int ix = i % BS, iy = (i / BS) % BS, iz = i / (BS * BS);
+    const int jx = j % BS, jy = (j / BS) % BS, jz = j / (BS * BS);
+    return (std::abs(ix - jx) + std::abs(iy - jy) + std::abs(iz - jz)) == 1 ? -1. : 0.;
+  };
+  std::vector<double> L(size_t(n) * n, 0.0), Li(size_t(n) * n, 0.0);
+  for (int i = 0; i < n; ++i) Li[size_t(i) * n + i] = 1.;
+  for (int i = 0; i < n; ++i) {
+    double s1 = 0;
+    for (int k = 0; k < i; ++k) s1 += L[size_t(i) * n + k] * L[size_t(i) * n + k];
+    L[size_t(i) * n + i] = std::sqrt(A(i, i) - s1);
+    for (int j = i + 1; j < n; ++j) {
+      double s2 = 0;
+      for (int k = 0; k < i; ++k) s2 += L[size_t(i) * n + k] * L[size_t(j) * n + k];
+      L[size_t(j) * n + i] = (A(j, i) - s2) / L[size_t(i) * n + i];
+    }
+  }
+  for (int br = 0; br < n; ++br) {
+    const double bsf = 1. / L[size_t(br) * n + br];
+    for (int c = 0; c <= br; ++c) Li[size_t(br) * n + c] *= bsf;
+    for (int wr = br + 1; wr < n; ++wr) {
+      const double wsf = L[size_t(wr) * n + br];
+      for (int c = 0; c <= br; ++c) Li[size_t(wr) * n + c] -= wsf * Li[size_t(br) * n + c];
+    }
+  }
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double aux = 0;
+      for (int k = std::max(i, j); k < n; ++k) aux += Li[size_t(k) * n + i] * Li[size_t(k) * n + j];
+      P[size_t(i) * n + j] = -aux;
+    }
+}
+
+// z = (1/h) P_inv p per block (cublasDgemm + blockDscal, BiCGSTAB.cu:526-527)
+extern "C" void orc_precond_pinv(orc_mesh* m, const double* P, const double* in, double* out) {
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < m->nb; ++b) {
+    const double invh = 1.0 / m->h[b];
+    const double* pi = in + int64_t(b) * BN;
+    double* po = out + int64_t(b) * BN;
+    for (int i = 0; i < BN; ++i) {
+      double s = 0;
+      for (int j = 0; j < BN; ++j) s += P[size_t(i) * BN + j] * pi[j];
+      po[i] = invh * s;
+    }
+  }
+}
+
+// Per-block CG on the zero-padded 7-point Laplacian, getZImplParallel and
+// kernelPoissonGetZInner (PoissonSolverAMRKernels.cpp:76-80,177-332).
+extern "C" void orc_precond_cg(orc_mesh* m, const double* in, double* out) {
+  constexpr double kDivEps = 1e-55;
+  constexpr double kRel2 = 1e-7 * 1e-7, kAbs2 = 1e-16 * 1e-16;
+  constexpr double N = BN;
+#pragma omp parallel
+  {
+    std::vector<double> r(BN), Ax(BN), p(10 * 10 * 10, 0.0);
+    auto P = [&](int x, int y, int z) -> double& { return p[(x + 1) + 10 * ((y + 1) + 10 * (z + 1))]; };
+#pragma omp for schedule(static)
+    for (int b = 0; b < m->nb; ++b) {
+      const double invh = 1.0 / m->h[b];
+      const double* blk = in + int64_t(b) * BN;
+      double* z = out + int64_t(b) * BN;
+      double rr = 0;
+      for (int zz = 0; zz < BS; ++zz)
+        for (int y = 0; y < BS; ++y)
+          for (int x = 0; x < BS; ++x) {
+            const int i = cell(x, y, zz);
+            r[i] = invh * blk[i];
+            rr += r[i] * r[i];
+            P(x, y, zz) = r[i];
+            z[i] = 0;
+          }
+      const double sqrNorm0 = rr / (N * N);
+      if (sqrNorm0 < 1e-32) continue;
+      for (int k = 0; k < 100; ++k) {
+        double a2 = 0;
+        for (int zz = 0; zz < BS; ++zz)
+          for (int y = 0; y < BS; ++y)
+            for (int x = 0; x < BS; ++x) {
+              const int i = cell(x, y, zz);
+              Ax[i] = P(x - 1, y, zz) + P(x + 1, y, zz) + P(x, y - 1, zz) + P(x, y + 1, zz) +
+                      P(x, y, zz - 1) + P(x, y, zz + 1) - 6 * P(x, y, zz);
+              a2 += P(x, y, zz) * Ax[i];
+            }
+        const double a = rr / (a2 + kDivEps);
+        double sqrSum = 0;
+        for (int zz = 0; zz < BS; ++zz)
+          for (int y = 0; y < BS; ++y)
+            for (int x = 0; x < BS; ++x) {
+              const int i = cell(x, y, zz);
+              z[i] += a * P(x, y, zz);
+              r[i] -= a * Ax[i];
+              sqrSum += r[i] * r[i];
+            }
+        const double beta = sqrSum / (rr + kDivEps);
+        const double sqrNorm = sqrSum / (N * N);
+        if (sqrNorm < kRel2 * sqrNorm0 || sqrNorm < kAbs2) break;
+        for (int zz = 0; zz < BS; ++zz)
+          for (int y = 0; y < BS; ++y)
+            for (int x = 0; x < BS; ++x) P(x, y, zz) = r[cell(x, y, zz)] + beta * P(x, y, zz);
+        rr = sqrSum;
+      }
+      // reset the interior of the padded block for the next block on this thread
+      std::fill(p.begin(), p.end(), 0.0);
+    }
+  }
+}
+
+// ============================================================================
+// Krylov solvers
+// ============================================================================
+namespace {
+struct Precond {
+  orc_mesh* m;
+  int kind;  // 0 exact block inverse, 1 block CG
+  std::vector<double> P;
+  Precond(orc_mesh* mm, int k) : m(mm), kind(k) {
+    if (kind == 0) {
+      P.resize(size_t(BN) * BN);
+      orc_pinv(P.data());
+    }
+  }
+  void apply(const double* in, double* out) {
+    if (kind == 0)
+      orc_precond_pinv(m, P.data(), in, out);
+    else
+      orc_precond_cg(m, in, out);
+  }
+};
+
+double dot(const double* a, const double* b, int64_t n) {
+  double s = 0;
+#pragma omp parallel for reduction(+ : s) schedule(static)
+  for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+}  // namespace
+
+// BiCGSTABSolver::main (BiCGSTAB.cu:416-628), one rank.  b and x are modified
+// the way getVec does for the mean row (PoissonSolverExp.cpp:402-410).
+extern "C" int orc_bicgstab_gpu(orc_mesh* m, int mc, int precond, const double* b_in, double* x,
+                                double max_error, double max_rel_error, int max_restarts,
+                                int max_iter, double* stats) {
+  const int64_t n = int64_t(m->nb) * BN;
+  std::vector<double> b(b_in, b_in + n), r(n), rhat(n), p(n), nu(n), t(n), z(n), xopt(n);
+  if ((mc == 1 || mc == 3) && m->mean_block >= 0) {
+    b[int64_t(m->mean_block) * BN] = 0.;
+    x[int64_t(m->mean_block) * BN] = 0.;
+  }
+  Precond M(m, precond);
+  const double eps = 1e-21;
+  double alpha = 1, beta = 1, omega = 1, rho_prev = 1, rho_curr = 1;
+  apply_A(m, mc, x, nu.data());
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - nu[i];
+  double error = std::sqrt(dot(r.data(), r.data(), n));
+  const double error_init = error;
+  double error_opt = error;
+  std::copy(x, x + n, xopt.begin());
+  rhat = r;
+  std::fill(nu.begin(), nu.end(), 0.);
+  std::fill(p.begin(), p.end(), 0.);
+  int restarts = 0, k = 0;
+  bool converged = false;
+  for (k = 0; k < max_iter; ++k) {
+    rho_curr = dot(rhat.data(), r.data(), n);
+    const double nr = dot(r.data(), r.data(), n), nrh = dot(rhat.data(), rhat.data(), n);
+    const bool breakdown = rho_curr * rho_curr < 1e-16 * nr * nrh;
+    beta = (rho_curr / (rho_prev + eps)) * (alpha / (omega + eps));
+    if (breakdown && max_restarts > 0) {
+      ++restarts;
+      if (restarts >= max_restarts) break;
+      rhat = r;
+      rho_curr = dot(rhat.data(), rhat.data(), n);
+      std::fill(nu.begin(), nu.end(), 0.);
+      std::fill(p.begin(), p.end(), 0.);
+      rho_prev = 1.;
+      alpha = 1.;
+      omega = 1.;
+      beta = (rho_curr / (rho_prev + eps)) * (alpha / (omega + eps));
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) p[i] = r[i] + beta * (p[i] - omega * nu[i]);
+    M.apply(p.data(), z.data());
+    apply_A(m, mc, z.data(), nu.data());
+    alpha = rho_curr / (dot(rhat.data(), nu.data(), n) + eps);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += alpha * z[i];
+      r[i] -= alpha * nu[i];
+    }
+    M.apply(r.data(), z.data());
+    apply_A(m, mc, z.data(), t.data());
+    const double ts = dot(t.data(), r.data(), n), tt = dot(t.data(), t.data(), n);
+    omega = ts / (tt + eps);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+      x[i] += omega * z[i];
+      r[i] -= omega * t[i];
+    }
+    error = std::sqrt(dot(r.data(), r.data(), n));
+    if (error < error_opt) {
+      error_opt = error;
+      std::copy(x, x + n, xopt.begin());
+      if (error <= max_error || error / error_init <= max_rel_error) {
+        converged = true;
+        break;
+      }
+    }
+    rho_prev = rho_curr;
+  }
+  std::copy(xopt.begin(), xopt.end(), x);
+  if (stats) {
+    stats[0] = k + (converged ? 1 : 0);
+    stats[1] = restarts;
+    stats[2] = error_init;
+    stats[3] = error_opt;
+    stats[4] = converged;
+  }
+  return converged ? 0 : 1;
+}
+
+// PoissonSolverAMR::solve (PoissonSolverAMR.cpp:13-358), pipelined BiCGSTAB of
+// Cools & Vanroose (Alg. 11) with residual replacement every 50 iterations.
+extern "C" int orc_bicgstab_pipelined(orc_mesh* m, int mc, int precond, const double* b_in,
+                                      double* x, double max_error, double max_rel_error,
+                                      int max_iter, double* stats) {
+  const int64_t N = int64_t(m->nb) * BN;
+  const double eps = 1e-100;
+  const int max_restarts = 100;
+  std::vector<double> b(b_in, b_in + N), phat(N), rhat(N), shat(N), what(N), zhat(N), qhat(N),
+      s(N), w(N), z(N), t(N), v(N), q(N), r(N), y(N), r0(N), xopt(N);
+  if ((mc == 1 || mc > 2) && m->mean_block >= 0) b[int64_t(m->mean_block) * BN] = 0.0;
+  r = b;
+  Precond M(m, precond);
+  apply_A(m, mc, x, r0.data());
+#pragma omp parallel for
+  for (int64_t i = 0; i < N; ++i) {
+    r0[i] = r[i] - r0[i];
+    r[i] = r0[i];
+  }
+  M.apply(r0.data(), rhat.data());
+  apply_A(m, mc, rhat.data(), w.data());
+  M.apply(w.data(), what.data());
+  apply_A(m, mc, what.data(), t.data());
+  double alpha = 0, norm = 0, beta = 0, omega = 0, r0r_prev;
+  {
+    const double t0 = dot(r0.data(), r0.data(), N), t1 = dot(r0.data(), w.data(), N);
+    alpha = t0 / (t1 + eps);
+    r0r_prev = t0;
+    norm = std::sqrt(t0);
+  }
+  const double init_norm = norm;
+  double min_norm = 1e50;
+  bool useXopt = false;
+  int restarts = 0, k;
+  bool converged = false;
+  for (k = 0; k < max_iter; ++k) {
+    double qy = 0, yy = 0;
+    if (k % 50 != 0) {
+#pragma omp parallel for reduction(+ : qy, yy)
+      for (int64_t j = 0; j < N; ++j) {
+        phat[j] = rhat[j] + beta * (phat[j] - omega * shat[j]);
+        s[j] = w[j] + beta * (s[j] - omega * z[j]);
+        shat[j] = what[j] + beta * (shat[j] - omega * zhat[j]);
+        z[j] = t[j] + beta * (z[j] - omega * v[j]);
+        q[j] = r[j] - alpha * s[j];
+        qhat[j] = rhat[j] - alpha * shat[j];
+        y[j] = w[j] - alpha * z[j];
+        qy += q[j] * y[j];
+        yy += y[j] * y[j];
+      }
+    } else {
+#pragma omp parallel for
+      for (int64_t j = 0; j < N; ++j) phat[j] = rhat[j] + beta * (phat[j] - omega * shat[j]);
+      apply_A(m, mc, phat.data(), s.data());
+      M.apply(s.data(), shat.data());
+      apply_A(m, mc, shat.data(), z.data());
+#pragma omp parallel for reduction(+ : qy, yy)
+      for (int64_t j = 0; j < N; ++j) {
+        q[j] = r[j] - alpha * s[j];
+        qhat[j] = rhat[j] - alpha * shat[j];
+        y[j] = w[j] - alpha * z[j];
+        qy += q[j] * y[j];
+        yy += y[j] * y[j];
+      }
+    }
+    M.apply(z.data(), zhat.data());
+    apply_A(m, mc, zhat.data(), v.data());
+    omega = qy / (yy + eps);
+    double r0r = 0, r0w = 0, r0s = 0, r0z = 0, norm_1 = 0, norm_2 = 0;
+    norm = 0;
+    if (k % 50 != 0) {
+#pragma omp parallel for reduction(+ : r0r, r0w, r0s, r0z, norm_1, norm_2, norm)
+      for (int64_t j = 0; j < N; ++j) {
+        x[j] = x[j] + alpha * phat[j] + omega * qhat[j];
+        r[j] = q[j] - omega * y[j];
+        rhat[j] = qhat[j] - omega * (what[j] - alpha * zhat[j]);
+        w[j] = y[j] - omega * (t[j] - alpha * v[j]);
+        r0r += r0[j] * r[j];
+        r0w += r0[j] * w[j];
+        r0s += r0[j] * s[j];
+        r0z += r0[j] * z[j];
+        norm += r[j] * r[j];
+        norm_1 += r[j] * r[j];
+        norm_2 += r0[j] * r0[j];
+      }
+    } else {
+#pragma omp parallel for
+      for (int64_t j = 0; j < N; ++j) x[j] = x[j] + alpha * phat[j] + omega * qhat[j];
+      apply_A(m, mc, x, r.data());
+#pragma omp parallel for
+      for (int64_t j = 0; j < N; ++j) r[j] = b[j] - r[j];
+      M.apply(r.data(), rhat.data());
+      apply_A(m, mc, rhat.data(), w.data());
+#pragma omp parallel for reduction(+ : r0r, r0w, r0s, r0z, norm_1, norm_2, norm)
+      for (int64_t j = 0; j < N; ++j) {
+        r0r += r0[j] * r[j];
+        r0w += r0[j] * w[j];
+        r0s += r0[j] * s[j];
+        r0z += r0[j] * z[j];
+        norm += r[j] * r[j];
+        norm_1 += r[j] * r[j];
+        norm_2 += r0[j] * r0[j];
+      }
+    }
+    M.apply(w.data(), what.data());
+    apply_A(m, mc, what.data(), t.data());
+    norm = std::sqrt(norm);
+    beta = alpha / (omega + eps) * r0r / (r0r_prev + eps);
+    alpha = r0r / (r0w + beta * r0s - beta * omega * r0z);
+    double alphat = 1.0 / (omega + eps) + r0w / (r0r + eps) - beta * omega * r0z / (r0r + eps);
+    alphat = 1.0 / (alphat + eps);
+    if (std::fabs(alphat) < 10 * std::fabs(alpha)) alpha = alphat;
+    r0r_prev = r0r;
+    const bool serious_breakdown = r0r * r0r < 1e-16 * norm_1 * norm_2;
+    if (serious_breakdown && restarts < max_restarts) {
+      ++restarts;
+      r0 = r;
+      M.apply(r0.data(), rhat.data());
+      apply_A(m, mc, rhat.data(), w.data());
+      const double t0 = dot(r0.data(), r0.data(), N), t1 = dot(r0.data(), w.data(), N);
+      M.apply(w.data(), what.data());
+      apply_A(m, mc, what.data(), t.data());
+      alpha = t0 / (t1 + eps);
+      r0r_prev = t0;
+      beta = 0.0;
+      omega = 0.0;
+    }
+    if (norm < min_norm) {
+      useXopt = true;
+      min_norm = norm;
+      std::copy(x, x + N, xopt.begin());
+    }
+    if (norm < max_error || norm / (init_norm + eps) < max_rel_error) {
+      converged = true;
+      break;
+    }
+  }
+  if (useXopt) std::copy(xopt.begin(), xopt.end(), x);
+  if (stats) {
+    stats[0] = k + (converged ? 1 : 0);
+    stats[1] = restarts;
+    stats[2] = init_norm;
+    stats[3] = min_norm;
+    stats[4] = converged;
+  }
+  return converged ? 0 : 1;
+}
+
+// ============================================================================
+// Labs: a block with G ghost layers along the 6 faces (star stencils only).
+// Same-level and periodic ghosts copy the neighbour (Cubism BlockLab); boundary
+// ghosts follow BlockLabBC::applyBCfaceOpen/Wall (Definitions.h:67-397) for
+// vector fields and zero-gradient Neumann for scalar fields.  Coarse-fine
+// ghosts (Cubism's interpolation is absent from the reference tree) are our
+// definition, shared with the device code:
+//   * coarse block, finer neighbour: mean of the 2x2x2 fine cells;
+//   * fine block, coarser neighbour C: tensor-product quadratic Lagrange
+//     interpolation from C's own cells (normal: C's layers 0,1,2; tangential:
+//     3 cells centred on the containing coarse cell, one-sided at C's edges).
+// ============================================================================
+namespace {
+
+inline void lagrange3(double xi, double w[3]) {
+  w[0] = 0.5 * (xi - 1.0) * (xi - 2.0);
+  w[1] = -xi * (xi - 2.0);
+  w[2] = 0.5 * xi * (xi - 1.0);
+}
+
+// Tangential stencil for fine cell t of a fine block whose half is `half`
+// inside the coarse block: start node and evaluation point.
+inline void tan_stencil(int t, int half, int& n0, double w[3]) {
+  const int c = half * (BS / 2) + (t >> 1);
+  const double eta = (t & 1) ? 0.25 : -0.25;
+  if (c == 0) {
+    n0 = 0;
+    lagrange3(eta, w);
+  } else if (c == BS - 1) {
+    n0 = BS - 3;
+    lagrange3(2.0 + eta, w);
+  } else {
+    n0 = c - 1;
+    lagrange3(1.0 + eta, w);
+  }
+}
+
+struct Lab {
+  int G, W, ncomp;
+  std::vector<double> v;
+  Lab(int g, int nc) : G(g), W(BS + 2 * g), ncomp(nc), v(size_t(nc) * W * W * W, 0.0) {}
+  double& at(int c, int x, int y, int z) {
+    return v[size_t(c) * W * W * W + size_t(z + G) * W * W + size_t(y + G) * W + (x + G)];
+  }
+};
+
+void fill_lab(const orc_mesh& m, const double* f, int ncomp, int G, int b, bool vector_bc,
+              Lab& lab) {
+  const int64_t nbn = int64_t(m.nb) * BN;
+  auto F = [&](int c, int blk, int x, int y, int z) {
+    return f[c * nbn + int64_t(blk) * BN + cell(x, y, z)];
+  };
+  for (int c = 0; c < ncomp; ++c)
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) lab.at(c, x, y, z) = F(c, b, x, y, z);
+  for (int d = 0; d < 3; ++d)
+    for (int side = 0; side < 2; ++side) {
+      const int f_ = 2 * d + side;
+      const int k = m.kind[b][f_];
+      const int t1 = tan1(d), t2 = tan2(d);
+      for (int l = 1; l <= G; ++l)
+        for (int b2 = 0; b2 < BS; ++b2)
+          for (int a = 0; a < BS; ++a) {
+            int g[3];  // ghost position in lab coordinates of block b
+            g[d] = side ? BS - 1 + l : -l;
+            g[t1] = a;
+            g[t2] = b2;
+            for (int c = 0; c < ncomp; ++c) {
+              double val = 0;
+              if (k == K_SAME) {
+                int q[3] = {g[0], g[1], g[2]};
+                q[d] = side ? l - 1 : BS - l;
+                val = F(c, m.nbr[b][f_][0], q[0], q[1], q[2]);
+              } else if (k == K_BOUNDARY) {
+                int q[3] = {g[0], g[1], g[2]};
+                q[d] = side ? BS - 1 : 0;
+                val = F(c, b, q[0], q[1], q[2]);
+                if (vector_bc) {
+                  const int bc = m.nbr[b][f_][0];
+                  if (bc == BC_WALL || c == d) val = -val;
+                }
+              } else if (k == K_FINER) {
+                const int ch = m.nbr[b][f_][(a >> 2) + 2 * (b2 >> 2)];
+                double s = 0;
+                for (int e2 = 0; e2 < 2; ++e2)
+                  for (int e1 = 0; e1 < 2; ++e1)
+                    for (int en = 0; en < 2; ++en) {
+                      int q[3];
+                      const int fl = 2 * (l - 1) + en;  // fine layer from the face
+                      q[d] = side ? fl : BS - 1 - fl;
+                      q[t1] = 2 * (a & 3) + e1;
+                      q[t2] = 2 * (b2 & 3) + e2;
+                      s += F(c, ch, q[0], q[1], q[2]);
+                    }
+                val = 0.125 * s;
+              } else {  // K_COARSER
+                const int cb = m.nbr[b][f_][0];
+                double wn[3], w1[3], w2[3];
+                lagrange3((l - 1.5) * 0.5, wn);
+                int n1, n2;
+                tan_stencil(a, m.idx[b][t1] & 1, n1, w1);
+                tan_stencil(b2, m.idx[b][t2] & 1, n2, w2);
+                double s = 0;
+                for (int i2 = 0; i2 < 3; ++i2)
+                  for (int i1 = 0; i1 < 3; ++i1)
+                    for (int in = 0; in < 3; ++in) {
+                      int q[3];
+                      q[d] = side ? in : BS - 1 - in;
+                      q[t1] = n1 + i1;
+                      q[t2] = n2 + i2;
+                      s += wn[in] * w1[i1] * w2[i2] * F(c, cb, q[0], q[1], q[2]);
+                    }
+                val = s;
+              }
+              lab.at(c, g[0], g[1], g[2]) = val;
+            }
+          }
+    }
+}
+
+// Face value storage for flux correction: per block, per face, ncomp x 64.
+struct Faces {
+  int nb, ncomp;
+  std::vector<double> v;
+  Faces(int n, int nc) : nb(n), ncomp(nc), v(size_t(n) * 6 * nc * 64, 0.0) {}
+  double& at(int b, int f, int c, int t) { return v[((size_t(b) * 6 + f) * ncomp + c) * 64 + t]; }
+};
+
+// Cubism FluxCorrection as used by compute<...>(..., applyFluxCorrection):
+// a coarse cell next to a finer face gets its own stored face value (which
+// cancels its face term) plus the four fine face values (the fine fluxes).
+// comp_mask: which components are corrected on faces normal to d
+// (bit c set in comp_mask[d]).
+void flux_correct(const orc_mesh& m, Faces& fc, double* out, int ncomp, const int comp_mask[3]) {
+  const int64_t nbn = int64_t(m.nb) * BN;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int b = 0; b < m.nb; ++b)
+    for (int d = 0; d < 3; ++d)
+      for (int side = 0; side < 2; ++side) {
+        const int f = 2 * d + side;
+        if (m.kind[b][f] != K_FINER) continue;
+        const int t1 = tan1(d), t2 = tan2(d);
+        for (int c2 = 0; c2 < BS; ++c2)
+          for (int c1 = 0; c1 < BS; ++c1) {
+            const int ch = m.nbr[b][f][(c1 >> 2) + 2 * (c2 >> 2)];
+            int q[3];
+            q[d] = side ? BS - 1 : 0;
+            q[t1] = c1;
+            q[t2] = c2;
+            for (int c = 0; c < ncomp; ++c) {
+              if (!((comp_mask[d] >> c) & 1)) continue;
+              double s = fc.at(b, f, c, c1 + BS * c2);
+              for (int e2 = 0; e2 < 2; ++e2)
+                for (int e1 = 0; e1 < 2; ++e1)
+                  s += fc.at(ch, f ^ 1, c, (2 * (c1 & 3) + e1) + BS * (2 * (c2 & 3) + e2));
+              out[c * nbn + int64_t(b) * BN + cell(q[0], q[1], q[2])] += s;
+            }
+          }
+      }
+}
+
+inline bool has_jump(const orc_mesh& m, int b, int f) {
+  return m.kind[b][f] == K_COARSER || m.kind[b][f] == K_FINER;
+}
+
+}  // namespace
+
+extern "C" void orc_fill_lab(orc_mesh* m, const double* field, int ncomp, int G, int block,
+                             int vector_bc, double* out) {
+  Lab lab(G, ncomp);
+  fill_lab(*m, field, ncomp, G, block, vector_bc != 0, lab);
+  std::memcpy(out, lab.v.data(), lab.v.size() * sizeof(double));
+}
+
+// ============================================================================
+// Time step control: findMaxU (ProcessHelpers.h:71-94), calcMaxTimestep
+// (Simulation.cpp:309-375)
+// ============================================================================
+extern "C" double orc_max_u(orc_mesh* m, const double* vel, const double* uinf) {
+  const int64_t n = int64_t(m->nb) * BN;
+  double mx = 0;
+#pragma omp parallel for reduction(max : mx) schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    const double a = std::fabs(vel[i] + uinf[0]);
+    const double b = std::fabs(vel[n + i] + uinf[1]);
+    const double c = std::fabs(vel[2 * n + i] + uinf[2]);
+    mx = std::max(mx, std::max({a, b, c}));
+  }
+  return mx;
+}
+
+extern "C" double orc_dt(double hmin, double nu, double cfl, double umax, int step, int rampup) {
+  const double dtDiffusion = (1.0 / 6.0) * hmin * hmin / (nu + (1.0 / 6.0) * hmin * umax);
+  const double dtAdvection = hmin / (umax + 1e-8);
+  if (step < rampup) {
+    const double x = step / (double)rampup;
+    const double rampCFL = std::exp(std::log(1e-3) * (1 - x) + std::log(cfl) * x);
+    return std::min(dtDiffusion, rampCFL * dtAdvection);
+  }
+  return std::min(dtDiffusion, cfl * dtAdvection);
+}
+
+// ============================================================================
+// AdvectionDiffusion (AdvectionDiffusion.cpp:19-322)
+// ============================================================================
+namespace {
+
+inline double weno5_plus(double um2, double um1, double u, double up1, double up2) {
+  const double e = 1e-6;
+  const double b1 = 13.0 / 12.0 * std::pow((um2 + u) - 2 * um1, 2) + 0.25 * std::pow((um2 + 3 * u) - 4 * um1, 2);
+  const double b2 = 13.0 / 12.0 * std::pow((um1 + up1) - 2 * u, 2) + 0.25 * std::pow(um1 - up1, 2);
+  const double b3 = 13.0 / 12.0 * std::pow((u + up2) - 2 * up1, 2) + 0.25 * std::pow((3 * u + up2) - 4 * up1, 2);
+  const double g1 = 0.1, g2 = 0.6, g3 = 0.3;
+  const double what1 = g1 / std::pow(b1 + e, 2);
+  const double what2 = g2 / std::pow(b2 + e, 2);
+  const double what3 = g3 / std::pow(b3 + e, 2);
+  const double aux = 1.0 / ((what1 + what3) + what2);
+  const double w1 = what1 * aux, w2 = what2 * aux, w3 = what3 * aux;
+  const double f1 = (11.0 / 6.0) * u + ((1.0 / 3.0) * um2 - (7.0 / 6.0) * um1);
+  const double f2 = (5.0 / 6.0) * u + ((-1.0 / 6.0) * um1 + (1.0 / 3.0) * up1);
+  const double f3 = (1.0 / 3.0) * u + ((+5.0 / 6.0) * up1 - (1.0 / 6.0) * up2);
+  return (w1 * f1 + w3 * f3) + w2 * f2;
+}
+inline double weno5_minus(double um2, double um1, double u, double up1, double up2) {
+  const double e = 1e-6;
+  const double b1 = 13.0 / 12.0 * std::pow((um2 + u) - 2 * um1, 2) + 0.25 * std::pow((um2 + 3 * u) - 4 * um1, 2);
+  const double b2 = 13.0 / 12.0 * std::pow((um1 + up1) - 2 * u, 2) + 0.25 * std::pow(um1 - up1, 2);
+  const double b3 = 13.0 / 12.0 * std::pow((u + up2) - 2 * up1, 2) + 0.25 * std::pow((3 * u + up2) - 4 * up1, 2);
+  const double g1 = 0.3, g2 = 0.6, g3 = 0.1;
+  const double what1 = g1 / std::pow(b1 + e, 2);
+  const double what2 = g2 / std::pow(b2 + e, 2);
+  const double what3 = g3 / std::pow(b3 + e, 2);
+  const double aux = 1.0 / ((what1 + what3) + what2);
+  const double w1 = what1 * aux, w2 = what2 * aux, w3 = what3 * aux;
+  const double f1 = (1.0 / 3.0) * u + ((-1.0 / 6.0) * um2 + (5.0 / 6.0) * um1);
+  const double f2 = (5.0 / 6.0) * u + ((1.0 / 3.0) * um1 - (1.0 / 6.0) * up1);
+  const double f3 = (11.0 / 6.0) * u + ((-7.0 / 6.0) * up1 + (1.0 / 3.0) * up2);
+  return (w1 * f1 + w3 * f3) + w2 * f2;
+}
+inline double deriv(int scheme, double U, double um3, double um2, double um1, double u, double up1,
+                    double up2, double up3) {
+  if (scheme == 1) {
+    double fp, fm;
+    if (U > 0) {
+      fp = weno5_plus(um2, um1, u, up1, up2);
+      fm = weno5_plus(um3, um2, um1, u, up1);
+    } else {
+      fp = weno5_minus(um1, u, up1, up2, up3);
+      fm = weno5_minus(um2, um1, u, up1, up2);
+    }
+    return fp - fm;
+  }
+  if (U > 0) return (-2 * um3 + 15 * um2 - 60 * um1 + 20 * u + 30 * up1 - 3 * up2) / 60.;
+  return (2 * up3 - 15 * up2 + 60 * up1 - 20 * u - 30 * um1 + 3 * um2) / 60.;
+}
+
+void advect_rhs(orc_mesh* m, const double* vel, double* tmpV, double dt, double nu,
+                const double* uinf, int scheme, double coef) {
+  const int64_t nbn = int64_t(m->nb) * BN;
+  Faces fc(m->nb, 3);
+#pragma omp parallel
+  {
+    Lab lab(3, 3);
+#pragma omp for schedule(dynamic, 4)
+    for (int b = 0; b < m->nb; ++b) {
+      fill_lab(*m, vel, 3, 3, b, true, lab);
+      const double h = m->h[b], h3 = h * h * h;
+      const double facA = -dt / h * h3 * coef;
+      const double facD = (nu / h) * (dt / h) * h3 * coef;
+      auto L = [&](int c, int x, int y, int z) { return lab.at(c, x, y, z); };
+      for (int z = 0; z < BS; ++z)
+        for (int y = 0; y < BS; ++y)
+          for (int x = 0; x < BS; ++x) {
+            const double uA[3] = {L(0, x, y, z) + uinf[0], L(1, x, y, z) + uinf[1], L(2, x, y, z) + uinf[2]};
+            double dd[3][3];  // dd[c][dir]
+            for (int c = 0; c < 3; ++c) {
+              dd[c][0] = deriv(scheme, uA[0], L(c, x - 3, y, z), L(c, x - 2, y, z), L(c, x - 1, y, z), L(c, x, y, z), L(c, x + 1, y, z), L(c, x + 2, y, z), L(c, x + 3, y, z));
+              dd[c][1] = deriv(scheme, uA[1], L(c, x, y - 3, z), L(c, x, y - 2, z), L(c, x, y - 1, z), L(c, x, y, z), L(c, x, y + 1, z), L(c, x, y + 2, z), L(c, x, y + 3, z));
+              dd[c][2] = deriv(scheme, uA[2], L(c, x, y, z - 3), L(c, x, y, z - 2), L(c, x, y, z - 1), L(c, x, y, z), L(c, x, y, z + 1), L(c, x, y, z + 2), L(c, x, y, z + 3));
+            }
+            const double duD = ((L(0, x + 1, y, z) + L(0, x - 1, y, z)) + ((L(0, x, y + 1, z) + L(0, x, y - 1, z)) + (L(0, x, y, z + 1) + L(0, x, y, z - 1)))) - 6 * L(0, x, y, z);
+            const double dvD = ((L(1, x, y + 1, z) + L(1, x, y - 1, z)) + ((L(1, x, y, z + 1) + L(1, x, y, z - 1)) + (L(1, x + 1, y, z) + L(1, x - 1, y, z)))) - 6 * L(1, x, y, z);
+            const double dwD = ((L(2, x, y, z + 1) + L(2, x, y, z - 1)) + ((L(2, x + 1, y, z) + L(2, x - 1, y, z)) + (L(2, x, y + 1, z) + L(2, x, y - 1, z)))) - 6 * L(2, x, y, z);
+            const double duA = uA[0] * dd[0][0] + (uA[1] * dd[0][1] + uA[2] * dd[0][2]);
+            const double dvA = uA[1] * dd[1][1] + (uA[2] * dd[1][2] + uA[0] * dd[1][0]);
+            const double dwA = uA[2] * dd[2][2] + (uA[0] * dd[2][0] + uA[1] * dd[2][1]);
+            const int64_t o = int64_t(b) * BN + cell(x, y, z);
+            tmpV[o] += facA * duA + facD * duD;
+            tmpV[nbn + o] += facA * dvA + facD * dvD;
+            tmpV[2 * nbn + o] += facA * dwA + facD * dwD;
+          }
+      // face fluxes (AdvectionDiffusion.cpp:138-213)
+      for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+          const int f = 2 * d + side;
+          if (!has_jump(*m, b, f)) continue;
+          const int t1 = tan1(d), t2 = tan2(d);
+          for (int b2 = 0; b2 < BS; ++b2)
+            for (int a = 0; a < BS; ++a) {
+              int q[3], g[3];
+              q[d] = side ? BS - 1 : 0;
+              q[t1] = a;
+              q[t2] = b2;
+              for (int e = 0; e < 3; ++e) g[e] = q[e];
+              g[d] += side ? 1 : -1;
+              for (int c = 0; c < 3; ++c)
+                fc.at(b, f, c, a + BS * b2) = facD * (L(c, q[0], q[1], q[2]) - L(c, g[0], g[1], g[2]));
+            }
+        }
+    }
+  }
+  const int mask[3] = {7, 7, 7};
+  flux_correct(*m, fc, tmpV, 3, mask);
+}
+
+}  // namespace
+
+extern "C" void orc_advect_rhs(orc_mesh* m, const double* vel, double* tmpV, double dt, double nu,
+                               const double* uinf, int scheme, double coef) {
+  advect_rhs(m, vel, tmpV, dt, nu, uinf, scheme, coef);
+}
+
+extern "C" void orc_advect_diffuse(orc_mesh* m, double* vel, double* tmpV, double dt, double nu,
+                                   const double* uinf, int scheme) {
+  const int64_t nbn = int64_t(m->nb) * BN;
+  const double alpha[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+  const double beta[3] = {-5.0 / 9.0, -153.0 / 128.0, 0.0};
+  std::fill(tmpV, tmpV + 3 * nbn, 0.0);
+  for (int s = 0; s < 3; ++s) {
+    advect_rhs(m, vel, tmpV, dt, nu, uinf, scheme, 1.0);
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < m->nb; ++b) {
+      const double ih3 = alpha[s] / (m->h[b] * m->h[b] * m->h[b]);
+      for (int c = 0; c < 3; ++c)
+        for (int i = 0; i < BN; ++i) {
+          const int64_t o = c * nbn + int64_t(b) * BN + i;
+          vel[o] += tmpV[o] * ih3;
+          tmpV[o] *= beta[s];
+        }
+    }
+  }
+}
+
+// ============================================================================
+// Penalization (Penalization.cpp:18-109)
+// ============================================================================
+extern "C" void orc_penalize(orc_mesh* m, double* vel, const double* chi, const int32_t* slot,
+                             int nslots, const double* chi_o, const double* udef_o,
+                             const double* ob, double dt, double lambda, int implicit,
+                             double* force_out) {
+  const int64_t nbn = int64_t(m->nb) * BN;
+  const double lambdaFac = implicit ? lambda : 1.0 / dt;
+  double F[6] = {0, 0, 0, 0, 0, 0};
+  std::vector<std::array<double, 6>> per(m->nb, {0, 0, 0, 0, 0, 0});
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int b = 0; b < m->nb; ++b) {
+    const int s = slot[b];
+    if (s < 0) continue;
+    const double h = m->h[b], dv = h * h * h;
+    const double org[3] = {m->idx[b][0] * BS * h, m->idx[b][1] * BS * h, m->idx[b][2] * BS * h};
+    double FX = 0, FY = 0, FZ = 0, TX = 0, TY = 0, TZ = 0;
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) {
+          const int i = cell(x, y, z);
+          const double CHI = chi_o[size_t(s) * BN + i];
+          if (chi[int64_t(b) * BN + i] > CHI) continue;
+          if (CHI <= 0) continue;
+          double p[3] = {org[0] + (x + 0.5) * h, org[1] + (y + 0.5) * h, org[2] + (z + 0.5) * h};
+          p[0] -= ob[0];
+          p[1] -= ob[1];
+          p[2] -= ob[2];
+          const double* vv = ob + 3;
+          const double* om = ob + 6;
+          const double U[3] = {
+              vv[0] + om[1] * p[2] - om[2] * p[1] + udef_o[(0 * size_t(nslots) + s) * BN + i],
+              vv[1] + om[2] * p[0] - om[0] * p[2] + udef_o[(1 * size_t(nslots) + s) * BN + i],
+              vv[2] + om[0] * p[1] - om[1] * p[0] + udef_o[(2 * size_t(nslots) + s) * BN + i]};
+          const double X = implicit ? (CHI > 0.5 ? 1.0 : 0.0) : CHI;
+          const double penalFac = implicit ? X * lambdaFac / (1 + X * lambdaFac * dt) : X * lambdaFac;
+          const int64_t o = int64_t(b) * BN + i;
+          const double FPX = penalFac * (U[0] - vel[o]);
+          const double FPY = penalFac * (U[1] - vel[nbn + o]);
+          const double FPZ = penalFac * (U[2] - vel[2 * nbn + o]);
+          vel[o] = vel[o] + dt * FPX;
+          vel[nbn + o] = vel[nbn + o] + dt * FPY;
+          vel[2 * nbn + o] = vel[2 * nbn + o] + dt * FPZ;
+          FX += dv * FPX;
+          FY += dv * FPY;
+          FZ += dv * FPZ;
+          TX += dv * (p[1] * FPZ - p[2] * FPY);
+          TY += dv * (p[2] * FPX - p[0] * FPZ);
+          TZ += dv * (p[0] * FPY - p[1] * FPX);
+        }
+    per[b] = {FX, FY, FZ, TX, TY, TZ};
+  }
+  for (int b = 0; b < m->nb; ++b)
+    for (int q = 0; q < 6; ++q) F[q] += per[b][q];
+  if (force_out)
+    for (int q = 0; q < 6; ++q) force_out[q] = F[q];
+}
+
+// ============================================================================
+// PressureProjection (PressureProjection.cpp:16-468)
+// ============================================================================
+namespace {
+
+// tmpV = udef where grid chi <= obstacle chi (kernelUpdateTmpV, :202-242)
+void udef_to_tmpV(orc_mesh* m, const double* chi, const int32_t* slot, int nslots,
+                  const double* chi_o, const double* udef_o, double* tmpV) {
+  const int64_t nbn = int64_t(m->nb) * BN;
+  std::fill(tmpV, tmpV + 3 * nbn, 0.0);
+  if (!slot) return;
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < m->nb; ++b) {
+    const int s = slot[b];
+    if (s < 0) continue;
+    for (int i = 0; i < BN; ++i) {
+      if (chi[int64_t(b) * BN + i] > chi_o[size_t(s) * BN + i]) continue;
+      for (int c = 0; c < 3; ++c)
+        tmpV[c * nbn + int64_t(b) * BN + i] += udef_o[(c * size_t(nslots) + s) * BN + i];
+    }
+  }
+}
+
+// KernelPressureRHS (:96-199) with flux correction
+void pressure_rhs(orc_mesh* m, const double* vel, const double* tmpV, const double* chi, double dt,
+                  double* lhs) {
+  Faces fc(m->nb, 1);
+#pragma omp parallel
+  {
+    Lab lab(1, 3), ulab(1, 3);
+#pragma omp for schedule(dynamic, 4)
+    for (int b = 0; b < m->nb; ++b) {
+      fill_lab(*m, vel, 3, 1, b, true, lab);
+      fill_lab(*m, tmpV, 3, 1, b, true, ulab);
+      const double h = m->h[b], fac = 0.5 * h * h / dt;
+      for (int z = 0; z < BS; ++z)
+        for (int y = 0; y < BS; ++y)
+          for (int x = 0; x < BS; ++x) {
+            const int64_t o = int64_t(b) * BN + cell(x, y, z);
+            double p = fac * (lab.at(0, x + 1, y, z) - lab.at(0, x - 1, y, z) + lab.at(1, x, y + 1, z) -
+                              lab.at(1, x, y - 1, z) + lab.at(2, x, y, z + 1) - lab.at(2, x, y, z - 1));
+            const double divUs = ulab.at(0, x + 1, y, z) - ulab.at(0, x - 1, y, z) + ulab.at(1, x, y + 1, z) -
+                                 ulab.at(1, x, y - 1, z) + ulab.at(2, x, y, z + 1) - ulab.at(2, x, y, z - 1);
+            p += -chi[o] * fac * divUs;
+            lhs[o] = p;
+          }
+      for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+          const int f = 2 * d + side;
+          if (!has_jump(*m, b, f)) continue;
+          const int t1 = tan1(d), t2 = tan2(d);
+          for (int b2 = 0; b2 < BS; ++b2)
+            for (int a = 0; a < BS; ++a) {
+              int q[3], g[3];
+              q[d] = side ? BS - 1 : 0;
+              q[t1] = a;
+              q[t2] = b2;
+              for (int e = 0; e < 3; ++e) g[e] = q[e];
+              g[d] += side ? 1 : -1;
+              const double c = chi[int64_t(b) * BN + cell(q[0], q[1], q[2])];
+              const double sg = side ? -1.0 : 1.0;
+              fc.at(b, f, 0, a + BS * b2) =
+                  sg * fac * (lab.at(d, g[0], g[1], g[2]) + lab.at(d, q[0], q[1], q[2])) -
+                  sg * c * fac * (ulab.at(d, g[0], g[1], g[2]) + ulab.at(d, q[0], q[1], q[2]));
+            }
+        }
+    }
+  }
+  const int mask[3] = {1, 1, 1};
+  flux_correct(*m, fc, lhs, 1, mask);
+}
+
+// KernelDivPressure (:16-94): out = h * Lap7(p) with flux correction
+void div_pressure(orc_mesh* m, const double* p, double* out) {
+  Faces fc(m->nb, 1);
+#pragma omp parallel
+  {
+    Lab lab(1, 1);
+#pragma omp for schedule(dynamic, 4)
+    for (int b = 0; b < m->nb; ++b) {
+      fill_lab(*m, p, 1, 1, b, false, lab);
+      const double fac = m->h[b];
+      for (int z = 0; z < BS; ++z)
+        for (int y = 0; y < BS; ++y)
+          for (int x = 0; x < BS; ++x)
+            out[int64_t(b) * BN + cell(x, y, z)] =
+                fac * (lab.at(0, x + 1, y, z) + lab.at(0, x - 1, y, z) + lab.at(0, x, y + 1, z) +
+                       lab.at(0, x, y - 1, z) + lab.at(0, x, y, z + 1) + lab.at(0, x, y, z - 1) -
+                       6.0 * lab.at(0, x, y, z));
+      for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+          const int f = 2 * d + side;
+          if (!has_jump(*m, b, f)) continue;
+          const int t1 = tan1(d), t2 = tan2(d);
+          for (int b2 = 0; b2 < BS; ++b2)
+            for (int a = 0; a < BS; ++a) {
+              int q[3], g[3];
+              q[d] = side ? BS - 1 : 0;
+              q[t1] = a;
+              q[t2] = b2;
+              for (int e = 0; e < 3; ++e) g[e] = q[e];
+              g[d] += side ? 1 : -1;
+              fc.at(b, f, 0, a + BS * b2) = fac * (lab.at(0, q[0], q[1], q[2]) - lab.at(0, g[0], g[1], g[2]));
+            }
+        }
+    }
+  }
+  const int mask[3] = {1, 1, 1};
+  flux_correct(*m, fc, out, 1, mask);
+}
+
+// KernelGradP (:244-323) + velocity update (:451-467)
+void grad_update(orc_mesh* m, double* vel, const double* p, double dt) {
+  const int64_t nbn = int64_t(m->nb) * BN;
+  std::vector<double> g(3 * nbn);
+  Faces fc(m->nb, 3);
+#pragma omp parallel
+  {
+    Lab lab(1, 1);
+#pragma omp for schedule(dynamic, 4)
+    for (int b = 0; b < m->nb; ++b) {
+      fill_lab(*m, p, 1, 1, b, false, lab);
+      const double h = m->h[b], fac = -0.5 * dt * h * h;
+      for (int z = 0; z < BS; ++z)
+        for (int y = 0; y < BS; ++y)
+          for (int x = 0; x < BS; ++x) {
+            const int64_t o = int64_t(b) * BN + cell(x, y, z);
+            g[o] = fac * (lab.at(0, x + 1, y, z) - lab.at(0, x - 1, y, z));
+            g[nbn + o] = fac * (lab.at(0, x, y + 1, z) - lab.at(0, x, y - 1, z));
+            g[2 * nbn + o] = fac * (lab.at(0, x, y, z + 1) - lab.at(0, x, y, z - 1));
+          }
+      for (int d = 0; d < 3; ++d)
+        for (int side = 0; side < 2; ++side) {
+          const int f = 2 * d + side;
+          if (!has_jump(*m, b, f)) continue;
+          const int t1 = tan1(d), t2 = tan2(d);
+          for (int b2 = 0; b2 < BS; ++b2)
+            for (int a = 0; a < BS; ++a) {
+              int q[3], gg[3];
+              q[d] = side ? BS - 1 : 0;
+              q[t1] = a;
+              q[t2] = b2;
+              for (int e = 0; e < 3; ++e) gg[e] = q[e];
+              gg[d] += side ? 1 : -1;
+              const double sg = side ? -1.0 : 1.0;
+              fc.at(b, f, d, a + BS * b2) = sg * fac * (lab.at(0, gg[0], gg[1], gg[2]) + lab.at(0, q[0], q[1], q[2]));
+            }
+        }
+    }
+  }
+  const int mask[3] = {1, 2, 4};
+  flux_correct(*m, fc, g.data(), 3, mask);
+#pragma omp parallel for schedule(static)
+  for (int b = 0; b < m->nb; ++b) {
+    const double fac = 1.0 / (m->h[b] * m->h[b] * m->h[b]);
+    for (int c = 0; c < 3; ++c)
+      for (int i = 0; i < BN; ++i) {
+        const int64_t o = c * nbn + int64_t(b) * BN + i;
+        vel[o] += fac * g[o];
+      }
+  }
+}
+
+}  // namespace
+
+extern "C" void orc_pressure_rhs(orc_mesh* m, const double* vel, const double* pres,
+                                 const double* chi, const int32_t* slot, int nslots,
+                                 const double* chi_o, const double* udef_o, double dt, int step,
+                                 double* lhs) {
+  const int64_t nbn = int64_t(m->nb) * BN;
+  std::vector<double> tmpV(3 * nbn);
+  std::vector<double> zchi;
+  if (!chi) {
+    zchi.assign(nbn, 0.0);
+    chi = zchi.data();
+  }
+  udef_to_tmpV(m, chi, slot, nslots, chi_o, udef_o, tmpV.data());
+  pressure_rhs(m, vel, tmpV.data(), chi, dt, lhs);
+  if (step > 2) {
+    std::vector<double> dp(nbn);
+    div_pressure(m, pres, dp.data());
+    for (int64_t i = 0; i < nbn; ++i) lhs[i] -= dp[i];
+  }
+}
+
+extern "C" void orc_grad_update(orc_mesh* m, double* vel, const double* pres, double dt) {
+  grad_update(m, vel, pres, dt);
+}
+
+extern "C" void orc_pressure_project(orc_mesh* m, double* vel, double* pres, const double* chi,
+                                     const int32_t* slot, int nslots, const double* chi_o,
+                                     const double* udef_o, double dt, int step, int mc, int solver,
+                                     double tol, double tol_rel, double* stats, double* lhs_out) {
+  const int64_t nbn = int64_t(m->nb) * BN;
+  std::vector<double> pOld(pres, pres + nbn), lhs(nbn);
+  orc_pressure_rhs(m, vel, pres, chi, slot, nslots, chi_o, udef_o, dt, step, lhs.data());
+  std::fill(pres, pres + nbn, 0.0);  // initial guess 0 (:381-393)
+  if (lhs_out) std::copy(lhs.begin(), lhs.end(), lhs_out);
+  if (solver == 0)
+    orc_bicgstab_gpu(m, mc, 0, lhs.data(), pres, tol, tol_rel, 100, 1000, stats);
+  else
+    orc_bicgstab_pipelined(m, mc, 1, lhs.data(), pres, tol, tol_rel, 1000, stats);
+  // zero mean (:404-431) and incremental pressure (:435-446)
+  double avg = 0, avg1 = 0;
+#pragma omp parallel for reduction(+ : avg, avg1) schedule(static)
+  for (int b = 0; b < m->nb; ++b) {
+    const double vv = m->h[b] * m->h[b] * m->h[b];
+    for (int i = 0; i < BN; ++i) {
+      avg += pres[int64_t(b) * BN + i] * vv;
+      avg1 += vv;
+    }
+  }
+  avg = avg / avg1;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < nbn; ++i) pres[i] -= avg;
+  if (step > 2)
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nbn; ++i) pres[i] += pOld[i];
+  grad_update(m, vel, pres, dt);
+}
+
+// ============================================================================
+// Learned preconditioner network (no reference counterpart; written from the
+// definition of a 3-D convolution).  Layer k maps C_in -> C_out channels with a
+// 3x3x3 kernel, weights w[k][co][ci][27], bias[k][co]; ReLU after layers 0-2.
+// Input: 10^3 (block + 1-cell halo), 1 channel.  Layer 0 is 'valid' (10^3 ->
+// 8^3); layers 1-3 are zero-padded 'same' on 8^3.  Output 8^3, 1 channel.
+// ============================================================================
+extern "C" void orc_cnn_forward(int nblk, int C, const float* w, const float* bias, const float* in,
+                                float* out, float* acts) {
+  const int cin[4] = {1, C, C, C}, cout[4] = {C, C, C, 1};
+  size_t woff[4], boff[4];
+  size_t wo = 0, bo = 0;
+  for (int k = 0; k < 4; ++k) {
+    woff[k] = wo;
+    boff[k] = bo;
+    wo += size_t(cout[k]) * cin[k] * 27;
+    bo += cout[k];
+  }
+#pragma omp parallel
+  {
+    std::vector<float> a(size_t(C) * BN), bbuf(size_t(C) * BN);
+#pragma omp for schedule(static)
+    for (int n = 0; n < nblk; ++n) {
+      const float* x = in + size_t(n) * 1000;
+      // layer 0: valid conv on 10^3
+      for (int co = 0; co < C; ++co)
+        for (int z = 0; z < BS; ++z)
+          for (int y = 0; y < BS; ++y)
+            for (int xx = 0; xx < BS; ++xx) {
+              float s = bias[boff[0] + co];
+              for (int kz = 0; kz < 3; ++kz)
+                for (int ky = 0; ky < 3; ++ky)
+                  for (int kx = 0; kx < 3; ++kx)
+                    s += w[woff[0] + size_t(co) * 27 + kx + 3 * ky + 9 * kz] *
+                         x[(xx + kx) + 10 * ((y + ky) + 10 * (z + kz))];
+              a[size_t(co) * BN + cell(xx, y, z)] = s > 0 ? s : 0;
+            }
+      if (acts) std::copy(a.begin(), a.end(), acts + (size_t(n) * 3 + 0) * C * BN);
+      for (int k = 1; k < 4; ++k) {
+        const int co_n = cout[k];
+        for (int co = 0; co < co_n; ++co)
+          for (int z = 0; z < BS; ++z)
+            for (int y = 0; y < BS; ++y)
+              for (int xx = 0; xx < BS; ++xx) {
+                float s = bias[boff[k] + co];
+                for (int ci = 0; ci < C; ++ci)
+                  for (int kz = 0; kz < 3; ++kz)
+                    for (int ky = 0; ky < 3; ++ky)
+                      for (int kx = 0; kx < 3; ++kx) {
+                        const int X = xx + kx - 1, Y = y + ky - 1, Z = z + kz - 1;
+                        if (X < 0 || Y < 0 || Z < 0 || X >= BS || Y >= BS || Z >= BS) continue;
+                        s += w[woff[k] + (size_t(co) * C + ci) * 27 + kx + 3 * ky + 9 * kz] *
+                             a[size_t(ci) * BN + cell(X, Y, Z)];
+                      }
+                if (k < 3)
+                  bbuf[size_t(co) * BN + cell(xx, y, z)] = s > 0 ? s : 0;
+                else
+                  out[size_t(n) * BN + cell(xx, y, z)] = s;
+              }
+        if (k < 3) {
+          std::swap(a, bbuf);
+          if (acts) std::copy(a.begin(), a.end(), acts + (size_t(n) * 3 + k) * C * BN);
+        }
+      }
+    }
+  }
+}
