@@ -136,3 +136,59 @@ class Context:
         st = cup_solve_stats()
         rc = check(lib().cup_poisson_solve(self._p, C.byref(st)), self._p)
         return rc, st.as_dict()
+
+    # ---- obstacles ----------------------------------------------------------
+    def obstacle_sphere(self, center, radius, vel=(0, 0, 0), omega=(0, 0, 0)):
+        c, v, o = (np.ascontiguousarray(a, dtype=np.float64) for a in (center, vel, omega))
+        check(lib().cup_obstacle_sphere(self._p, dptr(c), radius, dptr(v), dptr(o)), self._p)
+
+    def obstacle_ellipsoid(self, center, axes, quat, vel=(0, 0, 0), omega=(0, 0, 0)):
+        c, a, q, v, o = (np.ascontiguousarray(x, dtype=np.float64) for x in (center, axes, quat, vel, omega))
+        check(lib().cup_obstacle_ellipsoid(self._p, dptr(c), dptr(a), dptr(q), dptr(v), dptr(o)), self._p)
+
+    def set_obstacle(self, blocks, chi, udef, kin):
+        blocks = np.ascontiguousarray(blocks, np.int32)
+        chi, udef, kin = (np.ascontiguousarray(x, np.float64) for x in (chi, udef, kin))
+        check(lib().cup_set_obstacle(self._p, len(blocks), iptr(blocks), dptr(chi), dptr(udef), dptr(kin)), self._p)
+
+    def get_obstacle(self):
+        """(slot_of_block[nb], chi[nslots*512], udef[3*nslots*512], kin[9])"""
+        ns = check(lib().cup_get_obstacle(self._p, None, None, None, None), self._p)
+        blocks = np.zeros(ns, np.int32)
+        chi = np.zeros(ns * 512)
+        udef = np.zeros(3 * ns * 512)
+        kin = np.zeros(9)
+        check(lib().cup_get_obstacle(self._p, iptr(blocks), dptr(chi), dptr(udef), dptr(kin)), self._p)
+        slot = -np.ones(self.nb, np.int32)
+        slot[blocks] = np.arange(ns, dtype=np.int32)
+        return slot, chi, udef, kin
+
+    # ---- time-step operators -------------------------------------------------
+    def max_u(self):
+        out = C.c_double()
+        check(lib().cup_max_u(self._p, C.byref(out)), self._p)
+        return out.value
+
+    def compute_dt(self, step):
+        out = C.c_double()
+        check(lib().cup_compute_dt(self._p, step, C.byref(out)), self._p)
+        return out.value
+
+    def advect_diffuse(self, dt):
+        check(lib().cup_advect_diffuse(self._p, dt), self._p)
+
+    def penalize(self, dt):
+        f = np.zeros(6)
+        check(lib().cup_penalize(self._p, dt, dptr(f)), self._p)
+        return f
+
+    def pressure_project(self, dt, step):
+        st = cup_solve_stats()
+        rc = check(lib().cup_pressure_project(self._p, dt, step, C.byref(st)), self._p)
+        return rc, st.as_dict()
+
+    def step(self, step, dt=0.0):
+        used = C.c_double()
+        st = cup_solve_stats()
+        rc = check(lib().cup_step(self._p, step, dt, C.byref(used), C.byref(st)), self._p)
+        return used.value, rc, st.as_dict()

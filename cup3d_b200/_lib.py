@@ -95,6 +95,16 @@ SIGNATURES = {
     "cup_block_inverse_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_poisson_solve_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.POINTER(cup_solve_stats)]),
     "cup_poisson_solve": (C.c_int, [_P, C.POINTER(cup_solve_stats)]),
+    "cup_obstacle_sphere": (C.c_int, [_P, _D, C.c_double, _D, _D]),
+    "cup_obstacle_ellipsoid": (C.c_int, [_P, _D, _D, _D, _D, _D]),
+    "cup_set_obstacle": (C.c_int, [_P, C.c_int32, _I, _D, _D, _D]),
+    "cup_get_obstacle": (C.c_int, [_P, _I, _D, _D, _D]),
+    "cup_max_u": (C.c_int, [_P, _D]),
+    "cup_compute_dt": (C.c_int, [_P, C.c_int32, _D]),
+    "cup_advect_diffuse": (C.c_int, [_P, C.c_double]),
+    "cup_penalize": (C.c_int, [_P, C.c_double, _D]),
+    "cup_pressure_project": (C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(cup_solve_stats)]),
+    "cup_step": (C.c_int, [_P, C.c_int32, C.c_double, _D, C.POINTER(cup_solve_stats)]),
 }
 
 

@@ -105,9 +105,40 @@ __device__ bool grid_reduce(double (&v)[NR], const GridReduce& g, double* sm) {
   return true;
 }
 
+// Max-reduction counterpart of grid_reduce for one non-negative value.
+__device__ __forceinline__ bool grid_reduce_max(double& v, const GridReduce& g, double* sm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sm[w] = v;
+  __syncthreads();
+  __shared__ unsigned int s_ticket_m;
+  __shared__ double s_max;
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) m = fmax(m, sm[i]);
+    g.partial[blockIdx.x * 8] = m;
+    __threadfence();
+    s_ticket_m = atomicAdd(g.counter, 1u);
+  }
+  __syncthreads();
+  if (s_ticket_m != gridDim.x - 1) return false;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int i = 0; i < (int)gridDim.x; ++i) m = fmax(m, __ldcg(&g.partial[i * 8]));
+    s_max = m;
+    *g.counter = 0u;
+  }
+  __syncthreads();
+  v = s_max;
+  return true;
+}
+
 }  // namespace cup3d
 
-#define CUP_CUDA_TRY(expr)                                                        \
+#define CUP_CUDA_TRY(expr)                                                     \
   do {                                                                            \
     cudaError_t e_ = (expr);                                                      \
     if (e_ != cudaSuccess) return ::cup3d::set_cuda_error(e_, #expr, __FILE__, __LINE__); \

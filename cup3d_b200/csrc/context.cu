@@ -5,6 +5,8 @@
 #include <sstream>
 
 #include "context.h"
+#include "obstacles.h"
+#include "stencils.cuh"
 
 namespace cup3d {
 
@@ -420,6 +422,228 @@ int cup_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solve_stat
 int cup_poisson_solve(cup_ctx* c, cup_solve_stats* stats) {
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve: no mesh");
   return solve_impl(c, c->F.lhs, c->F.pres[c->F.pcur], stats);
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Obstacles and time-step operators
+// ===========================================================================
+namespace cup3d {
+
+static ObstacleView ob_view(const cup_ctx* c) {
+  ObstacleView v;
+  v.nslots = c->ob.nslots;
+  v.slot = c->ob.slot_of_block;
+  v.near = c->ob.near;
+  v.chi = c->ob.chi;
+  v.udef = c->ob.udef;
+  v.blk = c->ob.block_of_slot;
+  return v;
+}
+
+static int upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
+                           const double* kin) {
+  const Mesh& m = c->mesh;
+  c->obst_arena.release();
+  c->ob = DevObstacle();
+  if (nslots <= 0) return 0;
+  std::vector<int> slot(m.nb, -1), near(m.nb, 0);
+  for (int s = 0; s < nslots; ++s) {
+    if (blocks[s] < 0 || blocks[s] >= m.nb || slot[blocks[s]] >= 0)
+      return ctx_fail(c, CUP_ERR_ARG, "obstacle: invalid or repeated block id");
+    slot[blocks[s]] = s;
+  }
+  for (int b = 0; b < m.nb; ++b) {
+    bool nr = slot[b] >= 0;
+    for (int f = 0; f < 6 && !nr; ++f) {
+      const int k = m.face_kind[6 * b + f];
+      const int* nb = &m.face_nbr[24 * b + 4 * f];
+      if (k == FACE_SAME || k == FACE_COARSER) nr |= slot[nb[0]] >= 0;
+      if (k == FACE_FINER)
+        for (int q = 0; q < 4; ++q) nr |= slot[nb[q]] >= 0;
+    }
+    near[b] = nr;
+  }
+  DevObstacle& o = c->ob;
+  DevArena& A = c->obst_arena;
+  if (int rc = A.alloc(&o.slot_of_block, m.nb)) return keep(c, rc);
+  if (int rc = A.alloc(&o.near, m.nb)) return keep(c, rc);
+  if (int rc = A.alloc(&o.block_of_slot, nslots)) return keep(c, rc);
+  if (int rc = A.alloc(&o.chi, size_t(nslots) * BN)) return keep(c, rc);
+  if (int rc = A.alloc(&o.udef, 3 * size_t(nslots) * BN)) return keep(c, rc);
+  o.nslots = nslots;
+  o.h_blocks.assign(blocks, blocks + nslots);
+  o.h_chi.assign(chi, chi + size_t(nslots) * BN);
+  if (udef)
+    o.h_udef.assign(udef, udef + 3 * size_t(nslots) * BN);
+  else
+    o.h_udef.assign(3 * size_t(nslots) * BN, 0.0);
+  for (int i = 0; i < 9; ++i) o.kin[i] = kin ? kin[i] : 0.0;
+  CUP_CUDA_TRY(cudaMemcpy(o.slot_of_block, slot.data(), m.nb * sizeof(int), cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(o.near, near.data(), m.nb * sizeof(int), cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(o.block_of_slot, blocks, nslots * sizeof(int), cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(o.chi, o.h_chi.data(), o.h_chi.size() * 8, cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(o.udef, o.h_udef.data(), o.h_udef.size() * 8, cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(cudaMemcpy(c->d_scalars + SC_KIN, o.kin, 9 * sizeof(double), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static int install_host_obstacle(cup_ctx* c, const HostObstacle& h) {
+  if (int rc = upload_obstacle(c, int(h.blocks.size()), h.blocks.data(), h.chi.data(), h.udef.data(), h.kin))
+    return rc;
+  CUP_CUDA_TRY(cudaMemcpy(c->F.chi, h.grid_chi.data(), h.grid_chi.size() * 8, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+static double calc_dt(const cup_config& cfg, double hmin, double umax, int step) {
+  // Simulation::calcMaxTimestep (Simulation.cpp:326-338)
+  const double dtDiffusion = (1.0 / 6.0) * hmin * hmin / (cfg.nu + (1.0 / 6.0) * hmin * umax);
+  const double dtAdvection = hmin / (umax + 1e-8);
+  if (step < cfg.rampup) {
+    const double x = step / double(cfg.rampup);
+    const double rampCFL = std::exp(std::log(1e-3) * (1 - x) + std::log(cfg.cfl) * x);
+    return std::min(dtDiffusion, rampCFL * dtAdvection);
+  }
+  return std::min(dtDiffusion, cfg.cfl * dtAdvection);
+}
+
+static int grid_of(const cup_ctx* c) { return c->W.grid; }
+
+static int advect(cup_ctx* c, double dt) {
+  Fields& F = c->F;
+  for (int s = 0; s < 3; ++s) {
+    if (int rc = launch_advect_stage(c->dm, F.vel[F.vcur], F.vel[1 - F.vcur], F.tmpV, dt, c->cfg.nu, c->cfg.uinf,
+                                     c->cfg.advection, s, grid_of(c), c->stream))
+      return keep(c, rc);
+    F.vcur = 1 - F.vcur;
+  }
+  return 0;
+}
+
+static int penalize(cup_ctx* c, double dt) {
+  return keep(c, launch_penalize(c->dm, c->F.vel[c->F.vcur], c->F.chi, ob_view(c), c->d_scalars + SC_KIN, dt,
+                                 c->cfg.lambda, c->cfg.implicit_penalization, c->d_scalars + SC_FORCE, c->W.partial,
+                                 c->W.counters + 11, c->stream));
+}
+
+static int project(cup_ctx* c, double dt, int step, cup_solve_stats* stats) {
+  Fields& F = c->F;
+  double* pold = F.pres[F.pcur];
+  double* pnew = F.pres[1 - F.pcur];
+  if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], pold, F.chi, ob_view(c), dt, step, c->cfg.step_2nd_start,
+                                   F.lhs, F.phi, grid_of(c), c->stream))
+    return keep(c, rc);
+  cup_solve_stats st{};
+  const int rs = solve_impl(c, F.lhs, F.phi, &st);
+  if (rs < 0) return rs;
+  if (int rc = launch_weighted_sum(c->dm, F.phi, c->d_scalars + SC_SUMS, c->W, c->stream)) return keep(c, rc);
+  if (int rc = launch_grad_update(c->dm, F.vel[F.vcur], F.phi, pold, pnew, c->d_scalars + SC_SUMS, dt, step,
+                                  c->cfg.step_2nd_start, grid_of(c), c->stream))
+    return keep(c, rc);
+  F.pcur = 1 - F.pcur;
+  if (stats) *stats = st;
+  return rs;
+}
+
+}  // namespace cup3d
+
+extern "C" {
+
+int cup_obstacle_sphere(cup_ctx* c, const double* ctr, double r, const double* vel, const double* omega) {
+  if (!c || !ctr || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_sphere: bad arguments");
+  const double z[3] = {0, 0, 0};
+  HostObstacle h;
+  make_sphere(c->mesh, ctr, r, vel ? vel : z, omega ? omega : z, h);
+  return install_host_obstacle(c, h);
+}
+
+int cup_obstacle_ellipsoid(cup_ctx* c, const double* ctr, const double* ax, const double* q, const double* vel,
+                           const double* omega) {
+  if (!c || !ctr || !ax || !q || c->mesh.nb == 0 || c->host_only)
+    return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_ellipsoid: bad arguments");
+  const double z[3] = {0, 0, 0};
+  HostObstacle h;
+  make_ellipsoid(c->mesh, ctr, ax, q, vel ? vel : z, omega ? omega : z, h);
+  return install_host_obstacle(c, h);
+}
+
+int cup_set_obstacle(cup_ctx* c, int32_t nslots, const int32_t* blocks, const double* chi, const double* udef,
+                     const double* kin) {
+  if (!c || c->mesh.nb == 0 || c->host_only || (nslots > 0 && (!blocks || !chi)))
+    return ctx_fail(c, CUP_ERR_ARG, "cup_set_obstacle: bad arguments");
+  return upload_obstacle(c, nslots, blocks, chi, udef, kin);
+}
+
+int cup_get_obstacle(const cup_ctx* c, int32_t* blocks, double* chi, double* udef, double* kin) {
+  if (!c) return ctx_fail(nullptr, CUP_ERR_ARG, "null ctx");
+  const DevObstacle& o = c->ob;
+  if (blocks) std::copy(o.h_blocks.begin(), o.h_blocks.end(), blocks);
+  if (chi) std::copy(o.h_chi.begin(), o.h_chi.end(), chi);
+  if (udef) std::copy(o.h_udef.begin(), o.h_udef.end(), udef);
+  if (kin) std::copy(o.kin, o.kin + 9, kin);
+  return o.nslots;
+}
+
+int cup_max_u(cup_ctx* c, double* umax) {
+  if (!c || !umax || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_max_u: bad arguments");
+  if (int rc = launch_max_u(c->dm, c->F.vel[c->F.vcur], c->cfg.uinf, c->d_scalars + SC_UMAX, c->W.partial,
+                            c->W.counters + 10, grid_of(c), c->stream))
+    return keep(c, rc);
+  cudaError_t e = cudaMemcpyAsync(umax, c->d_scalars + SC_UMAX, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "max_u", __FILE__, __LINE__));
+  return 0;
+}
+
+int cup_compute_dt(cup_ctx* c, int32_t step, double* dt) {
+  double umax = 0;
+  if (int rc = cup_max_u(c, &umax)) return rc;
+  *dt = calc_dt(c->cfg, c->mesh.spec.hmin, umax, step);
+  if (!(*dt > 0)) return ctx_fail(c, CUP_ERR_NAN, "dt <= 0 or NaN (Simulation.cpp:344-347)");
+  return 0;
+}
+
+int cup_advect_diffuse(cup_ctx* c, double dt) {
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_advect_diffuse: no mesh");
+  if (int rc = advect(c, dt)) return rc;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "advect_diffuse", __FILE__, __LINE__));
+  return 0;
+}
+
+int cup_penalize(cup_ctx* c, double dt, double* force6) {
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_penalize: no mesh");
+  if (int rc = penalize(c, dt)) return rc;
+  cudaError_t e = cudaSuccess;
+  if (force6) e = cudaMemcpyAsync(force6, c->d_scalars + SC_FORCE, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "penalize", __FILE__, __LINE__));
+  return 0;
+}
+
+int cup_pressure_project(cup_ctx* c, double dt, int32_t step, cup_solve_stats* stats) {
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_pressure_project: no mesh");
+  const int rc = project(c, dt, step, stats);
+  if (rc < 0) return rc;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_project", __FILE__, __LINE__));
+  return rc;
+}
+
+int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_stats* stats) {
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_step: no mesh");
+  if (!(dt > 0))
+    if (int rc = cup_compute_dt(c, step, &dt)) return rc;
+  if (dt_used) *dt_used = dt;
+  if (int rc = advect(c, dt)) return rc;
+  if (c->ob.nslots > 0)
+    if (int rc = penalize(c, dt)) return rc;
+  const int rc = project(c, dt, step, stats);
+  if (rc < 0) return rc;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "step", __FILE__, __LINE__));
+  return rc;
 }
 
 }  // extern "C"

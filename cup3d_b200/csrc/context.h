@@ -34,11 +34,17 @@ struct DevArena {
 struct DevObstacle {
   int nslots = 0;
   int* slot_of_block = nullptr;   // nb, -1 when the block holds no obstacle cells
+  int* near = nullptr;            // nb, block or a face neighbour holds obstacle cells
   int* block_of_slot = nullptr;   // nslots
   double* chi = nullptr;          // nslots*512
   double* udef = nullptr;         // 3*nslots*512 (component-major)
   double kin[9] = {0};            // CM[3], vel[3], omega[3]
+  std::vector<int> h_blocks;      // host copies for cup_get_obstacle
+  std::vector<double> h_chi, h_udef;
 };
+
+// Offsets into cup_ctx::d_scalars
+enum : int { SC_SUMS = 0, SC_UMAX = 2, SC_FORCE = 8, SC_KIN = 16 };
 
 struct Fields {
   double* vel[2] = {nullptr, nullptr};  // ping-pong, 3*nb*512 each

@@ -1,0 +1,503 @@
+// Time-step stencil operators (FP64), one CTA per 8^3 block with its ghost
+// layers staged in shared memory.  Each kernel names the reference kernel it
+// computes; coarse-fine flux correction (Cubism FluxCorrection, absent from the
+// reference tree) adds, to a coarse cell next to a finer face, its own face
+// value plus the four fine face values, computed by the coarse block's CTA
+// from the fine blocks' face cells and their ghosts.
+#include "lab.cuh"
+#include "stencils.cuh"
+
+namespace cup3d {
+
+struct Vec3 {
+  double v[3];
+};
+
+// ---------------------------------------------------------------------------
+// AdvectionDiffusion: KernelAdvectDiffuse (AdvectionDiffusion.cpp:19-215)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double sq(double a) { return a * a; }
+
+__device__ __forceinline__ double weno5_plus(double um2, double um1, double u, double up1, double up2) {
+  const double e = 1e-6;
+  const double b1 = 13.0 / 12.0 * sq((um2 + u) - 2 * um1) + 0.25 * sq((um2 + 3 * u) - 4 * um1);
+  const double b2 = 13.0 / 12.0 * sq((um1 + up1) - 2 * u) + 0.25 * sq(um1 - up1);
+  const double b3 = 13.0 / 12.0 * sq((u + up2) - 2 * up1) + 0.25 * sq((3 * u + up2) - 4 * up1);
+  const double what1 = 0.1 / sq(b1 + e);
+  const double what2 = 0.6 / sq(b2 + e);
+  const double what3 = 0.3 / sq(b3 + e);
+  const double aux = 1.0 / ((what1 + what3) + what2);
+  const double w1 = what1 * aux, w2 = what2 * aux, w3 = what3 * aux;
+  const double f1 = (11.0 / 6.0) * u + ((1.0 / 3.0) * um2 - (7.0 / 6.0) * um1);
+  const double f2 = (5.0 / 6.0) * u + ((-1.0 / 6.0) * um1 + (1.0 / 3.0) * up1);
+  const double f3 = (1.0 / 3.0) * u + ((+5.0 / 6.0) * up1 - (1.0 / 6.0) * up2);
+  return (w1 * f1 + w3 * f3) + w2 * f2;
+}
+
+__device__ __forceinline__ double weno5_minus(double um2, double um1, double u, double up1, double up2) {
+  const double e = 1e-6;
+  const double b1 = 13.0 / 12.0 * sq((um2 + u) - 2 * um1) + 0.25 * sq((um2 + 3 * u) - 4 * um1);
+  const double b2 = 13.0 / 12.0 * sq((um1 + up1) - 2 * u) + 0.25 * sq(um1 - up1);
+  const double b3 = 13.0 / 12.0 * sq((u + up2) - 2 * up1) + 0.25 * sq((3 * u + up2) - 4 * up1);
+  const double what1 = 0.3 / sq(b1 + e);
+  const double what2 = 0.6 / sq(b2 + e);
+  const double what3 = 0.1 / sq(b3 + e);
+  const double aux = 1.0 / ((what1 + what3) + what2);
+  const double w1 = what1 * aux, w2 = what2 * aux, w3 = what3 * aux;
+  const double f1 = (1.0 / 3.0) * u + ((-1.0 / 6.0) * um2 + (5.0 / 6.0) * um1);
+  const double f2 = (5.0 / 6.0) * u + ((1.0 / 3.0) * um1 - (1.0 / 6.0) * up1);
+  const double f3 = (11.0 / 6.0) * u + ((-7.0 / 6.0) * up1 + (1.0 / 3.0) * up2);
+  return (w1 * f1 + w3 * f3) + w2 * f2;
+}
+
+template <int SCHEME>
+__device__ __forceinline__ double deriv(double U, double um3, double um2, double um1, double u, double up1,
+                                        double up2, double up3) {
+  if (SCHEME == 1) {
+    double fp, fm;
+    if (U > 0) {
+      fp = weno5_plus(um2, um1, u, up1, up2);
+      fm = weno5_plus(um3, um2, um1, u, up1);
+    } else {
+      fp = weno5_minus(um1, u, up1, up2, up3);
+      fm = weno5_minus(um2, um1, u, up1, up2);
+    }
+    return fp - fm;
+  }
+  if (U > 0) return (-2 * um3 + 15 * um2 - 60 * um1 + 20 * u + 30 * up1 - 3 * up2) / 60.;
+  return (2 * up3 - 15 * up2 + 60 * up1 - 20 * u - 30 * um1 + 3 * um2) / 60.;
+}
+
+__device__ __forceinline__ bool has_finer(const DevMesh& M, int b) {
+  bool r = false;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) r |= M.fkind[b * 6 + f] == K_FINER;
+  return r;
+}
+
+// lab coordinates of own face cell (layer 0) and the ghost at layer 1
+__device__ __forceinline__ void face_lab_pair(int d, int s, int a, int bb, int q[3], int g[3]) {
+  q[d] = s ? BS - 1 : 0;
+  q[tan1(d)] = a;
+  q[tan2(d)] = bb;
+  g[0] = q[0];
+  g[1] = q[1];
+  g[2] = q[2];
+  g[d] += s ? 1 : -1;
+}
+
+template <int SCHEME>
+__global__ void __launch_bounds__(NT, 2)
+    k_advect_stage(DevMesh M, const double* __restrict__ vin, double* __restrict__ vout, double* tmpV, double dt,
+                   double nu, Vec3 ui, int stage) {
+  extern __shared__ double smem[];
+  using LG = LabGeom<3>;
+  double* lab = smem;
+  double* corr = smem + 3 * LG::V;
+  const size_t n = size_t(M.nb) * BN;
+  const double alpha = stage == 0 ? 1.0 / 3.0 : (stage == 1 ? 15.0 / 16.0 : 8.0 / 15.0);
+  const double beta = stage == 0 ? -5.0 / 9.0 : (stage == 1 ? -153.0 / 128.0 : 0.0);
+  auto get = [&](int c, int blk, int cell) { return vin[c * n + size_t(blk) * BN + cell]; };
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    __syncthreads();
+    lab_fill<3, 3>(lab, M, b, get, true);
+    const bool fix = has_finer(M, b);
+    if (fix)
+      for (int i = threadIdx.x; i < 3 * BN; i += NT) corr[i] = 0.0;
+    __syncthreads();
+    const double h = M.h[b], h3 = h * h * h;
+    const double facA = -dt / h * h3;
+    const double facD = (nu / h) * (dt / h) * h3;
+    if (fix) {
+      for (int f = 0; f < 6; ++f) {
+        if (M.fkind[b * 6 + f] != K_FINER) continue;
+        const int d = f >> 1, s = f & 1;
+        if (threadIdx.x < 64) {
+          const int a = threadIdx.x & 7, bb = threadIdx.x >> 3;
+          int q[3], g[3];
+          face_lab_pair(d, s, a, bb, q, g);
+          const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
+          const double hf = M.h[ch];
+          const double facDf = (nu / hf) * (dt / hf) * hf * hf * hf;
+          const int oc = face_cell(d, s, 0, a, bb);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            double val = facD * (lab[c * LG::V + LG::at(q[0], q[1], q[2])] - lab[c * LG::V + LG::at(g[0], g[1], g[2])]);
+#pragma unroll
+            for (int e2 = 0; e2 < 2; ++e2)
+#pragma unroll
+              for (int e1 = 0; e1 < 2; ++e1) {
+                const int fa = 2 * (a & 3) + e1, fb = 2 * (bb & 3) + e2;
+                const double uf = vin[c * n + size_t(ch) * BN + face_cell(d, 1 - s, 0, fa, fb)];
+                const double gf = child_ghost1([&](int cell) { return vin[c * n + size_t(b) * BN + cell]; }, M,
+                                               ch, d, s, fa, fb);
+                val += facDf * (uf - gf);
+              }
+            corr[c * BN + oc] += val;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int qq = 0; qq < 2; ++qq) {
+      const int cell = threadIdx.x + qq * NT;
+      const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+      auto L = [&](int c, int xx, int yy, int zz) { return lab[c * LG::V + LG::at(xx, yy, zz)]; };
+      const double uA[3] = {L(0, x, y, z) + ui.v[0], L(1, x, y, z) + ui.v[1], L(2, x, y, z) + ui.v[2]};
+      double out[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const double dx = deriv<SCHEME>(uA[0], L(c, x - 3, y, z), L(c, x - 2, y, z), L(c, x - 1, y, z), L(c, x, y, z),
+                                        L(c, x + 1, y, z), L(c, x + 2, y, z), L(c, x + 3, y, z));
+        const double dy = deriv<SCHEME>(uA[1], L(c, x, y - 3, z), L(c, x, y - 2, z), L(c, x, y - 1, z), L(c, x, y, z),
+                                        L(c, x, y + 1, z), L(c, x, y + 2, z), L(c, x, y + 3, z));
+        const double dz = deriv<SCHEME>(uA[2], L(c, x, y, z - 3), L(c, x, y, z - 2), L(c, x, y, z - 1), L(c, x, y, z),
+                                        L(c, x, y, z + 1), L(c, x, y, z + 2), L(c, x, y, z + 3));
+        const double sx = L(c, x + 1, y, z) + L(c, x - 1, y, z);
+        const double sy = L(c, x, y + 1, z) + L(c, x, y - 1, z);
+        const double sz = L(c, x, y, z + 1) + L(c, x, y, z - 1);
+        double dD, dA;
+        if (c == 0) {
+          dD = (sx + (sy + sz)) - 6 * L(0, x, y, z);
+          dA = uA[0] * dx + (uA[1] * dy + uA[2] * dz);
+        } else if (c == 1) {
+          dD = (sy + (sz + sx)) - 6 * L(1, x, y, z);
+          dA = uA[1] * dy + (uA[2] * dz + uA[0] * dx);
+        } else {
+          dD = (sz + (sx + sy)) - 6 * L(2, x, y, z);
+          dA = uA[2] * dz + (uA[0] * dx + uA[1] * dy);
+        }
+        out[c] = facA * dA + facD * dD;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const size_t gi = c * n + size_t(b) * BN + cell;
+        double tot = (stage ? tmpV[gi] : 0.0) + out[c];
+        if (fix) tot += corr[c * BN + cell];
+        vout[gi] = L(c, x, y, z) + tot * (alpha / h3);
+        if (stage < 2) tmpV[gi] = tot * beta;
+      }
+    }
+  }
+}
+
+int launch_advect_stage(const DevMesh& M, const double* vin, double* vout, double* tmpV, double dt, double nu,
+                        const double* uinf, int scheme, int stage, int grid, cudaStream_t s) {
+  const size_t smem = (3 * LabGeom<3>::V + 3 * BN) * sizeof(double);
+  static bool attr_set[2] = {false, false};
+  Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
+  if (scheme == 1) {
+    if (!attr_set[1]) {
+      CUP_CUDA_TRY(cudaFuncSetAttribute(k_advect_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      attr_set[1] = true;
+    }
+    k_advect_stage<1><<<grid, NT, smem, s>>>(M, vin, vout, tmpV, dt, nu, ui, stage);
+  } else {
+    if (!attr_set[0]) {
+      CUP_CUDA_TRY(cudaFuncSetAttribute(k_advect_stage<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+      attr_set[0] = true;
+    }
+    k_advect_stage<0><<<grid, NT, smem, s>>>(M, vin, vout, tmpV, dt, nu, ui, stage);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// PressureProjection RHS: KernelPressureRHS (PressureProjection.cpp:96-199),
+// kernelUpdateTmpV (:202-242) and KernelDivPressure (:16-94, step > 2).
+// ---------------------------------------------------------------------------
+struct UdefGet {
+  ObstacleView ob;
+  const double* chi;
+  __device__ __forceinline__ double operator()(int c, int blk, int cell) const {
+    const int sl = ob.slot[blk];
+    if (sl < 0) return 0.0;
+    return chi[size_t(blk) * BN + cell] <= ob.chi[size_t(sl) * BN + cell]
+               ? ob.udef[(size_t(c) * ob.nslots + sl) * BN + cell]
+               : 0.0;
+  }
+};
+
+__global__ void __launch_bounds__(NT)
+    k_pressure_rhs(DevMesh M, const double* __restrict__ vel, const double* __restrict__ pold,
+                   const double* __restrict__ chi, ObstacleView ob, double dt, int use_pold, double* lhs, double* phi) {
+  extern __shared__ double smem[];
+  using LG = LabGeom<1>;
+  double* ulab = smem;
+  double* dlab = ulab + 3 * LG::V;
+  double* plab = dlab + 3 * LG::V;
+  double* corr = plab + LG::V;  // [0,512): RHS flux correction, [512,1024): div p correction
+  const size_t n = size_t(M.nb) * BN;
+  auto getV = [&](int c, int blk, int cell) { return vel[c * n + size_t(blk) * BN + cell]; };
+  auto getP = [&](int, int blk, int cell) { return pold[size_t(blk) * BN + cell]; };
+  UdefGet getD{ob, chi};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    __syncthreads();
+    const bool near = ob.near != nullptr && ob.near[b] != 0;
+    lab_fill<1, 3>(ulab, M, b, getV, true);
+    if (near) lab_fill<1, 3>(dlab, M, b, getD, true);
+    if (use_pold) lab_fill<1, 1>(plab, M, b, getP, false);
+    const bool fix = has_finer(M, b);
+    if (fix)
+      for (int i = threadIdx.x; i < 2 * BN; i += NT) corr[i] = 0.0;
+    __syncthreads();
+    const double h = M.h[b], fac = 0.5 * h * h / dt;
+    auto U = [&](int c, int x, int y, int z) { return ulab[c * LG::V + LG::at(x, y, z)]; };
+    auto D = [&](int c, int x, int y, int z) { return near ? dlab[c * LG::V + LG::at(x, y, z)] : 0.0; };
+    auto P = [&](int x, int y, int z) { return plab[LG::at(x, y, z)]; };
+    if (fix) {
+      for (int f = 0; f < 6; ++f) {
+        if (M.fkind[b * 6 + f] != K_FINER) continue;
+        const int d = f >> 1, s = f & 1;
+        if (threadIdx.x < 64) {
+          const int a = threadIdx.x & 7, bb = threadIdx.x >> 3;
+          int q[3], g[3];
+          face_lab_pair(d, s, a, bb, q, g);
+          const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
+          const double hf = M.h[ch], facf = 0.5 * hf * hf / dt;
+          const int oc = face_cell(d, s, 0, a, bb);
+          const double sg = s ? -1.0 : 1.0, sgc = -sg;
+          const double cq = chi[size_t(b) * BN + oc];
+          double vr = sg * fac * (U(d, g[0], g[1], g[2]) + U(d, q[0], q[1], q[2])) -
+                      sg * cq * fac * (D(d, g[0], g[1], g[2]) + D(d, q[0], q[1], q[2]));
+          double vp = use_pold ? h * (P(q[0], q[1], q[2]) - P(g[0], g[1], g[2])) : 0.0;
+#pragma unroll
+          for (int e2 = 0; e2 < 2; ++e2)
+#pragma unroll
+            for (int e1 = 0; e1 < 2; ++e1) {
+              const int fa = 2 * (a & 3) + e1, fb = 2 * (bb & 3) + e2;
+              const int cf = face_cell(d, 1 - s, 0, fa, fb);
+              const double uf = getV(d, ch, cf);
+              const double gu = child_ghost1([&](int cell) { return getV(d, b, cell); }, M, ch, d, s, fa, fb);
+              const double cf_chi = chi[size_t(ch) * BN + cf];
+              double df = 0.0, gd = 0.0;
+              if (near) {
+                df = getD(d, ch, cf);
+                gd = child_ghost1([&](int cell) { return getD(d, b, cell); }, M, ch, d, s, fa, fb);
+              }
+              vr += sgc * facf * (gu + uf) - sgc * cf_chi * facf * (gd + df);
+              if (use_pold) {
+                const double pf = getP(0, ch, cf);
+                const double gp = child_ghost1([&](int cell) { return getP(0, b, cell); }, M, ch, d, s, fa, fb);
+                vp += hf * (pf - gp);
+              }
+            }
+          corr[oc] += vr;
+          corr[BN + oc] += vp;
+        }
+        __syncthreads();
+      }
+    }
+    for (int qq = 0; qq < 2; ++qq) {
+      const int cell = threadIdx.x + qq * NT;
+      const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+      const size_t gi = size_t(b) * BN + cell;
+      double p = fac * (U(0, x + 1, y, z) - U(0, x - 1, y, z) + U(1, x, y + 1, z) - U(1, x, y - 1, z) +
+                        U(2, x, y, z + 1) - U(2, x, y, z - 1));
+      if (near) {
+        const double divUs = D(0, x + 1, y, z) - D(0, x - 1, y, z) + D(1, x, y + 1, z) - D(1, x, y - 1, z) +
+                             D(2, x, y, z + 1) - D(2, x, y, z - 1);
+        p += -chi[gi] * fac * divUs;
+      }
+      if (fix) p += corr[cell];
+      if (use_pold) {
+        double dp = h * (P(x + 1, y, z) + P(x - 1, y, z) + P(x, y + 1, z) + P(x, y - 1, z) + P(x, y, z + 1) +
+                         P(x, y, z - 1) - 6.0 * P(x, y, z));
+        if (fix) dp += corr[BN + cell];
+        p -= dp;
+      }
+      lhs[gi] = p;
+      phi[gi] = 0.0;
+    }
+  }
+}
+
+int launch_pressure_rhs(const DevMesh& M, const double* vel, const double* pold, const double* chi,
+                        const ObstacleView& ob, double dt, int step, int step_2nd_start, double* lhs, double* phi,
+                        int grid, cudaStream_t s) {
+  const size_t smem = (7 * LabGeom<1>::V + 2 * BN) * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    CUP_CUDA_TRY(cudaFuncSetAttribute(k_pressure_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    attr = true;
+  }
+  k_pressure_rhs<<<grid, NT, smem, s>>>(M, vel, pold, chi, ob, dt, step > step_2nd_start ? 1 : 0, lhs, phi);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Mean removal + incremental pressure (PressureProjection.cpp:404-446) fused
+// with KernelGradP (:244-323) and the velocity update (:451-467).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT)
+    k_grad_update(DevMesh M, double* vel, const double* __restrict__ phi, const double* __restrict__ pold,
+                  double* __restrict__ pnew, const double* sums, double dt, int use_pold) {
+  __shared__ double plab[LabGeom<1>::V];
+  __shared__ double corr[3 * BN];
+  using LG = LabGeom<1>;
+  const size_t n = size_t(M.nb) * BN;
+  const double avg = sums[0] / sums[1];
+  auto getP = [&](int, int blk, int cell) {
+    const size_t i = size_t(blk) * BN + cell;
+    const double p = phi[i] - avg;
+    return use_pold ? p + pold[i] : p;
+  };
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    __syncthreads();
+    lab_fill<1, 1>(plab, M, b, getP, false);
+    const bool fix = has_finer(M, b);
+    if (fix)
+      for (int i = threadIdx.x; i < 3 * BN; i += NT) corr[i] = 0.0;
+    __syncthreads();
+    const double h = M.h[b], fac = -0.5 * dt * h * h;
+    auto P = [&](int x, int y, int z) { return plab[LG::at(x, y, z)]; };
+    if (fix) {
+      for (int f = 0; f < 6; ++f) {
+        if (M.fkind[b * 6 + f] != K_FINER) continue;
+        const int d = f >> 1, s = f & 1;
+        if (threadIdx.x < 64) {
+          const int a = threadIdx.x & 7, bb = threadIdx.x >> 3;
+          int q[3], g[3];
+          face_lab_pair(d, s, a, bb, q, g);
+          const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
+          const double hf = M.h[ch], facf = -0.5 * dt * hf * hf;
+          const double sg = s ? -1.0 : 1.0, sgc = -sg;
+          double v = sg * fac * (P(g[0], g[1], g[2]) + P(q[0], q[1], q[2]));
+#pragma unroll
+          for (int e2 = 0; e2 < 2; ++e2)
+#pragma unroll
+            for (int e1 = 0; e1 < 2; ++e1) {
+              const int fa = 2 * (a & 3) + e1, fb = 2 * (bb & 3) + e2;
+              const int cf = face_cell(d, 1 - s, 0, fa, fb);
+              const double pf = getP(0, ch, cf);
+              const double gp = child_ghost1([&](int cell) { return getP(0, b, cell); }, M, ch, d, s, fa, fb);
+              v += sgc * facf * (gp + pf);
+            }
+          corr[d * BN + face_cell(d, s, 0, a, bb)] += v;
+        }
+        __syncthreads();
+      }
+    }
+    const double ih3 = 1.0 / (h * h * h);
+    for (int qq = 0; qq < 2; ++qq) {
+      const int cell = threadIdx.x + qq * NT;
+      const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+      const size_t gi = size_t(b) * BN + cell;
+      double g0 = fac * (P(x + 1, y, z) - P(x - 1, y, z));
+      double g1 = fac * (P(x, y + 1, z) - P(x, y - 1, z));
+      double g2 = fac * (P(x, y, z + 1) - P(x, y, z - 1));
+      if (fix) {
+        g0 += corr[cell];
+        g1 += corr[BN + cell];
+        g2 += corr[2 * BN + cell];
+      }
+      vel[gi] += ih3 * g0;
+      vel[n + gi] += ih3 * g1;
+      vel[2 * n + gi] += ih3 * g2;
+      pnew[gi] = P(x, y, z);
+    }
+  }
+}
+
+int launch_grad_update(const DevMesh& M, double* vel, const double* phi, const double* pold, double* pnew,
+                       const double* sums, double dt, int step, int step_2nd_start, int grid, cudaStream_t s) {
+  k_grad_update<<<grid, NT, 0, s>>>(M, vel, phi, pold, pnew, sums, dt, step > step_2nd_start ? 1 : 0);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Penalization: KernelPenalization (Penalization.cpp:56-89) on obstacle blocks
+// and the force/torque sums of kernelFinalizePenalizationForce (:91-109).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT)
+    k_penalize(DevMesh M, double* vel, const double* __restrict__ chi, ObstacleView ob, const double* __restrict__ kin,
+               double dt, double lambda, int implicit, GridReduce G, double* force) {
+  __shared__ double red[8 * 6];
+  const size_t n = size_t(M.nb) * BN;
+  const double lambdaFac = implicit ? lambda : 1.0 / dt;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const double CM[3] = {kin[0], kin[1], kin[2]};
+  const double V[3] = {kin[3], kin[4], kin[5]};
+  const double O[3] = {kin[6], kin[7], kin[8]};
+  for (int sl = blockIdx.x; sl < ob.nslots; sl += gridDim.x) {
+    const int b = ob.blk[sl];
+    const double h = M.h[b], dv = h * h * h;
+    for (int cell = threadIdx.x; cell < BN; cell += NT) {
+      const size_t gi = size_t(b) * BN + cell;
+      const double CHI = ob.chi[size_t(sl) * BN + cell];
+      if (chi[gi] > CHI) continue;
+      if (CHI <= 0) continue;
+      const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+      double p[3] = {(M.index[3 * b] * BS + x + 0.5) * h, (M.index[3 * b + 1] * BS + y + 0.5) * h,
+                     (M.index[3 * b + 2] * BS + z + 0.5) * h};
+      p[0] -= CM[0];
+      p[1] -= CM[1];
+      p[2] -= CM[2];
+      const double* ud = ob.udef;
+      const size_t ns = ob.nslots;
+      const double U0 = V[0] + O[1] * p[2] - O[2] * p[1] + ud[(0 * ns + sl) * BN + cell];
+      const double U1 = V[1] + O[2] * p[0] - O[0] * p[2] + ud[(1 * ns + sl) * BN + cell];
+      const double U2 = V[2] + O[0] * p[1] - O[1] * p[0] + ud[(2 * ns + sl) * BN + cell];
+      const double X = implicit ? (CHI > 0.5 ? 1.0 : 0.0) : CHI;
+      const double penalFac = implicit ? X * lambdaFac / (1 + X * lambdaFac * dt) : X * lambdaFac;
+      const double FPX = penalFac * (U0 - vel[gi]);
+      const double FPY = penalFac * (U1 - vel[n + gi]);
+      const double FPZ = penalFac * (U2 - vel[2 * n + gi]);
+      vel[gi] = vel[gi] + dt * FPX;
+      vel[n + gi] = vel[n + gi] + dt * FPY;
+      vel[2 * n + gi] = vel[2 * n + gi] + dt * FPZ;
+      acc[0] += dv * FPX;
+      acc[1] += dv * FPY;
+      acc[2] += dv * FPZ;
+      acc[3] += dv * (p[1] * FPZ - p[2] * FPY);
+      acc[4] += dv * (p[2] * FPX - p[0] * FPZ);
+      acc[5] += dv * (p[0] * FPY - p[1] * FPX);
+    }
+  }
+  if (grid_reduce<6>(acc, G, red) && threadIdx.x == 0)
+    for (int q = 0; q < 6; ++q) force[q] = acc[q];
+}
+
+int launch_penalize(const DevMesh& M, double* vel, const double* chi, const ObstacleView& ob, const double* kin,
+                    double dt, double lambda, int implicit, double* force, double* partial, unsigned* counter,
+                    cudaStream_t s) {
+  if (ob.nslots <= 0) {
+    CUP_CUDA_TRY(cudaMemsetAsync(force, 0, 6 * sizeof(double), s));
+    return 0;
+  }
+  const int grid = std::min(ob.nslots, 1184);
+  GridReduce G{partial, counter};
+  k_penalize<<<grid, NT, 0, s>>>(M, vel, chi, ob, kin, dt, lambda, implicit, G, force);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// findMaxU (ProcessHelpers.h:71-94)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_max_u(size_t n, const double* __restrict__ vel, Vec3 ui, GridReduce G,
+                                              double* out) {
+  __shared__ double red[8];
+  double m = 0.0;
+  for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n; i += size_t(gridDim.x) * NT) {
+    const double a = fabs(vel[i] + ui.v[0]);
+    const double b = fabs(vel[n + i] + ui.v[1]);
+    const double c = fabs(vel[2 * n + i] + ui.v[2]);
+    m = fmax(m, fmax(a, fmax(b, c)));
+  }
+  if (grid_reduce_max(m, G, red) && threadIdx.x == 0) *out = m;
+}
+
+int launch_max_u(const DevMesh& M, const double* vel, const double* uinf, double* out, double* partial,
+                 unsigned* counter, int grid, cudaStream_t s) {
+  GridReduce G{partial, counter};
+  Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
+  k_max_u<<<grid, NT, 0, s>>>(size_t(M.nb) * BN, vel, ui, G, out);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace cup3d

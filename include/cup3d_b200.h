@@ -133,6 +133,32 @@ int cup_poisson_solve_dev(cup_ctx* ctx, const double* d_b, double* d_x, cup_solv
 /* ---- PoissonSolverBase::solve(): RHS in CUP_FIELD_LHS, guess and result in CUP_FIELD_PRES ---- */
 int cup_poisson_solve(cup_ctx* ctx, cup_solve_stats* stats);
 
+/* ---- obstacles (host-side CreateObstacles; one body per context) ---- */
+/* Sphere of radius r at c (Sphere.cpp); chi by ObstaclesCreate.cpp:18-121;
+ * kin = velocity[3], angular velocity[3] (may be NULL).  Also sets CUP_FIELD_CHI. */
+int cup_obstacle_sphere(cup_ctx* ctx, const double* c, double r, const double* vel, const double* omega);
+/* Ellipsoid with semi-axes ax[3] rotated by the unit quaternion q = (w,x,y,z). */
+int cup_obstacle_ellipsoid(cup_ctx* ctx, const double* c, const double* ax, const double* q,
+                           const double* vel, const double* omega);
+/* Raw obstacle data: nslots obstacle blocks, block_of_slot[nslots] (device
+ * order), chi[nslots*512], udef[3*nslots*512] (component-major), kin[9] =
+ * centre of mass, velocity, angular velocity.  nslots = 0 removes the body. */
+int cup_set_obstacle(cup_ctx* ctx, int32_t nslots, const int32_t* block_of_slot, const double* chi,
+                     const double* udef, const double* kin);
+/* Reads back the obstacle data; returns nslots (arrays may be NULL to query). */
+int cup_get_obstacle(const cup_ctx* ctx, int32_t* block_of_slot, double* chi, double* udef, double* kin);
+
+/* ---- the time-step operators (Operator::operator()(dt) of the reference) ---- */
+int cup_max_u(cup_ctx* ctx, double* umax);                          /* findMaxU */
+/* calcMaxTimestep (Simulation.cpp:309-375) for `step`: dt from max|u+uinf|. */
+int cup_compute_dt(cup_ctx* ctx, int32_t step, double* dt);
+int cup_advect_diffuse(cup_ctx* ctx, double dt);                    /* AdvectionDiffusion */
+int cup_penalize(cup_ctx* ctx, double dt, double* force_torque6);   /* Penalization */
+int cup_pressure_project(cup_ctx* ctx, double dt, int32_t step, cup_solve_stats* stats);
+/* One time step: AdvectionDiffusion, Penalization (if a body is set),
+ * PressureProjection.  dt <= 0: computed by calcMaxTimestep; *dt_used gets it. */
+int cup_step(cup_ctx* ctx, int32_t step, double dt, double* dt_used, cup_solve_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

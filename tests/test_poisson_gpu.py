@@ -69,8 +69,11 @@ def test_solve_matches_oracle(name):
     rc, st = ctx.poisson_solve_dev(bd, xd)
     x = xd.cpu().numpy()
     assert rc == 0 and st["status"] == 1
-    assert abs(st["iterations"] - st_ref["iterations"]) <= 1, (st, st_ref)
     assert np.linalg.norm(x - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
+    # iteration counts agree up to the rounding-sensitive restart test
+    # (rho^2 < 1e-16 |r|^2 |rhat|^2, BiCGSTAB.cu:489)
+    slack = 1 if st_ref["restarts"] == 0 else 3
+    assert abs(st["iterations"] - st_ref["iterations"]) <= slack, (st, st_ref)
 
 
 def test_solve_through_fields_matches_device_buffers():
