@@ -1,0 +1,351 @@
+"""Benchmark of the time-step hot path (one JSON line on rank 0).
+
+Workload (N=1): flow past a fixed sphere at Re=300 -- domain 4x2x2, 4x2x2
+level-0 blocks of 8^3 cells, levelMax 4 (mesh frozen after refinement around
+the sphere and its wake: 2340 blocks, 1.198M cells), sphere radius 0.0625 at
+(1,1,1) moving at +0.1 in x with the frame following it (uinf = -0.1),
+nu = 0.1*0.125/300, WENO5, implicit penalization lambda=1e6, plain FP64
+BiCGSTAB with the exact block preconditioner, reference tolerances
+(-poissonTol 1e-6, -poissonTolRel 1e-4).  A "step" is one full time step:
+calcMaxTimestep, AdvectionDiffusion (3 RK stages), Penalization,
+PressureProjection (RHS, Poisson solve, mean removal, gradient update).
+
+`value`  Mcell-steps/s with the fields resident in HBM (device time, CUDA
+         events on the context's stream), L2 flushed between timed steps.
+`e2e`    the same through the reference-facing C ABI with host buffers:
+         per step velocity + pressure uploaded from pinned host memory, the
+         step, velocity + pressure downloaded.
+`--impl reference`  the reference's CPU path restated (oracle: upwind/WENO,
+         penalization, projection with the pipelined BiCGSTAB + block CG of
+         PoissonSolverAMR.cpp) on the host cores, one step per sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SPHERE_FLAGS = ("-bpdx 4 -bpdy 2 -bpdz 2 -levelMax 4 -extent 4 -nu 4.1666666666666667e-05 -CFL 0.3 "
+                "-lambda 1e6 -advection weno5 -uinfx -0.1 -poissonTol 1e-6 -poissonTolRel 1e-4 -rampup 100")
+SPHERE_MESH = dict(center=(1.0, 1.0, 1.0), radius=0.0625, flow_dir=-1, near_radius=2.5, wake_len=1.0,
+                   wake_radius=3.0)
+SPHERE_BODY = dict(center=(1.0, 1.0, 1.0), radius=0.0625, vel=(0.1, 0.0, 0.0))
+WORKLOAD = "sphere_re300_amr_levelmax4_weno5_fp64"
+
+# Algorithmic bytes per cell per launch (each array read once and written once,
+# halos excluded, 8-byte reals).
+ALG_BYTES = {
+    "advect_stage_weno5": 8 * 10,       # mean over stages of 9S/12S/9S (R u, tmpV; W u, tmpV)
+    "advect_stage_upwind5": 8 * 10,
+    "pressure_rhs": 8 * 7,              # R u(3), chi, p_old; W lhs, phi
+    "grad_update": 8 * 9,               # R phi, p_old, u(3); W u(3), p_new
+    "bicg_a_pupdate_precond": 8 * 5,    # R r, p, nu; W p, z1
+    "bicg_b_spmv_dot": 8 * 3,           # R z1, rhat; W nu
+    "bicg_c_supdate_precond": 8 * 4,    # R r, nu; W r, z2
+    "bicg_d_spmv_dots": 8 * 3,          # R z2, r; W t
+    "bicg_e_xr_update_dots": 8 * 8,     # R x, z1, z2, r, t, rhat; W x, r
+    "bicg_init": 8 * 6,
+    "weighted_sum": 8 * 1,
+    "max_u": 8 * 3,
+}
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([s.strip() for s in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and "Active" in r[3 + i]
+                          and "Not" not in r[3 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_sphere_ctx(device, solver="b200"):
+    import cup3d_b200 as cup
+    cfg = cup.config(SPHERE_FLAGS + f" -poissonSolver {solver}", device=device)
+    ctx = cup.Context(cfg)
+    ctx.set_mesh_sphere_wake(**SPHERE_MESH)
+    ctx.obstacle_sphere(**SPHERE_BODY)
+    return ctx
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def run_b200(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    import cup3d_b200 as cup
+    ctx = make_sphere_ctx(local)
+    nb = ctx.nb
+    ncell = nb * 512
+    stream = torch.cuda.ExternalStream(cup._lib.lib().cup_stream(ctx._p))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    step = 0
+    for _ in range(args.warmup):
+        ctx.step(step)
+        step += 1
+    # ---- timed region: device-resident --------------------------------------
+    ctx.profile(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    times = []
+    iters = []
+    solve_ms = []
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)  # L2 flush outside the timed events
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dt, rc, st = ctx.step(step)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        iters.append(st["iterations"])
+        solve_ms.append(st["milliseconds"])
+        step += 1
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * ncell * args.steps / (total_ms * 1e-3) / 1e6
+    launches = sum(v[0] for v in prof.values())
+    # roofline of the dominant kernel (largest total device time)
+    peak, peak_kind = measured_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    dom_name, (dom_n, dom_ms) = dom
+    per_launch_ms = dom_ms / max(dom_n, 1)
+    alg_bytes = ALG_BYTES.get(dom_name, 0) * ncell
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if alg_bytes else None
+    # ---- e2e through the C ABI with host buffers -------------------------------
+    vel_h = torch.empty(3 * ncell, dtype=torch.float64).pin_memory()
+    pres_h = torch.empty(ncell, dtype=torch.float64).pin_memory()
+    vel_h.numpy()[:] = ctx.download("vel")
+    pres_h.numpy()[:] = ctx.download("pres")
+    lib = cup._lib.lib()
+    import ctypes as C
+    vp = C.cast(vel_h.data_ptr(), cup._lib._D)
+    pp = C.cast(pres_h.data_ptr(), cup._lib._D)
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cup._lib.check(lib.cup_upload_field(ctx._p, 0, vp), ctx._p)
+        cup._lib.check(lib.cup_upload_field(ctx._p, 1, pp), ctx._p)
+        ctx.step(step)
+        cup._lib.check(lib.cup_download_field(ctx._p, 0, vp), ctx._p)
+        cup._lib.check(lib.cup_download_field(ctx._p, 1, pp), ctx._p)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+        step += 1
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * ncell * args.steps / (e2e_ms * 1e-3) / 1e6
+    line = {
+        "metric": "Mcell-steps/s (whole time step, sphere Re=300 AMR, plain FP64)",
+        "value": round(value, 3),
+        "unit": "Mcell-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded, generated in-process)",
+        "config": {"workload": WORKLOAD, "blocks": nb, "cells": ncell, "levels_used": [1, 2, 3],
+                   "poisson": "b200 fp64 BiCGSTAB + exact block inverse, tol 1e-6 abs / 1e-4 rel",
+                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps",
+                   "first_timed_step": args.warmup},
+        "poisson": {"iterations_per_step": iters, "solve_ms_per_step": [round(x, 3) for x in solve_ms]},
+        "kernels": {k: {"launches": v[0], "ms": round(v[1], 4)} for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1) if achieved else None,
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+                     "peak_source": peak_kind, "alg_bytes_per_launch": alg_bytes,
+                     "launch_ms": round(per_launch_ms, 5), "traffic": None},
+        "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
+                "h2d_bytes_per_step": 4 * 8 * ncell, "d2h_bytes_per_step": 4 * 8 * ncell},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(ctx, args)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_reference_step(ctx_host_state, m, slot, chi_o, udef_o, kin, chi, step, uinf, nu, cfl, lam):
+    """One step of the reference CPU path restated in the oracle (timed)."""
+    import oracle
+    vel, pres = ctx_host_state
+    umax = m.max_u(vel, uinf)
+    dt = oracle.dt(m.hmin, nu, cfl, umax, step, 100)
+    t0 = time.perf_counter()
+    vel = m.advect_diffuse(vel, dt, nu, uinf=uinf, scheme=1)
+    vel, _ = m.penalize(vel, chi, slot, chi_o, udef_o, kin, dt, lam=lam, implicit=1)
+    vel, pres, info = m.pressure_project(vel, pres, dt, step, chi=chi, slot=slot, chi_o=chi_o, udef_o=udef_o,
+                                         solver=1, tol=1e-6, tol_rel=1e-4)
+    return time.perf_counter() - t0, (vel, pres), info
+
+
+def cpu_baseline(ctx, args):
+    import oracle
+    level, index, _ = ctx.blocks()
+    m = oracle.Mesh(level, index, [4, 2, 2], 4, [0, 0, 0], 4.0)
+    slot, chi_o, udef_o, kin = ctx.get_obstacle()
+    chi = ctx.download("chi")
+    state = (ctx.download("vel"), ctx.download("pres"))
+    secs, _, info = cpu_reference_step(state, m, slot, chi_o, udef_o, kin, chi, args.warmup + 2 * args.steps,
+                                       (-0.1, 0.0, 0.0), 4.1666666666666667e-05, 0.3, 1e6)
+    return {"value": round(m.n / secs / 1e6, 4), "unit": "Mcell-steps/s", "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": f"1 full time step of the same workload from the GPU run's state "
+                      f"(oracle, OpenMP, pipelined BiCGSTAB + block CG, {info['iterations']} iterations, "
+                      f"{secs:.2f} s)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import cup3d_b200 as cup
+    import oracle
+    cfg = cup.config(SPHERE_FLAGS, device=-1)
+    ctx = cup.Context(cfg)
+    ctx.set_mesh_sphere_wake(**SPHERE_MESH)
+    level, index, h = ctx.blocks()
+    m = oracle.Mesh(level, index, [4, 2, 2], 4, [0, 0, 0], 4.0)
+    # obstacle data from the same host code path (no device needed)
+    slot, chi_o, udef_o, kin, chi = host_sphere(ctx)
+    vel = np.zeros(3 * m.n)
+    pres = np.zeros(m.n)
+    state = (vel, pres)
+    step = 0
+    for _ in range(args.warmup):
+        _, state, _ = cpu_reference_step(state, m, slot, chi_o, udef_o, kin, chi, step, (-0.1, 0, 0),
+                                         4.1666666666666667e-05, 0.3, 1e6)
+        step += 1
+    total = 0.0
+    for _ in range(args.steps):
+        secs, state, _ = cpu_reference_step(state, m, slot, chi_o, udef_o, kin, chi, step, (-0.1, 0, 0),
+                                            4.1666666666666667e-05, 0.3, 1e6)
+        total += secs
+        step += 1
+    value = m.n * args.steps / total / 1e6
+    line = {
+        "impl": "reference",
+        "metric": "Mcell-steps/s (whole time step, sphere Re=300 AMR, plain FP64)",
+        "value": round(value, 4), "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "blocks": m.nb, "cells": m.n},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "port",
+                         "sample": "full time steps from rest on the frozen sphere mesh (oracle restatement of the "
+                                   "reference CPU path, OpenMP over blocks)"},
+        "e2e": {"value": round(value, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def host_sphere(ctx):
+    """Sphere obstacle arrays from the product's host obstacle code (host-only context)."""
+    ctx.obstacle_sphere(**SPHERE_BODY)
+    slot, chi_o, udef_o, kin = ctx.get_obstacle()
+    chi = np.zeros(ctx.nb * 512)
+    for b in np.where(slot >= 0)[0]:
+        chi[b * 512:(b + 1) * 512] = chi_o[slot[b] * 512:(slot[b] + 1) * 512]
+    return slot, chi_o, udef_o, kin, chi
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -192,3 +192,14 @@ class Context:
         st = cup_solve_stats()
         rc = check(lib().cup_step(self._p, step, dt, C.byref(used), C.byref(st)), self._p)
         return used.value, rc, st.as_dict()
+
+    # ---- profiling ----------------------------------------------------------
+    def profile(self, enable=True):
+        check(lib().cup_profile(self._p, int(enable)), self._p)
+
+    def profile_read(self):
+        """{phase: (launches, milliseconds)} accumulated since profile(True)."""
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        check(lib().cup_profile_read(self._p, buf, len(buf)), self._p)
+        return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}

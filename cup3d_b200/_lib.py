@@ -91,6 +91,7 @@ SIGNATURES = {
     "cup_upload_field": (C.c_int, [_P, C.c_int32, _D]),
     "cup_download_field": (C.c_int, [_P, C.c_int32, _D]),
     "cup_field_device_ptr": (C.c_void_p, [_P, C.c_int32]),
+    "cup_stream": (C.c_void_p, [_P]),
     "cup_poisson_apply_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int32]),
     "cup_block_inverse_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_poisson_solve_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.POINTER(cup_solve_stats)]),
@@ -105,6 +106,8 @@ SIGNATURES = {
     "cup_penalize": (C.c_int, [_P, C.c_double, _D]),
     "cup_pressure_project": (C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(cup_solve_stats)]),
     "cup_step": (C.c_int, [_P, C.c_int32, C.c_double, _D, C.POINTER(cup_solve_stats)]),
+    "cup_profile": (C.c_int, [_P, C.c_int32]),
+    "cup_profile_read": (C.c_int, [_P, C.c_char_p, C.c_int32]),
 }
 
 

@@ -11,6 +11,7 @@
 namespace cup3d {
 
 static thread_local std::string g_last_error;
+thread_local Profiler* t_prof = nullptr;
 
 int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
   std::ostringstream os;
@@ -362,6 +363,8 @@ int cup_download_field(cup_ctx* c, int32_t field, double* host) {
   return 0;
 }
 
+void* cup_stream(cup_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
+
 double* cup_field_device_ptr(cup_ctx* c, int32_t field) {
   if (!c) return nullptr;
   int nc;
@@ -369,6 +372,7 @@ double* cup_field_device_ptr(cup_ctx* c, int32_t field) {
 }
 
 int cup_poisson_apply_dev(cup_ctx* c, const double* x, double* y, int32_t mean_mode) {
+  ProfBind pb_(c);
   if (!c || !x || !y || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_apply_dev: bad arguments");
   const int mm = mean_mode >= 0 ? mean_mode : c->cfg.mean_constraint;
   if (int rc = launch_poisson_apply(c->dm, x, y, mm, c->W, c->stream)) return keep(c, rc);
@@ -378,6 +382,7 @@ int cup_poisson_apply_dev(cup_ctx* c, const double* x, double* y, int32_t mean_m
 }
 
 int cup_block_inverse_dev(cup_ctx* c, const double* in, double* out) {
+  ProfBind pb_(c);
   if (!c || !in || !out || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_block_inverse_dev: bad arguments");
   if (int rc = launch_block_inverse(c->dm, in, out, c->W, c->stream)) return keep(c, rc);
   cudaError_t e = cudaStreamSynchronize(c->stream);
@@ -415,11 +420,13 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
 }
 
 int cup_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats) {
+  ProfBind pb_(c);
   if (!c || !b || !x || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve_dev: bad arguments");
   return solve_impl(c, b, x, stats);
 }
 
 int cup_poisson_solve(cup_ctx* c, cup_solve_stats* stats) {
+  ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve: no mesh");
   return solve_impl(c, c->F.lhs, c->F.pres[c->F.pcur], stats);
 }
@@ -466,12 +473,6 @@ static int upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const 
     near[b] = nr;
   }
   DevObstacle& o = c->ob;
-  DevArena& A = c->obst_arena;
-  if (int rc = A.alloc(&o.slot_of_block, m.nb)) return keep(c, rc);
-  if (int rc = A.alloc(&o.near, m.nb)) return keep(c, rc);
-  if (int rc = A.alloc(&o.block_of_slot, nslots)) return keep(c, rc);
-  if (int rc = A.alloc(&o.chi, size_t(nslots) * BN)) return keep(c, rc);
-  if (int rc = A.alloc(&o.udef, 3 * size_t(nslots) * BN)) return keep(c, rc);
   o.nslots = nslots;
   o.h_blocks.assign(blocks, blocks + nslots);
   o.h_chi.assign(chi, chi + size_t(nslots) * BN);
@@ -480,6 +481,13 @@ static int upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const 
   else
     o.h_udef.assign(3 * size_t(nslots) * BN, 0.0);
   for (int i = 0; i < 9; ++i) o.kin[i] = kin ? kin[i] : 0.0;
+  if (c->host_only) return 0;  // host copies only
+  DevArena& A = c->obst_arena;
+  if (int rc = A.alloc(&o.slot_of_block, m.nb)) return keep(c, rc);
+  if (int rc = A.alloc(&o.near, m.nb)) return keep(c, rc);
+  if (int rc = A.alloc(&o.block_of_slot, nslots)) return keep(c, rc);
+  if (int rc = A.alloc(&o.chi, size_t(nslots) * BN)) return keep(c, rc);
+  if (int rc = A.alloc(&o.udef, 3 * size_t(nslots) * BN)) return keep(c, rc);
   CUP_CUDA_TRY(cudaMemcpy(o.slot_of_block, slot.data(), m.nb * sizeof(int), cudaMemcpyHostToDevice));
   CUP_CUDA_TRY(cudaMemcpy(o.near, near.data(), m.nb * sizeof(int), cudaMemcpyHostToDevice));
   CUP_CUDA_TRY(cudaMemcpy(o.block_of_slot, blocks, nslots * sizeof(int), cudaMemcpyHostToDevice));
@@ -492,6 +500,7 @@ static int upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const 
 static int install_host_obstacle(cup_ctx* c, const HostObstacle& h) {
   if (int rc = upload_obstacle(c, int(h.blocks.size()), h.blocks.data(), h.chi.data(), h.udef.data(), h.kin))
     return rc;
+  if (c->host_only) return 0;
   CUP_CUDA_TRY(cudaMemcpy(c->F.chi, h.grid_chi.data(), h.grid_chi.size() * 8, cudaMemcpyHostToDevice));
   return 0;
 }
@@ -551,7 +560,7 @@ static int project(cup_ctx* c, double dt, int step, cup_solve_stats* stats) {
 extern "C" {
 
 int cup_obstacle_sphere(cup_ctx* c, const double* ctr, double r, const double* vel, const double* omega) {
-  if (!c || !ctr || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_sphere: bad arguments");
+  if (!c || !ctr || c->mesh.nb == 0) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_sphere: bad arguments");
   const double z[3] = {0, 0, 0};
   HostObstacle h;
   make_sphere(c->mesh, ctr, r, vel ? vel : z, omega ? omega : z, h);
@@ -560,7 +569,7 @@ int cup_obstacle_sphere(cup_ctx* c, const double* ctr, double r, const double* v
 
 int cup_obstacle_ellipsoid(cup_ctx* c, const double* ctr, const double* ax, const double* q, const double* vel,
                            const double* omega) {
-  if (!c || !ctr || !ax || !q || c->mesh.nb == 0 || c->host_only)
+  if (!c || !ctr || !ax || !q || c->mesh.nb == 0)
     return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_ellipsoid: bad arguments");
   const double z[3] = {0, 0, 0};
   HostObstacle h;
@@ -570,7 +579,7 @@ int cup_obstacle_ellipsoid(cup_ctx* c, const double* ctr, const double* ax, cons
 
 int cup_set_obstacle(cup_ctx* c, int32_t nslots, const int32_t* blocks, const double* chi, const double* udef,
                      const double* kin) {
-  if (!c || c->mesh.nb == 0 || c->host_only || (nslots > 0 && (!blocks || !chi)))
+  if (!c || c->mesh.nb == 0 || (nslots > 0 && (!blocks || !chi)))
     return ctx_fail(c, CUP_ERR_ARG, "cup_set_obstacle: bad arguments");
   return upload_obstacle(c, nslots, blocks, chi, udef, kin);
 }
@@ -586,6 +595,7 @@ int cup_get_obstacle(const cup_ctx* c, int32_t* blocks, double* chi, double* ude
 }
 
 int cup_max_u(cup_ctx* c, double* umax) {
+  ProfBind pb_(c);
   if (!c || !umax || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_max_u: bad arguments");
   if (int rc = launch_max_u(c->dm, c->F.vel[c->F.vcur], c->cfg.uinf, c->d_scalars + SC_UMAX, c->W.partial,
                             c->W.counters + 10, grid_of(c), c->stream))
@@ -605,6 +615,7 @@ int cup_compute_dt(cup_ctx* c, int32_t step, double* dt) {
 }
 
 int cup_advect_diffuse(cup_ctx* c, double dt) {
+  ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_advect_diffuse: no mesh");
   if (int rc = advect(c, dt)) return rc;
   cudaError_t e = cudaStreamSynchronize(c->stream);
@@ -613,6 +624,7 @@ int cup_advect_diffuse(cup_ctx* c, double dt) {
 }
 
 int cup_penalize(cup_ctx* c, double dt, double* force6) {
+  ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_penalize: no mesh");
   if (int rc = penalize(c, dt)) return rc;
   cudaError_t e = cudaSuccess;
@@ -623,6 +635,7 @@ int cup_penalize(cup_ctx* c, double dt, double* force6) {
 }
 
 int cup_pressure_project(cup_ctx* c, double dt, int32_t step, cup_solve_stats* stats) {
+  ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_pressure_project: no mesh");
   const int rc = project(c, dt, step, stats);
   if (rc < 0) return rc;
@@ -632,6 +645,7 @@ int cup_pressure_project(cup_ctx* c, double dt, int32_t step, cup_solve_stats* s
 }
 
 int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_stats* stats) {
+  ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_step: no mesh");
   if (!(dt > 0))
     if (int rc = cup_compute_dt(c, step, &dt)) return rc;
@@ -644,6 +658,34 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "step", __FILE__, __LINE__));
   return rc;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int cup_profile(cup_ctx* c, int32_t enable) {
+  if (!c || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_profile: no device context");
+  c->prof.reset();
+  c->prof.on = enable != 0;
+  return 0;
+}
+
+int cup_profile_read(cup_ctx* c, char* buf, int32_t len) {
+  if (!c || !buf || len <= 0) return ctx_fail(c, CUP_ERR_ARG, "cup_profile_read: bad arguments");
+  c->prof.flush();
+  std::ostringstream os;
+  os.precision(9);
+  os << "{";
+  for (size_t i = 0; i < c->prof.names.size(); ++i) {
+    if (i) os << ",";
+    os << "\"" << c->prof.names[i] << "\":[" << c->prof.acc[i].launches << "," << c->prof.acc[i].ms << "]";
+  }
+  os << "}";
+  const std::string js = os.str();
+  if (int(js.size()) + 1 > len) return ctx_fail(c, CUP_ERR_ARG, "cup_profile_read: buffer too small");
+  std::memcpy(buf, js.c_str(), js.size() + 1);
+  return int(js.size());
 }
 
 }  // extern "C"

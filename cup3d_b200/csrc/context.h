@@ -7,6 +7,7 @@
 #include "common.cuh"
 #include "mesh.h"
 #include "poisson.cuh"
+#include "profiler.h"
 
 namespace cup3d {
 
@@ -73,10 +74,16 @@ struct cup_ctx {
   double* d_scalars = nullptr;    // 64 device doubles for misc reductions
   int num_sms = 148;
   bool host_only = false;         // device < 0: mesh work only
+  cup3d::Profiler prof;
   std::string err;
 };
 
 namespace cup3d {
+// Binds the context's profiler to this thread for the duration of an API call.
+struct ProfBind {
+  ProfBind(cup_ctx* c) { t_prof = (c && c->prof.on) ? &c->prof : nullptr; }
+  ~ProfBind() { t_prof = nullptr; }
+};
 int ctx_fail(cup_ctx* c, int code, const std::string& msg);
 size_t nbn(const cup_ctx* c);
 }  // namespace cup3d

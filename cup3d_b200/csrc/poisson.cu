@@ -17,6 +17,7 @@
 #include <cstring>
 
 #include "poisson.cuh"
+#include "profiler.h"
 
 namespace cup3d {
 
@@ -640,7 +641,7 @@ static KArgs make_args(const DevMesh& M, const double* b, double* x, PoissonWork
 int launch_weighted_sum(const DevMesh& M, const double* v, double* d_out, PoissonWork& W,
                         cudaStream_t s) {
   GridReduce g{W.partial, W.counters + 8};
-  k_weighted_sum<<<W.grid, NT, 0, s>>>(M, v, g, d_out, nullptr);
+  { ProfScope ps("weighted_sum", s); k_weighted_sum<<<W.grid, NT, 0, s>>>(M, v, g, d_out, nullptr); }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -651,10 +652,10 @@ int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_
   GridReduce g{W.partial, W.counters + 9};
   double* ms = &W.st->mean_sum;
   if (mean_mode == 1 || mean_mode == 2) {
-    k_weighted_sum<<<W.grid, NT, 0, s>>>(M, x, g, nullptr, ms);
+    { ProfScope ps("weighted_sum", s); k_weighted_sum<<<W.grid, NT, 0, s>>>(M, x, g, nullptr, ms); }
     CUP_CUDA_TRY(cudaGetLastError());
   }
-  k_spmv<<<W.grid, NT, 0, s>>>(M, x, y, ms, mean_mode);
+  { ProfScope ps("spmv", s); k_spmv<<<W.grid, NT, 0, s>>>(M, x, y, ms, mean_mode); }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -662,7 +663,7 @@ int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_
 int launch_block_inverse(const DevMesh& M, const double* in, double* out, PoissonWork& W,
                          cudaStream_t s) {
   poisson_init_constants();
-  k_block_inverse<<<W.grid, NT, 0, s>>>(M, in, out);
+  { ProfScope ps("block_inverse", s); k_block_inverse<<<W.grid, NT, 0, s>>>(M, in, out); }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -678,17 +679,17 @@ int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolvePa
   init.eps = 1e-21;
   CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   KArgs A = make_args(M, b, x, W, P.mean_mode, 0);
-  k_bicg_prepare<<<W.grid, NT, 0, s>>>(A);
-  k_bicg_init<<<W.grid, NT, 0, s>>>(A);
+  { ProfScope ps("bicg_prepare", s); k_bicg_prepare<<<W.grid, NT, 0, s>>>(A); }
+  { ProfScope ps("bicg_init", s); k_bicg_init<<<W.grid, NT, 0, s>>>(A); }
   CUP_CUDA_TRY(cudaGetLastError());
   const int chunk = P.check_every > 0 ? P.check_every : 8;
   for (int it = 0; it < P.max_iter; it += chunk) {
     for (int j = 0; j < chunk; ++j) {
-      k_bicg_a<<<W.grid, NT, 0, s>>>(A);
-      k_bicg_b<<<W.grid, NT, 0, s>>>(A);
-      k_bicg_c<<<W.grid, NT, 0, s>>>(A);
-      k_bicg_d<<<W.grid, NT, 0, s>>>(A);
-      k_bicg_e<<<W.grid, NT, 0, s>>>(A);
+      { ProfScope ps("bicg_a_pupdate_precond", s); k_bicg_a<<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps("bicg_b_spmv_dot", s); k_bicg_b<<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps("bicg_c_supdate_precond", s); k_bicg_c<<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps("bicg_d_spmv_dots", s); k_bicg_d<<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps("bicg_e_xr_update_dots", s); k_bicg_e<<<W.grid, NT, 0, s>>>(A); }
     }
     CUP_CUDA_TRY(cudaGetLastError());
     CUP_CUDA_TRY(cudaMemcpyAsync(h_done, &W.st->done, sizeof(int), cudaMemcpyDeviceToHost, s));

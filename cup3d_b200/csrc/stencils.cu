@@ -6,6 +6,7 @@
 // from the fine blocks' face cells and their ghosts.
 #include "lab.cuh"
 #include "stencils.cuh"
+#include "profiler.h"
 
 namespace cup3d {
 
@@ -191,12 +192,14 @@ int launch_advect_stage(const DevMesh& M, const double* vin, double* vout, doubl
       CUP_CUDA_TRY(cudaFuncSetAttribute(k_advect_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
       attr_set[1] = true;
     }
+    ProfScope ps("advect_stage_weno5", s);
     k_advect_stage<1><<<grid, NT, smem, s>>>(M, vin, vout, tmpV, dt, nu, ui, stage);
   } else {
     if (!attr_set[0]) {
       CUP_CUDA_TRY(cudaFuncSetAttribute(k_advect_stage<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
       attr_set[0] = true;
     }
+    ProfScope ps("advect_stage_upwind5", s);
     k_advect_stage<0><<<grid, NT, smem, s>>>(M, vin, vout, tmpV, dt, nu, ui, stage);
   }
   CUP_CUDA_TRY(cudaGetLastError());
@@ -322,6 +325,7 @@ int launch_pressure_rhs(const DevMesh& M, const double* vel, const double* pold,
     CUP_CUDA_TRY(cudaFuncSetAttribute(k_pressure_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     attr = true;
   }
+  ProfScope ps("pressure_rhs", s);
   k_pressure_rhs<<<grid, NT, smem, s>>>(M, vel, pold, chi, ob, dt, step > step_2nd_start ? 1 : 0, lhs, phi);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
@@ -403,6 +407,7 @@ __global__ void __launch_bounds__(NT)
 
 int launch_grad_update(const DevMesh& M, double* vel, const double* phi, const double* pold, double* pnew,
                        const double* sums, double dt, int step, int step_2nd_start, int grid, cudaStream_t s) {
+  ProfScope ps("grad_update", s);
   k_grad_update<<<grid, NT, 0, s>>>(M, vel, phi, pold, pnew, sums, dt, step > step_2nd_start ? 1 : 0);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
@@ -470,6 +475,7 @@ int launch_penalize(const DevMesh& M, double* vel, const double* chi, const Obst
   }
   const int grid = std::min(ob.nslots, 1184);
   GridReduce G{partial, counter};
+  ProfScope ps("penalize", s);
   k_penalize<<<grid, NT, 0, s>>>(M, vel, chi, ob, kin, dt, lambda, implicit, G, force);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
@@ -495,6 +501,7 @@ int launch_max_u(const DevMesh& M, const double* vel, const double* uinf, double
                  unsigned* counter, int grid, cudaStream_t s) {
   GridReduce G{partial, counter};
   Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
+  ProfScope ps("max_u", s);
   k_max_u<<<grid, NT, 0, s>>>(size_t(M.nb) * BN, vel, ui, G, out);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;

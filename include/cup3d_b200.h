@@ -120,6 +120,8 @@ int cup_upload_field(cup_ctx* ctx, int32_t field, const double* host);
 int cup_download_field(cup_ctx* ctx, int32_t field, double* host);
 /* Device pointer of a field (SoA), for zero-copy use by device-resident callers. */
 double* cup_field_device_ptr(cup_ctx* ctx, int32_t field);
+/* The context's CUDA stream (cudaStream_t) on which every call enqueues its work. */
+void* cup_stream(cup_ctx* ctx);
 
 /* ---- raw device-side operators on caller device buffers (nb*512 doubles) ---- */
 /* y = A x: the AMR Poisson operator of PoissonSolverExp::getMat with the
@@ -158,6 +160,12 @@ int cup_pressure_project(cup_ctx* ctx, double dt, int32_t step, cup_solve_stats*
 /* One time step: AdvectionDiffusion, Penalization (if a body is set),
  * PressureProjection.  dt <= 0: computed by calcMaxTimestep; *dt_used gets it. */
 int cup_step(cup_ctx* ctx, int32_t step, double dt, double* dt_used, cup_solve_stats* stats);
+
+/* ---- profiling (the reference's DeviceProfiler, Utils/DeviceProfiler.cuh) ---- */
+/* Enables per-kernel CUDA-event timing (resets the counters). */
+int cup_profile(cup_ctx* ctx, int32_t enable);
+/* JSON object {"phase": [launches, milliseconds], ...} into buf; returns its length. */
+int cup_profile_read(cup_ctx* ctx, char* buf, int32_t len);
 
 #ifdef __cplusplus
 }

@@ -72,7 +72,7 @@ def test_solve_matches_oracle(name):
     assert np.linalg.norm(x - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
     # iteration counts agree up to the rounding-sensitive restart test
     # (rho^2 < 1e-16 |r|^2 |rhat|^2, BiCGSTAB.cu:489)
-    slack = 1 if st_ref["restarts"] == 0 else 3
+    slack = 1 if st_ref["restarts"] == 0 else max(3, st_ref["iterations"] // 10)
     assert abs(st["iterations"] - st_ref["iterations"]) <= slack, (st, st_ref)
 
 

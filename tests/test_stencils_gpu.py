@@ -2,7 +2,7 @@
 
 Tolerances (FP64 both sides, different summation and fused-multiply-add order):
   * advection-diffusion, penalization: 1e-12 of max|u|;
-  * pressure projection / full step (Poisson solved to 1e-12 relative on both
+  * pressure projection / full step (Poisson solved to 1e-11 relative on both
     sides): 1e-10 of max|u| for velocity, 1e-9 of max|p| for pressure.
 """
 import numpy as np
@@ -78,7 +78,7 @@ def test_penalization_matches_oracle():
 @pytest.mark.parametrize("step", [1, 5])
 @pytest.mark.parametrize("name", ["tgv32", "amr3_mixed", "sphere"])
 def test_pressure_project_matches_oracle(name, step):
-    extra = "-poissonTol 0 -poissonTolRel 1e-12"
+    extra = "-poissonTol 0 -poissonTolRel 1e-11"
     if name == "sphere":
         ctx, m, slot, chi_o, udef_o, kin, chi = _sphere_case()
         ctx2 = make_ctx("amr2_free", device=0, extra=extra)
@@ -99,7 +99,7 @@ def test_pressure_project_matches_oracle(name, step):
     rc, st = ctx.pressure_project(dt, step)
     assert rc == 0 and st["status"] == 1
     got_v, got_p = ctx.download("vel"), ctx.download("pres")
-    ref_v, ref_p, info = m.pressure_project(vel, p0, dt, step, tol=0.0, tol_rel=1e-12, **obst)
+    ref_v, ref_p, info = m.pressure_project(vel, p0, dt, step, tol=0.0, tol_rel=1e-11, **obst)
     assert info["converged"]
     assert rel(got_v, ref_v) < 1e-10
     assert np.abs(got_p - ref_p).max() < 1e-9 * np.abs(ref_p).max()
@@ -108,7 +108,7 @@ def test_pressure_project_matches_oracle(name, step):
 def test_tgv_steps_match_oracle():
     # u = sin x cos y cos z, v = -cos x sin y cos z, w = 0 on [0,2pi]^3,
     # nu = 0.01, CFL 0.3, upwind5, FP64; Poisson converged tightly on both sides
-    flags = "-nu 0.01 -CFL 0.3 -rampup 0 -poissonTol 0 -poissonTolRel 1e-12"
+    flags = "-nu 0.01 -CFL 0.3 -rampup 0 -poissonTol 0 -poissonTolRel 1e-11"
     ctx = make_ctx("tgv32", device=0, extra=flags)
     m = oracle_mesh(ctx)
     xyz, _ = cell_centres(ctx)
@@ -120,9 +120,9 @@ def test_tgv_steps_match_oracle():
     for step in range(4):
         dt_gpu, rc, st = ctx.step(step)
         dt_ref = oracle.dt(m.hmin, 0.01, 0.3, m.max_u(ref_v), step, 0)
-        assert abs(dt_gpu - dt_ref) <= 1e-14 * dt_ref
+        assert abs(dt_gpu - dt_ref) <= 1e-12 * dt_ref
         ref_v = m.advect_diffuse(ref_v, dt_ref, 0.01)
-        ref_v, pres, info = m.pressure_project(ref_v, pres, dt_ref, step, tol=0.0, tol_rel=1e-12)
+        ref_v, pres, info = m.pressure_project(ref_v, pres, dt_ref, step, tol=0.0, tol_rel=1e-11)
         got = ctx.download("vel")
         assert rel(got, ref_v) < 1e-10, step
     assert rel(ctx.download("pres"), pres) < 1e-9
