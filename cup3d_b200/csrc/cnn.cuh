@@ -1,0 +1,68 @@
+// Learned per-block preconditioner: a 3-D CNN applied to each block's
+// residual (block + one-cell halo) standing in for the block inverse inside
+// BiCGSTAB.  No counterpart in the reference (it is the new slot at the
+// preconditioner call sites PoissonSolverAMR.h:183-222 / BiCGSTAB.cu:526-527).
+//
+// Network: x (10^3, 1 channel) -> conv3^3 valid 1->C, ReLU -> conv3^3 same
+// C->C, ReLU -> conv3^3 same C->C, ReLU -> conv3^3 same C->1 -> z (8^3),
+// C = 16.  The input is normalised by its RMS s and the output scaled by s/h,
+// so z has the units of A^-1 r (A = h * Laplacian).
+#pragma once
+#include "common.cuh"
+
+namespace cup3d {
+
+constexpr int CNN_C = 16;
+// parameter counts (FP32 master copy, contiguous in this order)
+constexpr int CNN_W0 = CNN_C * 27;            // [co][tap]
+constexpr int CNN_B0 = CNN_C;
+constexpr int CNN_W1 = CNN_C * CNN_C * 27;    // [co][ci][tap]
+constexpr int CNN_B1 = CNN_C;
+constexpr int CNN_W2 = CNN_C * CNN_C * 27;
+constexpr int CNN_B2 = CNN_C;
+constexpr int CNN_W3 = CNN_C * 27;            // [ci][tap]
+constexpr int CNN_B3 = 1;
+constexpr int CNN_NPARAM = CNN_W0 + CNN_B0 + CNN_W1 + CNN_B1 + CNN_W2 + CNN_B2 + CNN_W3 + CNN_B3;
+// offsets
+constexpr int OFF_W0 = 0;
+constexpr int OFF_B0 = OFF_W0 + CNN_W0;
+constexpr int OFF_W1 = OFF_B0 + CNN_B0;
+constexpr int OFF_B1 = OFF_W1 + CNN_W1;
+constexpr int OFF_W2 = OFF_B1 + CNN_B1;
+constexpr int OFF_B2 = OFF_W2 + CNN_W2;
+constexpr int OFF_W3 = OFF_B2 + CNN_B2;
+constexpr int OFF_B3 = OFF_W3 + CNN_W3;
+
+struct CnnWeights {
+  float* master;      // CNN_NPARAM FP32 (training copy)
+  uint16_t* w1_bf16;  // [tap][co][ci] bf16 packed for the tensor cores
+  uint16_t* w2_bf16;
+  uint16_t* w1t_bf16; // [tap][ci][co] flipped-tap transposes for backward-data
+  uint16_t* w2t_bf16;
+};
+
+// Packs the BF16 tensor-core copies from the FP32 master weights.
+int cnn_pack(const CnnWeights& W, cudaStream_t s);
+
+// z = (s/h) CNN(r_lab / s) for every block; r and z are nb*512 vectors of T.
+template <class T>
+int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid, cudaStream_t s);
+
+// Network input of every block: the block + halo of v (10^3, zero edges and
+// corners) divided by its RMS, into in[nb*1000]; RMS into scale[nb].
+int cnn_gather(const DevMesh& M, const double* v, float* in, float* scale, int grid, cudaStream_t s);
+
+// Training on a device dataset of n samples: in[n*1000], target[n*512]
+// (targets already divided by the sample's scale/h).  One Adam step over a
+// minibatch of `batch` sample indices idx[batch]; loss (mean squared error)
+// into *loss_dev.  grad_partial: grid*CNN_NPARAM floats of scratch.
+int cnn_train_step(const CnnWeights& W, float* adam_m, float* adam_v, int t, float lr, const float* in,
+                   const float* target, const int* idx, int batch, float* grad_partial, float* grad, float* loss_dev,
+                   int grid, cudaStream_t s);
+
+// Forward and gradient (no update) on a batch, for checks against the oracle.
+int cnn_forward_batch(const CnnWeights& W, const float* in, float* out, int n, cudaStream_t s);
+int cnn_grad_batch(const CnnWeights& W, const float* in, const float* target, int n, float* grad_partial,
+                   float* grad, float* loss_dev, int grid, cudaStream_t s);
+
+}  // namespace cup3d

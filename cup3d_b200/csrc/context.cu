@@ -78,11 +78,15 @@ static int alloc_fields(cup_ctx* c) {
   for (double** v : vecs)
     if (int rc = A.alloc(v, n)) return rc;
   W.xs[0] = nullptr;
+  float** fvecs[] = {&W.fr, &W.frhat, &W.fp, &W.fnu, &W.ft, &W.fz1, &W.fz2, &W.fxs[0], &W.fxs[1], &W.fxs[2], &W.r32};
+  for (float** v : fvecs)
+    if (int rc = A.alloc(v, n)) return rc;
   // grid: a few CTAs per SM, never more than blocks
   W.grid = std::max(1, std::min(c->mesh.nb, c->num_sms * 8));
   if (int rc = A.alloc(&W.partial, size_t(W.grid) * 8)) return rc;
   if (int rc = A.alloc(&W.counters, 32)) return rc;
   if (int rc = A.alloc(&W.st, 1)) return rc;
+  if (int rc = A.alloc(&W.st2, 1)) return rc;
   CUP_CUDA_TRY(cudaMemset(W.counters, 0, 32 * sizeof(unsigned int)));
   for (int i = 0; i < 2; ++i) {
     CUP_CUDA_TRY(cudaMemset(F.vel[i], 0, 3 * n * 8));
@@ -390,7 +394,10 @@ int cup_block_inverse_dev(cup_ctx* c, const double* in, double* out) {
   return 0;
 }
 
-static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats) {
+// check_true: recompute ||b - A x||_2 in FP64 after the solve (stats.true_rel);
+// the time-step path skips it (-1) since the solvers already test their own
+// FP64 residual.
+static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats, bool check_true = true) {
   SolveParams P;
   P.tol_abs = c->cfg.poisson_tol;
   P.tol_rel = c->cfg.poisson_tol_rel;
@@ -400,11 +407,22 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   P.check_every = 8;
   SolveStats S{};
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
-  if (int rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned)) return keep(c, rc);
+  int rc = 0;
+  if (c->cfg.poisson_solver == CUP_POISSON_B200_MIXED)
+    rc = poisson_mixed(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned);
+  else
+    rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned);
+  if (rc) return keep(c, rc);
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   CUP_CUDA_TRY(cudaEventSynchronize(c->ev1));
   float ms = 0;
   CUP_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  double true_rel = -1.0;
+  if (check_true && S.status != SOLVE_NAN) {
+    double e = 0;
+    if (int rc2 = true_residual_norm(c->dm, b, x, P.mean_mode, c->W, &e, c->stream)) return keep(c, rc2);
+    true_rel = S.err_init > 0 ? e / S.err_init : 0.0;
+  }
   if (stats) {
     stats->iterations = S.iterations;
     stats->restarts = S.restarts;
@@ -412,7 +430,7 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
     stats->fallback = 0;
     stats->err_init = S.err_init;
     stats->err_final = S.err_opt;
-    stats->true_rel = S.err_init > 0 ? S.err_opt / S.err_init : 0.0;
+    stats->true_rel = true_rel;
     stats->milliseconds = ms;
   }
   if (S.status == SOLVE_NAN) return ctx_fail(c, CUP_ERR_NAN, "Poisson solve produced NaN");
@@ -544,7 +562,7 @@ static int project(cup_ctx* c, double dt, int step, cup_solve_stats* stats) {
                                    F.lhs, F.phi, grid_of(c), c->stream))
     return keep(c, rc);
   cup_solve_stats st{};
-  const int rs = solve_impl(c, F.lhs, F.phi, &st);
+  const int rs = solve_impl(c, F.lhs, F.phi, &st, false);
   if (rs < 0) return rs;
   if (int rc = launch_weighted_sum(c->dm, F.phi, c->d_scalars + SC_SUMS, c->W, c->stream)) return keep(c, rc);
   if (int rc = launch_grad_update(c->dm, F.vel[F.vcur], F.phi, pold, pnew, c->d_scalars + SC_SUMS, dt, step,

@@ -13,6 +13,7 @@
 //   * solver: BiCGSTABSolver::main (BiCGSTAB.cu:416-628) with the same
 //     scalars, restart rule and best-iterate return, but five fused kernels
 //     per iteration and no host round trip inside an iteration.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -166,10 +167,10 @@ __device__ void spmv_block(const DevMesh& M, int b, const T* __restrict__ x, dou
       if (t < 64) {
         const int h1 = M.index[b * 3 + tan1(d)] & 1, h2 = M.index[b * 3 + tan2(d)] & 1;
         const int c1 = h1 * 4 + (a >> 1), c2 = h2 * 4 + (bb >> 1);
-        const double T = cf_taylor(sm.cl, d, c1, c2, (a & 1) ? 1.0 : -1.0, (bb & 1) ? 1.0 : -1.0);
+        const double tay = cf_taylor(sm.cl, d, c1, c2, (a & 1) ? 1.0 : -1.0, (bb & 1) ? 1.0 : -1.0);
         const int cs = face_cell(d, s, 0, a, bb), ci = face_cell(d, s, 1, a, bb);
         const double xs = double(xb[cs]), xi = double(xb[ci]);
-        sm.ys[cs] += h * (2. / 3. * xs - 1. / 5. * xi + 8. / 15. * T - xs);
+        sm.ys[cs] += h * (2. / 3. * xs - 1. / 5. * xi + 8. / 15. * tay - xs);
       }
     } else {
       if (t < 64) sm.cl[t] = double(xb[face_cell(d, s, 0, a, bb)]);
@@ -185,8 +186,8 @@ __device__ void spmv_block(const DevMesh& M, int b, const T* __restrict__ x, dou
           const int fa = 2 * (a & 3) + f1, fb = 2 * (bb & 3) + f2;
           const double close = double(xc[face_cell(d, 1 - s, 0, fa, fb)]);
           const double far = double(xc[face_cell(d, 1 - s, 1, fa, fb)]);
-          const double T = cf_taylor(sm.cl, d, a, bb, f1 ? 1.0 : -1.0, f2 ? 1.0 : -1.0);
-          acc += hf * (close - (2. / 3. * close - 1. / 5. * far + 8. / 15. * T));
+          const double tay = cf_taylor(sm.cl, d, a, bb, f1 ? 1.0 : -1.0, f2 ? 1.0 : -1.0);
+          acc += hf * (close - (2. / 3. * close - 1. / 5. * far + 8. / 15. * tay));
         }
         sm.ys[face_cell(d, s, 0, a, bb)] += acc;
       }
@@ -311,44 +312,49 @@ __global__ void __launch_bounds__(NT) k_block_inverse(DevMesh M, const double* _
 }
 
 // ---------------------------------------------------------------------------
-// BiCGSTAB kernels
+// BiCGSTAB kernels, templated on the vector storage type T (double for the
+// FP64 solver, float for the inner solves of the mixed-precision solver).
+// Arithmetic, dot products and scalars are FP64 in both cases.
 // ---------------------------------------------------------------------------
+template <class T>
 struct KArgs {
   DevMesh M;
-  const double* b;
-  double* r;
-  double* rhat;
-  double* p;
-  double* nu;
-  double* t;
-  double* z1;
-  double* z2;
-  double* xs0;
-  double* xs1;
-  double* xs2;
+  const T* b;
+  T* r;
+  T* rhat;
+  T* p;
+  T* nu;
+  T* t;
+  T* z1;
+  T* z2;
+  T* xs0;
+  T* xs1;
+  T* xs2;
   KrylovState* st;
   GridReduce g;
   int mean_mode;
+  int zero_mean_row;  // b and x0 are zero at the mean row (getVec, modes 1 and 3)
 };
 
-__device__ __forceinline__ double* xslot(const KArgs& A, int i) {
+template <class T>
+__device__ __forceinline__ T* xslot(const KArgs<T>& A, int i) {
   return i == 0 ? A.xs0 : (i == 1 ? A.xs1 : A.xs2);
 }
 
 // x0[mean row] = 0 (getVec, PoissonSolverExp.cpp:402-410) and sum(x0 h^3)
-__global__ void __launch_bounds__(NT) k_bicg_prepare(KArgs A) {
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_prepare(KArgs<T> A) {
   __shared__ double red[64];
   const DevMesh& M = A.M;
-  if ((A.mean_mode == 1 || A.mean_mode == 3) && M.mean_block >= 0 && blockIdx.x == 0 && threadIdx.x == 0)
-    A.xs0[size_t(M.mean_block) * BN] = 0.0;
-  __syncthreads();
+  if (A.zero_mean_row && M.mean_block >= 0 && blockIdx.x == 0 && threadIdx.x == 0)
+    A.xs0[size_t(M.mean_block) * BN] = T(0);
   double acc[1] = {0.0};
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
     const double h = M.h[b], h3 = h * h * h;
     double s = 0.0;
     for (int c = threadIdx.x; c < BN; c += NT) {
       const size_t i = size_t(b) * BN + c;
-      s += (b == M.mean_block && c == 0 && (A.mean_mode == 1 || A.mean_mode == 3)) ? 0.0 : A.xs0[i];
+      s += (A.zero_mean_row && b == M.mean_block && c == 0) ? 0.0 : double(A.xs0[i]);
     }
     acc[0] += s * h3;
   }
@@ -356,7 +362,8 @@ __global__ void __launch_bounds__(NT) k_bicg_prepare(KArgs A) {
 }
 
 // r = b - A x0, rhat = r, p = nu = 0; err_init = ||r||
-__global__ void __launch_bounds__(NT) k_bicg_init(KArgs A) {
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
   __shared__ SpmvSmem sm;
   __shared__ double red[64];
   const DevMesh& M = A.M;
@@ -364,18 +371,18 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs A) {
   double acc[1] = {0.0};
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
     double o[2];
-    spmv_block<double>(M, b, A.xs0, ms, A.mean_mode, sm, o);
+    spmv_block<T>(M, b, A.xs0, ms, A.mean_mode, sm, o);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int c = threadIdx.x + q * NT;
       const size_t i = size_t(b) * BN + c;
-      double bi = A.b[i];
-      if ((A.mean_mode == 1 || A.mean_mode == 3) && b == M.mean_block && c == 0) bi = 0.0;
+      double bi = double(A.b[i]);
+      if (A.zero_mean_row && b == M.mean_block && c == 0) bi = 0.0;
       const double ri = bi - o[q];
-      A.r[i] = ri;
-      A.rhat[i] = ri;
-      A.p[i] = 0.0;
-      A.nu[i] = 0.0;
+      A.r[i] = T(ri);
+      A.rhat[i] = T(ri);
+      A.p[i] = T(0);
+      A.nu[i] = T(0);
       acc[0] += ri * ri;
     }
   }
@@ -411,7 +418,8 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs A) {
 
 // KA: p = r + beta (p - omega nu) (or p = r, rhat = r after a restart);
 //     z1 = M^-1 p; sum(z1 h^3)
-__global__ void __launch_bounds__(NT) k_bicg_a(KArgs A) {
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
   __shared__ FdSmem sm;
   __shared__ double red[64];
   const KrylovState& S = *A.st;
@@ -427,16 +435,16 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs A) {
     for (int q = 0; q < 2; ++q) {
       const int c = threadIdx.x + q * NT;
       const size_t i = size_t(b) * BN + c;
-      const double ri = A.r[i];
+      const double ri = double(A.r[i]);
       double pi;
       if (restart) {
         pi = ri;
-        A.rhat[i] = ri;
+        A.rhat[i] = T(ri);
       } else {
-        pi = ri + beta * (A.p[i] - omega * A.nu[i]);
+        pi = ri + beta * (double(A.p[i]) - omega * double(A.nu[i]));
       }
-      A.p[i] = pi;
-      sm.a[c] = pi;
+      A.p[i] = T(pi);
+      sm.a[c] = double(T(pi));
     }
     __syncthreads();
     const double h = M.h[b];
@@ -445,9 +453,9 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs A) {
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int c = threadIdx.x + q * NT;
-      const double zi = sm.a[c];
+      const T zi = T(sm.a[c]);
       A.z1[size_t(b) * BN + c] = zi;
-      s += zi;
+      s += double(zi);
     }
     acc[0] += s * h * h * h;
   }
@@ -463,7 +471,8 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs A) {
 }
 
 // KB: nu = A z1; alpha = rho / ((rhat, nu) + eps)
-__global__ void __launch_bounds__(NT) k_bicg_b(KArgs A) {
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_b(KArgs<T> A) {
   __shared__ SpmvSmem sm;
   __shared__ double red[64];
   const KrylovState& S = *A.st;
@@ -473,12 +482,13 @@ __global__ void __launch_bounds__(NT) k_bicg_b(KArgs A) {
   double acc[1] = {0.0};
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
     double o[2];
-    spmv_block<double>(M, b, A.z1, ms, A.mean_mode, sm, o);
+    spmv_block<T>(M, b, A.z1, ms, A.mean_mode, sm, o);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const size_t i = size_t(b) * BN + threadIdx.x + q * NT;
-      A.nu[i] = o[q];
-      acc[0] += A.rhat[i] * o[q];
+      const T v = T(o[q]);
+      A.nu[i] = v;
+      acc[0] += double(A.rhat[i]) * double(v);
     }
   }
   if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
@@ -488,7 +498,8 @@ __global__ void __launch_bounds__(NT) k_bicg_b(KArgs A) {
 }
 
 // KC: s = r - alpha nu (in place in r); z2 = M^-1 s; sum(z2 h^3)
-__global__ void __launch_bounds__(NT) k_bicg_c(KArgs A) {
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
   __shared__ FdSmem sm;
   __shared__ double red[64];
   const KrylovState& S = *A.st;
@@ -503,9 +514,9 @@ __global__ void __launch_bounds__(NT) k_bicg_c(KArgs A) {
     for (int q = 0; q < 2; ++q) {
       const int c = threadIdx.x + q * NT;
       const size_t i = size_t(b) * BN + c;
-      const double si = A.r[i] - alpha * A.nu[i];
+      const T si = T(double(A.r[i]) - alpha * double(A.nu[i]));
       A.r[i] = si;
-      sm.a[c] = si;
+      sm.a[c] = double(si);
     }
     __syncthreads();
     const double h = M.h[b];
@@ -514,9 +525,9 @@ __global__ void __launch_bounds__(NT) k_bicg_c(KArgs A) {
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int c = threadIdx.x + q * NT;
-      const double zi = sm.a[c];
+      const T zi = T(sm.a[c]);
       A.z2[size_t(b) * BN + c] = zi;
-      s += zi;
+      s += double(zi);
     }
     acc[0] += s * h * h * h;
   }
@@ -524,7 +535,8 @@ __global__ void __launch_bounds__(NT) k_bicg_c(KArgs A) {
 }
 
 // KD: t = A z2; omega = (t, s) / ((t, t) + eps)
-__global__ void __launch_bounds__(NT) k_bicg_d(KArgs A) {
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_d(KArgs<T> A) {
   __shared__ SpmvSmem sm;
   __shared__ double red[64];
   const KrylovState& S = *A.st;
@@ -534,13 +546,14 @@ __global__ void __launch_bounds__(NT) k_bicg_d(KArgs A) {
   double acc[2] = {0.0, 0.0};
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
     double o[2];
-    spmv_block<double>(M, b, A.z2, ms, A.mean_mode, sm, o);
+    spmv_block<T>(M, b, A.z2, ms, A.mean_mode, sm, o);
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const size_t i = size_t(b) * BN + threadIdx.x + q * NT;
-      A.t[i] = o[q];
-      acc[0] += o[q] * A.r[i];
-      acc[1] += o[q] * o[q];
+      const T v = T(o[q]);
+      A.t[i] = v;
+      acc[0] += double(v) * double(A.r[i]);
+      acc[1] += double(v) * double(v);
     }
   }
   if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
@@ -551,22 +564,23 @@ __global__ void __launch_bounds__(NT) k_bicg_d(KArgs A) {
 
 // KE: x_new = x + alpha z1 + omega z2; r = s - omega t; (rhat, r), (r, r);
 //     convergence, best iterate, restart decision, beta for the next KA.
-__global__ void __launch_bounds__(NT) k_bicg_e(KArgs A) {
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_e(KArgs<T> A) {
   __shared__ double red[64];
   const KrylovState& S = *A.st;
   if (S.done) return;
   const double alpha = S.alpha, omega = S.omega;
-  const double* xc = xslot(A, S.cur);
-  double* xn = xslot(A, S.nxt);
+  const T* xc = xslot(A, S.cur);
+  T* xn = xslot(A, S.nxt);
   const DevMesh& M = A.M;
   double acc[2] = {0.0, 0.0};
   const size_t n = size_t(M.nb) * BN;
   for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n; i += size_t(gridDim.x) * NT) {
-    xn[i] = (xc[i] + alpha * A.z1[i]) + omega * A.z2[i];
-    const double ri = A.r[i] - omega * A.t[i];
+    xn[i] = T((double(xc[i]) + alpha * double(A.z1[i])) + omega * double(A.z2[i]));
+    const T ri = T(double(A.r[i]) - omega * double(A.t[i]));
     A.r[i] = ri;
-    acc[0] += A.rhat[i] * ri;
-    acc[1] += ri * ri;
+    acc[0] += double(A.rhat[i]) * double(ri);
+    acc[1] += double(ri) * double(ri);
   }
   if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
     KrylovState& W = *A.st;
@@ -614,27 +628,83 @@ __global__ void __launch_bounds__(NT) k_bicg_e(KArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// Iterative refinement (mixed precision): FP64 true residual and update.
+// ---------------------------------------------------------------------------
+// x += e (e may be null: only the mean-row zeroing and sum); sum(x h^3)
+__global__ void __launch_bounds__(NT) k_refine_update(DevMesh M, double* x, const float* __restrict__ e,
+                                                      int zero_mean_row, KrylovState* st, GridReduce g) {
+  __shared__ double red[64];
+  double acc[1] = {0.0};
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    const double h = M.h[b], h3 = h * h * h;
+    double s = 0.0;
+    for (int c = threadIdx.x; c < BN; c += NT) {
+      const size_t i = size_t(b) * BN + c;
+      double v = x[i];
+      if (zero_mean_row && b == M.mean_block && c == 0) v = 0.0;
+      if (e) v += double(e[i]);
+      x[i] = v;
+      s += v;
+    }
+    acc[0] += s * h3;
+  }
+  if (grid_reduce<1>(acc, g, red) && threadIdx.x == 0) st->mean_sum = acc[0];
+}
+
+// r32 = b' - A x in FP64 arithmetic (b' = b with the mean row zeroed for modes
+// 1 and 3), ||b' - A x||_2 into st->err (the FP64-checked residual).
+__global__ void __launch_bounds__(NT) k_true_residual(DevMesh M, const double* __restrict__ b,
+                                                      const double* __restrict__ x, float* __restrict__ r32,
+                                                      int mean_mode, int zero_mean_row, KrylovState* st,
+                                                      GridReduce g) {
+  __shared__ SpmvSmem sm;
+  __shared__ double red[64];
+  const double ms = st->mean_sum;
+  double acc[1] = {0.0};
+  for (int blk = blockIdx.x; blk < M.nb; blk += gridDim.x) {
+    double o[2];
+    spmv_block<double>(M, blk, x, ms, mean_mode, sm, o);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = threadIdx.x + q * NT;
+      const size_t i = size_t(blk) * BN + c;
+      double bi = b[i];
+      if (zero_mean_row && blk == M.mean_block && c == 0) bi = 0.0;
+      const double ri = bi - o[q];
+      if (r32) r32[i] = float(ri);
+      acc[0] += ri * ri;
+    }
+  }
+  if (grid_reduce<1>(acc, g, red) && threadIdx.x == 0) {
+    st->rr = acc[0];
+    st->err = sqrt(acc[0]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-static KArgs make_args(const DevMesh& M, const double* b, double* x, PoissonWork& W, int mean_mode,
-                       int site) {
-  KArgs A;
+template <class T>
+static KArgs<T> make_args(const DevMesh& M, const T* b, T* x, T* const v[9], PoissonWork& W, KrylovState* st,
+                          int mean_mode, int zero_mean_row, int site) {
+  KArgs<T> A;
   A.M = M;
   A.b = b;
-  A.r = W.r;
-  A.rhat = W.rhat;
-  A.p = W.p;
-  A.nu = W.nu;
-  A.t = W.t;
-  A.z1 = W.z1;
-  A.z2 = W.z2;
+  A.r = v[0];
+  A.rhat = v[1];
+  A.p = v[2];
+  A.nu = v[3];
+  A.t = v[4];
+  A.z1 = v[5];
+  A.z2 = v[6];
   A.xs0 = x;
-  A.xs1 = W.xs[1];
-  A.xs2 = W.xs[2];
-  A.st = W.st;
+  A.xs1 = v[7];
+  A.xs2 = v[8];
+  A.st = st;
   A.g.partial = W.partial;
   A.g.counter = W.counters + site;
   A.mean_mode = mean_mode;
+  A.zero_mean_row = zero_mean_row;
   return A;
 }
 
@@ -668,9 +738,11 @@ int launch_block_inverse(const DevMesh& M, const double* in, double* out, Poisso
   return 0;
 }
 
-int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
-                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done) {
-  poisson_init_constants();
+// Runs BiCGSTAB on vectors of type T; x holds x0 on entry, x_opt on exit.
+template <class T>
+static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, int zero_mean_row,
+                        PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done) {
+  const bool f32 = sizeof(T) == 4;
   KrylovState init{};
   init.tol_abs = P.tol_abs;
   init.tol_rel = P.tol_rel;
@@ -678,18 +750,18 @@ int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolvePa
   init.max_restarts = P.max_restarts;
   init.eps = 1e-21;
   CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
-  KArgs A = make_args(M, b, x, W, P.mean_mode, 0);
-  { ProfScope ps("bicg_prepare", s); k_bicg_prepare<<<W.grid, NT, 0, s>>>(A); }
-  { ProfScope ps("bicg_init", s); k_bicg_init<<<W.grid, NT, 0, s>>>(A); }
+  KArgs<T> A = make_args<T>(M, b, x, v, W, W.st, P.mean_mode, zero_mean_row, 0);
+  { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); k_bicg_prepare<T><<<W.grid, NT, 0, s>>>(A); }
+  { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); k_bicg_init<T><<<W.grid, NT, 0, s>>>(A); }
   CUP_CUDA_TRY(cudaGetLastError());
   const int chunk = P.check_every > 0 ? P.check_every : 8;
   for (int it = 0; it < P.max_iter; it += chunk) {
     for (int j = 0; j < chunk; ++j) {
-      { ProfScope ps("bicg_a_pupdate_precond", s); k_bicg_a<<<W.grid, NT, 0, s>>>(A); }
-      { ProfScope ps("bicg_b_spmv_dot", s); k_bicg_b<<<W.grid, NT, 0, s>>>(A); }
-      { ProfScope ps("bicg_c_supdate_precond", s); k_bicg_c<<<W.grid, NT, 0, s>>>(A); }
-      { ProfScope ps("bicg_d_spmv_dots", s); k_bicg_d<<<W.grid, NT, 0, s>>>(A); }
-      { ProfScope ps("bicg_e_xr_update_dots", s); k_bicg_e<<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); k_bicg_a<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_b_spmv_dot" : "bicg_b_spmv_dot", s); k_bicg_b<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_c_supdate_precond" : "bicg_c_supdate_precond", s); k_bicg_c<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_d_spmv_dots" : "bicg_d_spmv_dots", s); k_bicg_d<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_e_xr_update_dots" : "bicg_e_xr_update_dots", s); k_bicg_e<T><<<W.grid, NT, 0, s>>>(A); }
     }
     CUP_CUDA_TRY(cudaGetLastError());
     CUP_CUDA_TRY(cudaMemcpyAsync(h_done, &W.st->done, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -700,15 +772,133 @@ int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolvePa
   CUP_CUDA_TRY(cudaMemcpyAsync(&fin, W.st, sizeof(fin), cudaMemcpyDeviceToHost, s));
   CUP_CUDA_TRY(cudaStreamSynchronize(s));
   if (fin.best != 0) {
-    double* src = fin.best == 1 ? W.xs[1] : W.xs[2];
-    CUP_CUDA_TRY(cudaMemcpyAsync(x, src, size_t(M.nb) * BN * sizeof(double),
-                                 cudaMemcpyDeviceToDevice, s));
+    T* src = fin.best == 1 ? v[7] : v[8];
+    CUP_CUDA_TRY(cudaMemcpyAsync(x, src, size_t(M.nb) * BN * sizeof(T), cudaMemcpyDeviceToDevice, s));
   }
   out.iterations = fin.k;
   out.restarts = fin.restarts;
   out.status = fin.done ? fin.status : SOLVE_MAXITER;
   out.err_init = fin.err_init;
   out.err_opt = fin.err_opt;
+  return 0;
+}
+
+int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
+                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done) {
+  poisson_init_constants();
+  double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
+  const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
+  return run_bicgstab<double>(M, b, x, v, P, zmr, W, out, s, h_done);
+}
+
+// Mixed precision: FP64 iterative refinement around FP32 BiCGSTAB inner solves.
+// Every outer step recomputes the true residual b - A x in FP64 (the
+// convergence test is on it), solves A e = r with FP32 vectors (FP64 dots and
+// scalars) to a relative tolerance tied to the remaining reduction, and adds e
+// to x in FP64.
+int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
+                  SolveStats& out, cudaStream_t s, int* h_done) {
+  poisson_init_constants();
+  const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
+  const size_t n = size_t(M.nb) * BN;
+  GridReduce g{W.partial, W.counters + 12};
+  KrylovState* so = W.st2;
+  float* const v[9] = {W.fr, W.frhat, W.fp, W.fnu, W.ft, W.fz1, W.fz2, W.fxs[1], W.fxs[2]};
+  float* e = W.fxs[0];
+  auto residual = [&](double* err) -> int {
+    {
+      ProfScope ps("refine_true_residual_fp64", s);
+      k_true_residual<<<W.grid, NT, 0, s>>>(M, b, x, W.r32, P.mean_mode, zmr, so, g);
+    }
+    CUP_CUDA_TRY(cudaGetLastError());
+    CUP_CUDA_TRY(cudaMemcpyAsync(err, &so->err, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  };
+  {
+    ProfScope ps("refine_update", s);
+    k_refine_update<<<W.grid, NT, 0, s>>>(M, x, nullptr, zmr, so, g);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  double err0 = 0, err = 0;
+  if (int rc = residual(&err0)) return rc;
+  err = err0;
+  out = SolveStats{};
+  out.err_init = err0;
+  out.err_opt = err0;
+  out.status = SOLVE_MAXITER;
+  if (!(err0 == err0)) {
+    out.status = SOLVE_NAN;
+    return 0;
+  }
+  if (err0 <= P.tol_abs) {
+    out.status = SOLVE_CONVERGED;
+    return 0;
+  }
+  int inner_total = 0, restarts = 0;
+  for (int outer = 0; outer < 40; ++outer) {
+    if (err <= P.tol_abs || err / err0 <= P.tol_rel) {
+      out.status = SOLVE_CONVERGED;
+      break;
+    }
+    // reduce the residual by what remains to be done, within FP32 reach
+    const double want = std::max(P.tol_abs, P.tol_rel * err0);
+    SolveParams Q = P;
+    Q.tol_abs = 0.0;
+    Q.tol_rel = std::min(0.5, std::max(2e-5, 0.5 * want / err));
+    Q.max_iter = std::max(1, P.max_iter - inner_total);
+    CUP_CUDA_TRY(cudaMemsetAsync(e, 0, n * sizeof(float), s));
+    SolveStats in{};
+    if (int rc = run_bicgstab<float>(M, W.r32, e, v, Q, 0, W, in, s, h_done)) return rc;
+    inner_total += in.iterations;
+    restarts += in.restarts;
+    if (in.status == SOLVE_NAN) {
+      out.status = SOLVE_NAN;
+      break;
+    }
+    {
+      ProfScope ps("refine_update", s);
+      k_refine_update<<<W.grid, NT, 0, s>>>(M, x, e, 0, so, g);
+    }
+    CUP_CUDA_TRY(cudaGetLastError());
+    const double prev = err;
+    if (int rc = residual(&err)) return rc;
+    out.err_opt = std::min(out.err_opt, err);
+    if (!(err == err)) {
+      out.status = SOLVE_NAN;
+      break;
+    }
+    if (err > 0.9 * prev && in.iterations > 0 && !(err <= P.tol_abs || err / err0 <= P.tol_rel)) {
+      out.status = SOLVE_MAXITER;  // refinement stagnated
+      break;
+    }
+    if (inner_total >= P.max_iter) {
+      if (err <= P.tol_abs || err / err0 <= P.tol_rel) out.status = SOLVE_CONVERGED;
+      break;
+    }
+    out.outer = outer + 1;
+  }
+  if (err <= P.tol_abs || err / err0 <= P.tol_rel) out.status = SOLVE_CONVERGED;
+  out.iterations = inner_total;
+  out.restarts = restarts;
+  out.err_opt = err;
+  return 0;
+}
+
+// FP64 ||b - A x||_2 (mean row of b zeroed as the solvers do); result in *err_host.
+int true_residual_norm(const DevMesh& M, const double* b, const double* x, int mean_mode, PoissonWork& W,
+                       double* err_host, cudaStream_t s) {
+  const int zmr = (mean_mode == 1 || mean_mode == 3) ? 1 : 0;
+  GridReduce g{W.partial, W.counters + 13};
+  KrylovState* so = W.st2;
+  {
+    ProfScope ps("true_residual_fp64", s);
+    k_weighted_sum<<<W.grid, NT, 0, s>>>(M, x, g, nullptr, &so->mean_sum);
+    k_true_residual<<<W.grid, NT, 0, s>>>(M, b, x, nullptr, mean_mode, zmr, so, g);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  CUP_CUDA_TRY(cudaMemcpyAsync(err_host, &so->err, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUP_CUDA_TRY(cudaStreamSynchronize(s));
   return 0;
 }
 

@@ -30,7 +30,10 @@ enum SolveStatus : int {
 struct PoissonWork {
   // vectors, nb*512 each
   double *r, *rhat, *p, *nu, *t, *z1, *z2, *xs[3];
+  // FP32 inner-solve vectors of the mixed-precision solver; fxs[0] = correction e
+  float *fr, *frhat, *fp, *fnu, *ft, *fz1, *fz2, *fxs[3], *r32;
   KrylovState* st;
+  KrylovState* st2;         // outer (refinement) state
   double* partial;          // grid * 8
   unsigned int* counters;   // 16
   int grid;                 // CTAs for block kernels
@@ -43,7 +46,7 @@ struct SolveParams {
 };
 
 struct SolveStats {
-  int iterations, restarts, status;
+  int iterations, restarts, status, outer;
   double err_init, err_opt;
 };
 
@@ -55,6 +58,13 @@ int launch_block_inverse(const DevMesh& M, const double* in, double* out, Poisso
 // Solves A x = b; x holds the initial guess on entry and x_opt on exit.
 int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
                      PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done_pinned);
+
+// Mixed precision: FP32 inner BiCGSTAB inside FP64 iterative refinement.
+int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
+                  SolveStats& out, cudaStream_t s, int* h_done_pinned);
+// FP64 ||b - A x||_2 with the solvers' mean-row convention.
+int true_residual_norm(const DevMesh& M, const double* b, const double* x, int mean_mode, PoissonWork& W,
+                       double* err_host, cudaStream_t s);
 
 // sum over cells of v*h^3 and of h^3 (zero-mean projection), into d_out[2]
 int launch_weighted_sum(const DevMesh& M, const double* v, double* d_out, PoissonWork& W,

@@ -1,0 +1,136 @@
+// C++ host layer over the C ABI with the reference's operator interfaces:
+//   class Operator { virtual void operator()(Real dt) = 0; virtual std::string getName() = 0; }
+//     (operators/Operator.h:12-20)
+//   class PoissonSolverBase { virtual void solve() = 0; } + makePoissonSolver(SimulationData&)
+//     (poisson/PoissonSolverBase.h:10-19, PoissonSolverBase.cpp:30-52)
+//   Simulation::calcMaxTimestep / advance (Simulation.cpp:309-412)
+//
+// Header-only; link against libcup3d_b200.so.  Hard errors of the C ABI become
+// std::runtime_error (the reference throws or aborts); soft statuses (Poisson
+// solve stopped at its caps) are recorded in SimulationData::last_solve.
+#pragma once
+#include <array>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cup3d_b200.h"
+
+namespace cubismup3d_b200 {
+
+using Real = double;
+
+inline void check(int rc, const cup_ctx* ctx) {
+  if (rc < 0) throw std::runtime_error(std::string("cup3d_b200: ") + cup_last_error(ctx));
+}
+
+// The run state the operators share (the reference's SimulationData, reduced
+// to what the time-step path reads).  Fields live on the device in `ctx`.
+struct SimulationData {
+  cup_config cfg{};
+  cup_ctx* ctx = nullptr;
+  int step = 0;
+  Real time = 0, dt = 0, uMax_measured = 0;
+  std::string poissonSolver = "b200";
+  cup_solve_stats last_solve{};
+  std::array<Real, 6> force_torque{};  // last Penalization force and torque
+  bool has_obstacle = false;
+
+  explicit SimulationData(const std::string& flags) {
+    cup_config_default(&cfg);
+    check(cup_config_parse(&cfg, flags.c_str()), nullptr);
+    static const char* names[] = {"b200", "b200_mixed", "b200_learned"};
+    poissonSolver = names[cfg.poisson_solver];
+    ctx = cup_create(&cfg);
+    if (!ctx) throw std::runtime_error(std::string("cup3d_b200: ") + cup_last_error(nullptr));
+  }
+  ~SimulationData() { cup_destroy(ctx); }
+  SimulationData(const SimulationData&) = delete;
+  SimulationData& operator=(const SimulationData&) = delete;
+};
+
+class Operator {
+ public:
+  SimulationData& sim;
+  explicit Operator(SimulationData& s) noexcept : sim(s) {}
+  virtual ~Operator() = default;
+  virtual void operator()(Real dt) = 0;
+  virtual std::string getName() = 0;
+};
+
+class AdvectionDiffusion : public Operator {
+ public:
+  using Operator::Operator;
+  void operator()(Real dt) override { check(cup_advect_diffuse(sim.ctx, dt), sim.ctx); }
+  std::string getName() override { return "AdvectionDiffusion"; }
+};
+
+class Penalization : public Operator {
+ public:
+  using Operator::Operator;
+  void operator()(Real dt) override {
+    if (!sim.has_obstacle) return;  // Penalization.cpp:513
+    check(cup_penalize(sim.ctx, dt, sim.force_torque.data()), sim.ctx);
+  }
+  std::string getName() override { return "Penalization"; }
+};
+
+class PoissonSolverBase {
+ public:
+  virtual ~PoissonSolverBase() = default;
+  virtual void solve() = 0;
+};
+
+// "b200", "b200_mixed", "b200_learned": RHS in sim.lhs, initial guess and
+// result in sim.pres (PoissonSolverAMR.cpp:20-21).
+class PoissonSolverB200 : public PoissonSolverBase {
+  SimulationData& sim;
+
+ public:
+  explicit PoissonSolverB200(SimulationData& s) : sim(s) {}
+  void solve() override { check(cup_poisson_solve(sim.ctx, &sim.last_solve), sim.ctx); }
+};
+
+inline std::shared_ptr<PoissonSolverBase> makePoissonSolver(SimulationData& s) {
+  if (s.poissonSolver == "b200" || s.poissonSolver == "b200_mixed" || s.poissonSolver == "b200_learned")
+    return std::make_shared<PoissonSolverB200>(s);
+  throw std::invalid_argument("Poisson solver: \"" + s.poissonSolver + "\" unrecognized!");
+}
+
+class PressureProjection : public Operator {
+ public:
+  std::shared_ptr<PoissonSolverBase> pressureSolver;
+  explicit PressureProjection(SimulationData& s) : Operator(s), pressureSolver(makePoissonSolver(s)) {}
+  void operator()(Real dt) override {
+    check(cup_pressure_project(sim.ctx, dt, sim.step, &sim.last_solve), sim.ctx);
+  }
+  std::string getName() override { return "PressureProjection"; }
+};
+
+// The time-step driver restricted to the hot path (Simulation.cpp:300-412):
+// mesh adaptation and obstacle creation stay with the caller.
+class Simulation {
+ public:
+  SimulationData sim;
+  std::vector<std::shared_ptr<Operator>> pipeline;
+
+  explicit Simulation(const std::string& flags) : sim(flags) {
+    pipeline.push_back(std::make_shared<AdvectionDiffusion>(sim));
+    pipeline.push_back(std::make_shared<Penalization>(sim));
+    pipeline.push_back(std::make_shared<PressureProjection>(sim));
+  }
+  Real calcMaxTimestep() {
+    Real dt = 0;
+    check(cup_compute_dt(sim.ctx, sim.step, &dt), sim.ctx);
+    sim.dt = dt;
+    return dt;
+  }
+  void advance(Real dt) {
+    for (auto& op : pipeline) (*op)(dt);
+    sim.step++;
+    sim.time += dt;
+  }
+};
+
+}  // namespace cubismup3d_b200

@@ -1,0 +1,57 @@
+"""Mixed-precision Poisson solver ("b200_mixed"): FP32 inner BiCGSTAB inside
+FP64 iterative refinement.  The convergence test is on the FP64 true
+residual, so the returned solution must meet the requested tolerance in FP64
+(checked here against the oracle's FP64 operator), and agree with the FP64
+solver's solution to the accuracy the tolerance implies."""
+import numpy as np
+import pytest
+
+from tests.meshes import make_ctx, oracle_mesh
+
+pytestmark = pytest.mark.gpu
+
+
+def torch_dev(a):
+    import torch
+    return torch.tensor(np.asarray(a, np.float64), device="cuda")
+
+
+def rhs(m, seed):
+    b = np.random.default_rng(seed).standard_normal(m.n)
+    hh = np.repeat(m.h, 512)
+    return b - np.sum(b * hh ** 3) / np.sum(hh ** 3)
+
+
+@pytest.mark.parametrize("tol_rel", [1e-6, 1e-10])
+@pytest.mark.parametrize("name", ["tgv32", "amr3_mixed"])
+def test_mixed_reaches_fp64_tolerance(name, tol_rel):
+    ctx = make_ctx(name, device=0, extra=f"-poissonSolver b200_mixed -poissonTol 0 -poissonTolRel {tol_rel}")
+    m = oracle_mesh(ctx)
+    b = rhs(m, 21)
+    bd, xd = torch_dev(b), torch_dev(np.zeros(m.n))
+    rc, st = ctx.poisson_solve_dev(bd, xd)
+    assert rc == 0 and st["status"] == 1, st
+    x = xd.cpu().numpy()
+    bb = b.copy()
+    mb = int(np.where((ctx.blocks()[1] == 0).all(axis=1))[0][0])
+    bb[mb * 512] = 0.0
+    r = bb - m.apply(x, mean_constraint=1)
+    true_rel = np.linalg.norm(r) / np.linalg.norm(bb)
+    assert true_rel <= tol_rel * 1.001, true_rel
+    assert abs(st["true_rel"] - true_rel) <= 1e-3 * true_rel + 1e-15
+    x_ref, _ = m.bicgstab_gpu(b, tol=0.0, tol_rel=1e-11)
+    assert np.linalg.norm(x - x_ref) <= 2e3 * tol_rel * np.linalg.norm(x_ref)
+
+
+def test_mixed_projection_step_matches_fp64():
+    # one pressure projection with the mixed solver at 1e-10 matches the FP64 one
+    from tests.test_stencils_gpu import smooth_velocity
+    outs = []
+    for solver in ("b200", "b200_mixed"):
+        ctx = make_ctx("amr3_mixed", device=0, extra=f"-poissonSolver {solver} -poissonTol 0 -poissonTolRel 1e-10")
+        vel = smooth_velocity(ctx)
+        ctx.upload("vel", vel)
+        rc, st = ctx.pressure_project(1e-3, 5)
+        assert rc == 0
+        outs.append(ctx.download("vel"))
+    assert np.abs(outs[0] - outs[1]).max() <= 1e-8 * np.abs(outs[0]).max()
