@@ -203,3 +203,65 @@ class Context:
         buf = C.create_string_buffer(1 << 16)
         check(lib().cup_profile_read(self._p, buf, len(buf)), self._p)
         return {k: (int(v[0]), float(v[1])) for k, v in json.loads(buf.value.decode()).items()}
+
+    # ---- solver settings ------------------------------------------------------
+    def set_poisson(self, solver="b200", tol_abs=1e-6, tol_rel=1e-4, max_iter=1000):
+        check(lib().cup_set_poisson(self._p, SOLVER[solver], tol_abs, tol_rel, max_iter), self._p)
+
+    def pressure_rhs(self, dt, step):
+        """Poisson right-hand side alone, into the 'lhs' field."""
+        check(lib().cup_pressure_rhs(self._p, dt, step), self._p)
+
+    # ---- learned preconditioner -------------------------------------------------
+    @staticmethod
+    def cnn_num_params():
+        return lib().cup_cnn_num_params()
+
+    def cnn_init(self, seed=0):
+        check(lib().cup_cnn_init(self._p, seed), self._p)
+
+    def cnn_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == self.cnn_num_params()
+        check(lib().cup_cnn_set_params(self._p, p.ctypes.data_as(C.POINTER(C.c_float))), self._p)
+
+    def cnn_get_params(self):
+        p = np.zeros(self.cnn_num_params(), np.float32)
+        check(lib().cup_cnn_get_params(self._p, p.ctypes.data_as(C.POINTER(C.c_float))), self._p)
+        return p
+
+    def cnn_dataset_reserve(self, capacity):
+        check(lib().cup_cnn_dataset_reserve(self._p, capacity), self._p)
+
+    def cnn_dataset_add(self, r, e):
+        """One sample per block from device vectors r (residual) and e (error)."""
+        check(lib().cup_cnn_dataset_add(self._p, _dev_ptr(r), _dev_ptr(e)), self._p)
+
+    def cnn_dataset_size(self):
+        return lib().cup_cnn_dataset_size(self._p)
+
+    def cnn_train(self, steps, batch=64, lr=1e-3, seed=0):
+        losses = np.zeros(max(steps, 1), np.float32)
+        check(lib().cup_cnn_train(self._p, steps, batch, lr, seed, losses.ctypes.data_as(C.POINTER(C.c_float))),
+              self._p)
+        return losses[:steps]
+
+    def cnn_forward(self, x, n):
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros(n * 512, np.float32)
+        fp = C.POINTER(C.c_float)
+        check(lib().cup_cnn_forward_host(self._p, x.ctypes.data_as(fp), out.ctypes.data_as(fp), n), self._p)
+        return out
+
+    def cnn_grad(self, x, target, n):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        g = np.zeros(self.cnn_num_params(), np.float32)
+        loss = np.zeros(1, np.float32)
+        fp = C.POINTER(C.c_float)
+        check(lib().cup_cnn_grad_host(self._p, x.ctypes.data_as(fp), t.ctypes.data_as(fp), n, g.ctypes.data_as(fp),
+                                      loss.ctypes.data_as(fp)), self._p)
+        return g, float(loss[0])
+
+    def cnn_precond(self, r, z):
+        check(lib().cup_cnn_precond_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)

@@ -24,7 +24,7 @@ CUP_ERR_STATE = -5
 
 BC = {"freespace": 0, "periodic": 1, "wall": 2}
 ADV = {"upwind5": 0, "upwind3": 0, "weno5": 1}
-SOLVER = {"b200": 0, "b200_mixed": 1, "b200_learned": 2}
+SOLVER = {"b200": 0, "b200_mixed": 1, "b200_learned": 2, "b200_learned_mixed": 3}
 FIELD = {"vel": 0, "pres": 1, "chi": 2, "lhs": 3, "tmpV": 4}
 FIELD_NCOMP = {"vel": 3, "pres": 1, "chi": 1, "lhs": 1, "tmpV": 3}
 
@@ -106,6 +106,20 @@ SIGNATURES = {
     "cup_penalize": (C.c_int, [_P, C.c_double, _D]),
     "cup_pressure_project": (C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(cup_solve_stats)]),
     "cup_step": (C.c_int, [_P, C.c_int32, C.c_double, _D, C.POINTER(cup_solve_stats)]),
+    "cup_pressure_rhs": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "cup_set_poisson": (C.c_int, [_P, C.c_int32, C.c_double, C.c_double, C.c_int32]),
+    "cup_cnn_num_params": (C.c_int32, []),
+    "cup_cnn_init": (C.c_int, [_P, C.c_uint64]),
+    "cup_cnn_set_params": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "cup_cnn_get_params": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "cup_cnn_dataset_reserve": (C.c_int, [_P, C.c_int32]),
+    "cup_cnn_dataset_add": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "cup_cnn_dataset_size": (C.c_int32, [_P]),
+    "cup_cnn_train": (C.c_int, [_P, C.c_int32, C.c_int32, C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "cup_cnn_forward_host": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32]),
+    "cup_cnn_grad_host": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,
+                                    C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "cup_cnn_precond_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_profile": (C.c_int, [_P, C.c_int32]),
     "cup_profile_read": (C.c_int, [_P, C.c_char_p, C.c_int32]),
 }

@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 
 #include "cnn.cuh"
+#include "fd.cuh"
 #include "lab.cuh"
 #include "profiler.h"
 
@@ -208,56 +209,106 @@ __device__ float gather_input(const DevMesh& M, int b, const T* v, float* x0, do
   return float(rms);
 }
 
+// Block inverse of the normalised input's interior (FdSmem aliased onto an
+// activation buffer that is free at this point); result zbj[512] = BJ(x0).
+__device__ void block_jacobi_of_input(const float* x0, double h, FdSmem& fs, double* zbj) {
+  fd_load_scale(fs);
+  for (int c = threadIdx.x; c < BN; c += blockDim.x)
+    fs.a[c] = double(x0[((c & 7) + 1) + 10 * ((((c >> 3) & 7) + 1) + 10 * ((c >> 6) + 1))]);
+  __syncthreads();
+  fd_apply(fs, -1.0 / h);
+  for (int c = threadIdx.x; c < BN; c += blockDim.x) zbj[c] = fs.a[c];
+  __syncthreads();
+}
+
+struct ApplySmem {
+  FwdSmem f;
+  double zbj[BN];
+};
+
+// z = BJ(r) + (s/h) CNN(r_lab / s) per block, and sum(z h^3) for the mean
+// constraint of the SpMV that follows (into *mean_sum when given).
 template <class T>
 __global__ void __launch_bounds__(NT, 1) k_cnn_apply(DevMesh M, const T* __restrict__ r, T* __restrict__ zout,
-                                                     CnnWeights W) {
+                                                     CnnWeights W, GridReduce G, double* mean_sum) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  FwdSmem& S = *reinterpret_cast<FwdSmem*>(smem_raw);
-  double* labd = reinterpret_cast<double*>(&S.b);  // the second act buffer doubles as gather scratch (8 KB)
+  ApplySmem& A = *reinterpret_cast<ApplySmem*>(smem_raw);
+  FwdSmem& S = A.f;
+  double* labd = reinterpret_cast<double*>(&S.b);  // gather scratch (8 KB of the free act buffer)
+  FdSmem& fs = *reinterpret_cast<FdSmem*>(&S.b);  // block-inverse scratch (12 KB), used after the gather
   load_weights(S, W);
+  double acc[1] = {0.0};
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
     __syncthreads();
     const float rms = gather_input<T>(M, b, r, S.x0, labd, S.red);
+    const double h = M.h[b];
+    if (rms > 0.f) block_jacobi_of_input(S.x0, h, fs, A.zbj);
     zero_act(S.a);
     zero_act(S.b);
     __syncthreads();
     if (rms > 0.f) forward_block(S);
-    const double sc = double(rms) / M.h[b];
-    for (int c = threadIdx.x; c < BN; c += NT) zout[size_t(b) * BN + c] = rms > 0.f ? T(sc * double(S.z[c])) : T(0);
+    double sum = 0.0;
+    for (int c = threadIdx.x; c < BN; c += NT) {
+      const T v = rms > 0.f ? T(double(rms) * (A.zbj[c] + double(S.z[c]) / h)) : T(0);
+      zout[size_t(b) * BN + c] = v;
+      sum += double(v);
+    }
+    acc[0] += sum * h * h * h;
   }
+  __shared__ double red[64];
+  if (grid_reduce<1>(acc, G, red) && threadIdx.x == 0 && mean_sum) *mean_sum = acc[0];
 }
 
 template <class T>
-int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid, cudaStream_t s) {
-  const size_t smem = sizeof(FwdSmem);
+int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid, cudaStream_t s, GridReduce G,
+              double* mean_sum) {
+  fd_init_constants();
+  const size_t smem = sizeof(ApplySmem);
   static bool attr = false;
   if (!attr) {
     CUP_CUDA_TRY(cudaFuncSetAttribute(k_cnn_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     attr = true;
   }
-  ProfScope ps(sizeof(T) == 4 ? "cnn_apply_f32io" : "cnn_apply_f64io", s);
-  k_cnn_apply<T><<<grid, NT, smem, s>>>(M, r, z, W);
+  ProfScope ps(sizeof(T) == 4 ? "cnn_precond_apply_f32io" : "cnn_precond_apply_f64io", s);
+  k_cnn_apply<T><<<grid, NT, smem, s>>>(M, r, z, W, G, mean_sum);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
-template int cnn_apply<double>(const DevMesh&, const double*, double*, const CnnWeights&, int, cudaStream_t);
-template int cnn_apply<float>(const DevMesh&, const float*, float*, const CnnWeights&, int, cudaStream_t);
+template int cnn_apply<double>(const DevMesh&, const double*, double*, const CnnWeights&, int, cudaStream_t,
+                               GridReduce, double*);
+template int cnn_apply<float>(const DevMesh&, const float*, float*, const CnnWeights&, int, cudaStream_t,
+                              GridReduce, double*);
 
-__global__ void __launch_bounds__(NT) k_cnn_gather(DevMesh M, const double* __restrict__ v, float* in, float* scale) {
+// Training pairs from a residual r and the error e = x* - x of the same
+// iterate: input = gather(r)/s, target = (e - BJ(r)) h / s on the block.
+__global__ void __launch_bounds__(NT) k_cnn_dataset(DevMesh M, const double* __restrict__ r,
+                                                    const double* __restrict__ e, float* in, float* target,
+                                                    int base, int cap, int* count) {
   __shared__ double labd[PV];
   __shared__ double red[64];
   __shared__ float x0[PV];
+  __shared__ FdSmem fs;
+  __shared__ double zbj[BN];
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    const int slot = base + b;
+    if (slot >= cap) break;
     __syncthreads();
-    const float rms = gather_input<double>(M, b, v, x0, labd, red);
-    for (int i = threadIdx.x; i < PV; i += NT) in[size_t(b) * PV + i] = x0[i];
-    if (threadIdx.x == 0) scale[b] = rms;
+    const float rms = gather_input<double>(M, b, r, x0, labd, red);
+    const double h = M.h[b];
+    const bool live = rms > 0.f;  // uniform across the CTA
+    if (live) block_jacobi_of_input(x0, h, fs, zbj);
+    for (int i = threadIdx.x; i < PV; i += NT) in[size_t(slot) * PV + i] = live ? x0[i] : 0.f;
+    for (int c = threadIdx.x; c < BN; c += NT)
+      target[size_t(slot) * BN + c] = live ? float((e[size_t(b) * BN + c] / double(rms) - zbj[c]) * h) : 0.f;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *count = min(cap, base + M.nb);
 }
 
-int cnn_gather(const DevMesh& M, const double* v, float* in, float* scale, int grid, cudaStream_t s) {
-  ProfScope ps("cnn_gather", s);
-  k_cnn_gather<<<grid, NT, 0, s>>>(M, v, in, scale);
+int cnn_dataset_add(const DevMesh& M, const double* r, const double* e, float* in, float* target, int base, int cap,
+                    int* count_dev, int grid, cudaStream_t s) {
+  fd_init_constants();
+  ProfScope ps("cnn_dataset_add", s);
+  k_cnn_dataset<<<grid, NT, 0, s>>>(M, r, e, in, target, base, cap, count_dev);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -396,7 +447,7 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* 
     __syncthreads();
     // dL/dz = grad_scale * 2 (z - t); loss += (z - t)^2
     for (int c = threadIdx.x; c < BN; c += NT) {
-      const float e = S.z[c] - target[size_t(smp) * BN + c];
+      const float e = S.z[c] - (target ? target[size_t(smp) * BN + c] : 0.f);
       if (out) out[size_t(sidx) * BN + c] = S.z[c];
       loss += e * e;
       S.z[c] = grad_scale * 2.f * e;
@@ -480,17 +531,17 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* 
 }
 
 // grad[i] = sum over CTAs of gpart[cta][i] (fixed order); loss = sum lpart * loss_scale
-__global__ void k_cnn_reduce(const float* gpart, int nparts, float* grad, const float* lpart, float loss_scale,
-                             float* loss) {
+__global__ void k_cnn_reduce(const float* gpart, int ngrad, float* grad, const float* lpart, int nloss,
+                             float loss_scale, float* loss) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < CNN_NPARAM) {
+  if (grad && i < CNN_NPARAM) {
     float s = 0.f;
-    for (int p = 0; p < nparts; ++p) s += gpart[size_t(p) * CNN_NPARAM + i];
+    for (int p = 0; p < ngrad; ++p) s += gpart[size_t(p) * CNN_NPARAM + i];
     grad[i] = s;
   }
   if (i == 0 && loss) {
     float s = 0.f;
-    for (int p = 0; p < nparts; ++p) s += lpart[p];
+    for (int p = 0; p < nloss; ++p) s += lpart[p];
     *loss = s * loss_scale;
   }
 }
@@ -507,6 +558,7 @@ __global__ void k_adam(float* w, const float* g, float* m, float* v, int t, floa
   w[i] -= lr * mh / (sqrtf(vh) + eps);
 }
 
+// gpart: >= grid*(CNN_NPARAM+1) floats (gradient rows, then one loss partial per CTA)
 static int train_launch(const CnnWeights& W, const float* in, const float* target, const int* idx, int n,
                         float* gpart, float* grad, float* loss_dev, float* out, int backward, int grid,
                         cudaStream_t s) {
@@ -519,28 +571,23 @@ static int train_launch(const CnnWeights& W, const float* in, const float* targe
   const int g = std::max(1, std::min(grid, n));
   // loss = mean over samples and cells; gradients of that mean
   const float scale = 1.0f / (float(n) * BN);
-  float* lpart = gpart + size_t(g) * CNN_NPARAM;  // g floats after the gradient rows
+  float* lpart = gpart + size_t(g) * CNN_NPARAM;
   {
     ProfScope ps(backward ? "cnn_train_fwd_bwd" : "cnn_forward_batch", s);
     k_cnn_train<<<g, NT, smem, s>>>(W, in, target, idx, n, scale, gpart, lpart, out, backward);
   }
   CUP_CUDA_TRY(cudaGetLastError());
   if (backward || loss_dev) {
-    k_cnn_reduce<<<(CNN_NPARAM + 255) / 256, 256, 0, s>>>(gpart, backward ? g : 0, grad, lpart, scale, loss_dev);
+    k_cnn_reduce<<<(CNN_NPARAM + 255) / 256, 256, 0, s>>>(gpart, g, backward ? grad : nullptr, lpart, g, scale,
+                                                          loss_dev);
     CUP_CUDA_TRY(cudaGetLastError());
-    if (!backward && loss_dev) {
-      // the reduce kernel above skipped the partial loss sum with nparts = 0
-      k_cnn_reduce<<<1, 32, 0, s>>>(gpart, 0, grad, lpart, scale, nullptr);
-    }
   }
   return 0;
 }
 
-int cnn_forward_batch(const CnnWeights& W, const float* in, float* out, int n, cudaStream_t s) {
-  // forward only: targets are not read when out is given and backward = 0;
-  // a zero target buffer is not needed because the loss is discarded.
-  return train_launch(W, in, out /* unused target reads happen before overwrite */, nullptr, n, nullptr, nullptr,
-                      nullptr, out, 0, 1184, s);
+int cnn_forward_batch(const CnnWeights& W, const float* in, float* out, int n, float* gpart, int grid,
+                      cudaStream_t s) {
+  return train_launch(W, in, nullptr, nullptr, n, gpart, nullptr, nullptr, out, 0, grid, s);
 }
 
 int cnn_grad_batch(const CnnWeights& W, const float* in, const float* target, int n, float* gpart, float* grad,

@@ -44,24 +44,30 @@ struct CnnWeights {
 // Packs the BF16 tensor-core copies from the FP32 master weights.
 int cnn_pack(const CnnWeights& W, cudaStream_t s);
 
-// z = (s/h) CNN(r_lab / s) for every block; r and z are nb*512 vectors of T.
+// z = BJ(r) + (s/h) CNN(r_lab / s) per block (BJ: the exact block inverse;
+// s: RMS of the block + halo input); sum(z h^3) into *mean_sum when given.
 template <class T>
-int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid, cudaStream_t s);
+int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid, cudaStream_t s, GridReduce G,
+              double* mean_sum);
 
-// Network input of every block: the block + halo of v (10^3, zero edges and
-// corners) divided by its RMS, into in[nb*1000]; RMS into scale[nb].
-int cnn_gather(const DevMesh& M, const double* v, float* in, float* scale, int grid, cudaStream_t s);
+// Appends one training sample per block from a residual r and its error
+// e = x* - x: input gather(r)/s (10^3), target (e - BJ(r)) h / s (8^3), at
+// rows base.. of in/target (capacity cap); the new count into *count_dev.
+int cnn_dataset_add(const DevMesh& M, const double* r, const double* e, float* in, float* target, int base, int cap,
+                    int* count_dev, int grid, cudaStream_t s);
 
 // Training on a device dataset of n samples: in[n*1000], target[n*512]
 // (targets already divided by the sample's scale/h).  One Adam step over a
 // minibatch of `batch` sample indices idx[batch]; loss (mean squared error)
-// into *loss_dev.  grad_partial: grid*CNN_NPARAM floats of scratch.
+// into *loss_dev.  grad_partial: grid*(CNN_NPARAM+1) floats of scratch.
 int cnn_train_step(const CnnWeights& W, float* adam_m, float* adam_v, int t, float lr, const float* in,
                    const float* target, const int* idx, int batch, float* grad_partial, float* grad, float* loss_dev,
                    int grid, cudaStream_t s);
 
 // Forward and gradient (no update) on a batch, for checks against the oracle.
-int cnn_forward_batch(const CnnWeights& W, const float* in, float* out, int n, cudaStream_t s);
+// gpart: >= grid*(CNN_NPARAM+1) floats of scratch.
+int cnn_forward_batch(const CnnWeights& W, const float* in, float* out, int n, float* gpart, int grid,
+                      cudaStream_t s);
 int cnn_grad_batch(const CnnWeights& W, const float* in, const float* target, int n, float* grad_partial,
                    float* grad, float* loss_dev, int grid, cudaStream_t s);
 

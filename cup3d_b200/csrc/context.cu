@@ -224,6 +224,7 @@ int cup_config_parse(cup_config* c, const char* args) {
       if (v == "b200") c->poisson_solver = CUP_POISSON_B200;
       else if (v == "b200_mixed") c->poisson_solver = CUP_POISSON_B200_MIXED;
       else if (v == "b200_learned") c->poisson_solver = CUP_POISSON_B200_LEARNED;
+      else if (v == "b200_learned_mixed") c->poisson_solver = CUP_POISSON_B200_LEARNED_MIXED;
       else return ctx_fail(nullptr, CUP_ERR_ARG, "Poisson solver: \"" + v + "\" unrecognized!");
     } else if (key == "device") {
       if (need_num()) return CUP_ERR_ARG;
@@ -405,14 +406,37 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   P.max_restarts = c->cfg.poisson_max_restarts;
   P.mean_mode = c->cfg.mean_constraint;
   P.check_every = 8;
+  P.stall_window = 0;
   SolveStats S{};
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   int rc = 0;
-  if (c->cfg.poisson_solver == CUP_POISSON_B200_MIXED)
-    rc = poisson_mixed(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned);
+  const int solver = c->cfg.poisson_solver;
+  const bool learned = solver == CUP_POISSON_B200_LEARNED || solver == CUP_POISSON_B200_LEARNED_MIXED;
+  if (learned && !c->cnn.ready)
+    return ctx_fail(c, CUP_ERR_STATE, "learned preconditioner has no weights (cup_cnn_init / cup_cnn_set_params)");
+  const CnnWeights* cnn = learned ? &c->cnn.W : nullptr;
+  int fallback = 0;
+  if (learned) P.stall_window = 40;  // a stall hands over to block-Jacobi below
+  if (solver == CUP_POISSON_B200_MIXED || solver == CUP_POISSON_B200_LEARNED_MIXED)
+    rc = poisson_mixed(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, cnn);
   else
-    rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned);
+    rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, cnn);
   if (rc) return keep(c, rc);
+  if (learned && S.status != SOLVE_CONVERGED && S.status != SOLVE_NAN) {
+    // The learned preconditioner stalled: plain block-Jacobi BiCGSTAB from the
+    // best iterate, against the original initial residual.
+    SolveParams Q = P;
+    Q.stall_window = 0;
+    Q.max_iter = std::max(1, P.max_iter - S.iterations);
+    if (S.err_init > 0) Q.tol_rel = std::min(1.0, P.tol_rel * S.err_init / std::max(S.err_opt, 1e-300));
+    SolveStats F{};
+    if (int rc2 = poisson_bicgstab(c->dm, b, x, Q, c->W, F, c->stream, c->h_pinned)) return keep(c, rc2);
+    S.iterations += F.iterations;
+    S.restarts += F.restarts;
+    S.status = F.status;
+    S.err_opt = F.err_opt;
+    fallback = 1;
+  }
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   CUP_CUDA_TRY(cudaEventSynchronize(c->ev1));
   float ms = 0;
@@ -427,14 +451,15 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
     stats->iterations = S.iterations;
     stats->restarts = S.restarts;
     stats->status = S.status;
-    stats->fallback = 0;
+    stats->fallback = fallback;
     stats->err_init = S.err_init;
     stats->err_final = S.err_opt;
     stats->true_rel = true_rel;
     stats->milliseconds = ms;
   }
   if (S.status == SOLVE_NAN) return ctx_fail(c, CUP_ERR_NAN, "Poisson solve produced NaN");
-  return S.status == SOLVE_CONVERGED ? CUP_OK : CUP_SOFT_MAXITER;
+  if (S.status != SOLVE_CONVERGED) return CUP_SOFT_MAXITER;
+  return fallback ? CUP_SOFT_FALLBACK : CUP_OK;
 }
 
 int cup_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats) {
@@ -649,6 +674,18 @@ int cup_penalize(cup_ctx* c, double dt, double* force6) {
   if (force6) e = cudaMemcpyAsync(force6, c->d_scalars + SC_FORCE, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "penalize", __FILE__, __LINE__));
+  return 0;
+}
+
+int cup_pressure_rhs(cup_ctx* c, double dt, int32_t step) {
+  ProfBind pb_(c);
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_pressure_rhs: no mesh");
+  Fields& F = c->F;
+  if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], F.pres[F.pcur], F.chi, ob_view(c), dt, step,
+                                   c->cfg.step_2nd_start, F.lhs, F.phi, grid_of(c), c->stream))
+    return keep(c, rc);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_rhs", __FILE__, __LINE__));
   return 0;
 }
 

@@ -6,6 +6,7 @@
 #include "../../include/cup3d_b200.h"
 #include "common.cuh"
 #include "mesh.h"
+#include "cnn.cuh"
 #include "poisson.cuh"
 #include "profiler.h"
 
@@ -44,6 +45,18 @@ struct DevObstacle {
   std::vector<double> h_chi, h_udef;
 };
 
+// Learned preconditioner state: weights, Adam moments, training scratch and
+// the device dataset of (input, target) samples.
+struct CnnState {
+  DevArena arena, data_arena;
+  CnnWeights W{};
+  float *adam_m = nullptr, *adam_v = nullptr, *grad = nullptr, *gpart = nullptr, *loss = nullptr;
+  float *ds_in = nullptr, *ds_target = nullptr;
+  int *ds_count = nullptr, *idx = nullptr;
+  int cap = 0, count = 0, adam_t = 0, train_grid = 148, idx_cap = 0;
+  bool ready = false;
+};
+
 // Offsets into cup_ctx::d_scalars
 enum : int { SC_SUMS = 0, SC_UMAX = 2, SC_FORCE = 8, SC_KIN = 16 };
 
@@ -75,14 +88,16 @@ struct cup_ctx {
   int num_sms = 148;
   bool host_only = false;         // device < 0: mesh work only
   cup3d::Profiler prof;
+  cup3d::CnnState cnn;
   std::string err;
 };
 
 namespace cup3d {
 // Binds the context's profiler to this thread for the duration of an API call.
 struct ProfBind {
-  ProfBind(cup_ctx* c) { t_prof = (c && c->prof.on) ? &c->prof : nullptr; }
-  ~ProfBind() { t_prof = nullptr; }
+  Profiler* prev;
+  ProfBind(cup_ctx* c) : prev(t_prof) { t_prof = (c && c->prof.on) ? &c->prof : nullptr; }
+  ~ProfBind() { t_prof = prev; }  // nested API calls restore the caller's binding
 };
 int ctx_fail(cup_ctx* c, int code, const std::string& msg);
 size_t nbn(const cup_ctx* c);

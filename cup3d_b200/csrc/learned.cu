@@ -1,0 +1,209 @@
+// C-ABI of the learned preconditioner: weights, dataset, training, checks.
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "context.h"
+
+namespace cup3d {
+
+static int ensure_cnn(cup_ctx* c) {
+  CnnState& S = c->cnn;
+  if (S.W.master) return 0;
+  DevArena& A = S.arena;
+  if (int rc = A.alloc(&S.W.master, CNN_NPARAM)) return rc;
+  if (int rc = A.alloc(&S.W.w1_bf16, 27 * 256)) return rc;
+  if (int rc = A.alloc(&S.W.w2_bf16, 27 * 256)) return rc;
+  if (int rc = A.alloc(&S.W.w1t_bf16, 27 * 256)) return rc;
+  if (int rc = A.alloc(&S.W.w2t_bf16, 27 * 256)) return rc;
+  if (int rc = A.alloc(&S.adam_m, CNN_NPARAM)) return rc;
+  if (int rc = A.alloc(&S.adam_v, CNN_NPARAM)) return rc;
+  if (int rc = A.alloc(&S.grad, CNN_NPARAM)) return rc;
+  if (int rc = A.alloc(&S.loss, 1)) return rc;
+  S.train_grid = std::max(1, c->num_sms);
+  if (int rc = A.alloc(&S.gpart, size_t(S.train_grid) * (CNN_NPARAM + 1))) return rc;
+  CUP_CUDA_TRY(cudaMemset(S.adam_m, 0, CNN_NPARAM * sizeof(float)));
+  CUP_CUDA_TRY(cudaMemset(S.adam_v, 0, CNN_NPARAM * sizeof(float)));
+  return 0;
+}
+
+static int set_params(cup_ctx* c, const float* p) {
+  if (int rc = ensure_cnn(c)) return rc;
+  CUP_CUDA_TRY(cudaMemcpy(c->cnn.W.master, p, CNN_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  if (int rc = cnn_pack(c->cnn.W, c->stream)) return rc;
+  CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->cnn.ready = true;
+  c->cnn.adam_t = 0;
+  CUP_CUDA_TRY(cudaMemset(c->cnn.adam_m, 0, CNN_NPARAM * sizeof(float)));
+  CUP_CUDA_TRY(cudaMemset(c->cnn.adam_v, 0, CNN_NPARAM * sizeof(float)));
+  return 0;
+}
+
+static bool dev_ok(cup_ctx* c) { return c && !c->host_only && c->mesh.nb > 0; }
+
+}  // namespace cup3d
+
+using namespace cup3d;
+
+extern "C" {
+
+int32_t cup_cnn_num_params(void) { return CNN_NPARAM; }
+
+int cup_cnn_init(cup_ctx* c, uint64_t seed) {
+  if (!c || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_init: no device context");
+  // He-normal weights (fan-in 27 * C_in), zero biases; the last layer starts
+  // small so the preconditioner starts as the block inverse.
+  std::mt19937_64 g(seed);
+  std::normal_distribution<float> n01(0.f, 1.f);
+  std::vector<float> p(CNN_NPARAM, 0.f);
+  auto fill = [&](int off, int cnt, float stdv) {
+    for (int i = 0; i < cnt; ++i) p[off + i] = stdv * n01(g);
+  };
+  fill(OFF_W0, CNN_W0, std::sqrt(2.f / 27.f));
+  fill(OFF_W1, CNN_W1, std::sqrt(2.f / (27.f * CNN_C)));
+  fill(OFF_W2, CNN_W2, std::sqrt(2.f / (27.f * CNN_C)));
+  fill(OFF_W3, CNN_W3, 0.01f * std::sqrt(1.f / (27.f * CNN_C)));
+  if (int rc = set_params(c, p.data())) return ctx_fail(c, rc, cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_cnn_set_params(cup_ctx* c, const float* params) {
+  if (!c || c->host_only || !params) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_set_params: bad arguments");
+  if (int rc = set_params(c, params)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_cnn_get_params(cup_ctx* c, float* params) {
+  if (!c || !params || !c->cnn.W.master) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_get_params: no weights");
+  cudaError_t e = cudaMemcpy(params, c->cnn.W.master, CNN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_get", __FILE__, __LINE__), cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_cnn_dataset_reserve(cup_ctx* c, int32_t capacity) {
+  if (!c || c->host_only || capacity <= 0) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_dataset_reserve: bad arguments");
+  CnnState& S = c->cnn;
+  S.data_arena.release();
+  S.cap = S.count = 0;
+  int rc = S.data_arena.alloc(&S.ds_in, size_t(capacity) * 1000);
+  if (!rc) rc = S.data_arena.alloc(&S.ds_target, size_t(capacity) * BN);
+  if (!rc) rc = S.data_arena.alloc(&S.ds_count, 1);
+  if (rc) return ctx_fail(c, rc, cup_last_error(nullptr));
+  S.cap = capacity;
+  return 0;
+}
+
+int cup_cnn_dataset_add(cup_ctx* c, const double* d_r, const double* d_e) {
+  ProfBind pb_(c);
+  if (!dev_ok(c) || !d_r || !d_e) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_dataset_add: bad arguments");
+  CnnState& S = c->cnn;
+  if (S.cap == 0) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_dataset_add: no dataset (cup_cnn_dataset_reserve)");
+  if (S.count >= S.cap) return 0;
+  if (int rc = cnn_dataset_add(c->dm, d_r, d_e, S.ds_in, S.ds_target, S.count, S.cap, S.ds_count, c->W.grid,
+                               c->stream))
+    return ctx_fail(c, rc, cup_last_error(nullptr));
+  S.count = std::min(S.cap, S.count + c->mesh.nb);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "dataset_add", __FILE__, __LINE__), cup_last_error(nullptr));
+  return 0;
+}
+
+int32_t cup_cnn_dataset_size(const cup_ctx* c) { return c ? c->cnn.count : 0; }
+
+int cup_cnn_train(cup_ctx* c, int32_t steps, int32_t batch, float lr, uint64_t seed, float* loss_out) {
+  ProfBind pb_(c);
+  if (!c || c->host_only || steps < 0 || batch <= 0) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_train: bad arguments");
+  CnnState& S = c->cnn;
+  if (!S.ready) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_train: no weights (cup_cnn_init)");
+  if (S.count <= 0) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_train: empty dataset");
+  if (S.idx_cap < batch) {
+    int* p = nullptr;
+    if (int rc = S.arena.alloc(&p, batch)) return ctx_fail(c, rc, cup_last_error(nullptr));
+    S.idx = p;
+    S.idx_cap = batch;
+  }
+  std::mt19937_64 g(seed);
+  std::uniform_int_distribution<int> pick(0, S.count - 1);
+  std::vector<int> idx(batch);
+  for (int it = 0; it < steps; ++it) {
+    for (int i = 0; i < batch; ++i) idx[i] = pick(g);
+    cudaError_t e = cudaMemcpyAsync(S.idx, idx.data(), batch * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "train idx", __FILE__, __LINE__), cup_last_error(nullptr));
+    S.adam_t += 1;
+    if (int rc = cnn_train_step(S.W, S.adam_m, S.adam_v, S.adam_t, lr, S.ds_in, S.ds_target, S.idx, batch, S.gpart,
+                                S.grad, S.loss, S.train_grid, c->stream))
+      return ctx_fail(c, rc, cup_last_error(nullptr));
+    if (loss_out) {
+      e = cudaMemcpyAsync(&loss_out[it], S.loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+      if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "train loss", __FILE__, __LINE__), cup_last_error(nullptr));
+    }
+    // the host index buffer is reused next iteration: wait for its copy
+    e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "train", __FILE__, __LINE__), cup_last_error(nullptr));
+  }
+  return 0;
+}
+
+int cup_cnn_forward_host(cup_ctx* c, const float* in, float* out, int32_t n) {
+  if (!c || c->host_only || !in || !out || n <= 0) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_forward_host: bad arguments");
+  CnnState& S = c->cnn;
+  if (!S.ready) return ctx_fail(c, CUP_ERR_STATE, "no weights");
+  DevArena tmp;
+  float *din, *dout;
+  int rc = tmp.alloc(&din, size_t(n) * 1000);
+  if (!rc) rc = tmp.alloc(&dout, size_t(n) * BN);
+  if (rc) return ctx_fail(c, rc, cup_last_error(nullptr));
+  cudaMemcpy(din, in, size_t(n) * 1000 * sizeof(float), cudaMemcpyHostToDevice);
+  if ((rc = cnn_forward_batch(S.W, din, dout, n, S.gpart, S.train_grid, c->stream)))
+    return ctx_fail(c, rc, cup_last_error(nullptr));
+  cudaError_t e = cudaMemcpyAsync(out, dout, size_t(n) * BN * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_forward", __FILE__, __LINE__), cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_cnn_grad_host(cup_ctx* c, const float* in, const float* target, int32_t n, float* grad, float* loss) {
+  if (!c || c->host_only || !in || !target || !grad || n <= 0)
+    return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_grad_host: bad arguments");
+  CnnState& S = c->cnn;
+  if (!S.ready) return ctx_fail(c, CUP_ERR_STATE, "no weights");
+  DevArena tmp;
+  float *din, *dt;
+  int rc = tmp.alloc(&din, size_t(n) * 1000);
+  if (!rc) rc = tmp.alloc(&dt, size_t(n) * BN);
+  if (rc) return ctx_fail(c, rc, cup_last_error(nullptr));
+  cudaMemcpy(din, in, size_t(n) * 1000 * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(dt, target, size_t(n) * BN * sizeof(float), cudaMemcpyHostToDevice);
+  if ((rc = cnn_grad_batch(S.W, din, dt, n, S.gpart, S.grad, S.loss, S.train_grid, c->stream)))
+    return ctx_fail(c, rc, cup_last_error(nullptr));
+  cudaError_t e = cudaMemcpyAsync(grad, S.grad, CNN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && loss) e = cudaMemcpyAsync(loss, S.loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_grad", __FILE__, __LINE__), cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_cnn_precond_dev(cup_ctx* c, const double* d_r, double* d_z) {
+  ProfBind pb_(c);
+  if (!dev_ok(c) || !d_r || !d_z) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_precond_dev: bad arguments");
+  if (!c->cnn.ready) return ctx_fail(c, CUP_ERR_STATE, "no weights");
+  GridReduce g{c->W.partial, c->W.counters + 15};
+  if (int rc = cnn_apply<double>(c->dm, d_r, d_z, c->cnn.W, c->W.grid, c->stream, g, nullptr))
+    return ctx_fail(c, rc, cup_last_error(nullptr));
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_precond", __FILE__, __LINE__), cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_set_poisson(cup_ctx* c, int32_t solver, double tol_abs, double tol_rel, int32_t max_iter) {
+  if (!c || solver < 0 || solver > CUP_POISSON_B200_LEARNED_MIXED || max_iter < 0)
+    return ctx_fail(c, CUP_ERR_ARG, "cup_set_poisson: bad arguments");
+  c->cfg.poisson_solver = solver;
+  c->cfg.poisson_tol = tol_abs;
+  c->cfg.poisson_tol_rel = tol_rel;
+  c->cfg.poisson_max_iter = max_iter;
+  return 0;
+}
+
+}  // extern "C"

@@ -17,28 +17,14 @@
 #include <cmath>
 #include <cstring>
 
+#include "cnn.cuh"
+#include "fd.cuh"
 #include "poisson.cuh"
 #include "profiler.h"
 
 namespace cup3d {
 
-// DST-I eigenvectors of tridiag(-1,2,-1) on 8 points and their eigenvalues.
-__constant__ double c_S[64];
-__constant__ double c_lam[8];
-static bool g_consts_ready = false;
-
-void poisson_init_constants() {
-  if (g_consts_ready) return;
-  double S[64], lam[8];
-  const double pi = 3.14159265358979323846;
-  for (int j = 0; j < 8; ++j) {
-    lam[j] = 2.0 - 2.0 * std::cos(pi * (j + 1) / 9.0);
-    for (int k = 0; k < 8; ++k) S[j * 8 + k] = std::sqrt(2.0 / 9.0) * std::sin(pi * (j + 1) * (k + 1) / 9.0);
-  }
-  cudaMemcpyToSymbol(c_S, S, sizeof(S));
-  cudaMemcpyToSymbol(c_lam, lam, sizeof(lam));
-  g_consts_ready = true;
-}
+void poisson_init_constants() { fd_init_constants(); }
 
 // ---------------------------------------------------------------------------
 // Coarse-fine interpolation of PoissonSolverExp::interpolate: the Taylor part
@@ -207,65 +193,6 @@ __device__ void spmv_block(const DevMesh& M, int b, const T* __restrict__ x, dou
 }
 
 // ---------------------------------------------------------------------------
-// z = (1/h) P_inv v = -(1/h) L_D^-1 v on one block by fast diagonalization.
-// Thread t owns mode index k = t&7 along the transformed axis and the two
-// transverse positions (t>>3) and (t>>3)+32.  buf holds the block on entry
-// and the result on exit.
-// ---------------------------------------------------------------------------
-struct FdSmem {
-  double a[512];
-  double b[512];
-  double inv_lam[512];
-};
-
-__device__ __forceinline__ void fd_load_scale(FdSmem& sm) {
-  for (int i = threadIdx.x; i < 512; i += NT) {
-    const int kx = i & 7, ky = (i >> 3) & 7, kz = i >> 6;
-    sm.inv_lam[i] = 1.0 / (c_lam[kx] + c_lam[ky] + c_lam[kz]);
-  }
-}
-
-// one mode product along axis `ax` (0=x,1=y,2=z): out = S x_ax in
-__device__ __forceinline__ void fd_pass(const double* in, double* out, int ax, const double Srow[8]) {
-  const int t = threadIdx.x, k = t & 7;
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const int o = (t >> 3) + 32 * q;  // transverse pair index 0..63
-    const int p0 = o & 7, p1 = o >> 3;
-    int base, stride;
-    if (ax == 0) { base = 8 * p0 + 64 * p1; stride = 1; }
-    else if (ax == 1) { base = p0 + 64 * p1; stride = 8; }
-    else { base = p0 + 8 * p1; stride = 64; }
-    double s = 0.0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) s = fma(Srow[i], in[base + stride * i], s);
-    out[base + stride * k] = s;
-  }
-}
-
-// in: sm.a, result in sm.a.  scale = -1/h
-__device__ __forceinline__ void fd_apply(FdSmem& sm, double scale) {
-  const int t = threadIdx.x, k = t & 7;
-  double Srow[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) Srow[i] = c_S[k * 8 + i];
-  fd_pass(sm.a, sm.b, 0, Srow);
-  __syncthreads();
-  fd_pass(sm.b, sm.a, 1, Srow);
-  __syncthreads();
-  fd_pass(sm.a, sm.b, 2, Srow);
-  __syncthreads();
-  for (int i = t; i < 512; i += NT) sm.b[i] *= scale * sm.inv_lam[i];
-  __syncthreads();
-  fd_pass(sm.b, sm.a, 0, Srow);
-  __syncthreads();
-  fd_pass(sm.a, sm.b, 1, Srow);
-  __syncthreads();
-  fd_pass(sm.b, sm.a, 2, Srow);
-  __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
 // Standalone kernels
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(NT) k_weighted_sum(DevMesh M, const double* __restrict__ v,
@@ -334,6 +261,7 @@ struct KArgs {
   GridReduce g;
   int mean_mode;
   int zero_mean_row;  // b and x0 are zero at the mean row (getVec, modes 1 and 3)
+  int ext_precond;    // 1: kernels a and c only update p and s; a separate kernel applies the preconditioner
 };
 
 template <class T>
@@ -405,6 +333,8 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
     S.converged = 0;
     S.done = 0;
     S.status = SOLVE_RUNNING;
+    S.last_improve_k = 0;
+    S.stall_ref = e;
     if (!(e == e)) {
       S.done = 1;
       S.status = SOLVE_NAN;
@@ -446,6 +376,7 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
       A.p[i] = T(pi);
       sm.a[c] = double(T(pi));
     }
+    if (A.ext_precond) continue;  // uniform; z1 comes from the external preconditioner
     __syncthreads();
     const double h = M.h[b];
     fd_apply(sm, -1.0 / h);
@@ -518,6 +449,7 @@ __global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
       A.r[i] = si;
       sm.a[c] = double(si);
     }
+    if (A.ext_precond) continue;  // uniform; z2 comes from the external preconditioner
     __syncthreads();
     const double h = M.h[b];
     fd_apply(sm, -1.0 / h);
@@ -608,6 +540,13 @@ __global__ void __launch_bounds__(NT) k_bicg_e(KArgs<T> A) {
     if (!W.done && W.k >= W.max_iter) {
       W.done = 1;
       W.status = SOLVE_MAXITER;
+    }
+    if (err < 0.9 * W.stall_ref) {
+      W.stall_ref = err;
+      W.last_improve_k = W.k;
+    } else if (!W.done && W.stall_window > 0 && W.k - W.last_improve_k >= W.stall_window) {
+      W.done = 1;
+      W.status = SOLVE_STALL;
     }
     W.rho_prev = W.rho;
     W.rho = acc[0];
@@ -705,6 +644,7 @@ static KArgs<T> make_args(const DevMesh& M, const T* b, T* x, T* const v[9], Poi
   A.g.counter = W.counters + site;
   A.mean_mode = mean_mode;
   A.zero_mean_row = zero_mean_row;
+  A.ext_precond = 0;
   return A;
 }
 
@@ -741,16 +681,20 @@ int launch_block_inverse(const DevMesh& M, const double* in, double* out, Poisso
 // Runs BiCGSTAB on vectors of type T; x holds x0 on entry, x_opt on exit.
 template <class T>
 static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, int zero_mean_row,
-                        PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done) {
+                        PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done,
+                        const CnnWeights* cnn = nullptr) {
   const bool f32 = sizeof(T) == 4;
   KrylovState init{};
   init.tol_abs = P.tol_abs;
   init.tol_rel = P.tol_rel;
   init.max_iter = P.max_iter;
   init.max_restarts = P.max_restarts;
+  init.stall_window = P.stall_window;
   init.eps = 1e-21;
   CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   KArgs<T> A = make_args<T>(M, b, x, v, W, W.st, P.mean_mode, zero_mean_row, 0);
+  A.ext_precond = cnn ? 1 : 0;
+  GridReduce gc{W.partial, W.counters + 14};
   { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); k_bicg_prepare<T><<<W.grid, NT, 0, s>>>(A); }
   { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); k_bicg_init<T><<<W.grid, NT, 0, s>>>(A); }
   CUP_CUDA_TRY(cudaGetLastError());
@@ -758,8 +702,12 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   for (int it = 0; it < P.max_iter; it += chunk) {
     for (int j = 0; j < chunk; ++j) {
       { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); k_bicg_a<T><<<W.grid, NT, 0, s>>>(A); }
+      if (cnn)
+        if (int rc = cnn_apply<T>(M, A.p, A.z1, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
       { ProfScope ps(f32 ? "bicg32_b_spmv_dot" : "bicg_b_spmv_dot", s); k_bicg_b<T><<<W.grid, NT, 0, s>>>(A); }
       { ProfScope ps(f32 ? "bicg32_c_supdate_precond" : "bicg_c_supdate_precond", s); k_bicg_c<T><<<W.grid, NT, 0, s>>>(A); }
+      if (cnn)
+        if (int rc = cnn_apply<T>(M, A.r, A.z2, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
       { ProfScope ps(f32 ? "bicg32_d_spmv_dots" : "bicg_d_spmv_dots", s); k_bicg_d<T><<<W.grid, NT, 0, s>>>(A); }
       { ProfScope ps(f32 ? "bicg32_e_xr_update_dots" : "bicg_e_xr_update_dots", s); k_bicg_e<T><<<W.grid, NT, 0, s>>>(A); }
     }
@@ -784,11 +732,11 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
 }
 
 int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
-                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done) {
+                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done, const CnnWeights* cnn) {
   poisson_init_constants();
   double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
   const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
-  return run_bicgstab<double>(M, b, x, v, P, zmr, W, out, s, h_done);
+  return run_bicgstab<double>(M, b, x, v, P, zmr, W, out, s, h_done, cnn);
 }
 
 // Mixed precision: FP64 iterative refinement around FP32 BiCGSTAB inner solves.
@@ -797,7 +745,7 @@ int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolvePa
 // scalars) to a relative tolerance tied to the remaining reduction, and adds e
 // to x in FP64.
 int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
-                  SolveStats& out, cudaStream_t s, int* h_done) {
+                  SolveStats& out, cudaStream_t s, int* h_done, const CnnWeights* cnn) {
   poisson_init_constants();
   const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
   const size_t n = size_t(M.nb) * BN;
@@ -849,7 +797,7 @@ int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParam
     Q.max_iter = std::max(1, P.max_iter - inner_total);
     CUP_CUDA_TRY(cudaMemsetAsync(e, 0, n * sizeof(float), s));
     SolveStats in{};
-    if (int rc = run_bicgstab<float>(M, W.r32, e, v, Q, 0, W, in, s, h_done)) return rc;
+    if (int rc = run_bicgstab<float>(M, W.r32, e, v, Q, 0, W, in, s, h_done, cnn)) return rc;
     inner_total += in.iterations;
     restarts += in.restarts;
     if (in.status == SOLVE_NAN) {

@@ -16,7 +16,9 @@ struct KrylovState {
   int k, restarts, max_restarts, max_iter;
   int done, converged, restart_pending, status;
   int cur, best, nxt;                // x buffer rotation (x_opt without copies)
-  int pad;
+  int stall_window;                  // > 0: stop when ||r|| has not dropped 10% in this many iterations
+  int last_improve_k;
+  double stall_ref;
 };
 
 enum SolveStatus : int {
@@ -24,7 +26,8 @@ enum SolveStatus : int {
   SOLVE_CONVERGED = 1,
   SOLVE_MAXITER = 2,
   SOLVE_RESTARTS = 3,
-  SOLVE_NAN = 4
+  SOLVE_NAN = 4,
+  SOLVE_STALL = 5
 };
 
 struct PoissonWork {
@@ -42,7 +45,8 @@ struct PoissonWork {
 struct SolveParams {
   double tol_abs, tol_rel;
   int max_iter, max_restarts, mean_mode;
-  int check_every;  // host checks convergence every this many iterations
+  int check_every;   // host checks convergence every this many iterations
+  int stall_window;  // 0: off (reference behaviour)
 };
 
 struct SolveStats {
@@ -56,12 +60,15 @@ int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_
 int launch_block_inverse(const DevMesh& M, const double* in, double* out, PoissonWork& W,
                          cudaStream_t s);
 // Solves A x = b; x holds the initial guess on entry and x_opt on exit.
+// cnn != nullptr: the learned preconditioner replaces the block inverse.
+struct CnnWeights;
 int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
-                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done_pinned);
+                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done_pinned,
+                     const CnnWeights* cnn = nullptr);
 
 // Mixed precision: FP32 inner BiCGSTAB inside FP64 iterative refinement.
 int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
-                  SolveStats& out, cudaStream_t s, int* h_done_pinned);
+                  SolveStats& out, cudaStream_t s, int* h_done_pinned, const CnnWeights* cnn = nullptr);
 // FP64 ||b - A x||_2 with the solvers' mean-row convention.
 int true_residual_norm(const DevMesh& M, const double* b, const double* x, int mean_mode, PoissonWork& W,
                        double* err_host, cudaStream_t s);

@@ -43,6 +43,7 @@ extern "C" {
 #define CUP_POISSON_B200 0          /* "b200": FP64 BiCGSTAB, exact block inverse */
 #define CUP_POISSON_B200_MIXED 1    /* "b200_mixed": FP32 inner, FP64 refinement */
 #define CUP_POISSON_B200_LEARNED 2  /* "b200_learned": CNN preconditioner, flexible */
+#define CUP_POISSON_B200_LEARNED_MIXED 3 /* "b200_learned_mixed": both */
 
 /* field ids */
 #define CUP_FIELD_VEL 0   /* 3 components */
@@ -157,9 +158,37 @@ int cup_compute_dt(cup_ctx* ctx, int32_t step, double* dt);
 int cup_advect_diffuse(cup_ctx* ctx, double dt);                    /* AdvectionDiffusion */
 int cup_penalize(cup_ctx* ctx, double dt, double* force_torque6);   /* Penalization */
 int cup_pressure_project(cup_ctx* ctx, double dt, int32_t step, cup_solve_stats* stats);
+/* The Poisson right-hand side of PressureProjection alone (KernelPressureRHS
+ * and, for step > 2, KernelDivPressure; PressureProjection.cpp:340-394) into
+ * CUP_FIELD_LHS, from the current velocity, pressure, chi and body. */
+int cup_pressure_rhs(cup_ctx* ctx, double dt, int32_t step);
 /* One time step: AdvectionDiffusion, Penalization (if a body is set),
  * PressureProjection.  dt <= 0: computed by calcMaxTimestep; *dt_used gets it. */
 int cup_step(cup_ctx* ctx, int32_t step, double dt, double* dt_used, cup_solve_stats* stats);
+
+/* Changes the Poisson solver settings of a context (-poissonSolver,
+ * -poissonTol, -poissonTolRel and the iteration cap). */
+int cup_set_poisson(cup_ctx* ctx, int32_t solver, double tol_abs, double tol_rel, int32_t max_iter);
+
+/* ---- learned preconditioner (no counterpart in the reference: the new slot at
+ * the preconditioner call sites PoissonSolverAMR.h:183-222, BiCGSTAB.cu:526-527).
+ * z = BJ(r) + (s/h) CNN(r_block+halo / s): the exact block inverse plus a
+ * per-block 3-D CNN correction (4 conv 3^3 layers, 16 channels). ---- */
+int32_t cup_cnn_num_params(void);
+int cup_cnn_init(cup_ctx* ctx, uint64_t seed);                 /* random initial weights */
+int cup_cnn_set_params(cup_ctx* ctx, const float* params);     /* cup_cnn_num_params() floats */
+int cup_cnn_get_params(cup_ctx* ctx, float* params);
+int cup_cnn_dataset_reserve(cup_ctx* ctx, int32_t capacity);   /* samples (one per block per pair) */
+/* adds one sample per block from device vectors: residual r and error e = x* - x */
+int cup_cnn_dataset_add(cup_ctx* ctx, const double* d_r, const double* d_e);
+int32_t cup_cnn_dataset_size(const cup_ctx* ctx);
+/* `steps` Adam steps on random minibatches (seeded); per-step loss into loss_out (or NULL) */
+int cup_cnn_train(cup_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed, float* loss_out);
+/* network forward / loss and gradient on host arrays (n samples of 10^3 inputs, 8^3 targets) */
+int cup_cnn_forward_host(cup_ctx* ctx, const float* in, float* out, int32_t n);
+int cup_cnn_grad_host(cup_ctx* ctx, const float* in, const float* target, int32_t n, float* grad, float* loss);
+/* z = learned preconditioner applied to the device vector r */
+int cup_cnn_precond_dev(cup_ctx* ctx, const double* d_r, double* d_z);
 
 /* ---- profiling (the reference's DeviceProfiler, Utils/DeviceProfiler.cuh) ---- */
 /* Enables per-kernel CUDA-event timing (resets the counters). */

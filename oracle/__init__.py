@@ -49,7 +49,8 @@ SIG = {
                                     C.c_int, C.c_double, C.c_double, _D, _D]),
     "orc_pressure_rhs": (None, [C.c_void_p, _D, _D, _D, _I, C.c_int, _D, _D, C.c_double, C.c_int, _D]),
     "orc_grad_update": (None, [C.c_void_p, _D, _D, C.c_double]),
-    "orc_cnn_forward": (None, [C.c_int, C.c_int, _F, _F, _F, _F, _F]),
+    "orc_cnn_nparam": (C.c_int, [C.c_int]),
+    "orc_cnn_fwd_grad": (None, [C.c_int, C.c_int, _D, _F, _F, _F, _D, _D]),
 }
 
 
@@ -250,10 +251,14 @@ def dt(hmin, nu, cfl, umax, step, rampup):
     return lib().orc_dt(hmin, nu, cfl, umax, step, rampup)
 
 
-def cnn_forward(w, b, x, C_):
+def cnn_fwd_grad(params, x, target=None, C_=16, want_grad=True):
+    """(out[n*512] float32, grad[nparam] or None, loss or None) of the CNN in FP64."""
+    params = np.ascontiguousarray(params, np.float64)
     x = np.ascontiguousarray(x, np.float32)
     n = x.size // 1000
     out = np.zeros(n * 512, np.float32)
-    lib().orc_cnn_forward(n, C_, _f(np.ascontiguousarray(w, np.float32)), _f(np.ascontiguousarray(b, np.float32)),
-                          _f(x), _f(out), None)
-    return out
+    grad = np.zeros(lib().orc_cnn_nparam(C_)) if (want_grad and target is not None) else None
+    loss = np.zeros(1)
+    t = None if target is None else np.ascontiguousarray(target, np.float32)
+    lib().orc_cnn_fwd_grad(n, C_, _d(params), _f(x), _f(t), _f(out), _d(grad), _d(loss) if t is not None else None)
+    return out, grad, (float(loss[0]) if t is not None else None)

@@ -1422,68 +1422,149 @@ extern "C" void orc_pressure_project(orc_mesh* m, double* vel, double* pres, con
 
 // ============================================================================
 // Learned preconditioner network (no reference counterpart; written from the
-// definition of a 3-D convolution).  Layer k maps C_in -> C_out channels with a
-// 3x3x3 kernel, weights w[k][co][ci][27], bias[k][co]; ReLU after layers 0-2.
-// Input: 10^3 (block + 1-cell halo), 1 channel.  Layer 0 is 'valid' (10^3 ->
-// 8^3); layers 1-3 are zero-padded 'same' on 8^3.  Output 8^3, 1 channel.
+// definition of a 3-D convolution).  Parameters in one array, in this order:
+// W0[co][tap] (1 -> C, 'valid' on the 10^3 input), b0[C], W1[co][ci][tap],
+// b1[C], W2[co][ci][tap], b2[C], W3[ci][tap] (C -> 1), b3; tap = kx + 3 ky + 9 kz.
+// ReLU after layers 0-2; layers 1-3 are zero-padded 'same' convolutions on
+// the 8^3 block.  Loss: mean over samples and cells of (z - target)^2.
 // ============================================================================
-extern "C" void orc_cnn_forward(int nblk, int C, const float* w, const float* bias, const float* in,
-                                float* out, float* acts) {
-  const int cin[4] = {1, C, C, C}, cout[4] = {C, C, C, 1};
-  size_t woff[4], boff[4];
-  size_t wo = 0, bo = 0;
-  for (int k = 0; k < 4; ++k) {
-    woff[k] = wo;
-    boff[k] = bo;
-    wo += size_t(cout[k]) * cin[k] * 27;
-    bo += cout[k];
+namespace {
+struct CnnDims {
+  int C, oW0, oB0, oW1, oB1, oW2, oB2, oW3, oB3, n;
+  explicit CnnDims(int c) : C(c) {
+    oW0 = 0;
+    oB0 = oW0 + C * 27;
+    oW1 = oB0 + C;
+    oB1 = oW1 + C * C * 27;
+    oW2 = oB1 + C;
+    oB2 = oW2 + C * C * 27;
+    oW3 = oB2 + C;
+    oB3 = oW3 + C * 27;
+    n = oB3 + 1;
   }
+};
+inline bool inb(int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < BS && y < BS && z < BS; }
+}  // namespace
+
+extern "C" int orc_cnn_nparam(int C) { return CnnDims(C).n; }
+
+extern "C" void orc_cnn_fwd_grad(int nblk, int C, const double* P, const float* in, const float* target,
+                                 float* out, double* grad, double* loss) {
+  const CnnDims D(C);
+  const double scale = 1.0 / (double(nblk) * BN);
+  std::vector<double> G(grad ? D.n : 0, 0.0);
+  double L = 0;
 #pragma omp parallel
   {
-    std::vector<float> a(size_t(C) * BN), bbuf(size_t(C) * BN);
+    std::vector<double> a1(C * BN), a2(C * BN), a3(C * BN), z(BN), d3(C * BN), d2(C * BN), d1(C * BN);
+    std::vector<double> g(grad ? D.n : 0, 0.0);
+    double l = 0;
 #pragma omp for schedule(static)
     for (int n = 0; n < nblk; ++n) {
       const float* x = in + size_t(n) * 1000;
-      // layer 0: valid conv on 10^3
+      auto X = [&](int xx, int yy, int zz) { return double(x[xx + 10 * (yy + 10 * zz)]); };
       for (int co = 0; co < C; ++co)
-        for (int z = 0; z < BS; ++z)
-          for (int y = 0; y < BS; ++y)
-            for (int xx = 0; xx < BS; ++xx) {
-              float s = bias[boff[0] + co];
-              for (int kz = 0; kz < 3; ++kz)
-                for (int ky = 0; ky < 3; ++ky)
-                  for (int kx = 0; kx < 3; ++kx)
-                    s += w[woff[0] + size_t(co) * 27 + kx + 3 * ky + 9 * kz] *
-                         x[(xx + kx) + 10 * ((y + ky) + 10 * (z + kz))];
-              a[size_t(co) * BN + cell(xx, y, z)] = s > 0 ? s : 0;
-            }
-      if (acts) std::copy(a.begin(), a.end(), acts + (size_t(n) * 3 + 0) * C * BN);
-      for (int k = 1; k < 4; ++k) {
-        const int co_n = cout[k];
-        for (int co = 0; co < co_n; ++co)
-          for (int z = 0; z < BS; ++z)
-            for (int y = 0; y < BS; ++y)
-              for (int xx = 0; xx < BS; ++xx) {
-                float s = bias[boff[k] + co];
-                for (int ci = 0; ci < C; ++ci)
-                  for (int kz = 0; kz < 3; ++kz)
-                    for (int ky = 0; ky < 3; ++ky)
-                      for (int kx = 0; kx < 3; ++kx) {
-                        const int X = xx + kx - 1, Y = y + ky - 1, Z = z + kz - 1;
-                        if (X < 0 || Y < 0 || Z < 0 || X >= BS || Y >= BS || Z >= BS) continue;
-                        s += w[woff[k] + (size_t(co) * C + ci) * 27 + kx + 3 * ky + 9 * kz] *
-                             a[size_t(ci) * BN + cell(X, Y, Z)];
-                      }
-                if (k < 3)
-                  bbuf[size_t(co) * BN + cell(xx, y, z)] = s > 0 ? s : 0;
-                else
-                  out[size_t(n) * BN + cell(xx, y, z)] = s;
-              }
-        if (k < 3) {
-          std::swap(a, bbuf);
-          if (acts) std::copy(a.begin(), a.end(), acts + (size_t(n) * 3 + k) * C * BN);
+        for (int c = 0; c < BN; ++c) {
+          const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
+          double s = P[D.oB0 + co];
+          for (int t = 0; t < 27; ++t) s += P[D.oW0 + co * 27 + t] * X(xx + t % 3, yy + (t / 3) % 3, zz + t / 9);
+          a1[co * BN + c] = s > 0 ? s : 0;
         }
+      auto same = [&](const std::vector<double>& a, int oW, int oB, std::vector<double>& o) {
+        for (int co = 0; co < C; ++co)
+          for (int c = 0; c < BN; ++c) {
+            const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
+            double s = P[oB + co];
+            for (int ci = 0; ci < C; ++ci)
+              for (int t = 0; t < 27; ++t) {
+                const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
+                if (inb(X2, Y2, Z2)) s += P[oW + (co * C + ci) * 27 + t] * a[ci * BN + cell(X2, Y2, Z2)];
+              }
+            o[co * BN + c] = s > 0 ? s : 0;
+          }
+      };
+      same(a1, D.oW1, D.oB1, a2);
+      same(a2, D.oW2, D.oB2, a3);
+      for (int c = 0; c < BN; ++c) {
+        const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
+        double s = P[D.oB3];
+        for (int ci = 0; ci < C; ++ci)
+          for (int t = 0; t < 27; ++t) {
+            const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
+            if (inb(X2, Y2, Z2)) s += P[D.oW3 + ci * 27 + t] * a3[ci * BN + cell(X2, Y2, Z2)];
+          }
+        z[c] = s;
+        if (out) out[size_t(n) * BN + c] = float(s);
       }
+      if (!target) continue;
+      for (int c = 0; c < BN; ++c) {
+        const double e = z[c] - target[size_t(n) * BN + c];
+        l += e * e;
+        z[c] = 2.0 * e * scale;  // dL/dz
+      }
+      if (!grad) continue;
+      // layer 3
+      for (int c = 0; c < BN; ++c) {
+        const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
+        g[D.oB3] += z[c];
+        for (int ci = 0; ci < C; ++ci)
+          for (int t = 0; t < 27; ++t) {
+            const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
+            if (inb(X2, Y2, Z2)) g[D.oW3 + ci * 27 + t] += a3[ci * BN + cell(X2, Y2, Z2)] * z[c];
+          }
+      }
+      std::fill(d3.begin(), d3.end(), 0.0);
+      for (int c = 0; c < BN; ++c) {
+        const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
+        for (int ci = 0; ci < C; ++ci)
+          for (int t = 0; t < 27; ++t) {
+            const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
+            if (inb(X2, Y2, Z2)) d3[ci * BN + cell(X2, Y2, Z2)] += P[D.oW3 + ci * 27 + t] * z[c];
+          }
+      }
+      for (int i = 0; i < C * BN; ++i)
+        if (!(a3[i] > 0)) d3[i] = 0;
+      auto back_same = [&](const std::vector<double>& a, const std::vector<double>& dp, int oW, int oB,
+                           std::vector<double>* da, const std::vector<double>* amask) {
+        for (int co = 0; co < C; ++co)
+          for (int c = 0; c < BN; ++c) {
+            const double dv = dp[co * BN + c];
+            if (dv == 0) continue;
+            const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
+            g[oB + co] += dv;
+            for (int ci = 0; ci < C; ++ci)
+              for (int t = 0; t < 27; ++t) {
+                const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
+                if (!inb(X2, Y2, Z2)) continue;
+                const int cc = cell(X2, Y2, Z2);
+                g[oW + (co * C + ci) * 27 + t] += a[ci * BN + cc] * dv;
+                if (da) (*da)[ci * BN + cc] += P[oW + (co * C + ci) * 27 + t] * dv;
+              }
+          }
+        if (da)
+          for (int i = 0; i < C * BN; ++i)
+            if (!((*amask)[i] > 0)) (*da)[i] = 0;
+      };
+      std::fill(d2.begin(), d2.end(), 0.0);
+      back_same(a2, d3, D.oW2, D.oB2, &d2, &a2);
+      std::fill(d1.begin(), d1.end(), 0.0);
+      back_same(a1, d2, D.oW1, D.oB1, &d1, &a1);
+      for (int co = 0; co < C; ++co)
+        for (int c = 0; c < BN; ++c) {
+          const double dv = d1[co * BN + c];
+          if (dv == 0) continue;
+          const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
+          g[D.oB0 + co] += dv;
+          for (int t = 0; t < 27; ++t) g[D.oW0 + co * 27 + t] += X(xx + t % 3, yy + (t / 3) % 3, zz + t / 9) * dv;
+        }
+    }
+#pragma omp critical(orc_cnn)
+    {
+      L += l;
+      for (size_t i = 0; i < g.size(); ++i) G[i] += g[i];
     }
   }
+  if (grad)
+    for (int i = 0; i < D.n; ++i) grad[i] = G[i];
+  if (loss) *loss = L * scale;
 }

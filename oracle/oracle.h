@@ -92,10 +92,11 @@ void orc_pressure_rhs(orc_mesh* m, const double* vel, const double* pres, const 
 /* grad p update alone: vel += (-dt h^2/2 grad p + flux corr)/h^3 */
 void orc_grad_update(orc_mesh* m, double* vel, const double* pres, double dt);
 
-/* ---- learned preconditioner network: 4 conv3d 3^3 layers 1->C->C->C->1,
- * input 10^3, 'valid' conv then zero-padded 'same' layers; see oracle.cpp. ---- */
-void orc_cnn_forward(int nblk, int C, const float* w, const float* bias, const float* in,
-                     float* out, float* acts /* optional */);
+/* ---- learned preconditioner network (see oracle.cpp for the layout) ---- */
+int orc_cnn_nparam(int C);
+/* forward (out may be NULL), loss and gradient (target/grad may be NULL) */
+void orc_cnn_fwd_grad(int nblk, int C, const double* params, const float* in, const float* target,
+                      float* out, double* grad, double* loss);
 
 #ifdef __cplusplus
 }

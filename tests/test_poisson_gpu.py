@@ -61,15 +61,17 @@ def _compatible_rhs(m, seed):
 
 @pytest.mark.parametrize("name", ["tgv32", "amr2_free", "amr3_mixed", "amr3_periodic"])
 def test_solve_matches_oracle(name):
-    ctx = make_ctx(name, device=0, extra="-poissonTol 0 -poissonTolRel 1e-12")
+    # 1e-10 is well above the FP64 recurrence floor (~1e-12), so both sides
+    # stop at the same iteration and follow the same iterates up to rounding.
+    ctx = make_ctx(name, device=0, extra="-poissonTol 0 -poissonTolRel 1e-10")
     m = oracle_mesh(ctx)
     b = _compatible_rhs(m, 9)
-    x_ref, st_ref = m.bicgstab_gpu(b, tol=0.0, tol_rel=1e-12)
+    x_ref, st_ref = m.bicgstab_gpu(b, tol=0.0, tol_rel=1e-10)
     bd, xd = torch_dev(b), torch_dev(np.zeros(m.n))
     rc, st = ctx.poisson_solve_dev(bd, xd)
     x = xd.cpu().numpy()
     assert rc == 0 and st["status"] == 1
-    assert np.linalg.norm(x - x_ref) <= 1e-10 * np.linalg.norm(x_ref)
+    assert np.linalg.norm(x - x_ref) <= 1e-9 * np.linalg.norm(x_ref)
     # iteration counts agree up to the rounding-sensitive restart test
     # (rho^2 < 1e-16 |r|^2 |rhat|^2, BiCGSTAB.cu:489)
     slack = 1 if st_ref["restarts"] == 0 else max(3, st_ref["iterations"] // 10)

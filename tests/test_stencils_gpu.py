@@ -3,7 +3,9 @@
 Tolerances (FP64 both sides, different summation and fused-multiply-add order):
   * advection-diffusion, penalization: 1e-12 of max|u|;
   * pressure projection / full step (Poisson solved to 1e-11 relative on both
-    sides): 1e-10 of max|u| for velocity, 1e-9 of max|p| for pressure.
+    sides): 5e-10 of max|u| for velocity, 1e-9 of max|p| for pressure; the
+    difference left is the solves' convergence (the operators alone agree to 1e-12,
+    see the RHS and advection tests).
 """
 import numpy as np
 import pytest
@@ -101,7 +103,7 @@ def test_pressure_project_matches_oracle(name, step):
     got_v, got_p = ctx.download("vel"), ctx.download("pres")
     ref_v, ref_p, info = m.pressure_project(vel, p0, dt, step, tol=0.0, tol_rel=1e-11, **obst)
     assert info["converged"]
-    assert rel(got_v, ref_v) < 1e-10
+    assert rel(got_v, ref_v) < 5e-10
     assert np.abs(got_p - ref_p).max() < 1e-9 * np.abs(ref_p).max()
 
 
@@ -124,5 +126,29 @@ def test_tgv_steps_match_oracle():
         ref_v = m.advect_diffuse(ref_v, dt_ref, 0.01)
         ref_v, pres, info = m.pressure_project(ref_v, pres, dt_ref, step, tol=0.0, tol_rel=1e-11)
         got = ctx.download("vel")
-        assert rel(got, ref_v) < 1e-10, step
+        assert rel(got, ref_v) < 5e-10, step
     assert rel(ctx.download("pres"), pres) < 1e-9
+
+
+@pytest.mark.parametrize("step", [1, 5])
+@pytest.mark.parametrize("name", ["tgv32", "amr3_mixed", "sphere"])
+def test_pressure_rhs_matches_oracle(name, step):
+    # KernelPressureRHS + kernelUpdateTmpV (+ KernelDivPressure for step > 2)
+    # with flux correction, alone: 1e-12 of max|rhs|
+    obst = {}
+    if name == "sphere":
+        ctx, m, slot, chi_o, udef_o, kin, chi = _sphere_case()
+        obst = dict(chi=chi, slot=slot, chi_o=chi_o, udef_o=udef_o)
+    else:
+        ctx = make_ctx(name, device=0)
+        m = oracle_mesh(ctx)
+    vel = smooth_velocity(ctx)
+    xyz, _ = cell_centres(ctx)
+    p0 = 0.1 * np.sin(xyz[:, 0] * 3.0) * np.cos(xyz[:, 1] * 2.0)
+    ctx.upload("vel", vel)
+    ctx.upload("pres", p0)
+    dt = 0.2 * m.hmin / np.abs(vel).max()
+    ctx.pressure_rhs(dt, step)
+    got = ctx.download("lhs")
+    ref = m.pressure_rhs(vel, p0, dt, step, **obst)
+    assert rel(got, ref) < 1e-12
