@@ -10,6 +10,7 @@ import ctypes as C
 
 import numpy as np
 
+from . import _lib
 from ._lib import (ADV, BC, FIELD, FIELD_NCOMP, SOLVER, CupError, check, cup_config,
                    cup_solve_stats, dptr, iptr, lib)
 
@@ -115,6 +116,24 @@ class Context:
         a = np.zeros(FIELD_NCOMP[name] * self.nb * 512, np.float64)
         check(lib().cup_download_field(self._p, FIELD[name], dptr(a)), self._p)
         return a
+
+    def upload_blocks(self, name, level, index, blocks):
+        """Upload from the reference's block storage: blocks[k] holds the 512
+        cells ([iz][iy][ix]) of block (level[k], index[k]), components interleaved."""
+        arrs = [np.ascontiguousarray(b, dtype=np.float64).reshape(-1) for b in blocks]
+        lv = np.ascontiguousarray(level, np.int32)
+        ix = np.ascontiguousarray(np.asarray(index).reshape(-1), np.int32)
+        ptrs = (_lib._D * len(arrs))(*[dptr(a) for a in arrs])
+        check(lib().cup_upload_field_blocks(self._p, FIELD[name], len(arrs), iptr(lv), iptr(ix), ptrs), self._p)
+
+    def download_blocks(self, name, level, index):
+        """Download into the reference's block storage (one array per block)."""
+        lv = np.ascontiguousarray(level, np.int32)
+        ix = np.ascontiguousarray(np.asarray(index).reshape(-1), np.int32)
+        arrs = [np.zeros(512 * FIELD_NCOMP[name], np.float64) for _ in range(len(lv))]
+        ptrs = (_lib._D * len(arrs))(*[dptr(a) for a in arrs])
+        check(lib().cup_download_field_blocks(self._p, FIELD[name], len(arrs), iptr(lv), iptr(ix), ptrs), self._p)
+        return arrs
 
     def field_ptr(self, name) -> int:
         return lib().cup_field_device_ptr(self._p, FIELD[name])

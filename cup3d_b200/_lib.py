@@ -90,6 +90,8 @@ SIGNATURES = {
     "cup_get_faces": (C.c_int, [_P, _I, _I]),
     "cup_upload_field": (C.c_int, [_P, C.c_int32, _D]),
     "cup_download_field": (C.c_int, [_P, C.c_int32, _D]),
+    "cup_upload_field_blocks": (C.c_int, [_P, C.c_int32, C.c_int32, _I, _I, C.POINTER(_D)]),
+    "cup_download_field_blocks": (C.c_int, [_P, C.c_int32, C.c_int32, _I, _I, C.POINTER(_D)]),
     "cup_field_device_ptr": (C.c_void_p, [_P, C.c_int32]),
     "cup_stream": (C.c_void_p, [_P]),
     "cup_poisson_apply_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_int32]),

@@ -29,6 +29,21 @@ int ctx_fail(cup_ctx* c, int code, const std::string& msg) {
 
 size_t nbn(const cup_ctx* c) { return size_t(c->mesh.nb) * BN; }
 
+cudaError_t stream_h2d(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+  const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
+cudaError_t stream_d2h(cudaStream_t s, void* dst, const void* src, size_t bytes) {
+  const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
+cudaError_t stream_zero(cudaStream_t s, void* dst, size_t bytes) {
+  const cudaError_t e = cudaMemsetAsync(dst, 0, bytes, s);
+  return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+}
+
 // Propagates the thread-local message of a failed internal call into ctx.
 static int keep(cup_ctx* c, int rc) {
   if (rc < 0 && c) c->err = g_last_error;
@@ -44,10 +59,10 @@ static int upload_mesh(cup_ctx* c) {
   if (int rc = c->mesh_arena.alloc(&fn, 24 * size_t(m.nb))) return rc;
   if (int rc = c->mesh_arena.alloc(&ix, 3 * size_t(m.nb))) return rc;
   if (int rc = c->mesh_arena.alloc(&h, size_t(m.nb))) return rc;
-  CUP_CUDA_TRY(cudaMemcpy(fk, m.face_kind.data(), 6 * size_t(m.nb) * 4, cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(fn, m.face_nbr.data(), 24 * size_t(m.nb) * 4, cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(ix, m.index.data(), 3 * size_t(m.nb) * 4, cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(h, m.h.data(), size_t(m.nb) * 8, cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(stream_h2d(c->stream, fk, m.face_kind.data(), 6 * size_t(m.nb) * 4));
+  CUP_CUDA_TRY(stream_h2d(c->stream, fn, m.face_nbr.data(), 24 * size_t(m.nb) * 4));
+  CUP_CUDA_TRY(stream_h2d(c->stream, ix, m.index.data(), 3 * size_t(m.nb) * 4));
+  CUP_CUDA_TRY(stream_h2d(c->stream, h, m.h.data(), size_t(m.nb) * 8));
   c->dm.nb = m.nb;
   c->dm.mean_block = m.mean_block;
   c->dm.fkind = fk;
@@ -83,19 +98,20 @@ static int alloc_fields(cup_ctx* c) {
     if (int rc = A.alloc(v, n)) return rc;
   // grid: a few CTAs per SM, never more than blocks
   W.grid = std::max(1, std::min(c->mesh.nb, c->num_sms * 8));
-  if (int rc = A.alloc(&W.partial, size_t(W.grid) * 8)) return rc;
+  W.ggrid = std::max(1, std::min((c->mesh.nb + GROUPS_PER_CTA - 1) / GROUPS_PER_CTA, c->num_sms * 8));
+  if (int rc = A.alloc(&W.partial, size_t(std::max(W.grid, W.ggrid)) * 8)) return rc;
   if (int rc = A.alloc(&W.counters, 32)) return rc;
   if (int rc = A.alloc(&W.st, 1)) return rc;
   if (int rc = A.alloc(&W.st2, 1)) return rc;
-  CUP_CUDA_TRY(cudaMemset(W.counters, 0, 32 * sizeof(unsigned int)));
+  CUP_CUDA_TRY(stream_zero(c->stream, W.counters, 32 * sizeof(unsigned int)));
   for (int i = 0; i < 2; ++i) {
-    CUP_CUDA_TRY(cudaMemset(F.vel[i], 0, 3 * n * 8));
-    CUP_CUDA_TRY(cudaMemset(F.pres[i], 0, n * 8));
+    CUP_CUDA_TRY(stream_zero(c->stream, F.vel[i], 3 * n * 8));
+    CUP_CUDA_TRY(stream_zero(c->stream, F.pres[i], n * 8));
   }
-  CUP_CUDA_TRY(cudaMemset(F.tmpV, 0, 3 * n * 8));
-  CUP_CUDA_TRY(cudaMemset(F.lhs, 0, n * 8));
-  CUP_CUDA_TRY(cudaMemset(F.chi, 0, n * 8));
-  CUP_CUDA_TRY(cudaMemset(F.phi, 0, n * 8));
+  CUP_CUDA_TRY(stream_zero(c->stream, F.tmpV, 3 * n * 8));
+  CUP_CUDA_TRY(stream_zero(c->stream, F.lhs, n * 8));
+  CUP_CUDA_TRY(stream_zero(c->stream, F.chi, n * 8));
+  CUP_CUDA_TRY(stream_zero(c->stream, F.phi, n * 8));
   return 0;
 }
 
@@ -368,6 +384,69 @@ int cup_download_field(cup_ctx* c, int32_t field, double* host) {
   return 0;
 }
 
+// Reference block storage <-> SoA device field.  Block k of the caller is
+// (level[k], index[3k..3k+2]) at block_ptrs[k]: GridBlock data[iz][iy][ix] of
+// VectorElement {u[3]} or ScalarElement {s} (Definitions.h:528-539), Real =
+// double.  Every leaf must appear exactly once.
+static int blocks_transfer(cup_ctx* c, int32_t field, int32_t n, const int32_t* level, const int32_t* index,
+                           double* const* ptrs, bool upload) {
+  const char* fn = upload ? "cup_upload_field_blocks" : "cup_download_field_blocks";
+  if (!c || c->mesh.nb == 0 || c->host_only || !level || !index || !ptrs)
+    return ctx_fail(c, CUP_ERR_ARG, std::string(fn) + ": bad arguments or no mesh");
+  if (n != c->mesh.nb)
+    return ctx_fail(c, CUP_ERR_ARG, std::string(fn) + ": block count differs from the mesh");
+  int nc;
+  double* d = field_ptr(c, field, &nc);
+  if (!d) return ctx_fail(c, CUP_ERR_ARG, "unknown field id");
+  const size_t nbc = nbn(c);
+  std::vector<int32_t> slot(n);
+  std::vector<char> seen(n, 0);
+  for (int k = 0; k < n; ++k) {
+    const int b = c->mesh.find(level[k], index[3 * k], index[3 * k + 1], index[3 * k + 2]);
+    if (b < 0 || seen[b] || !ptrs[k])
+      return ctx_fail(c, CUP_ERR_ARG, std::string(fn) + ": block " + std::to_string(k) +
+                                          " is not a leaf of the mesh, repeats one, or has no data");
+    seen[b] = 1;
+    slot[k] = b;
+  }
+  std::vector<double> soa(nc * nbc);
+  cudaError_t e = cudaSuccess;
+  if (!upload) {
+    e = cudaMemcpyAsync(soa.data(), d, soa.size() * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return keep(c, set_cuda_error(e, fn, __FILE__, __LINE__));
+  }
+  for (int k = 0; k < n; ++k) {
+    double* blk = ptrs[k];
+    const size_t base = size_t(slot[k]) * BN;
+    for (int q = 0; q < nc; ++q)
+      for (int cell = 0; cell < BN; ++cell) {
+        double& s = soa[q * nbc + base + cell];
+        double& r = blk[cell * nc + q];
+        if (upload)
+          s = r;
+        else
+          r = s;
+      }
+  }
+  if (upload) {
+    e = cudaMemcpyAsync(d, soa.data(), soa.size() * 8, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return keep(c, set_cuda_error(e, fn, __FILE__, __LINE__));
+  }
+  return 0;
+}
+
+int cup_upload_field_blocks(cup_ctx* c, int32_t field, int32_t nblocks, const int32_t* level,
+                            const int32_t* index, const double* const* block_ptrs) {
+  return blocks_transfer(c, field, nblocks, level, index, const_cast<double* const*>(block_ptrs), true);
+}
+
+int cup_download_field_blocks(cup_ctx* c, int32_t field, int32_t nblocks, const int32_t* level,
+                              const int32_t* index, double* const* block_ptrs) {
+  return blocks_transfer(c, field, nblocks, level, index, block_ptrs, false);
+}
+
 void* cup_stream(cup_ctx* c) { return c ? static_cast<void*>(c->stream) : nullptr; }
 
 double* cup_field_device_ptr(cup_ctx* c, int32_t field) {
@@ -465,6 +544,8 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
 int cup_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats) {
   ProfBind pb_(c);
   if (!c || !b || !x || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve_dev: bad arguments");
+  if (reinterpret_cast<uintptr_t>(x) % 16 != 0)
+    return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve_dev: d_x must be 16-byte aligned (the solver reads it as 2-wide vectors)");
   return solve_impl(c, b, x, stats);
 }
 
@@ -531,12 +612,12 @@ static int upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const 
   if (int rc = A.alloc(&o.block_of_slot, nslots)) return keep(c, rc);
   if (int rc = A.alloc(&o.chi, size_t(nslots) * BN)) return keep(c, rc);
   if (int rc = A.alloc(&o.udef, 3 * size_t(nslots) * BN)) return keep(c, rc);
-  CUP_CUDA_TRY(cudaMemcpy(o.slot_of_block, slot.data(), m.nb * sizeof(int), cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(o.near, near.data(), m.nb * sizeof(int), cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(o.block_of_slot, blocks, nslots * sizeof(int), cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(o.chi, o.h_chi.data(), o.h_chi.size() * 8, cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(o.udef, o.h_udef.data(), o.h_udef.size() * 8, cudaMemcpyHostToDevice));
-  CUP_CUDA_TRY(cudaMemcpy(c->d_scalars + SC_KIN, o.kin, 9 * sizeof(double), cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(stream_h2d(c->stream, o.slot_of_block, slot.data(), m.nb * sizeof(int)));
+  CUP_CUDA_TRY(stream_h2d(c->stream, o.near, near.data(), m.nb * sizeof(int)));
+  CUP_CUDA_TRY(stream_h2d(c->stream, o.block_of_slot, blocks, nslots * sizeof(int)));
+  CUP_CUDA_TRY(stream_h2d(c->stream, o.chi, o.h_chi.data(), o.h_chi.size() * 8));
+  CUP_CUDA_TRY(stream_h2d(c->stream, o.udef, o.h_udef.data(), o.h_udef.size() * 8));
+  CUP_CUDA_TRY(stream_h2d(c->stream, c->d_scalars + SC_KIN, o.kin, 9 * sizeof(double)));
   return 0;
 }
 
@@ -544,7 +625,7 @@ static int install_host_obstacle(cup_ctx* c, const HostObstacle& h) {
   if (int rc = upload_obstacle(c, int(h.blocks.size()), h.blocks.data(), h.chi.data(), h.udef.data(), h.kin))
     return rc;
   if (c->host_only) return 0;
-  CUP_CUDA_TRY(cudaMemcpy(c->F.chi, h.grid_chi.data(), h.grid_chi.size() * 8, cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(stream_h2d(c->stream, c->F.chi, h.grid_chi.data(), h.grid_chi.size() * 8));
   return 0;
 }
 

@@ -101,4 +101,11 @@ struct ProfBind {
 };
 int ctx_fail(cup_ctx* c, int code, const std::string& msg);
 size_t nbn(const cup_ctx* c);
+// Host<->device copies and fills ordered on a stream, waiting for it before
+// returning.  The context stream is non-blocking, so cudaMemcpy / cudaMemset
+// on the legacy default stream are not ordered with the kernels that follow
+// on it (a pageable cudaMemcpy may return before its DMA has landed).
+cudaError_t stream_h2d(cudaStream_t s, void* dst, const void* src, size_t bytes);
+cudaError_t stream_d2h(cudaStream_t s, void* dst, const void* src, size_t bytes);
+cudaError_t stream_zero(cudaStream_t s, void* dst, size_t bytes);
 }  // namespace cup3d

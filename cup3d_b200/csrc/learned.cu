@@ -23,20 +23,20 @@ static int ensure_cnn(cup_ctx* c) {
   if (int rc = A.alloc(&S.loss, 1)) return rc;
   S.train_grid = std::max(1, c->num_sms);
   if (int rc = A.alloc(&S.gpart, size_t(S.train_grid) * (CNN_NPARAM + 1))) return rc;
-  CUP_CUDA_TRY(cudaMemset(S.adam_m, 0, CNN_NPARAM * sizeof(float)));
-  CUP_CUDA_TRY(cudaMemset(S.adam_v, 0, CNN_NPARAM * sizeof(float)));
+  CUP_CUDA_TRY(stream_zero(c->stream, S.adam_m, CNN_NPARAM * sizeof(float)));
+  CUP_CUDA_TRY(stream_zero(c->stream, S.adam_v, CNN_NPARAM * sizeof(float)));
   return 0;
 }
 
 static int set_params(cup_ctx* c, const float* p) {
   if (int rc = ensure_cnn(c)) return rc;
-  CUP_CUDA_TRY(cudaMemcpy(c->cnn.W.master, p, CNN_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+  CUP_CUDA_TRY(stream_h2d(c->stream, c->cnn.W.master, p, CNN_NPARAM * sizeof(float)));
   if (int rc = cnn_pack(c->cnn.W, c->stream)) return rc;
   CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->cnn.ready = true;
   c->cnn.adam_t = 0;
-  CUP_CUDA_TRY(cudaMemset(c->cnn.adam_m, 0, CNN_NPARAM * sizeof(float)));
-  CUP_CUDA_TRY(cudaMemset(c->cnn.adam_v, 0, CNN_NPARAM * sizeof(float)));
+  CUP_CUDA_TRY(stream_zero(c->stream, c->cnn.adam_m, CNN_NPARAM * sizeof(float)));
+  CUP_CUDA_TRY(stream_zero(c->stream, c->cnn.adam_v, CNN_NPARAM * sizeof(float)));
   return 0;
 }
 
@@ -76,7 +76,7 @@ int cup_cnn_set_params(cup_ctx* c, const float* params) {
 
 int cup_cnn_get_params(cup_ctx* c, float* params) {
   if (!c || !params || !c->cnn.W.master) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_get_params: no weights");
-  cudaError_t e = cudaMemcpy(params, c->cnn.W.master, CNN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaError_t e = stream_d2h(c->stream, params, c->cnn.W.master, CNN_NPARAM * sizeof(float));
   if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_get", __FILE__, __LINE__), cup_last_error(nullptr));
   return 0;
 }
@@ -154,7 +154,8 @@ int cup_cnn_forward_host(cup_ctx* c, const float* in, float* out, int32_t n) {
   int rc = tmp.alloc(&din, size_t(n) * 1000);
   if (!rc) rc = tmp.alloc(&dout, size_t(n) * BN);
   if (rc) return ctx_fail(c, rc, cup_last_error(nullptr));
-  cudaMemcpy(din, in, size_t(n) * 1000 * sizeof(float), cudaMemcpyHostToDevice);
+  if (cudaError_t e = stream_h2d(c->stream, din, in, size_t(n) * 1000 * sizeof(float)))
+    return ctx_fail(c, set_cuda_error(e, "cnn_forward in", __FILE__, __LINE__), cup_last_error(nullptr));
   if ((rc = cnn_forward_batch(S.W, din, dout, n, S.gpart, S.train_grid, c->stream)))
     return ctx_fail(c, rc, cup_last_error(nullptr));
   cudaError_t e = cudaMemcpyAsync(out, dout, size_t(n) * BN * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
@@ -173,11 +174,12 @@ int cup_cnn_grad_host(cup_ctx* c, const float* in, const float* target, int32_t 
   int rc = tmp.alloc(&din, size_t(n) * 1000);
   if (!rc) rc = tmp.alloc(&dt, size_t(n) * BN);
   if (rc) return ctx_fail(c, rc, cup_last_error(nullptr));
-  cudaMemcpy(din, in, size_t(n) * 1000 * sizeof(float), cudaMemcpyHostToDevice);
-  cudaMemcpy(dt, target, size_t(n) * BN * sizeof(float), cudaMemcpyHostToDevice);
+  cudaError_t e = stream_h2d(c->stream, din, in, size_t(n) * 1000 * sizeof(float));
+  if (e == cudaSuccess) e = stream_h2d(c->stream, dt, target, size_t(n) * BN * sizeof(float));
+  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_grad in", __FILE__, __LINE__), cup_last_error(nullptr));
   if ((rc = cnn_grad_batch(S.W, din, dt, n, S.gpart, S.grad, S.loss, S.train_grid, c->stream)))
     return ctx_fail(c, rc, cup_last_error(nullptr));
-  cudaError_t e = cudaMemcpyAsync(grad, S.grad, CNN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+  e = cudaMemcpyAsync(grad, S.grad, CNN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess && loss) e = cudaMemcpyAsync(loss, S.loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_grad", __FILE__, __LINE__), cup_last_error(nullptr));

@@ -19,178 +19,247 @@
 
 #include "cnn.cuh"
 #include "fd.cuh"
+#include "group.cuh"
 #include "poisson.cuh"
 #include "profiler.h"
 
 namespace cup3d {
 
+static_assert(GROUPS == GROUPS_PER_CTA, "group layout");
+
 void poisson_init_constants() { fd_init_constants(); }
 
 // ---------------------------------------------------------------------------
 // Coarse-fine interpolation of PoissonSolverExp::interpolate: the Taylor part
-// p_c + s1 D1 + s2 D2' + D2(ds1) + D2(ds2) + s1 s2 Dmixed, evaluated on one
-// coarse face layer cl[t1 + 8 t2].  Faces normal to y use ds1 = z (tan2),
-// ds2 = x (tan1); the others ds1 = tan1, ds2 = tan2 (PoissonSolverExp.h:159-371).
+// p_c + s1 D1 + s2 D2' + D2(ds1) + D2(ds2) + s1 s2 Dmixed of one face layer
+// L(u, v) at coarse face cell (u, v) (PoissonSolverExp.h:159-371, D1/D2/Dmixed
+// at :384-478).  Faces normal to y use u = tan2 (z), v = tan1 (x); the others
+// u = tan1, v = tan2.  The one-sided forms apply at u, v = 0, 4 (forward) and
+// 3, 7 (backward), so every stencil stays inside the 4x4 quarter of the face
+// that holds (u, v).  The terms are evaluated without branches: all candidate
+// forms from clamped in-quarter loads, then selects (a divergent branch per
+// case serialises a warp up to nine times).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double cf_taylor(const double* cl, int d, int c1, int c2, double sa, double sb) {
-  int u, v;
-  double su, sv;
-  if (d == 1) {
-    u = c2; v = c1; su = sb; sv = sa;
-  } else {
-    u = c1; v = c2; su = sa; sv = sb;
+struct TaylorTerms {
+  double c, d1u, d1v, d2u, d2v, dm;
+  __device__ __forceinline__ double at(double su, double sv) const {
+    return c + su * d1u + sv * d1v + d2u + d2v + su * sv * dm;
   }
-  auto L = [&](int uu, int vv) -> double { return d == 1 ? cl[vv + 8 * uu] : cl[uu + 8 * vv]; };
-  const bool bdu = (u == 7 || u == 3), fdu = (u == 0 || u == 4);
-  const bool bdv = (v == 7 || v == 3), fdv = (v == 0 || v == 4);
-  const double c = L(u, v);
-  double d1u, d1v, d2u, d2v, dm;
-  if (bdu) {
-    d1u = 1. / 8. * L(u - 2, v) - 1. / 2. * L(u - 1, v) + 3. / 8. * c;
-    d2u = 1. / 32. * L(u - 2, v) - 1. / 16. * L(u - 1, v) + 1. / 32. * c;
-  } else if (fdu) {
-    d1u = -1. / 8. * L(u + 2, v) + 1. / 2. * L(u + 1, v) - 3. / 8. * c;
-    d2u = 1. / 32. * L(u + 2, v) - 1. / 16. * L(u + 1, v) + 1. / 32. * c;
-  } else {
-    d1u = -1. / 8. * L(u - 1, v) + 1. / 8. * L(u + 1, v);
-    d2u = 1. / 32. * L(u - 1, v) + 1. / 32. * L(u + 1, v) - 1. / 16. * c;
-  }
-  if (bdv) {
-    d1v = 1. / 8. * L(u, v - 2) - 1. / 2. * L(u, v - 1) + 3. / 8. * c;
-    d2v = 1. / 32. * L(u, v - 2) - 1. / 16. * L(u, v - 1) + 1. / 32. * c;
-  } else if (fdv) {
-    d1v = -1. / 8. * L(u, v + 2) + 1. / 2. * L(u, v + 1) - 3. / 8. * c;
-    d2v = 1. / 32. * L(u, v + 2) - 1. / 16. * L(u, v + 1) + 1. / 32. * c;
-  } else {
-    d1v = -1. / 8. * L(u, v - 1) + 1. / 8. * L(u, v + 1);
-    d2v = 1. / 32. * L(u, v - 1) + 1. / 32. * L(u, v + 1) - 1. / 16. * c;
-  }
-  auto N = [&](int a, int b) { return L(u + a, v + b); };
-  if (bdu && bdv)
-    dm = 1. / 16. * (N(0, 0) + N(-1, -1) - N(-1, 0) - N(0, -1));
-  else if (fdu && bdv)
-    dm = 1. / 16. * (N(1, 0) + N(0, -1) - N(1, -1) - N(0, 0));
-  else if (bdu && fdv)
-    dm = 1. / 16. * (N(0, 1) + N(-1, 0) - N(-1, 1) - N(0, 0));
-  else if (fdu && fdv)
-    dm = 1. / 16. * (N(1, 1) + N(0, 0) - N(1, 0) - N(0, 1));
-  else if (bdu)
-    dm = 1. / 32. * (N(0, 1) + N(-1, -1) - N(0, -1) - N(-1, 1));
-  else if (fdu)
-    dm = 1. / 32. * (N(1, 1) + N(0, -1) - N(1, -1) - N(0, 1));
-  else if (bdv)
-    dm = 1. / 32. * (N(1, 0) + N(-1, -1) - N(-1, 0) - N(1, -1));
-  else if (fdv)
-    dm = 1. / 32. * (N(1, 1) + N(-1, 0) - N(-1, 1) - N(1, 0));
-  else
-    dm = 1. / 64. * (N(1, 1) + N(-1, -1) - N(1, -1) - N(-1, 1));
-  return c + su * d1u + sv * d1v + d2u + d2v + su * sv * dm;
-}
-
-// ---------------------------------------------------------------------------
-// y = A x for one mesh block.  Thread t owns cells t and t+256.  Shared:
-// lab[1000] (block + 1 ghost layer), ys[512], cl[64].
-// ---------------------------------------------------------------------------
-struct SpmvSmem {
-  double lab[1000];
-  double ys[512];
-  double cl[64];
 };
 
-__device__ __forceinline__ int lab1(int x, int y, int z) { return (x + 1) + 10 * ((y + 1) + 10 * (z + 1)); }
+__device__ __forceinline__ int quarter_clamp(int w, int o) {
+  const int lo = w & 4, t = w + o;
+  return t < lo ? lo : (t > lo + 3 ? lo + 3 : t);
+}
+
+// L(u, v): the face layer in (u, v) order
+template <class Layer>
+__device__ __forceinline__ TaylorTerms cf_terms(Layer L, int u, int v) {
+  const bool bdu = (u & 3) == 3, fdu = (u & 3) == 0;
+  const bool bdv = (v & 3) == 3, fdv = (v & 3) == 0;
+  const int um1 = quarter_clamp(u, -1), up1 = quarter_clamp(u, 1), um2 = quarter_clamp(u, -2), up2 = quarter_clamp(u, 2);
+  const int vm1 = quarter_clamp(v, -1), vp1 = quarter_clamp(v, 1), vm2 = quarter_clamp(v, -2), vp2 = quarter_clamp(v, 2);
+  TaylorTerms T;
+  const double c = L(u, v);
+  const double Lum1 = L(um1, v), Lup1 = L(up1, v), Lum2 = L(um2, v), Lup2 = L(up2, v);
+  const double Lvm1 = L(u, vm1), Lvp1 = L(u, vp1), Lvm2 = L(u, vm2), Lvp2 = L(u, vp2);
+  const double Nmm = L(um1, vm1), Npp = L(up1, vp1), Npm = L(up1, vm1), Nmp = L(um1, vp1);
+  T.c = c;
+  T.d1u = bdu ? 1. / 8. * Lum2 - 1. / 2. * Lum1 + 3. / 8. * c
+        : fdu ? -1. / 8. * Lup2 + 1. / 2. * Lup1 - 3. / 8. * c
+              : -1. / 8. * Lum1 + 1. / 8. * Lup1;
+  T.d2u = bdu ? 1. / 32. * Lum2 - 1. / 16. * Lum1 + 1. / 32. * c
+        : fdu ? 1. / 32. * Lup2 - 1. / 16. * Lup1 + 1. / 32. * c
+              : 1. / 32. * Lum1 + 1. / 32. * Lup1 - 1. / 16. * c;
+  T.d1v = bdv ? 1. / 8. * Lvm2 - 1. / 2. * Lvm1 + 3. / 8. * c
+        : fdv ? -1. / 8. * Lvp2 + 1. / 2. * Lvp1 - 3. / 8. * c
+              : -1. / 8. * Lvm1 + 1. / 8. * Lvp1;
+  T.d2v = bdv ? 1. / 32. * Lvm2 - 1. / 16. * Lvm1 + 1. / 32. * c
+        : fdv ? 1. / 32. * Lvp2 - 1. / 16. * Lvp1 + 1. / 32. * c
+              : 1. / 32. * Lvm1 + 1. / 32. * Lvp1 - 1. / 16. * c;
+  double dm;
+  if (bdu && bdv)
+    dm = 1. / 16. * (c + Nmm - Lum1 - Lvm1);
+  else if (fdu && bdv)
+    dm = 1. / 16. * (Lup1 + Lvm1 - Npm - c);
+  else if (bdu && fdv)
+    dm = 1. / 16. * (Lvp1 + Lum1 - Nmp - c);
+  else if (fdu && fdv)
+    dm = 1. / 16. * (Npp + c - Lup1 - Lvp1);
+  else if (bdu)
+    dm = 1. / 32. * (Lvp1 + Nmm - Lvm1 - Nmp);
+  else if (fdu)
+    dm = 1. / 32. * (Npp + Lvm1 - Npm - Lvp1);
+  else if (bdv)
+    dm = 1. / 32. * (Lup1 + Nmm - Lum1 - Npm);
+  else if (fdv)
+    dm = 1. / 32. * (Npp + Lum1 - Nmp - Lup1);
+  else
+    dm = 1. / 64. * (Npp + Nmm - Npm - Nmp);
+  T.dm = dm;
+  return T;
+}
+
+// Flux across coarse-fine face f into face cell (a, bb) of block b
+// (PoissonSolverExp::makeFlux, PoissonSolverExp.cpp:157-219): the fine side
+// of a coarser face (coarse layer staged in tile.cl[f]), or the four fine
+// fluxes of a finer face (Taylor terms from the block's own layer).  Reads
+// the tile after the group barrier that follows its filling.
+template <class T>
+__device__ __forceinline__ double cf_flux(const DevMesh& M, int b, const T* __restrict__ x, const GroupTile& tile,
+                                          int f, int kind, int a, int bb) {
+  const int d = f >> 1, s = f & 1;
+  auto own = [&](int cell) { return tile.v[cell >> 6][(cell >> 3) & 7][cell & 7]; };
+  const double h = M.h[b];
+  if (kind == K_COARSER) {
+    const double* cl = tile.cl[f];
+    auto L = [&](int u, int v) { return d == 1 ? cl[v + 8 * u] : cl[u + 8 * v]; };
+    const int h1 = M.index[b * 3 + tan1(d)] & 1, h2 = M.index[b * 3 + tan2(d)] & 1;
+    const int c1 = h1 * 4 + (a >> 1), c2 = h2 * 4 + (bb >> 1);
+    const double sa = (a & 1) ? 1.0 : -1.0, sb = (bb & 1) ? 1.0 : -1.0;
+    const TaylorTerms Tt = d == 1 ? cf_terms(L, c2, c1) : cf_terms(L, c1, c2);
+    const double tay = d == 1 ? Tt.at(sb, sa) : Tt.at(sa, sb);
+    const double xs = own(face_cell(d, s, 0, a, bb)), xi = own(face_cell(d, s, 1, a, bb));
+    return h * (2. / 3. * xs - 1. / 5. * xi + 8. / 15. * tay - xs);
+  }
+  auto L = [&](int u, int v) { return d == 1 ? own(face_cell(d, s, 0, v, u)) : own(face_cell(d, s, 0, u, v)); };
+  const TaylorTerms Tt = d == 1 ? cf_terms(L, bb, a) : cf_terms(L, a, bb);
+  const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
+  const double hf = M.h[ch];
+  const T* xc = x + size_t(ch) * BN;
+  double close[4], far[4];
+#pragma unroll
+  for (int q4 = 0; q4 < 4; ++q4) {
+    const int fa = 2 * (a & 3) + (q4 & 1), fb = 2 * (bb & 3) + (q4 >> 1);
+    close[q4] = double(xc[face_cell(d, 1 - s, 0, fa, fb)]);
+    far[q4] = double(xc[face_cell(d, 1 - s, 1, fa, fb)]);
+  }
+  double acc = 0.0;
+#pragma unroll
+  for (int q4 = 0; q4 < 4; ++q4) {
+    const double sa = (q4 & 1) ? 1.0 : -1.0, sb = (q4 >> 1) ? 1.0 : -1.0;
+    const double tay = d == 1 ? Tt.at(sb, sa) : Tt.at(sa, sb);
+    acc += hf * (close[q4] - (2. / 3. * close[q4] - 1. / 5. * far[q4] + 8. / 15. * tay));
+  }
+  return acc;
+}
 
 template <class T>
-__device__ void spmv_block(const DevMesh& M, int b, const T* __restrict__ x, double mean_sum,
-                           int mean_mode, SpmvSmem& sm, double out[2]) {
-  const int t = threadIdx.x;
-  const double h = M.h[b];
-  const T* xb = x + size_t(b) * BN;
-  // interior
+__device__ __forceinline__ void load_col(const T* __restrict__ v, int b, const GroupIdx& G, double c[8]) {
+  const T* p = v + size_t(b) * BN + G.gy * 8 + G.gx;
 #pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const int c = t + q * NT;
-    sm.lab[lab1(c & 7, (c >> 3) & 7, c >> 6)] = double(xb[c]);
-  }
-  // ghosts: same-level neighbour values; zero-flux elsewhere (own value)
-  for (int g = t; g < 384; g += NT) {
-    const int f = g >> 6, a = g & 7, bb = (g >> 3) & 7;
-    const int d = f >> 1, s = f & 1;
-    const int kind = M.fkind[b * 6 + f];
-    double v;
-    if (kind == K_SAME) {
-      const int nbk = M.fnbr[b * 24 + 4 * f];
-      v = double(x[size_t(nbk) * BN + face_cell(d, 1 - s, 0, a, bb)]);
-    } else {
-      v = double(xb[face_cell(d, s, 0, a, bb)]);
-    }
-    int q[3];
-    q[d] = s ? BS : -1;
-    q[tan1(d)] = a;
-    q[tan2(d)] = bb;
-    sm.lab[lab1(q[0], q[1], q[2])] = v;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    const int c = t + q * NT;
-    const int X = c & 7, Y = (c >> 3) & 7, Z = c >> 6;
-    const double* L = sm.lab;
-    sm.ys[c] = h * (L[lab1(X - 1, Y, Z)] + L[lab1(X + 1, Y, Z)] + L[lab1(X, Y - 1, Z)] +
-                    L[lab1(X, Y + 1, Z)] + L[lab1(X, Y, Z - 1)] + L[lab1(X, Y, Z + 1)] -
-                    6.0 * L[lab1(X, Y, Z)]);
-  }
-  // coarse-fine faces
-  for (int f = 0; f < 6; ++f) {
-    const int kind = M.fkind[b * 6 + f];
-    if (kind != K_COARSER && kind != K_FINER) continue;
-    const int d = f >> 1, s = f & 1;
-    const int a = t & 7, bb = (t >> 3) & 7;
-    __syncthreads();
-    if (kind == K_COARSER) {
-      const int cb = M.fnbr[b * 24 + 4 * f];
-      if (t < 64) sm.cl[t] = double(x[size_t(cb) * BN + face_cell(d, 1 - s, 0, a, bb)]);
-      __syncthreads();
-      if (t < 64) {
-        const int h1 = M.index[b * 3 + tan1(d)] & 1, h2 = M.index[b * 3 + tan2(d)] & 1;
-        const int c1 = h1 * 4 + (a >> 1), c2 = h2 * 4 + (bb >> 1);
-        const double tay = cf_taylor(sm.cl, d, c1, c2, (a & 1) ? 1.0 : -1.0, (bb & 1) ? 1.0 : -1.0);
-        const int cs = face_cell(d, s, 0, a, bb), ci = face_cell(d, s, 1, a, bb);
-        const double xs = double(xb[cs]), xi = double(xb[ci]);
-        sm.ys[cs] += h * (2. / 3. * xs - 1. / 5. * xi + 8. / 15. * tay - xs);
-      }
-    } else {
-      if (t < 64) sm.cl[t] = double(xb[face_cell(d, s, 0, a, bb)]);
-      __syncthreads();
-      if (t < 64) {
-        const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
-        const double hf = M.h[ch];
-        const T* xc = x + size_t(ch) * BN;
-        double acc = 0.0;
-#pragma unroll
-        for (int q4 = 0; q4 < 4; ++q4) {
-          const int f1 = q4 & 1, f2 = q4 >> 1;
-          const int fa = 2 * (a & 3) + f1, fb = 2 * (bb & 3) + f2;
-          const double close = double(xc[face_cell(d, 1 - s, 0, fa, fb)]);
-          const double far = double(xc[face_cell(d, 1 - s, 1, fa, fb)]);
-          const double tay = cf_taylor(sm.cl, d, a, bb, f1 ? 1.0 : -1.0, f2 ? 1.0 : -1.0);
-          acc += hf * (close - (2. / 3. * close - 1. / 5. * far + 8. / 15. * tay));
-        }
-        sm.ys[face_cell(d, s, 0, a, bb)] += acc;
-      }
-    }
-  }
-  __syncthreads();
-  if (mean_mode == 1 && b == M.mean_block && t == 0) sm.ys[0] = mean_sum;
-  if (mean_mode == 3 && b == M.mean_block && t == 0) sm.ys[0] = h * double(xb[0]);
-  __syncthreads();
-  const double h3 = h * h * h;
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    out[q] = sm.ys[t + q * NT];
-    if (mean_mode == 2) out[q] += mean_sum * h3;
-  }
-  __syncthreads();
+  for (int z = 0; z < 8; ++z) c[z] = double(p[z * 64]);
 }
+
+// y = A x on the thread's column of block b (col = x there, already loaded).
+// Same-level and boundary faces from the tile and halos; coarse-fine faces:
+// each thread computes the flux of one face cell per face, owners add them.
+// Ends with a group barrier (tile free for reuse).
+template <class T>
+__device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const T* __restrict__ x, const double col[8], double ms,
+                           int mean_mode, GroupTile& tile, const GroupIdx& G, double y[8]) {
+  const int* fk = M.fkind + b * 6;
+  const int* fn = M.fnbr + b * 24;
+  const T* xb = x + size_t(b) * BN;
+  const int cxy = G.gy * 8 + G.gx;
+  int kind[6];
+#pragma unroll
+  for (int f = 0; f < 6; ++f) kind[f] = fk[f];
+  // z halo: same-level neighbour values, zero flux (own value) otherwise
+  double zm = col[0], zp = col[7];
+  if (kind[4] == K_SAME) zm = double(x[size_t(fn[16]) * BN + 7 * 64 + cxy]);
+  if (kind[5] == K_SAME) zp = double(x[size_t(fn[20]) * BN + cxy]);
+  // x / y face halos and coarser faces' coarse layers: the thread loads
+  // face-local cell (gx, gy) of each
+  bool cf = false;
+#pragma unroll
+  for (int f = 0; f < 6; ++f) {
+    const int d = f >> 1, s = f & 1;
+    if (f < 4) {
+      double v;
+      if (kind[f] == K_SAME)
+        v = double(x[size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy)]);
+      else
+        v = double(xb[face_cell(d, s, 0, G.gx, G.gy)]);
+      tile.hal[f][G.lane] = v;
+    }
+    if (kind[f] == K_COARSER) tile.cl[f][G.lane] = double(x[size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy)]);
+    cf |= kind[f] >= K_COARSER;
+  }
+#pragma unroll
+  for (int z = 0; z < 8; ++z) tile.v[z][G.gy][G.gx] = col[z];
+  group_sync(G.g);
+  double zf0 = 0.0, zf1 = 0.0;  // z-face fluxes of the own column (cells z = 0, 7)
+  if (cf) {                      // uniform per block
+#pragma unroll 1
+    for (int f = 0; f < 6; ++f) {
+      const int kf = fk[f];
+      if (kf < K_COARSER) continue;
+      const double fl = cf_flux<T>(M, b, x, tile, f, kf, G.gx, G.gy);
+      if (f < 4)
+        tile.flx[f][G.lane] = fl;
+      else if (f == 4)
+        zf0 = fl;
+      else
+        zf1 = fl;
+    }
+    group_sync(G.g);
+  }
+  const double h = M.h[b];
+  // x/y neighbours: in the tile, or in the halo on the block's faces (one
+  // shared load per neighbour through a selected base and z stride)
+  constexpr int ZS = BS * (BS + 1);
+  const double* pxm = G.gx > 0 ? &tile.v[0][G.gy][G.gx - 1] : &tile.hal[0][G.gy];
+  const double* pxp = G.gx < 7 ? &tile.v[0][G.gy][G.gx + 1] : &tile.hal[1][G.gy];
+  const double* pym = G.gy > 0 ? &tile.v[0][G.gy - 1][G.gx] : &tile.hal[2][G.gx];
+  const double* pyp = G.gy < 7 ? &tile.v[0][G.gy + 1][G.gx] : &tile.hal[3][G.gx];
+  const int sxm = G.gx > 0 ? ZS : BS, sxp = G.gx < 7 ? ZS : BS;
+  const int sym = G.gy > 0 ? ZS : BS, syp = G.gy < 7 ? ZS : BS;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    const double xm = pxm[z * sxm], xp = pxp[z * sxp], ym = pym[z * sym], yp = pyp[z * syp];
+    const double zmv = z > 0 ? col[z - 1] : zm;
+    const double zpv = z < 7 ? col[z + 1] : zp;
+    y[z] = h * (xm + xp + ym + yp + zmv + zpv - 6.0 * col[z]);
+  }
+  if (cf) {
+    // owners add the fluxes in face order
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      if (kind[f] < K_COARSER) continue;
+      const int s = f & 1;
+      if (f >= 4) {
+        y[s ? 7 : 0] += s ? zf1 : zf0;
+      } else if (f < 2) {
+        if (G.gx == (s ? 7 : 0))
+#pragma unroll
+          for (int z = 0; z < 8; ++z) y[z] += tile.flx[f][G.gy + 8 * z];
+      } else {
+        if (G.gy == (s ? 7 : 0))
+#pragma unroll
+          for (int z = 0; z < 8; ++z) y[z] += tile.flx[f][G.gx + 8 * z];
+      }
+    }
+  }
+  if (b == M.mean_block && G.lane == 0) {
+    if (mean_mode == 1) y[0] = ms;
+    if (mean_mode == 3) y[0] = h * col[0];
+  }
+  if (mean_mode == 2) {
+    const double h3 = h * h * h;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) y[z] += ms * h3;
+  }
+  group_sync(G.g);
+}
+
+__device__ __forceinline__ void block_inverse_group(double col[8], FdTile& tile, const GroupIdx& G, double h,
+                                                    const double* inv) {
+  fd_group(col, tile, G, -1.0 / h, inv);
+  group_sync(G.g);
+}
+
+#define GROUP_BLOCKS(b) for (int b = blockIdx.x * GROUPS + G.g; b < M.nb; b += gridDim.x * GROUPS)
 
 // ---------------------------------------------------------------------------
 // Standalone kernels
@@ -215,26 +284,33 @@ __global__ void __launch_bounds__(NT) k_weighted_sum(DevMesh M, const double* __
 __global__ void __launch_bounds__(NT) k_spmv(DevMesh M, const double* __restrict__ x,
                                              double* __restrict__ y, const double* mean_sum,
                                              int mean_mode) {
-  __shared__ SpmvSmem sm;
+  __shared__ GroupTile tiles[GROUPS];
+  const GroupIdx G;
   const double ms = mean_sum ? *mean_sum : 0.0;
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    double o[2];
-    spmv_block<double>(M, b, x, ms, mean_mode, sm, o);
-    y[size_t(b) * BN + threadIdx.x] = o[0];
-    y[size_t(b) * BN + threadIdx.x + NT] = o[1];
+  GROUP_BLOCKS(b) {
+    double col[8], out[8];
+    load_col(x, b, G, col);
+    spmv_group<double>(M, b, x, col, ms, mean_mode, tiles[G.g], G, out);
+    double* yb = y + size_t(b) * BN + G.gy * 8 + G.gx;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) yb[z * 64] = out[z];
   }
 }
 
 __global__ void __launch_bounds__(NT) k_block_inverse(DevMesh M, const double* __restrict__ in,
                                                       double* __restrict__ out) {
-  __shared__ FdSmem sm;
-  fd_load_scale(sm);
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    __syncthreads();
-    for (int c = threadIdx.x; c < BN; c += NT) sm.a[c] = in[size_t(b) * BN + c];
-    __syncthreads();
-    fd_apply(sm, -1.0 / M.h[b]);
-    for (int c = threadIdx.x; c < BN; c += NT) out[size_t(b) * BN + c] = sm.a[c];
+  __shared__ FdTile tiles[GROUPS];
+  __shared__ double inv_eig[BN];
+  const GroupIdx G;
+  fd_fill_inverse_eigen(inv_eig, c_lam);
+  __syncthreads();
+  GROUP_BLOCKS(b) {
+    double col[8];
+    load_col(in, b, G, col);
+    block_inverse_group(col, tiles[G.g], G, M.h[b], inv_eig);
+    double* ob = out + size_t(b) * BN + G.gy * 8 + G.gx;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) ob[z * 64] = col[z];
   }
 }
 
@@ -265,8 +341,26 @@ struct KArgs {
 };
 
 template <class T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
+template <class T>
 __device__ __forceinline__ T* xslot(const KArgs<T>& A, int i) {
   return i == 0 ? A.xs0 : (i == 1 ? A.xs1 : A.xs2);
+}
+
+template <class T>
+__device__ __forceinline__ void store_col(T* v, int b, const GroupIdx& G, const double c[8]) {
+  T* p = v + size_t(b) * BN + G.gy * 8 + G.gx;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) p[z * 64] = T(c[z]);
 }
 
 // x0[mean row] = 0 (getVec, PoissonSolverExp.cpp:402-410) and sum(x0 h^3)
@@ -292,27 +386,29 @@ __global__ void __launch_bounds__(NT) k_bicg_prepare(KArgs<T> A) {
 // r = b - A x0, rhat = r, p = nu = 0; err_init = ||r||
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
-  __shared__ SpmvSmem sm;
+  __shared__ GroupTile tiles[GROUPS];
   __shared__ double red[64];
+  const GroupIdx G;
   const DevMesh& M = A.M;
   const double ms = A.st->mean_sum;
   double acc[1] = {0.0};
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    double o[2];
-    spmv_block<T>(M, b, A.xs0, ms, A.mean_mode, sm, o);
+  GROUP_BLOCKS(b) {
+    double col[8], y[8], bc[8];
+    load_col(A.xs0, b, G, col);
+    spmv_group<T>(M, b, A.xs0, col, ms, A.mean_mode, tiles[G.g], G, y);
+    load_col(A.b, b, G, bc);
+    if (A.zero_mean_row && b == M.mean_block && G.lane == 0) bc[0] = 0.0;
+    double r[8], zero[8];
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = threadIdx.x + q * NT;
-      const size_t i = size_t(b) * BN + c;
-      double bi = double(A.b[i]);
-      if (A.zero_mean_row && b == M.mean_block && c == 0) bi = 0.0;
-      const double ri = bi - o[q];
-      A.r[i] = T(ri);
-      A.rhat[i] = T(ri);
-      A.p[i] = T(0);
-      A.nu[i] = T(0);
-      acc[0] += ri * ri;
+    for (int z = 0; z < 8; ++z) {
+      r[z] = bc[z] - y[z];
+      zero[z] = 0.0;
+      acc[0] += r[z] * r[z];
     }
+    store_col(A.r, b, G, r);
+    store_col(A.rhat, b, G, r);
+    store_col(A.p, b, G, zero);
+    store_col(A.nu, b, G, zero);
   }
   if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
     KrylovState& S = *A.st;
@@ -350,44 +446,45 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
 //     z1 = M^-1 p; sum(z1 h^3)
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
-  __shared__ FdSmem sm;
+  __shared__ FdTile tiles[GROUPS];
   __shared__ double red[64];
   const KrylovState& S = *A.st;
   if (S.done) return;
+  __shared__ double inv_eig[BN];
+  const GroupIdx G;
+  if (!A.ext_precond) {
+    fd_fill_inverse_eigen(inv_eig, c_lam);
+    __syncthreads();
+  }
   const double beta = S.beta, omega = S.omega;
   const bool restart = S.restart_pending != 0;
   const DevMesh& M = A.M;
-  fd_load_scale(sm);
   double acc[1] = {0.0};
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    __syncthreads();
+  GROUP_BLOCKS(b) {
+    double r[8], p[8];
+    load_col(A.r, b, G, r);
+    if (restart) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = threadIdx.x + q * NT;
-      const size_t i = size_t(b) * BN + c;
-      const double ri = double(A.r[i]);
-      double pi;
-      if (restart) {
-        pi = ri;
-        A.rhat[i] = T(ri);
-      } else {
-        pi = ri + beta * (double(A.p[i]) - omega * double(A.nu[i]));
-      }
-      A.p[i] = T(pi);
-      sm.a[c] = double(T(pi));
+      for (int z = 0; z < 8; ++z) p[z] = r[z];
+      store_col(A.rhat, b, G, r);
+    } else {
+      double pp[8], nu[8];
+      load_col(A.p, b, G, pp);
+      load_col(A.nu, b, G, nu);
+#pragma unroll
+      for (int z = 0; z < 8; ++z) p[z] = double(T(r[z] + beta * (pp[z] - omega * nu[z])));
     }
-    if (A.ext_precond) continue;  // uniform; z1 comes from the external preconditioner
-    __syncthreads();
+    store_col(A.p, b, G, p);
+    if (A.ext_precond) continue;  // z1 comes from the external preconditioner
     const double h = M.h[b];
-    fd_apply(sm, -1.0 / h);
+    block_inverse_group(p, tiles[G.g], G, h, inv_eig);
     double s = 0.0;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = threadIdx.x + q * NT;
-      const T zi = T(sm.a[c]);
-      A.z1[size_t(b) * BN + c] = zi;
-      s += double(zi);
+    for (int z = 0; z < 8; ++z) {
+      p[z] = double(T(p[z]));
+      s += p[z];
     }
+    store_col(A.z1, b, G, p);
     acc[0] += s * h * h * h;
   }
   if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
@@ -404,23 +501,25 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
 // KB: nu = A z1; alpha = rho / ((rhat, nu) + eps)
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_b(KArgs<T> A) {
-  __shared__ SpmvSmem sm;
+  __shared__ GroupTile tiles[GROUPS];
   __shared__ double red[64];
   const KrylovState& S = *A.st;
   if (S.done) return;
+  const GroupIdx G;
   const DevMesh& M = A.M;
   const double ms = S.mean_sum;
   double acc[1] = {0.0};
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    double o[2];
-    spmv_block<T>(M, b, A.z1, ms, A.mean_mode, sm, o);
+  GROUP_BLOCKS(b) {
+    double col[8], y[8], rh[8];
+    load_col(A.z1, b, G, col);
+    spmv_group<T>(M, b, A.z1, col, ms, A.mean_mode, tiles[G.g], G, y);
+    load_col(A.rhat, b, G, rh);
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const size_t i = size_t(b) * BN + threadIdx.x + q * NT;
-      const T v = T(o[q]);
-      A.nu[i] = v;
-      acc[0] += double(A.rhat[i]) * double(v);
+    for (int z = 0; z < 8; ++z) {
+      y[z] = double(T(y[z]));
+      acc[0] += rh[z] * y[z];
     }
+    store_col(A.nu, b, G, y);
   }
   if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
     KrylovState& W = *A.st;
@@ -431,36 +530,36 @@ __global__ void __launch_bounds__(NT) k_bicg_b(KArgs<T> A) {
 // KC: s = r - alpha nu (in place in r); z2 = M^-1 s; sum(z2 h^3)
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
-  __shared__ FdSmem sm;
+  __shared__ FdTile tiles[GROUPS];
   __shared__ double red[64];
   const KrylovState& S = *A.st;
   if (S.done) return;
+  __shared__ double inv_eig[BN];
+  const GroupIdx G;
+  if (!A.ext_precond) {
+    fd_fill_inverse_eigen(inv_eig, c_lam);
+    __syncthreads();
+  }
   const double alpha = S.alpha;
   const DevMesh& M = A.M;
-  fd_load_scale(sm);
   double acc[1] = {0.0};
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    __syncthreads();
+  GROUP_BLOCKS(b) {
+    double r[8], nu[8];
+    load_col(A.r, b, G, r);
+    load_col(A.nu, b, G, nu);
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = threadIdx.x + q * NT;
-      const size_t i = size_t(b) * BN + c;
-      const T si = T(double(A.r[i]) - alpha * double(A.nu[i]));
-      A.r[i] = si;
-      sm.a[c] = double(si);
-    }
-    if (A.ext_precond) continue;  // uniform; z2 comes from the external preconditioner
-    __syncthreads();
+    for (int z = 0; z < 8; ++z) r[z] = double(T(r[z] - alpha * nu[z]));
+    store_col(A.r, b, G, r);
+    if (A.ext_precond) continue;  // z2 comes from the external preconditioner
     const double h = M.h[b];
-    fd_apply(sm, -1.0 / h);
+    block_inverse_group(r, tiles[G.g], G, h, inv_eig);
     double s = 0.0;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = threadIdx.x + q * NT;
-      const T zi = T(sm.a[c]);
-      A.z2[size_t(b) * BN + c] = zi;
-      s += double(zi);
+    for (int z = 0; z < 8; ++z) {
+      r[z] = double(T(r[z]));
+      s += r[z];
     }
+    store_col(A.z2, b, G, r);
     acc[0] += s * h * h * h;
   }
   if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) A.st->mean_sum = acc[0];
@@ -469,24 +568,26 @@ __global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
 // KD: t = A z2; omega = (t, s) / ((t, t) + eps)
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_d(KArgs<T> A) {
-  __shared__ SpmvSmem sm;
+  __shared__ GroupTile tiles[GROUPS];
   __shared__ double red[64];
   const KrylovState& S = *A.st;
   if (S.done) return;
+  const GroupIdx G;
   const DevMesh& M = A.M;
   const double ms = S.mean_sum;
   double acc[2] = {0.0, 0.0};
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    double o[2];
-    spmv_block<T>(M, b, A.z2, ms, A.mean_mode, sm, o);
+  GROUP_BLOCKS(b) {
+    double col[8], y[8], sv[8];
+    load_col(A.z2, b, G, col);
+    spmv_group<T>(M, b, A.z2, col, ms, A.mean_mode, tiles[G.g], G, y);
+    load_col(A.r, b, G, sv);
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const size_t i = size_t(b) * BN + threadIdx.x + q * NT;
-      const T v = T(o[q]);
-      A.t[i] = v;
-      acc[0] += double(v) * double(A.r[i]);
-      acc[1] += double(v) * double(v);
+    for (int z = 0; z < 8; ++z) {
+      y[z] = double(T(y[z]));
+      acc[0] += y[z] * sv[z];
+      acc[1] += y[z] * y[z];
     }
+    store_col(A.t, b, G, y);
   }
   if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
     KrylovState& W = *A.st;
@@ -506,13 +607,30 @@ __global__ void __launch_bounds__(NT) k_bicg_e(KArgs<T> A) {
   T* xn = xslot(A, S.nxt);
   const DevMesh& M = A.M;
   double acc[2] = {0.0, 0.0};
-  const size_t n = size_t(M.nb) * BN;
-  for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n; i += size_t(gridDim.x) * NT) {
-    xn[i] = T((double(xc[i]) + alpha * double(A.z1[i])) + omega * double(A.z2[i]));
-    const T ri = T(double(A.r[i]) - omega * double(A.t[i]));
-    A.r[i] = ri;
-    acc[0] += double(A.rhat[i]) * double(ri);
-    acc[1] += double(ri) * double(ri);
+  // two cells per thread per pass with 2-wide vector accesses (nb*512 is even
+  // and every vector starts on a 16-byte boundary)
+  using V2 = typename Vec2<T>::type;
+  const size_t n2 = size_t(M.nb) * (BN / 2);
+  const V2* xc2 = reinterpret_cast<const V2*>(xc);
+  const V2* z12 = reinterpret_cast<const V2*>(A.z1);
+  const V2* z22 = reinterpret_cast<const V2*>(A.z2);
+  const V2* t2 = reinterpret_cast<const V2*>(A.t);
+  const V2* rh2 = reinterpret_cast<const V2*>(A.rhat);
+  V2* r2 = reinterpret_cast<V2*>(A.r);
+  V2* xn2 = reinterpret_cast<V2*>(xn);
+  for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n2; i += size_t(gridDim.x) * NT) {
+    const V2 x = xc2[i], z1 = z12[i], z2 = z22[i], t = t2[i], r = r2[i], rh = rh2[i];
+    V2 xo, ro;
+    xo.x = T((double(x.x) + alpha * double(z1.x)) + omega * double(z2.x));
+    xo.y = T((double(x.y) + alpha * double(z1.y)) + omega * double(z2.y));
+    ro.x = T(double(r.x) - omega * double(t.x));
+    ro.y = T(double(r.y) - omega * double(t.y));
+    xn2[i] = xo;
+    r2[i] = ro;
+    acc[0] += double(rh.x) * double(ro.x);
+    acc[0] += double(rh.y) * double(ro.y);
+    acc[1] += double(ro.x) * double(ro.x);
+    acc[1] += double(ro.y) * double(ro.y);
   }
   if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
     KrylovState& W = *A.st;
@@ -596,21 +714,22 @@ __global__ void __launch_bounds__(NT) k_true_residual(DevMesh M, const double* _
                                                       const double* __restrict__ x, float* __restrict__ r32,
                                                       int mean_mode, int zero_mean_row, KrylovState* st,
                                                       GridReduce g) {
-  __shared__ SpmvSmem sm;
+  __shared__ GroupTile tiles[GROUPS];
   __shared__ double red[64];
+  const GroupIdx G;
   const double ms = st->mean_sum;
   double acc[1] = {0.0};
-  for (int blk = blockIdx.x; blk < M.nb; blk += gridDim.x) {
-    double o[2];
-    spmv_block<double>(M, blk, x, ms, mean_mode, sm, o);
+  GROUP_BLOCKS(blk) {
+    double col[8], y[8], bc[8];
+    load_col(x, blk, G, col);
+    spmv_group<double>(M, blk, x, col, ms, mean_mode, tiles[G.g], G, y);
+    load_col(b, blk, G, bc);
+    if (zero_mean_row && blk == M.mean_block && G.lane == 0) bc[0] = 0.0;
+    float* rb = r32 ? r32 + size_t(blk) * BN + G.gy * 8 + G.gx : nullptr;
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = threadIdx.x + q * NT;
-      const size_t i = size_t(blk) * BN + c;
-      double bi = b[i];
-      if (zero_mean_row && blk == M.mean_block && c == 0) bi = 0.0;
-      const double ri = bi - o[q];
-      if (r32) r32[i] = float(ri);
+    for (int z = 0; z < 8; ++z) {
+      const double ri = bc[z] - y[z];
+      if (rb) rb[z * 64] = float(ri);
       acc[0] += ri * ri;
     }
   }
@@ -665,7 +784,7 @@ int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_
     { ProfScope ps("weighted_sum", s); k_weighted_sum<<<W.grid, NT, 0, s>>>(M, x, g, nullptr, ms); }
     CUP_CUDA_TRY(cudaGetLastError());
   }
-  { ProfScope ps("spmv", s); k_spmv<<<W.grid, NT, 0, s>>>(M, x, y, ms, mean_mode); }
+  { ProfScope ps("spmv", s); k_spmv<<<W.ggrid, NT, 0, s>>>(M, x, y, ms, mean_mode); }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -673,7 +792,7 @@ int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_
 int launch_block_inverse(const DevMesh& M, const double* in, double* out, PoissonWork& W,
                          cudaStream_t s) {
   poisson_init_constants();
-  { ProfScope ps("block_inverse", s); k_block_inverse<<<W.grid, NT, 0, s>>>(M, in, out); }
+  { ProfScope ps("block_inverse", s); k_block_inverse<<<W.ggrid, NT, 0, s>>>(M, in, out); }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -696,19 +815,19 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   A.ext_precond = cnn ? 1 : 0;
   GridReduce gc{W.partial, W.counters + 14};
   { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); k_bicg_prepare<T><<<W.grid, NT, 0, s>>>(A); }
-  { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); k_bicg_init<T><<<W.grid, NT, 0, s>>>(A); }
+  { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); k_bicg_init<T><<<W.ggrid, NT, 0, s>>>(A); }
   CUP_CUDA_TRY(cudaGetLastError());
   const int chunk = P.check_every > 0 ? P.check_every : 8;
   for (int it = 0; it < P.max_iter; it += chunk) {
     for (int j = 0; j < chunk; ++j) {
-      { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); k_bicg_a<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); k_bicg_a<T><<<W.ggrid, NT, 0, s>>>(A); }
       if (cnn)
         if (int rc = cnn_apply<T>(M, A.p, A.z1, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
-      { ProfScope ps(f32 ? "bicg32_b_spmv_dot" : "bicg_b_spmv_dot", s); k_bicg_b<T><<<W.grid, NT, 0, s>>>(A); }
-      { ProfScope ps(f32 ? "bicg32_c_supdate_precond" : "bicg_c_supdate_precond", s); k_bicg_c<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_b_spmv_dot" : "bicg_b_spmv_dot", s); k_bicg_b<T><<<W.ggrid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_c_supdate_precond" : "bicg_c_supdate_precond", s); k_bicg_c<T><<<W.ggrid, NT, 0, s>>>(A); }
       if (cnn)
         if (int rc = cnn_apply<T>(M, A.r, A.z2, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
-      { ProfScope ps(f32 ? "bicg32_d_spmv_dots" : "bicg_d_spmv_dots", s); k_bicg_d<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_d_spmv_dots" : "bicg_d_spmv_dots", s); k_bicg_d<T><<<W.ggrid, NT, 0, s>>>(A); }
       { ProfScope ps(f32 ? "bicg32_e_xr_update_dots" : "bicg_e_xr_update_dots", s); k_bicg_e<T><<<W.grid, NT, 0, s>>>(A); }
     }
     CUP_CUDA_TRY(cudaGetLastError());
@@ -756,7 +875,7 @@ int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParam
   auto residual = [&](double* err) -> int {
     {
       ProfScope ps("refine_true_residual_fp64", s);
-      k_true_residual<<<W.grid, NT, 0, s>>>(M, b, x, W.r32, P.mean_mode, zmr, so, g);
+      k_true_residual<<<W.ggrid, NT, 0, s>>>(M, b, x, W.r32, P.mean_mode, zmr, so, g);
     }
     CUP_CUDA_TRY(cudaGetLastError());
     CUP_CUDA_TRY(cudaMemcpyAsync(err, &so->err, sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -842,7 +961,7 @@ int true_residual_norm(const DevMesh& M, const double* b, const double* x, int m
   {
     ProfScope ps("true_residual_fp64", s);
     k_weighted_sum<<<W.grid, NT, 0, s>>>(M, x, g, nullptr, &so->mean_sum);
-    k_true_residual<<<W.grid, NT, 0, s>>>(M, b, x, nullptr, mean_mode, zmr, so, g);
+    k_true_residual<<<W.ggrid, NT, 0, s>>>(M, b, x, nullptr, mean_mode, zmr, so, g);
   }
   CUP_CUDA_TRY(cudaGetLastError());
   CUP_CUDA_TRY(cudaMemcpyAsync(err_host, &so->err, sizeof(double), cudaMemcpyDeviceToHost, s));

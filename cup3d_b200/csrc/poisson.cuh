@@ -30,6 +30,10 @@ enum SolveStatus : int {
   SOLVE_STALL = 5
 };
 
+// The operator and preconditioner kernels give each mesh block a 64-thread
+// group, four groups per 256-thread CTA.
+constexpr int GROUPS_PER_CTA = 4;
+
 struct PoissonWork {
   // vectors, nb*512 each
   double *r, *rhat, *p, *nu, *t, *z1, *z2, *xs[3];
@@ -40,6 +44,7 @@ struct PoissonWork {
   double* partial;          // grid * 8
   unsigned int* counters;   // 16
   int grid;                 // CTAs for block kernels
+  int ggrid;                // CTAs for block-group kernels (4 mesh blocks per CTA pass)
 };
 
 struct SolveParams {

@@ -9,9 +9,9 @@
  * Field layout on the host side of this ABI: structure-of-arrays, component c
  * of block b, cell (ix,iy,iz) at f[c*nb*512 + b*512 + iz*64 + iy*8 + ix], blocks
  * in the order cup_get_blocks() reports (the space-filling-curve order set by
- * cup_set_mesh).  cup_*_cubism variants take the reference's block layout
- * instead (one pointer per block, VectorBlock = 512 x {u,v,w}, ScalarBlock =
- * 512 x s, [iz][iy][ix]; Definitions.h:528-539).
+ * cup_set_mesh).  cup_upload_field_blocks / cup_download_field_blocks take
+ * the reference's block storage instead (one pointer per block, VectorBlock =
+ * 512 x {u,v,w}, ScalarBlock = 512 x s, [iz][iy][ix]; Definitions.h:528-539).
  */
 #ifndef CUP3D_B200_H
 #define CUP3D_B200_H
@@ -119,6 +119,14 @@ int cup_get_faces(const cup_ctx* ctx, int32_t* kinds, int32_t* nbrs);
 /* ---- fields ---- */
 int cup_upload_field(cup_ctx* ctx, int32_t field, const double* host);
 int cup_download_field(cup_ctx* ctx, int32_t field, double* host);
+/* The same in the reference's block storage: block k is (level[k],
+ * index[3k..3k+2]) with its GridBlock data (Real = double, cells [iz][iy][ix],
+ * VectorElement {u[3]} interleaved) at block_ptrs[k], blocks in any order
+ * (e.g. the order of the reference's vInfo()).  Every leaf exactly once. */
+int cup_upload_field_blocks(cup_ctx* ctx, int32_t field, int32_t nblocks, const int32_t* level,
+                            const int32_t* index, const double* const* block_ptrs);
+int cup_download_field_blocks(cup_ctx* ctx, int32_t field, int32_t nblocks, const int32_t* level,
+                              const int32_t* index, double* const* block_ptrs);
 /* Device pointer of a field (SoA), for zero-copy use by device-resident callers. */
 double* cup_field_device_ptr(cup_ctx* ctx, int32_t field);
 /* The context's CUDA stream (cudaStream_t) on which every call enqueues its work. */
@@ -130,7 +138,8 @@ void* cup_stream(cup_ctx* ctx);
 int cup_poisson_apply_dev(cup_ctx* ctx, const double* d_x, double* d_y, int32_t mean_mode);
 /* out = (1/h) P_inv in per block (the preconditioner of BiCGSTAB.cu:526-527). */
 int cup_block_inverse_dev(cup_ctx* ctx, const double* d_in, double* d_out);
-/* Solves A x = b on device buffers; x: initial guess in, solution out. */
+/* Solves A x = b on device buffers; x: initial guess in, solution out
+ * (d_x 16-byte aligned, as cudaMalloc returns it). */
 int cup_poisson_solve_dev(cup_ctx* ctx, const double* d_b, double* d_x, cup_solve_stats* stats);
 
 /* ---- PoissonSolverBase::solve(): RHS in CUP_FIELD_LHS, guess and result in CUP_FIELD_PRES ---- */
@@ -189,6 +198,7 @@ int cup_cnn_forward_host(cup_ctx* ctx, const float* in, float* out, int32_t n);
 int cup_cnn_grad_host(cup_ctx* ctx, const float* in, const float* target, int32_t n, float* grad, float* loss);
 /* z = learned preconditioner applied to the device vector r */
 int cup_cnn_precond_dev(cup_ctx* ctx, const double* d_r, double* d_z);
+
 
 /* ---- profiling (the reference's DeviceProfiler, Utils/DeviceProfiler.cuh) ---- */
 /* Enables per-kernel CUDA-event timing (resets the counters). */

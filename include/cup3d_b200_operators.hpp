@@ -40,7 +40,7 @@ struct SimulationData {
   explicit SimulationData(const std::string& flags) {
     cup_config_default(&cfg);
     check(cup_config_parse(&cfg, flags.c_str()), nullptr);
-    static const char* names[] = {"b200", "b200_mixed", "b200_learned"};
+    static const char* names[] = {"b200", "b200_mixed", "b200_learned", "b200_learned_mixed"};
     poissonSolver = names[cfg.poisson_solver];
     ctx = cup_create(&cfg);
     if (!ctx) throw std::runtime_error(std::string("cup3d_b200: ") + cup_last_error(nullptr));

