@@ -272,6 +272,14 @@ class Context:
         check(lib().cup_cnn_forward_host(self._p, x.ctypes.data_as(fp), out.ctypes.data_as(fp), n), self._p)
         return out
 
+    def cnn_forward_noalloc(self, x, n):
+        """cnn_forward without device allocation (at most 64 samples per call)."""
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros(n * 512, np.float32)
+        fp = C.POINTER(C.c_float)
+        check(lib().cup_cnn_forward_host_noalloc(self._p, x.ctypes.data_as(fp), out.ctypes.data_as(fp), n), self._p)
+        return out
+
     def cnn_grad(self, x, target, n):
         x = np.ascontiguousarray(x, np.float32)
         t = np.ascontiguousarray(target, np.float32)

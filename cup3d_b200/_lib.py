@@ -22,6 +22,8 @@ CUP_ERR_MESH = -3
 CUP_ERR_NAN = -4
 CUP_ERR_STATE = -5
 
+CNN_FORWARD_NOALLOC_MAX = 64  # CUP_CNN_FORWARD_NOALLOC_MAX
+
 BC = {"freespace": 0, "periodic": 1, "wall": 2}
 ADV = {"upwind5": 0, "upwind3": 0, "weno5": 1}
 SOLVER = {"b200": 0, "b200_mixed": 1, "b200_learned": 2, "b200_learned_mixed": 3}
@@ -122,6 +124,7 @@ SIGNATURES = {
     "cup_cnn_grad_host": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,
                                     C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "cup_cnn_precond_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "cup_cnn_forward_host_noalloc": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32]),
     "cup_profile": (C.c_int, [_P, C.c_int32]),
     "cup_profile_read": (C.c_int, [_P, C.c_char_p, C.c_int32]),
 }

@@ -199,6 +199,25 @@ int cup_cnn_grad_host(cup_ctx* ctx, const float* in, const float* target, int32_
 /* z = learned preconditioner applied to the device vector r */
 int cup_cnn_precond_dev(cup_ctx* ctx, const double* d_r, double* d_z);
 
+/* Network forward on host arrays, as cup_cnn_forward_host, without allocating
+ * or freeing device memory.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate: cup_cnn_forward_host allocates and frees
+ * staging buffers on every call, and cudaFree waits until the whole device is
+ * idle, which stalls a solve or time step running on other streams; a caller
+ * whose device memory is owned by another allocator may have none to give.
+ * This variant stages the samples in one static device array instead, so it
+ * takes at most CUP_CNN_FORWARD_NOALLOC_MAX samples per call (387,072 bytes
+ * of staging per device) and returns CUP_ERR_ARG, with a message, for more.
+ *
+ * The staging array is shared by every context on a device within the
+ * process: concurrent calls would race on it, so the library serialises the
+ * calls with a process-wide lock and each call returns only after its
+ * outputs are on the host.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress) and keeps it; make that first call before
+ * beginning any stream capture on the device. */
+#define CUP_CNN_FORWARD_NOALLOC_MAX 64
+int cup_cnn_forward_host_noalloc(cup_ctx* ctx, const float* in, float* out, int32_t n);
 
 /* ---- profiling (the reference's DeviceProfiler, Utils/DeviceProfiler.cuh) ---- */
 /* Enables per-kernel CUDA-event timing (resets the counters). */
