@@ -36,12 +36,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-SPHERE_FLAGS = ("-bpdx 4 -bpdy 2 -bpdz 2 -levelMax 4 -extent 4 -nu 4.1666666666666667e-05 -CFL 0.3 "
-                "-lambda 1e6 -advection weno5 -uinfx -0.1 -poissonTol 1e-6 -poissonTolRel 1e-4 -rampup 100")
-SPHERE_MESH = dict(center=(1.0, 1.0, 1.0), radius=0.0625, flow_dir=-1, near_radius=2.5, wake_len=1.0,
-                   wake_radius=3.0)
-SPHERE_BODY = dict(center=(1.0, 1.0, 1.0), radius=0.0625, vel=(0.1, 0.0, 0.0))
-WORKLOAD = "sphere_re300_amr_levelmax4_weno5_fp64"
+from cup3d_b200.workloads import (SPHERE_BODY, SPHERE_FLAGS, SPHERE_MESH, SPHERE_WORKLOAD as WORKLOAD,  # noqa: E402
+                                  make_sphere_ctx, poisson_rhs)
 
 # Algorithmic bytes per cell per launch (each array read once and written once,
 # halos excluded, 8-byte reals).
@@ -121,21 +117,80 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def make_sphere_ctx(device, solver="b200"):
-    import cup3d_b200 as cup
-    cfg = cup.config(SPHERE_FLAGS + f" -poissonSolver {solver}", device=device)
-    ctx = cup.Context(cfg)
-    ctx.set_mesh_sphere_wake(**SPHERE_MESH)
-    ctx.obstacle_sphere(**SPHERE_BODY)
-    return ctx
-
-
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
         return d["hbm_gbs"], "measured"
     return 6650.0, "fallback"
+
+
+def train_learned(ctx, seeds=range(6), iters=(0, 1, 2, 3, 5, 8, 12), steps=400, batch=128):
+    """Trains the block CNN on (residual, error) pairs of plain solves of
+    seeded white-noise right-hand sides on the context's mesh."""
+    import torch
+    _, hh = ctx.cell_centres()
+    w = hh ** 3
+    level, index, _ = ctx.blocks()
+    mb = int(np.where((index == 0).all(axis=1))[0][0])
+    ctx.cnn_init(7)
+    ctx.cnn_dataset_reserve(ctx.nb * len(seeds) * len(iters))
+    for seed in seeds:
+        bh = np.random.default_rng(1000 + seed).standard_normal(len(hh))
+        b = torch.tensor(bh - np.sum(bh * w) / np.sum(w), device="cuda")
+        xs = torch.zeros_like(b)
+        ctx.set_poisson("b200", 0.0, 1e-10, 1000)
+        ctx.poisson_solve_dev(b, xs)
+        for k in iters:
+            xk = torch.zeros_like(b)
+            if k > 0:
+                ctx.set_poisson("b200", 0.0, 1e-30, k)
+                ctx.poisson_solve_dev(b, xk)
+            ax = torch.zeros_like(b)
+            ctx.poisson_apply(xk, ax)
+            r = b - ax
+            r[mb * 512] = -ax[mb * 512]  # the mean-constraint row's right-hand side is zero
+            ctx.cnn_dataset_add(r.contiguous(), (xs - xk).contiguous())
+    losses = ctx.cnn_train(steps, batch, 2e-3, 11)
+    return {"samples": ctx.cnn_dataset_size(), "steps": steps, "batch": batch,
+            "loss_first10": float(np.mean(losses[:10])), "loss_last10": float(np.mean(losses[-10:]))}
+
+
+def poisson_at_tolerance(ctx, stream, flush, reps=3):
+    """Device time of one Poisson solve to a relative residual (FP64-checked
+    true residual), plain vs mixed vs learned, on the seeded right-hand side."""
+    import torch
+    b = torch.tensor(poisson_rhs(ctx), device="cuda")
+    t0 = time.perf_counter()
+    training = train_learned(ctx)
+    torch.cuda.synchronize()
+    training["seconds"] = round(time.perf_counter() - t0, 2)
+    res = {"rhs": "PCG64(20261203) white noise + 8 Gaussian sources, h^3-weighted zero mean; x0 = 0",
+           "training": training}
+    for tol in (1e-6, 1e-10):
+        for solver in ("b200", "b200_mixed", "b200_learned", "b200_learned_mixed"):
+            runs = []
+            for _ in range(reps):
+                x = torch.zeros_like(b)
+                ctx.set_poisson(solver, 0.0, tol, 1000)
+                with torch.cuda.stream(stream):
+                    flush.fill_(1.0)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                rc, st = ctx.poisson_solve_dev(b, x)
+                e1.record(stream)
+                e1.synchronize()
+                runs.append((e0.elapsed_time(e1), rc, st))
+            runs.sort(key=lambda t: t[0])
+            ms, rc, st = runs[len(runs) // 2]
+            res[f"{solver}@{tol:g}"] = {"ms": round(ms, 3), "iterations": st["iterations"],
+                                        "true_rel": float(f"{st['true_rel']:.3e}"), "fallback": st["fallback"],
+                                        "status": st["status"], "rc": rc}
+    base = res["b200@1e-06"]["ms"]
+    res["speedup_vs_b200@1e-06"] = {k.split("@")[0]: round(base / v["ms"], 3)
+                                    for k, v in res.items() if k.endswith("@1e-06")}
+    ctx.set_poisson("b200", 1e-6, 1e-4, 1000)
+    return res
 
 
 def run_b200(args):
@@ -270,6 +325,8 @@ def run_b200(args):
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if not args.no_poisson:
+        line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ctx, args)
     if world > 1:
@@ -369,6 +426,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson-to-tolerance comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -99,6 +99,17 @@ class Context:
         check(lib().cup_get_blocks(self._p, iptr(level), iptr(index), dptr(h)), self._p)
         return level, index.reshape(nb, 3), h
 
+    def cell_centres(self):
+        """Physical cell centres (nb*512, 3) and cell sizes (nb*512,) in device block order."""
+        level, index, h = self.blocks()
+        ix = np.arange(512) % 8
+        iy = (np.arange(512) // 8) % 8
+        iz = np.arange(512) // 64
+        xyz = np.zeros((len(level), 512, 3))
+        for d, i in enumerate((ix, iy, iz)):
+            xyz[:, :, d] = (index[:, d:d + 1] * 8 + i[None, :] + 0.5) * h[:, None]
+        return xyz.reshape(-1, 3), np.repeat(h, 512)
+
     def faces(self):
         nb = self.nb
         kinds = np.zeros(6 * nb, np.int32)

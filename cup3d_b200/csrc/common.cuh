@@ -66,6 +66,14 @@ __device__ __forceinline__ void block_reduce(double (&v)[NR], double* sm /* >= 8
   __syncthreads();
 }
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialization attribute may start while the previous kernel of its
+// stream is finishing; pdl_wait() blocks until that kernel has completed and
+// its memory is visible, so everything before it must read only data the
+// previous kernel does not write.  Without the attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 struct GridReduce {
   double* partial;        // gridDim.x * 8 doubles
   unsigned int* counter;  // one per reduction site, zero between launches

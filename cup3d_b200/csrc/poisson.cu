@@ -367,6 +367,8 @@ __device__ __forceinline__ void store_col(T* v, int b, const GroupIdx& G, const 
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_prepare(KArgs<T> A) {
   __shared__ double red[64];
+  pdl_wait();
+  pdl_launch_dependents();
   const DevMesh& M = A.M;
   if (A.zero_mean_row && M.mean_block >= 0 && blockIdx.x == 0 && threadIdx.x == 0)
     A.xs0[size_t(M.mean_block) * BN] = T(0);
@@ -389,6 +391,8 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
   __shared__ GroupTile tiles[GROUPS];
   __shared__ double red[64];
   const GroupIdx G;
+  pdl_wait();
+  pdl_launch_dependents();
   const DevMesh& M = A.M;
   const double ms = A.st->mean_sum;
   double acc[1] = {0.0};
@@ -448,14 +452,16 @@ template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
   __shared__ FdTile tiles[GROUPS];
   __shared__ double red[64];
-  const KrylovState& S = *A.st;
-  if (S.done) return;
   __shared__ double inv_eig[BN];
   const GroupIdx G;
-  if (!A.ext_precond) {
+  if (!A.ext_precond) {  // independent of the previous kernel: overlaps its tail
     fd_fill_inverse_eigen(inv_eig, c_lam);
     __syncthreads();
   }
+  pdl_wait();
+  pdl_launch_dependents();
+  const KrylovState& S = *A.st;
+  if (S.done) return;
   const double beta = S.beta, omega = S.omega;
   const bool restart = S.restart_pending != 0;
   const DevMesh& M = A.M;
@@ -503,6 +509,8 @@ template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_b(KArgs<T> A) {
   __shared__ GroupTile tiles[GROUPS];
   __shared__ double red[64];
+  pdl_wait();
+  pdl_launch_dependents();
   const KrylovState& S = *A.st;
   if (S.done) return;
   const GroupIdx G;
@@ -532,14 +540,16 @@ template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
   __shared__ FdTile tiles[GROUPS];
   __shared__ double red[64];
-  const KrylovState& S = *A.st;
-  if (S.done) return;
   __shared__ double inv_eig[BN];
   const GroupIdx G;
-  if (!A.ext_precond) {
+  if (!A.ext_precond) {  // independent of the previous kernel: overlaps its tail
     fd_fill_inverse_eigen(inv_eig, c_lam);
     __syncthreads();
   }
+  pdl_wait();
+  pdl_launch_dependents();
+  const KrylovState& S = *A.st;
+  if (S.done) return;
   const double alpha = S.alpha;
   const DevMesh& M = A.M;
   double acc[1] = {0.0};
@@ -570,6 +580,8 @@ template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_d(KArgs<T> A) {
   __shared__ GroupTile tiles[GROUPS];
   __shared__ double red[64];
+  pdl_wait();
+  pdl_launch_dependents();
   const KrylovState& S = *A.st;
   if (S.done) return;
   const GroupIdx G;
@@ -600,6 +612,8 @@ __global__ void __launch_bounds__(NT) k_bicg_d(KArgs<T> A) {
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_e(KArgs<T> A) {
   __shared__ double red[64];
+  pdl_wait();
+  pdl_launch_dependents();
   const KrylovState& S = *A.st;
   if (S.done) return;
   const double alpha = S.alpha, omega = S.omega;
@@ -797,6 +811,23 @@ int launch_block_inverse(const DevMesh& M, const double* in, double* out, Poisso
   return 0;
 }
 
+// Launches a solver kernel with programmatic stream serialization: its CTAs
+// may be scheduled while the previous kernel drains and wait in pdl_wait().
+template <class T>
+static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, const KArgs<T>& A) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, A);
+}
+
 // Runs BiCGSTAB on vectors of type T; x holds x0 on entry, x_opt on exit.
 template <class T>
 static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, int zero_mean_row,
@@ -814,21 +845,21 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   KArgs<T> A = make_args<T>(M, b, x, v, W, W.st, P.mean_mode, zero_mean_row, 0);
   A.ext_precond = cnn ? 1 : 0;
   GridReduce gc{W.partial, W.counters + 14};
-  { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); k_bicg_prepare<T><<<W.grid, NT, 0, s>>>(A); }
-  { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); k_bicg_init<T><<<W.ggrid, NT, 0, s>>>(A); }
+  { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_prepare<T>, W.grid, s, A)); }
+  { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_init<T>, W.ggrid, s, A)); }
   CUP_CUDA_TRY(cudaGetLastError());
   const int chunk = P.check_every > 0 ? P.check_every : 8;
   for (int it = 0; it < P.max_iter; it += chunk) {
     for (int j = 0; j < chunk; ++j) {
-      { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); k_bicg_a<T><<<W.ggrid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_a<T>, W.ggrid, s, A)); }
       if (cnn)
         if (int rc = cnn_apply<T>(M, A.p, A.z1, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
-      { ProfScope ps(f32 ? "bicg32_b_spmv_dot" : "bicg_b_spmv_dot", s); k_bicg_b<T><<<W.ggrid, NT, 0, s>>>(A); }
-      { ProfScope ps(f32 ? "bicg32_c_supdate_precond" : "bicg_c_supdate_precond", s); k_bicg_c<T><<<W.ggrid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_b_spmv_dot" : "bicg_b_spmv_dot", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_b<T>, W.ggrid, s, A)); }
+      { ProfScope ps(f32 ? "bicg32_c_supdate_precond" : "bicg_c_supdate_precond", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_c<T>, W.ggrid, s, A)); }
       if (cnn)
         if (int rc = cnn_apply<T>(M, A.r, A.z2, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
-      { ProfScope ps(f32 ? "bicg32_d_spmv_dots" : "bicg_d_spmv_dots", s); k_bicg_d<T><<<W.ggrid, NT, 0, s>>>(A); }
-      { ProfScope ps(f32 ? "bicg32_e_xr_update_dots" : "bicg_e_xr_update_dots", s); k_bicg_e<T><<<W.grid, NT, 0, s>>>(A); }
+      { ProfScope ps(f32 ? "bicg32_d_spmv_dots" : "bicg_d_spmv_dots", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_d<T>, W.ggrid, s, A)); }
+      { ProfScope ps(f32 ? "bicg32_e_xr_update_dots" : "bicg_e_xr_update_dots", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_e<T>, W.grid, s, A)); }
     }
     CUP_CUDA_TRY(cudaGetLastError());
     CUP_CUDA_TRY(cudaMemcpyAsync(h_done, &W.st->done, sizeof(int), cudaMemcpyDeviceToHost, s));

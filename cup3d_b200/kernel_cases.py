@@ -1,0 +1,46 @@
+"""Small single-GPU cases of the hot-path kernels, for profilers.
+
+    python -m cup3d_b200.kernel_cases spmv    # one Poisson operator application (sphere mesh)
+    python -m cup3d_b200.kernel_cases solve   # 16 BiCGSTAB iterations (sphere mesh, seeded RHS)
+    python -m cup3d_b200.kernel_cases step    # 4 full time steps of the sphere workload
+
+Each case builds the sphere mesh of cup3d_b200.workloads (2340 blocks,
+1.198M cells, ~0.3 GB of device memory) and exits 0 on success.
+"""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+
+
+def main(argv):
+    import torch
+
+    from cup3d_b200.workloads import make_sphere_ctx, poisson_rhs
+    case = argv[1] if len(argv) > 1 else "solve"
+    ctx = make_sphere_ctx(0)
+    n = ctx.nb * 512
+    if case == "spmv":
+        x = torch.tensor(np.random.default_rng(1).standard_normal(n), device="cuda")
+        y = torch.empty_like(x)
+        ctx.poisson_apply(x, y, 0)
+        torch.cuda.synchronize()
+        print(f"spmv ok: {ctx.nb} blocks")
+    elif case == "solve":
+        b = torch.tensor(poisson_rhs(ctx), device="cuda")
+        x = torch.zeros_like(b)
+        ctx.set_poisson("b200", 0.0, 1e-30, 16)
+        rc, st = ctx.poisson_solve_dev(b, x)
+        print(f"solve ok: rc {rc}, {st['iterations']} iterations")
+    elif case == "step":
+        for step in range(4):
+            ctx.step(step)
+        torch.cuda.synchronize()
+        print(f"step ok: {ctx.nb} blocks")
+    else:
+        raise SystemExit(f"unknown case {case!r}: spmv | solve | step")
+
+
+if __name__ == "__main__":
+    main(sys.argv)

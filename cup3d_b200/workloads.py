@@ -1,0 +1,49 @@
+"""Named workloads of the time-step hot path, shared by bench.py and the
+kernel profiling cases.
+
+Sphere at Re=300: domain 4x2x2, 4x2x2 level-0 blocks of 8^3 cells,
+levelMax 4 (mesh frozen after refinement around the sphere and its wake:
+2340 blocks, 1.198M cells), sphere radius 0.0625 at (1,1,1) moving at +0.1
+in x with the frame following it (uinf = -0.1), nu = 0.1*0.125/300, WENO5,
+implicit penalization lambda=1e6, plain FP64 BiCGSTAB with the exact block
+preconditioner, tolerances -poissonTol 1e-6, -poissonTolRel 1e-4.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+SPHERE_FLAGS = ("-bpdx 4 -bpdy 2 -bpdz 2 -levelMax 4 -extent 4 -nu 4.1666666666666667e-05 -CFL 0.3 "
+                "-lambda 1e6 -advection weno5 -uinfx -0.1 -poissonTol 1e-6 -poissonTolRel 1e-4 -rampup 100")
+SPHERE_MESH = dict(center=(1.0, 1.0, 1.0), radius=0.0625, flow_dir=-1, near_radius=2.5, wake_len=1.0,
+                   wake_radius=3.0)
+SPHERE_BODY = dict(center=(1.0, 1.0, 1.0), radius=0.0625, vel=(0.1, 0.0, 0.0))
+SPHERE_WORKLOAD = "sphere_re300_amr_levelmax4_weno5_fp64"
+
+
+def make_sphere_ctx(device, solver="b200"):
+    """Context with the frozen sphere mesh and the sphere obstacle."""
+    import cup3d_b200 as cup
+    cfg = cup.config(SPHERE_FLAGS + f" -poissonSolver {solver}", device=device)
+    ctx = cup.Context(cfg)
+    ctx.set_mesh_sphere_wake(**SPHERE_MESH)
+    ctx.obstacle_sphere(**SPHERE_BODY)
+    return ctx
+
+
+def poisson_rhs(ctx):
+    """Seeded Poisson right-hand side on the context's mesh: N(0,1) white
+    noise per cell plus 8 Gaussian sources (centres uniform in the sphere's
+    bounding box +-0.5, widths uniform in 2-8 local cells, amplitudes
+    10 N(0,1)), made h^3-weighted zero-mean."""
+    rng = np.random.Generator(np.random.PCG64(20261203))
+    xyz, hh = ctx.cell_centres()
+    b = rng.standard_normal(len(hh))
+    c0, r = np.array(SPHERE_BODY["center"]), SPHERE_BODY["radius"]
+    lo, hi = c0 - r - 0.5, c0 + r + 0.5
+    for _ in range(8):
+        c = rng.uniform(lo, hi)
+        d2 = np.sum((xyz - c) ** 2, axis=1)
+        sigma = rng.uniform(2.0, 8.0) * hh[np.argmin(d2)]
+        b += 10.0 * rng.standard_normal() * np.exp(-d2 / (2.0 * sigma ** 2))
+    w = hh ** 3
+    return b - np.sum(b * w) / np.sum(w)
