@@ -1,0 +1,67 @@
+"""The device path (C ABI) against the committed golden fixtures
+(tests/golden/), with the tolerances of the oracle parity tests."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from tests.meshes import make_ctx
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+CASES = ["tgv32", "amr2_free", "amr3_mixed", "amr3_periodic"]
+
+
+def torch_dev(a):
+    import torch
+    return torch.tensor(np.asarray(a, np.float64), device="cuda")
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_device_operator_and_block_inverse_match_golden(name):
+    g = np.load(GOLDEN / f"poisson_{name}.npz")
+    ctx = make_ctx(name, device=0)
+    n = ctx.nb * 512
+    x = np.random.default_rng(42).standard_normal(n)
+    xd, yd, zd = torch_dev(x), torch_dev(np.zeros(n)), torch_dev(np.zeros(n))
+    ctx.poisson_apply(xd, yd, 1)
+    ctx.block_inverse(xd, zd)
+    idx = g["idx"]
+    y, z = yd.cpu().numpy(), zd.cpu().numpy()
+    assert np.abs(y[idx] - g["y"]).max() <= 1e-13 * np.abs(g["y"]).max()
+    assert abs(np.linalg.norm(y) - g["y_norm"]) <= 1e-12 * g["y_norm"]
+    assert np.abs(z[idx] - g["z"]).max() <= 1e-13 * np.abs(g["z"]).max()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_device_solve_matches_golden(name):
+    g = np.load(GOLDEN / f"poisson_{name}.npz")
+    ctx = make_ctx(name, device=0, extra="-poissonTol 0 -poissonTolRel 1e-10")
+    _, _, h = ctx.blocks()
+    hh = np.repeat(h, 512)
+    b = np.random.default_rng(9).standard_normal(len(hh))
+    b -= np.sum(b * hh ** 3) / np.sum(hh ** 3)
+    bd, xd = torch_dev(b), torch_dev(np.zeros(len(hh)))
+    rc, st = ctx.poisson_solve_dev(bd, xd)
+    assert rc == 0 and st["status"] == 1
+    x = xd.cpu().numpy()
+    assert np.abs(x[g["idx"]] - g["x"]).max() <= 1e-8 * np.abs(g["x"]).max()
+    it = int(g["solve_iterations"])
+    slack = max(3, it // 10) if int(g["solve_restarts"]) == 0 else max(3, it // 4)
+    assert abs(st["iterations"] - it) <= slack
+
+
+def test_device_tgv_steps_match_golden():
+    g = np.load(GOLDEN / "tgv32_steps.npz")
+    ctx = make_ctx("tgv32", device=0, extra="-nu 0.01 -CFL 0.3 -rampup 0 -poissonTol 0 -poissonTolRel 1e-11")
+    xyz, _ = ctx.cell_centres()
+    x, y, z = xyz.T
+    ctx.upload("vel", np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), 0 * x]))
+    idx = g["idx"]
+    for step in range(4):
+        dt, rc, st = ctx.step(step)
+        assert rc == 0
+        assert abs(dt - float(g[f"dt{step}"])) <= 1e-12 * dt
+        vel = ctx.download("vel")
+        assert np.abs(vel[idx] - g[f"vel{step}"]).max() <= 5e-10 * np.abs(g[f"vel{step}"]).max(), step
