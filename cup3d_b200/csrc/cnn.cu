@@ -417,9 +417,9 @@ __device__ void load_train_weights(TrainSmem& S, const CnnWeights& W) {
 // loss partial (sum of squared errors) into lpart[blockIdx].  out (optional):
 // network outputs of the samples.
 __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* __restrict__ in,
-                                                     const float* __restrict__ target, const int* __restrict__ idx,
-                                                     int n, float grad_scale, float* gpart, float* lpart,
-                                                     float* out, int backward) {
+                                                     const float* __restrict__ target, float tscale,
+                                                     const int* __restrict__ idx, int n, float grad_scale,
+                                                     float* gpart, float* lpart, float* out, int backward) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
   load_train_weights(S, W);
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* 
     __syncthreads();
     // dL/dz = grad_scale * 2 (z - t); loss += (z - t)^2
     for (int c = threadIdx.x; c < BN; c += NT) {
-      const float e = S.z[c] - (target ? target[size_t(smp) * BN + c] : 0.f);
+      const float e = S.z[c] - (target ? tscale * target[size_t(smp) * BN + c] : 0.f);
       if (out) out[size_t(sidx) * BN + c] = S.z[c];
       loss += e * e;
       S.z[c] = grad_scale * 2.f * e;
@@ -559,8 +559,8 @@ __global__ void k_adam(float* w, const float* g, float* m, float* v, int t, floa
 }
 
 // gpart: >= grid*(CNN_NPARAM+1) floats (gradient rows, then one loss partial per CTA)
-static int train_launch(const CnnWeights& W, const float* in, const float* target, const int* idx, int n,
-                        float* gpart, float* grad, float* loss_dev, float* out, int backward, int grid,
+static int train_launch(const CnnWeights& W, const float* in, const float* target, float tscale, const int* idx,
+                        int n, float* gpart, float* grad, float* loss_dev, float* out, int backward, int grid,
                         cudaStream_t s) {
   const size_t smem = sizeof(TrainSmem);
   static bool attr = false;
@@ -574,7 +574,7 @@ static int train_launch(const CnnWeights& W, const float* in, const float* targe
   float* lpart = gpart + size_t(g) * CNN_NPARAM;
   {
     ProfScope ps(backward ? "cnn_train_fwd_bwd" : "cnn_forward_batch", s);
-    k_cnn_train<<<g, NT, smem, s>>>(W, in, target, idx, n, scale, gpart, lpart, out, backward);
+    k_cnn_train<<<g, NT, smem, s>>>(W, in, target, tscale, idx, n, scale, gpart, lpart, out, backward);
   }
   CUP_CUDA_TRY(cudaGetLastError());
   if (backward || loss_dev) {
@@ -587,18 +587,19 @@ static int train_launch(const CnnWeights& W, const float* in, const float* targe
 
 int cnn_forward_batch(const CnnWeights& W, const float* in, float* out, int n, float* gpart, int grid,
                       cudaStream_t s) {
-  return train_launch(W, in, nullptr, nullptr, n, gpart, nullptr, nullptr, out, 0, grid, s);
+  return train_launch(W, in, nullptr, 1.0f, nullptr, n, gpart, nullptr, nullptr, out, 0, grid, s);
 }
 
 int cnn_grad_batch(const CnnWeights& W, const float* in, const float* target, int n, float* gpart, float* grad,
                    float* loss_dev, int grid, cudaStream_t s) {
-  return train_launch(W, in, target, nullptr, n, gpart, grad, loss_dev, nullptr, 1, grid, s);
+  return train_launch(W, in, target, 1.0f, nullptr, n, gpart, grad, loss_dev, nullptr, 1, grid, s);
 }
 
 int cnn_train_step(const CnnWeights& W, float* adam_m, float* adam_v, int t, float lr, const float* in,
-                   const float* target, const int* idx, int batch, float* gpart, float* grad, float* loss_dev,
-                   int grid, cudaStream_t s) {
-  if (int rc = train_launch(W, in, target, idx, batch, gpart, grad, loss_dev, nullptr, 1, grid, s)) return rc;
+                   const float* target, float target_scale, const int* idx, int batch, float* gpart, float* grad,
+                   float* loss_dev, int grid, cudaStream_t s) {
+  if (int rc = train_launch(W, in, target, target_scale, idx, batch, gpart, grad, loss_dev, nullptr, 1, grid, s))
+    return rc;
   k_adam<<<(CNN_NPARAM + 255) / 256, 256, 0, s>>>(W.master, grad, adam_m, adam_v, t, lr);
   CUP_CUDA_TRY(cudaGetLastError());
   return cnn_pack(W, s);

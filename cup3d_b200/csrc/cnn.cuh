@@ -58,11 +58,12 @@ int cnn_dataset_add(const DevMesh& M, const double* r, const double* e, float* i
 
 // Training on a device dataset of n samples: in[n*1000], target[n*512]
 // (targets already divided by the sample's scale/h).  One Adam step over a
-// minibatch of `batch` sample indices idx[batch]; loss (mean squared error)
-// into *loss_dev.  grad_partial: grid*(CNN_NPARAM+1) floats of scratch.
+// minibatch of `batch` sample indices idx[batch]; the targets are read
+// multiplied by target_scale; loss (mean squared error) into *loss_dev.
+// grad_partial: grid*(CNN_NPARAM+1) floats of scratch.
 int cnn_train_step(const CnnWeights& W, float* adam_m, float* adam_v, int t, float lr, const float* in,
-                   const float* target, const int* idx, int batch, float* grad_partial, float* grad, float* loss_dev,
-                   int grid, cudaStream_t s);
+                   const float* target, float target_scale, const int* idx, int batch, float* grad_partial,
+                   float* grad, float* loss_dev, int grid, cudaStream_t s);
 
 // Forward and gradient (no update) on a batch, for checks against the oracle.
 // gpart: >= grid*(CNN_NPARAM+1) floats of scratch.

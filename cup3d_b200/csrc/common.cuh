@@ -74,6 +74,14 @@ __device__ __forceinline__ void block_reduce(double (&v)[NR], double* sm /* >= 8
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+// Load through L2 only (ld.global.cg).  Kernels whose CTAs read data that
+// other CTAs of the same launch wrote (after a grid barrier) use it, since
+// L1 is not coherent across SMs.
+template <class V>
+__device__ __forceinline__ V ld_stream(const V* p) {
+  return __ldcg(p);
+}
+
 struct GridReduce {
   double* partial;        // gridDim.x * 8 doubles
   unsigned int* counter;  // one per reduction site, zero between launches
@@ -133,14 +141,88 @@ __device__ __forceinline__ bool grid_reduce_max(double& v, const GridReduce& g, 
   __syncthreads();
   if (s_ticket_m != gridDim.x - 1) return false;
   __threadfence();
+  // the last CTA takes the maximum over all partials with all its threads
+  double m = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) m = fmax(m, __ldcg(&g.partial[i * 8]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (l == 0) sm[w] = m;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    double m = 0.0;
-    for (int i = 0; i < (int)gridDim.x; ++i) m = fmax(m, __ldcg(&g.partial[i * 8]));
-    s_max = m;
+    double mm = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) mm = fmax(mm, sm[i]);
+    s_max = mm;
     *g.counter = 0u;
   }
   __syncthreads();
   v = s_max;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Grid-wide barrier with a reduction, for cooperative (co-resident) launches.
+// Each CTA writes its NR partial sums; the last CTA to arrive sums them in
+// CTA order (deterministic), publishes the totals and releases the others,
+// which spin on a generation counter with a bounded wait: after
+// kBarrierSpinLimit polls (well over a second) a waiter sets *error and
+// returns false, so a barrier that can never complete ends the kernel
+// instead of hanging the device.
+// ---------------------------------------------------------------------------
+struct GridSync {
+  unsigned int* arrive;  // arrivals in the current barrier (0 between barriers)
+  unsigned int* gen;     // barrier generation
+  double* partial;       // gridDim.x * 8
+  double* totals;        // 8
+  int* error;            // set on a timed-out wait
+};
+
+constexpr long long kBarrierSpinLimit = 1ll << 24;
+
+template <int NR>
+__device__ bool grid_allreduce(double (&v)[NR], const GridSync& G, double* sm) {
+  block_reduce<NR>(v, sm);  // ends with __syncthreads: the CTA's writes precede the arrival
+  __shared__ unsigned int s_last, s_gen;
+  __shared__ int s_ok;
+  if (threadIdx.x == 0) {
+    s_gen = *reinterpret_cast<volatile unsigned int*>(G.gen);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) G.partial[blockIdx.x * 8 + r] = v[r];
+    __threadfence();
+    s_last = atomicAdd(G.arrive, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+#pragma unroll
+      for (int r = 0; r < NR; ++r) acc[r] += __ldcg(&G.partial[i * 8 + r]);
+    block_reduce<NR>(acc, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) G.totals[r] = acc[r];
+      *G.arrive = 0u;
+      __threadfence();
+      atomicAdd(G.gen, 1u);
+      s_ok = 1;
+    }
+  } else if (threadIdx.x == 0) {
+    volatile unsigned int* gen = G.gen;
+    long long spins = 0;
+    while (*gen == s_gen && spins < kBarrierSpinLimit) {
+      __nanosleep(32);
+      ++spins;
+    }
+    s_ok = *gen != s_gen;
+    if (!s_ok) atomicExch(G.error, 1);
+    __threadfence();
+  }
+  __syncthreads();
+  if (!s_ok) return false;
+#pragma unroll
+  for (int r = 0; r < NR; ++r) v[r] = __ldcg(&G.totals[r]);
   return true;
 }
 
@@ -154,4 +236,6 @@ __device__ __forceinline__ bool grid_reduce_max(double& v, const GridReduce& g, 
 
 namespace cup3d {
 int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+// Records a message for cup_last_error() and returns code.
+int set_error(int code, const char* msg);
 }

@@ -21,6 +21,11 @@ int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) 
   return CUP_ERR_CUDA;
 }
 
+int set_error(int code, const char* msg) {
+  g_last_error = msg;
+  return code;
+}
+
 int ctx_fail(cup_ctx* c, int code, const std::string& msg) {
   g_last_error = msg;
   if (c) c->err = msg;
@@ -101,9 +106,14 @@ static int alloc_fields(cup_ctx* c) {
   W.ggrid = std::max(1, std::min((c->mesh.nb + GROUPS_PER_CTA - 1) / GROUPS_PER_CTA, c->num_sms * 8));
   if (int rc = A.alloc(&W.partial, size_t(std::max(W.grid, W.ggrid)) * 8)) return rc;
   if (int rc = A.alloc(&W.counters, 32)) return rc;
+  if (int rc = A.alloc(&W.bar, 2)) return rc;
+  if (int rc = A.alloc(&W.bar_totals, 8)) return rc;
+  if (int rc = A.alloc(&W.bar_error, 1)) return rc;
   if (int rc = A.alloc(&W.st, 1)) return rc;
   if (int rc = A.alloc(&W.st2, 1)) return rc;
   CUP_CUDA_TRY(stream_zero(c->stream, W.counters, 32 * sizeof(unsigned int)));
+  CUP_CUDA_TRY(stream_zero(c->stream, W.bar, 2 * sizeof(unsigned int)));
+  CUP_CUDA_TRY(stream_zero(c->stream, W.bar_error, sizeof(int)));
   for (int i = 0; i < 2; ++i) {
     CUP_CUDA_TRY(stream_zero(c->stream, F.vel[i], 3 * n * 8));
     CUP_CUDA_TRY(stream_zero(c->stream, F.pres[i], n * 8));
@@ -486,6 +496,7 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   P.mean_mode = c->cfg.mean_constraint;
   P.check_every = 8;
   P.stall_window = 0;
+  P.persistent = 1;
   SolveStats S{};
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   int rc = 0;

@@ -58,7 +58,7 @@ struct CnnState {
 };
 
 // Offsets into cup_ctx::d_scalars
-enum : int { SC_SUMS = 0, SC_UMAX = 2, SC_FORCE = 8, SC_KIN = 16 };
+enum : int { SC_SUMS = 0, SC_UMAX = 2, SC_FORCE = 8, SC_KIN = 16, SC_TARGET_SUMSQ = 32 };
 
 struct Fields {
   double* vel[2] = {nullptr, nullptr};  // ping-pong, 3*nb*512 each

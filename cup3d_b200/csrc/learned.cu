@@ -28,6 +28,43 @@ static int ensure_cnn(cup_ctx* c) {
   return 0;
 }
 
+// sum of squares of v[0..n) into *out (deterministic grid reduction)
+__global__ void __launch_bounds__(NT) k_sumsq(const float* __restrict__ v, size_t n, GridReduce g, double* out) {
+  __shared__ double red[64];
+  double acc[1] = {0.0};
+  for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n; i += size_t(gridDim.x) * NT) {
+    const double x = v[i];
+    acc[0] += x * x;
+  }
+  if (grid_reduce<1>(acc, g, red) && threadIdx.x == 0) *out = acc[0];
+}
+
+__global__ void k_scale(float* v, size_t n, float s) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) v[i] *= s;
+}
+
+// RMS of the stored training targets.
+static int target_rms(cup_ctx* c, double* rms) {
+  CnnState& S = c->cnn;
+  const size_t n = size_t(S.count) * BN;
+  GridReduce g{c->W.partial, c->W.counters + 16};
+  double* d = c->d_scalars + SC_TARGET_SUMSQ;
+  k_sumsq<<<c->W.grid, NT, 0, c->stream>>>(S.ds_target, n, g, d);
+  CUP_CUDA_TRY(cudaGetLastError());
+  double ss = 0.0;
+  CUP_CUDA_TRY(stream_d2h(c->stream, &ss, d, sizeof(double)));
+  *rms = std::sqrt(ss / double(std::max<size_t>(n, 1)));
+  return 0;
+}
+
+// Scales the output layer (W3, b3) by s.  The output layer is linear, so the
+// network's outputs scale by s as well.
+static int scale_output_layer(cup_ctx* c, float s) {
+  k_scale<<<2, NT, 0, c->stream>>>(c->cnn.W.master + OFF_W3, size_t(CNN_W3 + CNN_B3), s);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 static int set_params(cup_ctx* c, const float* p) {
   if (int rc = ensure_cnn(c)) return rc;
   CUP_CUDA_TRY(stream_h2d(c->stream, c->cnn.W.master, p, CNN_NPARAM * sizeof(float)));
@@ -123,25 +160,45 @@ int cup_cnn_train(cup_ctx* c, int32_t steps, int32_t batch, float lr, uint64_t s
     S.idx = p;
     S.idx_cap = batch;
   }
+  // Train in normalised units: targets read divided by their RMS and the
+  // output layer expressed in the same units during the steps, then scaled
+  // back, so the stored network keeps predicting raw targets.  The reported
+  // losses are relative to the targets' mean square.
+  double rms = 0.0;
+  if (int rc = target_rms(c, &rms)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  if (!(rms > 0.0)) rms = 1.0;
+  if (int rc = scale_output_layer(c, float(1.0 / rms))) return ctx_fail(c, rc, cup_last_error(nullptr));
+  int train_rc = 0;
   std::mt19937_64 g(seed);
   std::uniform_int_distribution<int> pick(0, S.count - 1);
   std::vector<int> idx(batch);
-  for (int it = 0; it < steps; ++it) {
+  for (int it = 0; it < steps && !train_rc; ++it) {
     for (int i = 0; i < batch; ++i) idx[i] = pick(g);
     cudaError_t e = cudaMemcpyAsync(S.idx, idx.data(), batch * sizeof(int), cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "train idx", __FILE__, __LINE__), cup_last_error(nullptr));
+    if (e != cudaSuccess) {
+      train_rc = set_cuda_error(e, "train idx", __FILE__, __LINE__);
+      break;
+    }
     S.adam_t += 1;
-    if (int rc = cnn_train_step(S.W, S.adam_m, S.adam_v, S.adam_t, lr, S.ds_in, S.ds_target, S.idx, batch, S.gpart,
-                                S.grad, S.loss, S.train_grid, c->stream))
-      return ctx_fail(c, rc, cup_last_error(nullptr));
+    if ((train_rc = cnn_train_step(S.W, S.adam_m, S.adam_v, S.adam_t, lr, S.ds_in, S.ds_target, float(1.0 / rms),
+                                   S.idx, batch, S.gpart, S.grad, S.loss, S.train_grid, c->stream)))
+      break;
     if (loss_out) {
       e = cudaMemcpyAsync(&loss_out[it], S.loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream);
-      if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "train loss", __FILE__, __LINE__), cup_last_error(nullptr));
+      if (e != cudaSuccess) {
+        train_rc = set_cuda_error(e, "train loss", __FILE__, __LINE__);
+        break;
+      }
     }
     // the host index buffer is reused next iteration: wait for its copy
     e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "train", __FILE__, __LINE__), cup_last_error(nullptr));
+    if (e != cudaSuccess) train_rc = set_cuda_error(e, "train", __FILE__, __LINE__);
   }
+  const int back_rc = scale_output_layer(c, float(rms));
+  if (train_rc || back_rc) return ctx_fail(c, train_rc ? train_rc : back_rc, cup_last_error(nullptr));
+  if (int rc = cnn_pack(S.W, c->stream)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  if (cudaError_t e = cudaStreamSynchronize(c->stream))
+    return ctx_fail(c, set_cuda_error(e, "train", __FILE__, __LINE__), cup_last_error(nullptr));
   return 0;
 }
 

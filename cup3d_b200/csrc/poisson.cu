@@ -22,6 +22,7 @@
 #include "group.cuh"
 #include "poisson.cuh"
 #include "profiler.h"
+#include "cup3d_b200.h"
 
 namespace cup3d {
 
@@ -100,14 +101,25 @@ __device__ __forceinline__ TaylorTerms cf_terms(Layer L, int u, int v) {
   return T;
 }
 
+// ---------------------------------------------------------------------------
+// Vector accessors for the operator: x(i) gives the input vector's value at
+// global cell index i.  VecAt reads a stored vector through L2; an accessor
+// may also combine stored vectors at the point of use.
+// ---------------------------------------------------------------------------
+template <class T>
+struct VecAt {
+  const T* v;
+  __device__ __forceinline__ double operator()(size_t i) const { return double(ld_stream(v + i)); }
+};
+
 // Flux across coarse-fine face f into face cell (a, bb) of block b
 // (PoissonSolverExp::makeFlux, PoissonSolverExp.cpp:157-219): the fine side
 // of a coarser face (coarse layer staged in tile.cl[f]), or the four fine
 // fluxes of a finer face (Taylor terms from the block's own layer).  Reads
 // the tile after the group barrier that follows its filling.
-template <class T>
-__device__ __forceinline__ double cf_flux(const DevMesh& M, int b, const T* __restrict__ x, const GroupTile& tile,
-                                          int f, int kind, int a, int bb) {
+template <class X>
+__device__ __forceinline__ double cf_flux(const DevMesh& M, int b, const X& x, const GroupTile& tile, int f,
+                                          int kind, int a, int bb) {
   const int d = f >> 1, s = f & 1;
   auto own = [&](int cell) { return tile.v[cell >> 6][(cell >> 3) & 7][cell & 7]; };
   const double h = M.h[b];
@@ -126,13 +138,13 @@ __device__ __forceinline__ double cf_flux(const DevMesh& M, int b, const T* __re
   const TaylorTerms Tt = d == 1 ? cf_terms(L, bb, a) : cf_terms(L, a, bb);
   const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
   const double hf = M.h[ch];
-  const T* xc = x + size_t(ch) * BN;
+  const size_t xc = size_t(ch) * BN;
   double close[4], far[4];
 #pragma unroll
   for (int q4 = 0; q4 < 4; ++q4) {
     const int fa = 2 * (a & 3) + (q4 & 1), fb = 2 * (bb & 3) + (q4 >> 1);
-    close[q4] = double(xc[face_cell(d, 1 - s, 0, fa, fb)]);
-    far[q4] = double(xc[face_cell(d, 1 - s, 1, fa, fb)]);
+    close[q4] = x(xc + face_cell(d, 1 - s, 0, fa, fb));
+    far[q4] = x(xc + face_cell(d, 1 - s, 1, fa, fb));
   }
   double acc = 0.0;
 #pragma unroll
@@ -148,42 +160,36 @@ template <class T>
 __device__ __forceinline__ void load_col(const T* __restrict__ v, int b, const GroupIdx& G, double c[8]) {
   const T* p = v + size_t(b) * BN + G.gy * 8 + G.gx;
 #pragma unroll
-  for (int z = 0; z < 8; ++z) c[z] = double(p[z * 64]);
+  for (int z = 0; z < 8; ++z) c[z] = double(ld_stream(p + z * 64));
 }
 
 // y = A x on the thread's column of block b (col = x there, already loaded).
 // Same-level and boundary faces from the tile and halos; coarse-fine faces:
 // each thread computes the flux of one face cell per face, owners add them.
 // Ends with a group barrier (tile free for reuse).
-template <class T>
-__device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const T* __restrict__ x, const double col[8], double ms,
-                           int mean_mode, GroupTile& tile, const GroupIdx& G, double y[8]) {
+template <class X>
+__device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const X& x, const double col[8], double ms,
+                                           int mean_mode, GroupTile& tile, const GroupIdx& G, double y[8]) {
   const int* fk = M.fkind + b * 6;
   const int* fn = M.fnbr + b * 24;
-  const T* xb = x + size_t(b) * BN;
   const int cxy = G.gy * 8 + G.gx;
   int kind[6];
 #pragma unroll
   for (int f = 0; f < 6; ++f) kind[f] = fk[f];
   // z halo: same-level neighbour values, zero flux (own value) otherwise
   double zm = col[0], zp = col[7];
-  if (kind[4] == K_SAME) zm = double(x[size_t(fn[16]) * BN + 7 * 64 + cxy]);
-  if (kind[5] == K_SAME) zp = double(x[size_t(fn[20]) * BN + cxy]);
+  if (kind[4] == K_SAME) zm = x(size_t(fn[16]) * BN + 7 * 64 + cxy);
+  if (kind[5] == K_SAME) zp = x(size_t(fn[20]) * BN + cxy);
   // x / y face halos and coarser faces' coarse layers: the thread loads
   // face-local cell (gx, gy) of each
   bool cf = false;
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     const int d = f >> 1, s = f & 1;
-    if (f < 4) {
-      double v;
-      if (kind[f] == K_SAME)
-        v = double(x[size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy)]);
-      else
-        v = double(xb[face_cell(d, s, 0, G.gx, G.gy)]);
-      tile.hal[f][G.lane] = v;
-    }
-    if (kind[f] == K_COARSER) tile.cl[f][G.lane] = double(x[size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy)]);
+    if (f < 4 && kind[f] == K_SAME)
+      tile.hal[f][G.lane] = x(size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy));
+    if (kind[f] == K_COARSER)
+      tile.cl[f][G.lane] = x(size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy));
     cf |= kind[f] >= K_COARSER;
   }
 #pragma unroll
@@ -195,7 +201,7 @@ __device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const T* __r
     for (int f = 0; f < 6; ++f) {
       const int kf = fk[f];
       if (kf < K_COARSER) continue;
-      const double fl = cf_flux<T>(M, b, x, tile, f, kf, G.gx, G.gy);
+      const double fl = cf_flux(M, b, x, tile, f, kf, G.gx, G.gy);
       if (f < 4)
         tile.flx[f][G.lane] = fl;
       else if (f == 4)
@@ -215,9 +221,14 @@ __device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const T* __r
   const double* pyp = G.gy < 7 ? &tile.v[0][G.gy + 1][G.gx] : &tile.hal[3][G.gx];
   const int sxm = G.gx > 0 ? ZS : BS, sxp = G.gx < 7 ? ZS : BS;
   const int sym = G.gy > 0 ? ZS : BS, syp = G.gy < 7 ? ZS : BS;
+  // on a face that is not same-level the ghost is the cell itself (zero
+  // flux; coarse-fine faces get their flux below): the thread's own column
+  const bool oxm = G.gx == 0 && kind[0] != K_SAME, oxp = G.gx == 7 && kind[1] != K_SAME;
+  const bool oym = G.gy == 0 && kind[2] != K_SAME, oyp = G.gy == 7 && kind[3] != K_SAME;
 #pragma unroll
   for (int z = 0; z < 8; ++z) {
-    const double xm = pxm[z * sxm], xp = pxp[z * sxp], ym = pym[z * sym], yp = pyp[z * syp];
+    const double xm = oxm ? col[z] : pxm[z * sxm], xp = oxp ? col[z] : pxp[z * sxp];
+    const double ym = oym ? col[z] : pym[z * sym], yp = oyp ? col[z] : pyp[z * syp];
     const double zmv = z > 0 ? col[z - 1] : zm;
     const double zpv = z < 7 ? col[z + 1] : zp;
     y[z] = h * (xm + xp + ym + yp + zmv + zpv - 6.0 * col[z]);
@@ -290,7 +301,7 @@ __global__ void __launch_bounds__(NT) k_spmv(DevMesh M, const double* __restrict
   GROUP_BLOCKS(b) {
     double col[8], out[8];
     load_col(x, b, G, col);
-    spmv_group<double>(M, b, x, col, ms, mean_mode, tiles[G.g], G, out);
+    spmv_group(M, b, VecAt<double>{x}, col, ms, mean_mode, tiles[G.g], G, out);
     double* yb = y + size_t(b) * BN + G.gy * 8 + G.gx;
 #pragma unroll
     for (int z = 0; z < 8; ++z) yb[z * 64] = out[z];
@@ -399,7 +410,7 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
   GROUP_BLOCKS(b) {
     double col[8], y[8], bc[8];
     load_col(A.xs0, b, G, col);
-    spmv_group<T>(M, b, A.xs0, col, ms, A.mean_mode, tiles[G.g], G, y);
+    spmv_group(M, b, VecAt<T>{A.xs0}, col, ms, A.mean_mode, tiles[G.g], G, y);
     load_col(A.b, b, G, bc);
     if (A.zero_mean_row && b == M.mean_block && G.lane == 0) bc[0] = 0.0;
     double r[8], zero[8];
@@ -446,26 +457,22 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
   }
 }
 
-// KA: p = r + beta (p - omega nu) (or p = r, rhat = r after a restart);
-//     z1 = M^-1 p; sum(z1 h^3)
+// ---------------------------------------------------------------------------
+// The five phases of one BiCGSTAB iteration (BiCGSTAB.cu:416-628).  Each body
+// is one pass of the CTA over its blocks (or cells) and returns the CTA's
+// partial sums; each finalizer turns the grid totals into the scalars of the
+// next phase.  The per-phase kernels run one body per launch with a last-CTA
+// finalizer (the flexible solver of the learned preconditioner, whose network
+// runs between phases); the finalizers are shared with the three-phase
+// persistent solver below.
+// ---------------------------------------------------------------------------
+// A: p = r + beta (p - omega nu) (or p = r, rhat = r after a restart);
+//    z1 = M^-1 p; sum(z1 h^3)
 template <class T>
-__global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
-  __shared__ FdTile tiles[GROUPS];
-  __shared__ double red[64];
-  __shared__ double inv_eig[BN];
-  const GroupIdx G;
-  if (!A.ext_precond) {  // independent of the previous kernel: overlaps its tail
-    fd_fill_inverse_eigen(inv_eig, c_lam);
-    __syncthreads();
-  }
-  pdl_wait();
-  pdl_launch_dependents();
-  const KrylovState& S = *A.st;
-  if (S.done) return;
-  const double beta = S.beta, omega = S.omega;
-  const bool restart = S.restart_pending != 0;
+__device__ __forceinline__ double phase_a(const KArgs<T>& A, const GroupIdx& G, FdTile& tile, const double* inv,
+                                          double beta, double omega, bool restart) {
   const DevMesh& M = A.M;
-  double acc[1] = {0.0};
+  double acc = 0.0;
   GROUP_BLOCKS(b) {
     double r[8], p[8];
     load_col(A.r, b, G, r);
@@ -483,7 +490,7 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
     store_col(A.p, b, G, p);
     if (A.ext_precond) continue;  // z1 comes from the external preconditioner
     const double h = M.h[b];
-    block_inverse_group(p, tiles[G.g], G, h, inv_eig);
+    block_inverse_group(p, tile, G, h, inv);
     double s = 0.0;
 #pragma unroll
     for (int z = 0; z < 8; ++z) {
@@ -491,20 +498,199 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
       s += p[z];
     }
     store_col(A.z1, b, G, p);
-    acc[0] += s * h * h * h;
+    acc += s * h * h * h;
   }
-  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
-    KrylovState& W = *A.st;
-    W.mean_sum = acc[0];
-    if (restart) {
-      W.rho = W.rr;
-      W.rr_hat = W.rr;
-      W.restart_pending = 0;
-    }
+  return acc;
+}
+
+__device__ __forceinline__ void fin_a(KrylovState& W, double sum, bool restart) {
+  W.mean_sum = sum;
+  if (restart) {
+    W.rho = W.rr;
+    W.rr_hat = W.rr;
+    W.restart_pending = 0;
   }
 }
 
-// KB: nu = A z1; alpha = rho / ((rhat, nu) + eps)
+// B: nu = A z1; (rhat, nu)
+template <class T>
+__device__ __forceinline__ double phase_b(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, double ms) {
+  const DevMesh& M = A.M;
+  double acc = 0.0;
+  GROUP_BLOCKS(b) {
+    double col[8], y[8], rh[8];
+    load_col(A.z1, b, G, col);
+    spmv_group(M, b, VecAt<T>{A.z1}, col, ms, A.mean_mode, tile, G, y);
+    load_col(A.rhat, b, G, rh);
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      y[z] = double(T(y[z]));
+      acc += rh[z] * y[z];
+    }
+    store_col(A.nu, b, G, y);
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void fin_b(KrylovState& W, double rhat_nu) { W.alpha = W.rho / (rhat_nu + W.eps); }
+
+// C: s = r - alpha nu (in place in r); z2 = M^-1 s; sum(z2 h^3)
+template <class T>
+__device__ __forceinline__ double phase_c(const KArgs<T>& A, const GroupIdx& G, FdTile& tile, const double* inv,
+                                          double alpha) {
+  const DevMesh& M = A.M;
+  double acc = 0.0;
+  GROUP_BLOCKS(b) {
+    double r[8], nu[8];
+    load_col(A.r, b, G, r);
+    load_col(A.nu, b, G, nu);
+#pragma unroll
+    for (int z = 0; z < 8; ++z) r[z] = double(T(r[z] - alpha * nu[z]));
+    store_col(A.r, b, G, r);
+    if (A.ext_precond) continue;  // z2 comes from the external preconditioner
+    const double h = M.h[b];
+    block_inverse_group(r, tile, G, h, inv);
+    double s = 0.0;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      r[z] = double(T(r[z]));
+      s += r[z];
+    }
+    store_col(A.z2, b, G, r);
+    acc += s * h * h * h;
+  }
+  return acc;
+}
+
+__device__ __forceinline__ void fin_c(KrylovState& W, double sum) { W.mean_sum = sum; }
+
+// D: t = A z2; (t, s), (t, t)
+template <class T>
+__device__ __forceinline__ void phase_d(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, double ms,
+                                        double (&acc)[2]) {
+  const DevMesh& M = A.M;
+  GROUP_BLOCKS(b) {
+    double col[8], y[8], sv[8];
+    load_col(A.z2, b, G, col);
+    spmv_group(M, b, VecAt<T>{A.z2}, col, ms, A.mean_mode, tile, G, y);
+    load_col(A.r, b, G, sv);
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      y[z] = double(T(y[z]));
+      acc[0] += y[z] * sv[z];
+      acc[1] += y[z] * y[z];
+    }
+    store_col(A.t, b, G, y);
+  }
+}
+
+__device__ __forceinline__ void fin_d(KrylovState& W, const double (&acc)[2]) {
+  W.omega = acc[0] / (acc[1] + W.eps);
+}
+
+// E: x_new = x + alpha z1 + omega z2; r = s - omega t; (rhat, r), (r, r).
+// Two cells per thread per pass with 2-wide vector accesses (nb*512 is even
+// and every vector starts on a 16-byte boundary).
+template <class T>
+__device__ __forceinline__ void phase_e(const KArgs<T>& A, const T* xc, T* xn, double alpha, double omega,
+                                        double (&acc)[2]) {
+  using V2 = typename Vec2<T>::type;
+  const size_t n2 = size_t(A.M.nb) * (BN / 2);
+  const V2* xc2 = reinterpret_cast<const V2*>(xc);
+  const V2* z12 = reinterpret_cast<const V2*>(A.z1);
+  const V2* z22 = reinterpret_cast<const V2*>(A.z2);
+  const V2* t2 = reinterpret_cast<const V2*>(A.t);
+  const V2* rh2 = reinterpret_cast<const V2*>(A.rhat);
+  V2* r2 = reinterpret_cast<V2*>(A.r);
+  V2* xn2 = reinterpret_cast<V2*>(xn);
+  for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n2; i += size_t(gridDim.x) * NT) {
+    const V2 x = ld_stream(xc2 + i), z1 = ld_stream(z12 + i), z2 = ld_stream(z22 + i), t = ld_stream(t2 + i),
+             r = ld_stream(r2 + i), rh = ld_stream(rh2 + i);
+    V2 xo, ro;
+    xo.x = T((double(x.x) + alpha * double(z1.x)) + omega * double(z2.x));
+    xo.y = T((double(x.y) + alpha * double(z1.y)) + omega * double(z2.y));
+    ro.x = T(double(r.x) - omega * double(t.x));
+    ro.y = T(double(r.y) - omega * double(t.y));
+    xn2[i] = xo;
+    r2[i] = ro;
+    acc[0] += double(rh.x) * double(ro.x);
+    acc[0] += double(rh.y) * double(ro.y);
+    acc[1] += double(ro.x) * double(ro.x);
+    acc[1] += double(ro.y) * double(ro.y);
+  }
+}
+
+// convergence, best iterate, stall and restart decisions, beta for the next A
+__device__ __forceinline__ void fin_e(KrylovState& W, const double (&acc)[2]) {
+  const double err = sqrt(acc[1]);
+  W.err = err;
+  W.rr = acc[1];
+  W.k += 1;
+  W.cur = W.nxt;
+  if (!(err == err)) {
+    W.done = 1;
+    W.status = SOLVE_NAN;
+  } else if (err < W.err_opt) {
+    W.err_opt = err;
+    W.best = W.cur;
+    if (err <= W.tol_abs || err / W.err_init <= W.tol_rel) {
+      W.done = 1;
+      W.converged = 1;
+      W.status = SOLVE_CONVERGED;
+    }
+  }
+  // next free slot: neither the current nor the best iterate
+  int nx = 0;
+  while (nx == W.cur || nx == W.best) ++nx;
+  W.nxt = nx;
+  if (!W.done && W.k >= W.max_iter) {
+    W.done = 1;
+    W.status = SOLVE_MAXITER;
+  }
+  if (err < 0.9 * W.stall_ref) {
+    W.stall_ref = err;
+    W.last_improve_k = W.k;
+  } else if (!W.done && W.stall_window > 0 && W.k - W.last_improve_k >= W.stall_window) {
+    W.done = 1;
+    W.status = SOLVE_STALL;
+  }
+  W.rho_prev = W.rho;
+  W.rho = acc[0];
+  if (!W.done) {
+    const bool breakdown = W.rho * W.rho < 1e-16 * W.rr * W.rr_hat;
+    if (breakdown && W.max_restarts > 0) {
+      W.restarts += 1;
+      if (W.restarts >= W.max_restarts) {
+        W.done = 1;
+        W.status = SOLVE_RESTARTS;
+      } else {
+        W.restart_pending = 1;
+      }
+    }
+    W.beta = (W.rho / (W.rho_prev + W.eps)) * (W.alpha / (W.omega + W.eps));
+  }
+}
+
+// ---- per-phase kernels (one launch per phase, last-CTA finalizer) ----------
+template <class T>
+__global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
+  __shared__ FdTile tiles[GROUPS];
+  __shared__ double red[64];
+  __shared__ double inv_eig[BN];
+  const GroupIdx G;
+  if (!A.ext_precond) {  // independent of the previous kernel: overlaps its tail
+    fd_fill_inverse_eigen(inv_eig, c_lam);
+    __syncthreads();
+  }
+  pdl_wait();
+  pdl_launch_dependents();
+  const KrylovState& S = *A.st;
+  if (S.done) return;
+  const bool restart = S.restart_pending != 0;
+  double acc[1] = {phase_a<T>(A, G, tiles[G.g], inv_eig, S.beta, S.omega, restart)};
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) fin_a(*A.st, acc[0], restart);
+}
+
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_b(KArgs<T> A) {
   __shared__ GroupTile tiles[GROUPS];
@@ -514,28 +700,10 @@ __global__ void __launch_bounds__(NT) k_bicg_b(KArgs<T> A) {
   const KrylovState& S = *A.st;
   if (S.done) return;
   const GroupIdx G;
-  const DevMesh& M = A.M;
-  const double ms = S.mean_sum;
-  double acc[1] = {0.0};
-  GROUP_BLOCKS(b) {
-    double col[8], y[8], rh[8];
-    load_col(A.z1, b, G, col);
-    spmv_group<T>(M, b, A.z1, col, ms, A.mean_mode, tiles[G.g], G, y);
-    load_col(A.rhat, b, G, rh);
-#pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      y[z] = double(T(y[z]));
-      acc[0] += rh[z] * y[z];
-    }
-    store_col(A.nu, b, G, y);
-  }
-  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
-    KrylovState& W = *A.st;
-    W.alpha = W.rho / (acc[0] + W.eps);
-  }
+  double acc[1] = {phase_b<T>(A, G, tiles[G.g], S.mean_sum)};
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) fin_b(*A.st, acc[0]);
 }
 
-// KC: s = r - alpha nu (in place in r); z2 = M^-1 s; sum(z2 h^3)
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
   __shared__ FdTile tiles[GROUPS];
@@ -550,32 +718,10 @@ __global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
   pdl_launch_dependents();
   const KrylovState& S = *A.st;
   if (S.done) return;
-  const double alpha = S.alpha;
-  const DevMesh& M = A.M;
-  double acc[1] = {0.0};
-  GROUP_BLOCKS(b) {
-    double r[8], nu[8];
-    load_col(A.r, b, G, r);
-    load_col(A.nu, b, G, nu);
-#pragma unroll
-    for (int z = 0; z < 8; ++z) r[z] = double(T(r[z] - alpha * nu[z]));
-    store_col(A.r, b, G, r);
-    if (A.ext_precond) continue;  // z2 comes from the external preconditioner
-    const double h = M.h[b];
-    block_inverse_group(r, tiles[G.g], G, h, inv_eig);
-    double s = 0.0;
-#pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      r[z] = double(T(r[z]));
-      s += r[z];
-    }
-    store_col(A.z2, b, G, r);
-    acc[0] += s * h * h * h;
-  }
-  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) A.st->mean_sum = acc[0];
+  double acc[1] = {phase_c<T>(A, G, tiles[G.g], inv_eig, S.alpha)};
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) fin_c(*A.st, acc[0]);
 }
 
-// KD: t = A z2; omega = (t, s) / ((t, t) + eps)
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_d(KArgs<T> A) {
   __shared__ GroupTile tiles[GROUPS];
@@ -585,30 +731,11 @@ __global__ void __launch_bounds__(NT) k_bicg_d(KArgs<T> A) {
   const KrylovState& S = *A.st;
   if (S.done) return;
   const GroupIdx G;
-  const DevMesh& M = A.M;
-  const double ms = S.mean_sum;
   double acc[2] = {0.0, 0.0};
-  GROUP_BLOCKS(b) {
-    double col[8], y[8], sv[8];
-    load_col(A.z2, b, G, col);
-    spmv_group<T>(M, b, A.z2, col, ms, A.mean_mode, tiles[G.g], G, y);
-    load_col(A.r, b, G, sv);
-#pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      y[z] = double(T(y[z]));
-      acc[0] += y[z] * sv[z];
-      acc[1] += y[z] * y[z];
-    }
-    store_col(A.t, b, G, y);
-  }
-  if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
-    KrylovState& W = *A.st;
-    W.omega = acc[0] / (acc[1] + W.eps);
-  }
+  phase_d<T>(A, G, tiles[G.g], S.mean_sum, acc);
+  if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) fin_d(*A.st, acc);
 }
 
-// KE: x_new = x + alpha z1 + omega z2; r = s - omega t; (rhat, r), (r, r);
-//     convergence, best iterate, restart decision, beta for the next KA.
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_e(KArgs<T> A) {
   __shared__ double red[64];
@@ -616,85 +743,61 @@ __global__ void __launch_bounds__(NT) k_bicg_e(KArgs<T> A) {
   pdl_launch_dependents();
   const KrylovState& S = *A.st;
   if (S.done) return;
-  const double alpha = S.alpha, omega = S.omega;
-  const T* xc = xslot(A, S.cur);
-  T* xn = xslot(A, S.nxt);
-  const DevMesh& M = A.M;
   double acc[2] = {0.0, 0.0};
-  // two cells per thread per pass with 2-wide vector accesses (nb*512 is even
-  // and every vector starts on a 16-byte boundary)
-  using V2 = typename Vec2<T>::type;
-  const size_t n2 = size_t(M.nb) * (BN / 2);
-  const V2* xc2 = reinterpret_cast<const V2*>(xc);
-  const V2* z12 = reinterpret_cast<const V2*>(A.z1);
-  const V2* z22 = reinterpret_cast<const V2*>(A.z2);
-  const V2* t2 = reinterpret_cast<const V2*>(A.t);
-  const V2* rh2 = reinterpret_cast<const V2*>(A.rhat);
-  V2* r2 = reinterpret_cast<V2*>(A.r);
-  V2* xn2 = reinterpret_cast<V2*>(xn);
-  for (size_t i = size_t(blockIdx.x) * NT + threadIdx.x; i < n2; i += size_t(gridDim.x) * NT) {
-    const V2 x = xc2[i], z1 = z12[i], z2 = z22[i], t = t2[i], r = r2[i], rh = rh2[i];
-    V2 xo, ro;
-    xo.x = T((double(x.x) + alpha * double(z1.x)) + omega * double(z2.x));
-    xo.y = T((double(x.y) + alpha * double(z1.y)) + omega * double(z2.y));
-    ro.x = T(double(r.x) - omega * double(t.x));
-    ro.y = T(double(r.y) - omega * double(t.y));
-    xn2[i] = xo;
-    r2[i] = ro;
-    acc[0] += double(rh.x) * double(ro.x);
-    acc[0] += double(rh.y) * double(ro.y);
-    acc[1] += double(ro.x) * double(ro.x);
-    acc[1] += double(ro.y) * double(ro.y);
+  phase_e<T>(A, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.omega, acc);
+  if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) fin_e(*A.st, acc);
+}
+
+// ---- persistent solver: all iterations in one cooperative launch ----------
+// Every CTA keeps a copy of the Krylov state in shared memory and applies
+// the finalizers to the grid totals of each phase, so all copies stay equal;
+// CTA 0 writes the state back at the end.  Data written by other CTAs is read
+// after the grid barrier's acquire fence, with loads that bypass L1.
+template <class T>
+__global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync Gs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw);
+  double* inv_eig = reinterpret_cast<double*>(smem_raw + GROUPS * sizeof(GroupTile));
+  __shared__ double red[64];
+  __shared__ KrylovState S;
+  const GroupIdx G;
+  GroupTile& tile = tiles[G.g];
+  FdTile& ftile = reinterpret_cast<FdTile&>(tile);  // FdTile is GroupTile's leading member
+  fd_fill_inverse_eigen(inv_eig, c_lam);
+  if (threadIdx.x == 0) S = *A.st;
+  __syncthreads();
+  bool ok = true;
+  while (ok && !S.done) {
+    const bool restart = S.restart_pending != 0;
+    double a[1] = {phase_a<T>(A, G, ftile, inv_eig, S.beta, S.omega, restart)};
+    if (!(ok = grid_allreduce<1>(a, Gs, red))) break;
+    if (threadIdx.x == 0) fin_a(S, a[0], restart);
+    __syncthreads();
+    double b[1] = {phase_b<T>(A, G, tile, S.mean_sum)};
+    if (!(ok = grid_allreduce<1>(b, Gs, red))) break;
+    if (threadIdx.x == 0) fin_b(S, b[0]);
+    __syncthreads();
+    double c[1] = {phase_c<T>(A, G, ftile, inv_eig, S.alpha)};
+    if (!(ok = grid_allreduce<1>(c, Gs, red))) break;
+    if (threadIdx.x == 0) fin_c(S, c[0]);
+    __syncthreads();
+    double d[2] = {0.0, 0.0};
+    phase_d<T>(A, G, tile, S.mean_sum, d);
+    if (!(ok = grid_allreduce<2>(d, Gs, red))) break;
+    if (threadIdx.x == 0) fin_d(S, d);
+    __syncthreads();
+    double e[2] = {0.0, 0.0};
+    phase_e<T>(A, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.omega, e);
+    if (!(ok = grid_allreduce<2>(e, Gs, red))) break;
+    if (threadIdx.x == 0) fin_e(S, e);
+    __syncthreads();
   }
-  if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) {
-    KrylovState& W = *A.st;
-    const double err = sqrt(acc[1]);
-    W.err = err;
-    W.rr = acc[1];
-    W.k += 1;
-    W.cur = W.nxt;
-    if (!(err == err)) {
-      W.done = 1;
-      W.status = SOLVE_NAN;
-    } else if (err < W.err_opt) {
-      W.err_opt = err;
-      W.best = W.cur;
-      if (err <= W.tol_abs || err / W.err_init <= W.tol_rel) {
-        W.done = 1;
-        W.converged = 1;
-        W.status = SOLVE_CONVERGED;
-      }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!ok) {
+      S.done = 1;
+      S.status = SOLVE_BARRIER_TIMEOUT;
     }
-    // next free slot: neither the current nor the best iterate
-    int nx = 0;
-    while (nx == W.cur || nx == W.best) ++nx;
-    W.nxt = nx;
-    if (!W.done && W.k >= W.max_iter) {
-      W.done = 1;
-      W.status = SOLVE_MAXITER;
-    }
-    if (err < 0.9 * W.stall_ref) {
-      W.stall_ref = err;
-      W.last_improve_k = W.k;
-    } else if (!W.done && W.stall_window > 0 && W.k - W.last_improve_k >= W.stall_window) {
-      W.done = 1;
-      W.status = SOLVE_STALL;
-    }
-    W.rho_prev = W.rho;
-    W.rho = acc[0];
-    if (!W.done) {
-      const bool breakdown = W.rho * W.rho < 1e-16 * W.rr * W.rr_hat;
-      if (breakdown && W.max_restarts > 0) {
-        W.restarts += 1;
-        if (W.restarts >= W.max_restarts) {
-          W.done = 1;
-          W.status = SOLVE_RESTARTS;
-        } else {
-          W.restart_pending = 1;
-        }
-      }
-      W.beta = (W.rho / (W.rho_prev + W.eps)) * (W.alpha / (W.omega + W.eps));
-    }
+    *A.st = S;
   }
 }
 
@@ -736,7 +839,7 @@ __global__ void __launch_bounds__(NT) k_true_residual(DevMesh M, const double* _
   GROUP_BLOCKS(blk) {
     double col[8], y[8], bc[8];
     load_col(x, blk, G, col);
-    spmv_group<double>(M, blk, x, col, ms, mean_mode, tiles[G.g], G, y);
+    spmv_group(M, blk, VecAt<double>{x}, col, ms, mean_mode, tiles[G.g], G, y);
     load_col(b, blk, G, bc);
     if (zero_mean_row && blk == M.mean_block && G.lane == 0) bc[0] = 0.0;
     float* rb = r32 ? r32 + size_t(blk) * BN + G.gy * 8 + G.gx : nullptr;
@@ -814,11 +917,16 @@ int launch_block_inverse(const DevMesh& M, const double* in, double* out, Poisso
 // Launches a solver kernel with programmatic stream serialization: its CTAs
 // may be scheduled while the previous kernel drains and wait in pdl_wait().
 template <class T>
-static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, const KArgs<T>& A) {
+static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, const KArgs<T>& A,
+                              size_t dyn_smem = 0) {
+  if (dyn_smem > 0) {
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn_smem));
+    if (e != cudaSuccess) return e;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(NT);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = dyn_smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -826,6 +934,31 @@ static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kern, A);
+}
+
+// Launches the persistent solver: one cooperative grid (every CTA resident)
+// that runs iterations until the state says done.
+template <class T>
+static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, const char* name) {
+  const size_t dyn = GROUPS * sizeof(GroupTile) + BN * sizeof(double);
+  void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
+  CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+  int per_sm = 0, dev = 0, sms = 0;
+  CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, dyn));
+  CUP_CUDA_TRY(cudaGetDevice(&dev));
+  CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (per_sm < 1) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: kernel does not fit on an SM");
+  const int grid = std::max(1, std::min(per_sm * sms, (A.M.nb + GROUPS - 1) / GROUPS));
+  // arrivals, generation and the error flag start at zero (a timed-out
+  // barrier of an earlier launch may have left arrivals behind)
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned int), s));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
+  GridSync Gs{W.bar, W.bar + 1, W.partial, W.bar_totals, W.bar_error};
+  KArgs<T> Aa = A;
+  void* args[] = {(void*)&Aa, (void*)&Gs};
+  ProfScope ps(name, s);
+  CUP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(NT), args, dyn, s));
+  return 0;
 }
 
 // Runs BiCGSTAB on vectors of type T; x holds x0 on entry, x_opt on exit.
@@ -848,8 +981,16 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_prepare<T>, W.grid, s, A)); }
   { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_init<T>, W.ggrid, s, A)); }
   CUP_CUDA_TRY(cudaGetLastError());
+  const bool persistent = !cnn && P.persistent;
+  if (persistent) {
+    if (int rc = launch_persistent<T>(A, W, s, f32 ? "bicg32_persistent" : "bicg_persistent")) return rc;
+    int h_err = 0;
+    CUP_CUDA_TRY(cudaMemcpyAsync(&h_err, W.bar_error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h_err) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: a grid barrier wait timed out");
+  }
   const int chunk = P.check_every > 0 ? P.check_every : 8;
-  for (int it = 0; it < P.max_iter; it += chunk) {
+  for (int it = 0; it < P.max_iter && !persistent; it += chunk) {
     for (int j = 0; j < chunk; ++j) {
       { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_a<T>, W.ggrid, s, A)); }
       if (cnn)

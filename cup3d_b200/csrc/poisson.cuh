@@ -27,7 +27,8 @@ enum SolveStatus : int {
   SOLVE_MAXITER = 2,
   SOLVE_RESTARTS = 3,
   SOLVE_NAN = 4,
-  SOLVE_STALL = 5
+  SOLVE_STALL = 5,
+  SOLVE_BARRIER_TIMEOUT = 6  // persistent solver: a grid barrier wait timed out
 };
 
 // The operator and preconditioner kernels give each mesh block a 64-thread
@@ -43,6 +44,9 @@ struct PoissonWork {
   KrylovState* st2;         // outer (refinement) state
   double* partial;          // grid * 8
   unsigned int* counters;   // 16
+  unsigned int* bar;        // persistent solver: [0] arrivals, [1] generation
+  double* bar_totals;       // 8
+  int* bar_error;           // 1
   int grid;                 // CTAs for block kernels
   int ggrid;                // CTAs for block-group kernels (4 mesh blocks per CTA pass)
 };
@@ -52,6 +56,7 @@ struct SolveParams {
   int max_iter, max_restarts, mean_mode;
   int check_every;   // host checks convergence every this many iterations
   int stall_window;  // 0: off (reference behaviour)
+  int persistent;    // 1: all iterations in one cooperative launch (plain and mixed solvers)
 };
 
 struct SolveStats {
