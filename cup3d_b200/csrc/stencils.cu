@@ -19,50 +19,39 @@ struct Vec3 {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double sq(double a) { return a * a; }
 
-__device__ __forceinline__ double weno5_plus(double um2, double um1, double u, double up1, double up2) {
+// WENO5 reconstruction biased to the left (weno5_plus of
+// AdvectionDiffusion.cpp:34-64): candidate stencils f1..f3 with smoothness
+// indicators b1..b3, nonlinear weights w_k = (d_k/q_k) / sum_j d_j/q_j with
+// q_k = (b_k + eps)^2 and d = (0.1, 0.6, 0.3).  The weights are evaluated with
+// one division instead of four: multiplying numerator and denominator by
+// q1 q2 q3 gives  sum_k a_k f_k / sum_k a_k  with  a_1 = 0.1 q2 q3,
+// a_2 = 0.6 q1 q3, a_3 = 0.3 q1 q2  (q_k >= eps^2 = 1e-12, so no underflow).
+__device__ __forceinline__ double weno5_left(double um2, double um1, double u, double up1, double up2) {
   const double e = 1e-6;
   const double b1 = 13.0 / 12.0 * sq((um2 + u) - 2 * um1) + 0.25 * sq((um2 + 3 * u) - 4 * um1);
   const double b2 = 13.0 / 12.0 * sq((um1 + up1) - 2 * u) + 0.25 * sq(um1 - up1);
   const double b3 = 13.0 / 12.0 * sq((u + up2) - 2 * up1) + 0.25 * sq((3 * u + up2) - 4 * up1);
-  const double what1 = 0.1 / sq(b1 + e);
-  const double what2 = 0.6 / sq(b2 + e);
-  const double what3 = 0.3 / sq(b3 + e);
-  const double aux = 1.0 / ((what1 + what3) + what2);
-  const double w1 = what1 * aux, w2 = what2 * aux, w3 = what3 * aux;
+  const double q1 = sq(b1 + e), q2 = sq(b2 + e), q3 = sq(b3 + e);
+  const double a1 = 0.1 * (q2 * q3), a2 = 0.6 * (q1 * q3), a3 = 0.3 * (q1 * q2);
   const double f1 = (11.0 / 6.0) * u + ((1.0 / 3.0) * um2 - (7.0 / 6.0) * um1);
   const double f2 = (5.0 / 6.0) * u + ((-1.0 / 6.0) * um1 + (1.0 / 3.0) * up1);
   const double f3 = (1.0 / 3.0) * u + ((+5.0 / 6.0) * up1 - (1.0 / 6.0) * up2);
-  return (w1 * f1 + w3 * f3) + w2 * f2;
+  return ((a1 * f1 + a3 * f3) + a2 * f2) / ((a1 + a3) + a2);
 }
 
-__device__ __forceinline__ double weno5_minus(double um2, double um1, double u, double up1, double up2) {
-  const double e = 1e-6;
-  const double b1 = 13.0 / 12.0 * sq((um2 + u) - 2 * um1) + 0.25 * sq((um2 + 3 * u) - 4 * um1);
-  const double b2 = 13.0 / 12.0 * sq((um1 + up1) - 2 * u) + 0.25 * sq(um1 - up1);
-  const double b3 = 13.0 / 12.0 * sq((u + up2) - 2 * up1) + 0.25 * sq((3 * u + up2) - 4 * up1);
-  const double what1 = 0.3 / sq(b1 + e);
-  const double what2 = 0.6 / sq(b2 + e);
-  const double what3 = 0.1 / sq(b3 + e);
-  const double aux = 1.0 / ((what1 + what3) + what2);
-  const double w1 = what1 * aux, w2 = what2 * aux, w3 = what3 * aux;
-  const double f1 = (1.0 / 3.0) * u + ((-1.0 / 6.0) * um2 + (5.0 / 6.0) * um1);
-  const double f2 = (5.0 / 6.0) * u + ((1.0 / 3.0) * um1 - (1.0 / 6.0) * up1);
-  const double f3 = (11.0 / 6.0) * u + ((-7.0 / 6.0) * up1 + (1.0 / 3.0) * up2);
-  return (w1 * f1 + w3 * f3) + w2 * f2;
-}
-
+// Upwind derivative of KernelAdvectDiffuse (AdvectionDiffusion.cpp:66-103).
+// WENO5: the right-biased reconstruction (weno5_minus) is the left-biased one
+// of the mirrored stencil, weno5_minus(a,b,c,d,e) = weno5_plus(e,d,c,b,a), so
+// the upwind choice only selects the five inputs of two left-biased
+// evaluations and no warp diverges on the sign of U.
 template <int SCHEME>
 __device__ __forceinline__ double deriv(double U, double um3, double um2, double um1, double u, double up1,
                                         double up2, double up3) {
   if (SCHEME == 1) {
-    double fp, fm;
-    if (U > 0) {
-      fp = weno5_plus(um2, um1, u, up1, up2);
-      fm = weno5_plus(um3, um2, um1, u, up1);
-    } else {
-      fp = weno5_minus(um1, u, up1, up2, up3);
-      fm = weno5_minus(um2, um1, u, up1, up2);
-    }
+    const bool pos = U > 0;
+    // face i+1/2 and face i-1/2 reconstructions in the upwind direction
+    const double fp = weno5_left(pos ? um2 : up3, pos ? um1 : up2, pos ? u : up1, pos ? up1 : u, pos ? up2 : um1);
+    const double fm = weno5_left(pos ? um3 : up2, pos ? um2 : up1, pos ? um1 : u, pos ? u : um1, pos ? up1 : um2);
     return fp - fm;
   }
   if (U > 0) return (-2 * um3 + 15 * um2 - 60 * um1 + 20 * u + 30 * up1 - 3 * up2) / 60.;
