@@ -161,68 +161,66 @@ __device__ __forceinline__ bool grid_reduce_max(double& v, const GridReduce& g, 
 
 // ---------------------------------------------------------------------------
 // Grid-wide barrier with a reduction, for cooperative (co-resident) launches.
-// Each CTA writes its NR partial sums; the last CTA to arrive sums them in
-// CTA order (deterministic), publishes the totals and releases the others,
-// which spin on a generation counter with a bounded wait: after
-// kBarrierSpinLimit polls (well over a second) a waiter sets *error and
-// returns false, so a barrier that can never complete ends the kernel
-// instead of hanging the device.
+// Each CTA writes its NR partial sums into the slot of this barrier (two slots
+// alternate, so a CTA that runs ahead to the next barrier cannot overwrite
+// partials another CTA is still reading), arrives on a counter that only
+// grows, and waits until every CTA has arrived at this barrier.  Then every
+// CTA sums all partials itself, in the same order, so all CTAs hold the same
+// totals and no CTA has to publish them.  The wait is bounded: after about a
+// second of polling a waiter sets *error and returns false, so a barrier that
+// can never complete ends the kernel instead of hanging the device.
 // ---------------------------------------------------------------------------
 struct GridSync {
-  unsigned int* arrive;  // arrivals in the current barrier (0 between barriers)
-  unsigned int* gen;     // barrier generation
-  double* partial;       // gridDim.x * 8
-  double* totals;        // 8
+  unsigned int* arrive;  // arrivals since the launch (zero before it)
+  double* partial;       // 2 * gridDim.x * 8
   int* error;            // set on a timed-out wait
 };
 
-constexpr long long kBarrierSpinLimit = 1ll << 24;
+constexpr long long kBarrierClockLimit = 1ll << 31;  // SM clock cycles, about 1 s
 
+// epoch: the number of barriers this CTA has passed (shared, zero at launch)
 template <int NR>
-__device__ bool grid_allreduce(double (&v)[NR], const GridSync& G, double* sm) {
+__device__ bool grid_allreduce(double (&v)[NR], const GridSync& G, unsigned int& epoch, double* sm) {
+  const unsigned int k = epoch;
+  double* part = G.partial + size_t(k & 1u) * gridDim.x * 8;
   block_reduce<NR>(v, sm);  // ends with __syncthreads: the CTA's writes precede the arrival
-  __shared__ unsigned int s_last, s_gen;
   __shared__ int s_ok;
+  __shared__ double s_tot[8];
   if (threadIdx.x == 0) {
-    s_gen = *reinterpret_cast<volatile unsigned int*>(G.gen);
 #pragma unroll
-    for (int r = 0; r < NR; ++r) G.partial[blockIdx.x * 8 + r] = v[r];
+    for (int r = 0; r < NR; ++r) part[blockIdx.x * 8 + r] = v[r];
     __threadfence();
-    s_last = atomicAdd(G.arrive, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    double acc[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
-#pragma unroll
-      for (int r = 0; r < NR; ++r) acc[r] += __ldcg(&G.partial[i * 8 + r]);
-    block_reduce<NR>(acc, sm);
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int r = 0; r < NR; ++r) G.totals[r] = acc[r];
-      *G.arrive = 0u;
-      __threadfence();
-      atomicAdd(G.gen, 1u);
-      s_ok = 1;
+    atomicAdd(G.arrive, 1u);
+    const unsigned int target = (k + 1u) * gridDim.x;
+    volatile unsigned int* a = G.arrive;
+    const long long t0 = clock64();
+    int ok = 1;
+    while (*a < target) {
+      if (clock64() - t0 > kBarrierClockLimit) {
+        ok = 0;
+        break;
+      }
     }
-  } else if (threadIdx.x == 0) {
-    volatile unsigned int* gen = G.gen;
-    long long spins = 0;
-    while (*gen == s_gen && spins < kBarrierSpinLimit) {
-      __nanosleep(32);
-      ++spins;
-    }
-    s_ok = *gen != s_gen;
-    if (!s_ok) atomicExch(G.error, 1);
+    if (!ok) atomicExch(G.error, 1);
+    s_ok = ok;
+    epoch = k + 1u;
     __threadfence();
   }
   __syncthreads();
   if (!s_ok) return false;
+  double acc[NR];
 #pragma unroll
-  for (int r = 0; r < NR; ++r) v[r] = __ldcg(&G.totals[r]);
+  for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] += __ldcg(&part[i * 8 + r]);
+  block_reduce<NR>(acc, sm);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) s_tot[r] = acc[r];
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < NR; ++r) v[r] = s_tot[r];
   return true;
 }
 

@@ -106,13 +106,12 @@ static int alloc_fields(cup_ctx* c) {
   W.ggrid = std::max(1, std::min((c->mesh.nb + GROUPS_PER_CTA - 1) / GROUPS_PER_CTA, c->num_sms * 8));
   if (int rc = A.alloc(&W.partial, size_t(std::max(W.grid, W.ggrid)) * 8)) return rc;
   if (int rc = A.alloc(&W.counters, 32)) return rc;
-  if (int rc = A.alloc(&W.bar, 2)) return rc;
-  if (int rc = A.alloc(&W.bar_totals, 8)) return rc;
+  if (int rc = A.alloc(&W.bar, 1)) return rc;
   if (int rc = A.alloc(&W.bar_error, 1)) return rc;
   if (int rc = A.alloc(&W.st, 1)) return rc;
   if (int rc = A.alloc(&W.st2, 1)) return rc;
   CUP_CUDA_TRY(stream_zero(c->stream, W.counters, 32 * sizeof(unsigned int)));
-  CUP_CUDA_TRY(stream_zero(c->stream, W.bar, 2 * sizeof(unsigned int)));
+  CUP_CUDA_TRY(stream_zero(c->stream, W.bar, sizeof(unsigned int)));
   CUP_CUDA_TRY(stream_zero(c->stream, W.bar_error, sizeof(int)));
   for (int i = 0; i < 2; ++i) {
     CUP_CUDA_TRY(stream_zero(c->stream, F.vel[i], 3 * n * 8));

@@ -760,35 +760,39 @@ __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync 
   double* inv_eig = reinterpret_cast<double*>(smem_raw + GROUPS * sizeof(GroupTile));
   __shared__ double red[64];
   __shared__ KrylovState S;
+  __shared__ unsigned int epoch;
   const GroupIdx G;
   GroupTile& tile = tiles[G.g];
   FdTile& ftile = reinterpret_cast<FdTile&>(tile);  // FdTile is GroupTile's leading member
   fd_fill_inverse_eigen(inv_eig, c_lam);
-  if (threadIdx.x == 0) S = *A.st;
+  if (threadIdx.x == 0) {
+    S = *A.st;
+    epoch = 0u;
+  }
   __syncthreads();
   bool ok = true;
   while (ok && !S.done) {
     const bool restart = S.restart_pending != 0;
     double a[1] = {phase_a<T>(A, G, ftile, inv_eig, S.beta, S.omega, restart)};
-    if (!(ok = grid_allreduce<1>(a, Gs, red))) break;
+    if (!(ok = grid_allreduce<1>(a, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_a(S, a[0], restart);
     __syncthreads();
     double b[1] = {phase_b<T>(A, G, tile, S.mean_sum)};
-    if (!(ok = grid_allreduce<1>(b, Gs, red))) break;
+    if (!(ok = grid_allreduce<1>(b, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_b(S, b[0]);
     __syncthreads();
     double c[1] = {phase_c<T>(A, G, ftile, inv_eig, S.alpha)};
-    if (!(ok = grid_allreduce<1>(c, Gs, red))) break;
+    if (!(ok = grid_allreduce<1>(c, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_c(S, c[0]);
     __syncthreads();
     double d[2] = {0.0, 0.0};
     phase_d<T>(A, G, tile, S.mean_sum, d);
-    if (!(ok = grid_allreduce<2>(d, Gs, red))) break;
+    if (!(ok = grid_allreduce<2>(d, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_d(S, d);
     __syncthreads();
     double e[2] = {0.0, 0.0};
     phase_e<T>(A, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.omega, e);
-    if (!(ok = grid_allreduce<2>(e, Gs, red))) break;
+    if (!(ok = grid_allreduce<2>(e, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_e(S, e);
     __syncthreads();
   }
@@ -948,12 +952,12 @@ static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, 
   CUP_CUDA_TRY(cudaGetDevice(&dev));
   CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: kernel does not fit on an SM");
-  const int grid = std::max(1, std::min(per_sm * sms, (A.M.nb + GROUPS - 1) / GROUPS));
-  // arrivals, generation and the error flag start at zero (a timed-out
-  // barrier of an earlier launch may have left arrivals behind)
-  CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned int), s));
+  // two partial slots of 8 doubles per CTA must fit in the reduction buffer
+  const int grid = std::max(1, std::min({per_sm * sms, (A.M.nb + GROUPS - 1) / GROUPS, std::max(W.grid, W.ggrid) / 2}));
+  // the arrival counter and the error flag start at zero
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
-  GridSync Gs{W.bar, W.bar + 1, W.partial, W.bar_totals, W.bar_error};
+  GridSync Gs{W.bar, W.partial, W.bar_error};
   KArgs<T> Aa = A;
   void* args[] = {(void*)&Aa, (void*)&Gs};
   ProfScope ps(name, s);

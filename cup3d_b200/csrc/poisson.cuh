@@ -44,9 +44,8 @@ struct PoissonWork {
   KrylovState* st2;         // outer (refinement) state
   double* partial;          // grid * 8
   unsigned int* counters;   // 16
-  unsigned int* bar;        // persistent solver: [0] arrivals, [1] generation
-  double* bar_totals;       // 8
-  int* bar_error;           // 1
+  unsigned int* bar;        // persistent solver: grid-barrier arrivals
+  int* bar_error;           // persistent solver: set on a timed-out barrier wait
   int grid;                 // CTAs for block kernels
   int ggrid;                // CTAs for block-group kernels (4 mesh blocks per CTA pass)
 };

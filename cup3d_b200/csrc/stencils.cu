@@ -211,7 +211,7 @@ struct UdefGet {
   }
 };
 
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 3)
     k_pressure_rhs(DevMesh M, const double* __restrict__ vel, const double* __restrict__ pold,
                    const double* __restrict__ chi, ObstacleView ob, double dt, int use_pold, double* lhs, double* phi) {
   extern __shared__ double smem[];
@@ -324,7 +324,7 @@ int launch_pressure_rhs(const DevMesh& M, const double* vel, const double* pold,
 // Mean removal + incremental pressure (PressureProjection.cpp:404-446) fused
 // with KernelGradP (:244-323) and the velocity update (:451-467).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
     k_grad_update(DevMesh M, double* vel, const double* __restrict__ phi, const double* __restrict__ pold,
                   double* __restrict__ pnew, const double* sums, double dt, int use_pold) {
   __shared__ double plab[LabGeom<1>::V];
