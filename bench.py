@@ -58,6 +58,13 @@ ALG_BYTES = {
 }
 
 
+# DRAM bytes (read + write) per cell and iteration of the persistent solver,
+# measured by ncu on 16 iterations of `python -m cup3d_b200.kernel_cases solve`
+# (profiles/bicg_persistent_sphere_solve.md: 263.2 MB + 598.4 MB over 16
+# iterations of 1,198,080 cells); most of the 184 algorithmic bytes hit in L2.
+MEASURED_TRAFFIC_PER_CELL_ITER = {"bicg_persistent": 44.95}
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
@@ -211,6 +218,20 @@ def run_b200(args):
     for _ in range(args.warmup):
         ctx.step(step)
         step += 1
+    # The timed pass, the per-kernel pass and the end-to-end pass all run the
+    # same K steps from the same state (velocity and pressure are the whole
+    # state carried between steps), so their Poisson solves do the same work.
+    first_step = step
+    vel_h = torch.empty(3 * ncell, dtype=torch.float64).pin_memory()
+    pres_h = torch.empty(ncell, dtype=torch.float64).pin_memory()
+    vel0 = ctx.download("vel")
+    pres0 = ctx.download("pres")
+
+    def restore():
+        ctx.upload("vel", vel0)
+        ctx.upload("pres", pres0)
+        torch.cuda.synchronize()
+        return first_step
     # ---- timed region: device-resident --------------------------------------
     clocks = ClockSampler(local)
     clocks.start()
@@ -236,6 +257,7 @@ def run_b200(args):
     clk = clocks.stop()
     # ---- per-kernel pass: the same K steps again with CUDA events around every
     # launch (kept out of the timed region above, whose number it would lower)
+    step = restore()
     ctx.profile(True)
     prof_iters = []
     for _ in range(args.steps):
@@ -273,11 +295,15 @@ def run_b200(args):
     else:
         alg_bytes = ALG_BYTES.get(dom_name, 0) * ncell
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if alg_bytes else None
-    # ---- e2e through the C ABI with host buffers -------------------------------
-    vel_h = torch.empty(3 * ncell, dtype=torch.float64).pin_memory()
-    pres_h = torch.empty(ncell, dtype=torch.float64).pin_memory()
-    vel_h.numpy()[:] = ctx.download("vel")
-    pres_h.numpy()[:] = ctx.download("pres")
+    traffic = None
+    if dom_name in MEASURED_TRAFFIC_PER_CELL_ITER:
+        traffic = int(MEASURED_TRAFFIC_PER_CELL_ITER[dom_name] * ncell * sum(prof_iters) / max(dom_n, 1))
+    # ---- e2e through the C ABI with host buffers: the same K steps, the state
+    # uploaded from pinned host memory before and downloaded after every step
+    step = restore()
+    vel_h.numpy()[:] = vel0
+    pres_h.numpy()[:] = pres0
+    e2e_iters = []
     lib = cup._lib.lib()
     import ctypes as C
     vp = C.cast(vel_h.data_ptr(), cup._lib._D)
@@ -290,7 +316,8 @@ def run_b200(args):
         e0.record(stream)
         cup._lib.check(lib.cup_upload_field(ctx._p, 0, vp), ctx._p)
         cup._lib.check(lib.cup_upload_field(ctx._p, 1, pp), ctx._p)
-        ctx.step(step)
+        _, _, st = ctx.step(step)
+        e2e_iters.append(st["iterations"])
         cup._lib.check(lib.cup_download_field(ctx._p, 0, vp), ctx._p)
         cup._lib.check(lib.cup_download_field(ctx._p, 1, pp), ctx._p)
         e1.record(stream)
@@ -320,15 +347,17 @@ def run_b200(args):
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps",
                    "first_timed_step": args.warmup},
         "poisson": {"iterations_per_step": iters, "solve_ms_per_step": [round(x, 3) for x in solve_ms]},
-        "kernels": {"pass": f"{args.steps} further steps with per-launch CUDA events "
+        "kernels": {"pass": f"the same {args.steps} steps again with per-launch CUDA events "
                             f"(Poisson iterations {prof_iters})",
                     **{k: {"launches": v[0], "ms": round(v[1], 4)}
                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])}},
         "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1) if achieved else None,
                      "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
                      "peak_source": peak_kind, "alg_bytes_per_launch": alg_bytes,
-                     "launch_ms": round(per_launch_ms, 5), "traffic": None},
-        "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s",
+                     "launch_ms": round(per_launch_ms, 5), "traffic": traffic,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per iteration (16-iteration "
+                                       "capture), scaled by the iterations of the launch" if traffic else None},
+        "e2e": {"value": round(e2e_value, 3), "unit": "Mcell-steps/s", "poisson_iterations": e2e_iters,
                 "h2d_bytes_per_step": 4 * 8 * ncell, "d2h_bytes_per_step": 4 * 8 * ncell},
         "gpu_launches": launches,
         "clocks": clk,
@@ -336,7 +365,7 @@ def run_b200(args):
     if not args.no_poisson:
         line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush)
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(ctx, args)
+        line["cpu_baseline"] = cpu_baseline(ctx, args, (vel0, pres0), first_step)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -358,18 +387,19 @@ def cpu_reference_step(ctx_host_state, m, slot, chi_o, udef_o, kin, chi, step, u
     return time.perf_counter() - t0, (vel, pres), info
 
 
-def cpu_baseline(ctx, args):
+def cpu_baseline(ctx, args, state, step):
+    """One step of the oracle's restatement of the reference CPU path, from the
+    state of the first timed step."""
     import oracle
     level, index, _ = ctx.blocks()
     m = oracle.Mesh(level, index, [4, 2, 2], 4, [0, 0, 0], 4.0)
     slot, chi_o, udef_o, kin = ctx.get_obstacle()
     chi = ctx.download("chi")
-    state = (ctx.download("vel"), ctx.download("pres"))
-    secs, _, info = cpu_reference_step(state, m, slot, chi_o, udef_o, kin, chi, args.warmup + 2 * args.steps,
+    secs, _, info = cpu_reference_step(state, m, slot, chi_o, udef_o, kin, chi, step,
                                        (-0.1, 0.0, 0.0), 4.1666666666666667e-05, 0.3, 1e6)
     return {"value": round(m.n / secs / 1e6, 4), "unit": "Mcell-steps/s", "cores": os.cpu_count(),
             "kind": "port",
-            "sample": f"1 full time step of the same workload from the GPU run's state "
+            "sample": f"1 full time step of the same workload from the state of the first timed step "
                       f"(oracle, OpenMP, pipelined BiCGSTAB + block CG, {info['iterations']} iterations, "
                       f"{secs:.2f} s)"}
 
