@@ -22,6 +22,9 @@ struct DevMesh {
   const int* __restrict__ fnbr;   // 24*nb
   const int* __restrict__ index;  // 3*nb
   const double* __restrict__ h;   // nb
+  // Order in which the block-group kernels visit the blocks (a permutation of
+  // 0..nb-1, or null for 0..nb-1): visit slot i holds block order[i].
+  const int* __restrict__ order;
 };
 
 #ifndef CUP3D_TAN_HELPERS

@@ -74,6 +74,7 @@ static int upload_mesh(cup_ctx* c) {
   c->dm.fnbr = fn;
   c->dm.index = ix;
   c->dm.h = h;
+  c->dm.order = nullptr;  // set by alloc_fields
   return 0;
 }
 
@@ -121,6 +122,14 @@ static int alloc_fields(cup_ctx* c) {
   CUP_CUDA_TRY(stream_zero(c->stream, F.lhs, n * 8));
   CUP_CUDA_TRY(stream_zero(c->stream, F.chi, n * 8));
   CUP_CUDA_TRY(stream_zero(c->stream, F.phi, n * 8));
+  // visit order of the block-group kernels, balanced for the persistent solver's groups
+  int groups = 0;
+  if (int rc = persistent_solver_groups(c->mesh.nb, W, &groups)) return rc;
+  const std::vector<int32_t> order = mesh_visit_order(c->mesh, groups);
+  int* d_order = nullptr;
+  if (int rc = A.alloc(&d_order, order.size())) return rc;
+  CUP_CUDA_TRY(stream_h2d(c->stream, d_order, order.data(), order.size() * sizeof(int32_t)));
+  c->dm.order = d_order;
   return 0;
 }
 

@@ -338,4 +338,23 @@ std::vector<std::array<int32_t, 4>> mesh_random_leaves(const MeshSpec& spec, uin
   return mesh_refine_leaves(spec, tag);
 }
 
+std::vector<int32_t> mesh_visit_order(const Mesh& m, int groups) {
+  const int nb = m.nb;
+  std::vector<int32_t> cost(nb, 2), ids(nb), order(nb);
+  for (int b = 0; b < nb; ++b) {
+    for (int f = 0; f < 6; ++f) {
+      const int k = m.face_kind[6 * b + f];
+      cost[b] += k == FACE_COARSER ? 1 : (k == FACE_FINER ? 2 : 0);
+    }
+    ids[b] = b;
+  }
+  std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  groups = std::max(1, groups);
+  for (int r = 0; r * groups < nb; ++r) {
+    const int base = r * groups, cnt = std::min(groups, nb - base);
+    for (int j = 0; j < cnt; ++j) order[base + j] = ids[base + ((r & 1) ? cnt - 1 - j : j)];
+  }
+  return order;
+}
+
 }  // namespace cup3d

@@ -103,4 +103,11 @@ std::vector<std::array<int32_t, 4>> mesh_sphere_wake_leaves(
 std::vector<std::array<int32_t, 4>> mesh_random_leaves(const MeshSpec& spec, uint64_t seed,
                                                        double refine_prob);
 
+// Order in which `groups` workers that each take blocks slot g, g + groups,
+// g + 2 groups, ... should visit the blocks so that every worker gets a
+// similar share of the Poisson operator's cost: blocks sorted by estimated
+// cost (coarse-fine faces cost extra flux work), dealt in snake order (one
+// round forward, the next backward).  A permutation of 0..nb-1.
+std::vector<int32_t> mesh_visit_order(const Mesh& m, int groups);
+
 }  // namespace cup3d

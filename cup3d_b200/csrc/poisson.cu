@@ -270,7 +270,11 @@ __device__ __forceinline__ void block_inverse_group(double col[8], FdTile& tile,
   group_sync(G.g);
 }
 
-#define GROUP_BLOCKS(b) for (int b = blockIdx.x * GROUPS + G.g; b < M.nb; b += gridDim.x * GROUPS)
+// Loops a group over its blocks: visit slots g, g + groups, ... of the
+// mesh's visit order (a cost-balanced permutation, see mesh_visit_order).
+#define GROUP_BLOCKS(b)                                                              \
+  for (int slot_ = blockIdx.x * GROUPS + G.g, b = 0;                                \
+       slot_ < M.nb && ((b = M.order ? M.order[slot_] : slot_), true); slot_ += gridDim.x * GROUPS)
 
 // ---------------------------------------------------------------------------
 // Standalone kernels
@@ -940,10 +944,11 @@ static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, 
   return cudaLaunchKernelEx(&cfg, kern, A);
 }
 
-// Launches the persistent solver: one cooperative grid (every CTA resident)
-// that runs iterations until the state says done.
+// CTAs of the persistent solver for a mesh of nb blocks: all co-resident,
+// at most one per four blocks, two partial slots of 8 doubles per CTA in the
+// reduction buffer.
 template <class T>
-static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, const char* name) {
+static int persistent_grid(int nb, const PoissonWork& W, int* grid) {
   const size_t dyn = GROUPS * sizeof(GroupTile) + BN * sizeof(double);
   void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
   CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
@@ -952,8 +957,27 @@ static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, 
   CUP_CUDA_TRY(cudaGetDevice(&dev));
   CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: kernel does not fit on an SM");
-  // two partial slots of 8 doubles per CTA must fit in the reduction buffer
-  const int grid = std::max(1, std::min({per_sm * sms, (A.M.nb + GROUPS - 1) / GROUPS, std::max(W.grid, W.ggrid) / 2}));
+  *grid = std::max(1, std::min({per_sm * sms, (nb + GROUPS - 1) / GROUPS, std::max(W.grid, W.ggrid) / 2}));
+  return 0;
+}
+
+int persistent_solver_groups(int nb, const PoissonWork& W, int* groups) {
+  int g1 = 0, g2 = 0;
+  if (int rc = persistent_grid<double>(nb, W, &g1)) return rc;
+  if (int rc = persistent_grid<float>(nb, W, &g2)) return rc;
+  if (g1 != g2) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: FP64 and FP32 grids differ");
+  *groups = g1 * GROUPS;
+  return 0;
+}
+
+// Launches the persistent solver: one cooperative grid (every CTA resident)
+// that runs iterations until the state says done.
+template <class T>
+static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, const char* name) {
+  const size_t dyn = GROUPS * sizeof(GroupTile) + BN * sizeof(double);
+  void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
+  int grid = 0;
+  if (int rc = persistent_grid<T>(A.M.nb, W, &grid)) return rc;
   // the arrival counter and the error flag start at zero
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));

@@ -88,4 +88,8 @@ int launch_weighted_sum(const DevMesh& M, const double* v, double* d_out, Poisso
 
 void poisson_init_constants();
 
+// Number of 64-thread groups of the persistent solver on a mesh of nb blocks
+// (the visit order is balanced for this many groups).
+int persistent_solver_groups(int nb, const PoissonWork& W, int* groups);
+
 }  // namespace cup3d
