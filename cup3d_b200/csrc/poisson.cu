@@ -37,9 +37,9 @@ void poisson_init_constants() { fd_init_constants(); }
 // at :384-478).  Faces normal to y use u = tan2 (z), v = tan1 (x); the others
 // u = tan1, v = tan2.  The one-sided forms apply at u, v = 0, 4 (forward) and
 // 3, 7 (backward), so every stencil stays inside the 4x4 quarter of the face
-// that holds (u, v).  The terms are evaluated without branches: all candidate
-// forms from clamped in-quarter loads, then selects (a divergent branch per
-// case serialises a warp up to nine times).
+// that holds (u, v).  The terms are evaluated without branches, Dmixed
+// included: all candidate forms from clamped in-quarter loads, then selects
+// (a divergent branch per case serialises a warp up to nine times).
 // ---------------------------------------------------------------------------
 struct TaylorTerms {
   double c, d1u, d1v, d2u, d2v, dm;
@@ -78,25 +78,19 @@ __device__ __forceinline__ TaylorTerms cf_terms(Layer L, int u, int v) {
   T.d2v = bdv ? 1. / 32. * Lvm2 - 1. / 16. * Lvm1 + 1. / 32. * c
         : fdv ? 1. / 32. * Lvp2 - 1. / 16. * Lvp1 + 1. / 32. * c
               : 1. / 32. * Lvm1 + 1. / 32. * Lvp1 - 1. / 16. * c;
-  double dm;
-  if (bdu && bdv)
-    dm = 1. / 16. * (c + Nmm - Lum1 - Lvm1);
-  else if (fdu && bdv)
-    dm = 1. / 16. * (Lup1 + Lvm1 - Npm - c);
-  else if (bdu && fdv)
-    dm = 1. / 16. * (Lvp1 + Lum1 - Nmp - c);
-  else if (fdu && fdv)
-    dm = 1. / 16. * (Npp + c - Lup1 - Lvp1);
-  else if (bdu)
-    dm = 1. / 32. * (Lvp1 + Nmm - Lvm1 - Nmp);
-  else if (fdu)
-    dm = 1. / 32. * (Npp + Lvm1 - Npm - Lvp1);
-  else if (bdv)
-    dm = 1. / 32. * (Lup1 + Nmm - Lum1 - Npm);
-  else if (fdv)
-    dm = 1. / 32. * (Npp + Lum1 - Nmp - Lup1);
-  else
-    dm = 1. / 64. * (Npp + Nmm - Npm - Nmp);
+  // Dmixed: (N(u1,v1) + N(u0,v0)) - N(u0,v1) - N(u1,v0), N(i,j) = L(u+i, v+j),
+  // with the pair (u0,u1) = (-1,0) at a backward edge, (0,+1) at a forward
+  // edge and (-1,+1) at half weight in the middle (likewise for v): the nine
+  // cases of PoissonSolverExp.h:442-478 in one branch-free form
+  auto Nsel = [&](int i, int j) {
+    const double rm = j < 0 ? Nmm : (j > 0 ? Nmp : Lum1);
+    const double r0 = j < 0 ? Lvm1 : (j > 0 ? Lvp1 : c);
+    const double rp = j < 0 ? Npm : (j > 0 ? Npp : Lup1);
+    return i < 0 ? rm : (i > 0 ? rp : r0);
+  };
+  const int u1 = bdu ? 0 : 1, u0 = fdu ? 0 : -1, v1 = bdv ? 0 : 1, v0 = fdv ? 0 : -1;
+  const double wu = (bdu || fdu) ? 1.0 : 0.5, wv = (bdv || fdv) ? 1.0 : 0.5;
+  const double dm = (1. / 16.) * (wu * wv) * (((Nsel(u1, v1) + Nsel(u0, v0)) - Nsel(u0, v1)) - Nsel(u1, v0));
   T.dm = dm;
   return T;
 }
