@@ -16,11 +16,23 @@
 
 namespace cup3d {
 
+// Star-shaped lab: the 8^3 block followed by its six face slabs of G layers
+// (edges and corners are never read by the star stencils, so they are not
+// stored).  Slab f (0..5 = -x,+x,-y,+y,-z,+z), layer l (1..G) holds
+// face-local cells (a, bb) (tangential coordinates in increasing dimension
+// order) at 512 + (f*G + l-1)*64 + a + 8*bb.
 template <int G>
 struct LabGeom {
-  static constexpr int W = BS + 2 * G;
-  static constexpr int V = W * W * W;
-  __device__ static __forceinline__ int at(int x, int y, int z) { return (x + G) + W * ((y + G) + W * (z + G)); }
+  static constexpr int V = BN + 6 * G * BS * BS;
+  __device__ static __forceinline__ int at(int x, int y, int z) {
+    if (x < 0) return BN + (0 * G - 1 - x) * 64 + y + 8 * z;
+    if (x >= BS) return BN + (1 * G + x - BS) * 64 + y + 8 * z;
+    if (y < 0) return BN + (2 * G - 1 - y) * 64 + x + 8 * z;
+    if (y >= BS) return BN + (3 * G + y - BS) * 64 + x + 8 * z;
+    if (z < 0) return BN + (4 * G - 1 - z) * 64 + x + 8 * y;
+    if (z >= BS) return BN + (5 * G + z - BS) * 64 + x + 8 * y;
+    return x + BS * y + BS * BS * z;
+  }
 };
 
 __device__ __forceinline__ void lagrange3(double xi, double w[3]) {

@@ -77,7 +77,7 @@ __device__ __forceinline__ void face_lab_pair(int d, int s, int a, int bb, int q
 }
 
 template <int SCHEME>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 3)
     k_advect_stage(DevMesh M, const double* __restrict__ vin, double* __restrict__ vout, double* tmpV, double dt,
                    double nu, Vec3 ui, int stage) {
   extern __shared__ double smem[];
