@@ -24,6 +24,29 @@ inline int tan1(int d) { return d == 0 ? 1 : 0; }
 inline int tan2(int d) { return d == 2 ? 1 : 2; }
 inline int cell(int x, int y, int z) { return x + BS * y + BS * BS * z; }
 
+// Sum of term(i), i < n, in an order that does not depend on the thread
+// count or on scheduling: fixed chunks summed in parallel, chunk sums added
+// serially in chunk order.  (An OpenMP reduction combines the threads'
+// partials in arrival order, so its last bits vary from run to run, and
+// BiCGSTAB's iteration count with them where the restart test or the
+// stopping test is close.)
+template <class F>
+double det_sum(int64_t n, F term) {
+  constexpr int64_t C = 4096;
+  const int64_t nc = (n + C - 1) / C;
+  std::vector<double> part(size_t(std::max<int64_t>(nc, 1)), 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t c = 0; c < nc; ++c) {
+    double s = 0;
+    const int64_t e = std::min(n, (c + 1) * C);
+    for (int64_t i = c * C; i < e; ++i) s += term(i);
+    part[size_t(c)] = s;
+  }
+  double s = 0;
+  for (int64_t c = 0; c < nc; ++c) s += part[size_t(c)];
+  return s;
+}
+
 }  // namespace
 
 struct orc_mesh {
@@ -391,12 +414,12 @@ void apply_A(orc_mesh* m, int mc, const double* x, double* y) {
     y[r] = s;
   }
   if (mc == 1 || mc == 2) {
-    double avg = 0;
-#pragma omp parallel for reduction(+ : avg) schedule(static)
-    for (int b = 0; b < m->nb; ++b) {
+    const double avg = det_sum(m->nb, [&](int64_t b) {
       const double h3 = m->h[b] * m->h[b] * m->h[b];
-      for (int i = 0; i < BN; ++i) avg += x[int64_t(b) * BN + i] * h3;
-    }
+      double s = 0;
+      for (int i = 0; i < BN; ++i) s += x[b * BN + i] * h3;
+      return s;
+    });
     if (mc == 1) {
       if (m->mean_block >= 0) y[int64_t(m->mean_block) * BN] = avg;
     } else {
@@ -557,10 +580,7 @@ struct Precond {
 };
 
 double dot(const double* a, const double* b, int64_t n) {
-  double s = 0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-  for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
-  return s;
+  return det_sum(n, [&](int64_t i) { return a[i] * b[i]; });
 }
 }  // namespace
 
@@ -684,9 +704,8 @@ extern "C" int orc_bicgstab_pipelined(orc_mesh* m, int mc, int precond, const do
   int restarts = 0, k;
   bool converged = false;
   for (k = 0; k < max_iter; ++k) {
-    double qy = 0, yy = 0;
     if (k % 50 != 0) {
-#pragma omp parallel for reduction(+ : qy, yy)
+#pragma omp parallel for
       for (int64_t j = 0; j < N; ++j) {
         phat[j] = rhat[j] + beta * (phat[j] - omega * shat[j]);
         s[j] = w[j] + beta * (s[j] - omega * z[j]);
@@ -695,8 +714,6 @@ extern "C" int orc_bicgstab_pipelined(orc_mesh* m, int mc, int precond, const do
         q[j] = r[j] - alpha * s[j];
         qhat[j] = rhat[j] - alpha * shat[j];
         y[j] = w[j] - alpha * z[j];
-        qy += q[j] * y[j];
-        yy += y[j] * y[j];
       }
     } else {
 #pragma omp parallel for
@@ -704,34 +721,24 @@ extern "C" int orc_bicgstab_pipelined(orc_mesh* m, int mc, int precond, const do
       apply_A(m, mc, phat.data(), s.data());
       M.apply(s.data(), shat.data());
       apply_A(m, mc, shat.data(), z.data());
-#pragma omp parallel for reduction(+ : qy, yy)
+#pragma omp parallel for
       for (int64_t j = 0; j < N; ++j) {
         q[j] = r[j] - alpha * s[j];
         qhat[j] = rhat[j] - alpha * shat[j];
         y[j] = w[j] - alpha * z[j];
-        qy += q[j] * y[j];
-        yy += y[j] * y[j];
       }
     }
+    const double qy = dot(q.data(), y.data(), N), yy = dot(y.data(), y.data(), N);
     M.apply(z.data(), zhat.data());
     apply_A(m, mc, zhat.data(), v.data());
     omega = qy / (yy + eps);
-    double r0r = 0, r0w = 0, r0s = 0, r0z = 0, norm_1 = 0, norm_2 = 0;
-    norm = 0;
     if (k % 50 != 0) {
-#pragma omp parallel for reduction(+ : r0r, r0w, r0s, r0z, norm_1, norm_2, norm)
+#pragma omp parallel for
       for (int64_t j = 0; j < N; ++j) {
         x[j] = x[j] + alpha * phat[j] + omega * qhat[j];
         r[j] = q[j] - omega * y[j];
         rhat[j] = qhat[j] - omega * (what[j] - alpha * zhat[j]);
         w[j] = y[j] - omega * (t[j] - alpha * v[j]);
-        r0r += r0[j] * r[j];
-        r0w += r0[j] * w[j];
-        r0s += r0[j] * s[j];
-        r0z += r0[j] * z[j];
-        norm += r[j] * r[j];
-        norm_1 += r[j] * r[j];
-        norm_2 += r0[j] * r0[j];
       }
     } else {
 #pragma omp parallel for
@@ -741,17 +748,11 @@ extern "C" int orc_bicgstab_pipelined(orc_mesh* m, int mc, int precond, const do
       for (int64_t j = 0; j < N; ++j) r[j] = b[j] - r[j];
       M.apply(r.data(), rhat.data());
       apply_A(m, mc, rhat.data(), w.data());
-#pragma omp parallel for reduction(+ : r0r, r0w, r0s, r0z, norm_1, norm_2, norm)
-      for (int64_t j = 0; j < N; ++j) {
-        r0r += r0[j] * r[j];
-        r0w += r0[j] * w[j];
-        r0s += r0[j] * s[j];
-        r0z += r0[j] * z[j];
-        norm += r[j] * r[j];
-        norm_1 += r[j] * r[j];
-        norm_2 += r0[j] * r0[j];
-      }
     }
+    const double r0r = dot(r0.data(), r.data(), N), r0w = dot(r0.data(), w.data(), N);
+    const double r0s = dot(r0.data(), s.data(), N), r0z = dot(r0.data(), z.data(), N);
+    const double norm_1 = dot(r.data(), r.data(), N), norm_2 = dot(r0.data(), r0.data(), N);
+    norm = norm_1;
     M.apply(w.data(), what.data());
     apply_A(m, mc, what.data(), t.data());
     norm = std::sqrt(norm);
@@ -1402,15 +1403,18 @@ extern "C" void orc_pressure_project(orc_mesh* m, double* vel, double* pres, con
   else
     orc_bicgstab_pipelined(m, mc, 1, lhs.data(), pres, tol, tol_rel, 1000, stats);
   // zero mean (:404-431) and incremental pressure (:435-446)
-  double avg = 0, avg1 = 0;
-#pragma omp parallel for reduction(+ : avg, avg1) schedule(static)
-  for (int b = 0; b < m->nb; ++b) {
+  double avg = det_sum(m->nb, [&](int64_t b) {
     const double vv = m->h[b] * m->h[b] * m->h[b];
-    for (int i = 0; i < BN; ++i) {
-      avg += pres[int64_t(b) * BN + i] * vv;
-      avg1 += vv;
-    }
-  }
+    double s = 0;
+    for (int i = 0; i < BN; ++i) s += pres[b * BN + i] * vv;
+    return s;
+  });
+  const double avg1 = det_sum(m->nb, [&](int64_t b) {
+    const double vv = m->h[b] * m->h[b] * m->h[b];
+    double s = 0;
+    for (int i = 0; i < BN; ++i) s += vv;
+    return s;
+  });
   avg = avg / avg1;
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < nbn; ++i) pres[i] -= avg;

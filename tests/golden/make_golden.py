@@ -12,7 +12,7 @@ values, and the GPU tests compare the device path against the same values:
 * poisson_<case>.npz  y = A x (mean constraint 1) and z = P_inv x for a seeded x:
                       norms and 512 sampled entries; a solve to 1e-10: iterations,
                       solution norm and samples;
-* tgv32_steps.npz     configs[0] (Taylor-Green 32^3, nu 0.01, CFL 0.3, upwind5,
+* tgv32_steps.npz     the Taylor-Green case (32^3, nu 0.01, CFL 0.3, upwind5,
                       Poisson to 1e-11): dt and velocity samples/norms after 1..4 steps.
 """
 from __future__ import annotations

@@ -9,7 +9,7 @@ import oracle
 
 # name -> (flags, generator)
 CASES = {
-    # configs[0]: Taylor-Green, 4x4x4 blocks of 8^3, triply periodic
+    # Taylor-Green, 4x4x4 blocks of 8^3, triply periodic
     "tgv32": ("-bpdx 4 -bpdy 4 -bpdz 4 -levelMax 1 -extent 6.283185307179586 "
               "-BC_x periodic -BC_y periodic -BC_z periodic", ("uniform",)),
     # 2-level random AMR, free-space boundaries

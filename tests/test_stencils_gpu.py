@@ -108,7 +108,7 @@ def test_pressure_project_matches_oracle(name, step):
 
 
 def test_tgv_steps_match_oracle():
-    # u = sin x cos y cos z, v = -cos x sin y cos z, w = 0 on [0,2pi]^3,
+    # Taylor-Green: u = sin x cos y cos z, v = -cos x sin y cos z, w = 0 on [0,2pi]^3,
     # nu = 0.01, CFL 0.3, upwind5, FP64; Poisson converged tightly on both sides
     flags = "-nu 0.01 -CFL 0.3 -rampup 0 -poissonTol 0 -poissonTolRel 1e-11"
     ctx = make_ctx("tgv32", device=0, extra=flags)
