@@ -172,6 +172,9 @@ __device__ __forceinline__ bool grid_reduce_max(double& v, const GridReduce& g, 
 // totals and no CTA has to publish them.  The wait is bounded: after about a
 // second of polling a waiter sets *error and returns false, so a barrier that
 // can never complete ends the kernel instead of hanging the device.
+// Ordering: the CTA's stores precede its arrival through the CTA barrier and
+// the arrival's release; the waiter's acquire load and the CTA barrier after
+// it order every later load of the CTA behind all arrivals it has seen.
 // ---------------------------------------------------------------------------
 struct GridSync {
   unsigned int* arrive;  // arrivals since the launch (zero before it)
@@ -180,6 +183,16 @@ struct GridSync {
 };
 
 constexpr long long kBarrierClockLimit = 1ll << 31;  // SM clock cycles, about 1 s
+
+// GPU-scope release add (no result) and acquire load.
+__device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 
 // epoch: the number of barriers this CTA has passed (shared, zero at launch)
 template <int NR>
@@ -192,13 +205,11 @@ __device__ bool grid_allreduce(double (&v)[NR], const GridSync& G, unsigned int&
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int r = 0; r < NR; ++r) part[blockIdx.x * 8 + r] = v[r];
-    __threadfence();
-    atomicAdd(G.arrive, 1u);
+    red_add_release(G.arrive, 1u);
     const unsigned int target = (k + 1u) * gridDim.x;
-    volatile unsigned int* a = G.arrive;
     const long long t0 = clock64();
     int ok = 1;
-    while (*a < target) {
+    while (ld_acquire(G.arrive) < target) {
       if (clock64() - t0 > kBarrierClockLimit) {
         ok = 0;
         break;
@@ -207,7 +218,6 @@ __device__ bool grid_allreduce(double (&v)[NR], const GridSync& G, unsigned int&
     if (!ok) atomicExch(G.error, 1);
     s_ok = ok;
     epoch = k + 1u;
-    __threadfence();
   }
   __syncthreads();
   if (!s_ok) return false;

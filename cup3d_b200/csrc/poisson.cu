@@ -11,8 +11,10 @@
 //     applied by fast diagonalization (three DST-I mode products each way)
 //     rather than a 512x512 DGEMM: the same matrix, 96 instead of 1024 flop/cell;
 //   * solver: BiCGSTABSolver::main (BiCGSTAB.cu:416-628) with the same
-//     scalars, restart rule and best-iterate return, but five fused kernels
-//     per iteration and no host round trip inside an iteration.
+//     scalars, restart rule and best-iterate return, all iterations in one
+//     cooperative launch with three grid barriers per iteration (five fused
+//     kernels per iteration where a network preconditioner runs between
+//     them) and no host round trip inside a solve.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -746,11 +748,177 @@ __global__ void __launch_bounds__(NT) k_bicg_e(KArgs<T> A) {
   if (grid_reduce<2>(acc, A.g, red) && threadIdx.x == 0) fin_e(*A.st, acc);
 }
 
-// ---- persistent solver: all iterations in one cooperative launch ----------
+// ---- persistent solver: three grid barriers per iteration -----------------
+// The same iteration as the five phases above, reorganised by the linearity
+// of the block preconditioner M^-1 so that the two halo exchanges coincide
+// with reductions.  With zr = M^-1 r, zv = M^-1 nu and q = z1 - omega zv:
+//   z1 = M^-1 p  = zr + beta q     (p = r + beta (p - omega nu))
+//   z2 = M^-1 s  = zr - alpha zv   (s = r - alpha nu)
+// so the operator's inputs z1 and z2 are formed at the point of use from
+// vectors that the previous phase finished before its barrier.  Per
+// iteration:
+//   P1: nu = A (zr + beta q); zv = M^-1 nu; (rhat, nu), sum(zv h^3)
+//   P2: t = A (zr - alpha zv); s = r - alpha nu; (t, s), (t, t)
+//   P3: x += alpha z1 + omega z2; r = s - omega t; q = z1 - omega zv;
+//       zr = M^-1 r; (rhat, r), (r, r), sum(zr h^3), sum(q h^3)
+// p and s are never stored.  Buffers: zr in z1, zv in z2, q in p.  Every
+// vector a phase reads from other blocks (zr, q in P1; zr, zv in P2) is
+// written only in another phase, so no phase needs a second buffer.  The
+// scalars, the restart rule and the stopping tests are fin_a..fin_e's.
+// ---------------------------------------------------------------------------
+template <class T>
+struct Comb2At {  // a + c b
+  const T* a;
+  const T* b;
+  double c;
+  __device__ __forceinline__ double operator()(size_t i) const {
+    return double(ld_stream(a + i)) + c * double(ld_stream(b + i));
+  }
+};
+
+// P0 (once): zr = M^-1 r for the initial residual; sum(zr h^3)
+template <class T>
+__device__ __forceinline__ double phase_p0(const KArgs<T>& A, const GroupIdx& G, FdTile& tile, const double* inv) {
+  const DevMesh& M = A.M;
+  double acc = 0.0;
+  GROUP_BLOCKS(b) {
+    double c[8];
+    load_col(A.r, b, G, c);
+    const double h = M.h[b];
+    block_inverse_group(c, tile, G, h, inv);
+    double s = 0.0;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      c[z] = double(T(c[z]));
+      s += c[z];
+    }
+    store_col(A.z1, b, G, c);
+    acc += s * h * h * h;
+  }
+  return acc;
+}
+
+// P1: z1 = zr + beta q (beta = 0 after a restart, which also sets rhat = r);
+//     nu = A z1; zv = M^-1 nu; (rhat, nu), sum(zv h^3)
+template <class T>
+__device__ __forceinline__ void phase_p1(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, const double* inv,
+                                         double beta, double ms, bool restart, double (&acc)[2]) {
+  const DevMesh& M = A.M;
+  FdTile& ftile = reinterpret_cast<FdTile&>(tile);
+  const Comb2At<T> z1{A.z1, A.p, beta};
+  GROUP_BLOCKS(b) {
+    double col[8], y[8], rh[8];
+    {
+      double zr[8], q[8];
+      load_col(A.z1, b, G, zr);
+      load_col(A.p, b, G, q);
+#pragma unroll
+      for (int z = 0; z < 8; ++z) col[z] = zr[z] + beta * q[z];
+    }
+    spmv_group(M, b, z1, col, ms, A.mean_mode, tile, G, y);
+    if (restart) {
+      load_col(A.r, b, G, rh);
+      store_col(A.rhat, b, G, rh);
+    } else {
+      load_col(A.rhat, b, G, rh);
+    }
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      y[z] = double(T(y[z]));
+      acc[0] += rh[z] * y[z];
+    }
+    store_col(A.nu, b, G, y);
+    const double h = M.h[b];
+    block_inverse_group(y, ftile, G, h, inv);
+    double s = 0.0;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      y[z] = double(T(y[z]));
+      s += y[z];
+    }
+    store_col(A.z2, b, G, y);
+    acc[1] += s * h * h * h;
+  }
+}
+
+// P2: t = A (zr - alpha zv); s = r - alpha nu; (t, s), (t, t)
+template <class T>
+__device__ __forceinline__ void phase_p2(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, double alpha,
+                                         double ms, double (&acc)[2]) {
+  const DevMesh& M = A.M;
+  const Comb2At<T> z2{A.z1, A.z2, -alpha};
+  GROUP_BLOCKS(b) {
+    double col[8], y[8];
+    {
+      double zr[8], zv[8];
+      load_col(A.z1, b, G, zr);
+      load_col(A.z2, b, G, zv);
+#pragma unroll
+      for (int z = 0; z < 8; ++z) col[z] = zr[z] - alpha * zv[z];
+    }
+    spmv_group(M, b, z2, col, ms, A.mean_mode, tile, G, y);
+    double r[8], nu[8];
+    load_col(A.r, b, G, r);
+    load_col(A.nu, b, G, nu);
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      y[z] = double(T(y[z]));
+      const double sv = double(T(r[z] - alpha * nu[z]));
+      acc[0] += y[z] * sv;
+      acc[1] += y[z] * y[z];
+    }
+    store_col(A.t, b, G, y);
+  }
+}
+
+// P3: x_new = x + alpha z1 + omega z2; r = s - omega t; q = z1 - omega zv;
+//     zr = M^-1 r; (rhat, r), (r, r), sum(zr h^3), sum(q h^3)
+template <class T>
+__device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, FdTile& tile, const double* inv,
+                                         const T* xc, T* xn, double alpha, double beta, double omega,
+                                         double (&acc)[4]) {
+  const DevMesh& M = A.M;
+  GROUP_BLOCKS(b) {
+    const size_t o = size_t(b) * BN + G.gy * 8 + G.gx;
+    double rn[8], sq = 0.0;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      const size_t i = o + z * 64;
+      const double zr = double(ld_stream(A.z1 + i)), q = double(ld_stream(A.p + i));
+      const double zv = double(ld_stream(A.z2 + i)), x = double(ld_stream(xc + i));
+      const double r = double(ld_stream(A.r + i)), nu = double(ld_stream(A.nu + i));
+      const double t = double(ld_stream(A.t + i)), rh = double(ld_stream(A.rhat + i));
+      const double z1 = zr + beta * q, z2 = zr - alpha * zv;
+      const double sv = double(T(r - alpha * nu));
+      const T xo = T((x + alpha * z1) + omega * z2);
+      const T ro = T(sv - omega * t);
+      const T qo = T(z1 - omega * zv);
+      xn[i] = xo;
+      A.r[i] = ro;
+      A.p[i] = qo;
+      rn[z] = double(ro);
+      acc[0] += rh * rn[z];
+      acc[1] += rn[z] * rn[z];
+      sq += double(qo);
+    }
+    const double h = M.h[b], h3 = h * h * h;
+    block_inverse_group(rn, tile, G, h, inv);
+    double s = 0.0;
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      rn[z] = double(T(rn[z]));
+      s += rn[z];
+    }
+    store_col(A.z1, b, G, rn);
+    acc[2] += s * h3;
+    acc[3] += sq * h3;
+  }
+}
+
 // Every CTA keeps a copy of the Krylov state in shared memory and applies
 // the finalizers to the grid totals of each phase, so all copies stay equal;
 // CTA 0 writes the state back at the end.  Data written by other CTAs is read
-// after the grid barrier's acquire fence, with loads that bypass L1.
+// after the grid barrier's acquire, with loads that bypass L1.
 template <class T>
 __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync Gs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -758,6 +926,7 @@ __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync 
   double* inv_eig = reinterpret_cast<double*>(smem_raw + GROUPS * sizeof(GroupTile));
   __shared__ double red[64];
   __shared__ KrylovState S;
+  __shared__ double ms_zr;  // sum(zr h^3) of the current zr
   __shared__ unsigned int epoch;
   const GroupIdx G;
   GroupTile& tile = tiles[G.g];
@@ -769,29 +938,41 @@ __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync 
   }
   __syncthreads();
   bool ok = true;
+  if (!S.done) {
+    double a[1] = {phase_p0<T>(A, G, ftile, inv_eig)};
+    ok = grid_allreduce<1>(a, Gs, epoch, red);
+    // q = 0 at the start (p of k_bicg_init), so z1 = zr
+    if (threadIdx.x == 0) ms_zr = S.mean_sum = a[0];
+    __syncthreads();
+  }
   while (ok && !S.done) {
     const bool restart = S.restart_pending != 0;
-    double a[1] = {phase_a<T>(A, G, ftile, inv_eig, S.beta, S.omega, restart)};
-    if (!(ok = grid_allreduce<1>(a, Gs, epoch, red))) break;
-    if (threadIdx.x == 0) fin_a(S, a[0], restart);
-    __syncthreads();
-    double b[1] = {phase_b<T>(A, G, tile, S.mean_sum)};
-    if (!(ok = grid_allreduce<1>(b, Gs, epoch, red))) break;
-    if (threadIdx.x == 0) fin_b(S, b[0]);
-    __syncthreads();
-    double c[1] = {phase_c<T>(A, G, ftile, inv_eig, S.alpha)};
-    if (!(ok = grid_allreduce<1>(c, Gs, epoch, red))) break;
-    if (threadIdx.x == 0) fin_c(S, c[0]);
+    const double beta = restart ? 0.0 : S.beta;
+    double a[2] = {0.0, 0.0};
+    phase_p1<T>(A, G, tile, inv_eig, beta, S.mean_sum, restart, a);
+    if (!(ok = grid_allreduce<2>(a, Gs, epoch, red))) break;
+    if (threadIdx.x == 0) {
+      fin_a(S, S.mean_sum, restart);
+      fin_b(S, a[0]);
+      S.beta = beta;                        // the beta that formed z1, for P3
+      S.mean_sum = ms_zr - S.alpha * a[1];  // sum(z2 h^3)
+    }
     __syncthreads();
     double d[2] = {0.0, 0.0};
-    phase_d<T>(A, G, tile, S.mean_sum, d);
+    phase_p2<T>(A, G, tile, S.alpha, S.mean_sum, d);
     if (!(ok = grid_allreduce<2>(d, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_d(S, d);
     __syncthreads();
-    double e[2] = {0.0, 0.0};
-    phase_e<T>(A, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.omega, e);
-    if (!(ok = grid_allreduce<2>(e, Gs, epoch, red))) break;
-    if (threadIdx.x == 0) fin_e(S, e);
+    double e[4] = {0.0, 0.0, 0.0, 0.0};
+    phase_p3<T>(A, G, ftile, inv_eig, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.beta, S.omega, e);
+    if (!(ok = grid_allreduce<4>(e, Gs, epoch, red))) break;
+    if (threadIdx.x == 0) {
+      const double re[2] = {e[0], e[1]};
+      fin_e(S, re);
+      ms_zr = e[2];
+      // sum(z1 h^3) of the next P1
+      S.mean_sum = S.restart_pending ? e[2] : e[2] + S.beta * e[3];
+    }
     __syncthreads();
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
