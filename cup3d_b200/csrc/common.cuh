@@ -77,12 +77,14 @@ __device__ __forceinline__ void block_reduce(double (&v)[NR], double* sm /* >= 8
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
-// Load through L2 only (ld.global.cg).  Kernels whose CTAs read data that
-// other CTAs of the same launch wrote (after a grid barrier) use it, since
-// L1 is not coherent across SMs.
+// Plain (weak, L1-cached) load of solver vectors.  Within a launch, data
+// that other CTAs wrote before a grid barrier is read only after the
+// barrier's acquire and the CTA barrier behind it; the memory model orders
+// these weak loads after the writes, so they may hit L1 (halo values that
+// neighbouring blocks on the same SM read again) and still see fresh data.
 template <class V>
 __device__ __forceinline__ V ld_stream(const V* p) {
-  return __ldcg(p);
+  return *p;
 }
 
 struct GridReduce {

@@ -879,27 +879,37 @@ __device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, F
                                          double (&acc)[4]) {
   const DevMesh& M = A.M;
   GROUP_BLOCKS(b) {
-    const size_t o = size_t(b) * BN + G.gy * 8 + G.gx;
     double rn[8], sq = 0.0;
+    {
+      double r[8], nu[8], t[8], rh[8];
+      load_col(A.r, b, G, r);
+      load_col(A.nu, b, G, nu);
+      load_col(A.t, b, G, t);
+      load_col(A.rhat, b, G, rh);
 #pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      const size_t i = o + z * 64;
-      const double zr = double(ld_stream(A.z1 + i)), q = double(ld_stream(A.p + i));
-      const double zv = double(ld_stream(A.z2 + i)), x = double(ld_stream(xc + i));
-      const double r = double(ld_stream(A.r + i)), nu = double(ld_stream(A.nu + i));
-      const double t = double(ld_stream(A.t + i)), rh = double(ld_stream(A.rhat + i));
-      const double z1 = zr + beta * q, z2 = zr - alpha * zv;
-      const double sv = double(T(r - alpha * nu));
-      const T xo = T((x + alpha * z1) + omega * z2);
-      const T ro = T(sv - omega * t);
-      const T qo = T(z1 - omega * zv);
-      xn[i] = xo;
-      A.r[i] = ro;
-      A.p[i] = qo;
-      rn[z] = double(ro);
-      acc[0] += rh * rn[z];
-      acc[1] += rn[z] * rn[z];
-      sq += double(qo);
+      for (int z = 0; z < 8; ++z) {
+        const double sv = double(T(r[z] - alpha * nu[z]));
+        rn[z] = double(T(sv - omega * t[z]));
+        acc[0] += rh[z] * rn[z];
+        acc[1] += rn[z] * rn[z];
+      }
+      store_col(A.r, b, G, rn);
+    }
+    {
+      double zr[8], q[8], zv[8], x[8];
+      load_col(A.z1, b, G, zr);
+      load_col(A.p, b, G, q);
+      load_col(A.z2, b, G, zv);
+      load_col(xc, b, G, x);
+#pragma unroll
+      for (int z = 0; z < 8; ++z) {
+        const double z1 = zr[z] + beta * q[z], z2 = zr[z] - alpha * zv[z];
+        x[z] = double(T((x[z] + alpha * z1) + omega * z2));
+        q[z] = double(T(z1 - omega * zv[z]));
+        sq += q[z];
+      }
+      store_col(xn, b, G, x);
+      store_col(A.p, b, G, q);
     }
     const double h = M.h[b], h3 = h * h * h;
     block_inverse_group(rn, tile, G, h, inv);
