@@ -52,6 +52,7 @@ class cup_config(C.Structure):
         ("poisson_max_restarts", C.c_int32),
         ("step_2nd_start", C.c_int32),
         ("device", C.c_int32),
+        ("poisson_block_cache", C.c_int32),
     ]
 
 

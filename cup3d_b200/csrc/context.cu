@@ -190,6 +190,7 @@ void cup_config_default(cup_config* c) {
   c->poisson_max_restarts = 100;
   c->step_2nd_start = 2;
   c->device = 0;
+  c->poisson_block_cache = 4;
 }
 
 static int parse_bc(const std::string& v) {
@@ -263,6 +264,10 @@ int cup_config_parse(cup_config* c, const char* args) {
     } else if (key == "device") {
       if (need_num()) return CUP_ERR_ARG;
       c->device = int(dv);
+    } else if (key == "poissonBlockCache") {
+      if (need_num()) return CUP_ERR_ARG;
+      if (dv < 0 || dv > 4) return ctx_fail(nullptr, CUP_ERR_ARG, "poissonBlockCache must be 0-4");
+      c->poisson_block_cache = int(dv);
     } else {
       return ctx_fail(nullptr, CUP_ERR_ARG, "unknown flag " + k);
     }
@@ -505,6 +510,7 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   P.check_every = 8;
   P.stall_window = 0;
   P.persistent = 1;
+  P.block_cache = c->cfg.poisson_block_cache;
   SolveStats S{};
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   int rc = 0;

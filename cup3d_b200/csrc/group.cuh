@@ -32,14 +32,28 @@ struct FdTile {
   double v[BS][BS][BS + 1];  // [z][y][x]
 };
 
+// A block's entries of the mesh tables, staged in shared memory so that the
+// operator reads them without a global-memory round trip.
+struct BlockInfo {
+  int kind[6];   // face kinds (K_SAME, ...)
+  int nbr[24];   // face neighbours, four per face (fnbr row)
+  double h;      // grid spacing; finer neighbours have h/2, coarser 2h
+  int id;        // block index
+  int par;       // bit e: parity of the block's index along axis e
+  int mean;      // 1: the block holds the mean-constraint row
+  int pad_;
+};
+
 // Shared tile of one block for the operator: the block, its x/y face halos,
 // the face layers of coarser neighbours and the coarse-fine fluxes of x/y
-// faces (face-local index tan1 + 8 tan2 in every per-face array).
+// faces (face-local index tan1 + 8 tan2 in every per-face array), and the
+// block's table entries.  The transforms' FdTile aliases the leading member.
 struct GroupTile {
   double v[BS][BS][BS + 1];  // [z][y][x]
   double hal[4][BS * BS];    // -x, +x, -y, +y same-level neighbour layers
   double cl[6][BS * BS];     // per coarser face: the coarse block's layer on that face
   double flx[4][BS * BS];    // x/y coarse-fine face fluxes
+  BlockInfo bi;
 };
 
 // Orthogonal, symmetric DST-I of size 8: S(n,k) = sqrt(2/9) sin(pi (n+1)(k+1)/9).

@@ -108,21 +108,37 @@ struct VecAt {
   __device__ __forceinline__ double operator()(size_t i) const { return double(ld_stream(v + i)); }
 };
 
+// Group-cooperative copy of block b's table entries into bi (the caller
+// synchronises the group before reading it).
+__device__ __forceinline__ void fill_block_info(const DevMesh& M, int b, BlockInfo& bi, int lane) {
+  if (lane < 6) {
+    bi.kind[lane] = M.fkind[b * 6 + lane];
+  } else if (lane < 30) {
+    bi.nbr[lane - 6] = M.fnbr[b * 24 + lane - 6];
+  } else if (lane == 30) {
+    bi.h = M.h[b];
+    bi.id = b;
+    bi.mean = b == M.mean_block ? 1 : 0;
+  } else if (lane == 31) {
+    bi.par = (M.index[b * 3] & 1) | ((M.index[b * 3 + 1] & 1) << 1) | ((M.index[b * 3 + 2] & 1) << 2);
+  }
+}
+
 // Flux across coarse-fine face f into face cell (a, bb) of block b
 // (PoissonSolverExp::makeFlux, PoissonSolverExp.cpp:157-219): the fine side
 // of a coarser face (coarse layer staged in tile.cl[f]), or the four fine
 // fluxes of a finer face (Taylor terms from the block's own layer).  Reads
 // the tile after the group barrier that follows its filling.
 template <class X>
-__device__ __forceinline__ double cf_flux(const DevMesh& M, int b, const X& x, const GroupTile& tile, int f,
-                                          int kind, int a, int bb) {
+__device__ __forceinline__ double cf_flux(const BlockInfo& bi, const X& x, const GroupTile& tile, int f, int kind,
+                                          int a, int bb) {
   const int d = f >> 1, s = f & 1;
   auto own = [&](int cell) { return tile.v[cell >> 6][(cell >> 3) & 7][cell & 7]; };
-  const double h = M.h[b];
+  const double h = bi.h;
   if (kind == K_COARSER) {
     const double* cl = tile.cl[f];
     auto L = [&](int u, int v) { return d == 1 ? cl[v + 8 * u] : cl[u + 8 * v]; };
-    const int h1 = M.index[b * 3 + tan1(d)] & 1, h2 = M.index[b * 3 + tan2(d)] & 1;
+    const int h1 = (bi.par >> tan1(d)) & 1, h2 = (bi.par >> tan2(d)) & 1;
     const int c1 = h1 * 4 + (a >> 1), c2 = h2 * 4 + (bb >> 1);
     const double sa = (a & 1) ? 1.0 : -1.0, sb = (bb & 1) ? 1.0 : -1.0;
     const TaylorTerms Tt = d == 1 ? cf_terms(L, c2, c1) : cf_terms(L, c1, c2);
@@ -132,8 +148,8 @@ __device__ __forceinline__ double cf_flux(const DevMesh& M, int b, const X& x, c
   }
   auto L = [&](int u, int v) { return d == 1 ? own(face_cell(d, s, 0, v, u)) : own(face_cell(d, s, 0, u, v)); };
   const TaylorTerms Tt = d == 1 ? cf_terms(L, bb, a) : cf_terms(L, a, bb);
-  const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
-  const double hf = M.h[ch];
+  const int ch = bi.nbr[4 * f + (a >> 2) + 2 * (bb >> 2)];
+  const double hf = 0.5 * h;  // h = h0 2^-level: exact
   const size_t xc = size_t(ch) * BN;
   double close[4], far[4];
 #pragma unroll
@@ -164,14 +180,13 @@ __device__ __forceinline__ void load_col(const T* __restrict__ v, int b, const G
 // each thread computes the flux of one face cell per face, owners add them.
 // Ends with a group barrier (tile free for reuse).
 template <class X>
-__device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const X& x, const double col[8], double ms,
+__device__ __forceinline__ void spmv_group(const BlockInfo& bi, const X& x, const double col[8], double ms,
                                            int mean_mode, GroupTile& tile, const GroupIdx& G, double y[8]) {
-  const int* fk = M.fkind + b * 6;
-  const int* fn = M.fnbr + b * 24;
+  const int* fn = bi.nbr;
   const int cxy = G.gy * 8 + G.gx;
   int kind[6];
 #pragma unroll
-  for (int f = 0; f < 6; ++f) kind[f] = fk[f];
+  for (int f = 0; f < 6; ++f) kind[f] = bi.kind[f];
   // z halo: same-level neighbour values, zero flux (own value) otherwise
   double zm = col[0], zp = col[7];
   if (kind[4] == K_SAME) zm = x(size_t(fn[16]) * BN + 7 * 64 + cxy);
@@ -195,9 +210,9 @@ __device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const X& x, 
   if (cf) {                      // uniform per block
 #pragma unroll 1
     for (int f = 0; f < 6; ++f) {
-      const int kf = fk[f];
+      const int kf = bi.kind[f];
       if (kf < K_COARSER) continue;
-      const double fl = cf_flux(M, b, x, tile, f, kf, G.gx, G.gy);
+      const double fl = cf_flux(bi, x, tile, f, kf, G.gx, G.gy);
       if (f < 4)
         tile.flx[f][G.lane] = fl;
       else if (f == 4)
@@ -207,7 +222,7 @@ __device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const X& x, 
     }
     group_sync(G.g);
   }
-  const double h = M.h[b];
+  const double h = bi.h;
   // x/y neighbours: in the tile, or in the halo on the block's faces (one
   // shared load per neighbour through a selected base and z stride)
   constexpr int ZS = BS * (BS + 1);
@@ -248,7 +263,7 @@ __device__ __forceinline__ void spmv_group(const DevMesh& M, int b, const X& x, 
       }
     }
   }
-  if (b == M.mean_block && G.lane == 0) {
+  if (bi.mean && G.lane == 0) {
     if (mean_mode == 1) y[0] = ms;
     if (mean_mode == 3) y[0] = h * col[0];
   }
@@ -301,7 +316,9 @@ __global__ void __launch_bounds__(NT) k_spmv(DevMesh M, const double* __restrict
   GROUP_BLOCKS(b) {
     double col[8], out[8];
     load_col(x, b, G, col);
-    spmv_group(M, b, VecAt<double>{x}, col, ms, mean_mode, tiles[G.g], G, out);
+    fill_block_info(M, b, tiles[G.g].bi, G.lane);
+    group_sync(G.g);
+    spmv_group(tiles[G.g].bi, VecAt<double>{x}, col, ms, mean_mode, tiles[G.g], G, out);
     double* yb = y + size_t(b) * BN + G.gy * 8 + G.gx;
 #pragma unroll
     for (int z = 0; z < 8; ++z) yb[z * 64] = out[z];
@@ -349,6 +366,7 @@ struct KArgs {
   int mean_mode;
   int zero_mean_row;  // b and x0 are zero at the mean row (getVec, modes 1 and 3)
   int ext_precond;    // 1: kernels a and c only update p and s; a separate kernel applies the preconditioner
+  int ncache;         // persistent solver: block entries staged per group at launch (<= KB_CACHE)
 };
 
 template <class T>
@@ -410,7 +428,9 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
   GROUP_BLOCKS(b) {
     double col[8], y[8], bc[8];
     load_col(A.xs0, b, G, col);
-    spmv_group(M, b, VecAt<T>{A.xs0}, col, ms, A.mean_mode, tiles[G.g], G, y);
+    fill_block_info(M, b, tiles[G.g].bi, G.lane);
+    group_sync(G.g);
+    spmv_group(tiles[G.g].bi, VecAt<T>{A.xs0}, col, ms, A.mean_mode, tiles[G.g], G, y);
     load_col(A.b, b, G, bc);
     if (A.zero_mean_row && b == M.mean_block && G.lane == 0) bc[0] = 0.0;
     double r[8], zero[8];
@@ -520,7 +540,9 @@ __device__ __forceinline__ double phase_b(const KArgs<T>& A, const GroupIdx& G, 
   GROUP_BLOCKS(b) {
     double col[8], y[8], rh[8];
     load_col(A.z1, b, G, col);
-    spmv_group(M, b, VecAt<T>{A.z1}, col, ms, A.mean_mode, tile, G, y);
+    fill_block_info(M, b, tile.bi, G.lane);
+    group_sync(G.g);
+    spmv_group(tile.bi, VecAt<T>{A.z1}, col, ms, A.mean_mode, tile, G, y);
     load_col(A.rhat, b, G, rh);
 #pragma unroll
     for (int z = 0; z < 8; ++z) {
@@ -572,7 +594,9 @@ __device__ __forceinline__ void phase_d(const KArgs<T>& A, const GroupIdx& G, Gr
   GROUP_BLOCKS(b) {
     double col[8], y[8], sv[8];
     load_col(A.z2, b, G, col);
-    spmv_group(M, b, VecAt<T>{A.z2}, col, ms, A.mean_mode, tile, G, y);
+    fill_block_info(M, b, tile.bi, G.lane);
+    group_sync(G.g);
+    spmv_group(tile.bi, VecAt<T>{A.z2}, col, ms, A.mean_mode, tile, G, y);
     load_col(A.r, b, G, sv);
 #pragma unroll
     for (int z = 0; z < 8; ++z) {
@@ -776,16 +800,39 @@ struct Comb2At {  // a + c b
   }
 };
 
+// Blocks of group g in the persistent solver: visit slots g + k G_total of
+// the mesh's visit order (G_total groups in the grid), the same in every
+// phase.  Their table entries for k < ncache (at most KB_CACHE) are staged in
+// shared memory at launch; later ones are staged in the group's tile on the
+// way.
+constexpr int KB_CACHE = 4;
+
+__device__ __forceinline__ const BlockInfo& persistent_block(const DevMesh& M, const BlockInfo* cache, int ncache,
+                                                             GroupTile& tile, int k, int slot, const GroupIdx& G) {
+  if (k < ncache) return cache[G.g * KB_CACHE + k];
+  group_sync(G.g);  // the group is done with the previous staged entry
+  fill_block_info(M, M.order ? M.order[slot] : slot, tile.bi, G.lane);
+  group_sync(G.g);
+  return tile.bi;
+}
+
+#define PERSISTENT_BLOCKS(bi)                                                                   \
+  for (int k_ = 0, slot_ = blockIdx.x * GROUPS + G.g; slot_ < M.nb; ++k_, slot_ += gridDim.x * GROUPS) \
+    if (const BlockInfo& bi = persistent_block(M, cache, A.ncache, tile, k_, slot_, G); true)
+
 // P0 (once): zr = M^-1 r for the initial residual; sum(zr h^3)
 template <class T>
-__device__ __forceinline__ double phase_p0(const KArgs<T>& A, const GroupIdx& G, FdTile& tile, const double* inv) {
+__device__ __forceinline__ double phase_p0(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
+                                           const BlockInfo* cache, const double* inv) {
   const DevMesh& M = A.M;
+  FdTile& ftile = reinterpret_cast<FdTile&>(tile);
   double acc = 0.0;
-  GROUP_BLOCKS(b) {
+  PERSISTENT_BLOCKS(bi) {
+    const int b = bi.id;
+    const double h = bi.h;
     double c[8];
     load_col(A.r, b, G, c);
-    const double h = M.h[b];
-    block_inverse_group(c, tile, G, h, inv);
+    block_inverse_group(c, ftile, G, h, inv);
     double s = 0.0;
 #pragma unroll
     for (int z = 0; z < 8; ++z) {
@@ -801,12 +848,15 @@ __device__ __forceinline__ double phase_p0(const KArgs<T>& A, const GroupIdx& G,
 // P1: z1 = zr + beta q (beta = 0 after a restart, which also sets rhat = r);
 //     nu = A z1; zv = M^-1 nu; (rhat, nu), sum(zv h^3)
 template <class T>
-__device__ __forceinline__ void phase_p1(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, const double* inv,
-                                         double beta, double ms, bool restart, double (&acc)[2]) {
+__device__ __forceinline__ void phase_p1(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
+                                         const BlockInfo* cache, const double* inv, double beta, double ms,
+                                         bool restart, double (&acc)[2]) {
   const DevMesh& M = A.M;
   FdTile& ftile = reinterpret_cast<FdTile&>(tile);
   const Comb2At<T> z1{A.z1, A.p, beta};
-  GROUP_BLOCKS(b) {
+  PERSISTENT_BLOCKS(bi) {
+    const int b = bi.id;
+    const double h = bi.h;
     double col[8], y[8], rh[8];
     {
       double zr[8], q[8];
@@ -815,7 +865,7 @@ __device__ __forceinline__ void phase_p1(const KArgs<T>& A, const GroupIdx& G, G
 #pragma unroll
       for (int z = 0; z < 8; ++z) col[z] = zr[z] + beta * q[z];
     }
-    spmv_group(M, b, z1, col, ms, A.mean_mode, tile, G, y);
+    spmv_group(bi, z1, col, ms, A.mean_mode, tile, G, y);
     if (restart) {
       load_col(A.r, b, G, rh);
       store_col(A.rhat, b, G, rh);
@@ -828,7 +878,6 @@ __device__ __forceinline__ void phase_p1(const KArgs<T>& A, const GroupIdx& G, G
       acc[0] += rh[z] * y[z];
     }
     store_col(A.nu, b, G, y);
-    const double h = M.h[b];
     block_inverse_group(y, ftile, G, h, inv);
     double s = 0.0;
 #pragma unroll
@@ -843,11 +892,12 @@ __device__ __forceinline__ void phase_p1(const KArgs<T>& A, const GroupIdx& G, G
 
 // P2: t = A (zr - alpha zv); s = r - alpha nu; (t, s), (t, t)
 template <class T>
-__device__ __forceinline__ void phase_p2(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, double alpha,
-                                         double ms, double (&acc)[2]) {
+__device__ __forceinline__ void phase_p2(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
+                                         const BlockInfo* cache, double alpha, double ms, double (&acc)[2]) {
   const DevMesh& M = A.M;
   const Comb2At<T> z2{A.z1, A.z2, -alpha};
-  GROUP_BLOCKS(b) {
+  PERSISTENT_BLOCKS(bi) {
+    const int b = bi.id;
     double col[8], y[8];
     {
       double zr[8], zv[8];
@@ -856,7 +906,7 @@ __device__ __forceinline__ void phase_p2(const KArgs<T>& A, const GroupIdx& G, G
 #pragma unroll
       for (int z = 0; z < 8; ++z) col[z] = zr[z] - alpha * zv[z];
     }
-    spmv_group(M, b, z2, col, ms, A.mean_mode, tile, G, y);
+    spmv_group(bi, z2, col, ms, A.mean_mode, tile, G, y);
     double r[8], nu[8];
     load_col(A.r, b, G, r);
     load_col(A.nu, b, G, nu);
@@ -874,11 +924,14 @@ __device__ __forceinline__ void phase_p2(const KArgs<T>& A, const GroupIdx& G, G
 // P3: x_new = x + alpha z1 + omega z2; r = s - omega t; q = z1 - omega zv;
 //     zr = M^-1 r; (rhat, r), (r, r), sum(zr h^3), sum(q h^3)
 template <class T>
-__device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, FdTile& tile, const double* inv,
-                                         const T* xc, T* xn, double alpha, double beta, double omega,
-                                         double (&acc)[4]) {
+__device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
+                                         const BlockInfo* cache, const double* inv, const T* xc, T* xn,
+                                         double alpha, double beta, double omega, double (&acc)[4]) {
   const DevMesh& M = A.M;
-  GROUP_BLOCKS(b) {
+  FdTile& ftile = reinterpret_cast<FdTile&>(tile);
+  PERSISTENT_BLOCKS(bi) {
+    const int b = bi.id;
+    const double h = bi.h, h3 = h * h * h;
     double rn[8], sq = 0.0;
     {
       double r[8], nu[8], t[8], rh[8];
@@ -911,8 +964,7 @@ __device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, F
       store_col(xn, b, G, x);
       store_col(A.p, b, G, q);
     }
-    const double h = M.h[b], h3 = h * h * h;
-    block_inverse_group(rn, tile, G, h, inv);
+    block_inverse_group(rn, ftile, G, h, inv);
     double s = 0.0;
 #pragma unroll
     for (int z = 0; z < 8; ++z) {
@@ -928,20 +980,31 @@ __device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, F
 // Every CTA keeps a copy of the Krylov state in shared memory and applies
 // the finalizers to the grid totals of each phase, so all copies stay equal;
 // CTA 0 writes the state back at the end.  Data written by other CTAs is read
-// after the grid barrier's acquire, with loads that bypass L1.
+// after the grid barrier's acquire.
+// Dynamic shared memory: GROUPS tiles, the inverse eigenvalues (BN doubles),
+// GROUPS * KB_CACHE block entries.
+constexpr size_t kPersistentSmem = GROUPS * sizeof(GroupTile) + BN * sizeof(double) +
+                                   GROUPS * KB_CACHE * sizeof(BlockInfo);
+
 template <class T>
 __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync Gs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw);
   double* inv_eig = reinterpret_cast<double*>(smem_raw + GROUPS * sizeof(GroupTile));
+  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + GROUPS * sizeof(GroupTile) + BN * sizeof(double));
   __shared__ double red[64];
   __shared__ KrylovState S;
   __shared__ double ms_zr;  // sum(zr h^3) of the current zr
   __shared__ unsigned int epoch;
   const GroupIdx G;
+  const DevMesh& M = A.M;
   GroupTile& tile = tiles[G.g];
-  FdTile& ftile = reinterpret_cast<FdTile&>(tile);  // FdTile is GroupTile's leading member
   fd_fill_inverse_eigen(inv_eig, c_lam);
+  for (int i = threadIdx.x; i < GROUPS * KB_CACHE * 32; i += NT) {  // 32 lanes fill one entry
+    const int e = i >> 5, g = e / KB_CACHE, k = e % KB_CACHE;
+    const int slot = blockIdx.x * GROUPS + g + k * gridDim.x * GROUPS;
+    if (k < A.ncache && slot < M.nb) fill_block_info(M, M.order ? M.order[slot] : slot, cache[e], i & 31);
+  }
   if (threadIdx.x == 0) {
     S = *A.st;
     epoch = 0u;
@@ -949,7 +1012,7 @@ __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync 
   __syncthreads();
   bool ok = true;
   if (!S.done) {
-    double a[1] = {phase_p0<T>(A, G, ftile, inv_eig)};
+    double a[1] = {phase_p0<T>(A, G, tile, cache, inv_eig)};
     ok = grid_allreduce<1>(a, Gs, epoch, red);
     // q = 0 at the start (p of k_bicg_init), so z1 = zr
     if (threadIdx.x == 0) ms_zr = S.mean_sum = a[0];
@@ -959,7 +1022,7 @@ __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync 
     const bool restart = S.restart_pending != 0;
     const double beta = restart ? 0.0 : S.beta;
     double a[2] = {0.0, 0.0};
-    phase_p1<T>(A, G, tile, inv_eig, beta, S.mean_sum, restart, a);
+    phase_p1<T>(A, G, tile, cache, inv_eig, beta, S.mean_sum, restart, a);
     if (!(ok = grid_allreduce<2>(a, Gs, epoch, red))) break;
     if (threadIdx.x == 0) {
       fin_a(S, S.mean_sum, restart);
@@ -969,12 +1032,12 @@ __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync 
     }
     __syncthreads();
     double d[2] = {0.0, 0.0};
-    phase_p2<T>(A, G, tile, S.alpha, S.mean_sum, d);
+    phase_p2<T>(A, G, tile, cache, S.alpha, S.mean_sum, d);
     if (!(ok = grid_allreduce<2>(d, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_d(S, d);
     __syncthreads();
     double e[4] = {0.0, 0.0, 0.0, 0.0};
-    phase_p3<T>(A, G, ftile, inv_eig, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.beta, S.omega, e);
+    phase_p3<T>(A, G, tile, cache, inv_eig, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.beta, S.omega, e);
     if (!(ok = grid_allreduce<4>(e, Gs, epoch, red))) break;
     if (threadIdx.x == 0) {
       const double re[2] = {e[0], e[1]};
@@ -1032,7 +1095,9 @@ __global__ void __launch_bounds__(NT) k_true_residual(DevMesh M, const double* _
   GROUP_BLOCKS(blk) {
     double col[8], y[8], bc[8];
     load_col(x, blk, G, col);
-    spmv_group(M, blk, VecAt<double>{x}, col, ms, mean_mode, tiles[G.g], G, y);
+    fill_block_info(M, blk, tiles[G.g].bi, G.lane);
+    group_sync(G.g);
+    spmv_group(tiles[G.g].bi, VecAt<double>{x}, col, ms, mean_mode, tiles[G.g], G, y);
     load_col(b, blk, G, bc);
     if (zero_mean_row && blk == M.mean_block && G.lane == 0) bc[0] = 0.0;
     float* rb = r32 ? r32 + size_t(blk) * BN + G.gy * 8 + G.gx : nullptr;
@@ -1074,6 +1139,7 @@ static KArgs<T> make_args(const DevMesh& M, const T* b, T* x, T* const v[9], Poi
   A.mean_mode = mean_mode;
   A.zero_mean_row = zero_mean_row;
   A.ext_precond = 0;
+  A.ncache = 0;
   return A;
 }
 
@@ -1134,7 +1200,7 @@ static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, 
 // reduction buffer.
 template <class T>
 static int persistent_grid(int nb, const PoissonWork& W, int* grid) {
-  const size_t dyn = GROUPS * sizeof(GroupTile) + BN * sizeof(double);
+  const size_t dyn = kPersistentSmem;
   void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
   CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   int per_sm = 0, dev = 0, sms = 0;
@@ -1159,7 +1225,7 @@ int persistent_solver_groups(int nb, const PoissonWork& W, int* groups) {
 // that runs iterations until the state says done.
 template <class T>
 static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, const char* name) {
-  const size_t dyn = GROUPS * sizeof(GroupTile) + BN * sizeof(double);
+  const size_t dyn = kPersistentSmem;
   void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
   int grid = 0;
   if (int rc = persistent_grid<T>(A.M.nb, W, &grid)) return rc;
@@ -1190,6 +1256,7 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   KArgs<T> A = make_args<T>(M, b, x, v, W, W.st, P.mean_mode, zero_mean_row, 0);
   A.ext_precond = cnn ? 1 : 0;
+  A.ncache = std::max(0, std::min(P.block_cache, KB_CACHE));
   GridReduce gc{W.partial, W.counters + 14};
   { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_prepare<T>, W.grid, s, A)); }
   { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_init<T>, W.ggrid, s, A)); }

@@ -56,6 +56,7 @@ struct SolveParams {
   int check_every;   // host checks convergence every this many iterations
   int stall_window;  // 0: off (reference behaviour)
   int persistent;    // 1: all iterations in one cooperative launch (plain and mixed solvers)
+  int block_cache;   // persistent solver: table entries staged per block group at launch (0-4)
 };
 
 struct SolveStats {

@@ -76,6 +76,9 @@ typedef struct cup_config {
   int32_t poisson_max_restarts;/* 100 in the reference */
   int32_t step_2nd_start;      /* 2 in the reference */
   int32_t device;              /* CUDA device ordinal */
+  int32_t poisson_block_cache; /* -poissonBlockCache: mesh-table entries per block group kept in
+                                  shared memory by the persistent solver (0-4; 4 by default);
+                                  a tuning knob with no reference counterpart */
 } cup_config;
 
 typedef struct cup_solve_stats {

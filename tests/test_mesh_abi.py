@@ -87,3 +87,7 @@ def test_config_parse_flags():
     assert cfg.bc[0] == 1 and cfg.poisson_solver == 1 and cfg.advection == 1
     with pytest.raises(cup.CupError):
         cup.config("-poissonSolver cuda_iterative_typo")
+    assert cup.config("").poisson_block_cache == 4
+    assert cup.config("-poissonBlockCache 0").poisson_block_cache == 0
+    with pytest.raises(cup.CupError):
+        cup.config("-poissonBlockCache 5")

@@ -93,6 +93,25 @@ def test_solve_matches_oracle(name):
     assert abs(st["iterations"] - st_ref["iterations"]) <= slack, (st, st_ref)
 
 
+@pytest.mark.parametrize("solver", ["b200", "b200_mixed"])
+@pytest.mark.parametrize("name", ["amr3_mixed", "amr3_periodic"])
+def test_staged_block_entries_match_cached(name, solver):
+    # -poissonBlockCache 0: the persistent solver stages every block's table
+    # entries in the group's tile on the way (the path of meshes with more
+    # than four blocks per block group) instead of reading the copies made at
+    # launch; same values, same arithmetic, so the same bits
+    out = []
+    for cache in (4, 0):
+        ctx = make_ctx(name, device=0, extra=f"-poissonTol 0 -poissonTolRel 1e-10 -poissonSolver {solver} "
+                                             f"-poissonBlockCache {cache}")
+        m = oracle_mesh(ctx)
+        bd, xd = torch_dev(_compatible_rhs(m, 11)), torch_dev(np.zeros(m.n))
+        rc, st = ctx.poisson_solve_dev(bd, xd)
+        out.append((rc, st["iterations"], xd.cpu().numpy()))
+    assert out[0][:2] == out[1][:2]
+    assert np.array_equal(out[0][2], out[1][2])
+
+
 def test_solve_through_fields_matches_device_buffers():
     # PoissonSolverBase::solve() contract: RHS in sim.lhs, guess/result in sim.pres
     ctx = make_ctx("amr2_free", device=0, extra="-poissonTol 0 -poissonTolRel 1e-10")
