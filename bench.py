@@ -52,17 +52,17 @@ ALG_BYTES = {
     "bicg_d_spmv_dots": 8 * 3,          # R z2, r; W t
     "bicg_e_xr_update_dots": 8 * 8,     # R x, z1, z2, r, t, rhat; W x, r
     "bicg_init": 8 * 6,
-    "bicg_persistent": 8 * 23,          # per iteration: R/W of the five phases (40+24+32+24+64 B)
+    "bicg_persistent": 8 * 22,          # per iteration: R/W of the three phases (40+40+96 B)
     "weighted_sum": 8 * 1,
     "max_u": 8 * 3,
 }
 
 
 # DRAM bytes (read + write) per cell and iteration of the persistent solver,
-# measured by ncu on 16 iterations of `python -m cup3d_b200.kernel_cases solve`
-# (profiles/bicg_persistent_sphere_solve.md: 263.2 MB + 598.4 MB over 16
-# iterations of 1,198,080 cells); most of the 184 algorithmic bytes hit in L2.
-MEASURED_TRAFFIC_PER_CELL_ITER = {"bicg_persistent": 44.95}
+# measured by ncu (--set full) on 16 iterations of
+# `python -m cup3d_b200.kernel_cases solve`: 147.7 MB + 594.2 MB over 16
+# iterations of 1,198,080 cells; most of the 176 algorithmic bytes hit in L2.
+MEASURED_TRAFFIC_PER_CELL_ITER = {"bicg_persistent": 38.70}
 
 
 def dist_env():
@@ -290,7 +290,7 @@ def run_b200(args):
     dom_name, (dom_n, dom_ms) = dom
     per_launch_ms = dom_ms / max(dom_n, 1)
     if dom_name == "bicg_persistent":
-        # one launch per solve, 184 B/cell per iteration
+        # one launch per solve, 176 B/cell per iteration
         alg_bytes = int(ALG_BYTES[dom_name] * ncell * sum(prof_iters) / max(dom_n, 1))
     else:
         alg_bytes = ALG_BYTES.get(dom_name, 0) * ncell

@@ -807,6 +807,12 @@ struct Comb2At {  // a + c b
 // way.
 constexpr int KB_CACHE = 4;
 
+// Block groups per CTA of the persistent solver, two CTAs per SM.  (One
+// 512-thread CTA per SM halves the CTAs in every grid barrier but measured
+// 6% slower per iteration on the sphere mesh.)
+constexpr int PGROUPS = 4;
+constexpr int PNT = PGROUPS * GROUP;
+
 __device__ __forceinline__ const BlockInfo& persistent_block(const DevMesh& M, const BlockInfo* cache, int ncache,
                                                              GroupTile& tile, int k, int slot, const GroupIdx& G) {
   if (k < ncache) return cache[G.g * KB_CACHE + k];
@@ -817,7 +823,7 @@ __device__ __forceinline__ const BlockInfo& persistent_block(const DevMesh& M, c
 }
 
 #define PERSISTENT_BLOCKS(bi)                                                                   \
-  for (int k_ = 0, slot_ = blockIdx.x * GROUPS + G.g; slot_ < M.nb; ++k_, slot_ += gridDim.x * GROUPS) \
+  for (int k_ = 0, slot_ = blockIdx.x * PGROUPS + G.g; slot_ < M.nb; ++k_, slot_ += gridDim.x * PGROUPS) \
     if (const BlockInfo& bi = persistent_block(M, cache, A.ncache, tile, k_, slot_, G); true)
 
 // P0 (once): zr = M^-1 r for the initial residual; sum(zr h^3)
@@ -981,17 +987,17 @@ __device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, G
 // the finalizers to the grid totals of each phase, so all copies stay equal;
 // CTA 0 writes the state back at the end.  Data written by other CTAs is read
 // after the grid barrier's acquire.
-// Dynamic shared memory: GROUPS tiles, the inverse eigenvalues (BN doubles),
-// GROUPS * KB_CACHE block entries.
-constexpr size_t kPersistentSmem = GROUPS * sizeof(GroupTile) + BN * sizeof(double) +
-                                   GROUPS * KB_CACHE * sizeof(BlockInfo);
+// Dynamic shared memory: PGROUPS tiles, the inverse eigenvalues (BN doubles),
+// PGROUPS * KB_CACHE block entries.
+constexpr size_t kPersistentSmem = PGROUPS * sizeof(GroupTile) + BN * sizeof(double) +
+                                   PGROUPS * KB_CACHE * sizeof(BlockInfo);
 
 template <class T>
-__global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync Gs) {
+__global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A, GridSync Gs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw);
-  double* inv_eig = reinterpret_cast<double*>(smem_raw + GROUPS * sizeof(GroupTile));
-  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + GROUPS * sizeof(GroupTile) + BN * sizeof(double));
+  double* inv_eig = reinterpret_cast<double*>(smem_raw + PGROUPS * sizeof(GroupTile));
+  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + PGROUPS * sizeof(GroupTile) + BN * sizeof(double));
   __shared__ double red[64];
   __shared__ KrylovState S;
   __shared__ double ms_zr;  // sum(zr h^3) of the current zr
@@ -1000,9 +1006,9 @@ __global__ void __launch_bounds__(NT, 2) k_bicg_persistent(KArgs<T> A, GridSync 
   const DevMesh& M = A.M;
   GroupTile& tile = tiles[G.g];
   fd_fill_inverse_eigen(inv_eig, c_lam);
-  for (int i = threadIdx.x; i < GROUPS * KB_CACHE * 32; i += NT) {  // 32 lanes fill one entry
+  for (int i = threadIdx.x; i < PGROUPS * KB_CACHE * 32; i += PNT) {  // 32 lanes fill one entry
     const int e = i >> 5, g = e / KB_CACHE, k = e % KB_CACHE;
-    const int slot = blockIdx.x * GROUPS + g + k * gridDim.x * GROUPS;
+    const int slot = blockIdx.x * PGROUPS + g + k * gridDim.x * PGROUPS;
     if (k < A.ncache && slot < M.nb) fill_block_info(M, M.order ? M.order[slot] : slot, cache[e], i & 31);
   }
   if (threadIdx.x == 0) {
@@ -1196,7 +1202,7 @@ static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, 
 }
 
 // CTAs of the persistent solver for a mesh of nb blocks: all co-resident,
-// at most one per four blocks, two partial slots of 8 doubles per CTA in the
+// at most one per PGROUPS blocks, two partial slots of 8 doubles per CTA in the
 // reduction buffer.
 template <class T>
 static int persistent_grid(int nb, const PoissonWork& W, int* grid) {
@@ -1204,11 +1210,11 @@ static int persistent_grid(int nb, const PoissonWork& W, int* grid) {
   void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
   CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   int per_sm = 0, dev = 0, sms = 0;
-  CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, dyn));
+  CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PNT, dyn));
   CUP_CUDA_TRY(cudaGetDevice(&dev));
   CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: kernel does not fit on an SM");
-  *grid = std::max(1, std::min({per_sm * sms, (nb + GROUPS - 1) / GROUPS, std::max(W.grid, W.ggrid) / 2}));
+  *grid = std::max(1, std::min({per_sm * sms, (nb + PGROUPS - 1) / PGROUPS, std::max(W.grid, W.ggrid) / 2}));
   return 0;
 }
 
@@ -1217,7 +1223,7 @@ int persistent_solver_groups(int nb, const PoissonWork& W, int* groups) {
   if (int rc = persistent_grid<double>(nb, W, &g1)) return rc;
   if (int rc = persistent_grid<float>(nb, W, &g2)) return rc;
   if (g1 != g2) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: FP64 and FP32 grids differ");
-  *groups = g1 * GROUPS;
+  *groups = g1 * PGROUPS;
   return 0;
 }
 
@@ -1236,7 +1242,7 @@ static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, 
   KArgs<T> Aa = A;
   void* args[] = {(void*)&Aa, (void*)&Gs};
   ProfScope ps(name, s);
-  CUP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(NT), args, dyn, s));
+  CUP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(PNT), args, dyn, s));
   return 0;
 }
 
