@@ -303,3 +303,31 @@ class Context:
 
     def cnn_precond(self, r, z):
         check(lib().cup_cnn_precond_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
+class Batch(Context):
+    """Independent cases in one context (cup_batch_create): the cases' meshes
+    concatenated in case order; their Poisson solves run in one device
+    launch, each case with its own BiCGSTAB."""
+
+    def __init__(self, cases):
+        cases = list(cases)
+        arr = (C.c_void_p * len(cases))(*[c._p.value for c in cases])
+        p = lib().cup_batch_create(len(cases), arr)
+        if not p:
+            raise CupError(-1, lib().cup_last_error(None).decode())
+        self.cfg = cases[0].cfg
+        self._p = C.c_void_p(p)
+        self.ncase = int(lib().cup_batch_num_cases(self._p))
+
+    def case_blocks(self, k):
+        """(first block, number of blocks) of case k."""
+        first, n = C.c_int32(), C.c_int32()
+        check(lib().cup_batch_case_blocks(self._p, k, C.byref(first), C.byref(n)), self._p)
+        return first.value, n.value
+
+    def poisson_solve_dev(self, b, x):
+        """One BiCGSTAB per case in one launch: (rc, [stats per case])."""
+        st = (cup_solve_stats * self.ncase)()
+        rc = check(lib().cup_batch_poisson_solve_dev(self._p, _dev_ptr(b), _dev_ptr(x), st), self._p)
+        return rc, [s.as_dict() for s in st]
+
+

@@ -101,6 +101,10 @@ SIGNATURES = {
     "cup_block_inverse_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_poisson_solve_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.POINTER(cup_solve_stats)]),
     "cup_poisson_solve": (C.c_int, [_P, C.POINTER(cup_solve_stats)]),
+    "cup_batch_create": (_P, [C.c_int32, C.POINTER(_P)]),
+    "cup_batch_num_cases": (C.c_int32, [_P]),
+    "cup_batch_case_blocks": (C.c_int, [_P, C.c_int32, _I, _I]),
+    "cup_batch_poisson_solve_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.POINTER(cup_solve_stats)]),
     "cup_obstacle_sphere": (C.c_int, [_P, _D, C.c_double, _D, _D]),
     "cup_obstacle_ellipsoid": (C.c_int, [_P, _D, _D, _D, _D, _D]),
     "cup_set_obstacle": (C.c_int, [_P, C.c_int32, _I, _D, _D, _D]),

@@ -1,0 +1,228 @@
+// Batches of independent cases: one context over the concatenated meshes of
+// several contexts, whose Poisson solves run in one cooperative launch.
+//
+// No reference counterpart: the reference advances one case per process.
+// Each case keeps its own mesh, its own mean-constraint row and its own
+// BiCGSTAB scalars; only the device launch is shared.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "context.h"
+
+namespace cup3d {
+
+// Concatenates the cases' meshes: blocks of case k follow those of case k-1,
+// face-table entries that name blocks are shifted by the case's offset
+// (boundary entries hold a BC kind and stay), and no face joins two cases.
+static void concat_meshes(const std::vector<Mesh>& cases, Mesh& m, std::vector<int>& first,
+                          std::vector<int>& mean) {
+  m = Mesh();
+  m.spec = cases[0].spec;
+  first.assign(cases.size() + 1, 0);
+  mean.assign(cases.size(), -1);
+  for (size_t k = 0; k < cases.size(); ++k) first[k + 1] = first[k] + cases[k].nb;
+  m.nb = first.back();
+  for (size_t k = 0; k < cases.size(); ++k) {
+    const Mesh& c = cases[k];
+    const int off = first[k];
+    m.level.insert(m.level.end(), c.level.begin(), c.level.end());
+    m.index.insert(m.index.end(), c.index.begin(), c.index.end());
+    m.h.insert(m.h.end(), c.h.begin(), c.h.end());
+    m.origin.insert(m.origin.end(), c.origin.begin(), c.origin.end());
+    m.face_kind.insert(m.face_kind.end(), c.face_kind.begin(), c.face_kind.end());
+    for (int b = 0; b < c.nb; ++b)
+      for (int f = 0; f < 6; ++f) {
+        const int kind = c.face_kind[6 * b + f];
+        for (int q = 0; q < 4; ++q) {
+          const int v = c.face_nbr[24 * b + 4 * f + q];
+          m.face_nbr.push_back(kind != FACE_BOUNDARY && v >= 0 ? v + off : v);
+        }
+      }
+    mean[k] = c.mean_block >= 0 ? c.mean_block + off : -1;
+    m.max_level_used = std::max(m.max_level_used, c.max_level_used);
+  }
+  m.mean_block = mean[0];
+}
+
+// Block groups per case in proportion to its blocks (at least one, at most
+// one per block), then each case's blocks dealt to its groups in the
+// cost-balanced visit order of its own mesh.
+static int plan_groups(const std::vector<Mesh>& cases, const std::vector<int>& first, int groups,
+                       std::vector<int>& gcase, std::vector<int>& gfirst, std::vector<int>& goff,
+                       std::vector<int>& gblocks) {
+  const int K = int(cases.size());
+  if (K > groups) return set_error(CUP_ERR_ARG, "batch: more cases than block groups of the batched solver");
+  const double nbt = double(first.back());
+  std::vector<int> ng(K);
+  int used = 0;
+  for (int k = 0; k < K; ++k) {
+    ng[k] = std::max(1, std::min(cases[k].nb, int(groups * (cases[k].nb / nbt))));
+    used += ng[k];
+  }
+  // too many (the floors of one): take from the cases with the fewest blocks per group
+  while (used > groups) {
+    int best = -1;
+    for (int k = 0; k < K; ++k)
+      if (ng[k] > 1 && (best < 0 || double(cases[k].nb) / ng[k] < double(cases[best].nb) / ng[best])) best = k;
+    if (best < 0) break;
+    --ng[best];
+    --used;
+  }
+  // spare groups: to the cases with the most blocks per group
+  while (used < groups) {
+    int best = -1;
+    for (int k = 0; k < K; ++k)
+      if (ng[k] < cases[k].nb && (best < 0 || double(cases[k].nb) / ng[k] > double(cases[best].nb) / ng[best]))
+        best = k;
+    if (best < 0) break;
+    ++ng[best];
+    ++used;
+  }
+  gcase.assign(groups, -1);
+  gfirst.assign(K + 1, 0);
+  goff.assign(groups + 1, 0);
+  gblocks.clear();
+  int g = 0;
+  for (int k = 0; k < K; ++k) {
+    gfirst[k] = g;
+    const std::vector<int32_t> order = mesh_visit_order(cases[k], ng[k]);
+    for (int j = 0; j < ng[k]; ++j, ++g) {
+      gcase[g] = k;
+      goff[g] = int(gblocks.size());
+      for (int s = j; s < cases[k].nb; s += ng[k]) gblocks.push_back(first[k] + order[s]);
+    }
+  }
+  gfirst[K] = g;
+  for (; g <= groups; ++g) goff[g] = int(gblocks.size());
+  return 0;
+}
+
+static int upload_ints(cup_ctx* c, int** dst, const std::vector<int>& v) {
+  if (int rc = c->batch_arena.alloc(dst, v.size())) return rc;
+  CUP_CUDA_TRY(stream_h2d(c->stream, *dst, v.data(), v.size() * sizeof(int)));
+  return 0;
+}
+
+static int batch_setup(cup_ctx* c, const std::vector<Mesh>& cases) {
+  std::vector<int> first, mean;
+  concat_meshes(cases, c->mesh, first, mean);
+  c->ncase = int(cases.size());
+  c->case_first = first;
+  c->case_mesh = cases;
+  if (int rc = ctx_upload_mesh(c)) return rc;
+  if (int rc = ctx_alloc_fields(c)) return rc;
+  std::vector<int> bcase(c->mesh.nb);
+  for (int k = 0; k < c->ncase; ++k)
+    for (int b = first[k]; b < first[k + 1]; ++b) bcase[b] = k;
+  int *d_bcase = nullptr, *d_mean = nullptr;
+  if (int rc = upload_ints(c, &d_bcase, bcase)) return rc;
+  if (int rc = upload_ints(c, &d_mean, mean)) return rc;
+  c->dm.bcase = d_bcase;
+  c->dm.case_mean = d_mean;
+  BatchWork& B = c->B;
+  B.ncase = c->ncase;
+  if (int rc = batch_solver_shape(c->mesh.nb, &B.grid, &B.groups)) return rc;
+  std::vector<int> gcase, gfirst, goff, gblocks;
+  if (int rc = plan_groups(cases, first, B.groups, gcase, gfirst, goff, gblocks)) return rc;
+  if (int rc = upload_ints(c, &B.gcase, gcase)) return rc;
+  if (int rc = upload_ints(c, &B.gfirst, gfirst)) return rc;
+  if (int rc = upload_ints(c, &B.goff, goff)) return rc;
+  if (int rc = upload_ints(c, &B.gblocks, gblocks)) return rc;
+  if (int rc = c->batch_arena.alloc(&B.part, size_t(2) * B.groups * 8)) return rc;
+  if (int rc = c->batch_arena.alloc(&B.case_done, size_t(B.ncase))) return rc;
+  if (int rc = c->batch_arena.alloc(&B.st, size_t(B.ncase))) return rc;
+  return 0;
+}
+
+}  // namespace cup3d
+
+using namespace cup3d;
+
+extern "C" {
+
+cup_ctx* cup_batch_create(int32_t ncases, cup_ctx* const* cases) {
+  if (ncases < 1 || !cases) {
+    set_error(CUP_ERR_ARG, "cup_batch_create: no cases");
+    return nullptr;
+  }
+  std::vector<Mesh> meshes;
+  for (int k = 0; k < ncases; ++k) {
+    const cup_ctx* c = cases[k];
+    if (!c || c->host_only || c->mesh.nb == 0 || c->ncase != 1) {
+      set_error(CUP_ERR_ARG, "cup_batch_create: every case must be a device context with a mesh (not a batch)");
+      return nullptr;
+    }
+    if (c->cfg.device != cases[0]->cfg.device || c->cfg.mean_constraint != cases[0]->cfg.mean_constraint) {
+      set_error(CUP_ERR_ARG, "cup_batch_create: the cases must share the device and -bMeanConstraint");
+      return nullptr;
+    }
+    meshes.push_back(c->mesh);
+  }
+  cup_ctx* c = cup_create(&cases[0]->cfg);
+  if (!c) return nullptr;
+  if (int rc = batch_setup(c, meshes)) {
+    (void)rc;
+    const std::string msg = "cup_batch_create: " + std::string(cup_last_error(nullptr));
+    cup_destroy(c);
+    set_error(CUP_ERR_CUDA, msg.c_str());
+    return nullptr;
+  }
+  return c;
+}
+
+int32_t cup_batch_num_cases(const cup_ctx* c) { return c ? c->ncase : 0; }
+
+int cup_batch_case_blocks(const cup_ctx* c, int32_t k, int32_t* first, int32_t* nblocks) {
+  if (!c || k < 0 || k >= c->ncase || !first || !nblocks) return set_error(CUP_ERR_ARG, "cup_batch_case_blocks: bad arguments");
+  if (c->ncase == 1) {
+    *first = 0;
+    *nblocks = c->mesh.nb;
+  } else {
+    *first = c->case_first[k];
+    *nblocks = c->case_first[k + 1] - c->case_first[k];
+  }
+  return 0;
+}
+
+int cup_batch_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats) {
+  ProfBind pb_(c);
+  if (!c || !b || !x || !stats || c->ncase < 2) return ctx_fail(c, CUP_ERR_ARG, "cup_batch_poisson_solve_dev: not a batch or bad arguments");
+  if (reinterpret_cast<uintptr_t>(x) % 16 != 0 || reinterpret_cast<uintptr_t>(b) % 16 != 0)
+    return ctx_fail(c, CUP_ERR_ARG, "cup_batch_poisson_solve_dev: b and x must be 16-byte aligned");
+  SolveParams P{};
+  P.tol_abs = c->cfg.poisson_tol;
+  P.tol_rel = c->cfg.poisson_tol_rel;
+  P.max_iter = c->cfg.poisson_max_iter;
+  P.max_restarts = c->cfg.poisson_max_restarts;
+  P.mean_mode = c->cfg.mean_constraint;
+  P.persistent = 1;
+  P.block_cache = c->cfg.poisson_block_cache;
+  std::vector<SolveStats> S(c->ncase);
+  CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  if (int rc = poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S.data(), c->stream)) {
+    c->err = cup_last_error(nullptr);
+    return rc;
+  }
+  CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  CUP_CUDA_TRY(cudaEventSynchronize(c->ev1));
+  float ms = 0;
+  CUP_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  int rc = CUP_OK;
+  for (int k = 0; k < c->ncase; ++k) {
+    cup_solve_stats& o = stats[k];
+    o.iterations = S[k].iterations;
+    o.restarts = S[k].restarts;
+    o.status = S[k].status;
+    o.fallback = 0;
+    o.err_init = S[k].err_init;
+    o.err_final = S[k].err_opt;
+    o.true_rel = -1.0;
+    o.milliseconds = ms;
+    if (S[k].status == SOLVE_NAN) rc = ctx_fail(c, CUP_ERR_NAN, "batched Poisson solve produced NaN");
+    else if (S[k].status != SOLVE_CONVERGED && rc == CUP_OK) rc = CUP_SOFT_MAXITER;
+  }
+  return rc;
+}
+
+}  // extern "C"

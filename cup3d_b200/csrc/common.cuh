@@ -25,6 +25,10 @@ struct DevMesh {
   // Order in which the block-group kernels visit the blocks (a permutation of
   // 0..nb-1, or null for 0..nb-1): visit slot i holds block order[i].
   const int* __restrict__ order;
+  // Batches of independent cases (null for one case): the case of each block
+  // and each case's mean-constraint block.
+  const int* __restrict__ bcase;
+  const int* __restrict__ case_mean;
 };
 
 #ifndef CUP3D_TAN_HELPERS

@@ -55,7 +55,7 @@ static int keep(cup_ctx* c, int rc) {
   return rc;
 }
 
-static int upload_mesh(cup_ctx* c) {
+int ctx_upload_mesh(cup_ctx* c) {
   Mesh& m = c->mesh;
   c->mesh_arena.release();
   int *fk, *fn, *ix;
@@ -75,10 +75,12 @@ static int upload_mesh(cup_ctx* c) {
   c->dm.index = ix;
   c->dm.h = h;
   c->dm.order = nullptr;  // set by alloc_fields
+  c->dm.bcase = nullptr;  // set for batches
+  c->dm.case_mean = nullptr;
   return 0;
 }
 
-static int alloc_fields(cup_ctx* c) {
+int ctx_alloc_fields(cup_ctx* c) {
   c->field_arena.release();
   c->obst_arena.release();
   c->ob = DevObstacle();
@@ -134,6 +136,7 @@ static int alloc_fields(cup_ctx* c) {
 }
 
 static int install_mesh(cup_ctx* c, const std::vector<std::array<int32_t, 4>>& leaves) {
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "a batch of cases keeps the meshes it was made from");
   MeshSpec spec;
   for (int d = 0; d < 3; ++d) {
     spec.bpd[d] = c->cfg.bpd[d];
@@ -146,8 +149,8 @@ static int install_mesh(cup_ctx* c, const std::vector<std::array<int32_t, 4>>& l
   if (!mesh_build(spec, leaves, m, err)) return ctx_fail(c, CUP_ERR_MESH, "mesh: " + err);
   c->mesh = std::move(m);
   if (c->host_only) return 0;
-  if (int rc = upload_mesh(c)) return keep(c, rc);
-  if (int rc = alloc_fields(c)) return keep(c, rc);
+  if (int rc = ctx_upload_mesh(c)) return keep(c, rc);
+  if (int rc = ctx_alloc_fields(c)) return keep(c, rc);
   return 0;
 }
 
@@ -501,6 +504,7 @@ int cup_block_inverse_dev(cup_ctx* c, const double* in, double* out) {
 // the time-step path skips it (-1) since the solvers already test their own
 // FP64 residual.
 static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats, bool check_true = true) {
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "a batch of cases solves with cup_batch_poisson_solve_dev");
   SolveParams P;
   P.tol_abs = c->cfg.poisson_tol;
   P.tol_rel = c->cfg.poisson_tol_rel;
@@ -710,6 +714,7 @@ extern "C" {
 
 int cup_obstacle_sphere(cup_ctx* c, const double* ctr, double r, const double* vel, const double* omega) {
   if (!c || !ctr || c->mesh.nb == 0) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_sphere: bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_obstacle_sphere: not available on a batch of cases");
   const double z[3] = {0, 0, 0};
   HostObstacle h;
   make_sphere(c->mesh, ctr, r, vel ? vel : z, omega ? omega : z, h);
@@ -720,6 +725,7 @@ int cup_obstacle_ellipsoid(cup_ctx* c, const double* ctr, const double* ax, cons
                            const double* omega) {
   if (!c || !ctr || !ax || !q || c->mesh.nb == 0)
     return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_ellipsoid: bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_obstacle_ellipsoid: not available on a batch of cases");
   const double z[3] = {0, 0, 0};
   HostObstacle h;
   make_ellipsoid(c->mesh, ctr, ax, q, vel ? vel : z, omega ? omega : z, h);
@@ -730,6 +736,7 @@ int cup_set_obstacle(cup_ctx* c, int32_t nslots, const int32_t* blocks, const do
                      const double* kin) {
   if (!c || c->mesh.nb == 0 || (nslots > 0 && (!blocks || !chi)))
     return ctx_fail(c, CUP_ERR_ARG, "cup_set_obstacle: bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_set_obstacle: not available on a batch of cases");
   return upload_obstacle(c, nslots, blocks, chi, udef, kin);
 }
 
@@ -746,6 +753,7 @@ int cup_get_obstacle(const cup_ctx* c, int32_t* blocks, double* chi, double* ude
 int cup_max_u(cup_ctx* c, double* umax) {
   ProfBind pb_(c);
   if (!c || !umax || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_max_u: bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_max_u: not available on a batch of cases");
   if (int rc = launch_max_u(c->dm, c->F.vel[c->F.vcur], c->cfg.uinf, c->d_scalars + SC_UMAX, c->W.partial,
                             c->W.counters + 10, grid_of(c), c->stream))
     return keep(c, rc);
@@ -766,6 +774,7 @@ int cup_compute_dt(cup_ctx* c, int32_t step, double* dt) {
 int cup_advect_diffuse(cup_ctx* c, double dt) {
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_advect_diffuse: no mesh");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_advect_diffuse: not available on a batch of cases");
   if (int rc = advect(c, dt)) return rc;
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "advect_diffuse", __FILE__, __LINE__));
@@ -775,6 +784,7 @@ int cup_advect_diffuse(cup_ctx* c, double dt) {
 int cup_penalize(cup_ctx* c, double dt, double* force6) {
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_penalize: no mesh");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_penalize: not available on a batch of cases");
   if (int rc = penalize(c, dt)) return rc;
   cudaError_t e = cudaSuccess;
   if (force6) e = cudaMemcpyAsync(force6, c->d_scalars + SC_FORCE, 6 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
@@ -786,6 +796,7 @@ int cup_penalize(cup_ctx* c, double dt, double* force6) {
 int cup_pressure_rhs(cup_ctx* c, double dt, int32_t step) {
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_pressure_rhs: no mesh");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_pressure_rhs: not available on a batch of cases");
   Fields& F = c->F;
   if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], F.pres[F.pcur], F.chi, ob_view(c), dt, step,
                                    c->cfg.step_2nd_start, F.lhs, F.phi, grid_of(c), c->stream))
@@ -798,6 +809,7 @@ int cup_pressure_rhs(cup_ctx* c, double dt, int32_t step) {
 int cup_pressure_project(cup_ctx* c, double dt, int32_t step, cup_solve_stats* stats) {
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_pressure_project: no mesh");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_pressure_project: not available on a batch of cases");
   const int rc = project(c, dt, step, stats);
   if (rc < 0) return rc;
   cudaError_t e = cudaStreamSynchronize(c->stream);
@@ -808,6 +820,7 @@ int cup_pressure_project(cup_ctx* c, double dt, int32_t step, cup_solve_stats* s
 int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_stats* stats) {
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_step: no mesh");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_step: not available on a batch of cases");
   if (!(dt > 0))
     if (int rc = cup_compute_dt(c, step, &dt)) return rc;
   if (dt_used) *dt_used = dt;

@@ -90,6 +90,12 @@ struct cup_ctx {
   cup3d::Profiler prof;
   cup3d::CnnState cnn;
   std::string err;
+  // batches of independent cases (cup_batch_create); ncase == 1 otherwise
+  int ncase = 1;
+  std::vector<int> case_first;        // ncase + 1 block offsets
+  std::vector<cup3d::Mesh> case_mesh;  // each case's own mesh
+  cup3d::BatchWork B{};
+  cup3d::DevArena batch_arena;
 };
 
 namespace cup3d {
@@ -100,6 +106,9 @@ struct ProfBind {
   ~ProfBind() { t_prof = prev; }  // nested API calls restore the caller's binding
 };
 int ctx_fail(cup_ctx* c, int code, const std::string& msg);
+// Uploads c->mesh and (re)allocates the fields and solver work for it.
+int ctx_upload_mesh(cup_ctx* c);
+int ctx_alloc_fields(cup_ctx* c);
 size_t nbn(const cup_ctx* c);
 // Host<->device copies and fills ordered on a stream, waiting for it before
 // returning.  The context stream is non-blocking, so cudaMemcpy / cudaMemset

@@ -118,7 +118,7 @@ __device__ __forceinline__ void fill_block_info(const DevMesh& M, int b, BlockIn
   } else if (lane == 30) {
     bi.h = M.h[b];
     bi.id = b;
-    bi.mean = b == M.mean_block ? 1 : 0;
+    bi.mean = b == (M.bcase ? M.case_mean[M.bcase[b]] : M.mean_block) ? 1 : 0;
   } else if (lane == 31) {
     bi.par = (M.index[b * 3] & 1) | ((M.index[b * 3 + 1] & 1) << 1) | ((M.index[b * 3 + 2] & 1) << 2);
   }
@@ -414,6 +414,37 @@ __global__ void __launch_bounds__(NT) k_bicg_prepare(KArgs<T> A) {
   if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) A.st->mean_sum = acc[0];
 }
 
+// Scalars of iteration 0 from rr = (r0, r0) (BiCGSTAB.cu:416-470)
+__device__ __forceinline__ void fin_init(KrylovState& S, double rr) {
+  const double e = sqrt(rr);
+  S.err = S.err_init = S.err_opt = e;
+  S.rr = S.rr_hat = rr;
+  S.rho = rr;  // (rhat, r) of iteration 0
+  S.rho_prev = 1.0;
+  S.alpha = 1.0;
+  S.omega = 1.0;
+  S.beta = (S.rho / (S.rho_prev + S.eps)) * (S.alpha / (S.omega + S.eps));
+  S.k = 0;
+  S.restarts = 0;
+  S.cur = 0;
+  S.best = 0;
+  S.nxt = 1;
+  S.restart_pending = 0;
+  S.converged = 0;
+  S.done = 0;
+  S.status = SOLVE_RUNNING;
+  S.last_improve_k = 0;
+  S.stall_ref = e;
+  if (!(e == e)) {
+    S.done = 1;
+    S.status = SOLVE_NAN;
+  } else if (e <= S.tol_abs) {  // nothing to do (also covers b = A x0)
+    S.done = 1;
+    S.converged = 1;
+    S.status = SOLVE_CONVERGED;
+  }
+}
+
 // r = b - A x0, rhat = r, p = nu = 0; err_init = ||r||
 template <class T>
 __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
@@ -445,36 +476,7 @@ __global__ void __launch_bounds__(NT) k_bicg_init(KArgs<T> A) {
     store_col(A.p, b, G, zero);
     store_col(A.nu, b, G, zero);
   }
-  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) {
-    KrylovState& S = *A.st;
-    const double e = sqrt(acc[0]);
-    S.err = S.err_init = S.err_opt = e;
-    S.rr = S.rr_hat = acc[0];
-    S.rho = acc[0];  // (rhat, r) of iteration 0
-    S.rho_prev = 1.0;
-    S.alpha = 1.0;
-    S.omega = 1.0;
-    S.beta = (S.rho / (S.rho_prev + S.eps)) * (S.alpha / (S.omega + S.eps));
-    S.k = 0;
-    S.restarts = 0;
-    S.cur = 0;
-    S.best = 0;
-    S.nxt = 1;
-    S.restart_pending = 0;
-    S.converged = 0;
-    S.done = 0;
-    S.status = SOLVE_RUNNING;
-    S.last_improve_k = 0;
-    S.stall_ref = e;
-    if (!(e == e)) {
-      S.done = 1;
-      S.status = SOLVE_NAN;
-    } else if (e <= S.tol_abs) {  // nothing to do (also covers b = A x0)
-      S.done = 1;
-      S.converged = 1;
-      S.status = SOLVE_CONVERGED;
-    }
-  }
+  if (grid_reduce<1>(acc, A.g, red) && threadIdx.x == 0) fin_init(*A.st, acc[0]);
 }
 
 // ---------------------------------------------------------------------------
@@ -826,161 +828,149 @@ __device__ __forceinline__ const BlockInfo& persistent_block(const DevMesh& M, c
   for (int k_ = 0, slot_ = blockIdx.x * PGROUPS + G.g; slot_ < M.nb; ++k_, slot_ += gridDim.x * PGROUPS) \
     if (const BlockInfo& bi = persistent_block(M, cache, A.ncache, tile, k_, slot_, G); true)
 
+// Phase bodies for one block (bi) of a group; the persistent solvers loop
+// them over the group's blocks.
 // P0 (once): zr = M^-1 r for the initial residual; sum(zr h^3)
 template <class T>
-__device__ __forceinline__ double phase_p0(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
-                                           const BlockInfo* cache, const double* inv) {
-  const DevMesh& M = A.M;
+__device__ __forceinline__ double p0_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
+                                           const BlockInfo& bi, const double* inv) {
   FdTile& ftile = reinterpret_cast<FdTile&>(tile);
-  double acc = 0.0;
-  PERSISTENT_BLOCKS(bi) {
-    const int b = bi.id;
-    const double h = bi.h;
-    double c[8];
-    load_col(A.r, b, G, c);
-    block_inverse_group(c, ftile, G, h, inv);
-    double s = 0.0;
+  const int b = bi.id;
+  const double h = bi.h;
+  double c[8];
+  load_col(A.r, b, G, c);
+  block_inverse_group(c, ftile, G, h, inv);
+  double s = 0.0;
 #pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      c[z] = double(T(c[z]));
-      s += c[z];
-    }
-    store_col(A.z1, b, G, c);
-    acc += s * h * h * h;
+  for (int z = 0; z < 8; ++z) {
+    c[z] = double(T(c[z]));
+    s += c[z];
   }
-  return acc;
+  store_col(A.z1, b, G, c);
+  return s * h * h * h;
 }
 
 // P1: z1 = zr + beta q (beta = 0 after a restart, which also sets rhat = r);
 //     nu = A z1; zv = M^-1 nu; (rhat, nu), sum(zv h^3)
 template <class T>
-__device__ __forceinline__ void phase_p1(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
-                                         const BlockInfo* cache, const double* inv, double beta, double ms,
-                                         bool restart, double (&acc)[2]) {
-  const DevMesh& M = A.M;
+__device__ __forceinline__ void p1_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, const BlockInfo& bi,
+                                         const double* inv, double beta, double ms, bool restart,
+                                         double (&acc)[2]) {
   FdTile& ftile = reinterpret_cast<FdTile&>(tile);
   const Comb2At<T> z1{A.z1, A.p, beta};
-  PERSISTENT_BLOCKS(bi) {
-    const int b = bi.id;
-    const double h = bi.h;
-    double col[8], y[8], rh[8];
-    {
-      double zr[8], q[8];
-      load_col(A.z1, b, G, zr);
-      load_col(A.p, b, G, q);
+  const int b = bi.id;
+  const double h = bi.h;
+  double col[8], y[8], rh[8];
+  {
+    double zr[8], q[8];
+    load_col(A.z1, b, G, zr);
+    load_col(A.p, b, G, q);
 #pragma unroll
-      for (int z = 0; z < 8; ++z) col[z] = zr[z] + beta * q[z];
-    }
-    spmv_group(bi, z1, col, ms, A.mean_mode, tile, G, y);
-    if (restart) {
-      load_col(A.r, b, G, rh);
-      store_col(A.rhat, b, G, rh);
-    } else {
-      load_col(A.rhat, b, G, rh);
-    }
-#pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      y[z] = double(T(y[z]));
-      acc[0] += rh[z] * y[z];
-    }
-    store_col(A.nu, b, G, y);
-    block_inverse_group(y, ftile, G, h, inv);
-    double s = 0.0;
-#pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      y[z] = double(T(y[z]));
-      s += y[z];
-    }
-    store_col(A.z2, b, G, y);
-    acc[1] += s * h * h * h;
+    for (int z = 0; z < 8; ++z) col[z] = zr[z] + beta * q[z];
   }
+  spmv_group(bi, z1, col, ms, A.mean_mode, tile, G, y);
+  if (restart) {
+    load_col(A.r, b, G, rh);
+    store_col(A.rhat, b, G, rh);
+  } else {
+    load_col(A.rhat, b, G, rh);
+  }
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    y[z] = double(T(y[z]));
+    acc[0] += rh[z] * y[z];
+  }
+  store_col(A.nu, b, G, y);
+  block_inverse_group(y, ftile, G, h, inv);
+  double s = 0.0;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    y[z] = double(T(y[z]));
+    s += y[z];
+  }
+  store_col(A.z2, b, G, y);
+  acc[1] += s * h * h * h;
 }
 
 // P2: t = A (zr - alpha zv); s = r - alpha nu; (t, s), (t, t)
 template <class T>
-__device__ __forceinline__ void phase_p2(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
-                                         const BlockInfo* cache, double alpha, double ms, double (&acc)[2]) {
-  const DevMesh& M = A.M;
+__device__ __forceinline__ void p2_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, const BlockInfo& bi,
+                                         double alpha, double ms, double (&acc)[2]) {
   const Comb2At<T> z2{A.z1, A.z2, -alpha};
-  PERSISTENT_BLOCKS(bi) {
-    const int b = bi.id;
-    double col[8], y[8];
-    {
-      double zr[8], zv[8];
-      load_col(A.z1, b, G, zr);
-      load_col(A.z2, b, G, zv);
+  const int b = bi.id;
+  double col[8], y[8];
+  {
+    double zr[8], zv[8];
+    load_col(A.z1, b, G, zr);
+    load_col(A.z2, b, G, zv);
 #pragma unroll
-      for (int z = 0; z < 8; ++z) col[z] = zr[z] - alpha * zv[z];
-    }
-    spmv_group(bi, z2, col, ms, A.mean_mode, tile, G, y);
-    double r[8], nu[8];
-    load_col(A.r, b, G, r);
-    load_col(A.nu, b, G, nu);
-#pragma unroll
-    for (int z = 0; z < 8; ++z) {
-      y[z] = double(T(y[z]));
-      const double sv = double(T(r[z] - alpha * nu[z]));
-      acc[0] += y[z] * sv;
-      acc[1] += y[z] * y[z];
-    }
-    store_col(A.t, b, G, y);
+    for (int z = 0; z < 8; ++z) col[z] = zr[z] - alpha * zv[z];
   }
+  spmv_group(bi, z2, col, ms, A.mean_mode, tile, G, y);
+  double r[8], nu[8];
+  load_col(A.r, b, G, r);
+  load_col(A.nu, b, G, nu);
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    y[z] = double(T(y[z]));
+    const double sv = double(T(r[z] - alpha * nu[z]));
+    acc[0] += y[z] * sv;
+    acc[1] += y[z] * y[z];
+  }
+  store_col(A.t, b, G, y);
 }
 
 // P3: x_new = x + alpha z1 + omega z2; r = s - omega t; q = z1 - omega zv;
 //     zr = M^-1 r; (rhat, r), (r, r), sum(zr h^3), sum(q h^3)
 template <class T>
-__device__ __forceinline__ void phase_p3(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
-                                         const BlockInfo* cache, const double* inv, const T* xc, T* xn,
-                                         double alpha, double beta, double omega, double (&acc)[4]) {
-  const DevMesh& M = A.M;
+__device__ __forceinline__ void p3_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile, const BlockInfo& bi,
+                                         const double* inv, const T* xc, T* xn, double alpha, double beta,
+                                         double omega, double (&acc)[4]) {
   FdTile& ftile = reinterpret_cast<FdTile&>(tile);
-  PERSISTENT_BLOCKS(bi) {
-    const int b = bi.id;
-    const double h = bi.h, h3 = h * h * h;
-    double rn[8], sq = 0.0;
-    {
-      double r[8], nu[8], t[8], rh[8];
-      load_col(A.r, b, G, r);
-      load_col(A.nu, b, G, nu);
-      load_col(A.t, b, G, t);
-      load_col(A.rhat, b, G, rh);
-#pragma unroll
-      for (int z = 0; z < 8; ++z) {
-        const double sv = double(T(r[z] - alpha * nu[z]));
-        rn[z] = double(T(sv - omega * t[z]));
-        acc[0] += rh[z] * rn[z];
-        acc[1] += rn[z] * rn[z];
-      }
-      store_col(A.r, b, G, rn);
-    }
-    {
-      double zr[8], q[8], zv[8], x[8];
-      load_col(A.z1, b, G, zr);
-      load_col(A.p, b, G, q);
-      load_col(A.z2, b, G, zv);
-      load_col(xc, b, G, x);
-#pragma unroll
-      for (int z = 0; z < 8; ++z) {
-        const double z1 = zr[z] + beta * q[z], z2 = zr[z] - alpha * zv[z];
-        x[z] = double(T((x[z] + alpha * z1) + omega * z2));
-        q[z] = double(T(z1 - omega * zv[z]));
-        sq += q[z];
-      }
-      store_col(xn, b, G, x);
-      store_col(A.p, b, G, q);
-    }
-    block_inverse_group(rn, ftile, G, h, inv);
-    double s = 0.0;
+  const int b = bi.id;
+  const double h = bi.h, h3 = h * h * h;
+  double rn[8], sq = 0.0;
+  {
+    double r[8], nu[8], t[8], rh[8];
+    load_col(A.r, b, G, r);
+    load_col(A.nu, b, G, nu);
+    load_col(A.t, b, G, t);
+    load_col(A.rhat, b, G, rh);
 #pragma unroll
     for (int z = 0; z < 8; ++z) {
-      rn[z] = double(T(rn[z]));
-      s += rn[z];
+      const double sv = double(T(r[z] - alpha * nu[z]));
+      rn[z] = double(T(sv - omega * t[z]));
+      acc[0] += rh[z] * rn[z];
+      acc[1] += rn[z] * rn[z];
     }
-    store_col(A.z1, b, G, rn);
-    acc[2] += s * h3;
-    acc[3] += sq * h3;
+    store_col(A.r, b, G, rn);
   }
+  {
+    double zr[8], q[8], zv[8], x[8];
+    load_col(A.z1, b, G, zr);
+    load_col(A.p, b, G, q);
+    load_col(A.z2, b, G, zv);
+    load_col(xc, b, G, x);
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      const double z1 = zr[z] + beta * q[z], z2 = zr[z] - alpha * zv[z];
+      x[z] = double(T((x[z] + alpha * z1) + omega * z2));
+      q[z] = double(T(z1 - omega * zv[z]));
+      sq += q[z];
+    }
+    store_col(xn, b, G, x);
+    store_col(A.p, b, G, q);
+  }
+  block_inverse_group(rn, ftile, G, h, inv);
+  double s = 0.0;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    rn[z] = double(T(rn[z]));
+    s += rn[z];
+  }
+  store_col(A.z1, b, G, rn);
+  acc[2] += s * h3;
+  acc[3] += sq * h3;
 }
 
 // Every CTA keeps a copy of the Krylov state in shared memory and applies
@@ -1018,7 +1008,8 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
   __syncthreads();
   bool ok = true;
   if (!S.done) {
-    double a[1] = {phase_p0<T>(A, G, tile, cache, inv_eig)};
+    double a[1] = {0.0};
+    PERSISTENT_BLOCKS(bi) a[0] += p0_block<T>(A, G, tile, bi, inv_eig);
     ok = grid_allreduce<1>(a, Gs, epoch, red);
     // q = 0 at the start (p of k_bicg_init), so z1 = zr
     if (threadIdx.x == 0) ms_zr = S.mean_sum = a[0];
@@ -1028,7 +1019,7 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
     const bool restart = S.restart_pending != 0;
     const double beta = restart ? 0.0 : S.beta;
     double a[2] = {0.0, 0.0};
-    phase_p1<T>(A, G, tile, cache, inv_eig, beta, S.mean_sum, restart, a);
+    PERSISTENT_BLOCKS(bi) p1_block<T>(A, G, tile, bi, inv_eig, beta, S.mean_sum, restart, a);
     if (!(ok = grid_allreduce<2>(a, Gs, epoch, red))) break;
     if (threadIdx.x == 0) {
       fin_a(S, S.mean_sum, restart);
@@ -1038,12 +1029,13 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
     }
     __syncthreads();
     double d[2] = {0.0, 0.0};
-    phase_p2<T>(A, G, tile, cache, S.alpha, S.mean_sum, d);
+    PERSISTENT_BLOCKS(bi) p2_block<T>(A, G, tile, bi, S.alpha, S.mean_sum, d);
     if (!(ok = grid_allreduce<2>(d, Gs, epoch, red))) break;
     if (threadIdx.x == 0) fin_d(S, d);
     __syncthreads();
     double e[4] = {0.0, 0.0, 0.0, 0.0};
-    phase_p3<T>(A, G, tile, cache, inv_eig, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.beta, S.omega, e);
+    PERSISTENT_BLOCKS(bi)
+        p3_block<T>(A, G, tile, bi, inv_eig, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.beta, S.omega, e);
     if (!(ok = grid_allreduce<4>(e, Gs, epoch, red))) break;
     if (threadIdx.x == 0) {
       const double re[2] = {e[0], e[1]};
@@ -1060,6 +1052,255 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
       S.status = SOLVE_BARRIER_TIMEOUT;
     }
     *A.st = S;
+  }
+}
+
+// ---- batched persistent solver: independent cases in one launch ----------
+// The mesh holds several independent cases (no face joins two cases).  Every
+// block group works for one case and holds that case's Krylov state in
+// shared memory; the groups of a case sum only their own partials, in group
+// order, so each case runs its own BiCGSTAB (scalars, restarts, stopping
+// test, best iterate) while all cases share the grid barriers.  A case that
+// has stopped leaves its vectors alone; the launch ends when every case has
+// stopped.  Preparation (x0's mean row, sum(x0 h^3)), the initial residual
+// and zr = M^-1 r run in the same launch.
+
+// Sum of v over the 64 threads of a group, in a fixed order; every thread of
+// the group gets the totals.  gsm: 2 * NR doubles of the group.
+template <int NR>
+__device__ __forceinline__ void group_reduce(double (&v)[NR], double* gsm, const GroupIdx& G) {
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_xor_sync(0xffffffffu, v[r], o);
+  if ((G.lane & 31) == 0)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) gsm[(G.lane >> 5) * NR + r] = v[r];
+  group_sync(G.g);
+#pragma unroll
+  for (int r = 0; r < NR; ++r) v[r] = gsm[r] + gsm[NR + r];
+  group_sync(G.g);
+}
+
+struct BatchArgs {
+  const int* gcase;
+  const int* gfirst;
+  const int* goff;
+  const int* gblocks;
+  double* part;
+  int* case_done;
+  int ncase;
+  int groups;
+};
+
+// Grid barrier with per-case sums: each group's partials, then every group
+// of case c sums the partials of c's groups.  With ANY, also tells whether
+// any case was still running when the barrier was reached (case_done as
+// written before it).
+template <int NR, bool ANY>
+__device__ bool batch_allreduce(double (&v)[NR], const BatchArgs& B, const GridSync& Gs, unsigned int& epoch,
+                                double* gsm, const GroupIdx& G, int gidx, int c, bool* any) {
+  const unsigned int k = epoch;
+  double* part = B.part + size_t(k & 1u) * B.groups * 8;
+  group_reduce<NR>(v, gsm, G);
+  if (G.lane == 0)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) part[gidx * 8 + r] = v[r];
+  __shared__ int s_ok;
+  __syncthreads();  // the CTA's partials and phase stores precede the arrival
+  if (threadIdx.x == 0) {
+    red_add_release(Gs.arrive, 1u);
+    const unsigned int target = (k + 1u) * gridDim.x;
+    const long long t0 = clock64();
+    int ok = 1;
+    while (ld_acquire(Gs.arrive) < target) {
+      if (clock64() - t0 > kBarrierClockLimit) {
+        ok = 0;
+        break;
+      }
+    }
+    if (!ok) atomicExch(Gs.error, 1);
+    s_ok = ok;
+    epoch = k + 1u;
+  }
+  __syncthreads();
+  if (!s_ok) return false;
+  if (ANY) {
+    int running = 0;
+    for (int i = threadIdx.x; i < B.ncase; i += blockDim.x) running |= B.case_done[i] == 0;
+    *any = __syncthreads_or(running) != 0;
+  }
+  if (c >= 0) {
+    double acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = 0.0;
+    for (int g = B.gfirst[c] + G.lane; g < B.gfirst[c + 1]; g += GROUP)
+#pragma unroll
+      for (int r = 0; r < NR; ++r) acc[r] += part[g * 8 + r];
+    group_reduce<NR>(acc, gsm, G);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) v[r] = acc[r];
+  }
+  return true;
+}
+
+// A group's k-th block: the entries of its first KB_CACHE blocks are staged
+// at launch, later ones in the group's tile on the way.
+__device__ __forceinline__ const BlockInfo& batch_block(const DevMesh& M, const BlockInfo* cache, GroupTile& tile,
+                                                        const int* blocks, int k, const GroupIdx& G) {
+  if (k < KB_CACHE) return cache[G.g * KB_CACHE + k];
+  group_sync(G.g);
+  fill_block_info(M, blocks[k], tile.bi, G.lane);
+  group_sync(G.g);
+  return tile.bi;
+}
+
+#define BATCH_BLOCKS(bi) \
+  for (int k_ = 0; k_ < nblk; ++k_) if (const BlockInfo& bi = batch_block(M, cache, tile, myblocks, k_, G); true)
+
+// PREP: x0 = 0 on the case's mean row (modes 1 and 3); sum(x0 h^3)
+template <class T>
+__device__ __forceinline__ double prep_block(const KArgs<T>& A, const GroupIdx& G, const BlockInfo& bi) {
+  const int b = bi.id;
+  double c[8];
+  load_col(A.xs0, b, G, c);
+  if (A.zero_mean_row && bi.mean && G.lane == 0) {
+    A.xs0[size_t(b) * BN] = T(0);
+    c[0] = 0.0;
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) s += c[z];
+  return s * bi.h * bi.h * bi.h;
+}
+
+// INIT: r = b - A x0 (b = 0 on the mean row for modes 1 and 3), rhat = r,
+// p = 0; (r, r)
+template <class T>
+__device__ __forceinline__ double init_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
+                                             const BlockInfo& bi, double ms) {
+  const int b = bi.id;
+  double col[8], y[8], bc[8];
+  load_col(A.xs0, b, G, col);
+  spmv_group(bi, VecAt<T>{A.xs0}, col, ms, A.mean_mode, tile, G, y);
+  load_col(A.b, b, G, bc);
+  if (A.zero_mean_row && bi.mean && G.lane == 0) bc[0] = 0.0;
+  double r[8], zero[8], acc = 0.0;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    r[z] = double(T(bc[z] - y[z]));
+    zero[z] = 0.0;
+    acc += r[z] * r[z];
+  }
+  store_col(A.r, b, G, r);
+  store_col(A.rhat, b, G, r);
+  store_col(A.p, b, G, zero);
+  return acc;
+}
+
+template <class T>
+__global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, GridSync Gs, BatchArgs B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw);
+  double* inv_eig = reinterpret_cast<double*>(smem_raw + PGROUPS * sizeof(GroupTile));
+  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + PGROUPS * sizeof(GroupTile) + BN * sizeof(double));
+  __shared__ KrylovState Sg[PGROUPS];
+  __shared__ double gsm_all[PGROUPS][16];
+  __shared__ double ms_zr_g[PGROUPS];
+  __shared__ unsigned int epoch;
+  const GroupIdx G;
+  const DevMesh& M = A.M;
+  GroupTile& tile = tiles[G.g];
+  double* gsm = gsm_all[G.g];
+  KrylovState& S = Sg[G.g];
+  double& ms_zr = ms_zr_g[G.g];
+  const int gidx = blockIdx.x * PGROUPS + G.g;
+  const int c = B.gcase[gidx];
+  const int* myblocks = B.gblocks + B.goff[gidx];
+  const int nblk = c >= 0 ? B.goff[gidx + 1] - B.goff[gidx] : 0;
+  const bool lead = c >= 0 && gidx == B.gfirst[c];  // writes the case's state and done flag
+  fd_fill_inverse_eigen(inv_eig, c_lam);
+  for (int k = 0; k < KB_CACHE && k < nblk; ++k)
+    if (G.lane < 32) fill_block_info(M, myblocks[k], cache[G.g * KB_CACHE + k], G.lane);
+  if (G.lane == 0 && c >= 0) S = A.st[c];
+  if (threadIdx.x == 0) epoch = 0u;
+  __syncthreads();
+  bool ok = true, any = true;
+  // PREP, INIT, P0: one barrier each
+  {
+    double a[1] = {0.0};
+    BATCH_BLOCKS(bi) a[0] += prep_block<T>(A, G, bi);
+    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, c, nullptr);
+    if (ok && c >= 0 && G.lane == 0) S.mean_sum = a[0];
+    __syncthreads();
+  }
+  if (ok) {
+    double a[1] = {0.0};
+    BATCH_BLOCKS(bi) a[0] += init_block<T>(A, G, tile, bi, S.mean_sum);
+    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, c, nullptr);
+    if (ok && c >= 0 && G.lane == 0) {
+      fin_init(S, a[0]);
+      if (lead) B.case_done[c] = S.done;
+    }
+    __syncthreads();
+  }
+  if (ok) {
+    double a[1] = {0.0};
+    if (c >= 0 && !S.done) BATCH_BLOCKS(bi) a[0] += p0_block<T>(A, G, tile, bi, inv_eig);
+    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, c, nullptr);
+    // q = 0 at the start, so z1 = zr
+    if (ok && c >= 0 && G.lane == 0) ms_zr = S.mean_sum = a[0];
+    __syncthreads();
+  }
+  while (ok) {
+    const bool active = c >= 0 && !S.done;
+    const bool restart = active && S.restart_pending != 0;
+    const double beta = restart ? 0.0 : S.beta;
+    double a[2] = {0.0, 0.0};
+    if (active) BATCH_BLOCKS(bi) p1_block<T>(A, G, tile, bi, inv_eig, beta, S.mean_sum, restart, a);
+    if (!(ok = batch_allreduce<2, true>(a, B, Gs, epoch, gsm, G, gidx, c, &any))) break;
+    if (!any) break;  // every case had stopped: this pass did no work
+    if (active && G.lane == 0) {
+      fin_a(S, S.mean_sum, restart);
+      fin_b(S, a[0]);
+      S.beta = beta;                        // the beta that formed z1, for P3
+      S.mean_sum = ms_zr - S.alpha * a[1];  // sum(z2 h^3)
+    }
+    __syncthreads();
+    double d[2] = {0.0, 0.0};
+    if (active) BATCH_BLOCKS(bi) p2_block<T>(A, G, tile, bi, S.alpha, S.mean_sum, d);
+    if (!(ok = batch_allreduce<2, false>(d, B, Gs, epoch, gsm, G, gidx, c, nullptr))) break;
+    if (active && G.lane == 0) fin_d(S, d);
+    __syncthreads();
+    double e[4] = {0.0, 0.0, 0.0, 0.0};
+    if (active)
+      BATCH_BLOCKS(bi) p3_block<T>(A, G, tile, bi, inv_eig, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.beta,
+                                   S.omega, e);
+    if (!(ok = batch_allreduce<4, false>(e, B, Gs, epoch, gsm, G, gidx, c, nullptr))) break;
+    if (active && G.lane == 0) {
+      const double re[2] = {e[0], e[1]};
+      fin_e(S, re);
+      ms_zr = e[2];
+      S.mean_sum = S.restart_pending ? e[2] : e[2] + S.beta * e[3];  // sum(z1 h^3) of the next P1
+      if (lead) B.case_done[c] = S.done;
+    }
+    __syncthreads();
+  }
+  // each group moves its blocks' best iterate into x (slot 0)
+  if (ok && c >= 0 && S.best != 0) {
+    const T* src = xslot(A, S.best);
+    BATCH_BLOCKS(bi) {
+      double v[8];
+      load_col(src, bi.id, G, v);
+      store_col(A.xs0, bi.id, G, v);
+    }
+  }
+  if (lead && G.lane == 0) {
+    if (!ok) {
+      S.done = 1;
+      S.status = SOLVE_BARRIER_TIMEOUT;
+    }
+    A.st[c] = S;
   }
 }
 
@@ -1243,6 +1484,71 @@ static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, 
   void* args[] = {(void*)&Aa, (void*)&Gs};
   ProfScope ps(name, s);
   CUP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(PNT), args, dyn, s));
+  return 0;
+}
+
+// CTAs and block groups of the batched solver: every CTA resident (one
+// group per block at most), the same shape as the single-case solver.
+int batch_solver_shape(int nb, int* grid, int* groups) {
+  const size_t dyn = kPersistentSmem;
+  void (*kern)(KArgs<double>, GridSync, BatchArgs) = k_bicg_batched<double>;
+  CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+  int per_sm = 0, dev = 0, sms = 0;
+  CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PNT, dyn));
+  CUP_CUDA_TRY(cudaGetDevice(&dev));
+  CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (per_sm < 1) return set_error(CUP_ERR_CUDA, "batched BiCGSTAB: kernel does not fit on an SM");
+  *grid = std::max(1, std::min(per_sm * sms, (nb + PGROUPS - 1) / PGROUPS));
+  *groups = *grid * PGROUPS;
+  return 0;
+}
+
+int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
+                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s) {
+  poisson_init_constants();
+  if (B.ncase < 1 || !B.st) return set_error(CUP_ERR_STATE, "batched BiCGSTAB: not a batch");
+  double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
+  const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
+  std::vector<KrylovState> init(B.ncase);
+  for (KrylovState& k : init) {
+    k = KrylovState{};
+    k.tol_abs = P.tol_abs;
+    k.tol_rel = P.tol_rel;
+    k.max_iter = P.max_iter;
+    k.max_restarts = P.max_restarts;
+    k.stall_window = P.stall_window;
+    k.eps = 1e-21;
+  }
+  CUP_CUDA_TRY(cudaMemcpyAsync(B.st, init.data(), sizeof(KrylovState) * B.ncase, cudaMemcpyHostToDevice, s));
+  CUP_CUDA_TRY(cudaMemsetAsync(B.case_done, 0, sizeof(int) * B.ncase, s));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
+  KArgs<double> A = make_args<double>(M, b, x, v, W, B.st, P.mean_mode, zmr, 0);
+  A.ncache = KB_CACHE;
+  GridSync Gs{W.bar, W.partial, W.bar_error};
+  BatchArgs Ba{B.gcase, B.gfirst, B.goff, B.gblocks, B.part, B.case_done, B.ncase, B.groups};
+  void* args[] = {(void*)&A, (void*)&Gs, (void*)&Ba};
+  const size_t dyn = kPersistentSmem;
+  void (*kern)(KArgs<double>, GridSync, BatchArgs) = k_bicg_batched<double>;
+  CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+  {
+    ProfScope ps("bicg_batched", s);
+    CUP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(B.grid), dim3(PNT), args, dyn, s));
+  }
+  int h_err = 0;
+  std::vector<KrylovState> fin(B.ncase);
+  CUP_CUDA_TRY(cudaMemcpyAsync(&h_err, W.bar_error, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUP_CUDA_TRY(cudaMemcpyAsync(fin.data(), B.st, sizeof(KrylovState) * B.ncase, cudaMemcpyDeviceToHost, s));
+  CUP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h_err) return set_error(CUP_ERR_CUDA, "batched BiCGSTAB: a grid barrier wait timed out");
+  for (int c = 0; c < B.ncase; ++c) {
+    out[c].iterations = fin[c].k;
+    out[c].restarts = fin[c].restarts;
+    out[c].status = fin[c].done ? fin[c].status : SOLVE_MAXITER;
+    out[c].outer = 0;
+    out[c].err_init = fin[c].err_init;
+    out[c].err_opt = fin[c].err_opt;
+  }
   return 0;
 }
 

@@ -50,6 +50,22 @@ struct PoissonWork {
   int ggrid;                // CTAs for block-group kernels (4 mesh blocks per CTA pass)
 };
 
+// Batched solves: independent cases on disjoint blocks of one flattened mesh
+// (no face joins two cases), all in one cooperative launch.  Every block
+// group of the batched solver works for one case.
+struct BatchWork {
+  int ncase = 0;
+  int grid = 0;                  // CTAs of the batched solver
+  int groups = 0;                // grid * groups per CTA
+  int* gcase = nullptr;          // groups: case of each group (-1: idle)
+  int* gfirst = nullptr;         // ncase + 1: the groups of case c are gfirst[c] .. gfirst[c+1]-1
+  int* goff = nullptr;           // groups + 1: group g visits gblocks[goff[g] .. goff[g+1])
+  int* gblocks = nullptr;        // nb
+  double* part = nullptr;        // 2 * groups * 8 partial sums
+  int* case_done = nullptr;      // ncase: 1 once the case has stopped
+  KrylovState* st = nullptr;     // ncase
+};
+
 struct SolveParams {
   double tol_abs, tol_rel;
   int max_iter, max_restarts, mean_mode;
@@ -92,5 +108,11 @@ void poisson_init_constants();
 // Number of 64-thread groups of the persistent solver on a mesh of nb blocks
 // (the visit order is balanced for this many groups).
 int persistent_solver_groups(int nb, const PoissonWork& W, int* groups);
+// CTAs and block groups of the batched solver (all co-resident).
+int batch_solver_shape(int nb, int* grid, int* groups);
+// One BiCGSTAB per case of the batch (x holds x0 on entry and each case's
+// best iterate on exit); out[c] per case.
+int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
+                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s);
 
 }  // namespace cup3d

@@ -148,6 +148,24 @@ int cup_poisson_solve_dev(cup_ctx* ctx, const double* d_b, double* d_x, cup_solv
 /* ---- PoissonSolverBase::solve(): RHS in CUP_FIELD_LHS, guess and result in CUP_FIELD_PRES ---- */
 int cup_poisson_solve(cup_ctx* ctx, cup_solve_stats* stats);
 
+/* ---- batches of independent cases (no counterpart in the reference, which
+ * runs one case per process) ---- */
+/* A new context over the meshes of ncases device contexts, concatenated in
+ * case order (case k's blocks follow case k-1's, each case in its own block
+ * order); the cases keep their own mean-constraint rows.  The other settings
+ * (tolerances, -bMeanConstraint, device) are case 0's; every case must use
+ * the same device and -bMeanConstraint.  The cases are not modified.  NULL on
+ * failure: cup_last_error(NULL). */
+cup_ctx* cup_batch_create(int32_t ncases, cup_ctx* const* cases);
+int32_t cup_batch_num_cases(const cup_ctx* batch);  /* 1 for a plain context */
+/* Blocks first .. first+nblocks-1 of the batch (and of its fields) are case k's. */
+int cup_batch_case_blocks(const cup_ctx* batch, int32_t k, int32_t* first, int32_t* nblocks);
+/* One BiCGSTAB per case, all in one device launch: each case has its own
+ * scalars, restarts, stopping test and best iterate.  d_x (16-byte aligned):
+ * initial guess in, each case's solution out; stats[ncases].  Returns the
+ * worst outcome over the cases (true_rel is not computed: -1). */
+int cup_batch_poisson_solve_dev(cup_ctx* batch, const double* d_b, double* d_x, cup_solve_stats* stats);
+
 /* ---- obstacles (host-side CreateObstacles; one body per context) ---- */
 /* Sphere of radius r at c (Sphere.cpp); chi by ObstaclesCreate.cpp:18-121;
  * kin = velocity[3], angular velocity[3] (may be NULL).  Also sets CUP_FIELD_CHI. */

@@ -91,3 +91,11 @@ def test_config_parse_flags():
     assert cup.config("-poissonBlockCache 0").poisson_block_cache == 0
     with pytest.raises(cup.CupError):
         cup.config("-poissonBlockCache 5")
+
+
+def test_batch_needs_device_contexts():
+    ctx = cup.Context(cup.config("-bpdx 2 -bpdy 2 -bpdz 2", device=-1))
+    ctx.set_mesh_uniform()
+    with pytest.raises(cup.CupError, match="device context"):
+        cup.Batch([ctx])
+    assert cup.lib().cup_batch_num_cases(ctx._p) == 1
