@@ -47,3 +47,51 @@ def poisson_rhs(ctx):
         b += 10.0 * rng.standard_normal() * np.exp(-d2 / (2.0 * sigma ** 2))
     w = hh ** 3
     return b - np.sum(b * w) / np.sum(w)
+
+
+# Swarm of independent penalized ellipsoids (semi-axes 0.1 x 0.05 x 0.05),
+# one per case: case i draws from PCG64(64 + i) a unit quaternion uniform on
+# S^3, a speed uniform in [0.05, 0.2] along the body's long axis, 2 or 3
+# level-0 blocks per side of the unit cube, 3 or 4 levels and a centre in
+# [0.35, 0.65]^3; the mesh is refined around the body (near radius 0.6 of the
+# domain at the coarsest level, no wake), which gives 372-2659 blocks per case
+# over the first 64 cases (73,239 blocks, 37.5M cells in all).
+SWARM_AXES = (0.1, 0.05, 0.05)
+SWARM_FLAGS = ("-extent 1 -nu 1e-4 -CFL 0.3 -lambda 1e6 -advection weno5 -poissonTol 1e-6 "
+               "-poissonTolRel 1e-4 -rampup 0")
+SWARM_WORKLOAD = "ellipsoid_swarm_64_cases_weno5_fp64"
+
+
+def swarm_case(i):
+    """Parameters of swarm case i (see above)."""
+    rng = np.random.Generator(np.random.PCG64(64 + i))
+    q = rng.standard_normal(4)
+    q /= np.linalg.norm(q)
+    speed = rng.uniform(0.05, 0.2)
+    bpd = 2 + int(rng.integers(0, 2))
+    level_max = 3 + int(rng.integers(0, 2))
+    center = rng.uniform(0.35, 0.65, 3)
+    w, x, y, z = q
+    long_axis = np.array([1 - 2 * (y * y + z * z), 2 * (x * y + w * z), 2 * (x * z - w * y)])
+    return dict(quat=q, vel=speed * long_axis, bpd=bpd, level_max=level_max, center=center)
+
+
+def make_swarm_ctx(i, device):
+    """Context of swarm case i with its mesh and its ellipsoid."""
+    import cup3d_b200 as cup
+    p = swarm_case(i)
+    b = p["bpd"]
+    cfg = cup.config(SWARM_FLAGS + f" -bpdx {b} -bpdy {b} -bpdz {b} -levelMax {p['level_max']}", device=device)
+    ctx = cup.Context(cfg)
+    ctx.set_mesh_sphere_wake(p["center"], SWARM_AXES[0], 1, near_radius=0.6, wake_len=0.0, wake_radius=0.6)
+    if device >= 0:
+        ctx.obstacle_ellipsoid(p["center"], SWARM_AXES, p["quat"], vel=p["vel"])
+    return ctx
+
+
+def swarm_rhs(ctx, i):
+    """Seeded Poisson right-hand side of swarm case i: N(0,1) white noise per
+    cell from PCG64(1000 + i), made h^3-weighted zero-mean."""
+    hh = np.repeat(ctx.blocks()[2], 512)
+    b = np.random.Generator(np.random.PCG64(1000 + i)).standard_normal(len(hh))
+    return b - np.sum(b * hh ** 3) / np.sum(hh ** 3)
