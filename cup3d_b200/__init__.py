@@ -324,6 +324,23 @@ class Batch(Context):
         check(lib().cup_batch_case_blocks(self._p, k, C.byref(first), C.byref(n)), self._p)
         return first.value, n.value
 
+    def step(self, step, dt=None):
+        """One time step of every case: (rc, dt per case, force/torque (ncase, 6),
+        [stats per case]).  dt: per-case time steps, None for each case's CFL."""
+        dt_in = None if dt is None else np.ascontiguousarray(dt, np.float64)
+        dt_used = np.zeros(self.ncase)
+        force = np.zeros((self.ncase, 6))
+        st = (cup_solve_stats * self.ncase)()
+        rc = check(lib().cup_batch_step(self._p, step, None if dt_in is None else dptr(dt_in), dptr(dt_used),
+                                        dptr(force), st), self._p)
+        return rc, dt_used, force, [s.as_dict() for s in st]
+
+    def case_field(self, name, k):
+        """Case k's part of a downloaded field, (ncomp, nblocks*512)."""
+        first, n = self.case_blocks(k)
+        f = self.download(name).reshape(FIELD_NCOMP[name], -1)
+        return f[:, first * 512:(first + n) * 512]
+
     def poisson_solve_dev(self, b, x):
         """One BiCGSTAB per case in one launch: (rc, [stats per case])."""
         st = (cup_solve_stats * self.ncase)()

@@ -9,6 +9,7 @@
 #include <numeric>
 
 #include "context.h"
+#include "stencils.cuh"
 
 namespace cup3d {
 
@@ -102,6 +103,12 @@ static int plan_groups(const std::vector<Mesh>& cases, const std::vector<int>& f
   return 0;
 }
 
+// Keeps the thread's last error message on the context.
+static int keep_err(cup_ctx* c, int rc) {
+  c->err = cup_last_error(nullptr);
+  return rc;
+}
+
 static int upload_ints(cup_ctx* c, int** dst, const std::vector<int>& v) {
   if (int rc = c->batch_arena.alloc(dst, v.size())) return rc;
   CUP_CUDA_TRY(stream_h2d(c->stream, *dst, v.data(), v.size() * sizeof(int)));
@@ -139,6 +146,111 @@ static int batch_setup(cup_ctx* c, const std::vector<Mesh>& cases) {
   return 0;
 }
 
+// The cases' current fields (velocity, pressure, grid chi) into the batch's.
+static int copy_case_fields(cup_ctx* c, const std::vector<const cup_ctx*>& cases) {
+  const size_t N = size_t(c->mesh.nb) * BN;
+  for (size_t k = 0; k < cases.size(); ++k) {
+    const cup_ctx* s = cases[k];
+    CUP_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    const size_t n = size_t(s->mesh.nb) * BN, off = size_t(c->case_first[k]) * BN;
+    for (int d = 0; d < 3; ++d)
+      CUP_CUDA_TRY(cudaMemcpyAsync(c->F.vel[c->F.vcur] + d * N + off, s->F.vel[s->F.vcur] + d * n, n * 8,
+                                   cudaMemcpyDeviceToDevice, c->stream));
+    CUP_CUDA_TRY(cudaMemcpyAsync(c->F.pres[c->F.pcur] + off, s->F.pres[s->F.pcur], n * 8, cudaMemcpyDeviceToDevice,
+                                 c->stream));
+    CUP_CUDA_TRY(cudaMemcpyAsync(c->F.chi + off, s->F.chi, n * 8, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+// The cases' obstacles, concatenated in case order (slots of case k are
+// slot_first[k] .. slot_first[k+1]-1), and the per-case buffers of the step.
+static int batch_step_setup(cup_ctx* c, const std::vector<const cup_ctx*>& cases) {
+  const int K = c->ncase;
+  std::vector<int> blocks, slot_first(K + 1, 0);
+  std::vector<double> chi, udef, kin(9 * size_t(K), 0.0);
+  for (int k = 0; k < K; ++k) {
+    const DevObstacle& o = cases[k]->ob;
+    slot_first[k + 1] = slot_first[k] + o.nslots;
+    for (int sl = 0; sl < o.nslots; ++sl) blocks.push_back(o.h_blocks[sl] + c->case_first[k]);
+    chi.insert(chi.end(), o.h_chi.begin(), o.h_chi.end());
+    for (int i = 0; i < 9; ++i) kin[9 * k + i] = o.kin[i];
+  }
+  const int NS = slot_first[K];
+  udef.assign(3 * size_t(NS) * BN, 0.0);
+  for (int d = 0; d < 3; ++d)
+    for (int k = 0; k < K; ++k) {
+      const DevObstacle& o = cases[k]->ob;
+      for (int sl = 0; sl < o.nslots; ++sl)
+        std::copy_n(o.h_udef.begin() + (size_t(d) * o.nslots + sl) * BN, BN,
+                    udef.begin() + (size_t(d) * NS + slot_first[k] + sl) * BN);
+    }
+  if (NS > 0)
+    if (int rc = ctx_upload_obstacle(c, NS, blocks.data(), chi.data(), udef.data(), kin.data())) return rc;
+  BatchStep& T = c->T;
+  DevArena& A = c->batch_arena;
+  if (int rc = upload_ints(c, &T.first, c->case_first)) return rc;
+  if (int rc = upload_ints(c, &T.slot_first, slot_first)) return rc;
+  if (int rc = A.alloc(&T.dt, size_t(K))) return rc;
+  if (int rc = A.alloc(&T.sums, 2 * size_t(K))) return rc;
+  if (int rc = A.alloc(&T.kin, 9 * size_t(K))) return rc;
+  if (int rc = A.alloc(&T.umax, size_t(K))) return rc;
+  if (int rc = A.alloc(&T.force, 6 * size_t(K))) return rc;
+  if (int rc = A.alloc(&T.bscratch, 2 * size_t(c->mesh.nb))) return rc;
+  if (int rc = A.alloc(&T.slot_force, 6 * size_t(std::max(NS, 1)))) return rc;
+  CUP_CUDA_TRY(stream_h2d(c->stream, T.kin, kin.data(), kin.size() * 8));
+  CUP_CUDA_TRY(stream_zero(c->stream, T.force, 6 * size_t(K) * 8));
+  c->dm.case_dt = T.dt;
+  c->dm.case_sums = T.sums;
+  c->dm.case_kin = T.kin;
+  return 0;
+}
+
+static ObstacleView batch_ob_view(const cup_ctx* c) {
+  ObstacleView v;
+  v.nslots = c->ob.nslots;
+  v.slot = c->ob.slot_of_block;
+  v.near = c->ob.near;
+  v.chi = c->ob.chi;
+  v.udef = c->ob.udef;
+  v.blk = c->ob.block_of_slot;
+  return v;
+}
+
+static SolveParams batch_params(const cup_ctx* c) {
+  SolveParams P{};
+  P.tol_abs = c->cfg.poisson_tol;
+  P.tol_rel = c->cfg.poisson_tol_rel;
+  P.max_iter = c->cfg.poisson_max_iter;
+  P.max_restarts = c->cfg.poisson_max_restarts;
+  P.mean_mode = c->cfg.mean_constraint;
+  P.persistent = 1;
+  P.block_cache = c->cfg.poisson_block_cache;
+  return P;
+}
+
+// Worst outcome over the cases, stats per case.
+static int batch_stats(cup_ctx* c, const std::vector<SolveStats>& S, float ms, cup_solve_stats* stats) {
+  int rc = CUP_OK;
+  for (int k = 0; k < c->ncase; ++k) {
+    if (stats) {
+      cup_solve_stats& o = stats[k];
+      o.iterations = S[k].iterations;
+      o.restarts = S[k].restarts;
+      o.status = S[k].status;
+      o.fallback = 0;
+      o.err_init = S[k].err_init;
+      o.err_final = S[k].err_opt;
+      o.true_rel = -1.0;
+      o.milliseconds = ms;
+    }
+    if (S[k].status == SOLVE_NAN) rc = ctx_fail(c, CUP_ERR_NAN, "batched Poisson solve produced NaN");
+    else if (S[k].status != SOLVE_CONVERGED && rc == CUP_OK) rc = CUP_SOFT_MAXITER;
+  }
+  return rc;
+}
+
 }  // namespace cup3d
 
 using namespace cup3d;
@@ -165,7 +277,11 @@ cup_ctx* cup_batch_create(int32_t ncases, cup_ctx* const* cases) {
   }
   cup_ctx* c = cup_create(&cases[0]->cfg);
   if (!c) return nullptr;
-  if (int rc = batch_setup(c, meshes)) {
+  const std::vector<const cup_ctx*> cs(cases, cases + ncases);
+  int rc = batch_setup(c, meshes);
+  if (rc == 0) rc = copy_case_fields(c, cs);
+  if (rc == 0) rc = batch_step_setup(c, cs);
+  if (rc) {
     (void)rc;
     const std::string msg = "cup_batch_create: " + std::string(cup_last_error(nullptr));
     cup_destroy(c);
@@ -194,39 +310,77 @@ int cup_batch_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solv
   if (!c || !b || !x || !stats || c->ncase < 2) return ctx_fail(c, CUP_ERR_ARG, "cup_batch_poisson_solve_dev: not a batch or bad arguments");
   if (reinterpret_cast<uintptr_t>(x) % 16 != 0 || reinterpret_cast<uintptr_t>(b) % 16 != 0)
     return ctx_fail(c, CUP_ERR_ARG, "cup_batch_poisson_solve_dev: b and x must be 16-byte aligned");
-  SolveParams P{};
-  P.tol_abs = c->cfg.poisson_tol;
-  P.tol_rel = c->cfg.poisson_tol_rel;
-  P.max_iter = c->cfg.poisson_max_iter;
-  P.max_restarts = c->cfg.poisson_max_restarts;
-  P.mean_mode = c->cfg.mean_constraint;
-  P.persistent = 1;
-  P.block_cache = c->cfg.poisson_block_cache;
+  const SolveParams P = batch_params(c);
   std::vector<SolveStats> S(c->ncase);
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
-  if (int rc = poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S.data(), c->stream)) {
-    c->err = cup_last_error(nullptr);
-    return rc;
-  }
+  if (int rc = poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S.data(), c->stream)) return keep_err(c, rc);
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   CUP_CUDA_TRY(cudaEventSynchronize(c->ev1));
   float ms = 0;
   CUP_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-  int rc = CUP_OK;
-  for (int k = 0; k < c->ncase; ++k) {
-    cup_solve_stats& o = stats[k];
-    o.iterations = S[k].iterations;
-    o.restarts = S[k].restarts;
-    o.status = S[k].status;
-    o.fallback = 0;
-    o.err_init = S[k].err_init;
-    o.err_final = S[k].err_opt;
-    o.true_rel = -1.0;
-    o.milliseconds = ms;
-    if (S[k].status == SOLVE_NAN) rc = ctx_fail(c, CUP_ERR_NAN, "batched Poisson solve produced NaN");
-    else if (S[k].status != SOLVE_CONVERGED && rc == CUP_OK) rc = CUP_SOFT_MAXITER;
+  return batch_stats(c, S, ms, stats);
+}
+
+int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_used, double* force,
+                   cup_solve_stats* stats) {
+  ProfBind pb_(c);
+  if (!c || c->ncase < 2 || !dt_used) return ctx_fail(c, CUP_ERR_ARG, "cup_batch_step: not a batch or bad arguments");
+  const int K = c->ncase;
+  BatchStep& T = c->T;
+  Fields& F = c->F;
+  const int grid = c->W.grid;
+  // each case's dt: given, or Simulation::calcMaxTimestep from its own max |u| and hmin
+  std::vector<double> dt(K, 0.0), umax(K, 0.0);
+  bool need_umax = !dt_in;
+  for (int k = 0; k < K && !need_umax; ++k) need_umax = !(dt_in[k] > 0);
+  if (need_umax) {
+    if (int rc = launch_case_max_u(c->dm, F.vel[F.vcur], c->cfg.uinf, T.bscratch, T.first, K, T.umax, grid,
+                                   c->stream))
+      return keep_err(c, rc);
+    CUP_CUDA_TRY(stream_d2h(c->stream, umax.data(), T.umax, K * sizeof(double)));
   }
-  return rc;
+  for (int k = 0; k < K; ++k) {
+    dt[k] = dt_in && dt_in[k] > 0 ? dt_in[k] : ctx_calc_dt(c->cfg, c->case_mesh[k].spec.hmin, umax[k], step);
+    if (!(dt[k] > 0)) return ctx_fail(c, CUP_ERR_NAN, "cup_batch_step: dt <= 0 or NaN in case " + std::to_string(k));
+    dt_used[k] = dt[k];
+  }
+  CUP_CUDA_TRY(cudaMemcpyAsync(T.dt, dt.data(), K * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // advection-diffusion, penalization, pressure projection: the single-case
+  // kernels over all blocks, each block with its case's dt, kinematics and mean
+  for (int st = 0; st < 3; ++st) {
+    if (int rc = launch_advect_stage(c->dm, F.vel[F.vcur], F.vel[1 - F.vcur], F.tmpV, 0.0, c->cfg.nu, c->cfg.uinf,
+                                     c->cfg.advection, st, grid, c->stream))
+      return keep_err(c, rc);
+    F.vcur = 1 - F.vcur;
+  }
+  const ObstacleView ob = batch_ob_view(c);
+  if (ob.nslots > 0) {
+    if (int rc = launch_penalize(c->dm, F.vel[F.vcur], F.chi, ob, T.kin, 0.0, c->cfg.lambda,
+                                 c->cfg.implicit_penalization, nullptr, c->W.partial, c->W.counters + 11, c->stream,
+                                 T.slot_force))
+      return keep_err(c, rc);
+    if (int rc = launch_case_forces(T.slot_force, T.slot_first, K, T.force, c->stream)) return keep_err(c, rc);
+  }
+  double* pold = F.pres[F.pcur];
+  double* pnew = F.pres[1 - F.pcur];
+  if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], pold, F.chi, ob, 0.0, step, c->cfg.step_2nd_start, F.lhs,
+                                   F.phi, grid, c->stream))
+    return keep_err(c, rc);
+  std::vector<SolveStats> S(K);
+  CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+  if (int rc = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, batch_params(c), c->W, c->B, S.data(), c->stream))
+    return keep_err(c, rc);
+  CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+  if (int rc = launch_case_sums(c->dm, F.phi, T.bscratch, T.first, K, T.sums, grid, c->stream)) return keep_err(c, rc);
+  if (int rc = launch_grad_update(c->dm, F.vel[F.vcur], F.phi, pold, pnew, nullptr, 0.0, step,
+                                  c->cfg.step_2nd_start, grid, c->stream))
+    return keep_err(c, rc);
+  F.pcur = 1 - F.pcur;
+  if (force) CUP_CUDA_TRY(cudaMemcpyAsync(force, T.force, 6 * K * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  float ms = 0;
+  CUP_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  return batch_stats(c, S, ms, stats);
 }
 
 }  // extern "C"

@@ -26,10 +26,19 @@ struct DevMesh {
   // 0..nb-1, or null for 0..nb-1): visit slot i holds block order[i].
   const int* __restrict__ order;
   // Batches of independent cases (null for one case): the case of each block
-  // and each case's mean-constraint block.
+  // and each case's mean-constraint block, time step, (sum phi h^3, sum h^3)
+  // of the pressure increment, and obstacle kinematics (CM, vel, omega).
   const int* __restrict__ bcase;
   const int* __restrict__ case_mean;
+  const double* __restrict__ case_dt;
+  const double* __restrict__ case_sums;
+  const double* __restrict__ case_kin;
 };
+
+// Time step of block b: its case's in a batch, else dt.
+__device__ __forceinline__ double block_dt(const DevMesh& M, int b, double dt) {
+  return M.case_dt ? M.case_dt[M.bcase[b]] : dt;
+}
 
 #ifndef CUP3D_TAN_HELPERS
 #define CUP3D_TAN_HELPERS

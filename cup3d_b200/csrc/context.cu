@@ -77,6 +77,9 @@ int ctx_upload_mesh(cup_ctx* c) {
   c->dm.order = nullptr;  // set by alloc_fields
   c->dm.bcase = nullptr;  // set for batches
   c->dm.case_mean = nullptr;
+  c->dm.case_dt = nullptr;
+  c->dm.case_sums = nullptr;
+  c->dm.case_kin = nullptr;
   return 0;
 }
 
@@ -602,8 +605,8 @@ static ObstacleView ob_view(const cup_ctx* c) {
   return v;
 }
 
-static int upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
-                           const double* kin) {
+int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
+                        const double* kin) {
   const Mesh& m = c->mesh;
   c->obst_arena.release();
   c->ob = DevObstacle();
@@ -651,14 +654,14 @@ static int upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const 
 }
 
 static int install_host_obstacle(cup_ctx* c, const HostObstacle& h) {
-  if (int rc = upload_obstacle(c, int(h.blocks.size()), h.blocks.data(), h.chi.data(), h.udef.data(), h.kin))
+  if (int rc = ctx_upload_obstacle(c, int(h.blocks.size()), h.blocks.data(), h.chi.data(), h.udef.data(), h.kin))
     return rc;
   if (c->host_only) return 0;
   CUP_CUDA_TRY(stream_h2d(c->stream, c->F.chi, h.grid_chi.data(), h.grid_chi.size() * 8));
   return 0;
 }
 
-static double calc_dt(const cup_config& cfg, double hmin, double umax, int step) {
+double ctx_calc_dt(const cup_config& cfg, double hmin, double umax, int step) {
   // Simulation::calcMaxTimestep (Simulation.cpp:326-338)
   const double dtDiffusion = (1.0 / 6.0) * hmin * hmin / (cfg.nu + (1.0 / 6.0) * hmin * umax);
   const double dtAdvection = hmin / (umax + 1e-8);
@@ -737,7 +740,7 @@ int cup_set_obstacle(cup_ctx* c, int32_t nslots, const int32_t* blocks, const do
   if (!c || c->mesh.nb == 0 || (nslots > 0 && (!blocks || !chi)))
     return ctx_fail(c, CUP_ERR_ARG, "cup_set_obstacle: bad arguments");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_set_obstacle: not available on a batch of cases");
-  return upload_obstacle(c, nslots, blocks, chi, udef, kin);
+  return ctx_upload_obstacle(c, nslots, blocks, chi, udef, kin);
 }
 
 int cup_get_obstacle(const cup_ctx* c, int32_t* blocks, double* chi, double* udef, double* kin) {
@@ -766,7 +769,7 @@ int cup_max_u(cup_ctx* c, double* umax) {
 int cup_compute_dt(cup_ctx* c, int32_t step, double* dt) {
   double umax = 0;
   if (int rc = cup_max_u(c, &umax)) return rc;
-  *dt = calc_dt(c->cfg, c->mesh.spec.hmin, umax, step);
+  *dt = ctx_calc_dt(c->cfg, c->mesh.spec.hmin, umax, step);
   if (!(*dt > 0)) return ctx_fail(c, CUP_ERR_NAN, "dt <= 0 or NaN (Simulation.cpp:344-347)");
   return 0;
 }

@@ -57,6 +57,19 @@ struct CnnState {
   bool ready = false;
 };
 
+// Per-case device buffers of a batch's time step.
+struct BatchStep {
+  int* first = nullptr;         // ncase + 1 block offsets
+  int* slot_first = nullptr;    // ncase + 1 obstacle-slot offsets
+  double* dt = nullptr;         // ncase
+  double* sums = nullptr;       // 2 ncase: (sum phi h^3, sum h^3)
+  double* kin = nullptr;        // 9 ncase: CM, velocity, angular velocity
+  double* umax = nullptr;       // ncase
+  double* force = nullptr;      // 6 ncase: penalization force and torque
+  double* bscratch = nullptr;   // 2 nb
+  double* slot_force = nullptr; // 6 nslots
+};
+
 // Offsets into cup_ctx::d_scalars
 enum : int { SC_SUMS = 0, SC_UMAX = 2, SC_FORCE = 8, SC_KIN = 16, SC_TARGET_SUMSQ = 32 };
 
@@ -95,6 +108,7 @@ struct cup_ctx {
   std::vector<int> case_first;        // ncase + 1 block offsets
   std::vector<cup3d::Mesh> case_mesh;  // each case's own mesh
   cup3d::BatchWork B{};
+  cup3d::BatchStep T{};
   cup3d::DevArena batch_arena;
 };
 
@@ -109,6 +123,11 @@ int ctx_fail(cup_ctx* c, int code, const std::string& msg);
 // Uploads c->mesh and (re)allocates the fields and solver work for it.
 int ctx_upload_mesh(cup_ctx* c);
 int ctx_alloc_fields(cup_ctx* c);
+// Installs an obstacle (nslots blocks with chi, udef and kinematics kin[9]).
+int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
+                        const double* kin);
+// Simulation::calcMaxTimestep for spacing hmin and max |u| umax.
+double ctx_calc_dt(const cup_config& cfg, double hmin, double umax, int step);
 size_t nbn(const cup_ctx* c);
 // Host<->device copies and fills ordered on a stream, waiting for it before
 // returning.  The context stream is non-blocking, so cudaMemcpy / cudaMemset

@@ -96,8 +96,9 @@ __global__ void __launch_bounds__(NT, 3)
       for (int i = threadIdx.x; i < 3 * BN; i += NT) corr[i] = 0.0;
     __syncthreads();
     const double h = M.h[b], h3 = h * h * h;
-    const double facA = -dt / h * h3;
-    const double facD = (nu / h) * (dt / h) * h3;
+    const double dtb = block_dt(M, b, dt);
+    const double facA = -dtb / h * h3;
+    const double facD = (nu / h) * (dtb / h) * h3;
     if (fix) {
       for (int f = 0; f < 6; ++f) {
         if (M.fkind[b * 6 + f] != K_FINER) continue;
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(NT, 3)
           face_lab_pair(d, s, a, bb, q, g);
           const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
           const double hf = M.h[ch];
-          const double facDf = (nu / hf) * (dt / hf) * hf * hf * hf;
+          const double facDf = (nu / hf) * (dtb / hf) * hf * hf * hf;
           const int oc = face_cell(d, s, 0, a, bb);
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
@@ -234,7 +235,8 @@ __global__ void __launch_bounds__(NT, 3)
     if (fix)
       for (int i = threadIdx.x; i < 2 * BN; i += NT) corr[i] = 0.0;
     __syncthreads();
-    const double h = M.h[b], fac = 0.5 * h * h / dt;
+    const double dtb = block_dt(M, b, dt);
+    const double h = M.h[b], fac = 0.5 * h * h / dtb;
     auto U = [&](int c, int x, int y, int z) { return ulab[c * LG::V + LG::at(x, y, z)]; };
     auto D = [&](int c, int x, int y, int z) { return near ? dlab[c * LG::V + LG::at(x, y, z)] : 0.0; };
     auto P = [&](int x, int y, int z) { return plab[LG::at(x, y, z)]; };
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(NT, 3)
           int q[3], g[3];
           face_lab_pair(d, s, a, bb, q, g);
           const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
-          const double hf = M.h[ch], facf = 0.5 * hf * hf / dt;
+          const double hf = M.h[ch], facf = 0.5 * hf * hf / dtb;
           const int oc = face_cell(d, s, 0, a, bb);
           const double sg = s ? -1.0 : 1.0, sgc = -sg;
           const double cq = chi[size_t(b) * BN + oc];
@@ -331,20 +333,25 @@ __global__ void __launch_bounds__(NT, 4)
   __shared__ double corr[3 * BN];
   using LG = LabGeom<1>;
   const size_t n = size_t(M.nb) * BN;
-  const double avg = sums[0] / sums[1];
+  double avg = sums ? sums[0] / sums[1] : 0.0;  // the block's case's mean in a batch
   auto getP = [&](int, int blk, int cell) {
     const size_t i = size_t(blk) * BN + cell;
     const double p = phi[i] - avg;
     return use_pold ? p + pold[i] : p;
   };
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    if (M.case_sums) {
+      const int cs = M.bcase[b];
+      avg = M.case_sums[2 * cs] / M.case_sums[2 * cs + 1];
+    }
     __syncthreads();
     lab_fill<1, 1>(plab, M, b, getP, false);
     const bool fix = has_finer(M, b);
     if (fix)
       for (int i = threadIdx.x; i < 3 * BN; i += NT) corr[i] = 0.0;
     __syncthreads();
-    const double h = M.h[b], fac = -0.5 * dt * h * h;
+    const double dtb = block_dt(M, b, dt);
+    const double h = M.h[b], fac = -0.5 * dtb * h * h;
     auto P = [&](int x, int y, int z) { return plab[LG::at(x, y, z)]; };
     if (fix) {
       for (int f = 0; f < 6; ++f) {
@@ -355,7 +362,7 @@ __global__ void __launch_bounds__(NT, 4)
           int q[3], g[3];
           face_lab_pair(d, s, a, bb, q, g);
           const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
-          const double hf = M.h[ch], facf = -0.5 * dt * hf * hf;
+          const double hf = M.h[ch], facf = -0.5 * dtb * hf * hf;
           const double sg = s ? -1.0 : 1.0, sgc = -sg;
           double v = sg * fac * (P(g[0], g[1], g[2]) + P(q[0], q[1], q[2]));
 #pragma unroll
@@ -406,18 +413,22 @@ int launch_grad_update(const DevMesh& M, double* vel, const double* phi, const d
 // Penalization: KernelPenalization (Penalization.cpp:56-89) on obstacle blocks
 // and the force/torque sums of kernelFinalizePenalizationForce (:91-109).
 // ---------------------------------------------------------------------------
+// In a batch (M.bcase set) each slot takes its case's kinematics and time
+// step, and the force/torque sums go per slot into slot_force[6 * slot].
 __global__ void __launch_bounds__(NT)
     k_penalize(DevMesh M, double* vel, const double* __restrict__ chi, ObstacleView ob, const double* __restrict__ kin,
-               double dt, double lambda, int implicit, GridReduce G, double* force) {
+               double dt, double lambda, int implicit, GridReduce G, double* force, double* slot_force) {
   __shared__ double red[8 * 6];
   const size_t n = size_t(M.nb) * BN;
-  const double lambdaFac = implicit ? lambda : 1.0 / dt;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  const double CM[3] = {kin[0], kin[1], kin[2]};
-  const double V[3] = {kin[3], kin[4], kin[5]};
-  const double O[3] = {kin[6], kin[7], kin[8]};
   for (int sl = blockIdx.x; sl < ob.nslots; sl += gridDim.x) {
     const int b = ob.blk[sl];
+    const double* kn = M.case_kin ? M.case_kin + 9 * M.bcase[b] : kin;
+    const double CM[3] = {kn[0], kn[1], kn[2]};
+    const double V[3] = {kn[3], kn[4], kn[5]};
+    const double O[3] = {kn[6], kn[7], kn[8]};
+    const double dtb = block_dt(M, b, dt);
+    const double lambdaFac = implicit ? lambda : 1.0 / dtb;
     const double h = M.h[b], dv = h * h * h;
     for (int cell = threadIdx.x; cell < BN; cell += NT) {
       const size_t gi = size_t(b) * BN + cell;
@@ -436,13 +447,13 @@ __global__ void __launch_bounds__(NT)
       const double U1 = V[1] + O[2] * p[0] - O[0] * p[2] + ud[(1 * ns + sl) * BN + cell];
       const double U2 = V[2] + O[0] * p[1] - O[1] * p[0] + ud[(2 * ns + sl) * BN + cell];
       const double X = implicit ? (CHI > 0.5 ? 1.0 : 0.0) : CHI;
-      const double penalFac = implicit ? X * lambdaFac / (1 + X * lambdaFac * dt) : X * lambdaFac;
+      const double penalFac = implicit ? X * lambdaFac / (1 + X * lambdaFac * dtb) : X * lambdaFac;
       const double FPX = penalFac * (U0 - vel[gi]);
       const double FPY = penalFac * (U1 - vel[n + gi]);
       const double FPZ = penalFac * (U2 - vel[2 * n + gi]);
-      vel[gi] = vel[gi] + dt * FPX;
-      vel[n + gi] = vel[n + gi] + dt * FPY;
-      vel[2 * n + gi] = vel[2 * n + gi] + dt * FPZ;
+      vel[gi] = vel[gi] + dtb * FPX;
+      vel[n + gi] = vel[n + gi] + dtb * FPY;
+      vel[2 * n + gi] = vel[2 * n + gi] + dtb * FPZ;
       acc[0] += dv * FPX;
       acc[1] += dv * FPY;
       acc[2] += dv * FPZ;
@@ -450,22 +461,29 @@ __global__ void __launch_bounds__(NT)
       acc[4] += dv * (p[2] * FPX - p[0] * FPZ);
       acc[5] += dv * (p[0] * FPY - p[1] * FPX);
     }
+    if (slot_force) {  // uniform over the CTA
+      block_reduce<6>(acc, red);
+      if (threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) slot_force[6 * sl + q] = acc[q];
+      for (int q = 0; q < 6; ++q) acc[q] = 0.0;
+    }
   }
-  if (grid_reduce<6>(acc, G, red) && threadIdx.x == 0)
+  if (!slot_force && grid_reduce<6>(acc, G, red) && threadIdx.x == 0)
     for (int q = 0; q < 6; ++q) force[q] = acc[q];
 }
 
 int launch_penalize(const DevMesh& M, double* vel, const double* chi, const ObstacleView& ob, const double* kin,
                     double dt, double lambda, int implicit, double* force, double* partial, unsigned* counter,
-                    cudaStream_t s) {
+                    cudaStream_t s, double* slot_force) {
   if (ob.nslots <= 0) {
+    if (slot_force) return 0;
     CUP_CUDA_TRY(cudaMemsetAsync(force, 0, 6 * sizeof(double), s));
     return 0;
   }
   const int grid = std::min(ob.nslots, 1184);
   GridReduce G{partial, counter};
   ProfScope ps("penalize", s);
-  k_penalize<<<grid, NT, 0, s>>>(M, vel, chi, ob, kin, dt, lambda, implicit, G, force);
+  k_penalize<<<grid, NT, 0, s>>>(M, vel, chi, ob, kin, dt, lambda, implicit, G, force, slot_force);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -492,6 +510,107 @@ int launch_max_u(const DevMesh& M, const double* vel, const double* uinf, double
   Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
   ProfScope ps("max_u", s);
   k_max_u<<<grid, NT, 0, s>>>(size_t(M.nb) * BN, vel, ui, G, out);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Per-case reductions of a batch: per-item values (blocks or obstacle slots),
+// then one CTA per case over the case's item range, in a fixed order.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(NT) k_block_max_u(DevMesh M, const double* __restrict__ vel, Vec3 ui,
+                                                    double* bmax) {
+  __shared__ double red[NT / 32];
+  const size_t n = size_t(M.nb) * BN;
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    double m = 0.0;
+    for (int c = threadIdx.x; c < BN; c += NT) {
+      const size_t i = size_t(b) * BN + c;
+      m = fmax(m, fmax(fabs(vel[i] + ui.v[0]), fmax(fabs(vel[n + i] + ui.v[1]), fabs(vel[2 * n + i] + ui.v[2]))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double mm = 0.0;
+      for (int w = 0; w < NT / 32; ++w) mm = fmax(mm, red[w]);
+      bmax[b] = mm;
+    }
+  }
+}
+
+// (sum phi h^3, sum h^3) of each block
+__global__ void __launch_bounds__(NT) k_block_sums(DevMesh M, const double* __restrict__ phi, double* bsum) {
+  __shared__ double red[64];
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    const double h = M.h[b], h3 = h * h * h;
+    double v[1] = {0.0};
+    for (int c = threadIdx.x; c < BN; c += NT) v[0] += phi[size_t(b) * BN + c];
+    block_reduce<1>(v, red);
+    if (threadIdx.x == 0) {
+      bsum[2 * b] = v[0] * h3;
+      bsum[2 * b + 1] = BN * h3;
+    }
+  }
+}
+
+// out[NR c + r] = sum (MAX = 0) or max (MAX = 1) of in[NR i + r], i in [first[c], first[c+1])
+template <int NR, int MAX>
+__global__ void __launch_bounds__(NT) k_case_reduce(const double* __restrict__ in, const int* __restrict__ first,
+                                                    double* out) {
+  __shared__ double red[8 * NR];
+  const int c = blockIdx.x;
+  double v[NR];
+#pragma unroll
+  for (int r = 0; r < NR; ++r) v[r] = 0.0;
+  for (int i = first[c] + threadIdx.x; i < first[c + 1]; i += NT)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) v[r] = MAX ? fmax(v[r], in[size_t(NR) * i + r]) : v[r] + in[size_t(NR) * i + r];
+  if (MAX) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[r] = fmax(v[r], __shfl_xor_sync(0xffffffffu, v[r], o));
+      if ((threadIdx.x & 31) == 0) red[(threadIdx.x >> 5) * NR + r] = v[r];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int r = 0; r < NR; ++r) {
+        double m = 0.0;
+        for (int w = 0; w < NT / 32; ++w) m = fmax(m, red[w * NR + r]);
+        out[NR * c + r] = m;
+      }
+  } else {
+    block_reduce<NR>(v, red);
+    if (threadIdx.x == 0)
+      for (int r = 0; r < NR; ++r) out[NR * c + r] = v[r];
+  }
+}
+
+int launch_case_max_u(const DevMesh& M, const double* vel, const double* uinf, double* bmax, const int* first,
+                      int ncase, double* out, int grid, cudaStream_t s) {
+  Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
+  ProfScope ps("case_max_u", s);
+  k_block_max_u<<<grid, NT, 0, s>>>(M, vel, ui, bmax);
+  k_case_reduce<1, 1><<<ncase, NT, 0, s>>>(bmax, first, out);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_case_sums(const DevMesh& M, const double* phi, double* bsum, const int* first, int ncase, double* out,
+                     int grid, cudaStream_t s) {
+  ProfScope ps("case_sums", s);
+  k_block_sums<<<grid, NT, 0, s>>>(M, phi, bsum);
+  k_case_reduce<2, 0><<<ncase, NT, 0, s>>>(bsum, first, out);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+int launch_case_forces(const double* slot_force, const int* slot_first, int ncase, double* out, cudaStream_t s) {
+  ProfScope ps("case_forces", s);
+  k_case_reduce<6, 0><<<ncase, NT, 0, s>>>(slot_force, slot_first, out);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }

@@ -34,13 +34,24 @@ int launch_grad_update(const DevMesh& M, double* vel, const double* phi, const d
                        int grid, cudaStream_t s);
 
 // KernelPenalization + kernelFinalizePenalizationForce (Penalization.cpp:18-109).
-// kin = CM[3], vel[3], omega[3]; force[6] (F, T) reduced on the device.
+// kin = CM[3], vel[3], omega[3]; force[6] (F, T) reduced on the device.  In a
+// batch (slot_force set) the sums go per obstacle slot into slot_force[6 s].
 int launch_penalize(const DevMesh& M, double* vel, const double* chi, const ObstacleView& ob,
                     const double* kin_dev, double dt, double lambda, int implicit, double* force,
-                    double* partial, unsigned* counter, cudaStream_t s);
+                    double* partial, unsigned* counter, cudaStream_t s, double* slot_force = nullptr);
 
 // max |u + uinf| (findMaxU, ProcessHelpers.h:71-94) into *out.
 int launch_max_u(const DevMesh& M, const double* vel, const double* uinf, double* out,
                  double* partial, unsigned* counter, int grid, cudaStream_t s);
+
+// Batches: per-case max |u + uinf| (out[ncase]; bmax: nb scratch), per-case
+// (sum phi h^3, sum h^3) (out[2 ncase]; bsum: 2 nb scratch) and per-case
+// obstacle force/torque (out[6 ncase]) from per-slot sums.  first / slot_first:
+// the cases' block / obstacle-slot ranges (ncase + 1 entries).
+int launch_case_max_u(const DevMesh& M, const double* vel, const double* uinf, double* bmax, const int* first,
+                      int ncase, double* out, int grid, cudaStream_t s);
+int launch_case_sums(const DevMesh& M, const double* phi, double* bsum, const int* first, int ncase, double* out,
+                     int grid, cudaStream_t s);
+int launch_case_forces(const double* slot_force, const int* slot_first, int ncase, double* out, cudaStream_t s);
 
 }  // namespace cup3d

@@ -152,10 +152,12 @@ int cup_poisson_solve(cup_ctx* ctx, cup_solve_stats* stats);
  * runs one case per process) ---- */
 /* A new context over the meshes of ncases device contexts, concatenated in
  * case order (case k's blocks follow case k-1's, each case in its own block
- * order); the cases keep their own mean-constraint rows.  The other settings
- * (tolerances, -bMeanConstraint, device) are case 0's; every case must use
- * the same device and -bMeanConstraint.  The cases are not modified.  NULL on
- * failure: cup_last_error(NULL). */
+ * order); the cases keep their own mean-constraint rows, boundary
+ * conditions, obstacles and current velocity, pressure and chi fields, which
+ * are copied in.  The other settings (tolerances, -bMeanConstraint, nu, CFL,
+ * rampup, lambda, uinf, advection scheme, device) are case 0's; every case
+ * must use the same device and -bMeanConstraint.  The cases are not
+ * modified.  NULL on failure: cup_last_error(NULL). */
 cup_ctx* cup_batch_create(int32_t ncases, cup_ctx* const* cases);
 int32_t cup_batch_num_cases(const cup_ctx* batch);  /* 1 for a plain context */
 /* Blocks first .. first+nblocks-1 of the batch (and of its fields) are case k's. */
@@ -165,6 +167,14 @@ int cup_batch_case_blocks(const cup_ctx* batch, int32_t k, int32_t* first, int32
  * initial guess in, each case's solution out; stats[ncases].  Returns the
  * worst outcome over the cases (true_rel is not computed: -1). */
 int cup_batch_poisson_solve_dev(cup_ctx* batch, const double* d_b, double* d_x, cup_solve_stats* stats);
+/* One time step of every case (cup_step per case: advection-diffusion,
+ * penalization, pressure projection), each case with its own dt: dt_in[k]
+ * (or, when dt_in is NULL or dt_in[k] <= 0, Simulation::calcMaxTimestep from
+ * the case's own max |u| and finest spacing).  dt_used[ncases]; force[6 ncases]
+ * (penalization force and torque per case, may be NULL); stats[ncases] (may
+ * be NULL).  The Poisson solves of all cases run in one device launch. */
+int cup_batch_step(cup_ctx* batch, int32_t step, const double* dt_in, double* dt_used, double* force,
+                   cup_solve_stats* stats);
 
 /* ---- obstacles (host-side CreateObstacles; one body per context) ---- */
 /* Sphere of radius r at c (Sphere.cpp); chi by ObstaclesCreate.cpp:18-121;

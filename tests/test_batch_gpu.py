@@ -10,7 +10,9 @@
 * with more than four blocks per block group (three copies of the sphere
   mesh) the batch stages block tables on the way; every case's FP64
   residual on its own context's device operator is within the tolerance;
-* the single-case entry points refuse a batch.
+* the single-case entry points refuse a batch;
+* time steps of a batch (own dt, obstacle, mean and solve per case) match
+  the same cases stepped one by one.
 """
 import numpy as np
 import pytest
@@ -122,3 +124,57 @@ def test_batch_staged_tables_solve_every_case():
         bb = bs[k].copy()
         bb[mb * 512] = 0.0
         assert np.linalg.norm(bb - yk.cpu().numpy()) <= 1.05e-10 * np.linalg.norm(bb), k
+
+
+def _smooth_velocity(ctx, phase):
+    xyz, _ = ctx.cell_centres()
+    x, y, z = xyz.T
+    return np.concatenate([np.sin(2 * x + phase) * np.cos(3 * y), 0.5 * np.cos(x - phase) * np.sin(2 * z),
+                           0.3 * np.sin(y + z + phase)])
+
+
+def _step_cases():
+    flags = "-poissonTol 0 -poissonTolRel 1e-11 -nu 0.01 -CFL 0.3 -rampup 0 -advection weno5"
+    a = make_ctx("tgv32", device=0, extra=flags)
+    xyz, _ = a.cell_centres()
+    x, y, z = xyz.T
+    a.upload("vel", np.concatenate([np.sin(x) * np.cos(y) * np.cos(z), -np.cos(x) * np.sin(y) * np.cos(z), 0 * x]))
+    b = make_ctx("amr2_free", device=0, extra=flags)
+    b.upload("vel", _smooth_velocity(b, 0.3))
+    b.obstacle_sphere((0.5, 0.45, 0.55), 0.15, vel=(0.1, 0.0, 0.0))
+    c = make_ctx("amr3_mixed", device=0, extra=flags)
+    c.upload("vel", _smooth_velocity(c, 1.1))
+    q = np.array([0.9, 0.1, 0.3, 0.3])
+    c.obstacle_ellipsoid((1.0, 0.5, 0.75), (0.2, 0.1, 0.1), q / np.linalg.norm(q), vel=(0.0, 0.05, 0.0))
+    return [a, b, c]
+
+
+def test_batch_steps_match_single_cases():
+    # each case stepped alone (cup_compute_dt, cup_advect_diffuse,
+    # cup_penalize, cup_pressure_project) against the same cases stepped
+    # together, through two steps.  The Poisson solves to 1e-11 sum their
+    # dot products in another order, so the fields differ at that level:
+    # dt bit for bit in the first step (max |u| does not depend on the
+    # order) and within 1e-10 after; the single cases then step with the
+    # batch's dt; velocities within 1e-8 of max|u|, forces within 1e-8 of
+    # their size, pressure within 1e-7 of max|p|
+    singles = _step_cases()
+    batch = cup.Batch(_step_cases())
+    for step in range(2):
+        rc, dts, forces, stats = batch.step(step)
+        assert rc == 0 and all(s["status"] == 1 for s in stats)
+        for k, s in enumerate(singles):
+            dt1 = s.compute_dt(step)
+            assert (dt1 == dts[k]) if step == 0 else abs(dt1 - dts[k]) <= 1e-10 * dt1, (step, k, dt1, dts[k])
+            dt = dts[k]
+            s.advect_diffuse(dt)
+            f = s.penalize(dt) if k > 0 else np.zeros(6)
+            s.pressure_project(dt, step)
+            u1 = s.download("vel").reshape(3, -1)
+            ub = batch.case_field("vel", k)
+            scale = np.abs(u1).max()
+            assert np.abs(ub - u1).max() <= 1e-8 * scale, (step, k, np.abs(ub - u1).max() / scale)
+            assert np.abs(forces[k] - f).max() <= 1e-8 * max(np.abs(f).max(), 1e-30), (step, k, forces[k], f)
+            p1 = s.download("pres")
+            pb = batch.case_field("pres", k)[0]
+            assert np.abs(pb - p1).max() <= 1e-7 * np.abs(p1).max(), (step, k)
