@@ -46,61 +46,25 @@ static void concat_meshes(const std::vector<Mesh>& cases, Mesh& m, std::vector<i
   m.mean_block = mean[0];
 }
 
-// Block groups per case in proportion to its blocks (at least one, at most
-// one per block), then each case's blocks dealt to its groups in the
-// cost-balanced visit order of its own mesh.  Equal blocks per group is the
-// right share even when the cases need different iteration counts: every
-// phase ends at a grid barrier, so a phase lasts as long as the group with
-// the most blocks.  (Dealing groups by blocks x iterations, so that all cases
-// would finish together, made a 64-case batch 12-17% slower.)
-static int plan_groups(const std::vector<Mesh>& cases, const std::vector<int>& first, int groups,
-                       std::vector<int>& gcase, std::vector<int>& gfirst, std::vector<int>& goff,
-                       std::vector<int>& gblocks) {
-  const int K = int(cases.size());
-  if (K > groups) return set_error(CUP_ERR_ARG, "batch: more cases than block groups of the batched solver");
-  const double nbt = double(first.back());
-  std::vector<int> ng(K);
-  int used = 0;
-  for (int k = 0; k < K; ++k) {
-    ng[k] = std::max(1, std::min(cases[k].nb, int(groups * (cases[k].nb / nbt))));
-    used += ng[k];
+// Each case's blocks by decreasing operator cost (2 + coarser faces + 2 x
+// finer faces, the estimate of mesh_visit_order), at the case's own offsets:
+// the batched solver deals them round-robin to the case's groups.
+static std::vector<int> cost_sorted_blocks(const std::vector<Mesh>& cases, const std::vector<int>& first) {
+  std::vector<int> out(first.back());
+  for (size_t k = 0; k < cases.size(); ++k) {
+    const Mesh& m = cases[k];
+    std::vector<int> cost(m.nb, 2);
+    for (int b = 0; b < m.nb; ++b)
+      for (int f = 0; f < 6; ++f) {
+        const int kind = m.face_kind[6 * b + f];
+        cost[b] += kind == FACE_COARSER ? 1 : (kind == FACE_FINER ? 2 : 0);
+      }
+    std::vector<int> idx(m.nb);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    for (int i = 0; i < m.nb; ++i) out[first[k] + i] = first[k] + idx[i];
   }
-  // too many (the floors of one): take from the cases with the fewest blocks per group
-  while (used > groups) {
-    int best = -1;
-    for (int k = 0; k < K; ++k)
-      if (ng[k] > 1 && (best < 0 || double(cases[k].nb) / ng[k] < double(cases[best].nb) / ng[best])) best = k;
-    if (best < 0) break;
-    --ng[best];
-    --used;
-  }
-  // spare groups: to the cases with the most blocks per group
-  while (used < groups) {
-    int best = -1;
-    for (int k = 0; k < K; ++k)
-      if (ng[k] < cases[k].nb && (best < 0 || double(cases[k].nb) / ng[k] > double(cases[best].nb) / ng[best]))
-        best = k;
-    if (best < 0) break;
-    ++ng[best];
-    ++used;
-  }
-  gcase.assign(groups, -1);
-  gfirst.assign(K + 1, 0);
-  goff.assign(groups + 1, 0);
-  gblocks.clear();
-  int g = 0;
-  for (int k = 0; k < K; ++k) {
-    gfirst[k] = g;
-    const std::vector<int32_t> order = mesh_visit_order(cases[k], ng[k]);
-    for (int j = 0; j < ng[k]; ++j, ++g) {
-      gcase[g] = k;
-      goff[g] = int(gblocks.size());
-      for (int s = j; s < cases[k].nb; s += ng[k]) gblocks.push_back(first[k] + order[s]);
-    }
-  }
-  gfirst[K] = g;
-  for (; g <= groups; ++g) goff[g] = int(gblocks.size());
-  return 0;
+  return out;
 }
 
 // Keeps the thread's last error message on the context.
@@ -133,13 +97,10 @@ static int batch_setup(cup_ctx* c, const std::vector<Mesh>& cases) {
   c->dm.case_mean = d_mean;
   BatchWork& B = c->B;
   B.ncase = c->ncase;
-  if (int rc = batch_solver_shape(c->mesh.nb, &B.grid, &B.groups)) return rc;
-  std::vector<int> gcase, gfirst, goff, gblocks;
-  if (int rc = plan_groups(cases, first, B.groups, gcase, gfirst, goff, gblocks)) return rc;
-  if (int rc = upload_ints(c, &B.gcase, gcase)) return rc;
-  if (int rc = upload_ints(c, &B.gfirst, gfirst)) return rc;
-  if (int rc = upload_ints(c, &B.goff, goff)) return rc;
-  if (int rc = upload_ints(c, &B.gblocks, gblocks)) return rc;
+  if (int rc = batch_solver_shape(c->mesh.nb, c->ncase, &B.grid, &B.groups)) return rc;
+  if (B.groups < c->ncase) return set_error(CUP_ERR_ARG, "batch: more cases than block groups of the batched solver");
+  if (int rc = upload_ints(c, &B.cfirst, first)) return rc;
+  if (int rc = upload_ints(c, &B.cblocks, cost_sorted_blocks(cases, first))) return rc;
   if (int rc = c->batch_arena.alloc(&B.part, size_t(2) * B.groups * 8)) return rc;
   if (int rc = c->batch_arena.alloc(&B.case_done, size_t(B.ncase))) return rc;
   if (int rc = c->batch_arena.alloc(&B.st, size_t(B.ncase))) return rc;

@@ -1083,23 +1083,85 @@ __device__ __forceinline__ void group_reduce(double (&v)[NR], double* gsm, const
 }
 
 struct BatchArgs {
-  const int* gcase;
-  const int* gfirst;
-  const int* goff;
-  const int* gblocks;
+  const int* cfirst;
+  const int* cblocks;
   double* part;
   int* case_done;
   int ncase;
   int groups;
 };
 
+// Dynamic shared memory of the batched solver: the persistent solver's, then
+// the deal of the groups: gfirst and the previous gfirst (ncase + 1 ints
+// each) and the running flags (ncase ints).
+__host__ __device__ constexpr size_t batch_smem(int ncase) {
+  return kPersistentSmem + size_t(3 * ncase + 2) * sizeof(int);
+}
+
+// Deals the G block groups of the grid to the running cases, in case order,
+// in proportion to their blocks (at least one, at most one per block): the
+// groups of case c are gfirst[c] .. gfirst[c+1]-1 (none for a stopped case).
+// Integer arithmetic only, so every CTA computes the same deal.  One thread.
+__device__ void batch_deal(const int* cfirst, const int* running, int ncase, int G, int* gfirst) {
+  long long nba = 0;
+  for (int c = 0; c < ncase; ++c)
+    if (running[c]) nba += cfirst[c + 1] - cfirst[c];
+  int used = 0;
+  // first pass: floor of the proportional share, in gfirst[c+1] as a count
+  for (int c = 0; c < ncase; ++c) {
+    const int nb = cfirst[c + 1] - cfirst[c];
+    int q = 0;
+    if (running[c] && nba > 0) q = max(1, min(nb, int((long long)G * nb / nba)));
+    gfirst[c + 1] = q;
+    used += q;
+  }
+  // over (shares of one): take back round-robin from cases with more than one
+  for (int c = 0; used > G; c = (c + 1) % ncase)
+    if (gfirst[c + 1] > 1) {
+      --gfirst[c + 1];
+      --used;
+    }
+  // spare groups: round-robin to running cases with blocks left to share
+  bool any = true;
+  while (used < G && any) {
+    any = false;
+    for (int c = 0; c < ncase && used < G; ++c)
+      if (running[c] && gfirst[c + 1] < cfirst[c + 1] - cfirst[c]) {
+        ++gfirst[c + 1];
+        ++used;
+        any = true;
+      }
+  }
+  gfirst[0] = 0;
+  for (int c = 0; c < ncase; ++c) gfirst[c + 1] += gfirst[c];
+}
+
+// A group's place in the deal: case (-1: none), index within the case's
+// groups, the case's group count and the group's block count.
+struct GroupPlace {
+  int c, j, ng, nblk;
+};
+
+__device__ __forceinline__ GroupPlace group_place(const int* gfirst, const int* cfirst, int ncase, int gidx) {
+  GroupPlace p{-1, 0, 0, 0};
+  for (int c = 0; c < ncase; ++c)
+    if (gidx >= gfirst[c] && gidx < gfirst[c + 1]) {
+      p.c = c;
+      p.j = gidx - gfirst[c];
+      p.ng = gfirst[c + 1] - gfirst[c];
+      const int nb = cfirst[c + 1] - cfirst[c];
+      p.nblk = nb > p.j ? (nb - p.j + p.ng - 1) / p.ng : 0;
+    }
+  return p;
+}
+
 // Grid barrier with per-case sums: each group's partials, then every group
-// of case c sums the partials of c's groups.  With ANY, also tells whether
-// any case was still running when the barrier was reached (case_done as
-// written before it).
-template <int NR, bool ANY>
+// of case c sums the partials of the groups [g0, g1) that worked for c in
+// this phase.  With RUN, also loads the cases' running flags (case_done as
+// written before the barrier) into running[] in every CTA.
+template <int NR, bool RUN>
 __device__ bool batch_allreduce(double (&v)[NR], const BatchArgs& B, const GridSync& Gs, unsigned int& epoch,
-                                double* gsm, const GroupIdx& G, int gidx, int c, bool* any) {
+                                double* gsm, const GroupIdx& G, int gidx, int c, int g0, int g1, int* running) {
   const unsigned int k = epoch;
   double* part = B.part + size_t(k & 1u) * B.groups * 8;
   group_reduce<NR>(v, gsm, G);
@@ -1125,16 +1187,15 @@ __device__ bool batch_allreduce(double (&v)[NR], const BatchArgs& B, const GridS
   }
   __syncthreads();
   if (!s_ok) return false;
-  if (ANY) {
-    int running = 0;
-    for (int i = threadIdx.x; i < B.ncase; i += blockDim.x) running |= B.case_done[i] == 0;
-    *any = __syncthreads_or(running) != 0;
+  if (RUN) {
+    for (int i = threadIdx.x; i < B.ncase; i += blockDim.x) running[i] = B.case_done[i] == 0;
+    __syncthreads();
   }
   if (c >= 0) {
     double acc[NR];
 #pragma unroll
     for (int r = 0; r < NR; ++r) acc[r] = 0.0;
-    for (int g = B.gfirst[c] + G.lane; g < B.gfirst[c + 1]; g += GROUP)
+    for (int g = g0 + G.lane; g < g1; g += GROUP)
 #pragma unroll
       for (int r = 0; r < NR; ++r) acc[r] += part[g * 8 + r];
     group_reduce<NR>(acc, gsm, G);
@@ -1144,19 +1205,29 @@ __device__ bool batch_allreduce(double (&v)[NR], const BatchArgs& B, const GridS
   return true;
 }
 
-// A group's k-th block: the entries of its first KB_CACHE blocks are staged
-// at launch, later ones in the group's tile on the way.
-__device__ __forceinline__ const BlockInfo& batch_block(const DevMesh& M, const BlockInfo* cache, GroupTile& tile,
-                                                        const int* blocks, int k, const GroupIdx& G) {
+// A group's k-th block: blocks j, j + ng, j + 2 ng, ... of its case's list
+// (decreasing cost, so the groups' shares balance); the entries of the first
+// KB_CACHE are staged when the group is placed, later ones on the way.
+__device__ __forceinline__ const BlockInfo& batch_block(const DevMesh& M, const BatchArgs& B, const BlockInfo* cache,
+                                                        GroupTile& tile, const GroupPlace& P, int k,
+                                                        const GroupIdx& G) {
   if (k < KB_CACHE) return cache[G.g * KB_CACHE + k];
   group_sync(G.g);
-  fill_block_info(M, blocks[k], tile.bi, G.lane);
+  fill_block_info(M, B.cblocks[B.cfirst[P.c] + P.j + k * P.ng], tile.bi, G.lane);
   group_sync(G.g);
   return tile.bi;
 }
 
+// Stages the table entries of the group's first KB_CACHE blocks (the caller
+// synchronises the CTA before they are read).
+__device__ __forceinline__ void batch_fill_cache(const DevMesh& M, const BatchArgs& B, BlockInfo* cache,
+                                                 const GroupPlace& P, const GroupIdx& G) {
+  for (int k = 0; k < KB_CACHE && k < P.nblk; ++k)
+    if (G.lane < 32) fill_block_info(M, B.cblocks[B.cfirst[P.c] + P.j + k * P.ng], cache[G.g * KB_CACHE + k], G.lane);
+}
+
 #define BATCH_BLOCKS(bi) \
-  for (int k_ = 0; k_ < nblk; ++k_) if (const BlockInfo& bi = batch_block(M, cache, tile, myblocks, k_, G); true)
+  for (int k_ = 0; k_ < P.nblk; ++k_) if (const BlockInfo& bi = batch_block(M, B, cache, tile, P, k_, G); true)
 
 // PREP: x0 = 0 on the case's mean row (modes 1 and 3); sum(x0 h^3)
 template <class T>
@@ -1204,103 +1275,166 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, G
   GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw);
   double* inv_eig = reinterpret_cast<double*>(smem_raw + PGROUPS * sizeof(GroupTile));
   BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + PGROUPS * sizeof(GroupTile) + BN * sizeof(double));
+  int* gfirst = reinterpret_cast<int*>(smem_raw + kPersistentSmem);
+  int* gfirst_prev = gfirst + B.ncase + 1;
+  int* running = gfirst_prev + B.ncase + 1;
   __shared__ KrylovState Sg[PGROUPS];
   __shared__ double gsm_all[PGROUPS][16];
-  __shared__ double ms_zr_g[PGROUPS];
   __shared__ unsigned int epoch;
+  __shared__ int s_changed;
   const GroupIdx G;
   const DevMesh& M = A.M;
   GroupTile& tile = tiles[G.g];
   double* gsm = gsm_all[G.g];
   KrylovState& S = Sg[G.g];
-  double& ms_zr = ms_zr_g[G.g];
   const int gidx = blockIdx.x * PGROUPS + G.g;
-  const int c = B.gcase[gidx];
-  const int* myblocks = B.gblocks + B.goff[gidx];
-  const int nblk = c >= 0 ? B.goff[gidx + 1] - B.goff[gidx] : 0;
-  const bool lead = c >= 0 && gidx == B.gfirst[c];  // writes the case's state and done flag
+  const int Gtot = gridDim.x * PGROUPS;
   fd_fill_inverse_eigen(inv_eig, c_lam);
-  for (int k = 0; k < KB_CACHE && k < nblk; ++k)
-    if (G.lane < 32) fill_block_info(M, myblocks[k], cache[G.g * KB_CACHE + k], G.lane);
-  if (G.lane == 0 && c >= 0) S = A.st[c];
+  for (int i = threadIdx.x; i < B.ncase; i += blockDim.x) running[i] = 1;
   if (threadIdx.x == 0) epoch = 0u;
   __syncthreads();
-  bool ok = true, any = true;
+  if (threadIdx.x == 0) batch_deal(B.cfirst, running, B.ncase, Gtot, gfirst);
+  __syncthreads();
+  GroupPlace P = group_place(gfirst, B.cfirst, B.ncase, gidx);
+  batch_fill_cache(M, B, cache, P, G);
+  if (G.lane == 0 && P.c >= 0) S = A.st[P.c];
+  __syncthreads();
+  // the case's first group writes its state and done flag
+  auto lead = [&]() { return P.c >= 0 && gidx == gfirst[P.c] && G.lane == 0; };
+  bool ok = true;
   // PREP, INIT, P0: one barrier each
   {
     double a[1] = {0.0};
     BATCH_BLOCKS(bi) a[0] += prep_block<T>(A, G, bi);
-    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, c, nullptr);
-    if (ok && c >= 0 && G.lane == 0) S.mean_sum = a[0];
+    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, P.c, gfirst[max(P.c, 0)], gfirst[max(P.c, 0) + 1],
+                                   nullptr);
+    if (ok && P.c >= 0 && G.lane == 0) S.mean_sum = a[0];
     __syncthreads();
   }
   if (ok) {
     double a[1] = {0.0};
     BATCH_BLOCKS(bi) a[0] += init_block<T>(A, G, tile, bi, S.mean_sum);
-    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, c, nullptr);
-    if (ok && c >= 0 && G.lane == 0) {
-      fin_init(S, a[0]);
-      if (lead) B.case_done[c] = S.done;
-    }
+    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, P.c, gfirst[max(P.c, 0)], gfirst[max(P.c, 0) + 1],
+                                   nullptr);
+    if (ok && P.c >= 0 && G.lane == 0) fin_init(S, a[0]);
     __syncthreads();
   }
   if (ok) {
     double a[1] = {0.0};
-    if (c >= 0 && !S.done) BATCH_BLOCKS(bi) a[0] += p0_block<T>(A, G, tile, bi, inv_eig);
-    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, c, nullptr);
+    if (P.c >= 0 && !S.done) BATCH_BLOCKS(bi) a[0] += p0_block<T>(A, G, tile, bi, inv_eig);
+    ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, P.c, gfirst[max(P.c, 0)], gfirst[max(P.c, 0) + 1],
+                                   nullptr);
     // q = 0 at the start, so z1 = zr
-    if (ok && c >= 0 && G.lane == 0) ms_zr = S.mean_sum = a[0];
+    if (ok && P.c >= 0 && G.lane == 0) S.ms_zr = S.mean_sum = a[0];
+    if (ok && lead()) {
+      A.st[P.c] = S;
+      B.case_done[P.c] = S.done;
+    }
     __syncthreads();
   }
   while (ok) {
-    const bool active = c >= 0 && !S.done;
-    const bool restart = active && S.restart_pending != 0;
-    const double beta = restart ? 0.0 : S.beta;
+    bool active = P.c >= 0 && !S.done;
+    bool restart = active && S.restart_pending != 0;
+    double beta = restart ? 0.0 : S.beta;
     double a[2] = {0.0, 0.0};
     if (active) BATCH_BLOCKS(bi) p1_block<T>(A, G, tile, bi, inv_eig, beta, S.mean_sum, restart, a);
-    if (!(ok = batch_allreduce<2, true>(a, B, Gs, epoch, gsm, G, gidx, c, &any))) break;
-    if (!any) break;  // every case had stopped: this pass did no work
+    // the groups that did P1 for case c: this pass's deal
+    for (int i = threadIdx.x; i <= B.ncase; i += blockDim.x) gfirst_prev[i] = gfirst[i];
+    __syncthreads();
+    if (!(ok = batch_allreduce<2, true>(a, B, Gs, epoch, gsm, G, gidx, P.c, gfirst[max(P.c, 0)],
+                                        gfirst[max(P.c, 0) + 1], running)))
+      break;
+    // cases that stopped in the last iteration give their groups to the
+    // running ones: deal again, take up the new case's state (written by its
+    // first group after the last iteration) and its P1 sums over the groups
+    // that did its P1
+    if (threadIdx.x == 0) {
+      int any = 0, changed = 0;
+      for (int cc = 0; cc < B.ncase; ++cc) {
+        any |= running[cc];
+        changed |= (!running[cc]) && gfirst[cc + 1] > gfirst[cc];
+      }
+      s_changed = any ? changed : -1;
+      if (any && changed) batch_deal(B.cfirst, running, B.ncase, Gtot, gfirst);
+    }
+    __syncthreads();
+    if (s_changed < 0) break;  // every case has stopped
+    if (s_changed) {
+      const int old_c = P.c;
+      P = group_place(gfirst, B.cfirst, B.ncase, gidx);
+      batch_fill_cache(M, B, cache, P, G);
+      if (G.lane == 0 && P.c >= 0) S = A.st[P.c];
+      __syncthreads();
+      if (P.c >= 0 && P.c != old_c) {  // P1 sums of the new case, from the groups that did them
+        double acc[2] = {0.0, 0.0};
+        for (int g = gfirst_prev[P.c] + G.lane; g < gfirst_prev[P.c + 1]; g += GROUP) {
+          const double* part = B.part + size_t((epoch - 1u) & 1u) * B.groups * 8;
+          acc[0] += part[g * 8];
+          acc[1] += part[g * 8 + 1];
+        }
+        group_reduce<2>(acc, gsm, G);
+        a[0] = acc[0];
+        a[1] = acc[1];
+      }
+      active = P.c >= 0 && !S.done;
+      restart = active && S.restart_pending != 0;
+      beta = restart ? 0.0 : S.beta;
+    }
     if (active && G.lane == 0) {
       fin_a(S, S.mean_sum, restart);
       fin_b(S, a[0]);
-      S.beta = beta;                        // the beta that formed z1, for P3
-      S.mean_sum = ms_zr - S.alpha * a[1];  // sum(z2 h^3)
+      S.beta = beta;                          // the beta that formed z1, for P3
+      S.mean_sum = S.ms_zr - S.alpha * a[1];  // sum(z2 h^3)
     }
     __syncthreads();
+    const int g0 = gfirst[max(P.c, 0)], g1 = gfirst[max(P.c, 0) + 1];
     double d[2] = {0.0, 0.0};
     if (active) BATCH_BLOCKS(bi) p2_block<T>(A, G, tile, bi, S.alpha, S.mean_sum, d);
-    if (!(ok = batch_allreduce<2, false>(d, B, Gs, epoch, gsm, G, gidx, c, nullptr))) break;
+    if (!(ok = batch_allreduce<2, false>(d, B, Gs, epoch, gsm, G, gidx, P.c, g0, g1, nullptr))) break;
     if (active && G.lane == 0) fin_d(S, d);
     __syncthreads();
     double e[4] = {0.0, 0.0, 0.0, 0.0};
     if (active)
       BATCH_BLOCKS(bi) p3_block<T>(A, G, tile, bi, inv_eig, xslot(A, S.cur), xslot(A, S.nxt), S.alpha, S.beta,
                                    S.omega, e);
-    if (!(ok = batch_allreduce<4, false>(e, B, Gs, epoch, gsm, G, gidx, c, nullptr))) break;
+    if (!(ok = batch_allreduce<4, false>(e, B, Gs, epoch, gsm, G, gidx, P.c, g0, g1, nullptr))) break;
     if (active && G.lane == 0) {
       const double re[2] = {e[0], e[1]};
       fin_e(S, re);
-      ms_zr = e[2];
+      S.ms_zr = e[2];
       S.mean_sum = S.restart_pending ? e[2] : e[2] + S.beta * e[3];  // sum(z1 h^3) of the next P1
-      if (lead) B.case_done[c] = S.done;
+    }
+    if (active && lead()) {
+      A.st[P.c] = S;
+      B.case_done[P.c] = S.done;
     }
     __syncthreads();
   }
-  // each group moves its blocks' best iterate into x (slot 0)
-  if (ok && c >= 0 && S.best != 0) {
+  if (!ok) {  // a barrier timed out: every case reports it
+    if (threadIdx.x == 0 && blockIdx.x == 0)
+      for (int cc = 0; cc < B.ncase; ++cc) {
+        A.st[cc].done = 1;
+        A.st[cc].status = SOLVE_BARRIER_TIMEOUT;
+      }
+    return;
+  }
+  // every case has stopped: deal all cases again and move each case's best
+  // iterate into x (slot 0), block by block
+  for (int i = threadIdx.x; i < B.ncase; i += blockDim.x) running[i] = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) batch_deal(B.cfirst, running, B.ncase, Gtot, gfirst);
+  __syncthreads();
+  P = group_place(gfirst, B.cfirst, B.ncase, gidx);
+  batch_fill_cache(M, B, cache, P, G);
+  if (G.lane == 0 && P.c >= 0) S = A.st[P.c];
+  __syncthreads();
+  if (P.c >= 0 && S.best != 0) {
     const T* src = xslot(A, S.best);
     BATCH_BLOCKS(bi) {
       double v[8];
       load_col(src, bi.id, G, v);
       store_col(A.xs0, bi.id, G, v);
     }
-  }
-  if (lead && G.lane == 0) {
-    if (!ok) {
-      S.done = 1;
-      S.status = SOLVE_BARRIER_TIMEOUT;
-    }
-    A.st[c] = S;
   }
 }
 
@@ -1489,8 +1623,8 @@ static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, 
 
 // CTAs and block groups of the batched solver: every CTA resident (one
 // group per block at most), the same shape as the single-case solver.
-int batch_solver_shape(int nb, int* grid, int* groups) {
-  const size_t dyn = kPersistentSmem;
+int batch_solver_shape(int nb, int ncase, int* grid, int* groups) {
+  const size_t dyn = batch_smem(ncase);
   void (*kern)(KArgs<double>, GridSync, BatchArgs) = k_bicg_batched<double>;
   CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   int per_sm = 0, dev = 0, sms = 0;
@@ -1526,9 +1660,9 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   KArgs<double> A = make_args<double>(M, b, x, v, W, B.st, P.mean_mode, zmr, 0);
   A.ncache = KB_CACHE;
   GridSync Gs{W.bar, W.partial, W.bar_error};
-  BatchArgs Ba{B.gcase, B.gfirst, B.goff, B.gblocks, B.part, B.case_done, B.ncase, B.groups};
+  BatchArgs Ba{B.cfirst, B.cblocks, B.part, B.case_done, B.ncase, B.groups};
   void* args[] = {(void*)&A, (void*)&Gs, (void*)&Ba};
-  const size_t dyn = kPersistentSmem;
+  const size_t dyn = batch_smem(B.ncase);
   void (*kern)(KArgs<double>, GridSync, BatchArgs) = k_bicg_batched<double>;
   CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   {

@@ -12,6 +12,7 @@ struct KrylovState {
   double err, err_init, err_opt;     // ||r||_2 now, initially, best so far
   double tol_abs, tol_rel;
   double mean_sum;                   // sum(v h^3) of the vector the next SpMV reads
+  double ms_zr;                      // three-phase solvers: sum(zr h^3) of the current zr
   double eps;
   int k, restarts, max_restarts, max_iter;
   int done, converged, restart_pending, status;
@@ -52,15 +53,15 @@ struct PoissonWork {
 
 // Batched solves: independent cases on disjoint blocks of one flattened mesh
 // (no face joins two cases), all in one cooperative launch.  Every block
-// group of the batched solver works for one case.
+// group of the batched solver works for one case at a time; the groups are
+// dealt to the running cases in proportion to their blocks and dealt again
+// whenever a case stops.
 struct BatchWork {
   int ncase = 0;
   int grid = 0;                  // CTAs of the batched solver
   int groups = 0;                // grid * groups per CTA
-  int* gcase = nullptr;          // groups: case of each group (-1: idle)
-  int* gfirst = nullptr;         // ncase + 1: the groups of case c are gfirst[c] .. gfirst[c+1]-1
-  int* goff = nullptr;           // groups + 1: group g visits gblocks[goff[g] .. goff[g+1])
-  int* gblocks = nullptr;        // nb
+  int* cfirst = nullptr;         // ncase + 1: case c owns blocks cfirst[c] .. cfirst[c+1]-1
+  int* cblocks = nullptr;        // nb: each case's blocks by decreasing operator cost, at its own offsets
   double* part = nullptr;        // 2 * groups * 8 partial sums
   int* case_done = nullptr;      // ncase: 1 once the case has stopped
   KrylovState* st = nullptr;     // ncase
@@ -108,8 +109,8 @@ void poisson_init_constants();
 // Number of 64-thread groups of the persistent solver on a mesh of nb blocks
 // (the visit order is balanced for this many groups).
 int persistent_solver_groups(int nb, const PoissonWork& W, int* groups);
-// CTAs and block groups of the batched solver (all co-resident).
-int batch_solver_shape(int nb, int* grid, int* groups);
+// CTAs and block groups of the batched solver for ncase cases (all co-resident).
+int batch_solver_shape(int nb, int ncase, int* grid, int* groups);
 // One BiCGSTAB per case of the batch (x holds x0 on entry and each case's
 // best iterate on exit); out[c] per case.
 int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
