@@ -15,6 +15,9 @@ PressureProjection (RHS, Poisson solve, mean removal, gradient update).
 `e2e`    the same through the reference-facing C ABI with host buffers:
          per step velocity + pressure uploaded from pinned host memory, the
          step, velocity + pressure downloaded.
+`swarm_batch`  64 independent penalized-ellipsoid cases (372-2659 blocks
+         each, 37.5M cells) advanced together by cup_batch_step, with step 0
+         also taken case by case for comparison.
 `--impl reference`  the reference's CPU path restated (oracle: upwind/WENO,
          penalization, projection with the pipelined BiCGSTAB + block CG of
          PoissonSolverAMR.cpp) on the host cores, one step per sample.
@@ -201,6 +204,56 @@ def poisson_at_tolerance(ctx, stream, flush, reps=3):
     return res
 
 
+def swarm_batch(flush, steps=5):
+    """The 64-case ellipsoid swarm advanced as one batch (cup_batch_step: one
+    set of launches and one Poisson launch per step for all cases), against
+    the same cases stepped one by one; device time from CUDA events on the
+    stepping streams, L2 flushed before every timed step."""
+    import torch
+    import cup3d_b200 as cup
+    from cup3d_b200.workloads import SWARM_WORKLOAD, make_swarm_ctx
+    lib = cup._lib.lib()
+    ctxs = [make_swarm_ctx(i, torch.cuda.current_device()) for i in range(64)]
+    batch = cup.Batch(ctxs)
+    ncell = batch.nb * 512
+
+    def timed(ctx, fn):
+        st = torch.cuda.ExternalStream(lib.cup_stream(ctx._p))
+        with torch.cuda.stream(st):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    # step 0 of every case, one by one and as the batch, from the same state
+    single_ms = 0.0
+    for c in ctxs:
+        single_ms += timed(c, lambda: c.step(0))[0]
+    batch0_ms, (_, _, _, st0) = timed(batch, lambda: batch.step(0))
+    ms, its = [], []
+    for k in range(1, steps + 1):
+        t, (_, _, _, st) = timed(batch, lambda: batch.step(k))
+        ms.append(t)
+        its.append([x["iterations"] for x in st])
+    for c in ctxs:
+        c.close()
+    batch.close()
+    return {
+        "workload": SWARM_WORKLOAD, "cases": 64, "cells": ncell,
+        "metric": "Mcell-steps/s (batched time steps of all cases, plain FP64)",
+        "value": round(ncell * steps / (sum(ms) * 1e-3) / 1e6, 3), "steps": f"1..{steps} after step 0",
+        "ms_per_step": [round(x, 2) for x in ms],
+        "poisson_iterations_mean_max": [[round(sum(i) / len(i), 1), max(i)] for i in its],
+        "step0": {"batch_ms": round(batch0_ms, 2), "one_by_one_ms": round(single_ms, 2),
+                  "speedup": round(single_ms / batch0_ms, 3),
+                  "poisson_iterations_mean_max": [round(sum(x["iterations"] for x in st0) / 64, 1),
+                                                  max(x["iterations"] for x in st0)]},
+    }
+
+
 def run_b200(args):
     import torch
     rank, world, local = dist_env()
@@ -364,6 +417,8 @@ def run_b200(args):
     }
     if not args.no_poisson:
         line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush)
+    if rank == 0 and not args.no_swarm:
+        line["swarm_batch"] = swarm_batch(flush)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ctx, args, (vel0, pres0), first_step)
     if world > 1:
@@ -465,6 +520,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson-to-tolerance comparison")
+    ap.add_argument("--no-swarm", action="store_true", help="skip the batched ellipsoid-swarm measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
