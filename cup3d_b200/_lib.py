@@ -53,6 +53,7 @@ class cup_config(C.Structure):
         ("step_2nd_start", C.c_int32),
         ("device", C.c_int32),
         ("poisson_block_cache", C.c_int32),
+        ("step_graph", C.c_int32),
     ]
 
 

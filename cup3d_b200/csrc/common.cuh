@@ -35,9 +35,10 @@ struct DevMesh {
   const double* __restrict__ case_kin;
 };
 
-// Time step of block b: its case's in a batch, else dt.
+// Time step of block b: its case's in a batch, the device-computed one of a
+// captured step (case_dt set, bcase null), else dt.
 __device__ __forceinline__ double block_dt(const DevMesh& M, int b, double dt) {
-  return M.case_dt ? M.case_dt[M.bcase[b]] : dt;
+  return M.case_dt ? M.case_dt[M.bcase ? M.bcase[b] : 0] : dt;
 }
 
 #ifndef CUP3D_TAN_HELPERS

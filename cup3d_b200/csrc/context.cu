@@ -84,6 +84,7 @@ int ctx_upload_mesh(cup_ctx* c) {
 }
 
 int ctx_alloc_fields(cup_ctx* c) {
+  graph_reset(c);
   c->field_arena.release();
   c->obst_arena.release();
   c->ob = DevObstacle();
@@ -116,6 +117,7 @@ int ctx_alloc_fields(cup_ctx* c) {
   if (int rc = A.alloc(&W.bar_error, 1)) return rc;
   if (int rc = A.alloc(&W.st, 1)) return rc;
   if (int rc = A.alloc(&W.st2, 1)) return rc;
+  if (int rc = A.alloc(&W.st_init, 1)) return rc;
   CUP_CUDA_TRY(stream_zero(c->stream, W.counters, 32 * sizeof(unsigned int)));
   CUP_CUDA_TRY(stream_zero(c->stream, W.bar, sizeof(unsigned int)));
   CUP_CUDA_TRY(stream_zero(c->stream, W.bar_error, sizeof(int)));
@@ -197,6 +199,7 @@ void cup_config_default(cup_config* c) {
   c->step_2nd_start = 2;
   c->device = 0;
   c->poisson_block_cache = 4;
+  c->step_graph = 1;
 }
 
 static int parse_bc(const std::string& v) {
@@ -270,6 +273,9 @@ int cup_config_parse(cup_config* c, const char* args) {
     } else if (key == "device") {
       if (need_num()) return CUP_ERR_ARG;
       c->device = int(dv);
+    } else if (key == "stepGraph") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->step_graph = dv != 0 ? 1 : 0;
     } else if (key == "poissonBlockCache") {
       if (need_num()) return CUP_ERR_ARG;
       if (dv < 0 || dv > 4) return ctx_fail(nullptr, CUP_ERR_ARG, "poissonBlockCache must be 0-4");
@@ -302,6 +308,7 @@ cup_ctx* cup_create(const cup_config* cfg) {
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
   if (e == cudaSuccess) e = cudaMallocHost(&c->h_pinned, 4096);
+  if (e == cudaSuccess) e = cudaMallocHost(&c->gio, sizeof(GraphIO));
   if (e == cudaSuccess) e = cudaMalloc(&c->d_scalars, 64 * sizeof(double));
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, cfg->device);
   if (e != cudaSuccess) {
@@ -320,7 +327,10 @@ void cup_destroy(cup_ctx* c) {
   c->field_arena.release();
   c->obst_arena.release();
   if (c->d_scalars) cudaFree(c->d_scalars);
+  for (cudaGraphExec_t& g : c->gexec)
+    if (g) cudaGraphExecDestroy(g);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->gio) cudaFreeHost(c->gio);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -508,7 +518,7 @@ int cup_block_inverse_dev(cup_ctx* c, const double* in, double* out) {
 // FP64 residual.
 static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* stats, bool check_true = true) {
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "a batch of cases solves with cup_batch_poisson_solve_dev");
-  SolveParams P;
+  SolveParams P{};
   P.tol_abs = c->cfg.poisson_tol;
   P.tol_rel = c->cfg.poisson_tol_rel;
   P.max_iter = c->cfg.poisson_max_iter;
@@ -607,6 +617,7 @@ static ObstacleView ob_view(const cup_ctx* c) {
 
 int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
                         const double* kin) {
+  graph_reset(c);
   const Mesh& m = c->mesh;
   c->obst_arena.release();
   c->ob = DevObstacle();
@@ -661,16 +672,22 @@ static int install_host_obstacle(cup_ctx* c, const HostObstacle& h) {
   return 0;
 }
 
-double ctx_calc_dt(const cup_config& cfg, double hmin, double umax, int step) {
-  // Simulation::calcMaxTimestep (Simulation.cpp:326-338)
-  const double dtDiffusion = (1.0 / 6.0) * hmin * hmin / (cfg.nu + (1.0 / 6.0) * hmin * umax);
-  const double dtAdvection = hmin / (umax + 1e-8);
+// The CFL number of step `step`, ramped up from 1e-3 over the first `rampup`
+// steps (Simulation.cpp:329-333).
+static double cfl_factor(const cup_config& cfg, int step) {
   if (step < cfg.rampup) {
     const double x = step / double(cfg.rampup);
-    const double rampCFL = std::exp(std::log(1e-3) * (1 - x) + std::log(cfg.cfl) * x);
-    return std::min(dtDiffusion, rampCFL * dtAdvection);
+    return std::exp(std::log(1e-3) * (1 - x) + std::log(cfg.cfl) * x);
   }
-  return std::min(dtDiffusion, cfg.cfl * dtAdvection);
+  return cfg.cfl;
+}
+
+double ctx_calc_dt(const cup_config& cfg, double hmin, double umax, int step) {
+  // Simulation::calcMaxTimestep (Simulation.cpp:326-338); k_calc_dt repeats
+  // these operations on the device for captured steps
+  const double dtDiffusion = (1.0 / 6.0) * hmin * hmin / (cfg.nu + (1.0 / 6.0) * hmin * umax);
+  const double dtAdvection = hmin / (umax + 1e-8);
+  return std::min(dtDiffusion, cfl_factor(cfg, step) * dtAdvection);
 }
 
 static int grid_of(const cup_ctx* c) { return c->W.grid; }
@@ -709,6 +726,138 @@ static int project(cup_ctx* c, double dt, int step, cup_solve_stats* stats) {
   F.pcur = 1 - F.pcur;
   if (stats) *stats = st;
   return rs;
+}
+
+// ---------------------------------------------------------------------------
+// Captured time steps.  A step with the CFL dt and the plain solver has no
+// host decision inside: dt comes from k_calc_dt (the host supplies only the
+// CFL factor of the step, through pinned memory), the kernels read it from
+// the device (DevMesh::case_dt), the persistent solver moves its best iterate
+// itself, and the state is read back after the step.  The step is captured
+// once per (velocity buffer, pressure buffer, p_old term) and replayed.
+// ---------------------------------------------------------------------------
+void graph_reset(cup_ctx* c) {
+  for (cudaGraphExec_t& g : c->gexec)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
+
+static SolveParams plain_params(const cup_ctx* c) {
+  SolveParams P{};
+  P.tol_abs = c->cfg.poisson_tol;
+  P.tol_rel = c->cfg.poisson_tol_rel;
+  P.max_iter = c->cfg.poisson_max_iter;
+  P.max_restarts = c->cfg.poisson_max_restarts;
+  P.mean_mode = c->cfg.mean_constraint;
+  P.check_every = 8;
+  P.stall_window = 0;
+  P.persistent = 1;
+  P.block_cache = c->cfg.poisson_block_cache;
+  return P;
+}
+
+static int graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraphExec_t* out) {
+  Fields& F = c->F;
+  cudaStream_t s = c->stream;
+  const int grid = grid_of(c);
+  poisson_init_constants();  // before the capture: it writes constant memory
+  SolveParams P = plain_params(c);
+  P.graph = 1;
+  KrylovState init;
+  krylov_init_state(P, init);
+  CUP_CUDA_TRY(stream_h2d(s, c->W.st_init, &init, sizeof(init)));
+  DevMesh dmg = c->dm;
+  dmg.case_dt = c->d_scalars + SC_GDT;
+  const int step_arg = use_pold ? c->cfg.step_2nd_start + 1 : 0;
+  CUP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  auto run = [&]() -> int {
+    CUP_CUDA_TRY(cudaMemcpyAsync(c->d_scalars + SC_GFAC, &c->gio->cfl_fac, sizeof(double), cudaMemcpyHostToDevice, s));
+    if (int r = launch_max_u(c->dm, F.vel[vcur], c->cfg.uinf, c->d_scalars + SC_UMAX, c->W.partial,
+                             c->W.counters + 10, grid, s))
+      return r;
+    if (int r = launch_calc_dt(c->d_scalars + SC_UMAX, c->d_scalars + SC_GFAC, c->cfg.nu, c->mesh.spec.hmin,
+                               c->d_scalars + SC_GDT, s))
+      return r;
+    int v = vcur;
+    for (int st = 0; st < 3; ++st) {
+      if (int r = launch_advect_stage(dmg, F.vel[v], F.vel[1 - v], F.tmpV, 0.0, c->cfg.nu, c->cfg.uinf,
+                                      c->cfg.advection, st, grid, s))
+        return r;
+      v = 1 - v;
+    }
+    if (c->ob.nslots > 0)
+      if (int r = launch_penalize(dmg, F.vel[v], F.chi, ob_view(c), c->d_scalars + SC_KIN, 0.0, c->cfg.lambda,
+                                  c->cfg.implicit_penalization, c->d_scalars + SC_FORCE, c->W.partial,
+                                  c->W.counters + 11, s))
+        return r;
+    double* pold = F.pres[pcur];
+    double* pnew = F.pres[1 - pcur];
+    if (int r = launch_pressure_rhs(dmg, F.vel[v], pold, F.chi, ob_view(c), 0.0, step_arg, c->cfg.step_2nd_start,
+                                    F.lhs, F.phi, grid, s))
+      return r;
+    // event record nodes (external): the solve's device time, read after replay
+    CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev0, s, cudaEventRecordExternal));
+    SolveStats S{};
+    if (int r = poisson_bicgstab(c->dm, F.lhs, F.phi, P, c->W, S, s, c->h_pinned, nullptr)) return r;
+    CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev1, s, cudaEventRecordExternal));
+    if (int r = launch_weighted_sum(c->dm, F.phi, c->d_scalars + SC_SUMS, c->W, s)) return r;
+    if (int r = launch_grad_update(dmg, F.vel[v], F.phi, pold, pnew, c->d_scalars + SC_SUMS, 0.0, step_arg,
+                                   c->cfg.step_2nd_start, grid, s))
+      return r;
+    CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->dt, c->d_scalars + SC_GDT, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->st, c->W.st, sizeof(KrylovState), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->bar_error, c->W.bar_error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return 0;
+  };
+  solver_pdl(false);
+  rc = run();
+  solver_pdl(true);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  const cudaError_t e2 = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e2 != cudaSuccess) return set_cuda_error(e2, "cudaGraphInstantiate", __FILE__, __LINE__);
+  return 0;
+}
+
+static int graph_step(cup_ctx* c, int step, double* dt_used, cup_solve_stats* stats) {
+  Fields& F = c->F;
+  const int use_pold = step > c->cfg.step_2nd_start ? 1 : 0;
+  const int key = F.vcur | (F.pcur << 1) | (use_pold << 2);
+  if (!c->gexec[key])
+    if (int rc = graph_capture(c, F.vcur, F.pcur, use_pold, &c->gexec[key])) return keep(c, rc);
+  c->gio->cfl_fac = cfl_factor(c->cfg, step);
+  CUP_CUDA_TRY(cudaGraphLaunch(c->gexec[key], c->stream));
+  CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  F.vcur = 1 - F.vcur;  // three advection stages
+  F.pcur = 1 - F.pcur;
+  const KrylovState& K = c->gio->st;
+  if (c->gio->bar_error) return ctx_fail(c, CUP_ERR_CUDA, "persistent BiCGSTAB: a grid barrier wait timed out");
+  if (dt_used) *dt_used = c->gio->dt;
+  if (!(c->gio->dt > 0)) return ctx_fail(c, CUP_ERR_NAN, "dt <= 0 or NaN (Simulation.cpp:344-347)");
+  float ms = 0;
+  CUP_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  const int status = K.done ? K.status : SOLVE_MAXITER;
+  if (stats) {
+    stats->iterations = K.k;
+    stats->restarts = K.restarts;
+    stats->status = status;
+    stats->fallback = 0;
+    stats->err_init = K.err_init;
+    stats->err_final = K.err_opt;
+    stats->true_rel = -1.0;
+    stats->milliseconds = ms;
+  }
+  if (status == SOLVE_NAN) return ctx_fail(c, CUP_ERR_NAN, "Poisson solve produced NaN");
+  return status == SOLVE_CONVERGED ? CUP_OK : CUP_SOFT_MAXITER;
 }
 
 }  // namespace cup3d
@@ -824,6 +973,8 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_step: no mesh");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_step: not available on a batch of cases");
+  if (!(dt > 0) && c->cfg.step_graph && c->cfg.poisson_solver == CUP_POISSON_B200 && !c->prof.on)
+    return graph_step(c, step, dt_used, stats);
   if (!(dt > 0))
     if (int rc = cup_compute_dt(c, step, &dt)) return rc;
   if (dt_used) *dt_used = dt;

@@ -71,7 +71,15 @@ struct BatchStep {
 };
 
 // Offsets into cup_ctx::d_scalars
-enum : int { SC_SUMS = 0, SC_UMAX = 2, SC_FORCE = 8, SC_KIN = 16, SC_TARGET_SUMSQ = 32 };
+enum : int { SC_SUMS = 0, SC_UMAX = 2, SC_FORCE = 8, SC_KIN = 16, SC_TARGET_SUMSQ = 32, SC_GFAC = 48, SC_GDT = 49 };
+
+// Host side of a captured step: the CFL factor going in, the state coming out.
+struct GraphIO {
+  double cfl_fac;
+  double dt;
+  int bar_error;
+  KrylovState st;
+};
 
 struct Fields {
   double* vel[2] = {nullptr, nullptr};  // ping-pong, 3*nb*512 each
@@ -109,6 +117,9 @@ struct cup_ctx {
   std::vector<cup3d::Mesh> case_mesh;  // each case's own mesh
   cup3d::BatchWork B{};
   cup3d::BatchStep T{};
+  // captured time steps, by (velocity buffer, pressure buffer, p_old term)
+  cudaGraphExec_t gexec[8] = {};
+  cup3d::GraphIO* gio = nullptr;      // pinned
   cup3d::DevArena batch_arena;
 };
 
@@ -126,6 +137,9 @@ int ctx_alloc_fields(cup_ctx* c);
 // Installs an obstacle (nslots blocks with chi, udef and kinematics kin[9]).
 int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
                         const double* kin);
+// Drops the captured time steps (after any change of mesh, obstacle or
+// solver settings).
+void graph_reset(cup_ctx* c);
 // Simulation::calcMaxTimestep for spacing hmin and max |u| umax.
 double ctx_calc_dt(const cup_config& cfg, double hmin, double umax, int step);
 size_t nbn(const cup_ctx* c);

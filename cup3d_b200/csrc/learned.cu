@@ -262,6 +262,7 @@ int cup_set_poisson(cup_ctx* c, int32_t solver, double tol_abs, double tol_rel, 
   c->cfg.poisson_tol = tol_abs;
   c->cfg.poisson_tol_rel = tol_rel;
   c->cfg.poisson_max_iter = max_iter;
+  graph_reset(c);  // captured steps hold the old settings
   return 0;
 }
 

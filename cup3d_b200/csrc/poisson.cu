@@ -1046,6 +1046,16 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
     }
     __syncthreads();
   }
+  // every CTA holds the final state: its groups move the best iterate into
+  // x (slot 0) block by block
+  if (ok && S.best != 0) {
+    const T* src = xslot(A, S.best);
+    PERSISTENT_BLOCKS(bi) {
+      double v[8];
+      load_col(src, bi.id, G, v);
+      store_col(A.xs0, bi.id, G, v);
+    }
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (!ok) {
       S.done = 1;
@@ -1554,6 +1564,11 @@ int launch_block_inverse(const DevMesh& M, const double* in, double* out, Poisso
   return 0;
 }
 
+// Programmatic dependent launch for this thread's solver launches (off while
+// a step is captured into a CUDA graph).
+static thread_local bool t_pdl = true;
+void solver_pdl(bool on) { t_pdl = on; }
+
 // Launches a solver kernel with programmatic stream serialization: its CTAs
 // may be scheduled while the previous kernel drains and wait in pdl_wait().
 template <class T>
@@ -1572,7 +1587,7 @@ static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, 
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = t_pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, A);
 }
 
@@ -1593,11 +1608,12 @@ static int persistent_grid(int nb, const PoissonWork& W, int* grid) {
   return 0;
 }
 
-int persistent_solver_groups(int nb, const PoissonWork& W, int* groups) {
+int persistent_solver_groups(int nb, PoissonWork& W, int* groups) {
   int g1 = 0, g2 = 0;
   if (int rc = persistent_grid<double>(nb, W, &g1)) return rc;
   if (int rc = persistent_grid<float>(nb, W, &g2)) return rc;
   if (g1 != g2) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: FP64 and FP32 grids differ");
+  W.pgrid = g1;  // the launches use it (nothing to query while a graph is captured)
   *groups = g1 * PGROUPS;
   return 0;
 }
@@ -1608,8 +1624,9 @@ template <class T>
 static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, const char* name) {
   const size_t dyn = kPersistentSmem;
   void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
-  int grid = 0;
-  if (int rc = persistent_grid<T>(A.M.nb, W, &grid)) return rc;
+  int grid = W.pgrid;
+  if (grid <= 0)
+    if (int rc = persistent_grid<T>(A.M.nb, W, &grid)) return rc;
   // the arrival counter and the error flag start at zero
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
@@ -1686,20 +1703,30 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   return 0;
 }
 
-// Runs BiCGSTAB on vectors of type T; x holds x0 on entry, x_opt on exit.
-template <class T>
-static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, int zero_mean_row,
-                        PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done,
-                        const CnnWeights* cnn = nullptr) {
-  const bool f32 = sizeof(T) == 4;
-  KrylovState init{};
+void krylov_init_state(const SolveParams& P, KrylovState& init) {
+  init = KrylovState{};
   init.tol_abs = P.tol_abs;
   init.tol_rel = P.tol_rel;
   init.max_iter = P.max_iter;
   init.max_restarts = P.max_restarts;
   init.stall_window = P.stall_window;
   init.eps = 1e-21;
-  CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+}
+
+// Runs BiCGSTAB on vectors of type T; x holds x0 on entry, x_opt on exit.
+template <class T>
+static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, int zero_mean_row,
+                        PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done,
+                        const CnnWeights* cnn = nullptr) {
+  const bool f32 = sizeof(T) == 4;
+  KrylovState init;
+  krylov_init_state(P, init);
+  const bool persistent = !cnn && P.persistent;
+  if (P.graph && !persistent) return set_error(CUP_ERR_STATE, "captured solves need the persistent solver");
+  if (P.graph)
+    CUP_CUDA_TRY(cudaMemcpyAsync(W.st, W.st_init, sizeof(init), cudaMemcpyDeviceToDevice, s));
+  else
+    CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   KArgs<T> A = make_args<T>(M, b, x, v, W, W.st, P.mean_mode, zero_mean_row, 0);
   A.ext_precond = cnn ? 1 : 0;
   A.ncache = std::max(0, std::min(P.block_cache, KB_CACHE));
@@ -1707,9 +1734,9 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_prepare<T>, W.grid, s, A)); }
   { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_init<T>, W.ggrid, s, A)); }
   CUP_CUDA_TRY(cudaGetLastError());
-  const bool persistent = !cnn && P.persistent;
   if (persistent) {
     if (int rc = launch_persistent<T>(A, W, s, f32 ? "bicg32_persistent" : "bicg_persistent")) return rc;
+    if (P.graph) return 0;  // the caller reads the state after the graph runs
     int h_err = 0;
     CUP_CUDA_TRY(cudaMemcpyAsync(&h_err, W.bar_error, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUP_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1736,7 +1763,7 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   KrylovState fin;
   CUP_CUDA_TRY(cudaMemcpyAsync(&fin, W.st, sizeof(fin), cudaMemcpyDeviceToHost, s));
   CUP_CUDA_TRY(cudaStreamSynchronize(s));
-  if (fin.best != 0) {
+  if (fin.best != 0 && !persistent) {  // the persistent kernel moves it itself
     T* src = fin.best == 1 ? v[7] : v[8];
     CUP_CUDA_TRY(cudaMemcpyAsync(x, src, size_t(M.nb) * BN * sizeof(T), cudaMemcpyDeviceToDevice, s));
   }

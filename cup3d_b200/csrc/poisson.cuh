@@ -43,11 +43,13 @@ struct PoissonWork {
   float *fr, *frhat, *fp, *fnu, *ft, *fz1, *fz2, *fxs[3], *r32;
   KrylovState* st;
   KrylovState* st2;         // outer (refinement) state
+  KrylovState* st_init;     // captured solves: the initial state, uploaded before capture
   double* partial;          // grid * 8
   unsigned int* counters;   // 16
   unsigned int* bar;        // persistent solver: grid-barrier arrivals
   int* bar_error;           // persistent solver: set on a timed-out barrier wait
   int grid;                 // CTAs for block kernels
+  int pgrid;                // CTAs of the persistent solver (set with the visit order)
   int ggrid;                // CTAs for block-group kernels (4 mesh blocks per CTA pass)
 };
 
@@ -74,6 +76,8 @@ struct SolveParams {
   int stall_window;  // 0: off (reference behaviour)
   int persistent;    // 1: all iterations in one cooperative launch (plain and mixed solvers)
   int block_cache;   // persistent solver: table entries staged per block group at launch (0-4)
+  int graph;         // 1: being captured into a CUDA graph: the initial state comes from
+                     //    PoissonWork::st_init and nothing is read back (plain persistent solver only)
 };
 
 struct SolveStats {
@@ -108,7 +112,12 @@ void poisson_init_constants();
 
 // Number of 64-thread groups of the persistent solver on a mesh of nb blocks
 // (the visit order is balanced for this many groups).
-int persistent_solver_groups(int nb, const PoissonWork& W, int* groups);
+int persistent_solver_groups(int nb, PoissonWork& W, int* groups);
+// Programmatic dependent launch of the solver kernels on this thread (on by
+// default; off while capturing a CUDA graph).
+void solver_pdl(bool on);
+// The solver state before the first kernel (tolerances and caps of P).
+void krylov_init_state(const SolveParams& P, KrylovState& init);
 // CTAs and block groups of the batched solver for ncase cases (all co-resident).
 int batch_solver_shape(int nb, int ncase, int* grid, int* groups);
 // One BiCGSTAB per case of the batch (x holds x0 on entry and each case's

@@ -615,4 +615,26 @@ int launch_case_forces(const double* slot_force, const int* slot_first, int ncas
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Simulation::calcMaxTimestep on the device, for captured steps: the same
+// operations in the same order as the host version (no contraction), with
+// the CFL factor (ramped or not) computed on the host: bit-identical dt.
+// ---------------------------------------------------------------------------
+__global__ void k_calc_dt(const double* __restrict__ umax, const double* __restrict__ cfl_fac, double nu,
+                          double hmin, double* dt) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double u = *umax;
+  const double t = __dmul_rn(1.0 / 6.0, hmin);
+  const double dtDiffusion = __ddiv_rn(__dmul_rn(t, hmin), __dadd_rn(nu, __dmul_rn(t, u)));
+  const double dtAdvection = __ddiv_rn(hmin, __dadd_rn(u, 1e-8));
+  const double cand = __dmul_rn(*cfl_fac, dtAdvection);
+  *dt = cand < dtDiffusion ? cand : dtDiffusion;
+}
+
+int launch_calc_dt(const double* umax, const double* cfl_fac, double nu, double hmin, double* dt, cudaStream_t s) {
+  k_calc_dt<<<1, 32, 0, s>>>(umax, cfl_fac, nu, hmin, dt);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 }  // namespace cup3d

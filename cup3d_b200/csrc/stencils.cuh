@@ -54,4 +54,8 @@ int launch_case_sums(const DevMesh& M, const double* phi, double* bsum, const in
                      int grid, cudaStream_t s);
 int launch_case_forces(const double* slot_force, const int* slot_first, int ncase, double* out, cudaStream_t s);
 
+// dt = min(dtDiffusion, cfl_fac * dtAdvection) of Simulation::calcMaxTimestep
+// from the device's max |u|, bit-identical to the host computation.
+int launch_calc_dt(const double* umax, const double* cfl_fac, double nu, double hmin, double* dt, cudaStream_t s);
+
 }  // namespace cup3d

@@ -79,6 +79,9 @@ typedef struct cup_config {
   int32_t poisson_block_cache; /* -poissonBlockCache: mesh-table entries per block group kept in
                                   shared memory by the persistent solver (0-4; 4 by default);
                                   a tuning knob with no reference counterpart */
+  int32_t step_graph;          /* -stepGraph: cup_step with dt <= 0 and the plain solver replays a
+                                  CUDA graph of the whole step (1, default) or launches the
+                                  kernels one by one (0); the same kernels either way */
 } cup_config;
 
 typedef struct cup_solve_stats {
