@@ -208,12 +208,13 @@ def swarm_batch(flush, steps=5):
     """The 64-case ellipsoid swarm advanced as one batch (cup_batch_step: one
     set of launches and one Poisson launch per step for all cases), against
     the same cases stepped one by one; device time from CUDA events on the
-    stepping streams, L2 flushed before every timed step."""
+    stepping streams, L2 flushed before every timed step.  Kernel by kernel
+    (-stepGraph 0) on both sides, so that no step pays a graph capture."""
     import torch
     import cup3d_b200 as cup
     from cup3d_b200.workloads import SWARM_WORKLOAD, make_swarm_ctx
     lib = cup._lib.lib()
-    ctxs = [make_swarm_ctx(i, torch.cuda.current_device()) for i in range(64)]
+    ctxs = [make_swarm_ctx(i, torch.cuda.current_device(), "-stepGraph 0") for i in range(64)]
     batch = cup.Batch(ctxs)
     ncell = batch.nb * 512
 

@@ -162,6 +162,18 @@ static int batch_step_setup(cup_ctx* c, const std::vector<const cup_ctx*>& cases
   if (int rc = A.alloc(&T.slot_force, 6 * size_t(std::max(NS, 1)))) return rc;
   CUP_CUDA_TRY(stream_h2d(c->stream, T.kin, kin.data(), kin.size() * 8));
   CUP_CUDA_TRY(stream_zero(c->stream, T.force, 6 * size_t(K) * 8));
+  std::vector<double> hmin(K);
+  for (int k = 0; k < K; ++k) hmin[k] = c->case_mesh[k].spec.hmin;
+  if (int rc = A.alloc(&T.hmin, size_t(K))) return rc;
+  CUP_CUDA_TRY(stream_h2d(c->stream, T.hmin, hmin.data(), K * sizeof(double)));
+  if (int rc = A.alloc(&c->B.st_init, size_t(K))) return rc;
+  // pinned host copies for captured steps
+  const size_t bytes = sizeof(KrylovState) * K + sizeof(double) * 7 * K + sizeof(int) * 4;
+  CUP_CUDA_TRY(cudaMallocHost(&T.h_block, bytes));
+  T.h_st = static_cast<KrylovState*>(T.h_block);
+  T.h_dt = reinterpret_cast<double*>(T.h_st + K);
+  T.h_force = T.h_dt + K;
+  T.h_err = reinterpret_cast<int*>(T.h_force + 6 * K);
   c->dm.case_dt = T.dt;
   c->dm.case_sums = T.sums;
   c->dm.case_kin = T.kin;
@@ -210,6 +222,110 @@ static int batch_stats(cup_ctx* c, const std::vector<SolveStats>& S, float ms, c
     else if (S[k].status != SOLVE_CONVERGED && rc == CUP_OK) rc = CUP_SOFT_MAXITER;
   }
   return rc;
+}
+
+// A batch step with every case at its CFL dt, captured as a CUDA graph: the
+// per-case dt comes from k_case_calc_dt (the host supplies the step's CFL
+// factor through pinned memory), the solver starts from device templates and
+// moves its best iterates itself, and dt, forces, solver states and the
+// barrier flag are copied back by the graph.
+static int batch_graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraphExec_t* out) {
+  const int K = c->ncase;
+  Fields& F = c->F;
+  BatchStep& T = c->T;
+  cudaStream_t s = c->stream;
+  const int grid = c->W.grid;
+  poisson_init_constants();
+  SolveParams P = batch_params(c);
+  P.graph = 1;
+  std::vector<KrylovState> init(K);
+  for (KrylovState& k : init) krylov_init_state(P, k);
+  CUP_CUDA_TRY(stream_h2d(s, c->B.st_init, init.data(), K * sizeof(KrylovState)));
+  const ObstacleView ob = batch_ob_view(c);
+  const int step_arg = use_pold ? c->cfg.step_2nd_start + 1 : 0;
+  CUP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  auto run = [&]() -> int {
+    CUP_CUDA_TRY(cudaMemcpyAsync(c->d_scalars + SC_GFAC, &c->gio->cfl_fac, sizeof(double), cudaMemcpyHostToDevice, s));
+    if (int r = launch_case_max_u(c->dm, F.vel[vcur], c->cfg.uinf, T.bscratch, T.first, K, T.umax, grid, s)) return r;
+    if (int r = launch_case_calc_dt(T.umax, c->d_scalars + SC_GFAC, c->cfg.nu, T.hmin, K, T.dt, s)) return r;
+    int v = vcur;
+    for (int st = 0; st < 3; ++st) {
+      if (int r = launch_advect_stage(c->dm, F.vel[v], F.vel[1 - v], F.tmpV, 0.0, c->cfg.nu, c->cfg.uinf,
+                                      c->cfg.advection, st, grid, s))
+        return r;
+      v = 1 - v;
+    }
+    if (ob.nslots > 0) {
+      if (int r = launch_penalize(c->dm, F.vel[v], F.chi, ob, T.kin, 0.0, c->cfg.lambda, c->cfg.implicit_penalization,
+                                  nullptr, c->W.partial, c->W.counters + 11, s, T.slot_force))
+        return r;
+      if (int r = launch_case_forces(T.slot_force, T.slot_first, K, T.force, s)) return r;
+    }
+    double* pold = F.pres[pcur];
+    double* pnew = F.pres[1 - pcur];
+    if (int r = launch_pressure_rhs(c->dm, F.vel[v], pold, F.chi, ob, 0.0, step_arg, c->cfg.step_2nd_start, F.lhs,
+                                    F.phi, grid, s))
+      return r;
+    CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev0, s, cudaEventRecordExternal));
+    if (int r = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, P, c->W, c->B, nullptr, s)) return r;
+    CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev1, s, cudaEventRecordExternal));
+    if (int r = launch_case_sums(c->dm, F.phi, T.bscratch, T.first, K, T.sums, grid, s)) return r;
+    if (int r = launch_grad_update(c->dm, F.vel[v], F.phi, pold, pnew, nullptr, 0.0, step_arg,
+                                   c->cfg.step_2nd_start, grid, s))
+      return r;
+    CUP_CUDA_TRY(cudaMemcpyAsync(T.h_dt, T.dt, K * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaMemcpyAsync(T.h_force, T.force, 6 * K * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaMemcpyAsync(T.h_st, c->B.st, K * sizeof(KrylovState), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaMemcpyAsync(T.h_err, c->W.bar_error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return 0;
+  };
+  solver_pdl(false);
+  const int rc = run();
+  solver_pdl(true);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return set_cuda_error(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+  const cudaError_t e2 = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e2 != cudaSuccess) return set_cuda_error(e2, "cudaGraphInstantiate", __FILE__, __LINE__);
+  return 0;
+}
+
+static int batch_graph_step(cup_ctx* c, int step, double* dt_used, double* force, cup_solve_stats* stats) {
+  const int K = c->ncase;
+  Fields& F = c->F;
+  BatchStep& T = c->T;
+  const int use_pold = step > c->cfg.step_2nd_start ? 1 : 0;
+  const int key = F.vcur | (F.pcur << 1) | (use_pold << 2);
+  if (!c->gexec[key])
+    if (int rc = batch_graph_capture(c, F.vcur, F.pcur, use_pold, &c->gexec[key])) return keep_err(c, rc);
+  c->gio->cfl_fac = ctx_cfl_factor(c->cfg, step);
+  CUP_CUDA_TRY(cudaGraphLaunch(c->gexec[key], c->stream));
+  CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  F.vcur = 1 - F.vcur;  // three advection stages
+  F.pcur = 1 - F.pcur;
+  if (*T.h_err) return ctx_fail(c, CUP_ERR_CUDA, "batched BiCGSTAB: a grid barrier wait timed out");
+  for (int k = 0; k < K; ++k) {
+    dt_used[k] = T.h_dt[k];
+    if (!(T.h_dt[k] > 0)) return ctx_fail(c, CUP_ERR_NAN, "cup_batch_step: dt <= 0 or NaN in case " + std::to_string(k));
+  }
+  if (force) std::copy_n(T.h_force, 6 * K, force);
+  float ms = 0;
+  CUP_CUDA_TRY(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  std::vector<SolveStats> S(K);
+  for (int k = 0; k < K; ++k) {
+    const KrylovState& st = T.h_st[k];
+    S[k].iterations = st.k;
+    S[k].restarts = st.restarts;
+    S[k].status = st.done ? st.status : SOLVE_MAXITER;
+    S[k].err_init = st.err_init;
+    S[k].err_opt = st.err_opt;
+  }
+  return batch_stats(c, S, ms, stats);
 }
 
 }  // namespace cup3d
@@ -286,6 +402,7 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
                    cup_solve_stats* stats) {
   ProfBind pb_(c);
   if (!c || c->ncase < 2 || !dt_used) return ctx_fail(c, CUP_ERR_ARG, "cup_batch_step: not a batch or bad arguments");
+  if (!dt_in && c->cfg.step_graph && !c->prof.on) return batch_graph_step(c, step, dt_used, force, stats);
   const int K = c->ncase;
   BatchStep& T = c->T;
   Fields& F = c->F;

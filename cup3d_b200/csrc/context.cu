@@ -329,6 +329,7 @@ void cup_destroy(cup_ctx* c) {
   if (c->d_scalars) cudaFree(c->d_scalars);
   for (cudaGraphExec_t& g : c->gexec)
     if (g) cudaGraphExecDestroy(g);
+  if (c->T.h_block) cudaFreeHost(c->T.h_block);
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   if (c->gio) cudaFreeHost(c->gio);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -674,7 +675,7 @@ static int install_host_obstacle(cup_ctx* c, const HostObstacle& h) {
 
 // The CFL number of step `step`, ramped up from 1e-3 over the first `rampup`
 // steps (Simulation.cpp:329-333).
-static double cfl_factor(const cup_config& cfg, int step) {
+double ctx_cfl_factor(const cup_config& cfg, int step) {
   if (step < cfg.rampup) {
     const double x = step / double(cfg.rampup);
     return std::exp(std::log(1e-3) * (1 - x) + std::log(cfg.cfl) * x);
@@ -687,7 +688,7 @@ double ctx_calc_dt(const cup_config& cfg, double hmin, double umax, int step) {
   // these operations on the device for captured steps
   const double dtDiffusion = (1.0 / 6.0) * hmin * hmin / (cfg.nu + (1.0 / 6.0) * hmin * umax);
   const double dtAdvection = hmin / (umax + 1e-8);
-  return std::min(dtDiffusion, cfl_factor(cfg, step) * dtAdvection);
+  return std::min(dtDiffusion, ctx_cfl_factor(cfg, step) * dtAdvection);
 }
 
 static int grid_of(const cup_ctx* c) { return c->W.grid; }
@@ -834,7 +835,7 @@ static int graph_step(cup_ctx* c, int step, double* dt_used, cup_solve_stats* st
   const int key = F.vcur | (F.pcur << 1) | (use_pold << 2);
   if (!c->gexec[key])
     if (int rc = graph_capture(c, F.vcur, F.pcur, use_pold, &c->gexec[key])) return keep(c, rc);
-  c->gio->cfl_fac = cfl_factor(c->cfg, step);
+  c->gio->cfl_fac = ctx_cfl_factor(c->cfg, step);
   CUP_CUDA_TRY(cudaGraphLaunch(c->gexec[key], c->stream));
   CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
   F.vcur = 1 - F.vcur;  // three advection stages

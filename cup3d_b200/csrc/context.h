@@ -68,6 +68,13 @@ struct BatchStep {
   double* force = nullptr;      // 6 ncase: penalization force and torque
   double* bscratch = nullptr;   // 2 nb
   double* slot_force = nullptr; // 6 nslots
+  double* hmin = nullptr;       // ncase: finest spacing of each case
+  // pinned host copies filled by captured steps
+  double* h_dt = nullptr;       // ncase
+  double* h_force = nullptr;    // 6 ncase
+  KrylovState* h_st = nullptr;  // ncase
+  int* h_err = nullptr;
+  void* h_block = nullptr;      // the pinned allocation holding them
 };
 
 // Offsets into cup_ctx::d_scalars
@@ -140,6 +147,8 @@ int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const dou
 // Drops the captured time steps (after any change of mesh, obstacle or
 // solver settings).
 void graph_reset(cup_ctx* c);
+// The CFL number of a step (ramped up over the first -rampup steps).
+double ctx_cfl_factor(const cup_config& cfg, int step);
 // Simulation::calcMaxTimestep for spacing hmin and max |u| umax.
 double ctx_calc_dt(const cup_config& cfg, double hmin, double umax, int step);
 size_t nbn(const cup_ctx* c);

@@ -1660,17 +1660,13 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   if (B.ncase < 1 || !B.st) return set_error(CUP_ERR_STATE, "batched BiCGSTAB: not a batch");
   double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
   const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
-  std::vector<KrylovState> init(B.ncase);
-  for (KrylovState& k : init) {
-    k = KrylovState{};
-    k.tol_abs = P.tol_abs;
-    k.tol_rel = P.tol_rel;
-    k.max_iter = P.max_iter;
-    k.max_restarts = P.max_restarts;
-    k.stall_window = P.stall_window;
-    k.eps = 1e-21;
+  if (P.graph) {  // captured: the initial states come from the device template
+    CUP_CUDA_TRY(cudaMemcpyAsync(B.st, B.st_init, sizeof(KrylovState) * B.ncase, cudaMemcpyDeviceToDevice, s));
+  } else {
+    std::vector<KrylovState> init(B.ncase);
+    for (KrylovState& k : init) krylov_init_state(P, k);
+    CUP_CUDA_TRY(cudaMemcpyAsync(B.st, init.data(), sizeof(KrylovState) * B.ncase, cudaMemcpyHostToDevice, s));
   }
-  CUP_CUDA_TRY(cudaMemcpyAsync(B.st, init.data(), sizeof(KrylovState) * B.ncase, cudaMemcpyHostToDevice, s));
   CUP_CUDA_TRY(cudaMemsetAsync(B.case_done, 0, sizeof(int) * B.ncase, s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
@@ -1681,11 +1677,12 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   void* args[] = {(void*)&A, (void*)&Gs, (void*)&Ba};
   const size_t dyn = batch_smem(B.ncase);
   void (*kern)(KArgs<double>, GridSync, BatchArgs) = k_bicg_batched<double>;
-  CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+  if (!P.graph) CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   {
     ProfScope ps("bicg_batched", s);
     CUP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(B.grid), dim3(PNT), args, dyn, s));
   }
+  if (P.graph) return 0;  // the caller reads the states after the graph runs
   int h_err = 0;
   std::vector<KrylovState> fin(B.ncase);
   CUP_CUDA_TRY(cudaMemcpyAsync(&h_err, W.bar_error, sizeof(int), cudaMemcpyDeviceToHost, s));

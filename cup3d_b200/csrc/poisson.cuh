@@ -67,6 +67,7 @@ struct BatchWork {
   double* part = nullptr;        // 2 * groups * 8 partial sums
   int* case_done = nullptr;      // ncase: 1 once the case has stopped
   KrylovState* st = nullptr;     // ncase
+  KrylovState* st_init = nullptr;  // ncase: initial states of captured solves
 };
 
 struct SolveParams {

@@ -637,4 +637,24 @@ int launch_calc_dt(const double* umax, const double* cfl_fac, double nu, double 
   return 0;
 }
 
+// The same per case of a batch: dt[c] from umax[c] and hmin[c].
+__global__ void k_case_calc_dt(const double* __restrict__ umax, const double* __restrict__ cfl_fac, double nu,
+                               const double* __restrict__ hmin, int ncase, double* dt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncase) return;
+  const double u = umax[c], hm = hmin[c];
+  const double t = __dmul_rn(1.0 / 6.0, hm);
+  const double dtDiffusion = __ddiv_rn(__dmul_rn(t, hm), __dadd_rn(nu, __dmul_rn(t, u)));
+  const double dtAdvection = __ddiv_rn(hm, __dadd_rn(u, 1e-8));
+  const double cand = __dmul_rn(*cfl_fac, dtAdvection);
+  dt[c] = cand < dtDiffusion ? cand : dtDiffusion;
+}
+
+int launch_case_calc_dt(const double* umax, const double* cfl_fac, double nu, const double* hmin, int ncase,
+                        double* dt, cudaStream_t s) {
+  k_case_calc_dt<<<(ncase + 127) / 128, 128, 0, s>>>(umax, cfl_fac, nu, hmin, ncase, dt);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 }  // namespace cup3d

@@ -57,5 +57,8 @@ int launch_case_forces(const double* slot_force, const int* slot_first, int ncas
 // dt = min(dtDiffusion, cfl_fac * dtAdvection) of Simulation::calcMaxTimestep
 // from the device's max |u|, bit-identical to the host computation.
 int launch_calc_dt(const double* umax, const double* cfl_fac, double nu, double hmin, double* dt, cudaStream_t s);
+// The same for every case of a batch (hmin[ncase], umax[ncase] -> dt[ncase]).
+int launch_case_calc_dt(const double* umax, const double* cfl_fac, double nu, const double* hmin, int ncase,
+                        double* dt, cudaStream_t s);
 
 }  // namespace cup3d

@@ -76,12 +76,13 @@ def swarm_case(i):
     return dict(quat=q, vel=speed * long_axis, bpd=bpd, level_max=level_max, center=center)
 
 
-def make_swarm_ctx(i, device):
-    """Context of swarm case i with its mesh and its ellipsoid."""
+def make_swarm_ctx(i, device, extra=""):
+    """Context of swarm case i with its mesh and its ellipsoid (extra: more flags)."""
     import cup3d_b200 as cup
     p = swarm_case(i)
     b = p["bpd"]
-    cfg = cup.config(SWARM_FLAGS + f" -bpdx {b} -bpdy {b} -bpdz {b} -levelMax {p['level_max']}", device=device)
+    cfg = cup.config(SWARM_FLAGS + f" -bpdx {b} -bpdy {b} -bpdz {b} -levelMax {p['level_max']} {extra}",
+                     device=device)
     ctx = cup.Context(cfg)
     ctx.set_mesh_sphere_wake(p["center"], SWARM_AXES[0], 1, near_radius=0.6, wake_len=0.0, wake_radius=0.6)
     if device >= 0:

@@ -12,7 +12,8 @@
   residual on its own context's device operator is within the tolerance;
 * the single-case entry points refuse a batch;
 * time steps of a batch (own dt, obstacle, mean and solve per case) match
-  the same cases stepped one by one.
+  the same cases stepped one by one, and replayed from a CUDA graph they
+  match the kernel-by-kernel batch step bit for bit.
 """
 import numpy as np
 import pytest
@@ -133,8 +134,8 @@ def _smooth_velocity(ctx, phase):
                            0.3 * np.sin(y + z + phase)])
 
 
-def _step_cases():
-    flags = "-poissonTol 0 -poissonTolRel 1e-11 -nu 0.01 -CFL 0.3 -rampup 0 -advection weno5"
+def _step_cases(extra=""):
+    flags = "-poissonTol 0 -poissonTolRel 1e-11 -nu 0.01 -CFL 0.3 -rampup 0 -advection weno5 " + extra
     a = make_ctx("tgv32", device=0, extra=flags)
     xyz, _ = a.cell_centres()
     x, y, z = xyz.T
@@ -178,3 +179,16 @@ def test_batch_steps_match_single_cases():
             p1 = s.download("pres")
             pb = batch.case_field("pres", k)[0]
             assert np.abs(pb - p1).max() <= 1e-7 * np.abs(p1).max(), (step, k)
+
+
+def test_captured_batch_steps_match_launched_batch_steps():
+    # the batch step replayed as a CUDA graph (per-case dt on the device)
+    # against the same step launched kernel by kernel: bit for bit
+    batches = [cup.Batch(_step_cases(f"-stepGraph {g}")) for g in (1, 0)]
+    for step in range(4):
+        out = [b.step(step) for b in batches]
+        (rc1, dt1, f1, st1), (rc0, dt0, f0, st0) = out
+        assert rc1 == rc0 and np.array_equal(dt1, dt0) and np.array_equal(f1, f0), step
+        assert [s["iterations"] for s in st1] == [s["iterations"] for s in st0], step
+        assert np.array_equal(batches[0].download("vel"), batches[1].download("vel")), step
+        assert np.array_equal(batches[0].download("pres"), batches[1].download("pres")), step
