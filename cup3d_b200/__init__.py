@@ -223,6 +223,14 @@ class Context:
         rc = check(lib().cup_step(self._p, step, dt, C.byref(used), C.byref(st)), self._p)
         return used.value, rc, st.as_dict()
 
+    def autotune(self):
+        """Picks launch grids by timing (cup_autotune): ({kernel: grid}, {kernel: ms})."""
+        ch = (C.c_int32 * 4)()
+        ms = (C.c_float * 4)()
+        check(lib().cup_autotune(self._p, ch, ms), self._p)
+        names = ("advect", "pressure_rhs", "grad_update", "solver")
+        return dict(zip(names, list(ch))), dict(zip(names, list(ms)))
+
     # ---- profiling ----------------------------------------------------------
     def profile(self, enable=True):
         check(lib().cup_profile(self._p, int(enable)), self._p)

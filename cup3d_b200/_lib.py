@@ -107,6 +107,7 @@ SIGNATURES = {
     "cup_batch_case_blocks": (C.c_int, [_P, C.c_int32, _I, _I]),
     "cup_batch_poisson_solve_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.POINTER(cup_solve_stats)]),
     "cup_batch_step": (C.c_int, [_P, C.c_int32, _D, _D, _D, C.POINTER(cup_solve_stats)]),
+    "cup_autotune": (C.c_int, [_P, _I, C.POINTER(C.c_float)]),
     "cup_obstacle_sphere": (C.c_int, [_P, _D, C.c_double, _D, _D]),
     "cup_obstacle_ellipsoid": (C.c_int, [_P, _D, _D, _D, _D, _D]),
     "cup_set_obstacle": (C.c_int, [_P, C.c_int32, _I, _D, _D, _D]),

@@ -251,7 +251,7 @@ static int batch_graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cud
     int v = vcur;
     for (int st = 0; st < 3; ++st) {
       if (int r = launch_advect_stage(c->dm, F.vel[v], F.vel[1 - v], F.tmpV, 0.0, c->cfg.nu, c->cfg.uinf,
-                                      c->cfg.advection, st, grid, s))
+                                      c->cfg.advection, st, kgrid(c, TG_ADVECT), s))
         return r;
       v = 1 - v;
     }
@@ -264,14 +264,14 @@ static int batch_graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cud
     double* pold = F.pres[pcur];
     double* pnew = F.pres[1 - pcur];
     if (int r = launch_pressure_rhs(c->dm, F.vel[v], pold, F.chi, ob, 0.0, step_arg, c->cfg.step_2nd_start, F.lhs,
-                                    F.phi, grid, s))
+                                    F.phi, kgrid(c, TG_RHS), s))
       return r;
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev0, s, cudaEventRecordExternal));
     if (int r = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, P, c->W, c->B, nullptr, s)) return r;
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev1, s, cudaEventRecordExternal));
     if (int r = launch_case_sums(c->dm, F.phi, T.bscratch, T.first, K, T.sums, grid, s)) return r;
     if (int r = launch_grad_update(c->dm, F.vel[v], F.phi, pold, pnew, nullptr, 0.0, step_arg,
-                                   c->cfg.step_2nd_start, grid, s))
+                                   c->cfg.step_2nd_start, kgrid(c, TG_GRAD), s))
       return r;
     CUP_CUDA_TRY(cudaMemcpyAsync(T.h_dt, T.dt, K * sizeof(double), cudaMemcpyDeviceToHost, s));
     CUP_CUDA_TRY(cudaMemcpyAsync(T.h_force, T.force, 6 * K * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -427,7 +427,7 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
   // kernels over all blocks, each block with its case's dt, kinematics and mean
   for (int st = 0; st < 3; ++st) {
     if (int rc = launch_advect_stage(c->dm, F.vel[F.vcur], F.vel[1 - F.vcur], F.tmpV, 0.0, c->cfg.nu, c->cfg.uinf,
-                                     c->cfg.advection, st, grid, c->stream))
+                                     c->cfg.advection, st, kgrid(c, TG_ADVECT), c->stream))
       return keep_err(c, rc);
     F.vcur = 1 - F.vcur;
   }
@@ -442,7 +442,7 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
   double* pold = F.pres[F.pcur];
   double* pnew = F.pres[1 - F.pcur];
   if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], pold, F.chi, ob, 0.0, step, c->cfg.step_2nd_start, F.lhs,
-                                   F.phi, grid, c->stream))
+                                   F.phi, kgrid(c, TG_RHS), c->stream))
     return keep_err(c, rc);
   std::vector<SolveStats> S(K);
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
@@ -451,7 +451,7 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   if (int rc = launch_case_sums(c->dm, F.phi, T.bscratch, T.first, K, T.sums, grid, c->stream)) return keep_err(c, rc);
   if (int rc = launch_grad_update(c->dm, F.vel[F.vcur], F.phi, pold, pnew, nullptr, 0.0, step,
-                                  c->cfg.step_2nd_start, grid, c->stream))
+                                  c->cfg.step_2nd_start, kgrid(c, TG_GRAD), c->stream))
     return keep_err(c, rc);
   F.pcur = 1 - F.pcur;
   if (force) CUP_CUDA_TRY(cudaMemcpyAsync(force, T.force, 6 * K * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -697,7 +697,7 @@ static int advect(cup_ctx* c, double dt) {
   Fields& F = c->F;
   for (int s = 0; s < 3; ++s) {
     if (int rc = launch_advect_stage(c->dm, F.vel[F.vcur], F.vel[1 - F.vcur], F.tmpV, dt, c->cfg.nu, c->cfg.uinf,
-                                     c->cfg.advection, s, grid_of(c), c->stream))
+                                     c->cfg.advection, s, kgrid(c, TG_ADVECT), c->stream))
       return keep(c, rc);
     F.vcur = 1 - F.vcur;
   }
@@ -715,14 +715,14 @@ static int project(cup_ctx* c, double dt, int step, cup_solve_stats* stats) {
   double* pold = F.pres[F.pcur];
   double* pnew = F.pres[1 - F.pcur];
   if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], pold, F.chi, ob_view(c), dt, step, c->cfg.step_2nd_start,
-                                   F.lhs, F.phi, grid_of(c), c->stream))
+                                   F.lhs, F.phi, kgrid(c, TG_RHS), c->stream))
     return keep(c, rc);
   cup_solve_stats st{};
   const int rs = solve_impl(c, F.lhs, F.phi, &st, false);
   if (rs < 0) return rs;
   if (int rc = launch_weighted_sum(c->dm, F.phi, c->d_scalars + SC_SUMS, c->W, c->stream)) return keep(c, rc);
   if (int rc = launch_grad_update(c->dm, F.vel[F.vcur], F.phi, pold, pnew, c->d_scalars + SC_SUMS, dt, step,
-                                  c->cfg.step_2nd_start, grid_of(c), c->stream))
+                                  c->cfg.step_2nd_start, kgrid(c, TG_GRAD), c->stream))
     return keep(c, rc);
   F.pcur = 1 - F.pcur;
   if (stats) *stats = st;
@@ -785,7 +785,7 @@ static int graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraph
     int v = vcur;
     for (int st = 0; st < 3; ++st) {
       if (int r = launch_advect_stage(dmg, F.vel[v], F.vel[1 - v], F.tmpV, 0.0, c->cfg.nu, c->cfg.uinf,
-                                      c->cfg.advection, st, grid, s))
+                                      c->cfg.advection, st, kgrid(c, TG_ADVECT), s))
         return r;
       v = 1 - v;
     }
@@ -797,7 +797,7 @@ static int graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraph
     double* pold = F.pres[pcur];
     double* pnew = F.pres[1 - pcur];
     if (int r = launch_pressure_rhs(dmg, F.vel[v], pold, F.chi, ob_view(c), 0.0, step_arg, c->cfg.step_2nd_start,
-                                    F.lhs, F.phi, grid, s))
+                                    F.lhs, F.phi, kgrid(c, TG_RHS), s))
       return r;
     // event record nodes (external): the solve's device time, read after replay
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev0, s, cudaEventRecordExternal));
@@ -806,7 +806,7 @@ static int graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraph
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev1, s, cudaEventRecordExternal));
     if (int r = launch_weighted_sum(c->dm, F.phi, c->d_scalars + SC_SUMS, c->W, s)) return r;
     if (int r = launch_grad_update(dmg, F.vel[v], F.phi, pold, pnew, c->d_scalars + SC_SUMS, 0.0, step_arg,
-                                   c->cfg.step_2nd_start, grid, s))
+                                   c->cfg.step_2nd_start, kgrid(c, TG_GRAD), s))
       return r;
     CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->dt, c->d_scalars + SC_GDT, sizeof(double), cudaMemcpyDeviceToHost, s));
     CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->st, c->W.st, sizeof(KrylovState), cudaMemcpyDeviceToHost, s));
@@ -952,7 +952,7 @@ int cup_pressure_rhs(cup_ctx* c, double dt, int32_t step) {
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_pressure_rhs: not available on a batch of cases");
   Fields& F = c->F;
   if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], F.pres[F.pcur], F.chi, ob_view(c), dt, step,
-                                   c->cfg.step_2nd_start, F.lhs, F.phi, grid_of(c), c->stream))
+                                   c->cfg.step_2nd_start, F.lhs, F.phi, kgrid(c, TG_RHS), c->stream))
     return keep(c, rc);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_rhs", __FILE__, __LINE__));

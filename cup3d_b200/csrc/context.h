@@ -124,6 +124,8 @@ struct cup_ctx {
   std::vector<cup3d::Mesh> case_mesh;  // each case's own mesh
   cup3d::BatchWork B{};
   cup3d::BatchStep T{};
+  // launch grids of the stencil kernels chosen by cup_autotune (0: W.grid)
+  int tgrid[3] = {0, 0, 0};
   // captured time steps, by (velocity buffer, pressure buffer, p_old term)
   cudaGraphExec_t gexec[8] = {};
   cup3d::GraphIO* gio = nullptr;      // pinned
@@ -131,6 +133,9 @@ struct cup_ctx {
 };
 
 namespace cup3d {
+enum : int { TG_ADVECT = 0, TG_RHS = 1, TG_GRAD = 2 };
+// Launch grid of stencil kernel k (TG_*): the tuned one, else the default.
+inline int kgrid(const cup_ctx* c, int k) { return c->tgrid[k] > 0 ? c->tgrid[k] : c->W.grid; }
 // Binds the context's profiler to this thread for the duration of an API call.
 struct ProfBind {
   Profiler* prev;

@@ -812,7 +812,7 @@ constexpr int KB_CACHE = 4;
 // Block groups per CTA of the persistent solver, two CTAs per SM.  (One
 // 512-thread CTA per SM halves the CTAs in every grid barrier but measured
 // 6% slower per iteration on the sphere mesh.)
-constexpr int PGROUPS = 4;
+constexpr int PGROUPS = PERSISTENT_GROUPS_PER_CTA;
 constexpr int PNT = PGROUPS * GROUP;
 
 __device__ __forceinline__ const BlockInfo& persistent_block(const DevMesh& M, const BlockInfo* cache, int ncache,
@@ -1605,6 +1605,14 @@ static int persistent_grid(int nb, const PoissonWork& W, int* grid) {
   CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) return set_error(CUP_ERR_CUDA, "persistent BiCGSTAB: kernel does not fit on an SM");
   *grid = std::max(1, std::min({per_sm * sms, (nb + PGROUPS - 1) / PGROUPS, std::max(W.grid, W.ggrid) / 2}));
+  return 0;
+}
+
+int persistent_grid_max(int nb, const PoissonWork& W, int* grid) {
+  int g1 = 0, g2 = 0;
+  if (int rc = persistent_grid<double>(nb, W, &g1)) return rc;
+  if (int rc = persistent_grid<float>(nb, W, &g2)) return rc;
+  *grid = std::min(g1, g2);
   return 0;
 }
 

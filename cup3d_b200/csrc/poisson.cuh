@@ -35,6 +35,8 @@ enum SolveStatus : int {
 // The operator and preconditioner kernels give each mesh block a 64-thread
 // group, four groups per 256-thread CTA.
 constexpr int GROUPS_PER_CTA = 4;
+// Block groups per CTA of the persistent solvers.
+constexpr int PERSISTENT_GROUPS_PER_CTA = 4;
 
 struct PoissonWork {
   // vectors, nb*512 each
@@ -114,6 +116,8 @@ void poisson_init_constants();
 // Number of 64-thread groups of the persistent solver on a mesh of nb blocks
 // (the visit order is balanced for this many groups).
 int persistent_solver_groups(int nb, PoissonWork& W, int* groups);
+// Largest co-resident grid of the persistent solver for nb blocks.
+int persistent_grid_max(int nb, const PoissonWork& W, int* grid);
 // Programmatic dependent launch of the solver kernels on this thread (on by
 // default; off while capturing a CUDA graph).
 void solver_pdl(bool on);

@@ -179,6 +179,19 @@ int cup_batch_poisson_solve_dev(cup_ctx* batch, const double* d_b, double* d_x, 
 int cup_batch_step(cup_ctx* batch, int32_t step, const double* dt_in, double* dt_used, double* force,
                    cup_solve_stats* stats);
 
+/* ---- launch-shape tuning (no reference counterpart) ---- */
+/* Times candidate launch shapes on the context's own mesh and fields and
+ * keeps the fastest: the grids of the advection, pressure-RHS and gradient
+ * kernels (multiples of the SM count) and the CTA count of the persistent
+ * solver (one to two per SM; a plain context only), which sets how many
+ * blocks each block group takes per phase.  choice[4] = the chosen grids
+ * (advection, RHS, gradient, solver); best_ms[4] (may be NULL) = their times
+ * (per launch; per iteration for the solver).  Overwrites the scratch fields
+ * (CUP_FIELD_LHS, CUP_FIELD_TMPV and the buffers a step writes next); call it
+ * between steps.  Results do not depend on the grids except for the solver's
+ * summation order. */
+int cup_autotune(cup_ctx* ctx, int32_t* choice, float* best_ms);
+
 /* ---- obstacles (host-side CreateObstacles; one body per context) ---- */
 /* Sphere of radius r at c (Sphere.cpp); chi by ObstaclesCreate.cpp:18-121;
  * kin = velocity[3], angular velocity[3] (may be NULL).  Also sets CUP_FIELD_CHI. */

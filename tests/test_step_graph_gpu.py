@@ -52,3 +52,26 @@ def test_captured_steps_follow_new_solver_settings():
     _, _, st_p = p.step(1)
     assert st_g["iterations"] == st_p["iterations"] > 10
     assert np.array_equal(g.download("vel"), p.download("vel"))
+
+
+def test_autotune_changes_only_the_launch_shape():
+    # cup_autotune times launch grids on the context's own fields; the chosen
+    # grids leave the stencils' results unchanged and the solver's up to its
+    # summation order: two steps of a tuned and an untuned context agree to
+    # within what a solve to 1e-11 allows
+    extra = "-nu 0.001 -CFL 0.3 -rampup 0 -poissonTol 0 -poissonTolRel 1e-11"
+    a, b = (make_ctx("amr3_periodic", device=0, extra=extra) for _ in range(2))
+    for c in (a, b):
+        xyz, _ = c.cell_centres()
+        x, y, z = (2 * np.pi * t for t in xyz.T)
+        c.upload("vel", np.concatenate([np.sin(x) * np.cos(y), np.cos(z) * np.sin(x), 0.3 * np.sin(y)]))
+    choice, ms = a.autotune()
+    sms = 148
+    assert all(choice[k] >= 1 for k in choice), choice
+    assert all(ms[k] > 0 for k in ("advect", "pressure_rhs", "grad_update", "solver")), ms
+    for step in range(2):
+        dta, _, sta = a.step(step)
+        dtb, _, stb = b.step(step)
+        assert abs(dta - dtb) <= 1e-12 * dtb
+        ua, ub = a.download("vel"), b.download("vel")
+        assert np.abs(ua - ub).max() <= 1e-9 * np.abs(ub).max(), step
