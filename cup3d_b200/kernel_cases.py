@@ -3,9 +3,12 @@
     python -m cup3d_b200.kernel_cases spmv    # one Poisson operator application (sphere mesh)
     python -m cup3d_b200.kernel_cases solve   # 16 BiCGSTAB iterations (sphere mesh, seeded RHS)
     python -m cup3d_b200.kernel_cases step    # 4 full time steps of the sphere workload
+    python -m cup3d_b200.kernel_cases swarm   # 16 iterations of a batched solve over 8 swarm cases
 
-Each case builds the sphere mesh of cup3d_b200.workloads (2340 blocks,
-1.198M cells, ~0.3 GB of device memory) and exits 0 on success.
+The sphere cases build the sphere mesh of cup3d_b200.workloads (2340
+blocks, 1.198M cells, ~0.3 GB of device memory); the swarm case batches the
+first 8 ellipsoid-swarm cases (10,879 blocks, 5.6M cells, ~2.5 GB).  Each exits
+0 on success.
 """
 from __future__ import annotations
 
@@ -17,8 +20,18 @@ import numpy as np
 def main(argv):
     import torch
 
-    from cup3d_b200.workloads import make_sphere_ctx, poisson_rhs
+    from cup3d_b200.workloads import make_sphere_ctx, make_swarm_ctx, poisson_rhs, swarm_rhs
     case = argv[1] if len(argv) > 1 else "solve"
+    if case == "swarm":
+        import cup3d_b200 as cup
+        cases = [make_swarm_ctx(i, 0) for i in range(8)]
+        b = torch.tensor(np.concatenate([swarm_rhs(c, i) for i, c in enumerate(cases)]), device="cuda")
+        batch = cup.Batch(cases)
+        batch.set_poisson("b200", 0.0, 1e-30, 16)
+        x = torch.zeros_like(b)
+        rc, st = batch.poisson_solve_dev(b, x)
+        print(f"swarm ok: rc {rc}, {batch.nb} blocks, iterations {[s['iterations'] for s in st]}")
+        return
     ctx = make_sphere_ctx(0)
     n = ctx.nb * 512
     if case == "spmv":
