@@ -44,15 +44,16 @@ struct BlockInfo {
   int pad_;
 };
 
-// Shared tile of one block for the operator: the block, its x/y face halos,
-// the face layers of coarser neighbours and the coarse-fine fluxes of x/y
-// faces (face-local index tan1 + 8 tan2 in every per-face array), and the
-// block's table entries.  The transforms' FdTile aliases the leading member.
+// Shared tile of one block for the operator: the block with its x/y ghost
+// layers in one padded array (v[z][y+1][x+1] holds cell (x, y, z); x = -1, 8
+// and y = -1, 8 hold the ghosts, so every neighbour is a fixed offset), the
+// face layers of coarser neighbours and the coarse-fine fluxes of x/y faces
+// (face-local index tan1 + 8 tan2 in every per-face array), and the block's
+// table entries.  The transforms' FdTile aliases the leading member.
 struct GroupTile {
-  double v[BS][BS][BS + 1];  // [z][y][x]
-  double hal[4][BS * BS];    // -x, +x, -y, +y same-level neighbour layers
-  double cl[6][BS * BS];     // per coarser face: the coarse block's layer on that face
-  double flx[4][BS * BS];    // x/y coarse-fine face fluxes
+  double v[BS][BS + 2][BS + 2];  // [z][y+1][x+1]
+  double cl[6][BS * BS];         // per coarser face: the coarse block's layer on that face
+  double flx[4][BS * BS];        // x/y coarse-fine face fluxes
   BlockInfo bi;
 };
 

@@ -133,7 +133,7 @@ template <class X>
 __device__ __forceinline__ double cf_flux(const BlockInfo& bi, const X& x, const GroupTile& tile, int f, int kind,
                                           int a, int bb) {
   const int d = f >> 1, s = f & 1;
-  auto own = [&](int cell) { return tile.v[cell >> 6][(cell >> 3) & 7][cell & 7]; };
+  auto own = [&](int cell) { return tile.v[cell >> 6][((cell >> 3) & 7) + 1][(cell & 7) + 1]; };
   const double h = bi.h;
   if (kind == K_COARSER) {
     const double* cl = tile.cl[f];
@@ -191,20 +191,27 @@ __device__ __forceinline__ void spmv_group(const BlockInfo& bi, const X& x, cons
   double zm = col[0], zp = col[7];
   if (kind[4] == K_SAME) zm = x(size_t(fn[16]) * BN + 7 * 64 + cxy);
   if (kind[5] == K_SAME) zp = x(size_t(fn[20]) * BN + cxy);
-  // x / y face halos and coarser faces' coarse layers: the thread loads
-  // face-local cell (gx, gy) of each
+  // x / y ghost layers and coarser faces' coarse layers: the thread loads
+  // face-local cell (gx, gy) of each.  The ghost of a same-level face is the
+  // neighbour's face cell; on any other face it is the block's own face cell
+  // (zero flux; coarse-fine faces get their flux below).
   bool cf = false;
 #pragma unroll
   for (int f = 0; f < 6; ++f) {
     const int d = f >> 1, s = f & 1;
-    if (f < 4 && kind[f] == K_SAME)
-      tile.hal[f][G.lane] = x(size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy));
+    if (f < 4) {
+      const size_t src = kind[f] == K_SAME ? size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy)
+                                           : size_t(bi.id) * BN + face_cell(d, s, 0, G.gx, G.gy);
+      // face-local (a, b) = (gx, gy): (y, z) on x faces, (x, z) on y faces
+      double* ghost = d == 0 ? &tile.v[G.gy][G.gx + 1][s ? BS + 1 : 0] : &tile.v[G.gy][s ? BS + 1 : 0][G.gx + 1];
+      *ghost = x(src);
+    }
     if (kind[f] == K_COARSER)
       tile.cl[f][G.lane] = x(size_t(fn[4 * f]) * BN + face_cell(d, 1 - s, 0, G.gx, G.gy));
     cf |= kind[f] >= K_COARSER;
   }
 #pragma unroll
-  for (int z = 0; z < 8; ++z) tile.v[z][G.gy][G.gx] = col[z];
+  for (int z = 0; z < 8; ++z) tile.v[z][G.gy + 1][G.gx + 1] = col[z];
   group_sync(G.g);
   double zf0 = 0.0, zf1 = 0.0;  // z-face fluxes of the own column (cells z = 0, 7)
   if (cf) {                      // uniform per block
@@ -223,23 +230,13 @@ __device__ __forceinline__ void spmv_group(const BlockInfo& bi, const X& x, cons
     group_sync(G.g);
   }
   const double h = bi.h;
-  // x/y neighbours: in the tile, or in the halo on the block's faces (one
-  // shared load per neighbour through a selected base and z stride)
-  constexpr int ZS = BS * (BS + 1);
-  const double* pxm = G.gx > 0 ? &tile.v[0][G.gy][G.gx - 1] : &tile.hal[0][G.gy];
-  const double* pxp = G.gx < 7 ? &tile.v[0][G.gy][G.gx + 1] : &tile.hal[1][G.gy];
-  const double* pym = G.gy > 0 ? &tile.v[0][G.gy - 1][G.gx] : &tile.hal[2][G.gx];
-  const double* pyp = G.gy < 7 ? &tile.v[0][G.gy + 1][G.gx] : &tile.hal[3][G.gx];
-  const int sxm = G.gx > 0 ? ZS : BS, sxp = G.gx < 7 ? ZS : BS;
-  const int sym = G.gy > 0 ? ZS : BS, syp = G.gy < 7 ? ZS : BS;
-  // on a face that is not same-level the ghost is the cell itself (zero
-  // flux; coarse-fine faces get their flux below): the thread's own column
-  const bool oxm = G.gx == 0 && kind[0] != K_SAME, oxp = G.gx == 7 && kind[1] != K_SAME;
-  const bool oym = G.gy == 0 && kind[2] != K_SAME, oyp = G.gy == 7 && kind[3] != K_SAME;
+  // x/y neighbours: fixed offsets from the own cell in the padded tile
+  constexpr int RS = BS + 2, ZS = RS * RS;
+  const double* own_cell = &tile.v[0][G.gy + 1][G.gx + 1];
 #pragma unroll
   for (int z = 0; z < 8; ++z) {
-    const double xm = oxm ? col[z] : pxm[z * sxm], xp = oxp ? col[z] : pxp[z * sxp];
-    const double ym = oym ? col[z] : pym[z * sym], yp = oyp ? col[z] : pyp[z * syp];
+    const double xm = own_cell[z * ZS - 1], xp = own_cell[z * ZS + 1];
+    const double ym = own_cell[z * ZS - RS], yp = own_cell[z * ZS + RS];
     const double zmv = z > 0 ? col[z - 1] : zm;
     const double zpv = z < 7 ? col[z + 1] : zp;
     y[z] = h * (xm + xp + ym + yp + zmv + zpv - 6.0 * col[z]);
@@ -862,11 +859,9 @@ __device__ __forceinline__ void p1_block(const KArgs<T>& A, const GroupIdx& G, G
   const double h = bi.h;
   double col[8], y[8], rh[8];
   {
-    double zr[8], q[8];
-    load_col(A.z1, b, G, zr);
-    load_col(A.p, b, G, q);
+    const size_t o = size_t(b) * BN + G.gy * 8 + G.gx;
 #pragma unroll
-    for (int z = 0; z < 8; ++z) col[z] = zr[z] + beta * q[z];
+    for (int z = 0; z < 8; ++z) col[z] = z1(o + z * 64);  // the accessor the ghosts use: the same values
   }
   spmv_group(bi, z1, col, ms, A.mean_mode, tile, G, y);
   if (restart) {
@@ -900,11 +895,9 @@ __device__ __forceinline__ void p2_block(const KArgs<T>& A, const GroupIdx& G, G
   const int b = bi.id;
   double col[8], y[8];
   {
-    double zr[8], zv[8];
-    load_col(A.z1, b, G, zr);
-    load_col(A.z2, b, G, zv);
+    const size_t o = size_t(b) * BN + G.gy * 8 + G.gx;
 #pragma unroll
-    for (int z = 0; z < 8; ++z) col[z] = zr[z] - alpha * zv[z];
+    for (int z = 0; z < 8; ++z) col[z] = z2(o + z * 64);  // the accessor the ghosts use: the same values
   }
   spmv_group(bi, z2, col, ms, A.mean_mode, tile, G, y);
   double r[8], nu[8];
