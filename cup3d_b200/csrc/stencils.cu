@@ -130,13 +130,17 @@ __global__ void __launch_bounds__(NT, 3)
         __syncthreads();
       }
     }
+    // the cell and component loops stay rolled: the unrolled body (18 WENO
+    // reconstructions per cell) overflowed the instruction cache (the top
+    // stall was no_instruction); rolled, a stage takes 188 us instead of 204
+#pragma unroll 1
     for (int qq = 0; qq < 2; ++qq) {
       const int cell = threadIdx.x + qq * NT;
       const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
       auto L = [&](int c, int xx, int yy, int zz) { return lab[c * LG::V + LG::at(xx, yy, zz)]; };
       const double uA[3] = {L(0, x, y, z) + ui.v[0], L(1, x, y, z) + ui.v[1], L(2, x, y, z) + ui.v[2]};
       double out[3];
-#pragma unroll
+#pragma unroll 1
       for (int c = 0; c < 3; ++c) {
         const double dx = deriv<SCHEME>(uA[0], L(c, x - 3, y, z), L(c, x - 2, y, z), L(c, x - 1, y, z), L(c, x, y, z),
                                         L(c, x + 1, y, z), L(c, x + 2, y, z), L(c, x + 3, y, z));
