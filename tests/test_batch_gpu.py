@@ -192,3 +192,22 @@ def test_captured_batch_steps_match_launched_batch_steps():
         assert [s["iterations"] for s in st1] == [s["iterations"] for s in st0], step
         assert np.array_equal(batches[0].download("vel"), batches[1].download("vel")), step
         assert np.array_equal(batches[0].download("pres"), batches[1].download("pres")), step
+
+
+def test_batch_with_a_single_block_case():
+    # a one-block periodic case (every face its own neighbour) next to an AMR
+    # case: both solved in the same launch, each to the oracle's standard
+    one = cup.Context(cup.config("-bpdx 1 -bpdy 1 -bpdz 1 -levelMax 1 -extent 1 -BC_x periodic -BC_y periodic "
+                                 "-BC_z periodic " + FLAGS, device=0))
+    one.set_mesh_uniform()
+    amr = make_ctx("amr2_free", device=0, extra=FLAGS)
+    meshes = [oracle_mesh(one), oracle_mesh(amr)]
+    bs = [compatible_rhs(m, 60 + k) for k, m in enumerate(meshes)]
+    batch = cup.Batch([one, amr])
+    bd, xd = torch_dev(np.concatenate(bs)), torch_dev(np.zeros(sum(m.n for m in meshes)))
+    rc, stats = batch.poisson_solve_dev(bd, xd)
+    assert rc == 0
+    for m, b, x, st in zip(meshes, bs, split(batch, xd.cpu().numpy()), stats):
+        x_ref, _ = m.bicgstab_gpu(b, tol=0.0, tol_rel=1e-10)
+        assert st["status"] == 1
+        assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)

@@ -143,3 +143,17 @@ def test_nan_rhs_is_a_hard_error():
     bd, xd = torch_dev(b), torch_dev(np.zeros(m.n))
     with pytest.raises(cup.CupError):
         ctx.poisson_solve_dev(bd, xd)
+
+
+def test_single_block_solve_matches_oracle():
+    # one periodic block: every face is the block's own neighbour, one CTA
+    ctx = cup.Context(cup.config("-bpdx 1 -bpdy 1 -bpdz 1 -levelMax 1 -extent 1 -BC_x periodic -BC_y periodic "
+                                 "-BC_z periodic -poissonTol 0 -poissonTolRel 1e-10", device=0))
+    ctx.set_mesh_uniform()
+    m = oracle_mesh(ctx)
+    b = _compatible_rhs(m, 13)
+    x_ref, st_ref = m.bicgstab_gpu(b, tol=0.0, tol_rel=1e-10)
+    bd, xd = torch_dev(b), torch_dev(np.zeros(m.n))
+    rc, st = ctx.poisson_solve_dev(bd, xd)
+    assert rc == 0 and st["status"] == 1
+    assert np.linalg.norm(xd.cpu().numpy() - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
