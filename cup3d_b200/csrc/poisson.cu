@@ -825,6 +825,46 @@ __device__ __forceinline__ const BlockInfo& persistent_block(const DevMesh& M, c
   for (int k_ = 0, slot_ = blockIdx.x * PGROUPS + G.g; slot_ < M.nb; ++k_, slot_ += gridDim.x * PGROUPS) \
     if (const BlockInfo& bi = persistent_block(M, cache, A.ncache, tile, k_, slot_, G); true)
 
+// PREP: x0 = 0 on the (case's) mean row (modes 1 and 3); sum(x0 h^3)
+template <class T>
+__device__ __forceinline__ double prep_block(const KArgs<T>& A, const GroupIdx& G, const BlockInfo& bi) {
+  const int b = bi.id;
+  double c[8];
+  load_col(A.xs0, b, G, c);
+  if (A.zero_mean_row && bi.mean && G.lane == 0) {
+    A.xs0[size_t(b) * BN] = T(0);
+    c[0] = 0.0;
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) s += c[z];
+  return s * bi.h * bi.h * bi.h;
+}
+
+// INIT: r = b - A x0 (b = 0 on the mean row for modes 1 and 3), rhat = r,
+// p = 0; (r, r)
+template <class T>
+__device__ __forceinline__ double init_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
+                                             const BlockInfo& bi, double ms) {
+  const int b = bi.id;
+  double col[8], y[8], bc[8];
+  load_col(A.xs0, b, G, col);
+  spmv_group(bi, VecAt<T>{A.xs0}, col, ms, A.mean_mode, tile, G, y);
+  load_col(A.b, b, G, bc);
+  if (A.zero_mean_row && bi.mean && G.lane == 0) bc[0] = 0.0;
+  double r[8], zero[8], acc = 0.0;
+#pragma unroll
+  for (int z = 0; z < 8; ++z) {
+    r[z] = bc[z] - y[z];  // stored as T; (r, r) from the unrounded values, as k_bicg_init
+    zero[z] = 0.0;
+    acc += r[z] * r[z];
+  }
+  store_col(A.r, b, G, r);
+  store_col(A.rhat, b, G, r);
+  store_col(A.p, b, G, zero);
+  return acc;
+}
+
 // Phase bodies for one block (bi) of a group; the persistent solvers loop
 // them over the group's blocks.
 // P0 (once): zr = M^-1 r for the initial residual; sum(zr h^3)
@@ -1000,11 +1040,27 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
   }
   __syncthreads();
   bool ok = true;
-  if (!S.done) {
+  // PREP and INIT: x0's mean row and sum(x0 h^3); r = b - A x0, rhat = r,
+  // p = 0 and the scalars of iteration 0
+  {
+    double a[1] = {0.0};
+    PERSISTENT_BLOCKS(bi) a[0] += prep_block<T>(A, G, bi);
+    ok = grid_allreduce<1>(a, Gs, epoch, red);
+    if (threadIdx.x == 0) S.mean_sum = a[0];
+    __syncthreads();
+  }
+  if (ok) {
+    double a[1] = {0.0};
+    PERSISTENT_BLOCKS(bi) a[0] += init_block<T>(A, G, tile, bi, S.mean_sum);
+    ok = grid_allreduce<1>(a, Gs, epoch, red);
+    if (threadIdx.x == 0) fin_init(S, a[0]);
+    __syncthreads();
+  }
+  if (ok && !S.done) {
     double a[1] = {0.0};
     PERSISTENT_BLOCKS(bi) a[0] += p0_block<T>(A, G, tile, bi, inv_eig);
     ok = grid_allreduce<1>(a, Gs, epoch, red);
-    // q = 0 at the start (p of k_bicg_init), so z1 = zr
+    // q = 0 at the start (init_block), so z1 = zr
     if (threadIdx.x == 0) ms_zr = S.mean_sum = a[0];
     __syncthreads();
   }
@@ -1231,46 +1287,6 @@ __device__ __forceinline__ void batch_fill_cache(const DevMesh& M, const BatchAr
 
 #define BATCH_BLOCKS(bi) \
   for (int k_ = 0; k_ < P.nblk; ++k_) if (const BlockInfo& bi = batch_block(M, B, cache, tile, P, k_, G); true)
-
-// PREP: x0 = 0 on the case's mean row (modes 1 and 3); sum(x0 h^3)
-template <class T>
-__device__ __forceinline__ double prep_block(const KArgs<T>& A, const GroupIdx& G, const BlockInfo& bi) {
-  const int b = bi.id;
-  double c[8];
-  load_col(A.xs0, b, G, c);
-  if (A.zero_mean_row && bi.mean && G.lane == 0) {
-    A.xs0[size_t(b) * BN] = T(0);
-    c[0] = 0.0;
-  }
-  double s = 0.0;
-#pragma unroll
-  for (int z = 0; z < 8; ++z) s += c[z];
-  return s * bi.h * bi.h * bi.h;
-}
-
-// INIT: r = b - A x0 (b = 0 on the mean row for modes 1 and 3), rhat = r,
-// p = 0; (r, r)
-template <class T>
-__device__ __forceinline__ double init_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
-                                             const BlockInfo& bi, double ms) {
-  const int b = bi.id;
-  double col[8], y[8], bc[8];
-  load_col(A.xs0, b, G, col);
-  spmv_group(bi, VecAt<T>{A.xs0}, col, ms, A.mean_mode, tile, G, y);
-  load_col(A.b, b, G, bc);
-  if (A.zero_mean_row && bi.mean && G.lane == 0) bc[0] = 0.0;
-  double r[8], zero[8], acc = 0.0;
-#pragma unroll
-  for (int z = 0; z < 8; ++z) {
-    r[z] = double(T(bc[z] - y[z]));
-    zero[z] = 0.0;
-    acc += r[z] * r[z];
-  }
-  store_col(A.r, b, G, r);
-  store_col(A.rhat, b, G, r);
-  store_col(A.p, b, G, zero);
-  return acc;
-}
 
 template <class T>
 __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, GridSync Gs, BatchArgs B) {
@@ -1729,8 +1745,10 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   A.ext_precond = cnn ? 1 : 0;
   A.ncache = std::max(0, std::min(P.block_cache, KB_CACHE));
   GridReduce gc{W.partial, W.counters + 14};
-  { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_prepare<T>, W.grid, s, A)); }
-  { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_init<T>, W.ggrid, s, A)); }
+  if (!persistent) {  // the persistent kernel prepares and initialises itself
+    { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_prepare<T>, W.grid, s, A)); }
+    { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_init<T>, W.ggrid, s, A)); }
+  }
   CUP_CUDA_TRY(cudaGetLastError());
   if (persistent) {
     if (int rc = launch_persistent<T>(A, W, s, f32 ? "bicg32_persistent" : "bicg_persistent")) return rc;
