@@ -168,13 +168,17 @@ class Context:
         return rc, st.as_dict()
 
     # ---- obstacles ----------------------------------------------------------
-    def obstacle_sphere(self, center, radius, vel=(0, 0, 0), omega=(0, 0, 0)):
+    def obstacle_sphere(self, center, radius, vel=(0, 0, 0), omega=(0, 0, 0), on_device=False):
+        """Sphere body; on_device: created by kernels (cup_obstacle_sphere_dev)."""
         c, v, o = (np.ascontiguousarray(a, dtype=np.float64) for a in (center, vel, omega))
-        check(lib().cup_obstacle_sphere(self._p, dptr(c), radius, dptr(v), dptr(o)), self._p)
+        fn = lib().cup_obstacle_sphere_dev if on_device else lib().cup_obstacle_sphere
+        check(fn(self._p, dptr(c), radius, dptr(v), dptr(o)), self._p)
 
-    def obstacle_ellipsoid(self, center, axes, quat, vel=(0, 0, 0), omega=(0, 0, 0)):
+    def obstacle_ellipsoid(self, center, axes, quat, vel=(0, 0, 0), omega=(0, 0, 0), on_device=False):
+        """Ellipsoid body; on_device: created by kernels (cup_obstacle_ellipsoid_dev)."""
         c, a, q, v, o = (np.ascontiguousarray(x, dtype=np.float64) for x in (center, axes, quat, vel, omega))
-        check(lib().cup_obstacle_ellipsoid(self._p, dptr(c), dptr(a), dptr(q), dptr(v), dptr(o)), self._p)
+        fn = lib().cup_obstacle_ellipsoid_dev if on_device else lib().cup_obstacle_ellipsoid
+        check(fn(self._p, dptr(c), dptr(a), dptr(q), dptr(v), dptr(o)), self._p)
 
     def set_obstacle(self, blocks, chi, udef, kin):
         blocks = np.ascontiguousarray(blocks, np.int32)

@@ -110,6 +110,8 @@ SIGNATURES = {
     "cup_autotune": (C.c_int, [_P, _I, C.POINTER(C.c_float)]),
     "cup_obstacle_sphere": (C.c_int, [_P, _D, C.c_double, _D, _D]),
     "cup_obstacle_ellipsoid": (C.c_int, [_P, _D, _D, _D, _D, _D]),
+    "cup_obstacle_sphere_dev": (C.c_int, [_P, _D, C.c_double, _D, _D]),
+    "cup_obstacle_ellipsoid_dev": (C.c_int, [_P, _D, _D, _D, _D, _D]),
     "cup_set_obstacle": (C.c_int, [_P, C.c_int32, _I, _D, _D, _D]),
     "cup_get_obstacle": (C.c_int, [_P, _I, _D, _D, _D]),
     "cup_max_u": (C.c_int, [_P, _D]),

@@ -26,6 +26,9 @@ NVFLAGS = ARCH + [
     "-Xcompiler", "-Wall", "-I", str(ROOT / "include"),
 ]
 HOSTCXX = "g++"
+# Per-file flags: device obstacle creation repeats the host code's arithmetic
+# bit for bit, so it is compiled without fused multiply-adds.
+FILE_FLAGS = {"obstacles_dev.cu": ["--fmad=false"]}
 
 
 def _sources():
@@ -43,7 +46,7 @@ def _compile(src: Path, digest: str, verbose: bool) -> Path:
     obj = BUILD / f"{src.stem}.{src.suffix[1:]}.{digest}.o"
     if obj.exists() and obj.stat().st_mtime >= src.stat().st_mtime:
         return obj
-    cmd = [NVCC, "-ccbin", HOSTCXX] + NVFLAGS + ["-c", str(src), "-o", str(obj)]
+    cmd = [NVCC, "-ccbin", HOSTCXX] + NVFLAGS + FILE_FLAGS.get(src.name, []) + ["-c", str(src), "-o", str(obj)]
     if src.suffix == ".cpp":
         cmd = [NVCC, "-ccbin", HOSTCXX, "-x", "cu"] + NVFLAGS + ["-c", str(src), "-o", str(obj)]
     if verbose:

@@ -132,6 +132,7 @@ static int batch_step_setup(cup_ctx* c, const std::vector<const cup_ctx*>& cases
   std::vector<int> blocks, slot_first(K + 1, 0);
   std::vector<double> chi, udef, kin(9 * size_t(K), 0.0);
   for (int k = 0; k < K; ++k) {
+    if (int rc = ctx_obstacle_host_copies(const_cast<cup_ctx*>(cases[k]))) return rc;
     const DevObstacle& o = cases[k]->ob;
     slot_first[k + 1] = slot_first[k] + o.nslots;
     for (int sl = 0; sl < o.nslots; ++sl) blocks.push_back(o.h_blocks[sl] + c->case_first[k]);

@@ -893,8 +893,11 @@ int cup_set_obstacle(cup_ctx* c, int32_t nslots, const int32_t* blocks, const do
   return ctx_upload_obstacle(c, nslots, blocks, chi, udef, kin);
 }
 
-int cup_get_obstacle(const cup_ctx* c, int32_t* blocks, double* chi, double* udef, double* kin) {
-  if (!c) return ctx_fail(nullptr, CUP_ERR_ARG, "null ctx");
+int cup_get_obstacle(const cup_ctx* cc, int32_t* blocks, double* chi, double* udef, double* kin) {
+  if (!cc) return ctx_fail(nullptr, CUP_ERR_ARG, "null ctx");
+  cup_ctx* c = const_cast<cup_ctx*>(cc);  // a device-created body fetches its host copies here
+  if ((blocks || chi || udef) && !c->host_only)
+    if (int rc = ctx_obstacle_host_copies(c)) return keep(c, rc);
   const DevObstacle& o = c->ob;
   if (blocks) std::copy(o.h_blocks.begin(), o.h_blocks.end(), blocks);
   if (chi) std::copy(o.h_chi.begin(), o.h_chi.end(), chi);

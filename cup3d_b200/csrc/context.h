@@ -43,6 +43,13 @@ struct DevObstacle {
   double kin[9] = {0};            // CM[3], vel[3], omega[3]
   std::vector<int> h_blocks;      // host copies for cup_get_obstacle
   std::vector<double> h_chi, h_udef;
+  // created on the device (cup_obstacle_*_dev): buffers sized for every block
+  // of the mesh, the host copies fetched when read
+  int dev_cap = 0;
+  bool host_stale = false;
+  double* d_mom = nullptr;        // 4 per slot: sum chi h^3 (x, y, z), sum chi h^3
+  double* d_origin = nullptr;     // 3 nb block origins
+  void* d_result = nullptr;       // slot count, mass, kinematics
 };
 
 // Learned preconditioner state: weights, Adam moments, training scratch and
@@ -149,6 +156,8 @@ int ctx_alloc_fields(cup_ctx* c);
 // Installs an obstacle (nslots blocks with chi, udef and kinematics kin[9]).
 int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
                         const double* kin);
+// Fetches the host copies of a device-created obstacle (no-op otherwise).
+int ctx_obstacle_host_copies(cup_ctx* c);
 // Drops the captured time steps (after any change of mesh, obstacle or
 // solver settings).
 void graph_reset(cup_ctx* c);

@@ -96,16 +96,22 @@ void make_sphere(const Mesh& m, const double c[3], double r, const double vel[3]
     const double dx = x - c[0], dy = y - c[1], dz = z - c[2];
     return r - std::sqrt(dx * dx + dy * dy + dz * dz);
   };
-  fill_from_sdf(m, sdf, box, 2.0 + 1.0, vel, omega, out);
+  fill_from_sdf(m, sdf, box, kObstacleSafety, vel, omega, out);
+}
+
+void quat_rotation(const double q[4], double R[3][3]) {
+  const double w = q[0], x = q[1], y = q[2], z = q[3];
+  const double M[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)},
+                          {2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)},
+                          {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) R[i][j] = M[i][j];
 }
 
 void make_ellipsoid(const Mesh& m, const double c[3], const double ax[3], const double q[4], const double vel[3],
                     const double omega[3], HostObstacle& out) {
-  // rotation matrix of the unit quaternion (w, x, y, z): body -> lab
-  const double w = q[0], x = q[1], y = q[2], z = q[3];
-  const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)},
-                          {2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)},
-                          {2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)}};
+  double R[3][3];
+  quat_rotation(q, R);
   const double rmax = std::max({ax[0], ax[1], ax[2]});
   const double box[3][2] = {{c[0] - rmax, c[0] + rmax}, {c[1] - rmax, c[1] + rmax}, {c[2] - rmax, c[2] + rmax}};
   // Level set f = 1 - |p/a| (normalised radius) divided by |grad| to first
@@ -126,7 +132,7 @@ void make_ellipsoid(const Mesh& m, const double c[3], const double ax[3], const 
     const double grad = std::sqrt(g) / rho;  // |grad rho|
     return (1.0 - rho) / grad;
   };
-  fill_from_sdf(m, sdf, box, 2.0 + 1.0, vel, omega, out);
+  fill_from_sdf(m, sdf, box, kObstacleSafety, vel, omega, out);
 }
 
 }  // namespace cup3d

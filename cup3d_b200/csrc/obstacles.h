@@ -23,6 +23,12 @@ struct HostObstacle {
 void make_sphere(const Mesh& m, const double c[3], double r, const double vel[3], const double omega[3],
                  HostObstacle& out);
 
+// Rotation matrix (body -> lab) of the unit quaternion q = (w, x, y, z).
+void quat_rotation(const double q[4], double R[3][3]);
+
+// Bounding-box margin of the fill rule: (2 + 1) times the coarsest spacing.
+constexpr double kObstacleSafety = 2.0 + 1.0;
+
 // Ellipsoid with semi-axes ax[3] rotated by quaternion q (w, x, y, z); the
 // signed distance is the ellipsoid's algebraic level set scaled to distance
 // units near the surface (see obstacles.cpp).

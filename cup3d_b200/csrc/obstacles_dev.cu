@@ -1,0 +1,361 @@
+// Obstacle creation on the device: the fill rule, signed distances and chi of
+// obstacles.cpp (Sphere.cpp:47-51, the ellipsoid level set, and the Towers
+// smoothed Heaviside of KernelCharacteristicFunction, ObstaclesCreate.cpp:45-80)
+// as kernels, for bodies that are re-created without a host round trip of
+// their blocks.
+//
+// This file is compiled without fused multiply-adds (--fmad=false) and states
+// every expression in the host code's order, so the slot list, chi and the
+// grid chi equal the host creation's bit for bit (IEEE division and square
+// root on both sides).  The chi moments (mass and centre of mass) are summed
+// per block in a fixed tree and then over the slots in slot order, so they
+// match the host's sequential sums to rounding.
+//
+// Kernels, one launch each:
+//   k_obst_slots  one CTA: bounding-box test per block, slots in block order
+//                 (a CTA-wide scan of per-thread counts), the count;
+//   k_obst_near   per block: the block or a face neighbour holds a slot;
+//   k_obst_chi    one CTA per block: 10^3 signed-distance lab in shared
+//                 memory, chi and udef = 0 of its slot, grid chi (0 outside
+//                 the body's blocks), the block's four moments;
+//   k_obst_kin    one CTA: moments over the slots -> centre of mass, kinematics.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "context.h"
+#include "obstacles.h"
+
+namespace cup3d {
+namespace {
+
+constexpr double kEpsD = 2.220446049250313e-16;  // DBL_EPSILON (the host code's numeric_limits epsilon)
+
+struct Shape {
+  int kind;          // 0 sphere, 1 ellipsoid
+  double c[3];       // centre
+  double r;          // sphere radius
+  double ax[3];      // ellipsoid semi-axes
+  double R[3][3];    // ellipsoid rotation, body -> lab
+  double box[3][2];  // bounding box of the body
+  double safety;     // margin of the fill rule
+  double vel[3], omega[3];
+};
+
+// Result record read back by the host: slot count, mass, kinematics.
+struct ObstResult {
+  int nslots;
+  int pad_;
+  double mass;
+  double kin[9];
+};
+
+__device__ double shape_sdf(const Shape& s, double px, double py, double pz) {
+  if (s.kind == 0) {
+    const double dx = px - s.c[0], dy = py - s.c[1], dz = pz - s.c[2];
+    return s.r - sqrt(dx * dx + dy * dy + dz * dz);
+  }
+  const double d0 = px - s.c[0], d1 = py - s.c[1], d2 = pz - s.c[2];
+  double b[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) b[i] = s.R[0][i] * d0 + s.R[1][i] * d1 + s.R[2][i] * d2;  // lab -> body
+  double q = 0, g = 0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    q += (b[i] / s.ax[i]) * (b[i] / s.ax[i]);
+    g += (b[i] / (s.ax[i] * s.ax[i])) * (b[i] / (s.ax[i] * s.ax[i]));
+  }
+  const double rho = sqrt(q);
+  if (rho < 1e-300) return fmin(s.ax[0], fmin(s.ax[1], s.ax[2]));
+  const double grad = sqrt(g) / rho;
+  return (1.0 - rho) / grad;
+}
+
+__device__ __forceinline__ bool block_touches(const Shape& s, const double* origin, double h, int b) {
+  bool touch = true;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double lo = origin[3 * b + d] + 0.5 * h, hi = origin[3 * b + d] + (8 - 0.5) * h;
+    const double bl = s.box[d][0] - s.safety, bh = s.box[d][1] + s.safety;
+    const double a = lo < bl ? bl : lo;  // std::max(lo, bl)
+    const double c = bh < hi ? bh : hi;  // std::min(hi, bh)
+    touch &= c - a > 0;
+  }
+  return touch;
+}
+
+constexpr int SLOT_THREADS = 1024;
+
+__global__ void __launch_bounds__(SLOT_THREADS) k_obst_slots(int nb, const double* __restrict__ h,
+                                                             const double* __restrict__ origin, Shape s,
+                                                             int* __restrict__ slot_of_block,
+                                                             int* __restrict__ block_of_slot, ObstResult* res) {
+  __shared__ int part[SLOT_THREADS];
+  const int t = threadIdx.x;
+  const int chunk = (nb + SLOT_THREADS - 1) / SLOT_THREADS;
+  const int b0 = min(nb, t * chunk), b1 = min(nb, b0 + chunk);
+  int cnt = 0;
+  for (int b = b0; b < b1; ++b) cnt += block_touches(s, origin, h[b], b) ? 1 : 0;
+  part[t] = cnt;
+  __syncthreads();
+  // inclusive scan (Hillis-Steele) of the per-thread counts
+  for (int off = 1; off < SLOT_THREADS; off <<= 1) {
+    const int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int slot = part[t] - cnt;
+  for (int b = b0; b < b1; ++b) {
+    if (block_touches(s, origin, h[b], b)) {
+      slot_of_block[b] = slot;
+      block_of_slot[slot] = b;
+      ++slot;
+    } else {
+      slot_of_block[b] = -1;
+    }
+  }
+  if (t == SLOT_THREADS - 1) res->nslots = part[t];
+}
+
+__global__ void k_obst_near(DevMesh M, const int* __restrict__ slot_of_block, int* __restrict__ near) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < M.nb; b += gridDim.x * blockDim.x) {
+    bool nr = slot_of_block[b] >= 0;
+    for (int f = 0; f < 6 && !nr; ++f) {
+      const int k = M.fkind[6 * b + f];
+      const int* nbr = M.fnbr + 24 * b + 4 * f;
+      if (k == K_SAME || k == K_COARSER) nr |= slot_of_block[nbr[0]] >= 0;
+      if (k == K_FINER)
+        for (int q = 0; q < 4; ++q) nr |= slot_of_block[nbr[q]] >= 0;
+    }
+    near[b] = nr ? 1 : 0;
+  }
+}
+
+// Sum of v over the 512 threads of the CTA in a fixed order (warp shuffles,
+// then the 16 warp sums in order).
+__device__ __forceinline__ double cta_sum512(double v, double* sm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < 16; ++w) s += sm[w];
+  __syncthreads();
+  return s;
+}
+
+__global__ void __launch_bounds__(BN) k_obst_chi(const double* __restrict__ h_, const double* __restrict__ origin,
+                                                  Shape s, const int* __restrict__ slot_of_block,
+                                                  double* __restrict__ chi, double* __restrict__ udef,
+                                                  double* __restrict__ grid_chi, double* __restrict__ mom,
+                                                  const ObstResult* res) {
+  const int b = blockIdx.x, t = threadIdx.x;
+  const int slot = slot_of_block[b];
+  if (slot < 0) {
+    grid_chi[size_t(b) * BN + t] = 0.0;
+    return;
+  }
+  __shared__ double lab[10][10][10];
+  __shared__ double sm[16];
+  const double h = h_[b];
+  const double ox = origin[3 * b], oy = origin[3 * b + 1], oz = origin[3 * b + 2];
+  for (int i = t; i < 1000; i += BN) {
+    const int x = i % 10 - 1, y = (i / 10) % 10 - 1, z = i / 100 - 1;
+    lab[z + 1][y + 1][x + 1] = shape_sdf(s, ox + (x + 0.5) * h, oy + (y + 0.5) * h, oz + (z + 0.5) * h);
+  }
+  __syncthreads();
+  const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
+  const double inv2h = 0.5 / h, vol = h * h * h;
+  const double s0 = lab[z + 1][y + 1][x + 1];
+  double c;
+  if (s0 > h || s0 < -h) {
+    c = s0 > 0 ? 1 : 0;
+  } else {
+    const double dPx = lab[z + 1][y + 1][x + 2], dMx = lab[z + 1][y + 1][x];
+    const double dPy = lab[z + 1][y + 2][x + 1], dMy = lab[z + 1][y][x + 1];
+    const double dPz = lab[z + 2][y + 1][x + 1], dMz = lab[z][y + 1][x + 1];
+    const double gUX = inv2h * (dPx - dMx), gUY = inv2h * (dPy - dMy), gUZ = inv2h * (dPz - dMz);
+    const double gUSq = gUX * gUX + gUY * gUY + gUZ * gUZ + kEpsD;
+    const double gIX = inv2h * ((0.0 < dPx ? dPx : 0.0) - (0.0 < dMx ? dMx : 0.0));
+    const double gIY = inv2h * ((0.0 < dPy ? dPy : 0.0) - (0.0 < dMy ? dMy : 0.0));
+    const double gIZ = inv2h * ((0.0 < dPz ? dPz : 0.0) - (0.0 < dMz ? dMz : 0.0));
+    c = (gIX * gUX + gIY * gUY + gIZ * gUZ) / gUSq;
+  }
+  chi[size_t(slot) * BN + t] = c;
+  const size_t ns = size_t(res->nslots);  // udef is component-major: [3][nslots][512]
+  for (int d = 0; d < 3; ++d) udef[(d * ns + slot) * BN + t] = 0.0;
+  grid_chi[size_t(b) * BN + t] = 0.0 < c ? c : 0.0;  // std::max(0, chi)
+  const double px = ox + (x + 0.5) * h, py = oy + (y + 0.5) * h, pz = oz + (z + 0.5) * h;
+  const double cv = c * vol;
+  const double m0 = cta_sum512(cv * px, sm), m1 = cta_sum512(cv * py, sm), m2 = cta_sum512(cv * pz, sm),
+               m3 = cta_sum512(cv, sm);
+  if (t == 0) {
+    mom[4 * slot + 0] = m0;
+    mom[4 * slot + 1] = m1;
+    mom[4 * slot + 2] = m2;
+    mom[4 * slot + 3] = m3;
+  }
+}
+
+__global__ void __launch_bounds__(BN) k_obst_kin(const double* __restrict__ mom, Shape s, ObstResult* res,
+                                                  double* __restrict__ kin_out) {
+  __shared__ double sm[16];
+  const int n = res->nslots;
+  double a[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < n; i += BN)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] += mom[4 * i + k];
+  double tot[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) tot[k] = cta_sum512(a[k], sm);
+  if (threadIdx.x == 0) {
+    res->mass = tot[3];
+    for (int d = 0; d < 3; ++d) {
+      res->kin[d] = tot[3] > 0 ? tot[d] / tot[3] : 0.0;
+      res->kin[3 + d] = s.vel[d];
+      res->kin[6 + d] = s.omega[d];
+    }
+    for (int i = 0; i < 9; ++i) kin_out[i] = res->kin[i];
+  }
+}
+
+// Device buffers of a device-created obstacle, sized for every block of the
+// mesh (the slot count is known only after k_obst_slots).
+int obst_dev_buffers(cup_ctx* c) {
+  DevObstacle& o = c->ob;
+  const int nb = c->mesh.nb;
+  if (o.dev_cap == nb) return 0;
+  c->obst_arena.release();
+  o = DevObstacle();
+  DevArena& A = c->obst_arena;
+  if (int rc = A.alloc(&o.slot_of_block, nb)) return rc;
+  if (int rc = A.alloc(&o.near, nb)) return rc;
+  if (int rc = A.alloc(&o.block_of_slot, nb)) return rc;
+  if (int rc = A.alloc(&o.chi, size_t(nb) * BN)) return rc;
+  if (int rc = A.alloc(&o.udef, 3 * size_t(nb) * BN)) return rc;
+  if (int rc = A.alloc(&o.d_mom, 4 * size_t(nb))) return rc;
+  if (int rc = A.alloc(&o.d_origin, 3 * size_t(nb))) return rc;
+  ObstResult* r = nullptr;
+  if (int rc = A.alloc(&r, 1)) return rc;
+  o.d_result = r;
+  CUP_CUDA_TRY(stream_h2d(c->stream, o.d_origin, c->mesh.origin.data(), 3 * size_t(nb) * sizeof(double)));
+  o.dev_cap = nb;
+  return 0;
+}
+
+int create_obstacle_dev(cup_ctx* c, Shape& s) {
+  graph_reset(c);
+  const Mesh& m = c->mesh;
+  double hmax = 0;
+  for (int b = 0; b < m.nb; ++b) hmax = std::max(hmax, m.h[b]);
+  s.safety = kObstacleSafety * hmax;
+  if (int rc = obst_dev_buffers(c)) return rc;
+  DevObstacle& o = c->ob;
+  ObstResult* res = static_cast<ObstResult*>(o.d_result);
+  cudaStream_t st = c->stream;
+  {
+    ProfScope ps("obstacle_slots", st);
+    k_obst_slots<<<1, SLOT_THREADS, 0, st>>>(m.nb, c->dm.h, o.d_origin, s, o.slot_of_block, o.block_of_slot, res);
+  }
+  {
+    ProfScope ps("obstacle_near", st);
+    k_obst_near<<<std::max(1, std::min((m.nb + 255) / 256, c->num_sms * 4)), 256, 0, st>>>(c->dm, o.slot_of_block,
+                                                                                         o.near);
+  }
+  {
+    ProfScope ps("obstacle_chi", st);
+    k_obst_chi<<<m.nb, BN, 0, st>>>(c->dm.h, o.d_origin, s, o.slot_of_block, o.chi, o.udef, c->F.chi, o.d_mom, res);
+  }
+  {
+    ProfScope ps("obstacle_kin", st);
+    k_obst_kin<<<1, BN, 0, st>>>(o.d_mom, s, res, c->d_scalars + SC_KIN);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  ObstResult h{};
+  CUP_CUDA_TRY(stream_d2h(st, &h, res, sizeof(h)));
+  o.nslots = h.nslots;
+  for (int i = 0; i < 9; ++i) o.kin[i] = h.kin[i];
+  o.host_stale = true;
+  if (h.nslots == 0) {  // nothing of the body on the mesh: no obstacle
+    c->obst_arena.release();
+    c->ob = DevObstacle();
+  }
+  return 0;
+}
+
+int shape_args_ok(cup_ctx* c, const char* who) {
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, std::string(who) + ": bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, std::string(who) + ": not available on a batch of cases");
+  return 0;
+}
+
+void set_kinematics(Shape& s, const double* vel, const double* omega) {
+  for (int d = 0; d < 3; ++d) {
+    s.vel[d] = vel ? vel[d] : 0.0;
+    s.omega[d] = omega ? omega[d] : 0.0;
+  }
+}
+
+}  // namespace
+
+// Host copies of a device-created obstacle (slot list, chi, udef), fetched
+// when something reads them.
+int ctx_obstacle_host_copies(cup_ctx* c) {
+  DevObstacle& o = c->ob;
+  if (!o.host_stale) return 0;
+  o.h_blocks.resize(o.nslots);
+  o.h_chi.resize(size_t(o.nslots) * BN);
+  o.h_udef.resize(3 * size_t(o.nslots) * BN);
+  CUP_CUDA_TRY(stream_d2h(c->stream, o.h_blocks.data(), o.block_of_slot, o.h_blocks.size() * sizeof(int)));
+  CUP_CUDA_TRY(stream_d2h(c->stream, o.h_chi.data(), o.chi, o.h_chi.size() * sizeof(double)));
+  CUP_CUDA_TRY(stream_d2h(c->stream, o.h_udef.data(), o.udef, o.h_udef.size() * sizeof(double)));
+  o.host_stale = false;
+  return 0;
+}
+
+}  // namespace cup3d
+
+using namespace cup3d;
+
+extern "C" {
+
+int cup_obstacle_sphere_dev(cup_ctx* c, const double* ctr, double r, const double* vel, const double* omega) {
+  ProfBind pb_(c);
+  if (!ctr) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_sphere_dev: bad arguments");
+  if (int rc = shape_args_ok(c, "cup_obstacle_sphere_dev")) return rc;
+  Shape s{};
+  s.kind = 0;
+  for (int d = 0; d < 3; ++d) {
+    s.c[d] = ctr[d];
+    s.box[d][0] = ctr[d] - r;
+    s.box[d][1] = ctr[d] + r;
+  }
+  s.r = r;
+  set_kinematics(s, vel, omega);
+  if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_sphere_dev failed");
+  return 0;
+}
+
+int cup_obstacle_ellipsoid_dev(cup_ctx* c, const double* ctr, const double* ax, const double* q, const double* vel,
+                               const double* omega) {
+  ProfBind pb_(c);
+  if (!ctr || !ax || !q) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_ellipsoid_dev: bad arguments");
+  if (int rc = shape_args_ok(c, "cup_obstacle_ellipsoid_dev")) return rc;
+  Shape s{};
+  s.kind = 1;
+  quat_rotation(q, s.R);
+  const double rmax = std::max({ax[0], ax[1], ax[2]});
+  for (int d = 0; d < 3; ++d) {
+    s.c[d] = ctr[d];
+    s.ax[d] = ax[d];
+    s.box[d][0] = ctr[d] - rmax;
+    s.box[d][1] = ctr[d] + rmax;
+  }
+  set_kinematics(s, vel, omega);
+  if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_ellipsoid_dev failed");
+  return 0;
+}
+
+}  // extern "C"

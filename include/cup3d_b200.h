@@ -199,6 +199,14 @@ int cup_obstacle_sphere(cup_ctx* ctx, const double* c, double r, const double* v
 /* Ellipsoid with semi-axes ax[3] rotated by the unit quaternion q = (w,x,y,z). */
 int cup_obstacle_ellipsoid(cup_ctx* ctx, const double* c, const double* ax, const double* q,
                            const double* vel, const double* omega);
+/* The same bodies created on the device (no host work on the blocks): the slot
+ * list, chi, udef and CUP_FIELD_CHI equal those of cup_obstacle_sphere /
+ * cup_obstacle_ellipsoid bit for bit, the centre of mass to rounding (other
+ * summation order).  One 96-byte device-to-host read of the slot count and
+ * kinematics; cup_get_obstacle fetches the host copies when called. */
+int cup_obstacle_sphere_dev(cup_ctx* ctx, const double* c, double r, const double* vel, const double* omega);
+int cup_obstacle_ellipsoid_dev(cup_ctx* ctx, const double* c, const double* ax, const double* q,
+                               const double* vel, const double* omega);
 /* Raw obstacle data: nslots obstacle blocks, block_of_slot[nslots] (device
  * order), chi[nslots*512], udef[3*nslots*512] (component-major), kin[9] =
  * centre of mass, velocity, angular velocity.  nslots = 0 removes the body. */
