@@ -255,6 +255,51 @@ def swarm_batch(flush, steps=5):
     }
 
 
+def obstacle_creation(reps=7):
+    """Obstacle creation (CreateObstacles) on the host path (cup_obstacle_sphere:
+    signed distance and chi on the host, then the upload) against the device
+    path (cup_obstacle_sphere_dev: four kernels and one 96-byte read of the
+    slot count and kinematics): wall time of the call, median of reps, for the
+    sphere on the sphere mesh and for swarm case 0's ellipsoid.  Both paths
+    give the same slot list and chi bit for bit."""
+    import torch
+    import cup3d_b200 as cup
+    from cup3d_b200.workloads import SWARM_AXES, make_swarm_ctx, swarm_case
+    lib = cup._lib.lib()
+    dev = torch.cuda.current_device()
+    out = {}
+    sphere = make_sphere_ctx(dev)
+    p = swarm_case(0)
+    swarm = make_swarm_ctx(0, dev)
+    cases = {
+        "sphere": (sphere, lambda on: sphere.obstacle_sphere(**SPHERE_BODY, on_device=on)),
+        "swarm_case0_ellipsoid": (swarm, lambda on: swarm.obstacle_ellipsoid(p["center"], SWARM_AXES, p["quat"],
+                                                                              vel=p["vel"], on_device=on)),
+    }
+    for name, (ctx, make) in cases.items():
+        st = torch.cuda.ExternalStream(lib.cup_stream(ctx._p))
+        res = {"blocks": ctx.nb}
+        for on in (False, True):
+            make(on)  # warm
+            wall, dev_ms = [], []
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record(st)
+                t0 = time.perf_counter()
+                make(on)
+                wall.append((time.perf_counter() - t0) * 1e3)
+                e1.record(st)
+                e1.synchronize()
+                dev_ms.append(e0.elapsed_time(e1))
+            res["device" if on else "host"] = {"wall_ms": round(float(np.median(wall)), 4),
+                                               "stream_ms": round(float(np.median(dev_ms)), 4)}
+        res["slots"] = int((ctx.get_obstacle()[0] >= 0).sum())
+        res["speedup_wall"] = round(res["host"]["wall_ms"] / res["device"]["wall_ms"], 2)
+        out[name] = res
+    return out
+
+
 def run_b200(args):
     import torch
     rank, world, local = dist_env()
@@ -420,6 +465,8 @@ def run_b200(args):
         line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush)
     if rank == 0 and not args.no_swarm:
         line["swarm_batch"] = swarm_batch(flush)
+    if rank == 0 and not args.no_obstacle:
+        line["obstacle_creation"] = obstacle_creation()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ctx, args, (vel0, pres0), first_step)
     if world > 1:
@@ -522,6 +569,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson-to-tolerance comparison")
     ap.add_argument("--no-swarm", action="store_true", help="skip the batched ellipsoid-swarm measurement")
+    ap.add_argument("--no-obstacle", action="store_true", help="skip the obstacle-creation measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
