@@ -54,6 +54,7 @@ class cup_config(C.Structure):
         ("device", C.c_int32),
         ("poisson_block_cache", C.c_int32),
         ("step_graph", C.c_int32),
+        ("static_obstacles", C.c_int32),
     ]
 
 

@@ -200,6 +200,7 @@ void cup_config_default(cup_config* c) {
   c->device = 0;
   c->poisson_block_cache = 4;
   c->step_graph = 1;
+  c->static_obstacles = 0;
 }
 
 static int parse_bc(const std::string& v) {
@@ -276,6 +277,9 @@ int cup_config_parse(cup_config* c, const char* args) {
     } else if (key == "stepGraph") {
       if (need_num()) return CUP_ERR_ARG;
       c->step_graph = dv != 0 ? 1 : 0;
+    } else if (key == "StaticObstacles") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->static_obstacles = dv != 0 ? 1 : 0;
     } else if (key == "poissonBlockCache") {
       if (need_num()) return CUP_ERR_ARG;
       if (dv < 0 || dv > 4) return ctx_fail(nullptr, CUP_ERR_ARG, "poissonBlockCache must be 0-4");
@@ -871,6 +875,7 @@ int cup_obstacle_sphere(cup_ctx* c, const double* ctr, double r, const double* v
   const double z[3] = {0, 0, 0};
   HostObstacle h;
   make_sphere(c->mesh, ctr, r, vel ? vel : z, omega ? omega : z, h);
+  body_record(c, 0, false, ctr, &r, nullptr, vel, omega);
   return install_host_obstacle(c, h);
 }
 
@@ -882,6 +887,7 @@ int cup_obstacle_ellipsoid(cup_ctx* c, const double* ctr, const double* ax, cons
   const double z[3] = {0, 0, 0};
   HostObstacle h;
   make_ellipsoid(c->mesh, ctr, ax, q, vel ? vel : z, omega ? omega : z, h);
+  body_record(c, 1, false, ctr, ax, q, vel, omega);
   return install_host_obstacle(c, h);
 }
 
@@ -890,6 +896,7 @@ int cup_set_obstacle(cup_ctx* c, int32_t nslots, const int32_t* blocks, const do
   if (!c || c->mesh.nb == 0 || (nslots > 0 && (!blocks || !chi)))
     return ctx_fail(c, CUP_ERR_ARG, "cup_set_obstacle: bad arguments");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_set_obstacle: not available on a batch of cases");
+  c->body = BodyState();  // raw data: no shape to move
   return ctx_upload_obstacle(c, nslots, blocks, chi, udef, kin);
 }
 
@@ -977,11 +984,22 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_step: no mesh");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_step: not available on a batch of cases");
-  if (!(dt > 0) && c->cfg.step_graph && c->cfg.poisson_solver == CUP_POISSON_B200 && !c->prof.on)
-    return graph_step(c, step, dt_used, stats);
+  const bool moving = body_moves(c);
+  if (!(dt > 0) && c->cfg.step_graph && c->cfg.poisson_solver == CUP_POISSON_B200 && !c->prof.on && !moving) {
+    const int rc = graph_step(c, step, dt_used, stats);
+    if (rc >= 0) {
+      body_coef_u(c, step, c->gio->dt);
+      c->dt_prev = c->gio->dt;
+    }
+    return rc;
+  }
   if (!(dt > 0))
     if (int rc = cup_compute_dt(c, step, &dt)) return rc;
   if (dt_used) *dt_used = dt;
+  body_coef_u(c, step, dt);
+  c->dt_prev = dt;
+  if (moving)  // CreateObstacles: Obstacle::update, then chi at the new pose
+    if (int rc = body_advance(c, step, dt)) return keep(c, rc);
   if (int rc = advect(c, dt)) return rc;
   if (c->ob.nslots > 0)
     if (int rc = penalize(c, dt)) return rc;

@@ -95,6 +95,17 @@ struct GraphIO {
   KrylovState st;
 };
 
+// Shape, pose and motion of the context's body (Obstacle.h: position,
+// quaternion, transVel, angVel and their previous values for BDF2).
+struct BodyState {
+  int kind = -1;           // -1: none (or raw data), 0 sphere, 1 ellipsoid
+  bool on_device = false;  // re-created by the device path
+  double pos[3] = {0, 0, 0}, quat[4] = {1, 0, 0, 0};
+  double r = 0, ax[3] = {0, 0, 0};
+  double vel[3] = {0, 0, 0}, omega[3] = {0, 0, 0};
+  double old_pos[3] = {0, 0, 0}, old_quat[4] = {1, 0, 0, 0};
+};
+
 struct Fields {
   double* vel[2] = {nullptr, nullptr};  // ping-pong, 3*nb*512 each
   int vcur = 0;
@@ -137,6 +148,11 @@ struct cup_ctx {
   cudaGraphExec_t gexec[8] = {};
   cup3d::GraphIO* gio = nullptr;      // pinned
   cup3d::DevArena batch_arena;
+  // moving bodies: pose, the previous step's dt and the BDF2 coefficients of
+  // the pose update (SimulationData::coefU)
+  cup3d::BodyState body;
+  double dt_prev = 0.0;
+  double coef_u[3] = {1.5, -2.0, 0.5};
 };
 
 namespace cup3d {
@@ -156,6 +172,17 @@ int ctx_alloc_fields(cup_ctx* c);
 // Installs an obstacle (nslots blocks with chi, udef and kinematics kin[9]).
 int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
                         const double* kin);
+// Moving bodies (obstacles_dev.cu).  body_record keeps the shape and motion
+// of a body just created (r: the sphere radius or the ellipsoid axes; q null
+// for a sphere); body_moves: the body is not static and its velocity + uinf
+// or angular velocity is non-zero; body_coef_u: the BDF2 coefficients of the
+// step (Simulation.cpp:361-370); body_advance: Obstacle::update with dt, then
+// chi at the new pose by the path the body was created with.
+void body_record(cup_ctx* c, int kind, bool on_device, const double* ctr, const double* r, const double* q,
+                 const double* vel, const double* omega);
+bool body_moves(const cup_ctx* c);
+void body_coef_u(cup_ctx* c, int step, double dt);
+int body_advance(cup_ctx* c, int step, double dt);
 // Fetches the host copies of a device-created obstacle (no-op otherwise).
 int ctx_obstacle_host_copies(cup_ctx* c);
 // Drops the captured time steps (after any change of mesh, obstacle or

@@ -300,6 +300,97 @@ void set_kinematics(Shape& s, const double* vel, const double* omega) {
 
 }  // namespace
 
+void body_record(cup_ctx* c, int kind, bool on_device, const double* ctr, const double* r, const double* q,
+                 const double* vel, const double* omega) {
+  BodyState& B = c->body;
+  B = BodyState();
+  B.kind = kind;
+  B.on_device = on_device;
+  for (int d = 0; d < 3; ++d) {
+    B.pos[d] = B.old_pos[d] = ctr[d];
+    B.vel[d] = vel ? vel[d] : 0.0;
+    B.omega[d] = omega ? omega[d] : 0.0;
+  }
+  if (kind == 0) {
+    B.r = r[0];
+  } else {
+    for (int d = 0; d < 3; ++d) B.ax[d] = r[d];
+    for (int i = 0; i < 4; ++i) B.quat[i] = B.old_quat[i] = q[i];
+  }
+}
+
+bool body_moves(const cup_ctx* c) {
+  const BodyState& B = c->body;
+  if (B.kind < 0 || c->cfg.static_obstacles || c->ob.nslots == 0) return false;
+  for (int d = 0; d < 3; ++d)
+    if (B.vel[d] + c->cfg.uinf[d] != 0.0 || B.omega[d] != 0.0) return true;
+  return false;
+}
+
+void body_coef_u(cup_ctx* c, int step, double dt) {
+  if (step > c->cfg.step_2nd_start && c->dt_prev > 0) {  // Simulation.cpp:361-370
+    const double a = c->dt_prev, b = dt;
+    const double c1 = -(a + b) / (a * b);
+    const double c2 = b / (a + b) / a;
+    c->coef_u[0] = -b * (c1 + c2);
+    c->coef_u[1] = b * c1;
+    c->coef_u[2] = b * c2;
+  }
+}
+
+// Obstacle::update (Obstacle.cpp:306-368) for a body driven by its
+// prescribed velocities: explicit Euler for the first step_2nd_start steps,
+// BDF2 with coefU after; the quaternion is renormalised.
+static void body_update(BodyState& B, const double uinf[3], int step, int step_2nd_start, const double coef[3],
+                        double dt) {
+  const double* w = B.omega;
+  double* q = B.quat;
+  const double dqdt[4] = {0.5 * (-w[0] * q[1] - w[1] * q[2] - w[2] * q[3]),
+                          0.5 * (+w[0] * q[0] + w[1] * q[3] - w[2] * q[2]),
+                          0.5 * (-w[0] * q[3] + w[1] * q[0] + w[2] * q[1]),
+                          0.5 * (+w[0] * q[2] - w[1] * q[1] + w[2] * q[0])};
+  if (step < step_2nd_start) {
+    for (int d = 0; d < 3; ++d) {
+      B.old_pos[d] = B.pos[d];
+      B.pos[d] += dt * (B.vel[d] + uinf[d]);
+    }
+    for (int i = 0; i < 4; ++i) {
+      B.old_quat[i] = q[i];
+      q[i] += dt * dqdt[i];
+    }
+  } else {
+    const double aux = 1.0 / coef[0];
+    double tp[3], tq[4];
+    for (int d = 0; d < 3; ++d) {
+      tp[d] = B.pos[d];
+      B.pos[d] = aux * (dt * (B.vel[d] + uinf[d]) + (-coef[1] * B.pos[d] - coef[2] * B.old_pos[d]));
+    }
+    for (int i = 0; i < 4; ++i) {
+      tq[i] = q[i];
+      q[i] = aux * (dt * dqdt[i] + (-coef[1] * q[i] - coef[2] * B.old_quat[i]));
+    }
+    for (int d = 0; d < 3; ++d) B.old_pos[d] = tp[d];
+    for (int i = 0; i < 4; ++i) B.old_quat[i] = tq[i];
+  }
+  const double invD = 1.0 / std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  for (int i = 0; i < 4; ++i) q[i] *= invD;
+}
+
+int body_advance(cup_ctx* c, int step, double dt) {
+  BodyState& B = c->body;
+  body_update(B, c->cfg.uinf, step, c->cfg.step_2nd_start, c->coef_u, dt);
+  const BodyState keep_state = B;  // the creation calls below record the body afresh
+  int rc = 0;
+  if (B.kind == 0)
+    rc = B.on_device ? cup_obstacle_sphere_dev(c, B.pos, B.r, B.vel, B.omega)
+                     : cup_obstacle_sphere(c, B.pos, B.r, B.vel, B.omega);
+  else
+    rc = B.on_device ? cup_obstacle_ellipsoid_dev(c, B.pos, B.ax, B.quat, B.vel, B.omega)
+                     : cup_obstacle_ellipsoid(c, B.pos, B.ax, B.quat, B.vel, B.omega);
+  c->body = keep_state;
+  return rc;
+}
+
 // Host copies of a device-created obstacle (slot list, chi, udef), fetched
 // when something reads them.
 int ctx_obstacle_host_copies(cup_ctx* c) {
@@ -335,6 +426,7 @@ int cup_obstacle_sphere_dev(cup_ctx* c, const double* ctr, double r, const doubl
   s.r = r;
   set_kinematics(s, vel, omega);
   if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_sphere_dev failed");
+  body_record(c, 0, true, ctr, &r, nullptr, vel, omega);
   return 0;
 }
 
@@ -355,6 +447,7 @@ int cup_obstacle_ellipsoid_dev(cup_ctx* c, const double* ctr, const double* ax, 
   }
   set_kinematics(s, vel, omega);
   if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_ellipsoid_dev failed");
+  body_record(c, 1, true, ctr, ax, q, vel, omega);
   return 0;
 }
 

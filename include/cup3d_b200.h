@@ -82,6 +82,10 @@ typedef struct cup_config {
   int32_t step_graph;          /* -stepGraph: cup_step with dt <= 0 and the plain solver replays a
                                   CUDA graph of the whole step (1, default) or launches the
                                   kernels one by one (0); the same kernels either way */
+  int32_t static_obstacles;    /* -StaticObstacles (default 0): bodies created by cup_obstacle_sphere(_dev)
+                                  / cup_obstacle_ellipsoid(_dev) whose velocity + uinf or angular
+                                  velocity is non-zero move every cup_step (Obstacle::update) and
+                                  their chi is re-created at the new pose (CreateObstacles) */
 } cup_config;
 
 typedef struct cup_solve_stats {
@@ -175,7 +179,9 @@ int cup_batch_poisson_solve_dev(cup_ctx* batch, const double* d_b, double* d_x, 
  * (or, when dt_in is NULL or dt_in[k] <= 0, Simulation::calcMaxTimestep from
  * the case's own max |u| and finest spacing).  dt_used[ncases]; force[6 ncases]
  * (penalization force and torque per case, may be NULL); stats[ncases] (may
- * be NULL).  The Poisson solves of all cases run in one device launch. */
+ * be NULL).  The Poisson solves of all cases run in one device launch.
+ * Bodies stay where the cases had them when the batch was made (as with
+ * -StaticObstacles 1); moving bodies are stepped by cup_step on single cases. */
 int cup_batch_step(cup_ctx* batch, int32_t step, const double* dt_in, double* dt_used, double* force,
                    cup_solve_stats* stats);
 

@@ -110,3 +110,77 @@ def test_batch_of_device_created_bodies():
         assert rc0 == rc1 == 0 and np.array_equal(dt0, dt1), step
         assert all(_close(a, b) for a, b in zip(f0, f1)), step
         assert np.array_equal(batches[0].download("vel"), batches[1].download("vel")), step
+
+
+def _pose_update(b, uinf, step, coef, dt, step_2nd_start=2):
+    """Obstacle::update (Obstacle.cpp:306-368) restated: Euler for the first
+    step_2nd_start steps, BDF2 with coefU after, quaternion renormalised."""
+    w, q = b["omega"], b["quat"]
+    dqdt = [0.5 * (-w[0] * q[1] - w[1] * q[2] - w[2] * q[3]),
+            0.5 * (+w[0] * q[0] + w[1] * q[3] - w[2] * q[2]),
+            0.5 * (-w[0] * q[3] + w[1] * q[0] + w[2] * q[1]),
+            0.5 * (+w[0] * q[2] - w[1] * q[1] + w[2] * q[0])]
+    if step < step_2nd_start:
+        b["old_pos"], b["old_quat"] = list(b["pos"]), list(q)
+        b["pos"] = [b["pos"][d] + dt * (b["vel"][d] + uinf[d]) for d in range(3)]
+        q = [q[i] + dt * dqdt[i] for i in range(4)]
+    else:
+        aux = 1.0 / coef[0]
+        tp, tq = list(b["pos"]), list(q)
+        b["pos"] = [aux * (dt * (b["vel"][d] + uinf[d]) + (-coef[1] * b["pos"][d] - coef[2] * b["old_pos"][d]))
+                    for d in range(3)]
+        q = [aux * (dt * dqdt[i] + (-coef[1] * q[i] - coef[2] * b["old_quat"][i])) for i in range(4)]
+        b["old_pos"], b["old_quat"] = tp, tq
+    inv = 1.0 / np.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+    b["quat"] = [x * inv for x in q]
+
+
+@pytest.mark.parametrize("on_device", [True, False])
+def test_moving_body_is_recreated_at_its_integrated_pose(on_device):
+    # CreateObstacles every step: the pose integrated by Obstacle::update with
+    # the step's dt (Euler in steps 0-1, BDF2 with the default coefU in step
+    # 2, with coefU of the last two dts in step 3), then chi at that pose:
+    # bit for bit the host creation at the pose restated here
+    flags = "-poissonTol 0 -poissonTolRel 1e-6 -nu 0.01 -CFL 0.3 -rampup 0 -advection weno5"
+    ctx = make_ctx("amr2_free", device=0, extra=flags)
+    xyz, _ = ctx.cell_centres()
+    x, y, z = xyz.T
+    ctx.upload("vel", np.concatenate([np.sin(2 * x) * np.cos(3 * y), 0.5 * np.cos(x) * np.sin(2 * z), 0.3 * np.sin(y + z)]))
+    q0 = np.array([0.9, 0.1, 0.3, 0.3])
+    q0 = list(q0 / np.linalg.norm(q0))
+    body = dict(pos=[0.45, 0.5, 0.5], quat=q0, old_pos=[0.45, 0.5, 0.5], old_quat=list(q0), vel=[3.0, -1.0, 0.5],
+                omega=[5.0, -3.0, 2.0])
+    axes = (0.2, 0.1, 0.08)
+    ctx.obstacle_ellipsoid(body["pos"], axes, body["quat"], vel=body["vel"], omega=body["omega"], on_device=on_device)
+    chi0 = ctx.download("chi")
+    coef, dt_prev = [1.5, -2.0, 0.5], 0.0
+    for step in range(4):
+        dt, rc, st = ctx.step(step)
+        assert rc >= 0 and st["status"] == 1, (step, rc, st)
+        if step > 2 and dt_prev > 0:
+            a, b = dt_prev, dt
+            c1, c2 = -(a + b) / (a * b), b / (a + b) / a
+            coef = [-b * (c1 + c2), b * c1, b * c2]
+        dt_prev = dt
+        _pose_update(body, (0.0, 0.0, 0.0), step, coef, dt)
+    ref = make_ctx("amr2_free", device=0)
+    ref.obstacle_ellipsoid(body["pos"], axes, body["quat"], vel=body["vel"], omega=body["omega"])
+    slot, chi, _, kin = ctx.get_obstacle()
+    slot_r, chi_r, _, kin_r = ref.get_obstacle()
+    assert np.abs(ctx.download("chi") - chi0).max() > 0.5  # the body has moved by more than a cell
+    assert np.array_equal(slot, slot_r) and np.array_equal(chi, chi_r)
+    assert np.abs(kin[:3] - kin_r[:3]).max() <= 1e-14
+    assert np.array_equal(ctx.download("chi"), ref.download("chi"))
+
+
+def test_static_and_comoving_bodies_stay():
+    # -StaticObstacles 1, or a body whose velocity + uinf and angular velocity
+    # are zero (the sphere in its own frame): chi is never re-created
+    for flags, vel, uinf in (("-StaticObstacles 1", (0.2, 0.0, 0.0), 0.0), ("", (0.1, 0.0, 0.0), -0.1)):
+        ctx = make_ctx("amr2_free", device=0, extra=f"-rampup 0 -uinfx {uinf} {flags}")
+        ctx.obstacle_sphere((0.5, 0.5, 0.5), 0.15, vel=vel, on_device=True)
+        before = _obstacle_state(ctx)
+        for step in range(3):
+            _, rc, _ = ctx.step(step)
+            assert rc >= 0
+        _assert_same(before, _obstacle_state(ctx), 1.0)

@@ -27,7 +27,7 @@ def _pair(name, extra):
 
 @pytest.mark.parametrize("name,extra,body", [
     ("tgv32", "-nu 0.01 -CFL 0.3 -rampup 0", None),
-    ("amr2_free", "-nu 0.001 -CFL 0.4 -rampup 3 -advection weno5", ((0.5, 0.45, 0.55), 0.15)),
+    ("amr2_free", "-nu 0.001 -CFL 0.4 -rampup 3 -advection weno5 -StaticObstacles 1", ((0.5, 0.45, 0.55), 0.15)),
 ])
 def test_captured_steps_match_launched_steps(name, extra, body):
     g, p = _pair(name, extra)
