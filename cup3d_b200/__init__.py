@@ -180,6 +180,18 @@ class Context:
         fn = lib().cup_obstacle_ellipsoid_dev if on_device else lib().cup_obstacle_ellipsoid
         check(fn(self._p, dptr(c), dptr(a), dptr(q), dptr(v), dptr(o)), self._p)
 
+    def obstacle_free(self, trans=(1, 1, 1), rot=(1, 1, 1)):
+        """Free degrees of freedom of the body (cup_obstacle_free)."""
+        t, r = (np.ascontiguousarray(x, np.int32) for x in (trans, rot))
+        check(lib().cup_obstacle_free(self._p, iptr(t), iptr(r)), self._p)
+
+    def update_obstacles(self, dt):
+        """UpdateObstacles (cup_update_obstacles): dict of the body's velocity,
+        angular velocity, force and torque."""
+        out = np.zeros(12)
+        check(lib().cup_update_obstacles(self._p, dt, dptr(out)), self._p)
+        return {"vel": out[0:3], "omega": out[3:6], "force": out[6:9], "torque": out[9:12]}
+
     def set_obstacle(self, blocks, chi, udef, kin):
         blocks = np.ascontiguousarray(blocks, np.int32)
         chi, udef, kin = (np.ascontiguousarray(x, np.float64) for x in (chi, udef, kin))

@@ -1001,6 +1001,8 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   if (moving)  // CreateObstacles: Obstacle::update, then chi at the new pose
     if (int rc = body_advance(c, step, dt)) return keep(c, rc);
   if (int rc = advect(c, dt)) return rc;
+  if (body_free(c))  // UpdateObstacles: free degrees of freedom from the fluid momentum
+    if (int rc = update_obstacles(c, dt, nullptr)) return keep(c, rc);
   if (c->ob.nslots > 0)
     if (int rc = penalize(c, dt)) return rc;
   const int rc = project(c, dt, step, stats);

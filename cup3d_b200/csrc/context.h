@@ -50,6 +50,10 @@ struct DevObstacle {
   double* d_mom = nullptr;        // 4 per slot: sum chi h^3 (x, y, z), sum chi h^3
   double* d_origin = nullptr;     // 3 nb block origins
   void* d_result = nullptr;       // slot count, mass, kinematics
+  // momentum integrals of UpdateObstacles: 29 per slot, then their sums
+  double* d_qslot = nullptr;
+  double* d_qsum = nullptr;
+  int q_cap = 0;
 };
 
 // Learned preconditioner state: weights, Adam moments, training scratch and
@@ -104,6 +108,9 @@ struct BodyState {
   double r = 0, ax[3] = {0, 0, 0};
   double vel[3] = {0, 0, 0}, omega[3] = {0, 0, 0};
   double old_pos[3] = {0, 0, 0}, old_quat[4] = {1, 0, 0, 0};
+  // free degrees of freedom: velocities from the fluid momentum
+  // (!bForcedInSimFrame[d], !bBlockRotation[d]); the others keep vel / omega
+  int free_t[3] = {0, 0, 0}, free_r[3] = {0, 0, 0};
 };
 
 struct Fields {
@@ -181,6 +188,12 @@ int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const dou
 void body_record(cup_ctx* c, int kind, bool on_device, const double* ctr, const double* r, const double* q,
                  const double* vel, const double* omega);
 bool body_moves(const cup_ctx* c);
+// The body has a free degree of freedom (UpdateObstacles runs every step).
+bool body_free(const cup_ctx* c);
+// UpdateObstacles (ObstaclesUpdate.cpp:189-216): momentum integrals over the
+// body, Obstacle::computeVelocities, the new kinematics on the device.
+// out (may be null): translational and angular velocity, force, torque.
+int update_obstacles(cup_ctx* c, double dt, double out[12]);
 void body_coef_u(cup_ctx* c, int step, double dt);
 int body_advance(cup_ctx* c, int step, double dt);
 // Fetches the host copies of a device-created obstacle (no-op otherwise).

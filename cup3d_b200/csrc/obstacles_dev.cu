@@ -221,6 +221,128 @@ __global__ void __launch_bounds__(BN) k_obst_kin(const double* __restrict__ mom,
   }
 }
 
+// ---- UpdateObstacles ------------------------------------------------------
+constexpr int kMomQ = 29;  // momentum integrals per slot (13 explicit + 16 implicit)
+
+// Per slot s, the integrals of KernelIntegrateFluidMomenta
+// (ObstaclesUpdate.cpp:25-126) over the cells with chi > 0, arms p taken from
+// the centre of mass kin[0..2]:
+//   q[0] V, q[1..3] momentum, q[4..6] angular momentum, q[7..12] J0..J5,
+//   implicit penalization: q[13] penalM, q[14..16] sum pf p, q[17..22] the
+//   pf-weighted J, q[23..25] sum pf (u - udef), q[26..28] sum pf p x (u - udef),
+//   with pf = dv lambda dt X1 / (1 + X1 lambda dt), X1 = (chi > 0.5).
+__global__ void __launch_bounds__(BN) k_obst_momenta(DevMesh M, const int* __restrict__ block_of_slot,
+                                                      const double* __restrict__ chi,
+                                                      const double* __restrict__ udef, int nslots,
+                                                      const double* __restrict__ vel, const double* __restrict__ kin,
+                                                      double lambdt, int implicit, double* __restrict__ qslot) {
+  __shared__ double sm[16][kMomQ];
+  const int s = blockIdx.x, t = threadIdx.x;
+  const int b = block_of_slot[s];
+  const size_t n = size_t(M.nb) * BN;
+  double q[kMomQ];
+#pragma unroll
+  for (int k = 0; k < kMomQ; ++k) q[k] = 0.0;
+  const double X = chi[size_t(s) * BN + t];
+  if (X > 0) {
+    const double h = M.h[b], dv = h * h * h;
+    const int ix = t & 7, iy = (t >> 3) & 7, iz = t >> 6;
+    const double p[3] = {(M.index[3 * b] * 8 + ix + 0.5) * h - kin[0], (M.index[3 * b + 1] * 8 + iy + 0.5) * h - kin[1],
+                         (M.index[3 * b + 2] * 8 + iz + 0.5) * h - kin[2]};
+    double u[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) u[d] = vel[d * n + size_t(b) * BN + t];
+    const double Xdv = X * dv;
+    q[0] = Xdv;
+    q[1] = Xdv * u[0];
+    q[2] = Xdv * u[1];
+    q[3] = Xdv * u[2];
+    q[4] = Xdv * (p[1] * u[2] - p[2] * u[1]);
+    q[5] = Xdv * (p[2] * u[0] - p[0] * u[2]);
+    q[6] = Xdv * (p[0] * u[1] - p[1] * u[0]);
+    q[7] = Xdv * (p[1] * p[1] + p[2] * p[2]);
+    q[8] = Xdv * (p[0] * p[0] + p[2] * p[2]);
+    q[9] = Xdv * (p[0] * p[0] + p[1] * p[1]);
+    q[10] = -Xdv * p[0] * p[1];
+    q[11] = -Xdv * p[0] * p[2];
+    q[12] = -Xdv * p[1] * p[2];
+    if (implicit) {
+      const double X1 = X > 0.5 ? 1.0 : 0.0;
+      const double pf = dv * lambdt * X1 / (1 + X1 * lambdt);
+      double du[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) du[d] = u[d] - udef[(d * size_t(nslots) + s) * BN + t];
+      q[13] = pf;
+      q[14] = pf * p[0];
+      q[15] = pf * p[1];
+      q[16] = pf * p[2];
+      q[17] = pf * (p[1] * p[1] + p[2] * p[2]);
+      q[18] = pf * (p[0] * p[0] + p[2] * p[2]);
+      q[19] = pf * (p[0] * p[0] + p[1] * p[1]);
+      q[20] = -pf * p[0] * p[1];
+      q[21] = -pf * p[0] * p[2];
+      q[22] = -pf * p[1] * p[2];
+      q[23] = pf * du[0];
+      q[24] = pf * du[1];
+      q[25] = pf * du[2];
+      q[26] = pf * (p[1] * du[2] - p[2] * du[1]);
+      q[27] = pf * (p[2] * du[0] - p[0] * du[2]);
+      q[28] = pf * (p[0] * du[1] - p[1] * du[0]);
+    }
+  }
+  // fixed-order CTA sums: warp shuffles, then the 16 warp sums in order
+#pragma unroll
+  for (int k = 0; k < kMomQ; ++k) {
+    double v = q[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((t & 31) == 0) sm[t >> 5][k] = v;
+  }
+  __syncthreads();
+  if (t < kMomQ) {
+    double v = 0.0;
+    for (int w = 0; w < 16; ++w) v += sm[w][t];
+    qslot[size_t(s) * kMomQ + t] = v;
+  }
+}
+
+// Sums of the per-slot integrals in slot order (one thread per quantity).
+__global__ void k_obst_momenta_sum(const double* __restrict__ qslot, int nslots, double* __restrict__ qsum) {
+  const int k = threadIdx.x;
+  if (k >= kMomQ) return;
+  double v = 0.0;
+  for (int s = 0; s < nslots; ++s) v += qslot[size_t(s) * kMomQ + k];
+  qsum[k] = v;
+}
+
+// Solves A x = b (6x6, row-major) by LU decomposition with partial pivoting
+// (the method of gsl_linalg_LU_decomp / LU_solve).  Returns false when a
+// pivot is zero.
+static bool lu_solve6(double A[36], double b[6], double x[6]) {
+  for (int k = 0; k < 6; ++k) {
+    int piv = k;
+    for (int i = k + 1; i < 6; ++i)
+      if (std::fabs(A[i * 6 + k]) > std::fabs(A[piv * 6 + k])) piv = i;
+    if (A[piv * 6 + k] == 0.0) return false;
+    if (piv != k) {
+      for (int j = 0; j < 6; ++j) std::swap(A[k * 6 + j], A[piv * 6 + j]);
+      std::swap(b[k], b[piv]);
+    }
+    for (int i = k + 1; i < 6; ++i) {
+      const double f = A[i * 6 + k] / A[k * 6 + k];
+      A[i * 6 + k] = f;
+      for (int j = k + 1; j < 6; ++j) A[i * 6 + j] -= f * A[k * 6 + j];
+      b[i] -= f * b[k];
+    }
+  }
+  for (int i = 5; i >= 0; --i) {
+    double v = b[i];
+    for (int j = i + 1; j < 6; ++j) v -= A[i * 6 + j] * x[j];
+    x[i] = v / A[i * 6 + i];
+  }
+  return true;
+}
+
 // Device buffers of a device-created obstacle, sized for every block of the
 // mesh (the slot count is known only after k_obst_slots).
 int obst_dev_buffers(cup_ctx* c) {
@@ -319,9 +441,108 @@ void body_record(cup_ctx* c, int kind, bool on_device, const double* ctr, const 
   }
 }
 
+bool body_free(const cup_ctx* c) {
+  const BodyState& B = c->body;
+  if (B.kind < 0 || c->ob.nslots == 0) return false;
+  for (int d = 0; d < 3; ++d)
+    if (B.free_t[d] || B.free_r[d]) return true;
+  return false;
+}
+
+int update_obstacles(cup_ctx* c, double dt, double out[12]) {
+  DevObstacle& o = c->ob;
+  if (o.nslots == 0 || c->host_only) return 0;
+  if (o.q_cap < o.nslots) {
+    if (int rc = c->obst_arena.alloc(&o.d_qslot, size_t(o.nslots) * kMomQ)) return rc;
+    if (int rc = c->obst_arena.alloc(&o.d_qsum, kMomQ)) return rc;
+    o.q_cap = o.nslots;
+  }
+  const int implicit = c->cfg.implicit_penalization ? 1 : 0;
+  cudaStream_t st = c->stream;
+  {
+    ProfScope ps("obstacle_momenta", st);
+    k_obst_momenta<<<o.nslots, BN, 0, st>>>(c->dm, o.block_of_slot, o.chi, o.udef, o.nslots, c->F.vel[c->F.vcur],
+                                            c->d_scalars + SC_KIN, c->cfg.lambda * dt, implicit, o.d_qslot);
+    k_obst_momenta_sum<<<1, 32, 0, st>>>(o.d_qslot, o.nslots, o.d_qsum);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  double Mq[kMomQ];
+  CUP_CUDA_TRY(stream_d2h(st, Mq, o.d_qsum, sizeof(Mq)));
+  // kernelFinalizeObstacleVel (ObstaclesUpdate.cpp:128-186)
+  double penalM, penalCM[3], penalJ[6], lmom[3], amom[3];
+  if (implicit) {
+    penalM = Mq[13];
+    for (int d = 0; d < 3; ++d) {
+      penalCM[d] = Mq[14 + d];
+      lmom[d] = Mq[23 + d];
+      amom[d] = Mq[26 + d];
+    }
+    for (int i = 0; i < 6; ++i) penalJ[i] = Mq[17 + i];
+  } else {
+    penalM = Mq[0];
+    for (int d = 0; d < 3; ++d) {
+      penalCM[d] = 0.0;
+      lmom[d] = Mq[1 + d];
+      amom[d] = Mq[4 + d];
+    }
+    for (int i = 0; i < 6; ++i) penalJ[i] = Mq[7 + i];
+  }
+  // Obstacle::computeVelocities (Obstacle.cpp:143-269)
+  BodyState& B = c->body;
+  double A[36] = {penalM,      0.0,         0.0,         0.0,         +penalCM[2], -penalCM[1],
+                  0.0,         penalM,      0.0,         -penalCM[2], 0.0,         +penalCM[0],
+                  0.0,         0.0,         penalM,      +penalCM[1], -penalCM[0], 0.0,
+                  0.0,         -penalCM[2], +penalCM[1], penalJ[0],   penalJ[3],   penalJ[4],
+                  +penalCM[2], 0.0,         -penalCM[0], penalJ[3],   penalJ[1],   penalJ[5],
+                  -penalCM[1], +penalCM[0], 0.0,         penalJ[4],   penalJ[5],   penalJ[2]};
+  double rhs[6] = {lmom[0], lmom[1], lmom[2], amom[0], amom[1], amom[2]};
+  for (int d = 0; d < 3; ++d) {
+    if (!B.free_t[d]) {  // forced: the row keeps its diagonal, the velocity is imposed
+      for (int j = 0; j < 6; ++j)
+        if (j != d) A[d * 6 + j] = 0.0;
+      rhs[d] = penalM * B.vel[d];
+    }
+    if (!B.free_r[d]) {  // rotation imposed (blocked rotation: omega = 0)
+      const int r = 3 + d;
+      for (int j = 0; j < 6; ++j)
+        if (j != r) A[r * 6 + j] = 0.0;
+      rhs[r] = A[r * 6 + r] * B.omega[d];
+    }
+  }
+  double x[6];
+  if (!lu_solve6(A, rhs, x)) return set_error(CUP_ERR_NAN, "UpdateObstacles: singular 6x6 momentum system");
+  const double mass = Mq[0];
+  const double J[6] = {Mq[7], Mq[8], Mq[9], Mq[10], Mq[11], Mq[12]};
+  double force[3], torque[3], dAv[3];
+  for (int d = 0; d < 3; ++d) {
+    force[d] = mass * (x[d] - B.vel[d]) / dt;
+    dAv[d] = (x[3 + d] - B.omega[d]) / dt;
+  }
+  torque[0] = J[0] * dAv[0] + J[3] * dAv[1] + J[4] * dAv[2];
+  torque[1] = J[3] * dAv[0] + J[1] * dAv[1] + J[5] * dAv[2];
+  torque[2] = J[4] * dAv[0] + J[5] * dAv[1] + J[2] * dAv[2];
+  for (int d = 0; d < 3; ++d) {
+    if (B.free_t[d]) B.vel[d] = x[d];
+    if (B.free_r[d]) B.omega[d] = x[3 + d];
+    o.kin[3 + d] = B.vel[d];
+    o.kin[6 + d] = B.omega[d];
+  }
+  CUP_CUDA_TRY(stream_h2d(st, c->d_scalars + SC_KIN + 3, o.kin + 3, 6 * sizeof(double)));
+  if (out) {
+    for (int d = 0; d < 3; ++d) {
+      out[d] = B.vel[d];
+      out[3 + d] = B.omega[d];
+      out[6 + d] = force[d];
+      out[9 + d] = torque[d];
+    }
+  }
+  return 0;
+}
+
 bool body_moves(const cup_ctx* c) {
   const BodyState& B = c->body;
   if (B.kind < 0 || c->cfg.static_obstacles || c->ob.nslots == 0) return false;
+  if (body_free(c)) return true;
   for (int d = 0; d < 3; ++d)
     if (B.vel[d] + c->cfg.uinf[d] != 0.0 || B.omega[d] != 0.0) return true;
   return false;
@@ -427,6 +648,26 @@ int cup_obstacle_sphere_dev(cup_ctx* c, const double* ctr, double r, const doubl
   set_kinematics(s, vel, omega);
   if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_sphere_dev failed");
   body_record(c, 0, true, ctr, &r, nullptr, vel, omega);
+  return 0;
+}
+
+int cup_obstacle_free(cup_ctx* c, const int32_t* free_trans, const int32_t* free_rot) {
+  if (!c || c->ncase > 1) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_free: bad arguments");
+  if (c->body.kind < 0) return ctx_fail(c, CUP_ERR_STATE, "cup_obstacle_free: no sphere or ellipsoid body");
+  for (int d = 0; d < 3; ++d) {
+    c->body.free_t[d] = free_trans && free_trans[d] ? 1 : 0;
+    c->body.free_r[d] = free_rot && free_rot[d] ? 1 : 0;
+  }
+  graph_reset(c);
+  return 0;
+}
+
+int cup_update_obstacles(cup_ctx* c, double dt, double* out12) {
+  ProfBind pb_(c);
+  if (!c || c->mesh.nb == 0 || c->host_only || !(dt > 0))
+    return ctx_fail(c, CUP_ERR_ARG, "cup_update_obstacles: bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_update_obstacles: not available on a batch of cases");
+  if (int rc = update_obstacles(c, dt, out12)) return ctx_fail(c, rc, "cup_update_obstacles failed");
   return 0;
 }
 

@@ -213,6 +213,17 @@ int cup_obstacle_ellipsoid(cup_ctx* ctx, const double* c, const double* ax, cons
 int cup_obstacle_sphere_dev(cup_ctx* ctx, const double* c, double r, const double* vel, const double* omega);
 int cup_obstacle_ellipsoid_dev(cup_ctx* ctx, const double* c, const double* ax, const double* q,
                                const double* vel, const double* omega);
+/* Free degrees of freedom of the body (1 = free): translation along x, y, z
+ * (!bForcedInSimFrame) and rotation about x, y, z (!bBlockRotation).  Free
+ * ones take their velocity from the fluid momentum in every cup_step
+ * (UpdateObstacles); the others keep the creation's velocity / angular
+ * velocity.  Bodies are created with every degree of freedom imposed. */
+int cup_obstacle_free(cup_ctx* ctx, const int32_t* free_trans, const int32_t* free_rot);
+/* UpdateObstacles (ObstaclesUpdate.cpp:189-216): the momentum integrals of the
+ * current velocity over the body and Obstacle::computeVelocities (6x6 solve).
+ * out12 (may be NULL): translational velocity[3], angular velocity[3],
+ * force[3] = mass dV/dt, torque[3] = J dOmega/dt. */
+int cup_update_obstacles(cup_ctx* ctx, double dt, double* out12);
 /* Raw obstacle data: nslots obstacle blocks, block_of_slot[nslots] (device
  * order), chi[nslots*512], udef[3*nslots*512] (component-major), kin[9] =
  * centre of mass, velocity, angular velocity.  nslots = 0 removes the body. */

@@ -184,3 +184,115 @@ def test_static_and_comoving_bodies_stay():
             _, rc, _ = ctx.step(step)
             assert rc >= 0
         _assert_same(before, _obstacle_state(ctx), 1.0)
+
+
+def _momenta_restated(ctx, lam, dt, implicit):
+    """KernelIntegrateFluidMomenta + kernelFinalizeObstacleVel
+    (ObstaclesUpdate.cpp:25-186) in numpy: the 29 integrals of the body."""
+    slot, chi, udef, kin = ctx.get_obstacle()
+    xyz, hh = ctx.cell_centres()
+    u = ctx.download("vel").reshape(3, -1)
+    ns = len(chi) // 512
+    M = np.zeros(29)
+    for b in np.where(slot >= 0)[0]:
+        s = slot[b]
+        X = chi[s * 512:(s + 1) * 512]
+        m = X > 0
+        if not m.any():
+            continue
+        p = (xyz[b * 512:(b + 1) * 512][m] - kin[:3]).T
+        dv = hh[b * 512] ** 3
+        Xd = X[m] * dv
+        ub = u[:, b * 512:(b + 1) * 512][:, m]
+        M[0] += Xd.sum()
+        M[1:4] += (Xd * ub).sum(1)
+        M[4:7] += (Xd * np.cross(p.T, ub.T).T).sum(1)
+        M[7] += (Xd * (p[1] ** 2 + p[2] ** 2)).sum()
+        M[8] += (Xd * (p[0] ** 2 + p[2] ** 2)).sum()
+        M[9] += (Xd * (p[0] ** 2 + p[1] ** 2)).sum()
+        M[10] -= (Xd * p[0] * p[1]).sum()
+        M[11] -= (Xd * p[0] * p[2]).sum()
+        M[12] -= (Xd * p[1] * p[2]).sum()
+        if implicit:
+            X1 = (X[m] > 0.5).astype(float)
+            pf = dv * lam * dt * X1 / (1 + X1 * lam * dt)
+            du = ub - np.stack([udef[(d * ns + s) * 512:(d * ns + s + 1) * 512][m] for d in range(3)])
+            M[13] += pf.sum()
+            M[14:17] += (pf * p).sum(1)
+            M[17] += (pf * (p[1] ** 2 + p[2] ** 2)).sum()
+            M[18] += (pf * (p[0] ** 2 + p[2] ** 2)).sum()
+            M[19] += (pf * (p[0] ** 2 + p[1] ** 2)).sum()
+            M[20] -= (pf * p[0] * p[1]).sum()
+            M[21] -= (pf * p[0] * p[2]).sum()
+            M[22] -= (pf * p[1] * p[2]).sum()
+            M[23:26] += (pf * du).sum(1)
+            M[26:29] += (pf * np.cross(p.T, du.T).T).sum(1)
+    return M, kin
+
+
+def _velocities_restated(M, kin, implicit, free_t, free_r, dt):
+    """Obstacle::computeVelocities (Obstacle.cpp:143-269) with numpy's solver."""
+    if implicit:
+        pm, cm, J, lm, am = M[13], M[14:17], M[17:23], M[23:26], M[26:29]
+    else:
+        pm, cm, J, lm, am = M[0], np.zeros(3), M[7:13], M[1:4], M[4:7]
+    A = np.array([[pm, 0, 0, 0, cm[2], -cm[1]], [0, pm, 0, -cm[2], 0, cm[0]], [0, 0, pm, cm[1], -cm[0], 0],
+                  [0, -cm[2], cm[1], J[0], J[3], J[4]], [cm[2], 0, -cm[0], J[3], J[1], J[5]],
+                  [-cm[1], cm[0], 0, J[4], J[5], J[2]]], dtype=float)
+    rhs = np.concatenate([lm, am]).astype(float)
+    vel0, om0 = kin[3:6], kin[6:9]
+    for d in range(3):
+        if not free_t[d]:
+            A[d, [j for j in range(6) if j != d]] = 0
+            rhs[d] = pm * vel0[d]
+        if not free_r[d]:
+            r = 3 + d
+            A[r, [j for j in range(6) if j != r]] = 0
+            rhs[r] = A[r, r] * om0[d]
+    x = np.linalg.solve(A, rhs)
+    vel = np.where(free_t, x[:3], vel0)
+    om = np.where(free_r, x[3:], om0)
+    Jm = M[7:13]
+    dAv = (x[3:] - om0) / dt
+    torque = np.array([Jm[0] * dAv[0] + Jm[3] * dAv[1] + Jm[4] * dAv[2], Jm[3] * dAv[0] + Jm[1] * dAv[1] + Jm[5] * dAv[2],
+                       Jm[4] * dAv[0] + Jm[5] * dAv[1] + Jm[2] * dAv[2]])
+    return vel, om, M[0] * (x[:3] - vel0) / dt, torque
+
+
+@pytest.mark.parametrize("implicit,free_t,free_r", [(1, (1, 1, 1), (1, 1, 1)), (1, (1, 0, 1), (0, 0, 1)),
+                                                    (0, (1, 1, 1), (1, 1, 1))])
+def test_free_body_velocities_match_restated_momentum_integration(implicit, free_t, free_r):
+    lam, dt = 1e6, 2e-3
+    ctx = make_ctx("amr3_periodic", device=0, extra=f"-lambda {lam} -implicitPenalization {implicit}")
+    xyz, _ = ctx.cell_centres()
+    x, y, z = xyz.T
+    ctx.upload("vel", np.concatenate([np.sin(2 * np.pi * y), 0.5 * np.cos(2 * np.pi * z), 0.3 * np.sin(2 * np.pi * x)]))
+    q = np.array([0.8, 0.2, -0.4, 0.4])
+    ctx.obstacle_ellipsoid((0.55, 0.45, 0.5), (0.2, 0.12, 0.08), q / np.linalg.norm(q), vel=(0.1, -0.05, 0.02),
+                           omega=(0.3, 0.0, -0.2), on_device=True)
+    ctx.obstacle_free(free_t, free_r)
+    M, kin = _momenta_restated(ctx, lam, dt, implicit)
+    vel, om, force, torque = _velocities_restated(M, kin, implicit, np.array(free_t, bool), np.array(free_r, bool), dt)
+    out = ctx.update_obstacles(dt)
+    for key, ref in (("vel", vel), ("omega", om), ("force", force), ("torque", torque)):
+        scale = max(np.abs(ref).max(), 1e-300)
+        assert np.abs(out[key] - ref).max() <= 1e-10 * scale, (key, out[key], ref)
+    assert np.array_equal(ctx.get_obstacle()[3][3:6], out["vel"])
+
+
+def test_free_body_takes_the_uniform_flow_and_moves_with_it():
+    # a free sphere in uniform flow: its velocity becomes the flow's and
+    # cup_step carries it along (UpdateObstacles, then Obstacle::update)
+    ctx = make_ctx("amr2_free", device=0, extra="-rampup 0 -CFL 0.3 -nu 0.001")
+    n = ctx.nb * 512
+    ctx.upload("vel", np.concatenate([np.full(n, 0.3), np.zeros(n), np.zeros(n)]))
+    ctx.obstacle_sphere((0.4, 0.5, 0.5), 0.12, on_device=True)
+    ctx.obstacle_free()
+    out = ctx.update_obstacles(1e-3)
+    assert abs(out["vel"][0] - 0.3) <= 1e-12 and np.abs(out["vel"][1:]).max() <= 1e-12
+    assert np.abs(out["omega"]).max() <= 1e-10
+    chi0 = ctx.download("chi")
+    for step in range(3):
+        _, rc, _ = ctx.step(step)
+        assert rc >= 0
+    assert np.abs(ctx.download("chi") - chi0).max() > 0.1
