@@ -192,6 +192,16 @@ class Context:
         check(lib().cup_update_obstacles(self._p, dt, dptr(out)), self._p)
         return {"vel": out[0:3], "omega": out[3:6], "force": out[6:9], "torque": out[9:12]}
 
+    def write_restart(self, directory, step, time):
+        """Restart files of step `step` in `directory` (cup_write_restart)."""
+        check(lib().cup_write_restart(self._p, str(directory).encode(), step, time), self._p)
+
+    def read_restart(self, directory, step):
+        """Restores the state saved at step `step` (cup_read_restart); returns the saved time."""
+        t = np.zeros(1)
+        check(lib().cup_read_restart(self._p, str(directory).encode(), step, dptr(t)), self._p)
+        return float(t[0])
+
     def set_obstacle(self, blocks, chi, udef, kin):
         blocks = np.ascontiguousarray(blocks, np.int32)
         chi, udef, kin = (np.ascontiguousarray(x, np.float64) for x in (chi, udef, kin))

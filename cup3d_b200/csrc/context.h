@@ -108,6 +108,7 @@ struct BodyState {
   double r = 0, ax[3] = {0, 0, 0};
   double vel[3] = {0, 0, 0}, omega[3] = {0, 0, 0};
   double old_pos[3] = {0, 0, 0}, old_quat[4] = {1, 0, 0, 0};
+  double abs_pos[3] = {0, 0, 0}, old_abs_pos[3] = {0, 0, 0};  // position in the lab frame (absPos)
   // free degrees of freedom: velocities from the fluid momentum
   // (!bForcedInSimFrame[d], !bBlockRotation[d]); the others keep vel / omega
   int free_t[3] = {0, 0, 0}, free_r[3] = {0, 0, 0};

@@ -429,7 +429,7 @@ void body_record(cup_ctx* c, int kind, bool on_device, const double* ctr, const 
   B.kind = kind;
   B.on_device = on_device;
   for (int d = 0; d < 3; ++d) {
-    B.pos[d] = B.old_pos[d] = ctr[d];
+    B.pos[d] = B.old_pos[d] = B.abs_pos[d] = B.old_abs_pos[d] = ctr[d];
     B.vel[d] = vel ? vel[d] : 0.0;
     B.omega[d] = omega ? omega[d] : 0.0;
   }
@@ -573,7 +573,9 @@ static void body_update(BodyState& B, const double uinf[3], int step, int step_2
   if (step < step_2nd_start) {
     for (int d = 0; d < 3; ++d) {
       B.old_pos[d] = B.pos[d];
+      B.old_abs_pos[d] = B.abs_pos[d];
       B.pos[d] += dt * (B.vel[d] + uinf[d]);
+      B.abs_pos[d] += dt * B.vel[d];
     }
     for (int i = 0; i < 4; ++i) {
       B.old_quat[i] = q[i];
@@ -581,16 +583,21 @@ static void body_update(BodyState& B, const double uinf[3], int step, int step_2
     }
   } else {
     const double aux = 1.0 / coef[0];
-    double tp[3], tq[4];
+    double tp[3], ta[3], tq[4];
     for (int d = 0; d < 3; ++d) {
       tp[d] = B.pos[d];
+      ta[d] = B.abs_pos[d];
       B.pos[d] = aux * (dt * (B.vel[d] + uinf[d]) + (-coef[1] * B.pos[d] - coef[2] * B.old_pos[d]));
+      B.abs_pos[d] = aux * (dt * B.vel[d] + (-coef[1] * B.abs_pos[d] - coef[2] * B.old_abs_pos[d]));
     }
     for (int i = 0; i < 4; ++i) {
       tq[i] = q[i];
       q[i] = aux * (dt * dqdt[i] + (-coef[1] * q[i] - coef[2] * B.old_quat[i]));
     }
-    for (int d = 0; d < 3; ++d) B.old_pos[d] = tp[d];
+    for (int d = 0; d < 3; ++d) {
+      B.old_pos[d] = tp[d];
+      B.old_abs_pos[d] = ta[d];
+    }
     for (int i = 0; i < 4; ++i) B.old_quat[i] = tq[i];
   }
   const double invD = 1.0 / std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);

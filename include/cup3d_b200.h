@@ -232,6 +232,18 @@ int cup_set_obstacle(cup_ctx* ctx, int32_t nslots, const int32_t* block_of_slot,
 /* Reads back the obstacle data; returns nslots (arrays may be NULL to query). */
 int cup_get_obstacle(const cup_ctx* ctx, int32_t* block_of_slot, double* chi, double* udef, double* kin);
 
+/* ---- restart files (Simulation::serialize / deserialize) ---- */
+/* Writes dir/field.restart and dir/shape_0.restart in the reference's text
+ * formats (SimulationData.cpp:200-250, Obstacle.cpp:443-472; the body file
+ * adds the shape after the reference's keys) and dir/restart_<step>.cupf with
+ * the leaves, velocity and pressure (the reference's HDF5 dumps; no HDF5 here). */
+int cup_write_restart(cup_ctx* ctx, const char* dir, int32_t step, double time);
+/* Reads them back: mesh from the leaves, fields, uinf, the previous dt, the
+ * body with its pose history and its chi; *time (may be NULL) = the saved
+ * time.  Stepping on from step + 1... gives the results of the uninterrupted
+ * run bit for bit. */
+int cup_read_restart(cup_ctx* ctx, const char* dir, int32_t step, double* time);
+
 /* ---- the time-step operators (Operator::operator()(dt) of the reference) ---- */
 int cup_max_u(cup_ctx* ctx, double* umax);                          /* findMaxU */
 /* calcMaxTimestep (Simulation.cpp:309-375) for `step`: dt from max|u+uinf|. */
