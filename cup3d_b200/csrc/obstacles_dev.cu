@@ -451,7 +451,7 @@ bool body_free(const cup_ctx* c) {
 
 int update_obstacles(cup_ctx* c, double dt, double out[12]) {
   DevObstacle& o = c->ob;
-  if (o.nslots == 0 || c->host_only) return 0;
+  if (o.nslots == 0 || c->host_only || c->body.kind < 0) return 0;  // no body, or raw obstacle data
   if (o.q_cap < o.nslots) {
     if (int rc = c->obst_arena.alloc(&o.d_qslot, size_t(o.nslots) * kMomQ)) return rc;
     if (int rc = c->obst_arena.alloc(&o.d_qsum, kMomQ)) return rc;
@@ -666,6 +666,18 @@ int cup_obstacle_free(cup_ctx* c, const int32_t* free_trans, const int32_t* free
     c->body.free_r[d] = free_rot && free_rot[d] ? 1 : 0;
   }
   graph_reset(c);
+  return 0;
+}
+
+int cup_create_obstacles(cup_ctx* c, double dt, int32_t step) {
+  ProfBind pb_(c);
+  if (!c || c->mesh.nb == 0 || c->host_only || !(dt > 0))
+    return ctx_fail(c, CUP_ERR_ARG, "cup_create_obstacles: bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_create_obstacles: not available on a batch of cases");
+  body_coef_u(c, step, dt);
+  c->dt_prev = dt;
+  if (body_moves(c))
+    if (int rc = body_advance(c, step, dt)) return ctx_fail(c, rc, "cup_create_obstacles failed");
   return 0;
 }
 

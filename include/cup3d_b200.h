@@ -219,6 +219,10 @@ int cup_obstacle_ellipsoid_dev(cup_ctx* ctx, const double* c, const double* ax, 
  * (UpdateObstacles); the others keep the creation's velocity / angular
  * velocity.  Bodies are created with every degree of freedom imposed. */
 int cup_obstacle_free(cup_ctx* ctx, const int32_t* free_trans, const int32_t* free_rot);
+/* CreateObstacles (ObstaclesCreate.cpp:303-323) for the step `step` of length
+ * dt: the body's pose advanced by Obstacle::update and its chi re-created,
+ * when it moves (see static_obstacles); cup_step does this itself. */
+int cup_create_obstacles(cup_ctx* ctx, double dt, int32_t step);
 /* UpdateObstacles (ObstaclesUpdate.cpp:189-216): the momentum integrals of the
  * current velocity over the body and Obstacle::computeVelocities (6x6 solve).
  * out12 (may be NULL): translational velocity[3], angular velocity[3],

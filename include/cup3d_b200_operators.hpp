@@ -66,6 +66,31 @@ class AdvectionDiffusion : public Operator {
   std::string getName() override { return "AdvectionDiffusion"; }
 };
 
+// CreateObstacles (ObstaclesCreate.cpp:303-323): a moving body's pose and chi.
+class CreateObstacles : public Operator {
+ public:
+  using Operator::Operator;
+  void operator()(Real dt) override {
+    if (!sim.has_obstacle) return;
+    check(cup_create_obstacles(sim.ctx, dt, sim.step), sim.ctx);
+  }
+  std::string getName() override { return "CreateObstacles"; }
+};
+
+// UpdateObstacles (ObstaclesUpdate.cpp:189-216): velocities of the free
+// degrees of freedom from the fluid momentum; body_state = velocity, angular
+// velocity, force, torque.
+class UpdateObstacles : public Operator {
+ public:
+  using Operator::Operator;
+  std::array<Real, 12> body_state{};
+  void operator()(Real dt) override {
+    if (!sim.has_obstacle) return;
+    check(cup_update_obstacles(sim.ctx, dt, body_state.data()), sim.ctx);
+  }
+  std::string getName() override { return "UpdateObstacles"; }
+};
+
 class Penalization : public Operator {
  public:
   using Operator::Operator;
@@ -108,15 +133,18 @@ class PressureProjection : public Operator {
   std::string getName() override { return "PressureProjection"; }
 };
 
-// The time-step driver restricted to the hot path (Simulation.cpp:300-412):
-// mesh adaptation and obstacle creation stay with the caller.
+// The time-step driver restricted to the hot path (Simulation.cpp:300-412),
+// with the reference's operator order (Simulation.cpp:186-215); mesh
+// adaptation stays with the caller.
 class Simulation {
  public:
   SimulationData sim;
   std::vector<std::shared_ptr<Operator>> pipeline;
 
   explicit Simulation(const std::string& flags) : sim(flags) {
+    pipeline.push_back(std::make_shared<CreateObstacles>(sim));
     pipeline.push_back(std::make_shared<AdvectionDiffusion>(sim));
+    pipeline.push_back(std::make_shared<UpdateObstacles>(sim));
     pipeline.push_back(std::make_shared<Penalization>(sim));
     pipeline.push_back(std::make_shared<PressureProjection>(sim));
   }
