@@ -192,6 +192,12 @@ class Context:
         check(lib().cup_update_obstacles(self._p, dt, dptr(out)), self._p)
         return {"vel": out[0:3], "omega": out[3:6], "force": out[6:9], "torque": out[9:12]}
 
+    def dissipation(self):
+        """ComputeDissipation's 20 diagnostics of the current state (cup_compute_dissipation)."""
+        out = np.zeros(20)
+        check(lib().cup_compute_dissipation(self._p, dptr(out)), self._p)
+        return out
+
     def write_restart(self, directory, step, time):
         """Restart files of step `step` in `directory` (cup_write_restart)."""
         check(lib().cup_write_restart(self._p, str(directory).encode(), step, time), self._p)

@@ -86,6 +86,8 @@ int ctx_upload_mesh(cup_ctx* c) {
 int ctx_alloc_fields(cup_ctx* c) {
   graph_reset(c);
   c->field_arena.release();
+  c->d_diag = nullptr;
+  c->diag_cap = 0;
   c->obst_arena.release();
   c->ob = DevObstacle();
   const size_t n = nbn(c);

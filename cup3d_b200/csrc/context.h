@@ -159,6 +159,8 @@ struct cup_ctx {
   // moving bodies: pose, the previous step's dt and the BDF2 coefficients of
   // the pose update (SimulationData::coefU)
   cup3d::BodyState body;
+  double* d_diag = nullptr;  // ComputeDissipation partial sums (field arena)
+  int diag_cap = 0;
   double dt_prev = 0.0;
   double coef_u[3] = {1.5, -2.0, 0.5};
 };

@@ -236,6 +236,14 @@ int cup_set_obstacle(cup_ctx* ctx, int32_t nslots, const int32_t* block_of_slot,
 /* Reads back the obstacle data; returns nslots (arrays may be NULL to query). */
 int cup_get_obstacle(const cup_ctx* ctx, int32_t* block_of_slot, double* chi, double* udef, double* kin);
 
+/* ---- diagnostics ---- */
+/* ComputeDissipation (ComputeDissipation.cpp:17-140) of the current velocity,
+ * pressure and chi: out20 = circulation[3], linear impulse[3], linear
+ * momentum[3], angular impulse[3], angular momentum[3], pressure power,
+ * viscous power, helicity, kinetic energy, enstrophy (the columns of the
+ * reference's diagnostics.dat after step and time). */
+int cup_compute_dissipation(cup_ctx* ctx, double* out20);
+
 /* ---- restart files (Simulation::serialize / deserialize) ---- */
 /* Writes dir/field.restart and dir/shape_0.restart in the reference's text
  * formats (SimulationData.cpp:200-250, Obstacle.cpp:443-472; the body file

@@ -49,6 +49,7 @@ SIG = {
                                     C.c_int, C.c_double, C.c_double, _D, _D]),
     "orc_pressure_rhs": (None, [C.c_void_p, _D, _D, _D, _I, C.c_int, _D, _D, C.c_double, C.c_int, _D]),
     "orc_grad_update": (None, [C.c_void_p, _D, _D, C.c_double]),
+    "orc_dissipation": (None, [C.c_void_p, _D, _D, _D, C.c_double, _D]),
     "orc_cnn_nparam": (C.c_int, [C.c_int]),
     "orc_cnn_fwd_grad": (None, [C.c_int, C.c_int, _D, _F, _F, _F, _D, _D]),
 }
@@ -217,6 +218,16 @@ class Mesh:
                                _d(None if udef_o is None else np.ascontiguousarray(udef_o, np.float64)),
                                dt, step, _d(lhs))
         return lhs
+
+    def dissipation(self, vel, pres, chi, nu):
+        """The 20 diagnostics of ComputeDissipation (circulation, linear impulse,
+        linear momentum, angular impulse, angular momentum, pressure and viscous
+        power, helicity, kinetic energy, enstrophy)."""
+        out = np.zeros(20)
+        lib().orc_dissipation(self._p, _d(np.ascontiguousarray(vel, np.float64)),
+                              _d(np.ascontiguousarray(pres, np.float64)),
+                              _d(None if chi is None else np.ascontiguousarray(chi, np.float64)), nu, _d(out))
+        return out
 
     def grad_update(self, vel, pres, dt):
         vel = np.array(vel, np.float64)

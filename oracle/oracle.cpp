@@ -1389,6 +1389,73 @@ extern "C" void orc_grad_update(orc_mesh* m, double* vel, const double* pres, do
   grad_update(m, vel, pres, dt);
 }
 
+// ComputeDissipation's KernelDissipation (ComputeDissipation.cpp:17-109): the
+// 20 volume integrals of the diagnostics file from one-layer labs of the
+// velocity and the pressure, cell by cell in block order; positions relative
+// to the domain centre (extents / 2).
+extern "C" void orc_dissipation(orc_mesh* m, const double* vel, const double* pres, const double* chi, double nu,
+                                double* out) {
+  double Q[20] = {0};
+  const double center[3] = {0.5 * m->bpd[0] * BS * m->h0, 0.5 * m->bpd[1] * BS * m->h0,
+                            0.5 * m->bpd[2] * BS * m->h0};
+  Lab L(1, 3), P(1, 1);
+  for (int b = 0; b < m->nb; ++b) {
+    fill_lab(*m, vel, 3, 1, b, true, L);
+    fill_lab(*m, pres, 1, 1, b, false, P);
+    const double h = m->h[b];
+    const double hCube = std::pow(h, 3), inv2h = .5 / h, invHh = 1 / (h * h);
+    for (int iz = 0; iz < BS; ++iz)
+      for (int iy = 0; iy < BS; ++iy)
+        for (int ix = 0; ix < BS; ++ix) {
+          auto U = [&](int c, int dx, int dy, int dz) { return L.at(c, ix + dx, iy + dy, iz + dz); };
+          const double X = chi ? chi[int64_t(b) * BN + cell(ix, iy, iz)] : 0.0;
+          const double PX = (m->idx[b][0] * BS + ix + 0.5) * h - center[0];
+          const double PY = (m->idx[b][1] * BS + iy + 0.5) * h - center[1];
+          const double PZ = (m->idx[b][2] * BS + iz + 0.5) * h - center[2];
+          const double WX = inv2h * ((U(2, 0, 1, 0) - U(2, 0, -1, 0)) - (U(1, 0, 0, 1) - U(1, 0, 0, -1)));
+          const double WY = inv2h * ((U(0, 0, 0, 1) - U(0, 0, 0, -1)) - (U(2, 1, 0, 0) - U(2, -1, 0, 0)));
+          const double WZ = inv2h * ((U(1, 1, 0, 0) - U(1, -1, 0, 0)) - (U(0, 0, 1, 0) - U(0, 0, -1, 0)));
+          const double dPdx = inv2h * (P.at(0, ix + 1, iy, iz) - P.at(0, ix - 1, iy, iz));
+          const double dPdy = inv2h * (P.at(0, ix, iy + 1, iz) - P.at(0, ix, iy - 1, iz));
+          const double dPdz = inv2h * (P.at(0, ix, iy, iz + 1) - P.at(0, ix, iy, iz - 1));
+          double lap[3];
+          for (int c = 0; c < 3; ++c)
+            lap[c] = invHh * (U(c, 1, 0, 0) + U(c, -1, 0, 0) + U(c, 0, 1, 0) + U(c, 0, -1, 0) + U(c, 0, 0, 1) +
+                              U(c, 0, 0, -1) - 6 * U(c, 0, 0, 0));
+          const double u0 = U(0, 0, 0, 0), u1 = U(1, 0, 0, 0), u2 = U(2, 0, 0, 0);
+          const double V1 = lap[0] * u0 + lap[1] * u1 + lap[2] * u2;
+          const double D11 = inv2h * (U(0, 1, 0, 0) - U(0, -1, 0, 0));
+          const double D22 = inv2h * (U(1, 0, 1, 0) - U(1, 0, -1, 0));
+          const double D33 = inv2h * (U(2, 0, 0, 1) - U(2, 0, 0, -1));
+          const double D12 = inv2h * (U(0, 0, 1, 0) - U(0, 0, -1, 0) + U(1, 1, 0, 0) - U(1, -1, 0, 0)) / 2;
+          const double D13 = inv2h * (U(0, 0, 0, 1) - U(0, 0, 0, -1) + U(2, 1, 0, 0) - U(2, -1, 0, 0)) / 2;
+          const double D23 = inv2h * (U(2, 0, 1, 0) - U(2, 0, -1, 0) + U(1, 0, 0, 1) - U(1, 0, 0, -1)) / 2;
+          const double V2 = D11 * D11 + D22 * D22 + D33 * D33 + 2 * (D12 * D12 + D13 * D13 + D23 * D23);
+          Q[0] += hCube * WX;
+          Q[1] += hCube * WY;
+          Q[2] += hCube * WZ;
+          Q[3] += hCube / 2 * (PY * WZ - PZ * WY);
+          Q[4] += hCube / 2 * (PZ * WX - PX * WZ);
+          Q[5] += hCube / 2 * (PX * WY - PY * WX);
+          Q[6] += hCube * u0;
+          Q[7] += hCube * u1;
+          Q[8] += hCube * u2;
+          Q[9] += hCube / 3 * (PX * (PY * WY + PZ * WZ) - WX * (PY * PY + PZ * PZ));
+          Q[10] += hCube / 3 * (PY * (PX * WX + PZ * WZ) - WY * (PX * PX + PZ * PZ));
+          Q[11] += hCube / 3 * (PZ * (PX * WX + PY * WY) - WZ * (PX * PX + PY * PY));
+          Q[12] += hCube * (PY * u2 - PZ * u1);
+          Q[13] += hCube * (PZ * u0 - PX * u2);
+          Q[14] += hCube * (PX * u1 - PY * u0);
+          Q[15] -= (1 - X) * hCube * (dPdx * u0 + dPdy * u1 + dPdz * u2);
+          Q[16] += (1 - X) * hCube * nu * (V1 + 2 * V2);
+          Q[17] += hCube * (WX * u0 + WY * u1 + WZ * u2);
+          Q[18] += hCube * (u0 * u0 + u1 * u1 + u2 * u2) / 2;
+          Q[19] += hCube * std::sqrt(WX * WX + WY * WY + WZ * WZ);
+        }
+  }
+  for (int i = 0; i < 20; ++i) out[i] = Q[i];
+}
+
 extern "C" void orc_pressure_project(orc_mesh* m, double* vel, double* pres, const double* chi,
                                      const int32_t* slot, int nslots, const double* chi_o,
                                      const double* udef_o, double dt, int step, int mc, int solver,

@@ -91,6 +91,8 @@ void orc_pressure_rhs(orc_mesh* m, const double* vel, const double* pres, const 
                       const double* udef_o, double dt, int step, double* lhs);
 /* grad p update alone: vel += (-dt h^2/2 grad p + flux corr)/h^3 */
 void orc_grad_update(orc_mesh* m, double* vel, const double* pres, double dt);
+// ComputeDissipation's 20 diagnostics (ComputeDissipation.cpp:17-109).
+void orc_dissipation(orc_mesh* m, const double* vel, const double* pres, const double* chi, double nu, double* out);
 
 /* ---- learned preconditioner network (see oracle.cpp for the layout) ---- */
 int orc_cnn_nparam(int C);
