@@ -36,6 +36,8 @@ struct SimulationData {
   cup_solve_stats last_solve{};
   std::array<Real, 6> force_torque{};  // last Penalization force and torque
   bool has_obstacle = false;
+  int freqDiagnostics = 0;             // ComputeDissipation every this many steps (0: never)
+  std::array<Real, 20> diagnostics{};  // its last values (the columns of diagnostics.dat)
 
   explicit SimulationData(const std::string& flags) {
     cup_config_default(&cfg);
@@ -133,6 +135,18 @@ class PressureProjection : public Operator {
   std::string getName() override { return "PressureProjection"; }
 };
 
+// ComputeDissipation (ComputeDissipation.cpp:111-140): the 20 diagnostics
+// every freqDiagnostics steps.
+class ComputeDissipation : public Operator {
+ public:
+  using Operator::Operator;
+  void operator()(Real) override {
+    if (sim.freqDiagnostics == 0 || sim.step % sim.freqDiagnostics) return;
+    check(cup_compute_dissipation(sim.ctx, sim.diagnostics.data()), sim.ctx);
+  }
+  std::string getName() override { return "ComputeDissipation"; }
+};
+
 // The time-step driver restricted to the hot path (Simulation.cpp:300-412),
 // with the reference's operator order (Simulation.cpp:186-215); mesh
 // adaptation stays with the caller.
@@ -147,6 +161,7 @@ class Simulation {
     pipeline.push_back(std::make_shared<UpdateObstacles>(sim));
     pipeline.push_back(std::make_shared<Penalization>(sim));
     pipeline.push_back(std::make_shared<PressureProjection>(sim));
+    pipeline.push_back(std::make_shared<ComputeDissipation>(sim));
   }
   Real calcMaxTimestep() {
     Real dt = 0;

@@ -29,12 +29,16 @@ int main() {
       vel[n + b * 512 + c] = -std::cos(x) * std::sin(y) * std::cos(z);
     }
   check(cup_upload_field(S.sim.ctx, CUP_FIELD_VEL, vel.data()), S.sim.ctx);
+  S.sim.freqDiagnostics = 1;
   for (int s = 0; s < 3; ++s) {
     const Real dt = S.calcMaxTimestep();
     S.advance(dt);
     std::printf("step %d dt %.6e poisson iterations %d status %d\n", S.sim.step, dt, S.sim.last_solve.iterations,
                 S.sim.last_solve.status);
     if (S.sim.last_solve.status != 1) return 2;
+    // the decaying vortex: kinetic energy (the 19th diagnostic) below pi^3
+    std::printf("  kinetic energy %.9f\n", S.sim.diagnostics[18]);
+    if (!(S.sim.diagnostics[18] > 0.9 * 31.00627668 && S.sim.diagnostics[18] < 31.00627668)) return 7;
   }
   double umax = 0;
   check(cup_max_u(S.sim.ctx, &umax), S.sim.ctx);
