@@ -185,6 +185,17 @@ class Context:
         t, r = (np.ascontiguousarray(x, np.int32) for x in (trans, rot))
         check(lib().cup_obstacle_free(self._p, iptr(t), iptr(r)), self._p)
 
+    def obstacle_fix_frame(self, fix=(1, 0, 0)):
+        """The frame of reference follows the body along these axes (cup_obstacle_fix_frame)."""
+        f = np.ascontiguousarray(fix, np.int32)
+        check(lib().cup_obstacle_fix_frame(self._p, iptr(f)), self._p)
+
+    def uinf(self):
+        """The frame velocity in use (cup_get_uinf)."""
+        u = np.zeros(3)
+        check(lib().cup_get_uinf(self._p, dptr(u)), self._p)
+        return u
+
     def update_obstacles(self, dt):
         """UpdateObstacles (cup_update_obstacles): dict of the body's velocity,
         angular velocity, force and torque."""

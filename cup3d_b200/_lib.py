@@ -116,6 +116,8 @@ SIGNATURES = {
     "cup_obstacle_free": (C.c_int, [_P, _I, _I]),
     "cup_update_obstacles": (C.c_int, [_P, C.c_double, _D]),
     "cup_create_obstacles": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "cup_obstacle_fix_frame": (C.c_int, [_P, _I]),
+    "cup_get_uinf": (C.c_int, [_P, _D]),
     "cup_compute_dissipation": (C.c_int, [_P, _D]),
     "cup_write_restart": (C.c_int, [_P, C.c_char_p, C.c_int32, C.c_double]),
     "cup_read_restart": (C.c_int, [_P, C.c_char_p, C.c_int32, _D]),

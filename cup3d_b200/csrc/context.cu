@@ -986,6 +986,7 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_step: no mesh");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_step: not available on a batch of cases");
+  if (body_update_uinf(c)) graph_reset(c);  // CreateObstacles: the frame follows the body
   const bool moving = body_moves(c);
   if (!(dt > 0) && c->cfg.step_graph && c->cfg.poisson_solver == CUP_POISSON_B200 && !c->prof.on && !moving) {
     const int rc = graph_step(c, step, dt_used, stats);

@@ -112,6 +112,8 @@ struct BodyState {
   // free degrees of freedom: velocities from the fluid momentum
   // (!bForcedInSimFrame[d], !bBlockRotation[d]); the others keep vel / omega
   int free_t[3] = {0, 0, 0}, free_r[3] = {0, 0, 0};
+  // frame of reference following the body along these axes (bFixFrameOfRef)
+  int fix_frame[3] = {0, 0, 0};
 };
 
 struct Fields {
@@ -191,6 +193,9 @@ int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const dou
 void body_record(cup_ctx* c, int kind, bool on_device, const double* ctr, const double* r, const double* q,
                  const double* vel, const double* omega);
 bool body_moves(const cup_ctx* c);
+// ObstacleVector::updateUinf (ObstacleVector.h:74-83) for the axes the body
+// fixes: uinf = -velocity there; returns true when uinf changed.
+bool body_update_uinf(cup_ctx* c);
 // The body has a free degree of freedom (UpdateObstacles runs every step).
 bool body_free(const cup_ctx* c);
 // UpdateObstacles (ObstaclesUpdate.cpp:189-216): momentum integrals over the

@@ -539,6 +539,18 @@ int update_obstacles(cup_ctx* c, double dt, double out[12]) {
   return 0;
 }
 
+bool body_update_uinf(cup_ctx* c) {
+  const BodyState& B = c->body;
+  if (B.kind < 0 || c->ob.nslots == 0) return false;
+  bool changed = false;
+  for (int d = 0; d < 3; ++d)
+    if (B.fix_frame[d] && c->cfg.uinf[d] != -B.vel[d]) {
+      c->cfg.uinf[d] = -B.vel[d];
+      changed = true;
+    }
+  return changed;
+}
+
 bool body_moves(const cup_ctx* c) {
   const BodyState& B = c->body;
   if (B.kind < 0 || c->cfg.static_obstacles || c->ob.nslots == 0) return false;
@@ -674,10 +686,26 @@ int cup_create_obstacles(cup_ctx* c, double dt, int32_t step) {
   if (!c || c->mesh.nb == 0 || c->host_only || !(dt > 0))
     return ctx_fail(c, CUP_ERR_ARG, "cup_create_obstacles: bad arguments");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_create_obstacles: not available on a batch of cases");
+  if (body_update_uinf(c)) graph_reset(c);
   body_coef_u(c, step, dt);
   c->dt_prev = dt;
   if (body_moves(c))
     if (int rc = body_advance(c, step, dt)) return ctx_fail(c, rc, "cup_create_obstacles failed");
+  return 0;
+}
+
+int cup_obstacle_fix_frame(cup_ctx* c, const int32_t* fix) {
+  if (!c || c->ncase > 1) return ctx_fail(c, CUP_ERR_ARG, "cup_obstacle_fix_frame: bad arguments");
+  if (c->body.kind < 0) return ctx_fail(c, CUP_ERR_STATE, "cup_obstacle_fix_frame: no sphere or ellipsoid body");
+  for (int d = 0; d < 3; ++d) c->body.fix_frame[d] = fix && fix[d] ? 1 : 0;
+  body_update_uinf(c);
+  graph_reset(c);
+  return 0;
+}
+
+int cup_get_uinf(const cup_ctx* c, double* uinf) {
+  if (!c || !uinf) return ctx_fail(nullptr, CUP_ERR_ARG, "cup_get_uinf: bad arguments");
+  for (int d = 0; d < 3; ++d) uinf[d] = c->cfg.uinf[d];
   return 0;
 }
 

@@ -81,6 +81,7 @@ int write_text(cup_ctx* c, const std::string& dir, int step, double time) {
   for (int d = 0; d < 3; ++d) std::fprintf(f, "free_trans_%d: %d\n", d, B.free_t[d]);
   for (int d = 0; d < 3; ++d) std::fprintf(f, "free_rot_%d: %d\n", d, B.free_r[d]);
   std::fprintf(f, "on_device: %d\n", B.on_device ? 1 : 0);
+  for (int d = 0; d < 3; ++d) std::fprintf(f, "fix_frame_%d: %d\n", d, B.fix_frame[d]);
   return 0;
 }
 
@@ -133,6 +134,10 @@ int read_body(const std::string& dir, BodyState& B) {
     ok = ok && scan_i(f, key, &B.free_r[d]);
   }
   ok = ok && scan_i(f, "on_device: %d\n", &on_dev);
+  for (int d = 0; d < 3; ++d) {
+    std::snprintf(key, sizeof(key), "fix_frame_%d: %%d\n", d);
+    ok = ok && scan_i(f, key, &B.fix_frame[d]);
+  }
   B.on_device = on_dev != 0;
   if (!ok || (B.kind != 0 && B.kind != 1)) return set_error(CUP_ERR_ARG, ("malformed " + dir + "/shape_0.restart").c_str());
   return 0;

@@ -219,6 +219,13 @@ int cup_obstacle_ellipsoid_dev(cup_ctx* ctx, const double* c, const double* ax, 
  * (UpdateObstacles); the others keep the creation's velocity / angular
  * velocity.  Bodies are created with every degree of freedom imposed. */
 int cup_obstacle_free(cup_ctx* ctx, const int32_t* free_trans, const int32_t* free_rot);
+/* Frame of reference following the body (bFixFrameOfRef; ObstacleVector::
+ * updateUinf): along the axes with fix[d] = 1, uinf = -the body's velocity at
+ * the start of every step.  Other axes keep the configured uinf (the
+ * reference sets them to 0 whenever it updates uinf). */
+int cup_obstacle_fix_frame(cup_ctx* ctx, const int32_t* fix);
+/* The frame velocity uinf[3] in use. */
+int cup_get_uinf(const cup_ctx* ctx, double* uinf);
 /* CreateObstacles (ObstaclesCreate.cpp:303-323) for the step `step` of length
  * dt: the body's pose advanced by Obstacle::update and its chi re-created,
  * when it moves (see static_obstacles); cup_step does this itself. */

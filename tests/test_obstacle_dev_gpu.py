@@ -296,3 +296,30 @@ def test_free_body_takes_the_uniform_flow_and_moves_with_it():
         _, rc, _ = ctx.step(step)
         assert rc >= 0
     assert np.abs(ctx.download("chi") - chi0).max() > 0.1
+
+
+def test_frame_follows_a_free_body():
+    # a sphere free along x in a uniform flow u = 0.3, with the frame of
+    # reference fixed on it along x (bFixFrameOfRef): UpdateObstacles gives it
+    # the flow's velocity, the next step sets uinf_x = -0.3 (updateUinf), and
+    # the body stays where it is on the grid.  A periodic domain: on a
+    # free-space box the projection removes a uniform through-flow.
+    ctx = make_ctx("amr3_periodic", device=0, extra="-rampup 0 -CFL 0.3 -nu 0.001")
+    n = ctx.nb * 512
+    ctx.upload("vel", np.concatenate([np.full(n, 0.3), np.zeros(n), np.zeros(n)]))
+    ctx.obstacle_sphere((0.4, 0.5, 0.5), 0.12, on_device=True)
+    ctx.obstacle_free((1, 0, 0), (0, 0, 0))
+    ctx.obstacle_fix_frame((1, 0, 0))
+    assert np.array_equal(ctx.uinf(), [-0.0, 0.0, 0.0])
+    chi0 = ctx.download("chi")
+    for step in range(3):
+        _, rc, _ = ctx.step(step)
+        assert rc >= 0
+    vel = ctx.get_obstacle()[3][3:6]
+    assert abs(vel[0] - 0.3) <= 1e-3 and vel[1] == 0.0 and vel[2] == 0.0
+    u = ctx.uinf()
+    assert u[1] == 0.0 and u[2] == 0.0 and abs(u[0] + 0.3) <= 1e-3
+    # the pose moved only by the difference between the velocity of one step and
+    # the frame velocity set at the start of the next (at most the drift of one
+    # step's velocity change), far below a cell
+    assert np.abs(ctx.download("chi") - chi0).max() < 0.05
