@@ -289,9 +289,19 @@ class Context:
     def set_poisson(self, solver="b200", tol_abs=1e-6, tol_rel=1e-4, max_iter=1000):
         check(lib().cup_set_poisson(self._p, SOLVER[solver], tol_abs, tol_rel, max_iter), self._p)
 
+    def set_barrier_limit(self, cycles):
+        """Wait limit of the persistent solvers' grid barriers (0: default)."""
+        check(lib().cup_set_barrier_limit(self._p, int(cycles)), self._p)
+
     def pressure_rhs(self, dt, step):
-        """Poisson right-hand side alone, into the 'lhs' field."""
+        """Opens a split projection: the Poisson right-hand side into the 'lhs'
+        field; 'pres' is then the (zero) pressure increment that poisson_solve
+        solves for, until pressure_finish."""
         check(lib().cup_pressure_rhs(self._p, dt, step), self._p)
+
+    def pressure_finish(self, dt, step):
+        """Closes a split projection: zero mean, p += p_old, gradient update."""
+        check(lib().cup_pressure_finish(self._p, dt, step), self._p)
 
     # ---- learned preconditioner -------------------------------------------------
     @staticmethod

@@ -130,6 +130,8 @@ SIGNATURES = {
     "cup_pressure_project": (C.c_int, [_P, C.c_double, C.c_int32, C.POINTER(cup_solve_stats)]),
     "cup_step": (C.c_int, [_P, C.c_int32, C.c_double, _D, C.POINTER(cup_solve_stats)]),
     "cup_pressure_rhs": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "cup_pressure_finish": (C.c_int, [_P, C.c_double, C.c_int32]),
+    "cup_set_barrier_limit": (C.c_int, [_P, C.c_int64]),
     "cup_set_poisson": (C.c_int, [_P, C.c_int32, C.c_double, C.c_double, C.c_int32]),
     "cup_cnn_num_params": (C.c_int32, []),
     "cup_cnn_init": (C.c_int, [_P, C.c_uint64]),

@@ -264,11 +264,9 @@ int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid,
               double* mean_sum) {
   fd_init_constants();
   const size_t smem = sizeof(ApplySmem);
-  static bool attr = false;
-  if (!attr) {
+  static unsigned long long attr = 0;
+  if (first_on_device(attr))
     CUP_CUDA_TRY(cudaFuncSetAttribute(k_cnn_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    attr = true;
-  }
   ProfScope ps(sizeof(T) == 4 ? "cnn_precond_apply_f32io" : "cnn_precond_apply_f64io", s);
   k_cnn_apply<T><<<grid, NT, smem, s>>>(M, r, z, W, G, mean_sum);
   CUP_CUDA_TRY(cudaGetLastError());
@@ -563,11 +561,9 @@ static int train_launch(const CnnWeights& W, const float* in, const float* targe
                         int n, float* gpart, float* grad, float* loss_dev, float* out, int backward, int grid,
                         cudaStream_t s) {
   const size_t smem = sizeof(TrainSmem);
-  static bool attr = false;
-  if (!attr) {
+  static unsigned long long attr = 0;
+  if (first_on_device(attr))
     CUP_CUDA_TRY(cudaFuncSetAttribute(k_cnn_train, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    attr = true;
-  }
   const int g = std::max(1, std::min(grid, n));
   // loss = mean over samples and cells; gradients of that mean
   const float scale = 1.0f / (float(n) * BN);

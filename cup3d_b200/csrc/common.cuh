@@ -196,9 +196,10 @@ struct GridSync {
   unsigned int* arrive;  // arrivals since the launch (zero before it)
   double* partial;       // 2 * gridDim.x * 8
   int* error;            // set on a timed-out wait
+  long long limit;       // longest wait of one CTA at one barrier, in SM clock cycles
 };
 
-constexpr long long kBarrierClockLimit = 1ll << 31;  // SM clock cycles, about 1 s
+constexpr long long kBarrierClockLimit = 1ll << 31;  // default wait limit: about 1 s
 
 // GPU-scope release add (no result) and acquire load.
 __device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v) {
@@ -226,7 +227,7 @@ __device__ bool grid_allreduce(double (&v)[NR], const GridSync& G, unsigned int&
     const long long t0 = clock64();
     int ok = 1;
     while (ld_acquire(G.arrive) < target) {
-      if (clock64() - t0 > kBarrierClockLimit) {
+      if (clock64() - t0 > G.limit) {
         ok = 0;
         break;
       }
@@ -253,6 +254,20 @@ __device__ bool grid_allreduce(double (&v)[NR], const GridSync& G, unsigned int&
   return true;
 }
 
+}  // namespace cup3d
+
+namespace cup3d {
+// Function attributes (cudaFuncSetAttribute) hold per device: `done` keeps one
+// bit per device ordinal.  True, and marks the bit, the first time a launch
+// site asks on the current device.
+inline bool first_on_device(unsigned long long& done) {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d > 63) return true;
+  const unsigned long long bit = 1ull << d;
+  if (done & bit) return false;
+  done |= bit;
+  return true;
+}
 }  // namespace cup3d
 
 #define CUP_CUDA_TRY(expr)                                                     \

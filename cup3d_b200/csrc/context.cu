@@ -94,6 +94,7 @@ int ctx_alloc_fields(cup_ctx* c) {
   DevArena& A = c->field_arena;
   Fields& F = c->F;
   F = Fields();
+  c->proj_open = 0;
   for (int i = 0; i < 2; ++i) {
     if (int rc = A.alloc(&F.vel[i], 3 * n)) return rc;
     if (int rc = A.alloc(&F.pres[i], n)) return rc;
@@ -166,7 +167,7 @@ static double* field_ptr(cup_ctx* c, int field, int* ncomp) {
   if (c->host_only) return nullptr;
   switch (field) {
     case CUP_FIELD_VEL: *ncomp = 3; return c->F.vel[c->F.vcur];
-    case CUP_FIELD_PRES: return c->F.pres[c->F.pcur];
+    case CUP_FIELD_PRES: return c->proj_open ? c->F.phi : c->F.pres[c->F.pcur];
     case CUP_FIELD_CHI: return c->F.chi;
     case CUP_FIELD_LHS: return c->F.lhs;
     case CUP_FIELD_TMPV: *ncomp = 3; return c->F.tmpV;
@@ -268,7 +269,9 @@ int cup_config_parse(cup_config* c, const char* args) {
       if (need_num()) return CUP_ERR_ARG;
       c->poisson_tol_rel = dv;
     } else if (key == "poissonSolver") {
-      if (v == "b200") c->poisson_solver = CUP_POISSON_B200;
+      // the reference's own names ("iterative": PoissonSolverAMR, "cuda_iterative":
+      // PoissonSolverExp; PoissonSolverBase.cpp:10-32) select the plain FP64 solver
+      if (v == "b200" || v == "iterative" || v == "cuda_iterative") c->poisson_solver = CUP_POISSON_B200;
       else if (v == "b200_mixed") c->poisson_solver = CUP_POISSON_B200_MIXED;
       else if (v == "b200_learned") c->poisson_solver = CUP_POISSON_B200_LEARNED;
       else if (v == "b200_learned_mixed") c->poisson_solver = CUP_POISSON_B200_LEARNED_MIXED;
@@ -601,7 +604,7 @@ int cup_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solve_stat
 int cup_poisson_solve(cup_ctx* c, cup_solve_stats* stats) {
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_poisson_solve: no mesh");
-  return solve_impl(c, c->F.lhs, c->F.pres[c->F.pcur], stats);
+  return solve_impl(c, c->F.lhs, c->proj_open ? c->F.phi : c->F.pres[c->F.pcur], stats);
 }
 
 }  // extern "C"
@@ -718,6 +721,7 @@ static int penalize(cup_ctx* c, double dt) {
 
 static int project(cup_ctx* c, double dt, int step, cup_solve_stats* stats) {
   Fields& F = c->F;
+  c->proj_open = 0;
   double* pold = F.pres[F.pcur];
   double* pnew = F.pres[1 - F.pcur];
   if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], pold, F.chi, ob_view(c), dt, step, c->cfg.step_2nd_start,
@@ -963,11 +967,32 @@ int cup_pressure_rhs(cup_ctx* c, double dt, int32_t step) {
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_pressure_rhs: no mesh");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_pressure_rhs: not available on a batch of cases");
   Fields& F = c->F;
+  c->proj_open = 0;  // a second call starts the projection again from the same pressure
   if (int rc = launch_pressure_rhs(c->dm, F.vel[F.vcur], F.pres[F.pcur], F.chi, ob_view(c), dt, step,
                                    c->cfg.step_2nd_start, F.lhs, F.phi, kgrid(c, TG_RHS), c->stream))
     return keep(c, rc);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_rhs", __FILE__, __LINE__));
+  c->proj_open = 1;
+  return 0;
+}
+
+int cup_pressure_finish(cup_ctx* c, double dt, int32_t step) {
+  ProfBind pb_(c);
+  if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_pressure_finish: no mesh");
+  if (!c->proj_open)
+    return ctx_fail(c, CUP_ERR_STATE, "cup_pressure_finish: no projection open (call cup_pressure_rhs first)");
+  Fields& F = c->F;
+  double* pold = F.pres[F.pcur];
+  double* pnew = F.pres[1 - F.pcur];
+  if (int rc = launch_weighted_sum(c->dm, F.phi, c->d_scalars + SC_SUMS, c->W, c->stream)) return keep(c, rc);
+  if (int rc = launch_grad_update(c->dm, F.vel[F.vcur], F.phi, pold, pnew, c->d_scalars + SC_SUMS, dt, step,
+                                  c->cfg.step_2nd_start, kgrid(c, TG_GRAD), c->stream))
+    return keep(c, rc);
+  F.pcur = 1 - F.pcur;
+  c->proj_open = 0;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_finish", __FILE__, __LINE__));
   return 0;
 }
 
@@ -986,6 +1011,7 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   ProfBind pb_(c);
   if (!c || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_step: no mesh");
   if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_step: not available on a batch of cases");
+  c->proj_open = 0;
   if (body_update_uinf(c)) graph_reset(c);  // CreateObstacles: the frame follows the body
   const bool moving = body_moves(c);
   if (!(dt > 0) && c->cfg.step_graph && c->cfg.poisson_solver == CUP_POISSON_B200 && !c->prof.on && !moving) {

@@ -165,6 +165,11 @@ struct cup_ctx {
   int diag_cap = 0;
   double dt_prev = 0.0;
   double coef_u[3] = {1.5, -2.0, 0.5};
+  // A projection split at its solve (cup_pressure_rhs ... cup_pressure_finish):
+  // while open, CUP_FIELD_PRES is the pressure increment phi that the Poisson
+  // solve reads as its guess and writes, as sim.pres is in the reference
+  // between `pres = 0` and `pres += pOld` (PressureProjection.cpp:388-446).
+  int proj_open = 0;
 };
 
 namespace cup3d {

@@ -266,4 +266,11 @@ int cup_set_poisson(cup_ctx* c, int32_t solver, double tol_abs, double tol_rel, 
   return 0;
 }
 
+int cup_set_barrier_limit(cup_ctx* c, int64_t cycles) {
+  if (!c || cycles < 0) return ctx_fail(c, CUP_ERR_ARG, "cup_set_barrier_limit: bad arguments");
+  c->W.barrier_cycles = cycles;
+  graph_reset(c);  // captured steps hold the old limit
+  return 0;
+}
+
 }  // extern "C"

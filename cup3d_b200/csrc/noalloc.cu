@@ -78,14 +78,21 @@ extern "C" int cup_cnn_forward_host_noalloc(cup_ctx* c, const float* in, float* 
   if (int rc = stage_address(c->cfg.device, &stage)) return ctx_fail(c, rc, cup_last_error(nullptr));
   float* din = stage;
   float* dout = stage + size_t(kStageMaxSamples) * kInFloats;
-  cudaError_t e = cudaMemcpyAsync(din, in, size_t(n) * kInFloats * sizeof(float), cudaMemcpyHostToDevice, c->stream);
-  if (e != cudaSuccess)
-    return ctx_fail(c, set_cuda_error(e, "cnn_forward_noalloc in", __FILE__, __LINE__), cup_last_error(nullptr));
-  if (int rc = cnn_forward_batch(S.W, din, dout, n, S.gpart, S.train_grid, c->stream))
+  // Every return below happens with the lock held and, on an error after the
+  // first copy was queued, after waiting for the stream: the next call (maybe
+  // another context on another stream) must not find this call's copies or
+  // kernel still reading or writing the shared array.
+  auto fail_drained = [&](int rc) {
+    cudaStreamSynchronize(c->stream);  // its own error is the one already recorded
     return ctx_fail(c, rc, cup_last_error(nullptr));
+  };
+  cudaError_t e = cudaMemcpyAsync(din, in, size_t(n) * kInFloats * sizeof(float), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return fail_drained(set_cuda_error(e, "cnn_forward_noalloc in", __FILE__, __LINE__));
+  if (int rc = cnn_forward_batch(S.W, din, dout, n, S.gpart, S.train_grid, c->stream)) return fail_drained(rc);
   e = cudaMemcpyAsync(out, dout, size_t(n) * kOutFloats * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return fail_drained(set_cuda_error(e, "cnn_forward_noalloc out", __FILE__, __LINE__));
+  e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess)
-    return ctx_fail(c, set_cuda_error(e, "cnn_forward_noalloc out", __FILE__, __LINE__), cup_last_error(nullptr));
+    return ctx_fail(c, set_cuda_error(e, "cnn_forward_noalloc sync", __FILE__, __LINE__), cup_last_error(nullptr));
   return 0;
 }

@@ -1235,7 +1235,7 @@ __device__ bool batch_allreduce(double (&v)[NR], const BatchArgs& B, const GridS
     const long long t0 = clock64();
     int ok = 1;
     while (ld_acquire(Gs.arrive) < target) {
-      if (clock64() - t0 > kBarrierClockLimit) {
+      if (clock64() - t0 > Gs.limit) {
         ok = 0;
         break;
       }
@@ -1647,7 +1647,7 @@ static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, 
   // the arrival counter and the error flag start at zero
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
-  GridSync Gs{W.bar, W.partial, W.bar_error};
+  GridSync Gs{W.bar, W.partial, W.bar_error, W.barrier_cycles > 0 ? W.barrier_cycles : kBarrierClockLimit};
   KArgs<T> Aa = A;
   void* args[] = {(void*)&Aa, (void*)&Gs};
   ProfScope ps(name, s);
@@ -1689,7 +1689,7 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
   KArgs<double> A = make_args<double>(M, b, x, v, W, B.st, P.mean_mode, zmr, 0);
   A.ncache = KB_CACHE;
-  GridSync Gs{W.bar, W.partial, W.bar_error};
+  GridSync Gs{W.bar, W.partial, W.bar_error, W.barrier_cycles > 0 ? W.barrier_cycles : kBarrierClockLimit};
   BatchArgs Ba{B.cfirst, B.cblocks, B.part, B.case_done, B.ncase, B.groups};
   void* args[] = {(void*)&A, (void*)&Gs, (void*)&Ba};
   const size_t dyn = batch_smem(B.ncase);

@@ -50,6 +50,7 @@ struct PoissonWork {
   unsigned int* counters;   // 16
   unsigned int* bar;        // persistent solver: grid-barrier arrivals
   int* bar_error;           // persistent solver: set on a timed-out barrier wait
+  long long barrier_cycles; // persistent solvers: grid-barrier wait limit in SM cycles (0: default)
   int grid;                 // CTAs for block kernels
   int pgrid;                // CTAs of the persistent solver (set with the visit order)
   int ggrid;                // CTAs for block-group kernels (4 mesh blocks per CTA pass)

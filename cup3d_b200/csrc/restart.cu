@@ -134,9 +134,15 @@ int read_body(const std::string& dir, BodyState& B) {
     ok = ok && scan_i(f, key, &B.free_r[d]);
   }
   ok = ok && scan_i(f, "on_device: %d\n", &on_dev);
+  // fix_frame_* came later: a file without them (written before the frame of
+  // reference could follow a body) restores a body that fixes no axis
   for (int d = 0; d < 3; ++d) {
     std::snprintf(key, sizeof(key), "fix_frame_%d: %%d\n", d);
-    ok = ok && scan_i(f, key, &B.fix_frame[d]);
+    B.fix_frame[d] = 0;
+    if (ok && !scan_i(f, key, &B.fix_frame[d])) {
+      B.fix_frame[d] = 0;
+      break;  // end of file: the remaining axes stay 0
+    }
   }
   B.on_device = on_dev != 0;
   if (!ok || (B.kind != 0 && B.kind != 1)) return set_error(CUP_ERR_ARG, ("malformed " + dir + "/shape_0.restart").c_str());

@@ -179,20 +179,16 @@ __global__ void __launch_bounds__(NT, 3)
 int launch_advect_stage(const DevMesh& M, const double* vin, double* vout, double* tmpV, double dt, double nu,
                         const double* uinf, int scheme, int stage, int grid, cudaStream_t s) {
   const size_t smem = (3 * LabGeom<3>::V + 3 * BN) * sizeof(double);
-  static bool attr_set[2] = {false, false};
+  static unsigned long long attr_set[2] = {0, 0};
   Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
   if (scheme == 1) {
-    if (!attr_set[1]) {
+    if (first_on_device(attr_set[1]))
       CUP_CUDA_TRY(cudaFuncSetAttribute(k_advect_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      attr_set[1] = true;
-    }
     ProfScope ps("advect_stage_weno5", s);
     k_advect_stage<1><<<grid, NT, smem, s>>>(M, vin, vout, tmpV, dt, nu, ui, stage);
   } else {
-    if (!attr_set[0]) {
+    if (first_on_device(attr_set[0]))
       CUP_CUDA_TRY(cudaFuncSetAttribute(k_advect_stage<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-      attr_set[0] = true;
-    }
     ProfScope ps("advect_stage_upwind5", s);
     k_advect_stage<0><<<grid, NT, smem, s>>>(M, vin, vout, tmpV, dt, nu, ui, stage);
   }
@@ -315,11 +311,9 @@ int launch_pressure_rhs(const DevMesh& M, const double* vel, const double* pold,
                         const ObstacleView& ob, double dt, int step, int step_2nd_start, double* lhs, double* phi,
                         int grid, cudaStream_t s) {
   const size_t smem = (7 * LabGeom<1>::V + 2 * BN) * sizeof(double);
-  static bool attr = false;
-  if (!attr) {
+  static unsigned long long attr = 0;
+  if (first_on_device(attr))
     CUP_CUDA_TRY(cudaFuncSetAttribute(k_pressure_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    attr = true;
-  }
   ProfScope ps("pressure_rhs", s);
   k_pressure_rhs<<<grid, NT, smem, s>>>(M, vel, pold, chi, ob, dt, step > step_2nd_start ? 1 : 0, lhs, phi);
   CUP_CUDA_TRY(cudaGetLastError());

@@ -270,10 +270,20 @@ int cup_compute_dt(cup_ctx* ctx, int32_t step, double* dt);
 int cup_advect_diffuse(cup_ctx* ctx, double dt);                    /* AdvectionDiffusion */
 int cup_penalize(cup_ctx* ctx, double dt, double* force_torque6);   /* Penalization */
 int cup_pressure_project(cup_ctx* ctx, double dt, int32_t step, cup_solve_stats* stats);
-/* The Poisson right-hand side of PressureProjection alone (KernelPressureRHS
- * and, for step > 2, KernelDivPressure; PressureProjection.cpp:340-394) into
- * CUP_FIELD_LHS, from the current velocity, pressure, chi and body. */
+/* PressureProjection split at its Poisson solve, as the reference runs it
+ * (PressureProjection.cpp:331-468, solve() at :402):
+ *   cup_pressure_rhs    KernelPressureRHS and, for step > 2, KernelDivPressure
+ *                       (:340-394) into CUP_FIELD_LHS from the current velocity,
+ *                       pressure, chi and body; keeps the pressure as p_old and
+ *                       opens the projection: CUP_FIELD_PRES is then the
+ *                       pressure increment, zero, as sim.pres after `pres = 0`;
+ *   cup_poisson_solve   (PoissonSolverBase::solve) solves into that increment;
+ *   cup_pressure_finish zero mean, p += p_old for step > 2, KernelGradP and the
+ *                       velocity update (:404-467); closes the projection.
+ * cup_pressure_finish without an open projection returns CUP_ERR_STATE.
+ * cup_pressure_project and cup_step run all three in one call. */
 int cup_pressure_rhs(cup_ctx* ctx, double dt, int32_t step);
+int cup_pressure_finish(cup_ctx* ctx, double dt, int32_t step);
 /* One time step: AdvectionDiffusion, Penalization (if a body is set),
  * PressureProjection.  dt <= 0: computed by calcMaxTimestep; *dt_used gets it. */
 int cup_step(cup_ctx* ctx, int32_t step, double dt, double* dt_used, cup_solve_stats* stats);
@@ -281,6 +291,12 @@ int cup_step(cup_ctx* ctx, int32_t step, double dt, double* dt_used, cup_solve_s
 /* Changes the Poisson solver settings of a context (-poissonSolver,
  * -poissonTol, -poissonTolRel and the iteration cap). */
 int cup_set_poisson(cup_ctx* ctx, int32_t solver, double tol_abs, double tol_rel, int32_t max_iter);
+/* Longest wait, in SM clock cycles, of one CTA at one grid barrier of the
+ * persistent Poisson solvers (0: the default, 2^31 cycles, about a second).
+ * A wait that runs out ends the solve: every CTA leaves at its next barrier,
+ * the solve returns CUP_ERR_CUDA with "a grid barrier wait timed out", and
+ * the next solve starts afresh (the solution buffer holds partial results). */
+int cup_set_barrier_limit(cup_ctx* ctx, int64_t cycles);
 
 /* ---- learned preconditioner (no counterpart in the reference: the new slot at
  * the preconditioner call sites PoissonSolverAMR.h:183-222, BiCGSTAB.cu:526-527).

@@ -109,8 +109,9 @@ class PoissonSolverBase {
   virtual void solve() = 0;
 };
 
-// "b200", "b200_mixed", "b200_learned": RHS in sim.lhs, initial guess and
-// result in sim.pres (PoissonSolverAMR.cpp:20-21).
+// "b200", "b200_mixed", "b200_learned", "b200_learned_mixed": RHS in
+// sim.lhs, initial guess and result in sim.pres (PoissonSolverAMR.cpp:20-21).
+// The variant is the context's -poissonSolver setting.
 class PoissonSolverB200 : public PoissonSolverBase {
   SimulationData& sim;
 
@@ -119,18 +120,27 @@ class PoissonSolverB200 : public PoissonSolverBase {
   void solve() override { check(cup_poisson_solve(sim.ctx, &sim.last_solve), sim.ctx); }
 };
 
+// PoissonSolverBase.cpp:10-32: the solver named by -poissonSolver.  The
+// reference's "iterative" / "cuda_iterative" select the plain FP64 solver.
 inline std::shared_ptr<PoissonSolverBase> makePoissonSolver(SimulationData& s) {
-  if (s.poissonSolver == "b200" || s.poissonSolver == "b200_mixed" || s.poissonSolver == "b200_learned")
-    return std::make_shared<PoissonSolverB200>(s);
+  static const char* known[] = {"b200", "b200_mixed", "b200_learned", "b200_learned_mixed", "iterative",
+                                "cuda_iterative"};
+  for (const char* k : known)
+    if (s.poissonSolver == k) return std::make_shared<PoissonSolverB200>(s);
   throw std::invalid_argument("Poisson solver: \"" + s.poissonSolver + "\" unrecognized!");
 }
 
+// PressureProjection::operator() (PressureProjection.cpp:331-468): the RHS
+// and p_old, then pressureSolver->solve() on sim.lhs / sim.pres (:402), then
+// zero mean, p += p_old and the gradient update.
 class PressureProjection : public Operator {
  public:
   std::shared_ptr<PoissonSolverBase> pressureSolver;
   explicit PressureProjection(SimulationData& s) : Operator(s), pressureSolver(makePoissonSolver(s)) {}
   void operator()(Real dt) override {
-    check(cup_pressure_project(sim.ctx, dt, sim.step, &sim.last_solve), sim.ctx);
+    check(cup_pressure_rhs(sim.ctx, dt, sim.step), sim.ctx);
+    pressureSolver->solve();
+    check(cup_pressure_finish(sim.ctx, dt, sim.step), sim.ctx);
   }
   std::string getName() override { return "PressureProjection"; }
 };

@@ -46,6 +46,29 @@ int main() {
   // the decaying vortex keeps |u| <= 1 and loses energy slowly
   if (!(umax > 0.9 && umax <= 1.0)) return 3;
 
+  // makePoissonSolver for every solver name: a Simulation is built with each
+  // and steps, its projection calling pressureSolver->solve() in the middle
+  for (const char* name : {"b200", "b200_mixed", "b200_learned", "b200_learned_mixed", "iterative"}) {
+    Simulation T(std::string("-bpdx 4 -bpdy 4 -bpdz 4 -levelMax 1 -extent 6.283185307179586 -BC_x periodic "
+                             "-BC_y periodic -BC_z periodic -nu 0.01 -CFL 0.3 -rampup 0 -poissonTolRel 1e-8 "
+                             "-poissonTol 0 -poissonSolver ") + name);
+    check(cup_set_mesh_uniform(T.sim.ctx), T.sim.ctx);
+    check(cup_upload_field(T.sim.ctx, CUP_FIELD_VEL, vel.data()), T.sim.ctx);
+    if (T.sim.poissonSolver.find("learned") != std::string::npos) check(cup_cnn_init(T.sim.ctx, 5), T.sim.ctx);
+    for (int s = 0; s < 2; ++s) {
+      const Real dt = T.calcMaxTimestep();
+      T.advance(dt);
+      if (T.sim.last_solve.status != 1) {
+        std::printf("solver %s: step %d status %d\n", name, s, T.sim.last_solve.status);
+        return 8;
+      }
+    }
+    double um = 0;
+    check(cup_max_u(T.sim.ctx, &um), T.sim.ctx);
+    std::printf("solver %s: 2 steps, umax %.12f\n", name, um);
+    if (!(std::fabs(um - umax) < 0.02)) return 9;
+  }
+
   // A moving sphere: the pipeline of this layer (CreateObstacles, ...,
   // UpdateObstacles, Penalization, ...) against cup_step on a second context,
   // bit for bit.

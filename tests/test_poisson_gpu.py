@@ -157,3 +157,43 @@ def test_single_block_solve_matches_oracle():
     rc, st = ctx.poisson_solve_dev(bd, xd)
     assert rc == 0 and st["status"] == 1
     assert np.linalg.norm(xd.cpu().numpy() - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+
+
+@pytest.mark.parametrize("solver", ["b200", "b200_mixed"])
+def test_barrier_timeout_is_reported_and_context_recovers(solver):
+    # The persistent solvers' grid barriers wait a bounded time.  With the
+    # limit at one cycle a wait runs out (a CTA arrives before the others):
+    # the solve ends with an error status instead of hanging, and the next
+    # solve with the default limit is unaffected.
+    ctx = make_ctx("amr3_periodic", device=0, extra=f"-poissonTol 0 -poissonTolRel 1e-10 -poissonSolver {solver}")
+    m = oracle_mesh(ctx)
+    b = _compatible_rhs(m, 5)
+    ctx.upload("lhs", b)
+    ctx.upload("pres", np.zeros(m.n))
+    ctx.set_barrier_limit(1)
+    with pytest.raises(cup.CupError, match="grid barrier wait timed out"):
+        ctx.poisson_solve()
+    ctx.set_barrier_limit(0)
+    ctx.upload("pres", np.zeros(m.n))
+    rc, st = ctx.poisson_solve()
+    x = ctx.download("pres")
+    x_ref, _ = m.bicgstab_gpu(b, tol=0.0, tol_rel=1e-10)
+    assert rc == 0 and st["status"] == 1
+    assert np.linalg.norm(x - x_ref) <= 1e-8 * np.linalg.norm(x_ref)
+
+
+def test_barrier_timeout_in_a_captured_step():
+    # the same inside a captured time step (the persistent solver in a CUDA graph)
+    ctx = make_ctx("tgv32", device=0, extra="-nu 0.01 -CFL 0.3 -rampup 0 -poissonTol 0 -poissonTolRel 1e-8")
+    xyz, _ = ctx.cell_centres()
+    u = np.concatenate([np.sin(xyz[:, 0]) * np.cos(xyz[:, 1]) * np.cos(xyz[:, 2]),
+                        -np.cos(xyz[:, 0]) * np.sin(xyz[:, 1]) * np.cos(xyz[:, 2]), 0 * xyz[:, 0]])
+    ctx.upload("vel", u)
+    ctx.set_barrier_limit(1)
+    with pytest.raises(cup.CupError, match="grid barrier wait timed out"):
+        ctx.step(0)
+    ctx.set_barrier_limit(0)
+    ctx.upload("vel", u)
+    ctx.upload("pres", np.zeros(len(xyz)))
+    dt, rc, st = ctx.step(0)
+    assert rc == 0 and st["status"] == 1 and np.isfinite(ctx.download("vel")).all()

@@ -70,3 +70,25 @@ def test_restart_text_files_follow_the_reference_keys(tmp_path):
                      [f"old_position_{i}" for i in range(3)] + [f"old_absPos_{i}" for i in range(3)] +
                      [f"old_quaternion_{i}" for i in range(4)])
     assert (tmp_path / "restart_000000001.cupf").stat().st_size == 8 + 4 + 16 * a.nb + 32 * 512 * a.nb + 24
+
+
+def test_restart_without_fix_frame_keys_restores(tmp_path):
+    # shape_0.restart files written before the fix_frame_* keys existed: the
+    # body restores with no axis fixed, and the run continues as before
+    a = _start("ellipsoid")
+    t = 0.0
+    for step in range(2):
+        dt, rc, _ = a.step(step)
+        t += dt
+    a.write_restart(tmp_path, 2, t)
+    shape = tmp_path / "shape_0.restart"
+    lines = shape.read_text().split("\n")
+    assert any(ln.startswith("fix_frame_") for ln in lines)
+    shape.write_text("\n".join(ln for ln in lines if not ln.startswith("fix_frame_")))
+    b = make_ctx("amr2_free", device=0, extra=FLAGS)
+    assert b.read_restart(tmp_path, 2) == t
+    for step in range(2, 4):
+        (dta, _, _), (dtb, _, _) = a.step(step), b.step(step)
+        assert dta == dtb
+        for x, y in zip(_state(a), _state(b)):
+            assert np.array_equal(x, y), step

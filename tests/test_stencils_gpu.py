@@ -107,6 +107,35 @@ def test_pressure_project_matches_oracle(name, step):
     assert np.abs(got_p - ref_p).max() < 1e-9 * np.abs(ref_p).max()
 
 
+@pytest.mark.parametrize("step", [1, 5])
+def test_split_projection_equals_fused(step):
+    # PressureProjection as the reference runs it: RHS, then PoissonSolverBase::solve()
+    # on sim.lhs / sim.pres (the increment), then mean, p += p_old and gradient
+    # (PressureProjection.cpp:331-468): the same results as the fused call
+    extra = "-poissonTol 0 -poissonTolRel 1e-11"
+    outs = []
+    for split in (False, True):
+        ctx = make_ctx("amr3_mixed", device=0, extra=extra)
+        vel = smooth_velocity(ctx)
+        xyz, _ = cell_centres(ctx)
+        p0 = 0.1 * np.sin(xyz[:, 0] * 3.0) * np.cos(xyz[:, 1] * 2.0)
+        ctx.upload("vel", vel)
+        ctx.upload("pres", p0)
+        dt = 0.2 * oracle_mesh(ctx).hmin / np.abs(vel).max()
+        if split:
+            ctx.pressure_rhs(dt, step)
+            assert np.all(ctx.download("pres") == 0.0)  # the increment starts at zero
+            rc, st = ctx.poisson_solve()
+            ctx.pressure_finish(dt, step)
+        else:
+            rc, st = ctx.pressure_project(dt, step)
+        assert rc == 0 and st["status"] == 1
+        outs.append((ctx.download("vel"), ctx.download("pres")))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    with pytest.raises(Exception, match="no projection open"):
+        ctx.pressure_finish(1e-3, step)
+
+
 def test_tgv_steps_match_oracle():
     # Taylor-Green: u = sin x cos y cos z, v = -cos x sin y cos z, w = 0 on [0,2pi]^3,
     # nu = 0.01, CFL 0.3, upwind5, FP64; Poisson converged tightly on both sides
