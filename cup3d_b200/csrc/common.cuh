@@ -33,6 +33,9 @@ struct DevMesh {
   const double* __restrict__ case_dt;
   const double* __restrict__ case_sums;
   const double* __restrict__ case_kin;
+  // Error word of the staged stencil kernels: set to 1 when a wait for a
+  // block's bulk copies runs out (zero otherwise; read by the host).
+  int* kerr;
 };
 
 // Time step of block b: its case's in a batch, the device-computed one of a

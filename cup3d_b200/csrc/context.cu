@@ -58,8 +58,10 @@ static int keep(cup_ctx* c, int rc) {
 int ctx_upload_mesh(cup_ctx* c) {
   Mesh& m = c->mesh;
   c->mesh_arena.release();
-  int *fk, *fn, *ix;
+  int *fk, *fn, *ix, *kerr;
   double* h;
+  if (int rc = c->mesh_arena.alloc(&kerr, 1)) return rc;
+  CUP_CUDA_TRY(stream_zero(c->stream, kerr, sizeof(int)));
   if (int rc = c->mesh_arena.alloc(&fk, 6 * size_t(m.nb))) return rc;
   if (int rc = c->mesh_arena.alloc(&fn, 24 * size_t(m.nb))) return rc;
   if (int rc = c->mesh_arena.alloc(&ix, 3 * size_t(m.nb))) return rc;
@@ -80,6 +82,15 @@ int ctx_upload_mesh(cup_ctx* c) {
   c->dm.case_dt = nullptr;
   c->dm.case_sums = nullptr;
   c->dm.case_kin = nullptr;
+  c->dm.kerr = kerr;
+  return 0;
+}
+
+// Reads the staged kernels' error word after the stream has been synchronised.
+int ctx_check_kernels(cup_ctx* c) {
+  int e = 0;
+  CUP_CUDA_TRY(stream_d2h(c->stream, &e, c->dm.kerr, sizeof(int)));
+  if (e) return ctx_fail(c, CUP_ERR_CUDA, "stencil kernel: a wait for a block's bulk copies timed out");
   return 0;
 }
 
@@ -821,6 +832,7 @@ static int graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraph
     CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->dt, c->d_scalars + SC_GDT, sizeof(double), cudaMemcpyDeviceToHost, s));
     CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->st, c->W.st, sizeof(KrylovState), cudaMemcpyDeviceToHost, s));
     CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->bar_error, c->W.bar_error, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaMemcpyAsync(&c->gio->kerr, c->dm.kerr, sizeof(int), cudaMemcpyDeviceToHost, s));
     return 0;
   };
   solver_pdl(false);
@@ -852,6 +864,7 @@ static int graph_step(cup_ctx* c, int step, double* dt_used, cup_solve_stats* st
   F.pcur = 1 - F.pcur;
   const KrylovState& K = c->gio->st;
   if (c->gio->bar_error) return ctx_fail(c, CUP_ERR_CUDA, "persistent BiCGSTAB: a grid barrier wait timed out");
+  if (c->gio->kerr) return ctx_fail(c, CUP_ERR_CUDA, "stencil kernel: a wait for a block's bulk copies timed out");
   if (dt_used) *dt_used = c->gio->dt;
   if (!(c->gio->dt > 0)) return ctx_fail(c, CUP_ERR_NAN, "dt <= 0 or NaN (Simulation.cpp:344-347)");
   float ms = 0;
@@ -973,6 +986,7 @@ int cup_pressure_rhs(cup_ctx* c, double dt, int32_t step) {
     return keep(c, rc);
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_rhs", __FILE__, __LINE__));
+  if (int rk = ctx_check_kernels(c)) return rk;
   c->proj_open = 1;
   return 0;
 }
@@ -993,7 +1007,7 @@ int cup_pressure_finish(cup_ctx* c, double dt, int32_t step) {
   c->proj_open = 0;
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_finish", __FILE__, __LINE__));
-  return 0;
+  return ctx_check_kernels(c);
 }
 
 int cup_pressure_project(cup_ctx* c, double dt, int32_t step, cup_solve_stats* stats) {
@@ -1004,6 +1018,7 @@ int cup_pressure_project(cup_ctx* c, double dt, int32_t step, cup_solve_stats* s
   if (rc < 0) return rc;
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "pressure_project", __FILE__, __LINE__));
+  if (int rk = ctx_check_kernels(c)) return rk;
   return rc;
 }
 
@@ -1038,6 +1053,7 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   if (rc < 0) return rc;
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return keep(c, set_cuda_error(e, "step", __FILE__, __LINE__));
+  if (int rk = ctx_check_kernels(c)) return rk;
   return rc;
 }
 

@@ -96,6 +96,7 @@ struct GraphIO {
   double cfl_fac;
   double dt;
   int bar_error;
+  int kerr;  // the staged kernels' error word
   KrylovState st;
 };
 
@@ -185,6 +186,9 @@ struct ProfBind {
 int ctx_fail(cup_ctx* c, int code, const std::string& msg);
 // Uploads c->mesh and (re)allocates the fields and solver work for it.
 int ctx_upload_mesh(cup_ctx* c);
+// CUP_ERR_CUDA with a message when a staged stencil kernel reported a timed-out
+// wait (call after synchronising the context's stream).
+int ctx_check_kernels(cup_ctx* c);
 int ctx_alloc_fields(cup_ctx* c);
 // Installs an obstacle (nslots blocks with chi, udef and kinematics kin[9]).
 int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,

@@ -1,6 +1,8 @@
 // Host-side obstacle creation: see obstacles.h.
 #include "obstacles.h"
 
+#include "ellipsoid_distance.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <functional>
@@ -12,20 +14,17 @@ namespace {
 
 constexpr double kEps = std::numeric_limits<double>::epsilon();
 
-// Fills obstacle blocks from a signed distance (positive inside) and a bounding
-// box test.  chi per ObstaclesCreate.cpp:45-80 (Towers, "Finite difference
-// methods for approximating Heaviside functions", eq. 14).
+// Fills obstacle blocks from a signed distance (positive inside) on the
+// blocks whose cell-centre range meets `box` (Obstacle::create_base,
+// Obstacle.h:139-160).  chi per ObstaclesCreate.cpp:45-80 (Towers, "Finite
+// difference methods for approximating Heaviside functions", eq. 14).
 void fill_from_sdf(const Mesh& m, const std::function<double(double, double, double)>& sdf,
-                   const double box[3][2], double hsafe_factor, const double vel[3], const double omega[3],
-                   HostObstacle& out) {
+                   const double box[3][2], const double vel[3], const double omega[3], HostObstacle& out) {
   out = HostObstacle();
   out.grid_chi.assign(size_t(m.nb) * 512, 0.0);
-  double hmax = 0;
-  for (int b = 0; b < m.nb; ++b) hmax = std::max(hmax, m.h[b]);
-  const double safety = hsafe_factor * hmax;
   double mom[4] = {0, 0, 0, 0};
   for (int b = 0; b < m.nb; ++b) {
-    const double h = m.h[b];
+  const double h = m.h[b];
     double lo[3], hi[3];
     for (int d = 0; d < 3; ++d) {
       lo[d] = m.origin[3 * b + d] + 0.5 * h;          // info.pos(.., 0, 0, 0)
@@ -33,7 +32,7 @@ void fill_from_sdf(const Mesh& m, const std::function<double(double, double, dou
     }
     bool touch = true;
     for (int d = 0; d < 3; ++d) {
-      const double a = std::max(lo[d], box[d][0] - safety), c = std::min(hi[d], box[d][1] + safety);
+      const double a = std::max(lo[d], box[d][0]), c = std::min(hi[d], box[d][1]);
       touch &= c - a > 0;
     }
     if (!touch) continue;
@@ -89,14 +88,32 @@ void fill_from_sdf(const Mesh& m, const std::function<double(double, double, dou
 
 }  // namespace
 
+void sphere_fill_box(const double c[3], double r, double hmin, double box[3][2]) {
+  const double safety = (2 + 1) * hmin;
+  for (int d = 0; d < 3; ++d) {
+    box[d][0] = c[d] - (r + safety);
+    box[d][1] = c[d] + (r + safety);
+  }
+}
+
+void ellipsoid_fill_box(const double c[3], const double ax[3], double hmin, double box[3][2]) {
+  const double safety = (2 + 1) * hmin;
+  const double amax = std::max({ax[0], ax[1], ax[2]});
+  for (int d = 0; d < 3; ++d) {
+    box[d][0] = c[d] - 2 * (amax + safety);
+    box[d][1] = c[d] + 2 * (amax + safety);
+  }
+}
+
 void make_sphere(const Mesh& m, const double c[3], double r, const double vel[3], const double omega[3],
                  HostObstacle& out) {
-  const double box[3][2] = {{c[0] - r, c[0] + r}, {c[1] - r, c[1] + r}, {c[2] - r, c[2] + r}};
+  double box[3][2];
+  sphere_fill_box(c, r, m.spec.hmin, box);
   auto sdf = [&](double x, double y, double z) {
     const double dx = x - c[0], dy = y - c[1], dz = z - c[2];
     return r - std::sqrt(dx * dx + dy * dy + dz * dz);
   };
-  fill_from_sdf(m, sdf, box, kObstacleSafety, vel, omega, out);
+  fill_from_sdf(m, sdf, box, vel, omega, out);
 }
 
 void quat_rotation(const double q[4], double R[3][3]) {
@@ -110,29 +127,14 @@ void quat_rotation(const double q[4], double R[3][3]) {
 
 void make_ellipsoid(const Mesh& m, const double c[3], const double ax[3], const double q[4], const double vel[3],
                     const double omega[3], HostObstacle& out) {
-  double R[3][3];
-  quat_rotation(q, R);
-  const double rmax = std::max({ax[0], ax[1], ax[2]});
-  const double box[3][2] = {{c[0] - rmax, c[0] + rmax}, {c[1] - rmax, c[1] + rmax}, {c[2] - rmax, c[2] + rmax}};
-  // Level set f = 1 - |p/a| (normalised radius) divided by |grad| to first
-  // order: a signed-distance approximation that is exact on the surface and
-  // keeps the sign everywhere, which is what the chi formula needs within a
-  // cell of the surface.
+  double L[3][3], box[3][2];
+  quat_lab_to_body(q, L);
+  ellipsoid_fill_box(c, ax, m.spec.hmin, box);
   auto sdf = [&](double px, double py, double pz) {
-    const double d0 = px - c[0], d1 = py - c[1], d2 = pz - c[2];
-    double b[3];
-    for (int i = 0; i < 3; ++i) b[i] = R[0][i] * d0 + R[1][i] * d1 + R[2][i] * d2;  // lab -> body
-    double s = 0, g = 0;
-    for (int i = 0; i < 3; ++i) {
-      s += (b[i] / ax[i]) * (b[i] / ax[i]);
-      g += (b[i] / (ax[i] * ax[i])) * (b[i] / (ax[i] * ax[i]));
-    }
-    const double rho = std::sqrt(s);
-    if (rho < 1e-300) return std::min({ax[0], ax[1], ax[2]});
-    const double grad = std::sqrt(g) / rho;  // |grad rho|
-    return (1.0 - rho) / grad;
+    const double p[3] = {px - c[0], py - c[1], pz - c[2]};
+    return ellipsoid_signed_distance(ax, L, p);
   };
-  fill_from_sdf(m, sdf, box, kObstacleSafety, vel, omega, out);
+  fill_from_sdf(m, sdf, box, vel, omega, out);
 }
 
 }  // namespace cup3d

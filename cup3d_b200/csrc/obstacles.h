@@ -26,12 +26,17 @@ void make_sphere(const Mesh& m, const double c[3], double r, const double vel[3]
 // Rotation matrix (body -> lab) of the unit quaternion q = (w, x, y, z).
 void quat_rotation(const double q[4], double R[3][3]);
 
-// Bounding-box margin of the fill rule: (2 + 1) times the coarsest spacing.
-constexpr double kObstacleSafety = 2.0 + 1.0;
+// Fill boxes of the bodies: a block holds obstacle data when the range of its
+// cell centres meets the box (isTouching).  The margin is (2 + SURFDH) hmin,
+// SURFDH = 1 (ObstacleBlock.h:16), hmin the finest spacing the mesh may have
+// (SimulationData.cpp:162).  Sphere: centre +- (r + margin) (Sphere.cpp:22-27);
+// ellipsoid: centre +- 2 (largest semi-axis + margin) (Ellipsoid.cpp:252-258).
+void sphere_fill_box(const double c[3], double r, double hmin, double box[3][2]);
+void ellipsoid_fill_box(const double c[3], const double ax[3], double hmin, double box[3][2]);
 
 // Ellipsoid with semi-axes ax[3] rotated by quaternion q (w, x, y, z); the
-// signed distance is the ellipsoid's algebraic level set scaled to distance
-// units near the surface (see obstacles.cpp).
+// signed distance is the exact distance to the surface (Eberly's bisection,
+// ellipsoid_distance.cuh), positive inside.
 void make_ellipsoid(const Mesh& m, const double c[3], const double ax[3], const double q[4], const double vel[3],
                     const double omega[3], HostObstacle& out);
 

@@ -1,5 +1,6 @@
 // Obstacle creation on the device: the fill rule, signed distances and chi of
-// obstacles.cpp (Sphere.cpp:47-51, the ellipsoid level set, and the Towers
+// obstacles.cpp (Sphere.cpp:47-51, the ellipsoid distance of Ellipsoid.cpp:22-300
+// in ellipsoid_distance.cuh, and the Towers
 // smoothed Heaviside of KernelCharacteristicFunction, ObstaclesCreate.cpp:45-80)
 // as kernels, for bodies that are re-created without a host round trip of
 // their blocks.
@@ -25,6 +26,7 @@
 
 #include "context.h"
 #include "obstacles.h"
+#include "ellipsoid_distance.cuh"
 
 namespace cup3d {
 namespace {
@@ -36,9 +38,8 @@ struct Shape {
   double c[3];       // centre
   double r;          // sphere radius
   double ax[3];      // ellipsoid semi-axes
-  double R[3][3];    // ellipsoid rotation, body -> lab
-  double box[3][2];  // bounding box of the body
-  double safety;     // margin of the fill rule
+  double L[3][3];    // ellipsoid rotation, lab -> body
+  double box[3][2];  // fill box of the body, margin included (sphere_fill_box, ellipsoid_fill_box)
   double vel[3], omega[3];
 };
 
@@ -55,20 +56,8 @@ __device__ double shape_sdf(const Shape& s, double px, double py, double pz) {
     const double dx = px - s.c[0], dy = py - s.c[1], dz = pz - s.c[2];
     return s.r - sqrt(dx * dx + dy * dy + dz * dz);
   }
-  const double d0 = px - s.c[0], d1 = py - s.c[1], d2 = pz - s.c[2];
-  double b[3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) b[i] = s.R[0][i] * d0 + s.R[1][i] * d1 + s.R[2][i] * d2;  // lab -> body
-  double q = 0, g = 0;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    q += (b[i] / s.ax[i]) * (b[i] / s.ax[i]);
-    g += (b[i] / (s.ax[i] * s.ax[i])) * (b[i] / (s.ax[i] * s.ax[i]));
-  }
-  const double rho = sqrt(q);
-  if (rho < 1e-300) return fmin(s.ax[0], fmin(s.ax[1], s.ax[2]));
-  const double grad = sqrt(g) / rho;
-  return (1.0 - rho) / grad;
+  const double p[3] = {px - s.c[0], py - s.c[1], pz - s.c[2]};
+  return ellipsoid_signed_distance(s.ax, s.L, p);
 }
 
 __device__ __forceinline__ bool block_touches(const Shape& s, const double* origin, double h, int b) {
@@ -76,9 +65,8 @@ __device__ __forceinline__ bool block_touches(const Shape& s, const double* orig
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const double lo = origin[3 * b + d] + 0.5 * h, hi = origin[3 * b + d] + (8 - 0.5) * h;
-    const double bl = s.box[d][0] - s.safety, bh = s.box[d][1] + s.safety;
-    const double a = lo < bl ? bl : lo;  // std::max(lo, bl)
-    const double c = bh < hi ? bh : hi;  // std::min(hi, bh)
+    const double a = lo < s.box[d][0] ? s.box[d][0] : lo;  // std::max(lo, box lo)
+    const double c = s.box[d][1] < hi ? s.box[d][1] : hi;  // std::min(hi, box hi)
     touch &= c - a > 0;
   }
   return touch;
@@ -370,9 +358,6 @@ int obst_dev_buffers(cup_ctx* c) {
 int create_obstacle_dev(cup_ctx* c, Shape& s) {
   graph_reset(c);
   const Mesh& m = c->mesh;
-  double hmax = 0;
-  for (int b = 0; b < m.nb; ++b) hmax = std::max(hmax, m.h[b]);
-  s.safety = kObstacleSafety * hmax;
   if (int rc = obst_dev_buffers(c)) return rc;
   DevObstacle& o = c->ob;
   ObstResult* res = static_cast<ObstResult*>(o.d_result);
@@ -658,11 +643,8 @@ int cup_obstacle_sphere_dev(cup_ctx* c, const double* ctr, double r, const doubl
   if (int rc = shape_args_ok(c, "cup_obstacle_sphere_dev")) return rc;
   Shape s{};
   s.kind = 0;
-  for (int d = 0; d < 3; ++d) {
-    s.c[d] = ctr[d];
-    s.box[d][0] = ctr[d] - r;
-    s.box[d][1] = ctr[d] + r;
-  }
+  for (int d = 0; d < 3; ++d) s.c[d] = ctr[d];
+  sphere_fill_box(ctr, r, c->mesh.spec.hmin, s.box);
   s.r = r;
   set_kinematics(s, vel, omega);
   if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_sphere_dev failed");
@@ -725,14 +707,12 @@ int cup_obstacle_ellipsoid_dev(cup_ctx* c, const double* ctr, const double* ax, 
   if (int rc = shape_args_ok(c, "cup_obstacle_ellipsoid_dev")) return rc;
   Shape s{};
   s.kind = 1;
-  quat_rotation(q, s.R);
-  const double rmax = std::max({ax[0], ax[1], ax[2]});
+  quat_lab_to_body(q, s.L);
   for (int d = 0; d < 3; ++d) {
     s.c[d] = ctr[d];
     s.ax[d] = ax[d];
-    s.box[d][0] = ctr[d] - rmax;
-    s.box[d][1] = ctr[d] + rmax;
   }
+  ellipsoid_fill_box(ctr, ax, c->mesh.spec.hmin, s.box);
   set_kinematics(s, vel, omega);
   if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_ellipsoid_dev failed");
   body_record(c, 1, true, ctr, ax, q, vel, omega);

@@ -4,7 +4,12 @@
 // reference tree) adds, to a coarse cell next to a finer face, its own face
 // value plus the four fine face values, computed by the coarse block's CTA
 // from the fine blocks' face cells and their ghosts.
+#include <algorithm>
+#include <type_traits>
+
+#include "../../include/cup3d_b200.h"
 #include "lab.cuh"
+#include "staged.cuh"
 #include "stencils.cuh"
 #include "profiler.h"
 
@@ -130,6 +135,112 @@ __global__ void __launch_bounds__(NT, 3)
         __syncthreads();
       }
     }
+    if (SCHEME == 1) {
+      // WENO5: each face value is reconstructed once where the cells on both
+      // sides take the same upwind side.  Per direction: every cell
+      // reconstructs its upper face into fbuf; the lower faces of the first
+      // cells of the lines go to fstart; a cell then takes its lower face from
+      // the cell below, or reconstructs it itself where the upwind sign flips.
+      // The face values are those of deriv<1> (the same reconstruction of the
+      // same inputs), so the result does not change.
+      double* fbuf = corr + 3 * BN;   // 3 x 512: upper faces along the current direction
+      double* fstart = fbuf + 3 * BN; // 3 x 64: lower faces of the lines' first cells
+      auto L = [&](int c, int xx, int yy, int zz) { return lab[c * LG::V + LG::at(xx, yy, zz)]; };
+      double der[2][3][3];  // [cell slot][component][direction]
+      auto direction = [&](auto dconst) {
+        constexpr int d = decltype(dconst)::value;
+        constexpr int stride = d == 0 ? 1 : (d == 1 ? 8 : 64);
+        // reconstruction at the upper face of cell (p0, p1, p2) along d with
+        // the upwind side pos, as deriv<1>'s fp
+        auto face_up = [&](int c, int p0, int p1, int p2, bool pos) {
+          auto at = [&](int k) {
+            return L(c, p0 + (d == 0 ? k : 0), p1 + (d == 1 ? k : 0), p2 + (d == 2 ? k : 0));
+          };
+          const double um2 = at(-2), um1 = at(-1), u0 = at(0), up1 = at(1), up2 = at(2), up3 = at(3);
+          return weno5_left(pos ? um2 : up3, pos ? um1 : up2, pos ? u0 : up1, pos ? up1 : u0, pos ? up2 : um1);
+        };
+#pragma unroll 1
+        for (int qq = 0; qq < 2; ++qq) {
+          const int cell = threadIdx.x + qq * NT;
+          const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+          const bool pos = L(d, x, y, z) + ui.v[d] > 0;
+#pragma unroll 1
+          for (int c = 0; c < 3; ++c) fbuf[c * BN + cell] = face_up(c, x, y, z, pos);
+        }
+        if (threadIdx.x < 3 * 64) {
+          const int c = threadIdx.x >> 6, line = threadIdx.x & 63;
+          const int t1 = line & 7, t2 = line >> 3;
+          const int x = d == 0 ? 0 : t1, y = d == 1 ? 0 : (d == 0 ? t1 : t2), z = d == 2 ? 0 : t2;
+          const bool pos = L(d, x, y, z) + ui.v[d] > 0;  // the first cell's side
+          fstart[c * 64 + line] = face_up(c, x - (d == 0), y - (d == 1), z - (d == 2), pos);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int qq = 0; qq < 2; ++qq) {
+          const int cell = threadIdx.x + qq * NT;
+          const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+          const int pd = d == 0 ? x : (d == 1 ? y : z);
+          const bool pos = L(d, x, y, z) + ui.v[d] > 0;
+          double fm[3];
+          if (pd == 0) {
+            const int line = d == 0 ? y + 8 * z : (d == 1 ? x + 8 * z : x + 8 * y);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) fm[c] = fstart[c * 64 + line];
+          } else {
+            const int xm = x - (d == 0), ym = y - (d == 1), zm = z - (d == 2);
+            const bool pos_m = L(d, xm, ym, zm) + ui.v[d] > 0;
+            if (pos_m == pos) {
+#pragma unroll
+              for (int c = 0; c < 3; ++c) fm[c] = fbuf[c * BN + cell - stride];
+            } else {  // the upwind side flips between the two cells
+#pragma unroll
+              for (int c = 0; c < 3; ++c) fm[c] = face_up(c, xm, ym, zm, pos);
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) der[qq][c][d] = fbuf[c * BN + cell] - fm[c];
+        }
+        __syncthreads();
+      };
+      direction(std::integral_constant<int, 0>{});
+      direction(std::integral_constant<int, 1>{});
+      direction(std::integral_constant<int, 2>{});
+#pragma unroll 1
+      for (int qq = 0; qq < 2; ++qq) {
+        const int cell = threadIdx.x + qq * NT;
+        const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+        const double uA[3] = {L(0, x, y, z) + ui.v[0], L(1, x, y, z) + ui.v[1], L(2, x, y, z) + ui.v[2]};
+        double out[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double dx = der[qq][c][0], dy = der[qq][c][1], dz = der[qq][c][2];
+          const double sx = L(c, x + 1, y, z) + L(c, x - 1, y, z);
+          const double sy = L(c, x, y + 1, z) + L(c, x, y - 1, z);
+          const double sz = L(c, x, y, z + 1) + L(c, x, y, z - 1);
+          double dD, dA;
+          if (c == 0) {
+            dD = (sx + (sy + sz)) - 6 * L(0, x, y, z);
+            dA = uA[0] * dx + (uA[1] * dy + uA[2] * dz);
+          } else if (c == 1) {
+            dD = (sy + (sz + sx)) - 6 * L(1, x, y, z);
+            dA = uA[1] * dy + (uA[2] * dz + uA[0] * dx);
+          } else {
+            dD = (sz + (sx + sy)) - 6 * L(2, x, y, z);
+            dA = uA[2] * dz + (uA[0] * dx + uA[1] * dy);
+          }
+          out[c] = facA * dA + facD * dD;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const size_t gi = c * n + size_t(b) * BN + cell;
+          double tot = (stage ? tmpV[gi] : 0.0) + out[c];
+          if (fix) tot += corr[c * BN + cell];
+          vout[gi] = L(c, x, y, z) + tot * (alpha / h3);
+          if (stage < 2) tmpV[gi] = tot * beta;
+        }
+      }
+      continue;
+    }
     // the cell and component loops stay rolled: the unrolled body (18 WENO
     // reconstructions per cell) overflowed the instruction cache (the top
     // stall was no_instruction); rolled, a stage takes 188 us instead of 204
@@ -178,7 +289,8 @@ __global__ void __launch_bounds__(NT, 3)
 
 int launch_advect_stage(const DevMesh& M, const double* vin, double* vout, double* tmpV, double dt, double nu,
                         const double* uinf, int scheme, int stage, int grid, cudaStream_t s) {
-  const size_t smem = (3 * LabGeom<3>::V + 3 * BN) * sizeof(double);
+  // lab, flux correction; WENO5 adds the face buffers (3 x 512 + 3 x 64)
+  const size_t smem = (3 * LabGeom<3>::V + 3 * BN + (scheme == 1 ? 3 * BN + 3 * 64 : 0)) * sizeof(double);
   static unsigned long long attr_set[2] = {0, 0};
   Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
   if (scheme == 1) {
@@ -212,50 +324,59 @@ struct UdefGet {
   }
 };
 
-__global__ void __launch_bounds__(NT, 3)
+// One CTA walks its blocks through the staged pipeline (staged.cuh): the
+// velocity and p_old labs arrive by bulk copies and per-cell async copies
+// while the previous block is computed.  Blocks next to the body (rare) add
+// the u_def lab with plain loads.
+template <int USE_POLD>
+__global__ void __launch_bounds__(NT, 2)
     k_pressure_rhs(DevMesh M, const double* __restrict__ vel, const double* __restrict__ pold,
-                   const double* __restrict__ chi, ObstacleView ob, double dt, int use_pold, double* lhs, double* phi) {
-  extern __shared__ double smem[];
+                   const double* __restrict__ chi, ObstacleView ob, double dt, double* __restrict__ lhs,
+                   double* __restrict__ phi) {
+  extern __shared__ __align__(16) unsigned char stage_smem[];
+  constexpr int NCH = 3 + USE_POLD;
+  using SS = StagedShape<NCH, 0>;
   using LG = LabGeom<1>;
-  double* ulab = smem;
-  double* dlab = ulab + 3 * LG::V;
-  double* plab = dlab + 3 * LG::V;
-  double* corr = plab + LG::V;  // [0,512): RHS flux correction, [512,1024): div p correction
+  double* dlab = reinterpret_cast<double*>(stage_smem + SS::kBytes);
+  double* corr = dlab + 3 * LG::V;  // [0,512): RHS flux correction, [512,1024): div p correction
   const size_t n = size_t(M.nb) * BN;
+  const double* src[NCH];
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) src[c] = c < 3 ? vel + c * n : pold;
   auto getV = [&](int c, int blk, int cell) { return vel[c * n + size_t(blk) * BN + cell]; };
   auto getP = [&](int, int blk, int cell) { return pold[size_t(blk) * BN + cell]; };
   UdefGet getD{ob, chi};
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    __syncthreads();
-    const bool near = ob.near != nullptr && ob.near[b] != 0;
-    lab_fill<1, 3>(ulab, M, b, getV, true);
+  staged_blocks<NCH, 0>(M, src, ob.near, stage_smem, M.kerr, [&](int, int b, const StageMeta& m, double* ulab) {
+    double* plab = ulab + 3 * LG::V;
+    stage_fixup<3>(ulab, M, m, getV, true);
+    if (USE_POLD) stage_fixup<1>(plab, M, m, getP, false);
+    const bool near = m.flag != 0;
     if (near) lab_fill<1, 3>(dlab, M, b, getD, true);
-    if (use_pold) lab_fill<1, 1>(plab, M, b, getP, false);
-    const bool fix = has_finer(M, b);
+    const bool fix = meta_has_finer(m);
     if (fix)
       for (int i = threadIdx.x; i < 2 * BN; i += NT) corr[i] = 0.0;
     __syncthreads();
     const double dtb = block_dt(M, b, dt);
-    const double h = M.h[b], fac = 0.5 * h * h / dtb;
+    const double h = m.h, fac = 0.5 * h * h / dtb;
     auto U = [&](int c, int x, int y, int z) { return ulab[c * LG::V + LG::at(x, y, z)]; };
     auto D = [&](int c, int x, int y, int z) { return near ? dlab[c * LG::V + LG::at(x, y, z)] : 0.0; };
     auto P = [&](int x, int y, int z) { return plab[LG::at(x, y, z)]; };
     if (fix) {
       for (int f = 0; f < 6; ++f) {
-        if (M.fkind[b * 6 + f] != K_FINER) continue;
+        if (m.kind[f] != K_FINER) continue;
         const int d = f >> 1, s = f & 1;
         if (threadIdx.x < 64) {
           const int a = threadIdx.x & 7, bb = threadIdx.x >> 3;
           int q[3], g[3];
           face_lab_pair(d, s, a, bb, q, g);
-          const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
+          const int ch = m.nbr[4 * f + (a >> 2) + 2 * (bb >> 2)];
           const double hf = M.h[ch], facf = 0.5 * hf * hf / dtb;
           const int oc = face_cell(d, s, 0, a, bb);
           const double sg = s ? -1.0 : 1.0, sgc = -sg;
           const double cq = chi[size_t(b) * BN + oc];
           double vr = sg * fac * (U(d, g[0], g[1], g[2]) + U(d, q[0], q[1], q[2])) -
                       sg * cq * fac * (D(d, g[0], g[1], g[2]) + D(d, q[0], q[1], q[2]));
-          double vp = use_pold ? h * (P(q[0], q[1], q[2]) - P(g[0], g[1], g[2])) : 0.0;
+          double vp = USE_POLD ? h * (P(q[0], q[1], q[2]) - P(g[0], g[1], g[2])) : 0.0;
 #pragma unroll
           for (int e2 = 0; e2 < 2; ++e2)
 #pragma unroll
@@ -271,7 +392,7 @@ __global__ void __launch_bounds__(NT, 3)
                 gd = child_ghost1([&](int cell) { return getD(d, b, cell); }, M, ch, d, s, fa, fb);
               }
               vr += sgc * facf * (gu + uf) - sgc * cf_chi * facf * (gd + df);
-              if (use_pold) {
+              if (USE_POLD) {
                 const double pf = getP(0, ch, cf);
                 const double gp = child_ghost1([&](int cell) { return getP(0, b, cell); }, M, ch, d, s, fa, fb);
                 vp += hf * (pf - gp);
@@ -295,7 +416,7 @@ __global__ void __launch_bounds__(NT, 3)
         p += -chi[gi] * fac * divUs;
       }
       if (fix) p += corr[cell];
-      if (use_pold) {
+      if (USE_POLD) {
         double dp = h * (P(x + 1, y, z) + P(x - 1, y, z) + P(x, y + 1, z) + P(x, y - 1, z) + P(x, y, z + 1) +
                          P(x, y, z - 1) - 6.0 * P(x, y, z));
         if (fix) dp += corr[BN + cell];
@@ -304,62 +425,111 @@ __global__ void __launch_bounds__(NT, 3)
       lhs[gi] = p;
       phi[gi] = 0.0;
     }
+    __syncthreads();
+  });
+}
+
+// CTAs of a staged kernel that fit on the device at once: the pipeline wants
+// one resident wave of CTAs, each walking several blocks.
+template <class K>
+static int resident_ctas(K kern, size_t smem, unsigned long long& cached_mask, int* cache) {
+  int dev = 0;
+  CUP_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev > 63) return set_error(CUP_ERR_ARG, "device ordinal above 63");
+  if (first_on_device(cached_mask)) {
+    int per_sm = 0, sms = 0;
+    CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) return set_error(CUP_ERR_CUDA, "staged stencil kernel does not fit on an SM");
+    cache[dev] = per_sm * sms;
   }
+  return 0;
+}
+
+template <int USE_POLD>
+constexpr size_t rhs_smem() {
+  return StagedShape<3 + USE_POLD, 0>::kBytes + (3 * LabGeom<1>::V + 2 * BN) * sizeof(double);
 }
 
 int launch_pressure_rhs(const DevMesh& M, const double* vel, const double* pold, const double* chi,
                         const ObstacleView& ob, double dt, int step, int step_2nd_start, double* lhs, double* phi,
                         int grid, cudaStream_t s) {
-  const size_t smem = (7 * LabGeom<1>::V + 2 * BN) * sizeof(double);
-  static unsigned long long attr = 0;
-  if (first_on_device(attr))
-    CUP_CUDA_TRY(cudaFuncSetAttribute(k_pressure_rhs, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  static unsigned long long attr[2] = {0, 0};
+  static int resident[2][64];
+  int dev = 0;
+  CUP_CUDA_TRY(cudaGetDevice(&dev));
   ProfScope ps("pressure_rhs", s);
-  k_pressure_rhs<<<grid, NT, smem, s>>>(M, vel, pold, chi, ob, dt, step > step_2nd_start ? 1 : 0, lhs, phi);
+  if (step > step_2nd_start) {
+    if (int rc = resident_ctas(k_pressure_rhs<1>, rhs_smem<1>(), attr[1], resident[1])) return rc;
+    grid = std::max(1, std::min({grid, resident[1][dev], M.nb}));
+    k_pressure_rhs<1><<<grid, NT, rhs_smem<1>(), s>>>(M, vel, pold, chi, ob, dt, lhs, phi);
+  } else {
+    if (int rc = resident_ctas(k_pressure_rhs<0>, rhs_smem<0>(), attr[0], resident[0])) return rc;
+    grid = std::max(1, std::min({grid, resident[0][dev], M.nb}));
+    k_pressure_rhs<0><<<grid, NT, rhs_smem<0>(), s>>>(M, vel, pold, chi, ob, dt, lhs, phi);
+  }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
 
 // ---------------------------------------------------------------------------
 // Mean removal + incremental pressure (PressureProjection.cpp:404-446) fused
-// with KernelGradP (:244-323) and the velocity update (:451-467).
+// with KernelGradP (:244-323) and the velocity update (:451-467).  The
+// pressure p = phi - avg (+ p_old) is formed at the point of use from the
+// staged phi and p_old labs; the velocity comes in with them as interiors.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT, 4)
+template <int USE_POLD>
+__global__ void __launch_bounds__(NT, 3)
     k_grad_update(DevMesh M, double* vel, const double* __restrict__ phi, const double* __restrict__ pold,
-                  double* __restrict__ pnew, const double* sums, double dt, int use_pold) {
-  __shared__ double plab[LabGeom<1>::V];
-  __shared__ double corr[3 * BN];
+                  double* __restrict__ pnew, const double* sums, double dt) {
+  extern __shared__ __align__(16) unsigned char stage_smem[];
+  constexpr int NCH = 1 + USE_POLD;
+  using SS = StagedShape<NCH, 3>;
   using LG = LabGeom<1>;
+  double* corr = reinterpret_cast<double*>(stage_smem + SS::kBytes);  // 3 BN
   const size_t n = size_t(M.nb) * BN;
-  double avg = sums ? sums[0] / sums[1] : 0.0;  // the block's case's mean in a batch
-  auto getP = [&](int, int blk, int cell) {
-    const size_t i = size_t(blk) * BN + cell;
-    const double p = phi[i] - avg;
-    return use_pold ? p + pold[i] : p;
-  };
-  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
-    if (M.case_sums) {
-      const int cs = M.bcase[b];
-      avg = M.case_sums[2 * cs] / M.case_sums[2 * cs + 1];
-    }
-    __syncthreads();
-    lab_fill<1, 1>(plab, M, b, getP, false);
-    const bool fix = has_finer(M, b);
+  const double* src[NCH + 3];
+#pragma unroll
+  for (int c = 0; c < NCH; ++c) src[c] = c == 0 ? phi : pold;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) src[NCH + c] = vel + c * n;
+  auto getPhi = [&](int, int blk, int cell) { return phi[size_t(blk) * BN + cell]; };
+  auto getPold = [&](int, int blk, int cell) { return pold[size_t(blk) * BN + cell]; };
+  staged_blocks<NCH, 3>(M, src, nullptr, stage_smem, M.kerr, [&](int, int b, const StageMeta& m, double* st) {
+    double* flab = st;
+    double* olab = st + LG::V;
+    const double* vin = st + NCH * LG::V;
+    const double avg = M.case_sums ? M.case_sums[2 * M.bcase[b]] / M.case_sums[2 * M.bcase[b] + 1]
+                                   : (sums ? sums[0] / sums[1] : 0.0);
+    // the pressure of any cell of the mesh (coarse-fine flux correction)
+    auto getP = [&](int, int blk, int cell) {
+      const size_t i = size_t(blk) * BN + cell;
+      const double p = phi[i] - avg;
+      return USE_POLD ? p + pold[i] : p;
+    };
+    stage_fixup<1>(flab, M, m, getPhi, false);
+    if (USE_POLD) stage_fixup<1>(olab, M, m, getPold, false);
+    const bool fix = meta_has_finer(m);
     if (fix)
       for (int i = threadIdx.x; i < 3 * BN; i += NT) corr[i] = 0.0;
     __syncthreads();
     const double dtb = block_dt(M, b, dt);
-    const double h = M.h[b], fac = -0.5 * dtb * h * h;
-    auto P = [&](int x, int y, int z) { return plab[LG::at(x, y, z)]; };
+    const double h = m.h, fac = -0.5 * dtb * h * h;
+    auto P = [&](int x, int y, int z) {
+      const int i = LG::at(x, y, z);
+      const double p = flab[i] - avg;
+      return USE_POLD ? p + olab[i] : p;
+    };
     if (fix) {
       for (int f = 0; f < 6; ++f) {
-        if (M.fkind[b * 6 + f] != K_FINER) continue;
+        if (m.kind[f] != K_FINER) continue;
         const int d = f >> 1, s = f & 1;
         if (threadIdx.x < 64) {
           const int a = threadIdx.x & 7, bb = threadIdx.x >> 3;
           int q[3], g[3];
           face_lab_pair(d, s, a, bb, q, g);
-          const int ch = M.fnbr[b * 24 + 4 * f + (a >> 2) + 2 * (bb >> 2)];
+          const int ch = m.nbr[4 * f + (a >> 2) + 2 * (bb >> 2)];
           const double hf = M.h[ch], facf = -0.5 * dtb * hf * hf;
           const double sg = s ? -1.0 : 1.0, sgc = -sg;
           double v = sg * fac * (P(g[0], g[1], g[2]) + P(q[0], q[1], q[2]));
@@ -391,18 +561,36 @@ __global__ void __launch_bounds__(NT, 4)
         g1 += corr[BN + cell];
         g2 += corr[2 * BN + cell];
       }
-      vel[gi] += ih3 * g0;
-      vel[n + gi] += ih3 * g1;
-      vel[2 * n + gi] += ih3 * g2;
+      vel[gi] = vin[cell] + ih3 * g0;
+      vel[n + gi] = vin[BN + cell] + ih3 * g1;
+      vel[2 * n + gi] = vin[2 * BN + cell] + ih3 * g2;
       pnew[gi] = P(x, y, z);
     }
-  }
+    __syncthreads();
+  });
+}
+
+template <int USE_POLD>
+constexpr size_t grad_smem() {
+  return StagedShape<1 + USE_POLD, 3>::kBytes + 3 * BN * sizeof(double);
 }
 
 int launch_grad_update(const DevMesh& M, double* vel, const double* phi, const double* pold, double* pnew,
                        const double* sums, double dt, int step, int step_2nd_start, int grid, cudaStream_t s) {
+  static unsigned long long attr[2] = {0, 0};
+  static int resident[2][64];
+  int dev = 0;
+  CUP_CUDA_TRY(cudaGetDevice(&dev));
   ProfScope ps("grad_update", s);
-  k_grad_update<<<grid, NT, 0, s>>>(M, vel, phi, pold, pnew, sums, dt, step > step_2nd_start ? 1 : 0);
+  if (step > step_2nd_start) {
+    if (int rc = resident_ctas(k_grad_update<1>, grad_smem<1>(), attr[1], resident[1])) return rc;
+    grid = std::max(1, std::min({grid, resident[1][dev], M.nb}));
+    k_grad_update<1><<<grid, NT, grad_smem<1>(), s>>>(M, vel, phi, pold, pnew, sums, dt);
+  } else {
+    if (int rc = resident_ctas(k_grad_update<0>, grad_smem<0>(), attr[0], resident[0])) return rc;
+    grid = std::max(1, std::min({grid, resident[0][dev], M.nb}));
+    k_grad_update<0><<<grid, NT, grad_smem<0>(), s>>>(M, vel, phi, pold, pnew, sums, dt);
+  }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }

@@ -50,6 +50,7 @@ SIG = {
     "orc_pressure_rhs": (None, [C.c_void_p, _D, _D, _D, _I, C.c_int, _D, _D, C.c_double, C.c_int, _D]),
     "orc_grad_update": (None, [C.c_void_p, _D, _D, C.c_double]),
     "orc_dissipation": (None, [C.c_void_p, _D, _D, _D, C.c_double, _D]),
+    "orc_create_obstacle": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _I, _I, _D, _D, _D]),
     "orc_cnn_nparam": (C.c_int, [C.c_int]),
     "orc_cnn_fwd_grad": (None, [C.c_int, C.c_int, _D, _F, _F, _F, _D, _D]),
 }
@@ -228,6 +229,25 @@ class Mesh:
                               _d(np.ascontiguousarray(pres, np.float64)),
                               _d(None if chi is None else np.ascontiguousarray(chi, np.float64)), nu, _d(out))
         return out
+
+    def create_obstacle(self, kind, centre, shape, quat=(1.0, 0.0, 0.0, 0.0)):
+        """CreateObstacles' chi for a sphere (kind "sphere", shape = radius) or an
+        ellipsoid (kind "ellipsoid", shape = semi-axes, quat = (w, x, y, z)).
+        Returns dict(slot[nb], block_of_slot[ns], chi_o[ns*512], chi[nb*512],
+        mass, com[3])."""
+        nb = self.nb
+        c = np.ascontiguousarray(centre, np.float64)
+        sh = np.ascontiguousarray(np.atleast_1d(shape), np.float64)
+        q = np.ascontiguousarray(quat, np.float64)
+        slot = np.zeros(nb, np.int32)
+        bos = np.zeros(nb, np.int32)
+        chi_o = np.zeros(nb * 512)
+        chi = np.zeros(nb * 512)
+        mom = np.zeros(4)
+        ns = lib().orc_create_obstacle(self._p, 0 if kind == "sphere" else 1, _d(c), _d(sh), _d(q), _i(slot),
+                                       _i(bos), _d(chi_o), _d(chi), _d(mom))
+        return dict(slot=slot, block_of_slot=bos[:ns].copy(), chi_o=chi_o[:ns * 512].copy(), chi=chi,
+                    mass=mom[3], com=mom[:3] / mom[3] if mom[3] > 0 else np.zeros(3))
 
     def grad_update(self, vel, pres, dt):
         vel = np.array(vel, np.float64)

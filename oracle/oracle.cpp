@@ -8,6 +8,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <unordered_map>
 #include <vector>
@@ -1638,4 +1639,285 @@ extern "C" void orc_cnn_fwd_grad(int nblk, int C, const double* P, const float* 
   if (grad)
     for (int i = 0; i < D.n; ++i) grad[i] = G[i];
   if (loss) *loss = L * scale;
+}
+
+// ============================================================================
+// Obstacle creation (CreateObstacles, ObstaclesCreate.cpp:18-148): for every
+// block the body's box touches (Obstacle::create_base, Obstacle.h:139-160,
+// isTouching of Sphere.cpp:31-45 / Ellipsoid.cpp:266-280, margin (2+SURFDH)
+// sim.hmin with SURFDH = 1, ObstacleBlock.h:16), the signed distance on the
+// block and a one-cell halo (FillBlocksBase, ObstacleLibrary.h:44-59), then
+// chi by Towers' FDMH eq. (14) with the chi moments
+// (KernelCharacteristicFunction, ObstaclesCreate.cpp:28-88), the grid chi
+// max(chi, grid chi) and the centre of mass (kernelComputeGridCoM, :128-148).
+// Block origins are index * 8 * h and cell centres origin + (i + 0.5) h
+// (Cubism's BlockInfo::pos; Cubism is not in the reference tree).
+// ============================================================================
+namespace obst_orc {
+
+constexpr double EPS = std::numeric_limits<double>::epsilon();
+constexpr int IMAX = 2 * std::numeric_limits<double>::max_exponent;
+
+// Ellipsoid.cpp:22-69 (distPointEllipseSpecial): e0 >= e1, y in the first quadrant.
+double ellipse_special(const double e[2], const double y[2], double x[2]) {
+  if (y[1] > 0) {
+    if (y[0] > 0) {
+      const double esqr[2] = {e[0] * e[0], e[1] * e[1]};
+      const double ey[2] = {e[0] * y[0], e[1] * y[1]};
+      double t0 = -esqr[1] + ey[1];
+      double t1 = -esqr[1] + std::sqrt(ey[0] * ey[0] + ey[1] * ey[1]);
+      double t = t0;
+      for (int i = 0; i < IMAX; ++i) {
+        t = 0.5 * (t0 + t1);
+        if (std::fabs(t - t0) < EPS || std::fabs(t - t1) < EPS) break;
+        const double r[2] = {ey[0] / (t + esqr[0]), ey[1] / (t + esqr[1])};
+        const double f = r[0] * r[0] + r[1] * r[1] - 1;
+        if (f > 0) t0 = t;
+        else if (f < 0) t1 = t;
+        else break;
+      }
+      x[0] = esqr[0] * y[0] / (t + esqr[0]);
+      x[1] = esqr[1] * y[1] / (t + esqr[1]);
+      const double d[2] = {x[0] - y[0], x[1] - y[1]};
+      return std::sqrt(d[0] * d[0] + d[1] * d[1]);
+    }
+    x[0] = 0;
+    x[1] = e[1];
+    return std::fabs(y[1] - e[1]);
+  }
+  const double denom0 = e[0] * e[0] - e[1] * e[1];
+  const double e0y0 = e[0] * y[0];
+  if (e0y0 < denom0) {
+    const double x0de0 = e0y0 / denom0;
+    const double x0de0sqr = x0de0 * x0de0;
+    x[0] = e[0] * x0de0;
+    x[1] = e[1] * std::sqrt(std::fabs(1.0 - x0de0sqr));
+    const double d0 = x[0] - y[0];
+    return std::sqrt(d0 * d0 + x[1] * x[1]);
+  }
+  x[0] = e[0];
+  x[1] = 0;
+  return std::fabs(y[0] - e[0]);
+}
+
+// Ellipsoid.cpp:117-203 (distPointEllipsoidSpecial): e0 >= e1 >= e2, first octant.
+double ellipsoid_special(const double e[3], const double y[3], double x[3]) {
+  if (y[2] > 0) {
+    if (y[1] > 0) {
+      if (y[0] > 0) {
+        const double esq[3] = {e[0] * e[0], e[1] * e[1], e[2] * e[2]};
+        const double ey[3] = {e[0] * y[0], e[1] * y[1], e[2] * y[2]};
+        double t0 = -esq[2] + ey[2];
+        double t1 = -esq[2] + std::sqrt(ey[0] * ey[0] + ey[1] * ey[1] + ey[2] * ey[2]);
+        double t = t0;
+        for (int i = 0; i < IMAX; ++i) {
+          t = 0.5 * (t0 + t1);
+          if (std::fabs(t - t0) < EPS || std::fabs(t - t1) < EPS) break;
+          const double r[3] = {ey[0] / (t + esq[0]), ey[1] / (t + esq[1]), ey[2] / (t + esq[2])};
+          const double f = r[0] * r[0] + r[1] * r[1] + r[2] * r[2] - 1;
+          if (f > 0) t0 = t;
+          else if (f < 0) t1 = t;
+          else break;
+        }
+        x[0] = esq[0] * y[0] / (t + esq[0]);
+        x[1] = esq[1] * y[1] / (t + esq[1]);
+        x[2] = esq[2] * y[2] / (t + esq[2]);
+        const double d[3] = {x[0] - y[0], x[1] - y[1], x[2] - y[2]};
+        return std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      }
+      x[0] = 0;
+      const double et[2] = {e[1], e[2]}, yt[2] = {y[1], y[2]};
+      double xt[2];
+      const double dist = ellipse_special(et, yt, xt);
+      x[1] = xt[0];
+      x[2] = xt[1];
+      return dist;
+    }
+    x[1] = 0;
+    if (y[0] > 0) {
+      const double et[2] = {e[0], e[2]}, yt[2] = {y[0], y[2]};
+      double xt[2];
+      const double dist = ellipse_special(et, yt, xt);
+      x[0] = xt[0];
+      x[2] = xt[1];
+      return dist;
+    }
+    x[0] = 0;
+    x[2] = e[2];
+    return std::fabs(y[2] - e[2]);
+  }
+  const double denom[2] = {e[0] * e[0] - e[2] * e[2], e[1] * e[1] - e[2] * e[2]};
+  const double ey[2] = {e[0] * y[0], e[1] * y[1]};
+  if (ey[0] < denom[0] && ey[1] < denom[1]) {
+    const double xde[2] = {ey[0] / denom[0], ey[1] / denom[1]};
+    const double xdesqr[2] = {xde[0] * xde[0], xde[1] * xde[1]};
+    const double discr = 1 - xdesqr[0] - xdesqr[1];
+    if (discr > 0) {
+      x[0] = e[0] * xde[0];
+      x[1] = e[1] * xde[1];
+      x[2] = e[2] * std::sqrt(discr);
+      const double d[2] = {x[0] - y[0], x[1] - y[1]};
+      return std::sqrt(d[0] * d[0] + d[1] * d[1] + x[2] * x[2]);
+    }
+    x[2] = 0;
+    return ellipse_special(e, y, x);
+  }
+  x[2] = 0;
+  return ellipse_special(e, y, x);
+}
+
+// Ellipsoid.cpp:211-258 (distancePointEllipsoid): reflection and axis order.
+double ellipsoid_distance(const double e[3], const double y[3], double x[3]) {
+  const bool reflect[3] = {y[0] < 0, y[1] < 0, y[2] < 0};
+  int permute[3];
+  if (e[0] < e[1]) {
+    if (e[2] < e[0]) { permute[0] = 1; permute[1] = 0; permute[2] = 2; }
+    else if (e[2] < e[1]) { permute[0] = 1; permute[1] = 2; permute[2] = 0; }
+    else { permute[0] = 2; permute[1] = 1; permute[2] = 0; }
+  } else {
+    if (e[2] < e[1]) { permute[0] = 0; permute[1] = 1; permute[2] = 2; }
+    else if (e[2] < e[0]) { permute[0] = 0; permute[1] = 2; permute[2] = 1; }
+    else { permute[0] = 2; permute[1] = 0; permute[2] = 1; }
+  }
+  int invpermute[3];
+  for (int i = 0; i < 3; ++i) invpermute[permute[i]] = i;
+  double locE[3], locY[3], locX[3];
+  for (int i = 0; i < 3; ++i) {
+    const int j = permute[i];
+    locE[i] = e[j];
+    locY[i] = y[j];
+    if (reflect[j]) locY[i] = -locY[i];
+  }
+  const double distance = ellipsoid_special(locE, locY, locX);
+  for (int i = 0; i < 3; ++i) {
+    const int j = invpermute[i];
+    if (reflect[j]) locX[j] = -locX[j];
+    x[i] = locX[j];
+  }
+  return distance;
+}
+
+struct Body {
+  int kind;  // 0 sphere, 1 ellipsoid
+  double pos[3], radius, e[3], R[3][3], box[3][2];
+  // Sphere.cpp:47-51; Ellipsoid.cpp:282-299 with positive inside (the
+  // obstacle contract, ObstacleLibrary.h:30-32)
+  double sdf(double xo, double yo, double zo) const {
+    if (kind == 0) {
+      const double dx = xo - pos[0], dy = yo - pos[1], dz = zo - pos[2];
+      return radius - std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+    const double p[3] = {xo - pos[0], yo - pos[1], zo - pos[2]};
+    const double t[3] = {R[0][0] * p[0] + R[0][1] * p[1] + R[0][2] * p[2],
+                         R[1][0] * p[0] + R[1][1] * p[1] + R[1][2] * p[2],
+                         R[2][0] * p[0] + R[2][1] * p[1] + R[2][2] * p[2]};
+    double xs[3];
+    const double dist = ellipsoid_distance(e, t, xs);
+    const double Dcentre = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+    const double Dsurf = xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2];
+    return Dcentre > Dsurf ? -dist : dist;
+  }
+  bool touching(const double minp[3], const double maxp[3]) const {
+    bool ok = true;
+    for (int d = 0; d < 3; ++d) {
+      const double lo = std::max(minp[d], box[d][0]), hi = std::min(maxp[d], box[d][1]);
+      ok = ok && hi - lo > 0;
+    }
+    return ok;
+  }
+};
+
+}  // namespace obst_orc
+
+extern "C" int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, const double* shape,
+                                   const double* q, int32_t* obst_slot, int32_t* block_of_slot, double* chi_o,
+                                   double* chi_grid, double* mom) {
+  using namespace obst_orc;
+  Body B{};
+  B.kind = kind;
+  for (int d = 0; d < 3; ++d) B.pos[d] = centre[d];
+  const double h = m->hmin, safety = (2 + 1) * h;
+  if (kind == 0) {
+    B.radius = shape[0];
+    for (int d = 0; d < 3; ++d) {
+      B.box[d][0] = B.pos[d] - (B.radius + safety);
+      B.box[d][1] = B.pos[d] + (B.radius + safety);
+    }
+  } else {
+    for (int d = 0; d < 3; ++d) B.e[d] = shape[d];
+    const double maxAxis = std::max({B.e[0], B.e[1], B.e[2]});
+    for (int d = 0; d < 3; ++d) {
+      B.box[d][0] = B.pos[d] - 2 * (maxAxis + safety);
+      B.box[d][1] = B.pos[d] + 2 * (maxAxis + safety);
+    }
+    const double w = q[0], x = q[1], y = q[2], z = q[3];
+    const double R[3][3] = {{1 - 2 * (y * y + z * z), 2 * (x * y + z * w), 2 * (x * z - y * w)},
+                            {2 * (x * y - z * w), 1 - 2 * (x * x + z * z), 2 * (y * z + x * w)},
+                            {2 * (x * z + y * w), 2 * (y * z - x * w), 1 - 2 * (x * x + y * y)}};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) B.R[i][j] = R[i][j];
+  }
+  const int nb = m->nb;
+  std::fill(chi_grid, chi_grid + size_t(nb) * BN, 0.0);
+  int ns = 0;
+  std::vector<double> bm(4 * size_t(nb), 0.0);  // per-block CoM_x, CoM_y, CoM_z, mass
+  for (int b = 0; b < nb; ++b) {
+    obst_slot[b] = -1;
+    const double hb = m->h[b];
+    double org[3], minp[3], maxp[3];
+    for (int d = 0; d < 3; ++d) {
+      org[d] = m->idx[b][d] * 8 * hb;
+      minp[d] = org[d] + hb * (0 + 0.5);
+      maxp[d] = org[d] + hb * (BS - 1 + 0.5);
+    }
+    if (!B.touching(minp, maxp)) continue;
+    const int s = ns++;
+    obst_slot[b] = s;
+    block_of_slot[s] = b;
+    static thread_local double lab[BS + 2][BS + 2][BS + 2];
+    for (int iz = -1; iz < BS + 1; ++iz)
+      for (int iy = -1; iy < BS + 1; ++iy)
+        for (int ix = -1; ix < BS + 1; ++ix)
+          lab[iz + 1][iy + 1][ix + 1] =
+              B.sdf(org[0] + hb * (ix + 0.5), org[1] + hb * (iy + 0.5), org[2] + hb * (iz + 0.5));
+    const double inv2h = .5 / hb, vol = hb * hb * hb;
+    double* CHI = chi_o + size_t(s) * BN;
+    double* M4 = &bm[4 * size_t(b)];
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) {
+          const double s0 = lab[z + 1][y + 1][x + 1];
+          double chi;
+          if (s0 > +hb || s0 < -hb) {
+            chi = s0 > 0 ? 1 : 0;
+          } else {
+            const double distPx = lab[z + 1][y + 1][x + 2], distMx = lab[z + 1][y + 1][x];
+            const double distPy = lab[z + 1][y + 2][x + 1], distMy = lab[z + 1][y][x + 1];
+            const double distPz = lab[z + 2][y + 1][x + 1], distMz = lab[z][y + 1][x + 1];
+            const double gradUX = inv2h * (distPx - distMx);
+            const double gradUY = inv2h * (distPy - distMy);
+            const double gradUZ = inv2h * (distPz - distMz);
+            const double gradUSq = gradUX * gradUX + gradUY * gradUY + gradUZ * gradUZ + EPS;
+            const double gradIX = inv2h * (std::max(0.0, distPx) - std::max(0.0, distMx));
+            const double gradIY = inv2h * (std::max(0.0, distPy) - std::max(0.0, distMy));
+            const double gradIZ = inv2h * (std::max(0.0, distPz) - std::max(0.0, distMz));
+            const double numH = gradIX * gradUX + gradIY * gradUY + gradIZ * gradUZ;
+            chi = numH / gradUSq;
+          }
+          const int c = x + BS * y + BS * BS * z;
+          CHI[c] = chi;
+          chi_grid[size_t(b) * BN + c] = std::max(chi, chi_grid[size_t(b) * BN + c]);
+          const double p[3] = {org[0] + hb * (x + 0.5), org[1] + hb * (y + 0.5), org[2] + hb * (z + 0.5)};
+          M4[0] += chi * vol * p[0];
+          M4[1] += chi * vol * p[1];
+          M4[2] += chi * vol * p[2];
+          M4[3] += chi * vol;
+        }
+  }
+  // kernelComputeGridCoM: block sums in block order
+  for (int k = 0; k < 4; ++k) mom[k] = 0.0;
+  for (int b = 0; b < nb; ++b)
+    if (obst_slot[b] >= 0)
+      for (int k = 0; k < 4; ++k) mom[k] += bm[4 * size_t(b) + k];
+  return ns;
 }

@@ -94,6 +94,17 @@ void orc_grad_update(orc_mesh* m, double* vel, const double* pres, double dt);
 // ComputeDissipation's 20 diagnostics (ComputeDissipation.cpp:17-109).
 void orc_dissipation(orc_mesh* m, const double* vel, const double* pres, const double* chi, double nu, double* out);
 
+/* ---- obstacle creation (ObstaclesCreate.cpp:18-148, Sphere.cpp:19-51,
+ * Ellipsoid.cpp:22-300).  kind 0 sphere (shape[0] = radius), 1 ellipsoid
+ * (shape = semi-axes, q = unit quaternion w, x, y, z).  Fill margin 3 hmin,
+ * hmin the finest possible spacing of the mesh (SimulationData.cpp:162).
+ * Outputs: obst_slot[nb] (-1 or the slot, slots in block order),
+ * block_of_slot[nb], chi_o[nb*512] (per slot), chi_grid[nb*512],
+ * mom[4] = sum chi h^3 (x, y, z), sum chi h^3.  Returns the slot count. ---- */
+int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, const double* shape, const double* q,
+                        int32_t* obst_slot, int32_t* block_of_slot, double* chi_o, double* chi_grid,
+                        double* mom);
+
 /* ---- learned preconditioner network (see oracle.cpp for the layout) ---- */
 int orc_cnn_nparam(int C);
 /* forward (out may be NULL), loss and gradient (target/grad may be NULL) */

@@ -14,6 +14,18 @@ values, and the GPU tests compare the device path against the same values:
                       solution norm and samples;
 * tgv32_steps.npz     the Taylor-Green case (32^3, nu 0.01, CFL 0.3, upwind5,
                       Poisson to 1e-11): dt and velocity samples/norms after 1..4 steps.
+
+All of these fixtures are self-pinned: they record what this repository's
+oracle and host mesh code compute, so they catch regressions but say nothing
+about the reference by themselves.  What ties the oracle to the reference's
+own tests and values is elsewhere:
+
+* tests/test_obstacle_moments.py  the reference's sphere chi-moment test
+                      (tests/python/test_obstacles.py:7-74) with its tolerances;
+* tests/test_oracle_kat.py        the reference's periodic ghost-shift test
+                      (tests/cubismup3d/TestBoundaries.cpp:19-104) and known
+                      answers built from the reference's formulas (stencil
+                      exactness, P_inv L = I, RK3 coefficients).
 """
 from __future__ import annotations
 

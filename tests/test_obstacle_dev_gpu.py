@@ -1,6 +1,12 @@
-"""Obstacle creation on the device (cup_obstacle_sphere_dev /
-cup_obstacle_ellipsoid_dev) against the host creation (obstacles.cpp, the
-restatement of Sphere.cpp / ObstaclesCreate.cpp:18-121):
+"""Obstacle creation on the host (cup_obstacle_sphere / cup_obstacle_ellipsoid)
+and on the device (cup_obstacle_sphere_dev / cup_obstacle_ellipsoid_dev):
+
+* both against the oracle's CreateObstacles (ObstaclesCreate.cpp:18-148,
+  Sphere.cpp:19-51, Ellipsoid.cpp:22-300): slot list, chi and grid chi bit for
+  bit, centre of mass to rounding, on the benchmarked sphere mesh, AMR meshes
+  with a rotated ellipsoid and the reference's own sphere moment case
+  (tests/python/test_obstacles.py:7-74) with its tolerances;
+* device against host:
 
 * slot list, chi, udef and the grid chi field bit for bit; centre of mass
   within 1e-14 of the domain size (the moments are summed in another order);
@@ -37,6 +43,59 @@ def _assert_same(a, b, extent):
     assert np.array_equal(g_a, g_b)
     assert np.abs(kin_a[:3] - kin_b[:3]).max() <= 1e-14 * extent
     assert np.array_equal(kin_a[3:], kin_b[3:])
+
+
+def _assert_matches_oracle(ctx, kind, centre, shape, quat=(1.0, 0.0, 0.0, 0.0), extent=1.0):
+    """The context's obstacle (slot list, chi, zero udef, grid chi, centre of
+    mass) against the oracle's CreateObstacles on the same mesh."""
+    from tests.meshes import oracle_mesh
+    ref = oracle_mesh(ctx).create_obstacle(kind, centre, shape, quat)
+    slot, chi, udef, kin, grid = _obstacle_state(ctx)
+    assert np.array_equal(slot, ref["slot"])
+    assert np.array_equal(chi, ref["chi_o"])
+    assert np.array_equal(grid, ref["chi"])
+    assert np.all(udef == 0.0)
+    assert np.abs(kin[:3] - ref["com"]).max() <= 1e-14 * extent
+
+
+@pytest.mark.parametrize("on_device", [False, True])
+def test_sphere_creation_matches_oracle(on_device):
+    # the benchmarked sphere on its 2340-block, four-level mesh
+    from cup3d_b200.workloads import SPHERE_BODY, make_sphere_ctx
+    ctx = make_sphere_ctx(0)
+    ctx.obstacle_sphere(**SPHERE_BODY, on_device=on_device)
+    _assert_matches_oracle(ctx, "sphere", SPHERE_BODY["center"], SPHERE_BODY["radius"], extent=4.0)
+
+
+@pytest.mark.parametrize("on_device", [False, True])
+@pytest.mark.parametrize("name", ["amr2_free", "amr3_mixed", "amr3_periodic"])
+def test_ellipsoid_creation_matches_oracle(name, on_device):
+    ctx = make_ctx(name, device=0)
+    q = np.array([0.9, 0.1, 0.3, 0.3])
+    q /= np.linalg.norm(q)
+    ctx.obstacle_ellipsoid((0.6, 0.45, 0.5), (0.2, 0.1, 0.08), q, on_device=on_device)
+    _assert_matches_oracle(ctx, "ellipsoid", (0.6, 0.45, 0.5), (0.2, 0.1, 0.08), q)
+
+
+@pytest.mark.parametrize("on_device", [False, True])
+def test_reference_sphere_moment_case(on_device):
+    # tests/python/test_obstacles.py:7-74: Sphere L=3 at (3.125, 2.5, 2.5) on
+    # 8x4x4 blocks, extent 10, levelMax 2, chi on the level-1 grid; the
+    # product's chi equals the oracle's and meets the reference's tolerances
+    from tests.test_obstacle_moments import BPD, CTR, R, _moments, _uniform_level1
+    level, index = _uniform_level1()
+    ctx = cup.Context(cup.config(f"-bpdx {BPD[0]} -bpdy {BPD[1]} -bpdz {BPD[2]} -levelMax 2 -extent 10",
+                                 device=0))
+    ctx.set_mesh(level, index)
+    ctx.obstacle_sphere(CTR, R, on_device=on_device)
+    _assert_matches_oracle(ctx, "sphere", CTR, R, extent=10.0)
+    from tests.meshes import oracle_mesh
+    mo = _moments(oracle_mesh(ctx), ctx.download("chi"))
+    assert round(mo["M"] - 4 / 3 * np.pi * R ** 3, 3) == 0
+    for k in ("Mx", "My", "Mz", "Mxy", "Myz", "Mzx"):
+        assert abs(mo[k]) < 1e-9, k
+    for k in ("Mxx", "Myy", "Mzz"):
+        assert round(mo[k] - 4 / 15 * np.pi * R ** 5, 1) == 0, k
 
 
 def test_sphere_on_the_sphere_mesh():
