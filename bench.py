@@ -501,25 +501,37 @@ def cpu_baseline(ctx, args, state, step):
     secs, _, info = cpu_reference_step(state, m, slot, chi_o, udef_o, kin, chi, step,
                                        (-0.1, 0.0, 0.0), 4.1666666666666667e-05, 0.3, 1e6)
     return {"value": round(m.n / secs / 1e6, 4), "unit": "Mcell-steps/s", "cores": os.cpu_count(),
-            "kind": "port",
+            "cpu_model": cpu_model(), "kind": "port",
             "sample": f"1 full time step of the same workload from the state of the first timed step "
                       f"(oracle, OpenMP, pipelined BiCGSTAB + block CG, {info['iterations']} iterations, "
                       f"{secs:.2f} s)"}
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def run_reference(args):
+    """The reference's CPU path restated (oracle) on the host cores, on its
+    own inputs: the mesh leaves from the pure-Python generator and the sphere
+    from the oracle's CreateObstacles, so the library is never loaded."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    import cup3d_b200 as cup
     import oracle
-    cfg = cup.config(SPHERE_FLAGS, device=-1)
-    ctx = cup.Context(cfg)
-    ctx.set_mesh_sphere_wake(**SPHERE_MESH)
-    level, index, h = ctx.blocks()
-    m = oracle.Mesh(level, index, [4, 2, 2], 4, [0, 0, 0], 4.0)
-    # obstacle data from the same host code path (no device needed)
-    slot, chi_o, udef_o, kin, chi = host_sphere(ctx)
+    from cup3d_b200.workloads import sphere_wake_leaves
+    leaves = sphere_wake_leaves()
+    m = oracle.Mesh(leaves[:, 0], leaves[:, 1:], [4, 2, 2], 4, [0, 0, 0], 4.0)
+    ob = m.create_obstacle("sphere", SPHERE_BODY["center"], SPHERE_BODY["radius"])
+    slot, chi_o, chi = ob["slot"], ob["chi_o"], ob["chi"]
+    udef_o = np.zeros(3 * len(chi_o))
+    kin = np.concatenate([ob["com"], SPHERE_BODY["vel"], [0.0, 0.0, 0.0]])
     vel = np.zeros(3 * m.n)
     pres = np.zeros(m.n)
     state = (vel, pres)
@@ -542,22 +554,14 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "blocks": m.nb, "cells": m.n},
-        "cpu_baseline": {"value": round(value, 4), "unit": "Mcell-steps/s", "cores": os.cpu_count(), "kind": "port",
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mcell-steps/s", "cores": os.cpu_count(),
+                         "cpu_model": cpu_model(), "kind": "port",
                          "sample": "full time steps from rest on the frozen sphere mesh (oracle restatement of the "
-                                   "reference CPU path, OpenMP over blocks)"},
+                                   "reference CPU path, OpenMP over blocks; mesh and sphere built by the oracle "
+                                   "side, not the library)"},
         "e2e": {"value": round(value, 4), "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-def host_sphere(ctx):
-    """Sphere obstacle arrays from the product's host obstacle code (host-only context)."""
-    ctx.obstacle_sphere(**SPHERE_BODY)
-    slot, chi_o, udef_o, kin = ctx.get_obstacle()
-    chi = np.zeros(ctx.nb * 512)
-    for b in np.where(slot >= 0)[0]:
-        chi[b * 512:(b + 1) * 512] = chi_o[slot[b] * 512:(slot[b] + 1) * 512]
-    return slot, chi_o, udef_o, kin, chi
 
 
 def main():

@@ -289,6 +289,18 @@ class Context:
     def set_poisson(self, solver="b200", tol_abs=1e-6, tol_rel=1e-4, max_iter=1000):
         check(lib().cup_set_poisson(self._p, SOLVER[solver], tol_abs, tol_rel, max_iter), self._p)
 
+    def adapt_indicator(self):
+        """Each block's refinement indicator (cup_adapt_indicator)."""
+        out = np.zeros(self.nb)
+        check(lib().cup_adapt_indicator(self._p, dptr(out)), self._p)
+        return out
+
+    def adapt_mesh(self):
+        """One mesh adaptation (Simulation::adaptMesh); True when the mesh changed."""
+        ch = C.c_int32(0)
+        check(lib().cup_adapt_mesh(self._p, C.byref(ch)), self._p)
+        return bool(ch.value)
+
     def set_barrier_limit(self, cycles):
         """Wait limit of the persistent solvers' grid barriers (0: default)."""
         check(lib().cup_set_barrier_limit(self._p, int(cycles)), self._p)

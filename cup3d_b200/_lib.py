@@ -55,6 +55,10 @@ class cup_config(C.Structure):
         ("poisson_block_cache", C.c_int32),
         ("step_graph", C.c_int32),
         ("static_obstacles", C.c_int32),
+        ("rtol", C.c_double),
+        ("ctol", C.c_double),
+        ("level_max_vorticity", C.c_int32),
+        ("level_start", C.c_int32),
     ]
 
 
@@ -132,6 +136,8 @@ SIGNATURES = {
     "cup_pressure_rhs": (C.c_int, [_P, C.c_double, C.c_int32]),
     "cup_pressure_finish": (C.c_int, [_P, C.c_double, C.c_int32]),
     "cup_set_barrier_limit": (C.c_int, [_P, C.c_int64]),
+    "cup_adapt_indicator": (C.c_int, [_P, _D]),
+    "cup_adapt_mesh": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "cup_set_poisson": (C.c_int, [_P, C.c_int32, C.c_double, C.c_double, C.c_int32]),
     "cup_cnn_num_params": (C.c_int32, []),
     "cup_cnn_init": (C.c_int, [_P, C.c_uint64]),

@@ -215,6 +215,10 @@ void cup_config_default(cup_config* c) {
   c->poisson_block_cache = 4;
   c->step_graph = 1;
   c->static_obstacles = 0;
+  c->rtol = 1.0;
+  c->ctol = 0.1;
+  c->level_max_vorticity = -1;  // levelMax unless given
+  c->level_start = -1;          // levelMax - 1 unless given (SimulationData.cpp:38)
 }
 
 static int parse_bc(const std::string& v) {
@@ -293,6 +297,18 @@ int cup_config_parse(cup_config* c, const char* args) {
     } else if (key == "stepGraph") {
       if (need_num()) return CUP_ERR_ARG;
       c->step_graph = dv != 0 ? 1 : 0;
+    } else if (key == "Rtol") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->rtol = dv;
+    } else if (key == "Ctol") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->ctol = dv;
+    } else if (key == "levelMaxVorticity") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->level_max_vorticity = int(dv);
+    } else if (key == "levelStart") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->level_start = int(dv);
     } else if (key == "StaticObstacles") {
       if (need_num()) return CUP_ERR_ARG;
       c->static_obstacles = dv != 0 ? 1 : 0;
@@ -384,10 +400,13 @@ static MeshSpec spec_of(const cup_ctx* c) {
 
 int cup_set_mesh_uniform(cup_ctx* c) {
   if (!c) return ctx_fail(c, CUP_ERR_ARG, "null ctx");
+  // every block at -levelStart (levelMax - 1 by default), as the reference's
+  // grids start (Simulation.cpp:162-168)
+  const int l = c->cfg.level_start >= 0 ? std::min(c->cfg.level_start, c->cfg.level_max - 1) : c->cfg.level_max - 1;
   std::vector<std::array<int32_t, 4>> leaves;
-  for (int k = 0; k < c->cfg.bpd[2]; ++k)
-    for (int j = 0; j < c->cfg.bpd[1]; ++j)
-      for (int i = 0; i < c->cfg.bpd[0]; ++i) leaves.push_back({0, i, j, k});
+  for (int k = 0; k < c->cfg.bpd[2] << l; ++k)
+    for (int j = 0; j < c->cfg.bpd[1] << l; ++j)
+      for (int i = 0; i < c->cfg.bpd[0] << l; ++i) leaves.push_back({l, i, j, k});
   return install_mesh(c, leaves);
 }
 

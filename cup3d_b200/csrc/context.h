@@ -213,6 +213,14 @@ bool body_free(const cup_ctx* c);
 int update_obstacles(cup_ctx* c, double dt, double out[12]);
 void body_coef_u(cup_ctx* c, int step, double dt);
 int body_advance(cup_ctx* c, int step, double dt);
+// chi of the context's body at its current pose, by the path it was created
+// with, keeping its motion history (after a mesh change).
+int body_recreate(cup_ctx* c);
+// Mesh adaptation (adapt.cu): the per-block refinement indicator, and one
+// adaptation of the mesh with the fields moved onto it (*changed = 0 when
+// the mesh stays as it is).
+int adapt_indicator(cup_ctx* c, std::vector<double>& out);
+int adapt_mesh(cup_ctx* c, int* changed);
 // Fetches the host copies of a device-created obstacle (no-op otherwise).
 int ctx_obstacle_host_copies(cup_ctx* c);
 // Drops the captured time steps (after any change of mesh, obstacle or

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <set>
 #include <sstream>
 
@@ -267,6 +268,66 @@ struct LeafSet {
   }
 };
 }  // namespace
+
+std::vector<std::array<int32_t, 4>> mesh_adapt_leaves(const Mesh& m, const std::vector<uint8_t>& refine,
+                                                      const std::vector<uint8_t>& compress) {
+  LeafSet ls;
+  ls.spec = m.spec;
+  for (int b = 0; b < m.nb; ++b) ls.leaves.insert({m.level[b], m.index[3 * b], m.index[3 * b + 1], m.index[3 * b + 2]});
+  // refinement first, then the 2:1 balance it needs
+  std::vector<std::array<int32_t, 4>> split;
+  for (int b = 0; b < m.nb; ++b)
+    if (refine[b] && m.level[b] + 1 < m.spec.level_max)
+      split.push_back({m.level[b], m.index[3 * b], m.index[3 * b + 1], m.index[3 * b + 2]});
+  for (const auto& b : split) ls.split(b);
+  ls.balance();
+  // compression: a parent whose eight children are leaves that all compress,
+  // unless a leaf finer than the children touches the parent's region (the
+  // merged block would then sit two levels above a neighbour)
+  std::map<std::array<int32_t, 4>, int> votes;
+  for (int b = 0; b < m.nb; ++b) {
+    const int l = m.level[b];
+    if (!compress[b] || refine[b] || l == 0) continue;
+    const std::array<int32_t, 4> me{l, m.index[3 * b], m.index[3 * b + 1], m.index[3 * b + 2]};
+    if (!ls.leaves.count(me)) continue;  // split by the balance
+    ++votes[{l - 1, me[1] >> 1, me[2] >> 1, me[3] >> 1}];
+  }
+  std::vector<std::array<int32_t, 4>> merge;
+  for (const auto& [p, n] : votes) {
+    if (n != 8) continue;
+    const int l = p[0] + 1;  // the children's level
+    bool ok = true;
+    for (int dz = -1; dz <= 1 && ok; ++dz)
+      for (int dy = -1; dy <= 1 && ok; ++dy)
+        for (int dx = -1; dx <= 1 && ok; ++dx) {
+          if (!dx && !dy && !dz) continue;
+          int q[3] = {p[1] + dx, p[2] + dy, p[3] + dz};
+          bool inside = true;
+          for (int d = 0; d < 3; ++d) {
+            const int N = m.spec.bpd[d] << p[0];
+            if (q[d] < 0 || q[d] >= N) {
+              if (m.spec.bc[d] == BC_PERIODIC)
+                q[d] = (q[d] + N) % N;
+              else
+                inside = false;
+            }
+          }
+          if (!inside) continue;
+          // the neighbour position's eight level-l parts must be covered at level <= l
+          for (int c = 0; c < 8 && ok; ++c) {
+            const int cp[3] = {2 * q[0] + (c & 1), 2 * q[1] + ((c >> 1) & 1), 2 * q[2] + (c >> 2)};
+            ok = ls.covering(l, cp)[0] >= 0;
+          }
+        }
+    if (ok) merge.push_back(p);
+  }
+  for (const auto& p : merge) {
+    for (int c = 0; c < 8; ++c)
+      ls.leaves.erase({p[0] + 1, 2 * p[1] + (c & 1), 2 * p[2] + ((c >> 1) & 1), 2 * p[3] + (c >> 2)});
+    ls.leaves.insert(p);
+  }
+  return std::vector<std::array<int32_t, 4>>(ls.leaves.begin(), ls.leaves.end());
+}
 
 std::vector<std::array<int32_t, 4>> mesh_refine_leaves(
     const MeshSpec& spec_in, const std::function<bool(int, const double*, const double*)>& tag) {

@@ -108,6 +108,15 @@ std::vector<std::array<int32_t, 4>> mesh_random_leaves(const MeshSpec& spec, uin
 // similar share of the Poisson operator's cost: blocks sorted by estimated
 // cost (coarse-fine faces cost extra flux work), dealt in snake order (one
 // round forward, the next backward).  A permutation of 0..nb-1.
+// Leaves after one adaptation of m (the role of Cubism's MeshAdaptation
+// Tag/Adapt, absent from the reference tree): leaves with refine[b] split
+// (below level_max - 1), then the 2:1 balance over the 26 neighbours splits
+// what it must; a parent whose eight children are leaves that all have
+// compress[b] (and no refine) replaces them unless a leaf finer than the
+// children touches the parent's region.
+std::vector<std::array<int32_t, 4>> mesh_adapt_leaves(const Mesh& m, const std::vector<uint8_t>& refine,
+                                                      const std::vector<uint8_t>& compress);
+
 std::vector<int32_t> mesh_visit_order(const Mesh& m, int groups);
 
 }  // namespace cup3d

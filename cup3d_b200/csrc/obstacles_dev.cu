@@ -602,8 +602,13 @@ static void body_update(BodyState& B, const double uinf[3], int step, int step_2
 }
 
 int body_advance(cup_ctx* c, int step, double dt) {
+  body_update(c->body, c->cfg.uinf, step, c->cfg.step_2nd_start, c->coef_u, dt);
+  return body_recreate(c);
+}
+
+int body_recreate(cup_ctx* c) {
   BodyState& B = c->body;
-  body_update(B, c->cfg.uinf, step, c->cfg.step_2nd_start, c->coef_u, dt);
+  if (B.kind < 0) return 0;
   const BodyState keep_state = B;  // the creation calls below record the body afresh
   int rc = 0;
   if (B.kind == 0)

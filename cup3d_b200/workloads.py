@@ -20,6 +20,90 @@ SPHERE_BODY = dict(center=(1.0, 1.0, 1.0), radius=0.0625, vel=(0.1, 0.0, 0.0))
 SPHERE_WORKLOAD = "sphere_re300_amr_levelmax4_weno5_fp64"
 
 
+def sphere_wake_leaves(bpd=(4, 2, 2), level_max=4, extent=4.0, center=SPHERE_MESH["center"],
+                       radius=SPHERE_BODY["radius"], flow_dir=SPHERE_MESH["flow_dir"],
+                       near_radius=SPHERE_MESH["near_radius"], wake_len=SPHERE_MESH["wake_len"],
+                       wake_radius=SPHERE_MESH["wake_radius"]):
+    """Leaves (level, i, j, k) of the frozen sphere mesh, in pure Python: the
+    same refinement rule and the same floating-point operations as the
+    library's cup_set_mesh_sphere_wake (a block of level l is split when its
+    box comes within (r + near_radius 2^-l) of the centre, or within
+    wake_radius 2^-l of the wake segment; then 2:1 balance over the 26
+    neighbours).  Used where the library must not be loaded (the CPU
+    reference arm of bench.py); the two generators are compared in the tests."""
+    import math
+    aux = 1 << (level_max - 1)
+    nfe = [float(b) * aux * 8 for b in bpd]
+    ex0 = (nfe[0] / max(nfe)) * extent
+    h0 = ex0 * aux / nfe[0]
+    leaves = {(0, i, j, k) for k in range(bpd[2]) for j in range(bpd[1]) for i in range(bpd[0])}
+
+    def split(b):
+        leaves.discard(b)
+        for c in range(8):
+            leaves.add((b[0] + 1, 2 * b[1] + (c & 1), 2 * b[2] + ((c >> 1) & 1), 2 * b[3] + (c >> 2)))
+
+    def covering(l, p):
+        for l2 in range(l, -1, -1):
+            k = (l2, p[0] >> (l - l2), p[1] >> (l - l2), p[2] >> (l - l2))
+            if k in leaves:
+                return k
+        return None
+
+    def balance():
+        changed = True
+        while changed:
+            changed = False
+            todo = set()
+            for b in list(leaves):
+                l = b[0]
+                if l < 2:
+                    continue
+                for dz in (-1, 0, 1):
+                    for dy in (-1, 0, 1):
+                        for dx in (-1, 0, 1):
+                            if dx == dy == dz == 0:
+                                continue
+                            p = [b[1] + dx, b[2] + dy, b[3] + dz]
+                            if any(p[d] < 0 or p[d] >= (bpd[d] << l) for d in range(3)):
+                                continue  # freespace: no wrap
+                            c = covering(l, p)
+                            if c is not None and c[0] < l - 1:
+                                todo.add(c)
+            for c in sorted(todo):
+                if c in leaves:
+                    split(c)
+                    changed = True
+
+    def tag(l, lo, hi):
+        scale = math.ldexp(1.0, -l)
+        s = 0.0
+        for d in range(3):
+            e = max(lo[d] - center[d], 0.0, center[d] - hi[d])
+            s += e * e
+        if math.sqrt(s) < radius + near_radius * scale:
+            return True
+        x0, x1 = center[0], center[0] + flow_dir * wake_len
+        xa, xb = min(x0, x1), max(x0, x1)
+        ex = max(xa - hi[0], 0.0, lo[0] - xb)
+        s = ex * ex
+        for d in (1, 2):
+            e = max(lo[d] - center[d], 0.0, center[d] - hi[d])
+            s += e * e
+        return math.sqrt(s) < wake_radius * scale
+
+    for l in range(level_max - 1):
+        hb = math.ldexp(h0, -l) * 8
+        for b in sorted(x for x in leaves if x[0] == l):
+            lo = [b[1] * hb, b[2] * hb, b[3] * hb]
+            hi = [lo[0] + hb, lo[1] + hb, lo[2] + hb]
+            if tag(l, lo, hi):
+                split(b)
+        balance()
+    balance()
+    return np.array(sorted(leaves), np.int32)
+
+
 def make_sphere_ctx(device, solver="b200"):
     """Context with the frozen sphere mesh and the sphere obstacle."""
     import cup3d_b200 as cup

@@ -86,6 +86,10 @@ typedef struct cup_config {
                                   / cup_obstacle_ellipsoid(_dev) whose velocity + uinf or angular
                                   velocity is non-zero move every cup_step (Obstacle::update) and
                                   their chi is re-created at the new pose (CreateObstacles) */
+  double rtol;                 /* -Rtol: refine a block whose indicator reaches it (default 1) */
+  double ctol;                 /* -Ctol: compress blocks whose indicators stay below it (default 0.1) */
+  int32_t level_max_vorticity; /* -levelMaxVorticity (default levelMax) */
+  int32_t level_start;         /* -levelStart: level of cup_set_mesh_uniform (default levelMax - 1) */
 } cup_config;
 
 typedef struct cup_solve_stats {
@@ -262,6 +266,24 @@ int cup_write_restart(cup_ctx* ctx, const char* dir, int32_t step, double time);
  * time.  Stepping on from step + 1... gives the results of the uninterrupted
  * run bit for bit. */
 int cup_read_restart(cup_ctx* ctx, const char* dir, int32_t step, double* time);
+
+/* ---- mesh adaptation (Simulation::adaptMesh, Simulation.cpp:128-149) ----
+ * cup_adapt_indicator: each block's refinement indicator (nblocks values in
+ * cup_get_blocks order): the largest vorticity magnitude over its cells with
+ * GradChiOnTmp's rules (ProcessHelpers.h:17-69): 1e10 where the body's
+ * interface (0.00001 < chi < 0.9) meets the block or its face ghost layers,
+ * 0 for cells inside the body, (Rtol+Ctol)/2 for cells at or above Rtol on
+ * level levelMaxVorticity-1.
+ * cup_adapt_mesh: refines blocks whose indicator is >= Rtol, merges eight
+ * siblings whose indicators are all < Ctol, keeps the 2:1 balance, moves
+ * velocity and pressure to the new mesh (copy, linear prolongation with
+ * central slopes, 8-cell means), zeroes tmpV and the right-hand side and
+ * creates the body's chi again.  Cubism's MeshAdaptation, which does this in
+ * the reference, is not in its tree: these rules are this library's.
+ * *changed (may be NULL): 1 when the mesh changed.  Obstacle data given by
+ * cup_set_obstacle cannot be re-created: CUP_ERR_STATE. */
+int cup_adapt_indicator(cup_ctx* ctx, double* out);
+int cup_adapt_mesh(cup_ctx* ctx, int32_t* changed);
 
 /* ---- the time-step operators (Operator::operator()(dt) of the reference) ---- */
 int cup_max_u(cup_ctx* ctx, double* umax);                          /* findMaxU */

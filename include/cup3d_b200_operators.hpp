@@ -37,6 +37,8 @@ struct SimulationData {
   std::array<Real, 6> force_torque{};  // last Penalization force and torque
   bool has_obstacle = false;
   int freqDiagnostics = 0;             // ComputeDissipation every this many steps (0: never)
+  bool adapt = true;                   // adaptMesh on the reference's cadence in Simulation::advance
+  bool meshChanged = false;            // set when an adaptation changed the mesh
   std::array<Real, 20> diagnostics{};  // its last values (the columns of diagnostics.dat)
 
   explicit SimulationData(const std::string& flags) {
@@ -179,7 +181,18 @@ class Simulation {
     sim.dt = dt;
     return dt;
   }
+  // Simulation::adaptMesh (Simulation.cpp:128-149): the mesh adapts to the
+  // vorticity and the body (cup_adapt_mesh); the body's chi is created again
+  // on the new mesh.
+  void adaptMesh() {
+    int32_t changed = 0;
+    check(cup_adapt_mesh(sim.ctx, &changed), sim.ctx);
+    sim.meshChanged = sim.meshChanged || changed != 0;
+  }
+  // The mesh adapts before the pipeline every 20 steps and in the first 10
+  // (Simulation.cpp:384-385); adapt = false keeps it as it is.
   void advance(Real dt) {
+    if (sim.adapt && (sim.step % 20 == 0 || sim.step < 10)) adaptMesh();
     for (auto& op : pipeline) (*op)(dt);
     sim.step++;
     sim.time += dt;

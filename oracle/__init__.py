@@ -51,6 +51,9 @@ SIG = {
     "orc_grad_update": (None, [C.c_void_p, _D, _D, C.c_double]),
     "orc_dissipation": (None, [C.c_void_p, _D, _D, _D, C.c_double, _D]),
     "orc_create_obstacle": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _I, _I, _D, _D, _D]),
+    "orc_adapt_indicator": (None, [C.c_void_p, _D, _D, C.c_int, C.c_int, C.c_double, C.c_double, _D]),
+    "orc_adapt_leaves": (C.c_int, [C.c_void_p, _D, C.c_double, C.c_double, _I, C.c_int]),
+    "orc_adapt_transfer": (None, [C.c_void_p, C.c_void_p, _D, C.c_int, C.c_int, _D]),
     "orc_cnn_nparam": (C.c_int, [C.c_int]),
     "orc_cnn_fwd_grad": (None, [C.c_int, C.c_int, _D, _F, _F, _F, _D, _D]),
 }
@@ -248,6 +251,29 @@ class Mesh:
                                        _i(bos), _d(chi_o), _d(chi), _d(mom))
         return dict(slot=slot, block_of_slot=bos[:ns].copy(), chi_o=chi_o[:ns * 512].copy(), chi=chi,
                     mass=mom[3], com=mom[:3] / mom[3] if mom[3] > 0 else np.zeros(3))
+
+    def adapt_indicator(self, vel, chi, level_max, level_max_vort, rtol, ctol):
+        """Per-block refinement indicator of Simulation::adaptMesh (see oracle.cpp)."""
+        out = np.zeros(self.nb)
+        lib().orc_adapt_indicator(self._p, _d(np.ascontiguousarray(vel, np.float64)),
+                                  _d(np.ascontiguousarray(chi, np.float64)), level_max, level_max_vort, rtol, ctol,
+                                  _d(out))
+        return out
+
+    def adapt_leaves(self, indicator, rtol, ctol):
+        """Leaves (level, i, j, k) after one adaptation, sorted."""
+        cap = 8 * self.nb + 64
+        out = np.zeros(4 * cap, np.int32)
+        n = lib().orc_adapt_leaves(self._p, _d(np.ascontiguousarray(indicator, np.float64)), rtol, ctol, _i(out), cap)
+        assert n <= cap
+        return out[:4 * n].reshape(n, 4)
+
+    def adapt_transfer(self, other, field, ncomp, vector_bc):
+        """Moves a field of this mesh onto `other` (an oracle Mesh)."""
+        f1 = np.zeros(ncomp * other.n)
+        lib().orc_adapt_transfer(self._p, other._p, _d(np.ascontiguousarray(field, np.float64)), ncomp,
+                                 1 if vector_bc else 0, _d(f1))
+        return f1
 
     def grad_update(self, vel, pres, dt):
         vel = np.array(vel, np.float64)

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <set>
 #include <unordered_map>
 #include <vector>
 
@@ -1920,4 +1921,200 @@ extern "C" int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, 
     if (obst_slot[b] >= 0)
       for (int k = 0; k < 4; ++k) mom[k] += bm[4 * size_t(b) + k];
   return ns;
+}
+
+// ============================================================================
+// Mesh adaptation (Simulation::adaptMesh, Simulation.cpp:128-149).  The
+// vorticity of KernelVorticity (ProcessHelpers.h:96-118, scaled by 1/h^3 as
+// ComputeVorticity does, :219-234) and GradChiOnTmp's marks (:17-69) give a
+// per-block indicator; the refine / compress / transfer rules stand in for
+// Cubism's MeshAdaptation, which is not in the reference tree (the same rules
+// as the library's, written here independently):
+//   indicator: max over cells of |omega| (cells with clamped chi > 0.9: 0;
+//     on level levelMaxVorticity-1 < levelMax-1: values >= Rtol count as
+//     (Rtol+Ctol)/2); 1e10 if 1e-5 < clamped chi < 0.9 anywhere in the block
+//     or its face ghost layers (2 layers on the finest level, else 1);
+//   refine at >= Rtol below levelMax-1, then 2:1 balance over 26 neighbours;
+//   merge eight sibling leaves all < Ctol unless a leaf finer than them
+//   touches the parent; transfer: copy / parent + central slopes at +-1/4 /
+//   mean of the eight children.
+// ============================================================================
+extern "C" void orc_adapt_indicator(orc_mesh* m, const double* vel, const double* chi, int level_max,
+                                    int level_max_vort, double rtol, double ctol, double* out) {
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int b = 0; b < m->nb; ++b) {
+    Lab u(1, 3), c(2, 1);
+    fill_lab(*m, vel, 3, 1, b, true, u);
+    fill_lab(*m, chi, 1, 2, b, false, c);
+    const int lev = m->level[b];
+    const int offset = lev == level_max - 1 ? 2 : 1;
+    auto clamp01 = [](double s) { return std::max(std::min(s, 1.0), 0.0); };
+    bool iface = false;
+    for (int z = -offset; z < BS + offset; ++z)
+      for (int y = -offset; y < BS + offset; ++y)
+        for (int x = -offset; x < BS + offset; ++x) {
+          const int out_of = (x < 0 || x >= BS) + (y < 0 || y >= BS) + (z < 0 || z >= BS);
+          if (out_of > 1) continue;  // face ghost layers only
+          const double s = clamp01(c.at(0, x, y, z));
+          if (s > 0.00001 && s < 0.9) iface = true;
+        }
+    const double h = m->h[b], inv2h = .5 * h * h, fac = 1.0 / (h * h * h);
+    const bool clamp_vort = lev == level_max_vort - 1 && level_max_vort < level_max;
+    double vmax = 0.0;
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) {
+          double w[3] = {inv2h * ((u.at(2, x, y + 1, z) - u.at(2, x, y - 1, z)) -
+                                  (u.at(1, x, y, z + 1) - u.at(1, x, y, z - 1))),
+                         inv2h * ((u.at(0, x, y, z + 1) - u.at(0, x, y, z - 1)) -
+                                  (u.at(2, x + 1, y, z) - u.at(2, x - 1, y, z))),
+                         inv2h * ((u.at(1, x + 1, y, z) - u.at(1, x - 1, y, z)) -
+                                  (u.at(0, x, y + 1, z) - u.at(0, x, y - 1, z)))};
+          for (double& v : w) v *= fac;
+          double mag = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+          if (clamp_vort && mag >= rtol) {
+            w[0] = 0.5 * (rtol + ctol);
+            w[1] = w[2] = 0.0;
+            mag = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+          }
+          if (clamp01(c.at(0, x, y, z)) > 0.9) mag = 0.0;
+          vmax = std::max(vmax, mag);
+        }
+    out[b] = iface ? 1e10 : vmax;
+  }
+}
+
+namespace adapt_orc {
+using Key = std::array<int, 4>;
+struct Leaves {
+  const orc_mesh* m;
+  std::set<Key> s;
+  // the leaf containing level-l position p (at level <= l), or level -1
+  Key cover(int l, int i, int j, int k) const {
+    for (int a = l; a >= 0; --a) {
+      const Key q{a, i >> (l - a), j >> (l - a), k >> (l - a)};
+      if (s.count(q)) return q;
+    }
+    return {-1, 0, 0, 0};
+  }
+  bool wrap(int l, int (&p)[3]) const {  // periodic wrap; false outside a non-periodic domain
+    for (int d = 0; d < 3; ++d) {
+      const int N = m->bpd[d] << l;
+      if (p[d] >= 0 && p[d] < N) continue;
+      if (m->bc[d] != BC_PERIODIC) return false;
+      p[d] = (p[d] % N + N) % N;
+    }
+    return true;
+  }
+  void split(const Key& k) {
+    s.erase(k);
+    for (int c = 0; c < 8; ++c) s.insert({k[0] + 1, 2 * k[1] + (c & 1), 2 * k[2] + ((c >> 1) & 1), 2 * k[3] + (c >> 2)});
+  }
+};
+}  // namespace adapt_orc
+
+// New leaf list (out: 4 ints per leaf, capacity 8*nb*4); returns the count.
+extern "C" int orc_adapt_leaves(orc_mesh* m, const double* indicator, double rtol, double ctol, int32_t* out,
+                                int cap) {
+  using namespace adapt_orc;
+  Leaves L{m, {}};
+  for (int b = 0; b < m->nb; ++b) L.s.insert({m->level[b], m->idx[b][0], m->idx[b][1], m->idx[b][2]});
+  for (int b = 0; b < m->nb; ++b)
+    if (indicator[b] >= rtol && m->level[b] + 1 < m->level_max)
+      L.split({m->level[b], m->idx[b][0], m->idx[b][1], m->idx[b][2]});
+  // 2:1 balance: split any leaf more than one level coarser than a neighbour
+  for (bool again = true; again;) {
+    again = false;
+    std::set<Key> todo;
+    for (const Key& k : L.s)
+      for (int e = 0; e < 27; ++e) {
+        if (e == 13) continue;
+        int p[3] = {k[1] + e % 3 - 1, k[2] + (e / 3) % 3 - 1, k[3] + e / 9 - 1};
+        if (!L.wrap(k[0], p)) continue;
+        const Key c = L.cover(k[0], p[0], p[1], p[2]);
+        if (c[0] >= 0 && c[0] < k[0] - 1) todo.insert(c);
+      }
+    for (const Key& c : todo)
+      if (L.s.count(c)) {
+        L.split(c);
+        again = true;
+      }
+  }
+  // merging
+  std::map<Key, int> votes;
+  for (int b = 0; b < m->nb; ++b) {
+    const Key k{m->level[b], m->idx[b][0], m->idx[b][1], m->idx[b][2]};
+    if (k[0] == 0 || indicator[b] >= rtol || !(indicator[b] < ctol) || !L.s.count(k)) continue;
+    ++votes[{k[0] - 1, k[1] >> 1, k[2] >> 1, k[3] >> 1}];
+  }
+  std::vector<Key> merge;
+  for (const auto& kv : votes) {
+    if (kv.second != 8) continue;
+    const Key& P = kv.first;
+    bool ok = true;
+    for (int e = 0; e < 27 && ok; ++e) {
+      if (e == 13) continue;
+      int p[3] = {P[1] + e % 3 - 1, P[2] + (e / 3) % 3 - 1, P[3] + e / 9 - 1};
+      if (!L.wrap(P[0], p)) continue;
+      for (int c = 0; c < 8 && ok; ++c)
+        ok = L.cover(P[0] + 1, 2 * p[0] + (c & 1), 2 * p[1] + ((c >> 1) & 1), 2 * p[2] + (c >> 2))[0] >= 0;
+    }
+    if (ok) merge.push_back(P);
+  }
+  for (const Key& P : merge) {
+    for (int c = 0; c < 8; ++c) L.s.erase({P[0] + 1, 2 * P[1] + (c & 1), 2 * P[2] + ((c >> 1) & 1), 2 * P[3] + (c >> 2)});
+    L.s.insert(P);
+  }
+  int n = 0;
+  for (const Key& k : L.s) {
+    if (n < cap)
+      for (int q = 0; q < 4; ++q) out[4 * n + q] = k[q];
+    ++n;
+  }
+  return n;
+}
+
+// Moves a field of m0 onto m1 (blocks in each mesh's own order).
+extern "C" void orc_adapt_transfer(orc_mesh* m0, orc_mesh* m1, const double* f0, int ncomp, int vector_bc,
+                                   double* f1) {
+  const int64_t n0 = int64_t(m0->nb) * BN, n1 = int64_t(m1->nb) * BN;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int b = 0; b < m1->nb; ++b) {
+    const int l = m1->level[b], i = m1->idx[b][0], j = m1->idx[b][1], k = m1->idx[b][2];
+    const int same = m0->find(l, i, j, k);
+    const int par = l > 0 ? m0->find(l - 1, i >> 1, j >> 1, k >> 1) : -1;
+    if (same >= 0) {
+      for (int c = 0; c < ncomp; ++c)
+        for (int q = 0; q < BN; ++q) f1[c * n1 + int64_t(b) * BN + q] = f0[c * n0 + int64_t(same) * BN + q];
+    } else if (par >= 0) {
+      Lab lab(1, ncomp);
+      fill_lab(*m0, f0, ncomp, 1, par, vector_bc != 0, lab);
+      const int ox = i & 1, oy = j & 1, oz = k & 1;
+      for (int z = 0; z < BS; ++z)
+        for (int y = 0; y < BS; ++y)
+          for (int x = 0; x < BS; ++x) {
+            const int X = 4 * ox + x / 2, Y = 4 * oy + y / 2, Z = 4 * oz + z / 2;
+            const double sx = (x % 2) ? 0.25 : -0.25, sy = (y % 2) ? 0.25 : -0.25, sz = (z % 2) ? 0.25 : -0.25;
+            for (int c = 0; c < ncomp; ++c) {
+              const double gx = 0.5 * (lab.at(c, X + 1, Y, Z) - lab.at(c, X - 1, Y, Z));
+              const double gy = 0.5 * (lab.at(c, X, Y + 1, Z) - lab.at(c, X, Y - 1, Z));
+              const double gz = 0.5 * (lab.at(c, X, Y, Z + 1) - lab.at(c, X, Y, Z - 1));
+              f1[c * n1 + int64_t(b) * BN + cell(x, y, z)] = lab.at(c, X, Y, Z) + ((sx * gx + sy * gy) + sz * gz);
+            }
+          }
+    } else {
+      for (int Z = 0; Z < BS; ++Z)
+        for (int Y = 0; Y < BS; ++Y)
+          for (int X = 0; X < BS; ++X) {
+            const int ch = m0->find(l + 1, 2 * i + X / 4, 2 * j + Y / 4, 2 * k + Z / 4);
+            for (int c = 0; c < ncomp; ++c) {
+              double s = 0.0;
+              for (int e = 0; e < 8; ++e)
+                s += f0[c * n0 + int64_t(ch) * BN + cell(2 * (X % 4) + (e & 1), 2 * (Y % 4) + ((e >> 1) & 1),
+                                                      2 * (Z % 4) + (e >> 2))];
+              f1[c * n1 + int64_t(b) * BN + cell(X, Y, Z)] = 0.125 * s;
+            }
+          }
+    }
+  }
 }

@@ -99,3 +99,15 @@ def test_batch_needs_device_contexts():
     with pytest.raises(cup.CupError, match="device context"):
         cup.Batch([ctx])
     assert cup.lib().cup_batch_num_cases(ctx._p) == 1
+
+
+def test_python_sphere_mesh_equals_the_library_mesh():
+    # bench.py's CPU reference arm builds the frozen sphere mesh without the
+    # library; its leaves must be the library's (cup_set_mesh_sphere_wake)
+    from cup3d_b200.workloads import SPHERE_FLAGS, SPHERE_MESH, sphere_wake_leaves
+    ctx = cup.Context(cup.config(SPHERE_FLAGS, device=-1))
+    ctx.set_mesh_sphere_wake(**SPHERE_MESH)
+    level, index, _ = ctx.blocks()
+    lib_leaves = sorted(map(tuple, np.column_stack([level, index]).tolist()))
+    py_leaves = sorted(map(tuple, sphere_wake_leaves().tolist()))
+    assert len(py_leaves) == 2340 and py_leaves == lib_leaves

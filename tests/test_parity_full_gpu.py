@@ -5,9 +5,9 @@ at 1e-10 relative per step.
   four-level mesh (1.2M cells), WENO5, implicit penalization lambda = 1e6,
   uinf = -0.1, CFL 0.3 ramped over 100 steps, from rest.  Each compared step
   starts the oracle from the device's state (velocity and pressure) and
-  compares the step's velocity and pressure (Simulation.cpp:377-412:
-  AdvectionDiffusion, Penalization, PressureProjection), both sides solving
-  the Poisson equation by FP64 iterative refinement to below 1e-12.
+  compares each operator of the step (Simulation.cpp:377-412:
+  AdvectionDiffusion, Penalization, PressureProjection) at 1e-12, and the
+  whole step at the accuracy the Poisson solve allows there (see the test).
 * The Taylor-Green vortex 32^3 (nu 0.01, CFL 0.3, upwind5) for its 100
   steps, device and oracle each evolving on their own.
 * The mixed-precision solve (FP32 inner, FP64 refinement) on the sphere mesh
@@ -66,12 +66,17 @@ def _refined(solve, apply, b, mb, hh3, rounds=3):
 
 
 def test_sphere_workload_steps_match_oracle():
-    # BiCGSTAB alone stalls near 3e-10 relative on these right-hand sides
-    # (step 0 from rest: the implicit penalization's jump at the body), on
-    # the device and in the oracle alike.  Both sides therefore solve by FP64
-    # iterative refinement around their own BiCGSTAB (1e-7 per round), which
-    # takes the true residual to the FP64 floor; the device does it through
-    # the split projection (cup_pressure_rhs, solves, cup_pressure_finish).
+    # Per compared step, from the same state on both sides:
+    #  * every operator of the step agrees to 1e-12: advection-diffusion
+    #    (WENO5, 3 RK stages), penalization, the Poisson right-hand side, and
+    #    the end of the projection (mean, p_old, gradient) given the same
+    #    pressure increment;
+    #  * the whole step (each side solving its own Poisson equation by FP64
+    #    iterative refinement around its BiCGSTAB) agrees to the accuracy the
+    #    solve allows: on this mesh the true residual of either solver stalls
+    #    near 1e-10 (the FP64 floor eps ||A|| ||x|| / ||b|| of the pinned
+    #    Neumann problem; 2e-9 to 6e-9 once the flow has developed), where the
+    #    solution is determined to about 1e-6 (velocity) and 1e-5 (pressure).
     import torch
     ctx = _sphere_ctx("-poissonTol 0 -poissonTolRel 1e-7 -stepGraph 0")
     m = oracle_mesh(ctx)
@@ -99,32 +104,50 @@ def test_sphere_workload_steps_match_oracle():
     def orc_solve(r):
         return m.bicgstab_gpu(r, tol=0.0, tol_rel=1e-7)[0]
 
+    def finish_ref(v, x, pres0, dt, step):
+        p = x - np.sum(x * hh3) / np.sum(hh3)  # zero mean, PressureProjection.cpp:404-431
+        if step > ctx.cfg.step_2nd_start:
+            p = p + pres0                      # :435-446
+        return m.grad_update(v, p, dt), p
+
     for step in range(4):
         vel0, pres0 = ctx.download("vel"), ctx.download("pres")
         dt = ctx.compute_dt(step)
         assert abs(dt - oracle.dt(m.hmin, nu, ctx.cfg.cfl, m.max_u(vel0, uinf), step, ctx.cfg.rampup)) <= 1e-13 * dt
         ctx.advect_diffuse(dt)
+        compare = step in (0, 3)  # step 0 from rest, step 3 with the p_old terms
+        if compare:
+            v_ref = m.advect_diffuse(vel0, dt, nu, uinf=uinf, scheme=1)
+            e_adv = rel(ctx.download("vel"), v_ref)
         ctx.penalize(dt)
+        if compare:
+            v_ref, _ = m.penalize(v_ref, chi, slot, chi_o, udef_o, kin, dt, lam=lam, implicit=1)
+            v_pen = ctx.download("vel")
+            e_pen = rel(v_pen, v_ref)
         ctx.pressure_rhs(dt, step)
-        x_dev, hist_dev = _refined(dev_solve, dev_apply, ctx.download("lhs"), mb, hh3)
-        ctx.upload("pres", x_dev)  # the increment while the projection is open
-        ctx.pressure_finish(dt, step)
-        if step in (1, 2):  # compared: step 0 (from rest) and step 3 (p_old term on)
+        b_dev = ctx.download("lhs")
+        x_dev, hist_dev = _refined(dev_solve, dev_apply, b_dev, mb, hh3)
+        if not compare:
+            ctx.upload("pres", x_dev)
+            ctx.pressure_finish(dt, step)
             continue
-        # the oracle's step from the same state with the same dt
-        v = m.advect_diffuse(vel0, dt, nu, uinf=uinf, scheme=1)
-        v, _ = m.penalize(v, chi, slot, chi_o, udef_o, kin, dt, lam=lam, implicit=1)
-        lhs = m.pressure_rhs(v, pres0, dt, step, chi=chi, slot=slot, chi_o=chi_o, udef_o=udef_o)
-        x_orc, hist_orc = _refined(orc_solve, m.apply, lhs, mb, hh3)
-        p = x_orc - np.sum(x_orc * hh3) / np.sum(hh3)  # zero mean, PressureProjection.cpp:404-431
-        if step > ctx.cfg.step_2nd_start:
-            p = p + pres0                              # :435-446
-        v = m.grad_update(v, p, dt)
-        ev, ep = rel(ctx.download("vel"), v), rel(ctx.download("pres"), p)
-        print(f"sphere step {step}: dt {dt:.6e} vel {ev:.2e} pres {ep:.2e}; true residual per round "
-              f"device {['%.1e' % r for r in hist_dev]} oracle {['%.1e' % r for r in hist_orc]}")
-        assert hist_dev[-1] < 1e-12 and hist_orc[-1] < 1e-12
-        assert ev < STEP_TOL and ep < STEP_TOL, (step, ev, ep)
+        lhs_ref = m.pressure_rhs(v_pen, pres0, dt, step, chi=chi, slot=slot, chi_o=chi_o, udef_o=udef_o)
+        e_rhs = rel(b_dev, lhs_ref)
+        x_orc, hist_orc = _refined(orc_solve, m.apply, lhs_ref, mb, hh3)
+        # the end of the projection with the oracle's increment on both sides
+        ctx.upload("pres", x_orc)
+        ctx.pressure_finish(dt, step)
+        v_fin, p_fin = finish_ref(v_pen, x_orc, pres0, dt, step)
+        e_fin_v, e_fin_p = rel(ctx.download("vel"), v_fin), rel(ctx.download("pres"), p_fin)
+        # the whole step: each side with its own solve
+        v_own, p_own = finish_ref(v_pen, x_dev, pres0, dt, step)
+        e_step_v, e_step_p = rel(v_own, v_fin), rel(p_own, p_fin)
+        print(f"sphere step {step}: dt {dt:.6e}; operators: advect {e_adv:.1e} penalize {e_pen:.1e} rhs {e_rhs:.1e} "
+              f"projection end vel {e_fin_v:.1e} pres {e_fin_p:.1e}; whole step vel {e_step_v:.1e} pres {e_step_p:.1e}; "
+              f"true residual per round device {['%.1e' % r for r in hist_dev]} oracle {['%.1e' % r for r in hist_orc]}")
+        assert max(e_adv, e_pen, e_rhs, e_fin_v, e_fin_p) < 1e-12
+        assert hist_dev[-1] < 1e-8 and hist_orc[-1] < 1e-8
+        assert e_step_v < 1e-6 and e_step_p < 1e-5
 
 
 def test_tgv_100_steps_match_oracle():
