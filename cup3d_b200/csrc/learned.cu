@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "context.h"
+#include "lmap.cuh"
 
 namespace cup3d {
 
@@ -39,6 +40,13 @@ __global__ void __launch_bounds__(NT) k_sumsq(const float* __restrict__ v, size_
   if (grid_reduce<1>(acc, g, red) && threadIdx.x == 0) *out = acc[0];
 }
 
+// out = x + a y
+__global__ void k_axpy(size_t n, const double* __restrict__ x, double a, const double* __restrict__ y,
+                       double* __restrict__ out) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    out[i] = x[i] + a * y[i];
+}
+
 __global__ void k_scale(float* v, size_t n, float s) {
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) v[i] *= s;
 }
@@ -68,6 +76,7 @@ static int scale_output_layer(cup_ctx* c, float s) {
 static int set_params(cup_ctx* c, const float* p) {
   if (int rc = ensure_cnn(c)) return rc;
   CUP_CUDA_TRY(stream_h2d(c->stream, c->cnn.W.master, p, CNN_NPARAM * sizeof(float)));
+  c->cnn.folded = false;
   if (int rc = cnn_pack(c->cnn.W, c->stream)) return rc;
   CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
   c->cnn.ready = true;
@@ -79,6 +88,42 @@ static int set_params(cup_ctx* c, const float* p) {
 
 static bool dev_ok(cup_ctx* c) { return c && !c->host_only && c->mesh.nb > 0; }
 
+// The learned map's two phases as kernels of their own (the solver runs
+// them inside its persistent launch).
+__global__ void __launch_bounds__(256) k_lmap_gather(DevMesh M, const double* v, uint16_t* lab) {
+  __shared__ double labd[LMAP_K];
+  lmap_gather<double>(M, v, lab, labd);
+}
+
+__global__ void __launch_bounds__(256) k_lmap_gemm(DevMesh M, const uint4* W, const uint16_t* lab, double* z) {
+  extern __shared__ __align__(16) unsigned char lmap_smem[];
+  (void)lmap_gemm<double>(M, W, lab, z, reinterpret_cast<uint16_t*>(lmap_smem));
+}
+
+int lmap_prepare(cup_ctx* c, LocalMap* out) {
+  CnnState& S = c->cnn;
+  if (!S.ready) return set_error(CUP_ERR_STATE, "learned preconditioner has no weights (cup_cnn_init / cup_cnn_set_params)");
+  if (!S.lmap_w) {
+    if (int rc = S.arena.alloc(&S.lmap_w, LMAP_W_WORDS)) return rc;
+    if (int rc = S.arena.alloc(&S.fold_in, size_t(LMAP_K) * 1000)) return rc;
+    if (int rc = S.arena.alloc(&S.fold_out, size_t(LMAP_K) * BN)) return rc;
+    S.folded = false;
+  }
+  const size_t need = size_t(c->mesh.nb) * LMAP_K;
+  if (S.lab_cap < need) {
+    S.lab_arena.release();
+    S.lab_cap = 0;
+    if (int rc = S.lab_arena.alloc(&S.lmap_lab, need)) return rc;
+    S.lab_cap = need;
+  }
+  if (!S.folded) {
+    if (int rc = cnn_fold(S.W, S.fold_in, S.fold_out, S.lmap_w, S.gpart, S.train_grid, c->stream)) return rc;
+    S.folded = true;
+  }
+  *out = LocalMap{S.lmap_w, S.lmap_lab};
+  return 0;
+}
+
 }  // namespace cup3d
 
 using namespace cup3d;
@@ -89,17 +134,18 @@ int32_t cup_cnn_num_params(void) { return CNN_NPARAM; }
 
 int cup_cnn_init(cup_ctx* c, uint64_t seed) {
   if (!c || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_init: no device context");
-  // He-normal weights (fan-in 27 * C_in), zero biases; the last layer starts
-  // small so the preconditioner starts as the block inverse.
+  // Variance-preserving normal weights for linear layers (1 / fan-in, fan-in
+  // 27 C_in); the last layer starts small, so the preconditioner starts close
+  // to the two-level one without the network.
   std::mt19937_64 g(seed);
   std::normal_distribution<float> n01(0.f, 1.f);
   std::vector<float> p(CNN_NPARAM, 0.f);
   auto fill = [&](int off, int cnt, float stdv) {
     for (int i = 0; i < cnt; ++i) p[off + i] = stdv * n01(g);
   };
-  fill(OFF_W0, CNN_W0, std::sqrt(2.f / 27.f));
-  fill(OFF_W1, CNN_W1, std::sqrt(2.f / (27.f * CNN_C)));
-  fill(OFF_W2, CNN_W2, std::sqrt(2.f / (27.f * CNN_C)));
+  fill(OFF_W0, CNN_W0, std::sqrt(1.f / 27.f));
+  fill(OFF_W1, CNN_W1, std::sqrt(1.f / (27.f * CNN_C)));
+  fill(OFF_W2, CNN_W2, std::sqrt(1.f / (27.f * CNN_C)));
   fill(OFF_W3, CNN_W3, 0.01f * std::sqrt(1.f / (27.f * CNN_C)));
   if (int rc = set_params(c, p.data())) return ctx_fail(c, rc, cup_last_error(nullptr));
   return 0;
@@ -137,7 +183,19 @@ int cup_cnn_dataset_add(cup_ctx* c, const double* d_r, const double* d_e) {
   CnnState& S = c->cnn;
   if (S.cap == 0) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_dataset_add: no dataset (cup_cnn_dataset_reserve)");
   if (S.count >= S.cap) return 0;
-  if (int rc = cnn_dataset_add(c->dm, d_r, d_e, S.ds_in, S.ds_target, S.count, S.cap, S.ds_count, c->W.grid,
+  // The network adds to the coarse correction and the block inverse of the
+  // two-level preconditioner: its target is what they leave of the error,
+  // e - P A_c^-1 P^T r (the block inverse's part is removed per sample).
+  if (int rc = coarse_build(c)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  double* zc = c->W.t;
+  double* rest = c->W.nu;
+  const size_t n = nbn(c);
+  CUP_CUDA_TRY(cudaMemsetAsync(zc, 0, n * sizeof(double), c->stream));
+  if (int rc = coarse_apply<double>(c->coarse.view(), d_r, zc, nullptr, c->num_sms, c->stream))
+    return ctx_fail(c, rc, cup_last_error(nullptr));
+  k_axpy<<<c->W.grid, NT, 0, c->stream>>>(n, d_e, -1.0, zc, rest);
+  CUP_CUDA_TRY(cudaGetLastError());
+  if (int rc = cnn_dataset_add(c->dm, d_r, rest, S.ds_in, S.ds_target, S.count, S.cap, S.ds_count, c->W.grid,
                                c->stream))
     return ctx_fail(c, rc, cup_last_error(nullptr));
   S.count = std::min(S.cap, S.count + c->mesh.nb);
@@ -170,7 +228,8 @@ int cup_cnn_train(cup_ctx* c, int32_t steps, int32_t batch, float lr, uint64_t s
   if (int rc = scale_output_layer(c, float(1.0 / rms))) return ctx_fail(c, rc, cup_last_error(nullptr));
   int train_rc = 0;
   std::mt19937_64 g(seed);
-  std::uniform_int_distribution<int> pick(0, S.count - 1);
+  const int ntrain = S.count - std::min(S.ntest, S.count - 1);
+  std::uniform_int_distribution<int> pick(0, ntrain - 1);
   std::vector<int> idx(batch);
   for (int it = 0; it < steps && !train_rc; ++it) {
     for (int i = 0; i < batch; ++i) idx[i] = pick(g);
@@ -194,11 +253,45 @@ int cup_cnn_train(cup_ctx* c, int32_t steps, int32_t batch, float lr, uint64_t s
     e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) train_rc = set_cuda_error(e, "train", __FILE__, __LINE__);
   }
+  c->cnn.folded = false;
   const int back_rc = scale_output_layer(c, float(rms));
   if (train_rc || back_rc) return ctx_fail(c, train_rc ? train_rc : back_rc, cup_last_error(nullptr));
   if (int rc = cnn_pack(S.W, c->stream)) return ctx_fail(c, rc, cup_last_error(nullptr));
   if (cudaError_t e = cudaStreamSynchronize(c->stream))
     return ctx_fail(c, set_cuda_error(e, "train", __FILE__, __LINE__), cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_cnn_holdout(cup_ctx* c, int32_t ntest) {
+  if (!c || ntest < 0) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_holdout: bad arguments");
+  c->cnn.ntest = ntest;
+  return 0;
+}
+
+int cup_cnn_eval(cup_ctx* c, float* rel_loss) {
+  ProfBind pb_(c);
+  if (!c || !rel_loss || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_eval: bad arguments");
+  CnnState& S = c->cnn;
+  if (!S.ready) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_eval: no weights");
+  const int nt = std::min(S.ntest, S.count);
+  if (nt <= 0) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_eval: no held-out samples (cup_cnn_holdout)");
+  const int first = S.count - nt;
+  const float* in = S.ds_in + size_t(first) * 1000;
+  const float* tg = S.ds_target + size_t(first) * BN;
+  // the residual-norm loss of the network and of the zero prediction over them
+  double err = 0.0, ms = 0.0;
+  for (int b0 = 0; b0 < nt; b0 += S.train_grid) {
+    const int nb_ = std::min(S.train_grid, nt - b0);
+    for (int zero = 0; zero < 2; ++zero) {
+      if (int rc = cnn_residual_loss(S.W, in + size_t(b0) * 1000, tg + size_t(b0) * BN, nb_, zero, S.gpart, S.loss,
+                                     S.train_grid, c->stream))
+        return ctx_fail(c, rc, cup_last_error(nullptr));
+      float l = 0.f;
+      CUP_CUDA_TRY(stream_d2h(c->stream, &l, S.loss, sizeof(float)));
+      (zero ? ms : err) += double(l) * nb_;
+    }
+  }
+  *rel_loss = float(ms > 0 ? err / ms : 0.0);
   return 0;
 }
 
@@ -255,8 +348,27 @@ int cup_cnn_precond_dev(cup_ctx* c, const double* d_r, double* d_z) {
   return 0;
 }
 
+int cup_cnn_map_apply_dev(cup_ctx* c, const double* d_r, double* d_z) {
+  ProfBind pb_(c);
+  if (!dev_ok(c) || !d_r || !d_z) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_map_apply_dev: bad arguments");
+  LocalMap lm{};
+  if (int rc = lmap_prepare(c, &lm)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  if (int rc = launch_block_inverse(c->dm, d_r, d_z, c->W, c->stream)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  const int grid = std::max(1, std::min(c->num_sms * 2, c->mesh.nb));
+  k_lmap_gather<<<grid, 256, 0, c->stream>>>(c->dm, d_r, c->cnn.lmap_lab);
+  CUP_CUDA_TRY(cudaGetLastError());
+  static unsigned long long attr = 0;
+  if (first_on_device(attr))
+    CUP_CUDA_TRY(cudaFuncSetAttribute(k_lmap_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LMAP_TILE_BYTES)));
+  k_lmap_gemm<<<grid, 256, LMAP_TILE_BYTES, c->stream>>>(c->dm, lm.w, lm.lab, d_z);
+  CUP_CUDA_TRY(cudaGetLastError());
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_map_apply", __FILE__, __LINE__), cup_last_error(nullptr));
+  return 0;
+}
+
 int cup_set_poisson(cup_ctx* c, int32_t solver, double tol_abs, double tol_rel, int32_t max_iter) {
-  if (!c || solver < 0 || solver > CUP_POISSON_B200_LEARNED_MIXED || max_iter < 0)
+  if (!c || solver < 0 || solver > CUP_POISSON_B200_TWOLEVEL || max_iter < 0)
     return ctx_fail(c, CUP_ERR_ARG, "cup_set_poisson: bad arguments");
   c->cfg.poisson_solver = solver;
   c->cfg.poisson_tol = tol_abs;

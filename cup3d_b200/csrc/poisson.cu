@@ -19,9 +19,9 @@
 #include <cmath>
 #include <cstring>
 
-#include "cnn.cuh"
 #include "fd.cuh"
 #include "group.cuh"
+#include "lmap.cuh"
 #include "poisson.cuh"
 #include "profiler.h"
 #include "cup3d_b200.h"
@@ -362,8 +362,18 @@ struct KArgs {
   GridReduce g;
   int mean_mode;
   int zero_mean_row;  // b and x0 are zero at the mean row (getVec, modes 1 and 3)
-  int ext_precond;    // 1: kernels a and c only update p and s; a separate kernel applies the preconditioner
   int ncache;         // persistent solver: block entries staged per group at launch (<= KB_CACHE)
+  // two-level preconditioner (persistent solver): A_c^-1 (cnb x cnb, cnb = 0:
+  // none), the restricted vectors of zv and zr and the blocks' 512 h^3
+  int cnb;
+  const double* cinv;
+  double* crc_v;
+  double* crc_r;
+  const double* cw;
+  // learned local map (persistent solver, lmap.cuh): W in fragment order
+  // (null: none) and the [nb][896] BF16 lab buffer
+  const uint4* lw;
+  uint16_t* llab;
 };
 
 template <class T>
@@ -507,7 +517,6 @@ __device__ __forceinline__ double phase_a(const KArgs<T>& A, const GroupIdx& G, 
       for (int z = 0; z < 8; ++z) p[z] = double(T(r[z] + beta * (pp[z] - omega * nu[z])));
     }
     store_col(A.p, b, G, p);
-    if (A.ext_precond) continue;  // z1 comes from the external preconditioner
     const double h = M.h[b];
     block_inverse_group(p, tile, G, h, inv);
     double s = 0.0;
@@ -568,7 +577,6 @@ __device__ __forceinline__ double phase_c(const KArgs<T>& A, const GroupIdx& G, 
 #pragma unroll
     for (int z = 0; z < 8; ++z) r[z] = double(T(r[z] - alpha * nu[z]));
     store_col(A.r, b, G, r);
-    if (A.ext_precond) continue;  // z2 comes from the external preconditioner
     const double h = M.h[b];
     block_inverse_group(r, tile, G, h, inv);
     double s = 0.0;
@@ -701,10 +709,8 @@ __global__ void __launch_bounds__(NT) k_bicg_a(KArgs<T> A) {
   __shared__ double red[64];
   __shared__ double inv_eig[BN];
   const GroupIdx G;
-  if (!A.ext_precond) {  // independent of the previous kernel: overlaps its tail
-    fd_fill_inverse_eigen(inv_eig, c_lam);
-    __syncthreads();
-  }
+  fd_fill_inverse_eigen(inv_eig, c_lam);  // independent of the previous kernel: overlaps its tail
+  __syncthreads();
   pdl_wait();
   pdl_launch_dependents();
   const KrylovState& S = *A.st;
@@ -733,10 +739,8 @@ __global__ void __launch_bounds__(NT) k_bicg_c(KArgs<T> A) {
   __shared__ double red[64];
   __shared__ double inv_eig[BN];
   const GroupIdx G;
-  if (!A.ext_precond) {  // independent of the previous kernel: overlaps its tail
-    fd_fill_inverse_eigen(inv_eig, c_lam);
-    __syncthreads();
-  }
+  fd_fill_inverse_eigen(inv_eig, c_lam);  // independent of the previous kernel: overlaps its tail
+  __syncthreads();
   pdl_wait();
   pdl_launch_dependents();
   const KrylovState& S = *A.st;
@@ -867,6 +871,50 @@ __device__ __forceinline__ double init_block(const KArgs<T>& A, const GroupIdx& 
 
 // Phase bodies for one block (bi) of a group; the persistent solvers loop
 // them over the group's blocks.
+// Sum of v over the 64 threads of a group, in a fixed order; every thread of
+// the group gets the totals.  gsm: 2 * NR doubles of the group.
+template <int NR>
+__device__ __forceinline__ void group_reduce(double (&v)[NR], double* gsm, const GroupIdx& G) {
+#pragma unroll
+  for (int r = 0; r < NR; ++r)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_xor_sync(0xffffffffu, v[r], o);
+  if ((G.lane & 31) == 0)
+#pragma unroll
+    for (int r = 0; r < NR; ++r) gsm[(G.lane >> 5) * NR + r] = v[r];
+  group_sync(G.g);
+#pragma unroll
+  for (int r = 0; r < NR; ++r) v[r] = gsm[r] + gsm[NR + r];
+  group_sync(G.g);
+}
+
+// Two-level preconditioner in the persistent solver: the restriction of a
+// vector is its block sums (lane 0 of the group writes rc[b]); the coarse
+// correction of block b is yc = row b of A_c^-1 times rc, added to every cell
+// of the block (the group reads its row, 8 * nb bytes, coalesced).  Returns
+// yc 512 h^3, the correction's part of sum(v h^3), in lane 0 (0 elsewhere).
+__device__ __forceinline__ void coarse_restrict(const double c[8], double* rc, int b, double* gsm, const GroupIdx& G) {
+  double s[1] = {((c[0] + c[1]) + (c[2] + c[3])) + ((c[4] + c[5]) + (c[6] + c[7]))};
+  group_reduce<1>(s, gsm, G);
+  if (G.lane == 0) rc[b] = s[0];
+}
+
+template <class T>
+__device__ __forceinline__ double coarse_block(const KArgs<T>& A, const GroupIdx& G, int b, const double* rc, T* v,
+                                               double* gsm) {
+  const double* row = A.cinv + size_t(b) * A.cnb;
+  double s[1] = {0.0};
+  for (int j = G.lane; j < A.cnb; j += GROUP) s[0] += row[j] * __ldcg(rc + j);
+  group_reduce<1>(s, gsm, G);
+  const double yc = s[0];
+  double c[8];
+  load_col(v, b, G, c);
+#pragma unroll
+  for (int z = 0; z < 8; ++z) c[z] = double(T(c[z] + yc));
+  store_col(v, b, G, c);
+  return G.lane == 0 ? yc * A.cw[b] : 0.0;  // summed over the CTA's threads by the grid reduction
+}
+
 // P0 (once): zr = M^-1 r for the initial residual; sum(zr h^3)
 template <class T>
 __device__ __forceinline__ double p0_block(const KArgs<T>& A, const GroupIdx& G, GroupTile& tile,
@@ -876,6 +924,7 @@ __device__ __forceinline__ double p0_block(const KArgs<T>& A, const GroupIdx& G,
   const double h = bi.h;
   double c[8];
   load_col(A.r, b, G, c);
+  if (A.cnb) coarse_restrict(c, A.crc_r, b, ftile.v[0][0] + 0, G);
   block_inverse_group(c, ftile, G, h, inv);
   double s = 0.0;
 #pragma unroll
@@ -916,6 +965,7 @@ __device__ __forceinline__ void p1_block(const KArgs<T>& A, const GroupIdx& G, G
     acc[0] += rh[z] * y[z];
   }
   store_col(A.nu, b, G, y);
+  if (A.cnb) coarse_restrict(y, A.crc_v, b, ftile.v[0][0] + 0, G);
   block_inverse_group(y, ftile, G, h, inv);
   double s = 0.0;
 #pragma unroll
@@ -994,6 +1044,7 @@ __device__ __forceinline__ void p3_block(const KArgs<T>& A, const GroupIdx& G, G
     store_col(xn, b, G, x);
     store_col(A.p, b, G, q);
   }
+  if (A.cnb) coarse_restrict(rn, A.crc_r, b, ftile.v[0][0] + 0, G);
   block_inverse_group(rn, ftile, G, h, inv);
   double s = 0.0;
 #pragma unroll
@@ -1010,21 +1061,28 @@ __device__ __forceinline__ void p3_block(const KArgs<T>& A, const GroupIdx& G, G
 // the finalizers to the grid totals of each phase, so all copies stay equal;
 // CTA 0 writes the state back at the end.  Data written by other CTAs is read
 // after the grid barrier's acquire.
-// Dynamic shared memory: PGROUPS tiles, the inverse eigenvalues (BN doubles),
-// PGROUPS * KB_CACHE block entries.
-constexpr size_t kPersistentSmem = PGROUPS * sizeof(GroupTile) + BN * sizeof(double) +
-                                   PGROUPS * KB_CACHE * sizeof(BlockInfo);
+// Dynamic shared memory: the inverse eigenvalues (BN doubles), PGROUPS *
+// KB_CACHE block entries, PGROUPS tiles.  The learned map's phases use the
+// tiles' space as scratch (the lab of the gather, the staged labs of a GEMM
+// tile), which is longer than the tiles: kLearnedSmem.
+constexpr size_t kSmemCache = BN * sizeof(double);
+constexpr size_t kSmemTiles = kSmemCache + PGROUPS * KB_CACHE * sizeof(BlockInfo);
+constexpr size_t kPersistentSmem = kSmemTiles + PGROUPS * sizeof(GroupTile);
+constexpr size_t kLearnedSmem = std::max(kPersistentSmem, kSmemTiles + LMAP_TILE_BYTES);
+static_assert(kSmemTiles % 16 == 0, "tiles and staged labs start 16-byte aligned");
+static_assert(LMAP_K * sizeof(double) <= PGROUPS * sizeof(GroupTile), "the gather's lab fits in the tiles");
 
 template <class T>
 __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A, GridSync Gs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw);
-  double* inv_eig = reinterpret_cast<double*>(smem_raw + PGROUPS * sizeof(GroupTile));
-  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + PGROUPS * sizeof(GroupTile) + BN * sizeof(double));
+  double* inv_eig = reinterpret_cast<double*>(smem_raw);
+  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + kSmemCache);
+  GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw + kSmemTiles);
   __shared__ double red[64];
   __shared__ KrylovState S;
   __shared__ double ms_zr;  // sum(zr h^3) of the current zr
   __shared__ unsigned int epoch;
+  __shared__ double gred[2 * PGROUPS];  // per-group reduction scratch of the coarse phases
   const GroupIdx G;
   const DevMesh& M = A.M;
   GroupTile& tile = tiles[G.g];
@@ -1056,12 +1114,39 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
     if (threadIdx.x == 0) fin_init(S, a[0]);
     __syncthreads();
   }
+  // The parts of the preconditioner that need the whole vector v (nu or r)
+  // in place, added to its block part z (zv or zr):
+  //   * the coarse correction of the two-level preconditioner, from v's
+  //     restriction rc: every group adds it on its blocks;
+  //   * the learned local map (lmap.cuh): the CTAs gather v's labs, then,
+  //     after a grid barrier, the GEMM adds W lab / h.
+  // The grid sum of the added sum(z h^3) comes back in every CTA.  One grid
+  // barrier, two with the learned map.
+  auto extra_phases = [&](const double* rc, const T* v, T* z, double& added) -> bool {
+    double a[1] = {0.0};
+    if (A.cnb) PERSISTENT_BLOCKS(bi) a[0] += coarse_block<T>(A, G, bi.id, rc, z, &gred[2 * G.g]);
+    if (A.lw) {
+      __syncthreads();  // the groups are done with their tiles
+      lmap_gather<T>(M, v, A.llab, reinterpret_cast<double*>(smem_raw + kSmemTiles));
+    }
+    if (!grid_allreduce<1>(a, Gs, epoch, red)) return false;
+    added = a[0];
+    if (A.lw) {
+      double l[1] = {lmap_gemm<T>(M, A.lw, A.llab, z, reinterpret_cast<uint16_t*>(smem_raw + kSmemTiles))};
+      if (!grid_allreduce<1>(l, Gs, epoch, red)) return false;
+      added += l[0];
+    }
+    return true;
+  };
+  const bool extra = A.cnb || A.lw;
   if (ok && !S.done) {
     double a[1] = {0.0};
     PERSISTENT_BLOCKS(bi) a[0] += p0_block<T>(A, G, tile, bi, inv_eig);
     ok = grid_allreduce<1>(a, Gs, epoch, red);
+    double cz = 0.0;
+    if (ok && extra) ok = extra_phases(A.crc_r, A.r, A.z1, cz);
     // q = 0 at the start (init_block), so z1 = zr
-    if (threadIdx.x == 0) ms_zr = S.mean_sum = a[0];
+    if (threadIdx.x == 0) ms_zr = S.mean_sum = a[0] + cz;
     __syncthreads();
   }
   while (ok && !S.done) {
@@ -1077,6 +1162,12 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
       S.mean_sum = ms_zr - S.alpha * a[1];  // sum(z2 h^3)
     }
     __syncthreads();
+    if (extra) {  // zv += the rest of M^-1 nu; sum(z2 h^3) with it
+      double cv = 0.0;
+      if (!(ok = extra_phases(A.crc_v, A.nu, A.z2, cv))) break;
+      if (threadIdx.x == 0) S.mean_sum = ms_zr - S.alpha * (a[1] + cv);
+      __syncthreads();
+    }
     double d[2] = {0.0, 0.0};
     PERSISTENT_BLOCKS(bi) p2_block<T>(A, G, tile, bi, S.alpha, S.mean_sum, d);
     if (!(ok = grid_allreduce<2>(d, Gs, epoch, red))) break;
@@ -1094,6 +1185,15 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
       S.mean_sum = S.restart_pending ? e[2] : e[2] + S.beta * e[3];
     }
     __syncthreads();
+    if (extra && !S.done) {  // zr += the rest of M^-1 r; the sums with it
+      double cr = 0.0;
+      if (!(ok = extra_phases(A.crc_r, A.r, A.z1, cr))) break;
+      if (threadIdx.x == 0) {
+        ms_zr = e[2] + cr;
+        S.mean_sum = S.restart_pending ? ms_zr : ms_zr + S.beta * e[3];
+      }
+      __syncthreads();
+    }
   }
   // every CTA holds the final state: its groups move the best iterate into
   // x (slot 0) block by block
@@ -1123,23 +1223,6 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
 // has stopped leaves its vectors alone; the launch ends when every case has
 // stopped.  Preparation (x0's mean row, sum(x0 h^3)), the initial residual
 // and zr = M^-1 r run in the same launch.
-
-// Sum of v over the 64 threads of a group, in a fixed order; every thread of
-// the group gets the totals.  gsm: 2 * NR doubles of the group.
-template <int NR>
-__device__ __forceinline__ void group_reduce(double (&v)[NR], double* gsm, const GroupIdx& G) {
-#pragma unroll
-  for (int r = 0; r < NR; ++r)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_xor_sync(0xffffffffu, v[r], o);
-  if ((G.lane & 31) == 0)
-#pragma unroll
-    for (int r = 0; r < NR; ++r) gsm[(G.lane >> 5) * NR + r] = v[r];
-  group_sync(G.g);
-#pragma unroll
-  for (int r = 0; r < NR; ++r) v[r] = gsm[r] + gsm[NR + r];
-  group_sync(G.g);
-}
 
 struct BatchArgs {
   const int* cfirst;
@@ -1291,9 +1374,9 @@ __device__ __forceinline__ void batch_fill_cache(const DevMesh& M, const BatchAr
 template <class T>
 __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, GridSync Gs, BatchArgs B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw);
-  double* inv_eig = reinterpret_cast<double*>(smem_raw + PGROUPS * sizeof(GroupTile));
-  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + PGROUPS * sizeof(GroupTile) + BN * sizeof(double));
+  double* inv_eig = reinterpret_cast<double*>(smem_raw);
+  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + kSmemCache);
+  GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw + kSmemTiles);
   int* gfirst = reinterpret_cast<int*>(smem_raw + kPersistentSmem);
   int* gfirst_prev = gfirst + B.ncase + 1;
   int* running = gfirst_prev + B.ncase + 1;
@@ -1538,8 +1621,13 @@ static KArgs<T> make_args(const DevMesh& M, const T* b, T* x, T* const v[9], Poi
   A.g.counter = W.counters + site;
   A.mean_mode = mean_mode;
   A.zero_mean_row = zero_mean_row;
-  A.ext_precond = 0;
   A.ncache = 0;
+  A.cnb = 0;
+  A.cinv = nullptr;
+  A.crc_v = A.crc_r = nullptr;
+  A.cw = nullptr;
+  A.lw = nullptr;
+  A.llab = nullptr;
   return A;
 }
 
@@ -1604,8 +1692,7 @@ static cudaError_t launch_pdl(void (*kern)(KArgs<T>), int grid, cudaStream_t s, 
 // at most one per PGROUPS blocks, two partial slots of 8 doubles per CTA in the
 // reduction buffer.
 template <class T>
-static int persistent_grid(int nb, const PoissonWork& W, int* grid) {
-  const size_t dyn = kPersistentSmem;
+static int persistent_grid(int nb, const PoissonWork& W, int* grid, size_t dyn = kPersistentSmem) {
   void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
   CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   int per_sm = 0, dev = 0, sms = 0;
@@ -1639,11 +1726,11 @@ int persistent_solver_groups(int nb, PoissonWork& W, int* groups) {
 // that runs iterations until the state says done.
 template <class T>
 static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, const char* name) {
-  const size_t dyn = kPersistentSmem;
+  const size_t dyn = A.lw ? kLearnedSmem : kPersistentSmem;
   void (*kern)(KArgs<T>, GridSync) = k_bicg_persistent<T>;
   int grid = W.pgrid;
-  if (grid <= 0)
-    if (int rc = persistent_grid<T>(A.M.nb, W, &grid)) return rc;
+  if (grid <= 0 || A.lw)
+    if (int rc = persistent_grid<T>(A.M.nb, W, &grid, dyn)) return rc;
   // the arrival counter and the error flag start at zero
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
@@ -1731,20 +1818,31 @@ void krylov_init_state(const SolveParams& P, KrylovState& init) {
 template <class T>
 static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, int zero_mean_row,
                         PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done,
-                        const CnnWeights* cnn = nullptr) {
+                        const LocalMap* lmap = nullptr, const CoarseView* coarse = nullptr,
+                        int sms = 148) {
   const bool f32 = sizeof(T) == 4;
   KrylovState init;
   krylov_init_state(P, init);
-  const bool persistent = !cnn && P.persistent;
+  const bool persistent = P.persistent;
   if (P.graph && !persistent) return set_error(CUP_ERR_STATE, "captured solves need the persistent solver");
+  if (lmap && !persistent) return set_error(CUP_ERR_STATE, "the learned preconditioner needs the persistent solver");
   if (P.graph)
     CUP_CUDA_TRY(cudaMemcpyAsync(W.st, W.st_init, sizeof(init), cudaMemcpyDeviceToDevice, s));
   else
     CUP_CUDA_TRY(cudaMemcpyAsync(W.st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
   KArgs<T> A = make_args<T>(M, b, x, v, W, W.st, P.mean_mode, zero_mean_row, 0);
-  A.ext_precond = cnn ? 1 : 0;
   A.ncache = std::max(0, std::min(P.block_cache, KB_CACHE));
-  GridReduce gc{W.partial, W.counters + 14};
+  if (coarse && coarse->nb > 0 && persistent) {  // the persistent solver adds it itself
+    A.cnb = coarse->nb;
+    A.cinv = coarse->inv;
+    A.crc_v = coarse->rc;
+    A.crc_r = coarse->rc2;
+    A.cw = coarse->w;
+  }
+  if (lmap) {
+    A.lw = lmap->w;
+    A.llab = lmap->lab;
+  }
   if (!persistent) {  // the persistent kernel prepares and initialises itself
     { ProfScope ps(f32 ? "bicg32_prepare" : "bicg_prepare", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_prepare<T>, W.grid, s, A)); }
     { ProfScope ps(f32 ? "bicg32_init" : "bicg_init", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_init<T>, W.ggrid, s, A)); }
@@ -1762,12 +1860,12 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
   for (int it = 0; it < P.max_iter && !persistent; it += chunk) {
     for (int j = 0; j < chunk; ++j) {
       { ProfScope ps(f32 ? "bicg32_a_pupdate_precond" : "bicg_a_pupdate_precond", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_a<T>, W.ggrid, s, A)); }
-      if (cnn)
-        if (int rc = cnn_apply<T>(M, A.p, A.z1, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
+      if (coarse && coarse->nb > 0)
+        if (int rc = coarse_apply<T>(*coarse, A.p, A.z1, &W.st->mean_sum, sms, s)) return rc;
       { ProfScope ps(f32 ? "bicg32_b_spmv_dot" : "bicg_b_spmv_dot", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_b<T>, W.ggrid, s, A)); }
       { ProfScope ps(f32 ? "bicg32_c_supdate_precond" : "bicg_c_supdate_precond", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_c<T>, W.ggrid, s, A)); }
-      if (cnn)
-        if (int rc = cnn_apply<T>(M, A.r, A.z2, *cnn, W.grid, s, gc, &W.st->mean_sum)) return rc;
+      if (coarse && coarse->nb > 0)
+        if (int rc = coarse_apply<T>(*coarse, A.r, A.z2, &W.st->mean_sum, sms, s)) return rc;
       { ProfScope ps(f32 ? "bicg32_d_spmv_dots" : "bicg_d_spmv_dots", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_d<T>, W.ggrid, s, A)); }
       { ProfScope ps(f32 ? "bicg32_e_xr_update_dots" : "bicg_e_xr_update_dots", s); CUP_CUDA_TRY(launch_pdl<T>(k_bicg_e<T>, W.grid, s, A)); }
     }
@@ -1792,11 +1890,12 @@ static int run_bicgstab(const DevMesh& M, const T* b, T* x, T* const v[9], const
 }
 
 int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
-                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done, const CnnWeights* cnn) {
+                     PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done, const LocalMap* lmap,
+                     const CoarseView* coarse, int sms) {
   poisson_init_constants();
   double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
   const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
-  return run_bicgstab<double>(M, b, x, v, P, zmr, W, out, s, h_done, cnn);
+  return run_bicgstab<double>(M, b, x, v, P, zmr, W, out, s, h_done, lmap, coarse, sms);
 }
 
 // Mixed precision: FP64 iterative refinement around FP32 BiCGSTAB inner solves.
@@ -1805,7 +1904,8 @@ int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolvePa
 // scalars) to a relative tolerance tied to the remaining reduction, and adds e
 // to x in FP64.
 int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
-                  SolveStats& out, cudaStream_t s, int* h_done, const CnnWeights* cnn) {
+                  SolveStats& out, cudaStream_t s, int* h_done, const LocalMap* lmap, const CoarseView* coarse,
+                  int sms) {
   poisson_init_constants();
   const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
   const size_t n = size_t(M.nb) * BN;
@@ -1857,7 +1957,7 @@ int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParam
     Q.max_iter = std::max(1, P.max_iter - inner_total);
     CUP_CUDA_TRY(cudaMemsetAsync(e, 0, n * sizeof(float), s));
     SolveStats in{};
-    if (int rc = run_bicgstab<float>(M, W.r32, e, v, Q, 0, W, in, s, h_done, cnn)) return rc;
+    if (int rc = run_bicgstab<float>(M, W.r32, e, v, Q, 0, W, in, s, h_done, lmap, coarse, sms)) return rc;
     inner_total += in.iterations;
     restarts += in.restarts;
     if (in.status == SOLVE_NAN) {

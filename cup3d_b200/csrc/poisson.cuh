@@ -95,15 +95,37 @@ int launch_poisson_apply(const DevMesh& M, const double* x, double* y, int mean_
 int launch_block_inverse(const DevMesh& M, const double* in, double* out, PoissonWork& W,
                          cudaStream_t s);
 // Solves A x = b; x holds the initial guess on entry and x_opt on exit.
-// cnn != nullptr: the learned preconditioner replaces the block inverse.
-struct CnnWeights;
+// Coarse space of the two-level preconditioners (built by coarse_build):
+// A_c^-1 (nb x nb, row-major), two restriction buffers, the apply buffer and
+// the blocks' 512 h^3.  nb = 0: no coarse correction.
+struct CoarseView {
+  int nb;
+  const double* inv;
+  double* rc;
+  double* rc2;
+  double* yc;
+  const double* w;
+};
+
+// Learned local map of the preconditioner (lmap.cuh): the folded network in
+// fragment order (LMAP_W_WORDS words) and a [nb][896] BF16 lab buffer.
+struct LocalMap {
+  const uint4* w;
+  uint16_t* lab;
+};
+
+// coarse != nullptr: the coarse correction of the two-level preconditioners
+// is added to the per-block preconditioner (sms: the device's SM count).
+// lmap != nullptr: the learned local map is added as well (persistent solver
+// only).
 int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolveParams& P,
                      PoissonWork& W, SolveStats& out, cudaStream_t s, int* h_done_pinned,
-                     const CnnWeights* cnn = nullptr);
+                     const LocalMap* lmap = nullptr, const CoarseView* coarse = nullptr, int sms = 148);
 
 // Mixed precision: FP32 inner BiCGSTAB inside FP64 iterative refinement.
 int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
-                  SolveStats& out, cudaStream_t s, int* h_done_pinned, const CnnWeights* cnn = nullptr);
+                  SolveStats& out, cudaStream_t s, int* h_done_pinned, const LocalMap* lmap = nullptr,
+                  const CoarseView* coarse = nullptr, int sms = 148);
 // FP64 ||b - A x||_2 with the solvers' mean-row convention.
 int true_residual_norm(const DevMesh& M, const double* b, const double* x, int mean_mode, PoissonWork& W,
                        double* err_host, cudaStream_t s);
@@ -113,6 +135,12 @@ int launch_weighted_sum(const DevMesh& M, const double* v, double* d_out, Poisso
                         cudaStream_t s);
 
 void poisson_init_constants();
+
+// Two-level preconditioners: z += P A_c^-1 P^T r over the mesh blocks
+// (coarse.cu); mean_sum (may be null) gets the added sum(z h^3).
+constexpr int kCoarseMaxBlocks = 8192;
+template <class T>
+int coarse_apply(const CoarseView& C, const T* r, T* z, double* mean_sum, int sms, cudaStream_t s);
 
 // Number of 64-thread groups of the persistent solver on a mesh of nb blocks
 // (the visit order is balanced for this many groups).

@@ -42,8 +42,13 @@ extern "C" {
 /* Poisson solvers selectable by -poissonSolver (PoissonSolverBase.cpp:30-52) */
 #define CUP_POISSON_B200 0          /* "b200": FP64 BiCGSTAB, exact block inverse */
 #define CUP_POISSON_B200_MIXED 1    /* "b200_mixed": FP32 inner, FP64 refinement */
-#define CUP_POISSON_B200_LEARNED 2  /* "b200_learned": CNN preconditioner, flexible */
+#define CUP_POISSON_B200_LEARNED 2  /* "b200_learned": flexible BiCGSTAB, two-level preconditioner
+                                       with the CNN on each block (coarse correction + block
+                                       inverse + learned correction) */
 #define CUP_POISSON_B200_LEARNED_MIXED 3 /* "b200_learned_mixed": both */
+#define CUP_POISSON_B200_TWOLEVEL 4 /* "b200_twolevel": BiCGSTAB, two-level preconditioner without
+                                       the network (coarse correction + block inverse); the
+                                       method the learned one is compared with */
 
 /* field ids */
 #define CUP_FIELD_VEL 0   /* 3 components */
@@ -322,23 +327,37 @@ int cup_set_barrier_limit(cup_ctx* ctx, int64_t cycles);
 
 /* ---- learned preconditioner (no counterpart in the reference: the new slot at
  * the preconditioner call sites PoissonSolverAMR.h:183-222, BiCGSTAB.cu:526-527).
- * z = BJ(r) + (s/h) CNN(r_block+halo / s): the exact block inverse plus a
- * per-block 3-D CNN correction (4 conv 3^3 layers, 16 channels). ---- */
+ * z = P A_c^-1 P^T r + BJ(r) + (s/h) CNN(r_block+halo / s): the coarse correction,
+ * the exact block inverse and a per-block 3-D CNN correction (4 conv 3^3 layers,
+ * 16 channels, BF16 weights, FP32 accumulation). ---- */
 int32_t cup_cnn_num_params(void);
 int cup_cnn_init(cup_ctx* ctx, uint64_t seed);                 /* random initial weights */
 int cup_cnn_set_params(cup_ctx* ctx, const float* params);     /* cup_cnn_num_params() floats */
 int cup_cnn_get_params(cup_ctx* ctx, float* params);
 int cup_cnn_dataset_reserve(cup_ctx* ctx, int32_t capacity);   /* samples (one per block per pair) */
-/* adds one sample per block from device vectors: residual r and error e = x* - x */
+/* adds one sample per block from device vectors: residual r and error e = x* - x; the
+ * sample's target is what the coarse correction and the block inverse leave of e
+ * (e - P A_c^-1 P^T r - B^-1 r, the network's part of the two-level preconditioner) */
 int cup_cnn_dataset_add(cup_ctx* ctx, const double* d_r, const double* d_e);
 int32_t cup_cnn_dataset_size(const cup_ctx* ctx);
-/* `steps` Adam steps on random minibatches (seeded); per-step loss into loss_out (or NULL) */
+/* the last ntest samples are held out of training; cup_cnn_eval: the network's
+ * residual-norm loss on them (|L (z - t)|^2, L the block Laplacian, the loss the
+ * training minimises) relative to that of the zero prediction */
+int cup_cnn_holdout(cup_ctx* ctx, int32_t ntest);
+int cup_cnn_eval(cup_ctx* ctx, float* rel_loss);
+/* `steps` Adam steps on random minibatches (seeded) minimising the residual-norm loss
+ * |L (z - t)|^2 (L: the 7-point Laplacian of the 8^3 block, zero outside), relative to
+ * the targets' scale; per-step loss into loss_out (or NULL) */
 int cup_cnn_train(cup_ctx* ctx, int32_t steps, int32_t batch, float lr, uint64_t seed, float* loss_out);
 /* network forward / loss and gradient on host arrays (n samples of 10^3 inputs, 8^3 targets) */
 int cup_cnn_forward_host(cup_ctx* ctx, const float* in, float* out, int32_t n);
 int cup_cnn_grad_host(cup_ctx* ctx, const float* in, const float* target, int32_t n, float* grad, float* loss);
-/* z = learned preconditioner applied to the device vector r */
+/* z = block inverse of r + the network on r's block labs (the network's own
+ * convolution layers), per block */
 int cup_cnn_precond_dev(cup_ctx* ctx, const double* d_r, double* d_z);
+/* The same through the solver's path: block inverse + the network folded into
+ * one 512 x 896 matrix (BF16 tensor-core GEMM on the BF16 star labs of r). */
+int cup_cnn_map_apply_dev(cup_ctx* ctx, const double* d_r, double* d_z);
 
 /* Network forward on host arrays, as cup_cnn_forward_host, without allocating
  * or freeing device memory.  No counterpart in the reference.
@@ -359,6 +378,17 @@ int cup_cnn_precond_dev(cup_ctx* ctx, const double* d_r, double* d_z);
  * beginning any stream capture on the device. */
 #define CUP_CNN_FORWARD_NOALLOC_MAX 64
 int cup_cnn_forward_host_noalloc(cup_ctx* ctx, const float* in, float* out, int32_t n);
+
+/* ---- coarse space of the two-level solvers (no counterpart in the reference,
+ * whose preconditioner is block-local).  One unknown per block; A_c = P^T A P
+ * with P constant over each block, built through the device operator once
+ * per mesh (at most 8192 blocks), inverted once on the device. ----
+ * cup_coarse_matrix: builds it; out (may be NULL): A_c, nblocks^2 doubles,
+ * row-major, blocks in cup_get_blocks order; *colours (may be NULL): the
+ * colours of the set-up's block colouring.
+ * cup_coarse_apply_dev: d_z = P A_c^-1 P^T d_r on device buffers. */
+int cup_coarse_matrix(cup_ctx* ctx, double* out, int32_t* colours);
+int cup_coarse_apply_dev(cup_ctx* ctx, const double* d_r, double* d_z);
 
 /* ---- profiling (the reference's DeviceProfiler, Utils/DeviceProfiler.cuh) ---- */
 /* Enables per-kernel CUDA-event timing (resets the counters). */

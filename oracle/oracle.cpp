@@ -1498,8 +1498,10 @@ extern "C" void orc_pressure_project(orc_mesh* m, double* vel, double* pres, con
 // definition of a 3-D convolution).  Parameters in one array, in this order:
 // W0[co][tap] (1 -> C, 'valid' on the 10^3 input), b0[C], W1[co][ci][tap],
 // b1[C], W2[co][ci][tap], b2[C], W3[ci][tap] (C -> 1), b3; tap = kx + 3 ky + 9 kz.
-// ReLU after layers 0-2; layers 1-3 are zero-padded 'same' convolutions on
-// the 8^3 block.  Loss: mean over samples and cells of (z - target)^2.
+// The layers are linear (no activation) and the bias slots are not used, so
+// the network is a linear map of its input (it serves as a preconditioner);
+// layers 1-3 are zero-padded 'same' convolutions on the 8^3 block.  Loss:
+// mean over samples and cells of (z - target)^2; the bias gradients are 0.
 // ============================================================================
 namespace {
 struct CnnDims {
@@ -1539,28 +1541,28 @@ extern "C" void orc_cnn_fwd_grad(int nblk, int C, const double* P, const float* 
       for (int co = 0; co < C; ++co)
         for (int c = 0; c < BN; ++c) {
           const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
-          double s = P[D.oB0 + co];
+          double s = 0.0;
           for (int t = 0; t < 27; ++t) s += P[D.oW0 + co * 27 + t] * X(xx + t % 3, yy + (t / 3) % 3, zz + t / 9);
-          a1[co * BN + c] = s > 0 ? s : 0;
+          a1[co * BN + c] = s;
         }
-      auto same = [&](const std::vector<double>& a, int oW, int oB, std::vector<double>& o) {
+      auto same = [&](const std::vector<double>& a, int oW, std::vector<double>& o) {
         for (int co = 0; co < C; ++co)
           for (int c = 0; c < BN; ++c) {
             const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
-            double s = P[oB + co];
+            double s = 0.0;
             for (int ci = 0; ci < C; ++ci)
               for (int t = 0; t < 27; ++t) {
                 const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
                 if (inb(X2, Y2, Z2)) s += P[oW + (co * C + ci) * 27 + t] * a[ci * BN + cell(X2, Y2, Z2)];
               }
-            o[co * BN + c] = s > 0 ? s : 0;
+            o[co * BN + c] = s;
           }
       };
-      same(a1, D.oW1, D.oB1, a2);
-      same(a2, D.oW2, D.oB2, a3);
+      same(a1, D.oW1, a2);
+      same(a2, D.oW2, a3);
       for (int c = 0; c < BN; ++c) {
         const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
-        double s = P[D.oB3];
+        double s = 0.0;
         for (int ci = 0; ci < C; ++ci)
           for (int t = 0; t < 27; ++t) {
             const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
@@ -1579,7 +1581,6 @@ extern "C" void orc_cnn_fwd_grad(int nblk, int C, const double* P, const float* 
       // layer 3
       for (int c = 0; c < BN; ++c) {
         const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
-        g[D.oB3] += z[c];
         for (int ci = 0; ci < C; ++ci)
           for (int t = 0; t < 27; ++t) {
             const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
@@ -1595,16 +1596,13 @@ extern "C" void orc_cnn_fwd_grad(int nblk, int C, const double* P, const float* 
             if (inb(X2, Y2, Z2)) d3[ci * BN + cell(X2, Y2, Z2)] += P[D.oW3 + ci * 27 + t] * z[c];
           }
       }
-      for (int i = 0; i < C * BN; ++i)
-        if (!(a3[i] > 0)) d3[i] = 0;
-      auto back_same = [&](const std::vector<double>& a, const std::vector<double>& dp, int oW, int oB,
-                           std::vector<double>* da, const std::vector<double>* amask) {
+      auto back_same = [&](const std::vector<double>& a, const std::vector<double>& dp, int oW,
+                           std::vector<double>* da) {
         for (int co = 0; co < C; ++co)
           for (int c = 0; c < BN; ++c) {
             const double dv = dp[co * BN + c];
             if (dv == 0) continue;
             const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
-            g[oB + co] += dv;
             for (int ci = 0; ci < C; ++ci)
               for (int t = 0; t < 27; ++t) {
                 const int X2 = xx + t % 3 - 1, Y2 = yy + (t / 3) % 3 - 1, Z2 = zz + t / 9 - 1;
@@ -1614,20 +1612,16 @@ extern "C" void orc_cnn_fwd_grad(int nblk, int C, const double* P, const float* 
                 if (da) (*da)[ci * BN + cc] += P[oW + (co * C + ci) * 27 + t] * dv;
               }
           }
-        if (da)
-          for (int i = 0; i < C * BN; ++i)
-            if (!((*amask)[i] > 0)) (*da)[i] = 0;
       };
       std::fill(d2.begin(), d2.end(), 0.0);
-      back_same(a2, d3, D.oW2, D.oB2, &d2, &a2);
+      back_same(a2, d3, D.oW2, &d2);
       std::fill(d1.begin(), d1.end(), 0.0);
-      back_same(a1, d2, D.oW1, D.oB1, &d1, &a1);
+      back_same(a1, d2, D.oW1, &d1);
       for (int co = 0; co < C; ++co)
         for (int c = 0; c < BN; ++c) {
           const double dv = d1[co * BN + c];
           if (dv == 0) continue;
           const int xx = c % 8, yy = (c / 8) % 8, zz = c / 64;
-          g[D.oB0 + co] += dv;
           for (int t = 0; t < 27; ++t) g[D.oW0 + co * 27 + t] += X(xx + t % 3, yy + (t / 3) % 3, zz + t / 9) * dv;
         }
     }
