@@ -401,6 +401,10 @@ class Context:
     def cnn_map_apply(self, r, z):
         """z = block inverse + folded network on r, the solver's path."""
         check(lib().cup_cnn_map_apply_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
+
+    def schwarz_apply(self, r, z):
+        """z = block inverse + the one-cell-overlap local solve's correction on r."""
+        check(lib().cup_schwarz_apply_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
 class Batch(Context):
     """Independent cases in one context (cup_batch_create): the cases' meshes
     concatenated in case order; their Poisson solves run in one device

@@ -26,7 +26,7 @@ CNN_FORWARD_NOALLOC_MAX = 64  # CUP_CNN_FORWARD_NOALLOC_MAX
 
 BC = {"freespace": 0, "periodic": 1, "wall": 2}
 ADV = {"upwind5": 0, "upwind3": 0, "weno5": 1}
-SOLVER = {"b200": 0, "b200_mixed": 1, "b200_learned": 2, "b200_learned_mixed": 3, "b200_twolevel": 4}
+SOLVER = {"b200": 0, "b200_mixed": 1, "b200_learned": 2, "b200_learned_mixed": 3, "b200_twolevel": 4, "b200_schwarz": 5}
 FIELD = {"vel": 0, "pres": 1, "chi": 2, "lhs": 3, "tmpV": 4}
 FIELD_NCOMP = {"vel": 3, "pres": 1, "chi": 1, "lhs": 1, "tmpV": 3}
 
@@ -156,6 +156,7 @@ SIGNATURES = {
                                     C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "cup_cnn_precond_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_cnn_map_apply_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "cup_schwarz_apply_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_cnn_forward_host_noalloc": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32]),
     "cup_profile": (C.c_int, [_P, C.c_int32]),
     "cup_profile_read": (C.c_int, [_P, C.c_char_p, C.c_int32]),

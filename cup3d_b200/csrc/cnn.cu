@@ -172,16 +172,22 @@ __device__ void forward_block(FwdSmem& S) {
   __syncthreads();
 }
 
-// Input of one block: block + one-cell halo of v (lab rules of lab.cuh, edges
-// and corners zero), divided by its RMS; returns the RMS.
-// labd holds the star lab of lab_fill (LabGeom<1>: the block, then its six
+// Input of one block: its residual lab (block + one-cell face layers, the
+// rules of lmap.cuh; edges and corners zero), divided by its RMS; returns
+// the RMS.  labd holds the star lab (LabGeom<1>: the block, then its six
 // face layers), which is expanded into the 10^3 cube x0.
 template <class T>
-__device__ float gather_input(const DevMesh& M, int b, const T* v, float* x0, double* labd, double* red) {
+__device__ float gather_input(const DevMesh& M, int b, const T* v, float* x0, double* labd, double* red,
+                              int mean_blk) {
   using LG = LabGeom<1>;
+  __shared__ LabMeta meta;
   __syncthreads();
-  auto get = [&](int, int blk, int cell) { return double(v[size_t(blk) * BN + cell]); };
-  lab_fill<1, 1>(labd, M, b, get, false);
+  if (threadIdx.x < 64) lab_meta_load(meta, M, b, threadIdx.x);
+  __syncthreads();
+  for (int i = threadIdx.x; i < LG::V; i += blockDim.x) {
+    const int g = i - BN;
+    labd[i] = i < BN ? double(v[size_t(b) * BN + i]) : rlab_ghost(v, meta, g >> 6, g & 7, (g >> 3) & 7, mean_blk);
+  }
   __syncthreads();
   double acc[1] = {0.0};
   for (int i = threadIdx.x; i < LG::V; i += blockDim.x) acc[0] += labd[i] * labd[i];
@@ -221,7 +227,7 @@ struct ApplySmem {
 // constraint of the SpMV that follows (into *mean_sum when given).
 template <class T>
 __global__ void __launch_bounds__(NT, 1) k_cnn_apply(DevMesh M, const T* __restrict__ r, T* __restrict__ zout,
-                                                     CnnWeights W, GridReduce G, double* mean_sum) {
+                                                     CnnWeights W, GridReduce G, double* mean_sum, int mean_blk) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ApplySmem& A = *reinterpret_cast<ApplySmem*>(smem_raw);
   FwdSmem& S = A.f;
@@ -231,7 +237,7 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_apply(DevMesh M, const T* __restr
   double acc[1] = {0.0};
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
     __syncthreads();
-    const float rms = gather_input<T>(M, b, r, S.x0, labd, S.red);
+    const float rms = gather_input<T>(M, b, r, S.x0, labd, S.red, mean_blk);
     const double h = M.h[b];
     if (rms > 0.f) block_jacobi_of_input(S.x0, h, fs, A.zbj);
     zero_act(S.a);
@@ -252,52 +258,48 @@ __global__ void __launch_bounds__(NT, 1) k_cnn_apply(DevMesh M, const T* __restr
 
 template <class T>
 int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid, cudaStream_t s, GridReduce G,
-              double* mean_sum) {
+              double* mean_sum, int mean_blk) {
   fd_init_constants();
   const size_t smem = sizeof(ApplySmem);
   static unsigned long long attr = 0;
   if (first_on_device(attr))
     CUP_CUDA_TRY(cudaFuncSetAttribute(k_cnn_apply<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   ProfScope ps(sizeof(T) == 4 ? "cnn_precond_apply_f32io" : "cnn_precond_apply_f64io", s);
-  k_cnn_apply<T><<<grid, NT, smem, s>>>(M, r, z, W, G, mean_sum);
+  k_cnn_apply<T><<<grid, NT, smem, s>>>(M, r, z, W, G, mean_sum, mean_blk);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
 template int cnn_apply<double>(const DevMesh&, const double*, double*, const CnnWeights&, int, cudaStream_t,
-                               GridReduce, double*);
+                               GridReduce, double*, int);
 template int cnn_apply<float>(const DevMesh&, const float*, float*, const CnnWeights&, int, cudaStream_t,
-                              GridReduce, double*);
+                              GridReduce, double*, int);
 
-// Training pairs from a residual r and the error e = x* - x of the same
-// iterate: input = gather(r)/s, target = (e - BJ(r)) h / s on the block.
+// Training samples from a residual r and a correction field corr (in the
+// units of A^-1 r): input = gather(r)/s, target = corr h / s on the block.
 __global__ void __launch_bounds__(NT) k_cnn_dataset(DevMesh M, const double* __restrict__ r,
-                                                    const double* __restrict__ e, float* in, float* target,
-                                                    int base, int cap, int* count) {
+                                                    const double* __restrict__ corr, float* in, float* target,
+                                                    int base, int cap, int* count, int mean_blk) {
   __shared__ double labd[PV];
   __shared__ double red[64];
   __shared__ float x0[PV];
-  __shared__ FdSmem fs;
-  __shared__ double zbj[BN];
   for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
     const int slot = base + b;
     if (slot >= cap) break;
     __syncthreads();
-    const float rms = gather_input<double>(M, b, r, x0, labd, red);
+    const float rms = gather_input<double>(M, b, r, x0, labd, red, mean_blk);
     const double h = M.h[b];
     const bool live = rms > 0.f;  // uniform across the CTA
-    if (live) block_jacobi_of_input(x0, h, fs, zbj);
     for (int i = threadIdx.x; i < PV; i += NT) in[size_t(slot) * PV + i] = live ? x0[i] : 0.f;
     for (int c = threadIdx.x; c < BN; c += NT)
-      target[size_t(slot) * BN + c] = live ? float((e[size_t(b) * BN + c] / double(rms) - zbj[c]) * h) : 0.f;
+      target[size_t(slot) * BN + c] = live ? float(corr[size_t(b) * BN + c] * h / double(rms)) : 0.f;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *count = min(cap, base + M.nb);
 }
 
-int cnn_dataset_add(const DevMesh& M, const double* r, const double* e, float* in, float* target, int base, int cap,
-                    int* count_dev, int grid, cudaStream_t s) {
-  fd_init_constants();
+int cnn_dataset_add(const DevMesh& M, const double* r, const double* corr, float* in, float* target, int base,
+                    int cap, int* count_dev, int grid, cudaStream_t s, int mean_blk) {
   ProfScope ps("cnn_dataset_add", s);
-  k_cnn_dataset<<<grid, NT, 0, s>>>(M, r, e, in, target, base, cap, count_dev);
+  k_cnn_dataset<<<grid, NT, 0, s>>>(M, r, corr, in, target, base, cap, count_dev, mean_blk);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;
 }
@@ -630,6 +632,10 @@ int cnn_fold(const CnnWeights& W, float* in, float* out, uint4* wfrag, float* gp
   k_fold_inputs<<<256, 256, 0, s>>>(in);
   CUP_CUDA_TRY(cudaGetLastError());
   if (int rc = cnn_forward_batch(W, in, out, LMAP_K, gpart, grid, s)) return rc;
+  return lmap_pack(out, wfrag, s);
+}
+
+int lmap_pack(const float* out, uint4* wfrag, cudaStream_t s) {
   k_fold_pack<<<(LMAP_W_WORDS + 255) / 256, 256, 0, s>>>(out, wfrag);
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;

@@ -56,18 +56,22 @@ int cnn_pack(const CnnWeights& W, cudaStream_t s);
 // floats of scratch), then the fragment-ordered BF16 copy into wfrag
 // (LMAP_W_WORDS 16-byte words).  gpart: as cnn_forward_batch.
 int cnn_fold(const CnnWeights& W, float* in, float* out, uint4* wfrag, float* gpart, int grid, cudaStream_t s);
+// The fragment-ordered BF16 copy alone: W[c][j] = out[j * 512 + c].
+int lmap_pack(const float* out, uint4* wfrag, cudaStream_t s);
 
 // z = BJ(r) + (s/h) CNN(r_lab / s) per block (BJ: the exact block inverse;
-// s: RMS of the block + halo input); sum(z h^3) into *mean_sum when given.
+// r_lab: the residual lab of lmap.cuh, s: its RMS); sum(z h^3) into
+// *mean_sum when given.  mean_blk: the block of a mean-constraint row, -1 none.
 template <class T>
 int cnn_apply(const DevMesh& M, const T* r, T* z, const CnnWeights& W, int grid, cudaStream_t s, GridReduce G,
-              double* mean_sum);
+              double* mean_sum, int mean_blk);
 
-// Appends one training sample per block from a residual r and its error
-// e = x* - x: input gather(r)/s (10^3), target (e - BJ(r)) h / s (8^3), at
-// rows base.. of in/target (capacity cap); the new count into *count_dev.
-int cnn_dataset_add(const DevMesh& M, const double* r, const double* e, float* in, float* target, int base, int cap,
-                    int* count_dev, int grid, cudaStream_t s);
+// Appends one training sample per block from a residual r and a correction
+// field corr (units of A^-1 r): input gather(r)/s (10^3), target corr h / s
+// (8^3), at rows base.. of in/target (capacity cap); the new count into
+// *count_dev.
+int cnn_dataset_add(const DevMesh& M, const double* r, const double* corr, float* in, float* target, int base,
+                    int cap, int* count_dev, int grid, cudaStream_t s, int mean_blk);
 
 // Training on a device dataset of n samples: in[n*1000], target[n*512]
 // (targets already divided by the sample's scale/h).  One Adam step over a

@@ -154,6 +154,43 @@ __global__ void __launch_bounds__(NT) k_coarse_mean(int nb, const double* __rest
 
 }  // namespace
 
+// Inverse of the n x n host matrix a (row-major) by Gauss-Jordan with partial
+// pivoting on the device, into d_inv (n x n, device, row-major); returns
+// CUP_ERR_MESH for a singular matrix.
+int device_inverse(const double* a, int n, double* d_inv, int sms, cudaStream_t s) {
+  DevArena tmp;
+  double *G = nullptr, *fac = nullptr;
+  int* sing = nullptr;
+  if (int rc = tmp.alloc(&G, size_t(n) * 2 * n)) return rc;
+  if (int rc = tmp.alloc(&fac, n)) return rc;
+  if (int rc = tmp.alloc(&sing, 1)) return rc;
+  {
+    std::vector<double> Gh(size_t(n) * 2 * n, 0.0);
+    for (int i = 0; i < n; ++i) {
+      std::copy(a + size_t(i) * n, a + size_t(i) * n + n, &Gh[size_t(i) * 2 * n]);
+      Gh[size_t(i) * 2 * n + n + i] = 1.0;
+    }
+    CUP_CUDA_TRY(stream_h2d(s, G, Gh.data(), Gh.size() * sizeof(double)));
+  }
+  CUP_CUDA_TRY(stream_zero(s, sing, sizeof(int)));
+  {
+    ProfScope ps("gauss_jordan_inverse", s);
+    const int eg = std::max(1, sms * 8);
+    for (int k = 0; k < n; ++k) {
+      k_gj_pivot<<<1, 1024, 0, s>>>(G, n, k, fac, sing);
+      k_gj_eliminate<<<eg, NT, 0, s>>>(G, n, k, fac);
+    }
+    CUP_CUDA_TRY(cudaGetLastError());
+  }
+  int h_sing = 0;
+  CUP_CUDA_TRY(stream_d2h(s, &h_sing, sing, sizeof(int)));  // synchronises: tmp is free to go
+  if (h_sing) return set_error(CUP_ERR_MESH, "Gauss-Jordan inverse: singular matrix");
+  k_gj_extract<<<std::max(1, sms * 8), NT, 0, s>>>(G, n, d_inv);
+  CUP_CUDA_TRY(cudaGetLastError());
+  CUP_CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
 // Builds the coarse space of the context's mesh (see above).
 int coarse_build(cup_ctx* c) {
   CoarseSpace& C = c->coarse;
@@ -245,40 +282,14 @@ int coarse_build(cup_ctx* c) {
     }
   }
   // A_c^-1 by Gauss-Jordan on the device
-  double *G = nullptr, *fac = nullptr;
-  int* sing = nullptr;
-  if (int rc = tmp.alloc(&G, size_t(nb) * 2 * nb)) return rc;
-  if (int rc = tmp.alloc(&fac, nb)) return rc;
-  if (int rc = tmp.alloc(&sing, 1)) return rc;
-  {
-    std::vector<double> Gh(size_t(nb) * 2 * nb, 0.0);
-    for (int i = 0; i < nb; ++i) {
-      std::copy(&Ac[size_t(i) * nb], &Ac[size_t(i) * nb] + nb, &Gh[size_t(i) * 2 * nb]);
-      Gh[size_t(i) * 2 * nb + nb + i] = 1.0;
-    }
-    CUP_CUDA_TRY(stream_h2d(s, G, Gh.data(), Gh.size() * sizeof(double)));
-  }
-  CUP_CUDA_TRY(stream_zero(s, sing, sizeof(int)));
-  {
-    ProfScope ps("coarse_gauss_jordan", s);
-    const int eg = std::max(1, c->num_sms * 8);
-    for (int k = 0; k < nb; ++k) {
-      k_gj_pivot<<<1, 1024, 0, s>>>(G, nb, k, fac, sing);
-      k_gj_eliminate<<<eg, NT, 0, s>>>(G, nb, k, fac);
-    }
-    CUP_CUDA_TRY(cudaGetLastError());
-  }
-  int h_sing = 0;
-  CUP_CUDA_TRY(stream_d2h(s, &h_sing, sing, sizeof(int)));
-  if (h_sing) return set_error(CUP_ERR_MESH, "two-level preconditioner: singular coarse operator");
   DevArena& A = C.arena;
   if (int rc = A.alloc(&C.inv, size_t(nb) * nb)) return rc;
+  if (int rc = device_inverse(Ac.data(), nb, C.inv, c->num_sms, s))
+    return rc == CUP_ERR_MESH ? set_error(CUP_ERR_MESH, "two-level preconditioner: singular coarse operator") : rc;
   if (int rc = A.alloc(&C.rc, nb)) return rc;
   if (int rc = A.alloc(&C.yc, nb)) return rc;
   if (int rc = A.alloc(&C.rc2, nb)) return rc;
   if (int rc = A.alloc(&C.w, nb)) return rc;
-  k_gj_extract<<<std::max(1, c->num_sms * 8), NT, 0, s>>>(G, nb, C.inv);
-  CUP_CUDA_TRY(cudaGetLastError());
   CUP_CUDA_TRY(stream_h2d(s, C.w, w.data(), nb * sizeof(double)));
   C.host_ac.swap(Ac);
   C.nb = nb;

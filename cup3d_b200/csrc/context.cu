@@ -292,6 +292,7 @@ int cup_config_parse(cup_config* c, const char* args) {
       else if (v == "b200_learned") c->poisson_solver = CUP_POISSON_B200_LEARNED;
       else if (v == "b200_learned_mixed") c->poisson_solver = CUP_POISSON_B200_LEARNED_MIXED;
       else if (v == "b200_twolevel") c->poisson_solver = CUP_POISSON_B200_TWOLEVEL;
+      else if (v == "b200_schwarz") c->poisson_solver = CUP_POISSON_B200_SCHWARZ;
       else return ctx_fail(nullptr, CUP_ERR_ARG, "Poisson solver: \"" + v + "\" unrecognized!");
     } else if (key == "device") {
       if (need_num()) return CUP_ERR_ARG;
@@ -576,16 +577,20 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   const bool learned = solver == CUP_POISSON_B200_LEARNED || solver == CUP_POISSON_B200_LEARNED_MIXED;
   // the two-level solvers: the coarse space of the mesh, built once per mesh
   // (outside the solve's timed region)
-  const bool twolevel = learned || solver == CUP_POISSON_B200_TWOLEVEL;
+  const bool schwarz = solver == CUP_POISSON_B200_SCHWARZ;
+  const bool twolevel = learned || schwarz || solver == CUP_POISSON_B200_TWOLEVEL;
   if (twolevel)
     if (int rc2 = coarse_build(c)) return keep(c, rc2);
   if (learned && !c->cnn.ready)
     return ctx_fail(c, CUP_ERR_STATE, "learned preconditioner has no weights (cup_cnn_init / cup_cnn_set_params)");
-  // the learned map of the current weights (folded outside the timed region)
+  // the local map: the learned one of the current weights (folded outside
+  // the timed region), or the exact overlap solve
   LocalMap lm{};
   if (learned)
     if (int rc2 = lmap_prepare(c, &lm)) return keep(c, rc2);
-  const LocalMap* lmap = learned ? &lm : nullptr;
+  if (schwarz)
+    if (int rc2 = schwarz_prepare(c, &lm)) return keep(c, rc2);
+  const LocalMap* lmap = (learned || schwarz) ? &lm : nullptr;
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
   int fallback = 0;
   if (learned) P.stall_window = 40;  // a stall hands over to block-Jacobi below

@@ -73,6 +73,7 @@ struct CnnState {
   uint4* lmap_w = nullptr;
   float *fold_in = nullptr, *fold_out = nullptr;
   uint16_t* lmap_lab = nullptr;
+  uint4* schwarz_w = nullptr;  // the one-cell-overlap local solve (schwarz_prepare)
   size_t lab_cap = 0;
   bool folded = false;
 };
@@ -251,9 +252,15 @@ int adapt_indicator(cup_ctx* c, std::vector<double>& out);
 int adapt_mesh(cup_ctx* c, int* changed);
 // Builds (once per mesh) the coarse space of the two-level preconditioners.
 int coarse_build(cup_ctx* c);
+// Inverse of an n x n host matrix (row-major) on the device (coarse.cu).
+int device_inverse(const double* a, int n, double* d_inv, int sms, cudaStream_t s);
 // The learned map of the current weights for the solver (folds them when they
 // changed; the lab buffer for the current mesh).
 int lmap_prepare(cup_ctx* c, LocalMap* out);
+// The exact one-cell-overlap local solve as a local map (built once).
+int schwarz_prepare(cup_ctx* c, LocalMap* out);
+// The block of the mean-constraint row when the mean mode replaces a row, else -1.
+int mean_block_of(const cup_ctx* c);
 // Fetches the host copies of a device-created obstacle (no-op otherwise).
 int ctx_obstacle_host_copies(cup_ctx* c);
 // Drops the captured time steps (after any change of mesh, obstacle or

@@ -77,17 +77,18 @@ __device__ __forceinline__ double c2f_ghost(Get get, int d, int s, int l, int a,
   return sum;
 }
 
-// Fills lab (NC components, each LabGeom<G>::V doubles) for block b.
-// get(c, blk, cell) reads component c of the field.
+// Fills lab (NC components, each LabGeom<G>::V doubles) for block b, with
+// threads t0, t0 + nt, ... (lab_fill: the whole CTA).  get(c, blk, cell)
+// reads component c of the field.
 template <int G, int NC, class Get>
-__device__ void lab_fill(double* lab, const DevMesh& M, int b, Get get, bool vector_bc) {
+__device__ void lab_fill_part(double* lab, const DevMesh& M, int b, Get get, bool vector_bc, int t0, int nt) {
   using LG = LabGeom<G>;
-  for (int i = threadIdx.x; i < BN; i += blockDim.x) {
+  for (int i = t0; i < BN; i += nt) {
     const int x = i & 7, y = (i >> 3) & 7, z = i >> 6;
 #pragma unroll
     for (int c = 0; c < NC; ++c) lab[c * LG::V + LG::at(x, y, z)] = get(c, b, i);
   }
-  for (int g = threadIdx.x; g < 6 * G * 64; g += blockDim.x) {
+  for (int g = t0; g < 6 * G * 64; g += nt) {
     const int f = g / (G * 64), rem = g - f * (G * 64);
     const int l = rem / 64 + 1, a = rem & 7, bb = (rem >> 3) & 7;
     const int d = f >> 1, s = f & 1;
@@ -133,6 +134,11 @@ __device__ void lab_fill(double* lab, const DevMesh& M, int b, Get get, bool vec
         lab[c * LG::V + li] = c2f_ghost([&](int cell) { return get(c, cb, cell); }, d, s, l, a, bb, h1, h2);
     }
   }
+}
+
+template <int G, int NC, class Get>
+__device__ __forceinline__ void lab_fill(double* lab, const DevMesh& M, int b, Get get, bool vector_bc) {
+  lab_fill_part<G, NC>(lab, M, b, get, vector_bc, int(threadIdx.x), int(blockDim.x));
 }
 
 // Value of the child's ghost at layer 1 beyond its face toward the coarse block

@@ -6,6 +6,7 @@
 
 #include "context.h"
 #include "lmap.cuh"
+#include "profiler.h"
 
 namespace cup3d {
 
@@ -38,13 +39,6 @@ __global__ void __launch_bounds__(NT) k_sumsq(const float* __restrict__ v, size_
     acc[0] += x * x;
   }
   if (grid_reduce<1>(acc, g, red) && threadIdx.x == 0) *out = acc[0];
-}
-
-// out = x + a y
-__global__ void k_axpy(size_t n, const double* __restrict__ x, double a, const double* __restrict__ y,
-                       double* __restrict__ out) {
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
-    out[i] = x[i] + a * y[i];
 }
 
 __global__ void k_scale(float* v, size_t n, float s) {
@@ -90,14 +84,33 @@ static bool dev_ok(cup_ctx* c) { return c && !c->host_only && c->mesh.nb > 0; }
 
 // The learned map's two phases as kernels of their own (the solver runs
 // them inside its persistent launch).
-__global__ void __launch_bounds__(256) k_lmap_gather(DevMesh M, const double* v, uint16_t* lab) {
-  __shared__ double labd[LMAP_K];
-  lmap_gather<double>(M, v, lab, labd);
+__global__ void __launch_bounds__(256) k_lmap_gather(DevMesh M, const double* v, uint16_t* lab, int mean_blk) {
+  __shared__ LabMeta meta[LMAP_GATHER];
+  lmap_gather<double>(M, v, lab, meta, mean_blk);
 }
 
 __global__ void __launch_bounds__(256) k_lmap_gemm(DevMesh M, const uint4* W, const uint16_t* lab, double* z) {
   extern __shared__ __align__(16) unsigned char lmap_smem[];
   (void)lmap_gemm<double>(M, W, lab, z, reinterpret_cast<uint16_t*>(lmap_smem));
+}
+
+// The mean-constraint row's block (cell 0) when the configured mean mode
+// replaces a row (1 and 3), else -1.
+int mean_block_of(const cup_ctx* c) {
+  const int m = c->cfg.mean_constraint;
+  return (m == 1 || m == 3) ? c->dm.mean_block : -1;
+}
+
+// The solver's lab buffer for the current mesh.
+static int ensure_lab(cup_ctx* c) {
+  CnnState& S = c->cnn;
+  const size_t need = size_t(c->mesh.nb) * LMAP_K;
+  if (S.lab_cap >= need) return 0;
+  S.lab_arena.release();
+  S.lab_cap = 0;
+  if (int rc = S.lab_arena.alloc(&S.lmap_lab, need)) return rc;
+  S.lab_cap = need;
+  return 0;
 }
 
 int lmap_prepare(cup_ctx* c, LocalMap* out) {
@@ -109,18 +122,111 @@ int lmap_prepare(cup_ctx* c, LocalMap* out) {
     if (int rc = S.arena.alloc(&S.fold_out, size_t(LMAP_K) * BN)) return rc;
     S.folded = false;
   }
-  const size_t need = size_t(c->mesh.nb) * LMAP_K;
-  if (S.lab_cap < need) {
-    S.lab_arena.release();
-    S.lab_cap = 0;
-    if (int rc = S.lab_arena.alloc(&S.lmap_lab, need)) return rc;
-    S.lab_cap = need;
-  }
+  if (int rc = ensure_lab(c)) return rc;
   if (!S.folded) {
     if (int rc = cnn_fold(S.W, S.fold_in, S.fold_out, S.lmap_w, S.gpart, S.train_grid, c->stream)) return rc;
     S.folded = true;
   }
   *out = LocalMap{S.lmap_w, S.lmap_lab};
+  return 0;
+}
+
+// Star-lab index of cube position q (x, y, z in -1..8): the block's cells,
+// then the six one-cell face layers (LabGeom<1>); -1 for edges, corners and
+// positions beyond the layers.
+static int star_index(const int q[3]) {
+  int out = -1, n = 0;
+  for (int d = 0; d < 3; ++d) {
+    if (q[d] < -1 || q[d] > BS) return -1;
+    if (q[d] == -1 || q[d] == BS) {
+      out = d;
+      ++n;
+    }
+  }
+  if (n == 0) return q[0] + BS * q[1] + BS * BS * q[2];
+  if (n > 1) return -1;
+  const int d = out, s = q[d] == BS ? 1 : 0;
+  return BN + (2 * d + s) * 64 + q[tan1(d)] + 8 * q[tan2(d)];
+}
+
+// The one-cell-overlap local solve (restricted additive Schwarz with a
+// one-cell overlap) as a local map: z_b = [L_s^-1 lab_b]_interior / h_b, with
+// L_s the 7-point Laplacian of unit spacing on the 896 star cells (the block
+// and its six face layers; zero beyond them: edges, corners and the next
+// layer).  The solver's phases already apply the block inverse
+// [L_b^-1 | 0] (L_b: the same operator on the block alone), so the map holds
+// the difference [L_s^-1]_interior - [L_b^-1 | 0].  A = h L on a uniform
+// neighbourhood (the AMR operator's same-level rows), hence the 1/h.
+int schwarz_prepare(cup_ctx* c, LocalMap* out) {
+  CnnState& S = c->cnn;
+  if (!S.schwarz_w) {
+    std::vector<double> Ls(size_t(LMAP_K) * LMAP_K, 0.0), Lb(size_t(BN) * BN, 0.0);
+    for (int j = 0; j < LMAP_K; ++j) {
+      int q[3];
+      lmap_lab_pos(j, q);
+      Ls[size_t(j) * LMAP_K + j] = -6.0;
+      if (j < BN) Lb[size_t(j) * BN + j] = -6.0;
+      for (int d = 0; d < 3; ++d)
+        for (int e = -1; e <= 1; e += 2) {
+          int r[3] = {q[0], q[1], q[2]};
+          r[d] += e;
+          const int k = star_index(r);
+          if (k < 0) continue;
+          Ls[size_t(j) * LMAP_K + k] = 1.0;
+          if (j < BN && k < BN) Lb[size_t(j) * BN + k] = 1.0;
+        }
+    }
+    DevArena tmp;
+    double *dLs = nullptr, *dLb = nullptr;
+    if (int rc = tmp.alloc(&dLs, Ls.size())) return rc;
+    if (int rc = tmp.alloc(&dLb, Lb.size())) return rc;
+    if (int rc = device_inverse(Ls.data(), LMAP_K, dLs, c->num_sms, c->stream)) return rc;
+    if (int rc = device_inverse(Lb.data(), BN, dLb, c->num_sms, c->stream)) return rc;
+    CUP_CUDA_TRY(stream_d2h(c->stream, Ls.data(), dLs, Ls.size() * sizeof(double)));
+    CUP_CUDA_TRY(stream_d2h(c->stream, Lb.data(), dLb, Lb.size() * sizeof(double)));
+    // W[r][j] in the fold's layout out[j * 512 + r]
+    std::vector<float> w(size_t(LMAP_K) * BN);
+    for (int r = 0; r < BN; ++r)
+      for (int j = 0; j < LMAP_K; ++j)
+        w[size_t(j) * BN + r] = float(Ls[size_t(r) * LMAP_K + j] - (j < BN ? Lb[size_t(r) * BN + j] : 0.0));
+    float* dw = nullptr;
+    if (int rc = tmp.alloc(&dw, w.size())) return rc;
+    CUP_CUDA_TRY(stream_h2d(c->stream, dw, w.data(), w.size() * sizeof(float)));
+    uint4* wf = nullptr;
+    if (int rc = S.arena.alloc(&wf, LMAP_W_WORDS)) return rc;
+    if (int rc = lmap_pack(dw, wf, c->stream)) return rc;
+    CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    S.schwarz_w = wf;
+  }
+  if (int rc = ensure_lab(c)) return rc;
+  *out = LocalMap{S.schwarz_w, S.lmap_lab};
+  return 0;
+}
+
+// z += the local map on r's labs (its two phases as kernels of their own).
+static int map_correction(cup_ctx* c, const LocalMap& lm, const double* d_r, double* d_z) {
+  const int grid = std::max(1, std::min(c->num_sms * 2, (c->mesh.nb + LMAP_GATHER - 1) / LMAP_GATHER));
+  {
+    ProfScope ps("lmap_gather", c->stream);
+    k_lmap_gather<<<grid, 256, 0, c->stream>>>(c->dm, d_r, lm.lab, mean_block_of(c));
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  static unsigned long long attr = 0;
+  if (first_on_device(attr))
+    CUP_CUDA_TRY(cudaFuncSetAttribute(k_lmap_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LMAP_TILE_BYTES)));
+  {
+    ProfScope ps("lmap_gemm", c->stream);
+    k_lmap_gemm<<<std::max(1, c->num_sms * 2), 256, LMAP_TILE_BYTES, c->stream>>>(c->dm, lm.w, lm.lab, d_z);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+// z = block inverse of r + the local map on r's labs.
+static int map_apply(cup_ctx* c, const LocalMap& lm, const double* d_r, double* d_z) {
+  if (int rc = launch_block_inverse(c->dm, d_r, d_z, c->W, c->stream)) return rc;
+  if (int rc = map_correction(c, lm, d_r, d_z)) return rc;
+  CUP_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -177,26 +283,20 @@ int cup_cnn_dataset_reserve(cup_ctx* c, int32_t capacity) {
   return 0;
 }
 
-int cup_cnn_dataset_add(cup_ctx* c, const double* d_r, const double* d_e) {
+int cup_cnn_dataset_add(cup_ctx* c, const double* d_r, const double* /*d_e*/) {
   ProfBind pb_(c);
-  if (!dev_ok(c) || !d_r || !d_e) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_dataset_add: bad arguments");
+  if (!dev_ok(c) || !d_r) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_dataset_add: bad arguments");
   CnnState& S = c->cnn;
   if (S.cap == 0) return ctx_fail(c, CUP_ERR_STATE, "cup_cnn_dataset_add: no dataset (cup_cnn_dataset_reserve)");
   if (S.count >= S.cap) return 0;
-  // The network adds to the coarse correction and the block inverse of the
-  // two-level preconditioner: its target is what they leave of the error,
-  // e - P A_c^-1 P^T r (the block inverse's part is removed per sample).
-  if (int rc = coarse_build(c)) return ctx_fail(c, rc, cup_last_error(nullptr));
-  double* zc = c->W.t;
-  double* rest = c->W.nu;
-  const size_t n = nbn(c);
-  CUP_CUDA_TRY(cudaMemsetAsync(zc, 0, n * sizeof(double), c->stream));
-  if (int rc = coarse_apply<double>(c->coarse.view(), d_r, zc, nullptr, c->num_sms, c->stream))
-    return ctx_fail(c, rc, cup_last_error(nullptr));
-  k_axpy<<<c->W.grid, NT, 0, c->stream>>>(n, d_e, -1.0, zc, rest);
-  CUP_CUDA_TRY(cudaGetLastError());
-  if (int rc = cnn_dataset_add(c->dm, d_r, rest, S.ds_in, S.ds_target, S.count, S.cap, S.ds_count, c->W.grid,
-                               c->stream))
+  // the target: the overlap solve's correction of r (its local map alone)
+  LocalMap lm{};
+  if (int rc = schwarz_prepare(c, &lm)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  double* corr = c->W.t;
+  CUP_CUDA_TRY(cudaMemsetAsync(corr, 0, nbn(c) * sizeof(double), c->stream));
+  if (int rc = map_correction(c, lm, d_r, corr)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  if (int rc = cnn_dataset_add(c->dm, d_r, corr, S.ds_in, S.ds_target, S.count, S.cap, S.ds_count, c->W.grid,
+                               c->stream, mean_block_of(c)))
     return ctx_fail(c, rc, cup_last_error(nullptr));
   S.count = std::min(S.cap, S.count + c->mesh.nb);
   cudaError_t e = cudaStreamSynchronize(c->stream);
@@ -341,7 +441,7 @@ int cup_cnn_precond_dev(cup_ctx* c, const double* d_r, double* d_z) {
   if (!dev_ok(c) || !d_r || !d_z) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_precond_dev: bad arguments");
   if (!c->cnn.ready) return ctx_fail(c, CUP_ERR_STATE, "no weights");
   GridReduce g{c->W.partial, c->W.counters + 15};
-  if (int rc = cnn_apply<double>(c->dm, d_r, d_z, c->cnn.W, c->W.grid, c->stream, g, nullptr))
+  if (int rc = cnn_apply<double>(c->dm, d_r, d_z, c->cnn.W, c->W.grid, c->stream, g, nullptr, mean_block_of(c)))
     return ctx_fail(c, rc, cup_last_error(nullptr));
   cudaError_t e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_precond", __FILE__, __LINE__), cup_last_error(nullptr));
@@ -353,22 +453,21 @@ int cup_cnn_map_apply_dev(cup_ctx* c, const double* d_r, double* d_z) {
   if (!dev_ok(c) || !d_r || !d_z) return ctx_fail(c, CUP_ERR_ARG, "cup_cnn_map_apply_dev: bad arguments");
   LocalMap lm{};
   if (int rc = lmap_prepare(c, &lm)) return ctx_fail(c, rc, cup_last_error(nullptr));
-  if (int rc = launch_block_inverse(c->dm, d_r, d_z, c->W, c->stream)) return ctx_fail(c, rc, cup_last_error(nullptr));
-  const int grid = std::max(1, std::min(c->num_sms * 2, c->mesh.nb));
-  k_lmap_gather<<<grid, 256, 0, c->stream>>>(c->dm, d_r, c->cnn.lmap_lab);
-  CUP_CUDA_TRY(cudaGetLastError());
-  static unsigned long long attr = 0;
-  if (first_on_device(attr))
-    CUP_CUDA_TRY(cudaFuncSetAttribute(k_lmap_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, int(LMAP_TILE_BYTES)));
-  k_lmap_gemm<<<grid, 256, LMAP_TILE_BYTES, c->stream>>>(c->dm, lm.w, lm.lab, d_z);
-  CUP_CUDA_TRY(cudaGetLastError());
-  cudaError_t e = cudaStreamSynchronize(c->stream);
-  if (e != cudaSuccess) return ctx_fail(c, set_cuda_error(e, "cnn_map_apply", __FILE__, __LINE__), cup_last_error(nullptr));
+  if (int rc = map_apply(c, lm, d_r, d_z)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  return 0;
+}
+
+int cup_schwarz_apply_dev(cup_ctx* c, const double* d_r, double* d_z) {
+  ProfBind pb_(c);
+  if (!dev_ok(c) || !d_r || !d_z) return ctx_fail(c, CUP_ERR_ARG, "cup_schwarz_apply_dev: bad arguments");
+  LocalMap lm{};
+  if (int rc = schwarz_prepare(c, &lm)) return ctx_fail(c, rc, cup_last_error(nullptr));
+  if (int rc = map_apply(c, lm, d_r, d_z)) return ctx_fail(c, rc, cup_last_error(nullptr));
   return 0;
 }
 
 int cup_set_poisson(cup_ctx* c, int32_t solver, double tol_abs, double tol_rel, int32_t max_iter) {
-  if (!c || solver < 0 || solver > CUP_POISSON_B200_TWOLEVEL || max_iter < 0)
+  if (!c || solver < 0 || solver > CUP_POISSON_B200_SCHWARZ || max_iter < 0)
     return ctx_fail(c, CUP_ERR_ARG, "cup_set_poisson: bad arguments");
   c->cfg.poisson_solver = solver;
   c->cfg.poisson_tol = tol_abs;

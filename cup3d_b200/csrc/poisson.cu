@@ -1070,7 +1070,8 @@ constexpr size_t kSmemTiles = kSmemCache + PGROUPS * KB_CACHE * sizeof(BlockInfo
 constexpr size_t kPersistentSmem = kSmemTiles + PGROUPS * sizeof(GroupTile);
 constexpr size_t kLearnedSmem = std::max(kPersistentSmem, kSmemTiles + LMAP_TILE_BYTES);
 static_assert(kSmemTiles % 16 == 0, "tiles and staged labs start 16-byte aligned");
-static_assert(LMAP_K * sizeof(double) <= PGROUPS * sizeof(GroupTile), "the gather's lab fits in the tiles");
+static_assert(LMAP_GATHER * sizeof(LabMeta) <= PGROUPS * sizeof(GroupTile), "the gather's table entries fit in the tiles");
+static_assert(PNT == 256, "the learned map's phases run on 8 warps (4 groups of 64 threads)");
 
 template <class T>
 __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A, GridSync Gs) {
@@ -1114,6 +1115,8 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
     if (threadIdx.x == 0) fin_init(S, a[0]);
     __syncthreads();
   }
+  // the mean-constraint row (modes 1 and 3 replace cell 0 of the mean block)
+  const int mean_blk = (A.mean_mode == 1 || A.mean_mode == 3) ? M.mean_block : -1;
   // The parts of the preconditioner that need the whole vector v (nu or r)
   // in place, added to its block part z (zv or zr):
   //   * the coarse correction of the two-level preconditioner, from v's
@@ -1127,7 +1130,7 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_persistent(KArgs<T> A
     if (A.cnb) PERSISTENT_BLOCKS(bi) a[0] += coarse_block<T>(A, G, bi.id, rc, z, &gred[2 * G.g]);
     if (A.lw) {
       __syncthreads();  // the groups are done with their tiles
-      lmap_gather<T>(M, v, A.llab, reinterpret_cast<double*>(smem_raw + kSmemTiles));
+      lmap_gather<T>(M, v, A.llab, reinterpret_cast<LabMeta*>(smem_raw + kSmemTiles), mean_blk);
     }
     if (!grid_allreduce<1>(a, Gs, epoch, red)) return false;
     added = a[0];

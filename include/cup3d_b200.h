@@ -49,6 +49,10 @@ extern "C" {
 #define CUP_POISSON_B200_TWOLEVEL 4 /* "b200_twolevel": BiCGSTAB, two-level preconditioner without
                                        the network (coarse correction + block inverse); the
                                        method the learned one is compared with */
+#define CUP_POISSON_B200_SCHWARZ 5  /* "b200_schwarz": the two-level preconditioner with the exact
+                                       one-cell-overlap local solve of each block (restricted
+                                       additive Schwarz) in place of the block inverse; the local
+                                       map the network is trained to reproduce */
 
 /* field ids */
 #define CUP_FIELD_VEL 0   /* 3 components */
@@ -327,17 +331,23 @@ int cup_set_barrier_limit(cup_ctx* ctx, int64_t cycles);
 
 /* ---- learned preconditioner (no counterpart in the reference: the new slot at
  * the preconditioner call sites PoissonSolverAMR.h:183-222, BiCGSTAB.cu:526-527).
- * z = P A_c^-1 P^T r + BJ(r) + (s/h) CNN(r_block+halo / s): the coarse correction,
- * the exact block inverse and a per-block 3-D CNN correction (4 conv 3^3 layers,
- * 16 channels, BF16 weights, FP32 accumulation). ---- */
+ * z = P A_c^-1 P^T r + BJ(r) + (s/h) CNN(r_lab / s): the coarse correction, the exact
+ * block inverse and a per-block 3-D CNN correction of the block's residual lab (4 linear
+ * conv 3^3 layers, 16 channels, BF16 weights, FP32 accumulation; no biases, so the
+ * preconditioner is a fixed linear map).  The solver applies the network folded into one
+ * 512 x 896 matrix on the tensor cores. ---- */
 int32_t cup_cnn_num_params(void);
 int cup_cnn_init(cup_ctx* ctx, uint64_t seed);                 /* random initial weights */
 int cup_cnn_set_params(cup_ctx* ctx, const float* params);     /* cup_cnn_num_params() floats */
 int cup_cnn_get_params(cup_ctx* ctx, float* params);
 int cup_cnn_dataset_reserve(cup_ctx* ctx, int32_t capacity);   /* samples (one per block per pair) */
-/* adds one sample per block from device vectors: residual r and error e = x* - x; the
- * sample's target is what the coarse correction and the block inverse leave of e
- * (e - P A_c^-1 P^T r - B^-1 r, the network's part of the two-level preconditioner) */
+/* adds one sample per block from a device residual r of a solver iterate: the input is r's
+ * block lab (block + one-cell face layers, residual rules), the target the correction of the
+ * one-cell-overlap local solve over the block inverse, [L_s^-1 lab]_interior - B^-1 r (the
+ * "b200_schwarz" local map).  d_e (the iterate's error x* - x) is accepted and not used (may
+ * be NULL): a local map fitted to the error itself is a poor preconditioner, because the
+ * error's smooth part cannot be told from a block's lab (a least-squares fit of it made the
+ * two-level solve of a uniform test problem take 534 instead of 28 iterations). */
 int cup_cnn_dataset_add(cup_ctx* ctx, const double* d_r, const double* d_e);
 int32_t cup_cnn_dataset_size(const cup_ctx* ctx);
 /* the last ntest samples are held out of training; cup_cnn_eval: the network's
@@ -358,6 +368,9 @@ int cup_cnn_precond_dev(cup_ctx* ctx, const double* d_r, double* d_z);
 /* The same through the solver's path: block inverse + the network folded into
  * one 512 x 896 matrix (BF16 tensor-core GEMM on the BF16 star labs of r). */
 int cup_cnn_map_apply_dev(cup_ctx* ctx, const double* d_r, double* d_z);
+/* z = block inverse of r + the one-cell-overlap local solve's correction (the
+ * "b200_schwarz" local map), per block, on the same path */
+int cup_schwarz_apply_dev(cup_ctx* ctx, const double* d_r, double* d_z);
 
 /* Network forward on host arrays, as cup_cnn_forward_host, without allocating
  * or freeing device memory.  No counterpart in the reference.

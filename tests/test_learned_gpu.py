@@ -1,15 +1,18 @@
-"""Learned preconditioner (a per-block CNN correction on top of the coarse
-correction and the exact block inverse, inside flexible BiCGSTAB with a
-block-Jacobi fallback).
+"""Learned preconditioner (a per-block linear CNN correction on top of the
+coarse correction and the exact block inverse, inside BiCGSTAB with a
+block-Jacobi fallback; the solver applies the network folded into one
+matrix).
 
 * forward and gradient of the BF16 tensor-core kernels against the oracle's
   FP64 CNN: relative error <= 2e-2 (BF16 activations and weights, FP32
   accumulation);
-* training on residual/error pairs the plain solver produces lowers the loss
-  on held-out samples (another right-hand side);
+* training on the residuals the plain solver produces (target: the
+  one-cell-overlap local solve's correction of each block) lowers the loss
+  on held-out samples (another right-hand side) below a tenth;
 * the trained preconditioner solves to the FP64 tolerance (checked on the
-  true residual); its iterations against the plain solver and against the
-  two-level method without the network are printed and bounded;
+  true residual), in fewer iterations than the untrained network and within
+  a bound of the two-level method without the network (the numbers, with
+  the exact overlap solve's, are printed);
 * a preconditioner that stalls hands over to block-Jacobi (fallback flag).
 """
 import numpy as np
@@ -99,22 +102,29 @@ def test_training_reduces_held_out_loss_and_solver_converges():
     assert ctx.cnn_dataset_size() > 2000
     ctx.cnn_holdout(m.nb)  # the last right-hand side's samples are held out
     before = ctx.cnn_eval()
+    params0 = ctx.cnn_get_params()
     losses = ctx.cnn_train(300, 64, 1e-3, 11)
     after = ctx.cnn_eval()
     assert np.isfinite(losses).all()
     print(f"held-out relative loss {before:.4f} -> {after:.4f}; training loss "
           f"{np.mean(losses[:10]):.4f} -> {np.mean(losses[-10:]):.4f}")
-    assert after < 0.9 * before, (before, after)
+    assert after < 0.1 * before, (before, after)
     assert np.mean(losses[-20:]) < np.mean(losses[:20])
     # held-out right-hand sides: iterations of the plain solver, of the
-    # two-level preconditioner without the network and with it
+    # two-level preconditioner without the network, with the exact overlap
+    # solve, with the trained network and with the untrained one
     its = {}
-    for solver in ("b200", "b200_twolevel", "b200_learned"):
+    trained = ctx.cnn_get_params()
+    for solver in ("b200", "b200_twolevel", "b200_schwarz", "b200_learned", "untrained"):
+        if solver == "untrained":
+            ctx.cnn_set_params(params0)
+        else:
+            ctx.cnn_set_params(trained)
         tot = 0
         for seed in (90, 91):
             b = rhs(m, seed)
             bd, xd = torch_dev(b), torch_dev(np.zeros(m.n))
-            ctx.set_poisson(solver, 0.0, 1e-8, 1000)
+            ctx.set_poisson("b200_learned" if solver == "untrained" else solver, 0.0, 1e-8, 1000)
             rc, st = ctx.poisson_solve_dev(bd, xd)
             assert st["status"] == 1 and st["true_rel"] <= 1.001e-8 * 1.5
             x = xd.cpu().numpy()
@@ -126,7 +136,8 @@ def test_training_reduces_held_out_loss_and_solver_converges():
         its[solver] = tot
     print("iterations", its)
     assert its["b200_twolevel"] < its["b200"], its
-    assert its["b200_learned"] <= 1.5 * its["b200_twolevel"] + 6, its
+    assert its["b200_learned"] < its["untrained"], its
+    assert its["b200_learned"] <= 1.15 * its["b200_twolevel"] + 4, its
 
 
 def test_stalling_preconditioner_falls_back():
@@ -165,8 +176,9 @@ def test_zero_network_is_the_block_inverse():
 
 
 def test_untrained_network_keeps_the_two_level_convergence():
-    # the initial network's output is small: the learned solve converges like
-    # the two-level preconditioner without the network, with no fallback
+    # the initial network's output is small: the learned solve converges
+    # within a quarter of the two-level preconditioner's iterations, with no
+    # fallback
     ctx = make_ctx("amr3_mixed", device=0)
     m = oracle_mesh(ctx)
     ctx.cnn_init(7)
@@ -177,4 +189,4 @@ def test_untrained_network_keeps_the_two_level_convergence():
         rc, st = ctx.poisson_solve_dev(bd, xd)
         assert rc == 0 and st["status"] == 1 and st["fallback"] == 0, (solver, st)
         its[solver] = st["iterations"]
-    assert its["b200_learned"] <= its["b200_twolevel"] + 5, its
+    assert its["b200_learned"] <= 1.25 * its["b200_twolevel"], its
