@@ -136,22 +136,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def train_learned(ctx, seeds=range(6), iters=(0, 1, 2, 3, 5, 8, 12), steps=600, batch=128, lr=5e-4):
-    """Trains the block CNN on (residual, error) pairs of plain solves of
-    seeded white-noise right-hand sides on the context's mesh."""
+def train_learned(ctx, rhs_list, iters=(0, 1, 2, 3, 5, 8, 12), steps=600, batch=128, lr=1e-3):
+    """Trains the block CNN on the residuals of plain solves of the flow's own
+    pressure right-hand sides (rhs_list, collected during the run; the last one
+    is held out), at the iterates `iters`.  The target of each block sample
+    is the one-cell-overlap local solve's correction of its residual."""
     import torch
-    _, hh = ctx.cell_centres()
-    w = hh ** 3
     level, index, _ = ctx.blocks()
     mb = int(np.where((index == 0).all(axis=1))[0][0])
     ctx.cnn_init(7)
-    ctx.cnn_dataset_reserve(ctx.nb * len(seeds) * len(iters))
-    for seed in seeds:
-        bh = np.random.default_rng(1000 + seed).standard_normal(len(hh))
-        b = torch.tensor(bh - np.sum(bh * w) / np.sum(w), device="cuda")
-        xs = torch.zeros_like(b)
-        ctx.set_poisson("b200", 0.0, 1e-10, 1000)
-        ctx.poisson_solve_dev(b, xs)
+    ctx.cnn_dataset_reserve(ctx.nb * len(rhs_list) * len(iters))
+    for bh in rhs_list:
+        b = torch.tensor(bh, device="cuda")
         for k in iters:
             xk = torch.zeros_like(b)
             if k > 0:
@@ -161,25 +157,33 @@ def train_learned(ctx, seeds=range(6), iters=(0, 1, 2, 3, 5, 8, 12), steps=600, 
             ctx.poisson_apply(xk, ax)
             r = b - ax
             r[mb * 512] = -ax[mb * 512]  # the mean-constraint row's right-hand side is zero
-            ctx.cnn_dataset_add(r.contiguous(), (xs - xk).contiguous())
+            ctx.cnn_dataset_add(r.contiguous())
+    ctx.cnn_holdout(ctx.nb * len(iters))
+    before = ctx.cnn_eval()
     losses = ctx.cnn_train(steps, batch, lr, 11)
-    return {"samples": ctx.cnn_dataset_size(), "steps": steps, "batch": batch, "lr": lr,
-            "loss_first10": float(np.mean(losses[:10])), "loss_last10": float(np.mean(losses[-10:]))}
+    return {"pairs": f"residuals of plain BiCGSTAB iterates {list(iters)} on {len(rhs_list)} pressure right-hand "
+                     f"sides of the sphere flow (the last held out)",
+            "samples": ctx.cnn_dataset_size(), "steps": steps, "batch": batch, "lr": lr,
+            "loss_first10": float(np.mean(losses[:10])), "loss_last10": float(np.mean(losses[-10:])),
+            "held_out_rel_loss": [round(float(before), 4), round(float(ctx.cnn_eval()), 4)]}
 
 
-def poisson_at_tolerance(ctx, stream, flush, reps=3):
+SOLVERS = ("b200", "b200_mixed", "b200_twolevel", "b200_schwarz", "b200_learned", "b200_learned_mixed")
+
+
+def poisson_at_tolerance(ctx, stream, flush, rhs_list, reps=3):
     """Device time of one Poisson solve to a relative residual (FP64-checked
-    true residual), plain vs mixed vs learned, on the seeded right-hand side."""
+    true residual) for every solver, on the seeded right-hand side."""
     import torch
     b = torch.tensor(poisson_rhs(ctx), device="cuda")
     t0 = time.perf_counter()
-    training = train_learned(ctx)
+    training = train_learned(ctx, rhs_list)
     torch.cuda.synchronize()
     training["seconds"] = round(time.perf_counter() - t0, 2)
     res = {"rhs": "PCG64(20261203) white noise + 8 Gaussian sources, h^3-weighted zero mean; x0 = 0",
            "training": training}
     for tol in (1e-6, 1e-10):
-        for solver in ("b200", "b200_mixed", "b200_learned", "b200_learned_mixed"):
+        for solver in SOLVERS:
             runs = []
             for _ in range(reps):
                 x = torch.zeros_like(b)
@@ -200,7 +204,7 @@ def poisson_at_tolerance(ctx, stream, flush, reps=3):
     base = res["b200@1e-06"]["ms"]
     res["speedup_vs_b200@1e-06"] = {k.split("@")[0]: round(base / v["ms"], 3)
                                     for k, v in res.items() if k.endswith("@1e-06")}
-    ctx.set_poisson("b200", 1e-6, 1e-4, 1000)
+    ctx.set_poisson(ctx.solver_name, 1e-6, 1e-4, 1000)
     return res
 
 
@@ -308,15 +312,22 @@ def run_b200(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     import cup3d_b200 as cup
-    ctx = make_sphere_ctx(local)
+    ctx = make_sphere_ctx(local, args.solver)
+    ctx.solver_name = args.solver
     nb = ctx.nb
     ncell = nb * 512
     stream = torch.cuda.ExternalStream(cup._lib.lib().cup_stream(ctx._p))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     step = 0
-    for _ in range(args.warmup):
+    # untimed: the warm-up steps, then settling steps past the start of the
+    # CFL ramp; the flow's pressure right-hand sides of some of them are kept
+    # as training data of the learned preconditioner
+    rhs_list = []
+    for k in range(args.warmup + args.settle):
         ctx.step(step)
         step += 1
+        if k % 8 == 7 and len(rhs_list) < 6:
+            rhs_list.append(ctx.download("lhs"))
     # The timed pass, the per-kernel pass and the end-to-end pass all run the
     # same K steps from the same state (velocity and pressure are the whole
     # state carried between steps), so their Poisson solves do the same work.
@@ -389,13 +400,17 @@ def run_b200(args):
     dom_name, (dom_n, dom_ms) = dom
     per_launch_ms = dom_ms / max(dom_n, 1)
     if dom_name == "bicg_persistent":
-        # one launch per solve, 176 B/cell per iteration
-        alg_bytes = int(ALG_BYTES[dom_name] * ncell * sum(prof_iters) / max(dom_n, 1))
+        # one launch per solve, 176 B/cell per iteration; the two-level solver
+        # adds two coarse corrections per iteration: a read-modify-write of z
+        # (16 B/cell) and a row of A_c^-1 per block (8 nb^2 bytes) each
+        per_cell = ALG_BYTES[dom_name] + (32 if args.solver == "b200_twolevel" else 0)
+        per_iter = per_cell * ncell + (16 * nb * nb if args.solver == "b200_twolevel" else 0)
+        alg_bytes = int(per_iter * sum(prof_iters) / max(dom_n, 1))
     else:
         alg_bytes = ALG_BYTES.get(dom_name, 0) * ncell
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if alg_bytes else None
     traffic = None
-    if dom_name in MEASURED_TRAFFIC_PER_CELL_ITER:
+    if dom_name in MEASURED_TRAFFIC_PER_CELL_ITER and args.solver == "b200":
         traffic = int(MEASURED_TRAFFIC_PER_CELL_ITER[dom_name] * ncell * sum(prof_iters) / max(dom_n, 1))
     # ---- e2e through the C ABI with host buffers: the same K steps, the state
     # uploaded from pinned host memory before and downloaded after every step
@@ -429,7 +444,7 @@ def run_b200(args):
         e2e_ms = float(t.item())
     e2e_value = world * ncell * args.steps / (e2e_ms * 1e-3) / 1e6
     line = {
-        "metric": "Mcell-steps/s (whole time step, sphere Re=300 AMR, plain FP64)",
+        "metric": "Mcell-steps/s (whole time step, sphere Re=300 AMR, FP64)",
         "value": round(value, 3),
         "unit": "Mcell-steps/s",
         "n_gpus": world,
@@ -442,9 +457,12 @@ def run_b200(args):
         "dtype": "f64",
         "data": "synthetic (seeded, generated in-process)",
         "config": {"workload": WORKLOAD, "blocks": nb, "cells": ncell, "levels_used": [1, 2, 3],
-                   "poisson": "b200 fp64 BiCGSTAB + exact block inverse, tol 1e-6 abs / 1e-4 rel",
+                   "poisson": f"{args.solver}: FP64 BiCGSTAB, "
+                              + ("two-level preconditioner (block-constant coarse space + exact block inverse)"
+                                 if args.solver == "b200_twolevel" else "exact block inverse")
+                              + ", tol 1e-6 abs / 1e-4 rel (PoissonErrorTol / PoissonErrorTolRel)",
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps",
-                   "first_timed_step": args.warmup},
+                   "first_timed_step": args.warmup + args.settle},
         "poisson": {"iterations_per_step": iters, "solve_ms_per_step": [round(x, 3) for x in solve_ms]},
         "kernels": {"pass": f"the same {args.steps} steps again with per-launch CUDA events "
                             f"(Poisson iterations {prof_iters})",
@@ -462,7 +480,7 @@ def run_b200(args):
         "clocks": clk,
     }
     if not args.no_poisson:
-        line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush)
+        line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush, rhs_list)
     if rank == 0 and not args.no_swarm:
         line["swarm_batch"] = swarm_batch(flush)
     if rank == 0 and not args.no_obstacle:
@@ -549,7 +567,7 @@ def run_reference(args):
     value = m.n * args.steps / total / 1e6
     line = {
         "impl": "reference",
-        "metric": "Mcell-steps/s (whole time step, sphere Re=300 AMR, plain FP64)",
+        "metric": "Mcell-steps/s (whole time step, sphere Re=300 AMR, FP64)",
         "value": round(value, 4), "unit": "Mcell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -570,6 +588,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--solver", default="b200_twolevel", choices=["b200", "b200_twolevel"],
+                    help="Poisson solver of the timed steps")
+    ap.add_argument("--settle", type=int, default=50, help="untimed steps after the warm-up")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson-to-tolerance comparison")
     ap.add_argument("--no-swarm", action="store_true", help="skip the batched ellipsoid-swarm measurement")

@@ -357,9 +357,11 @@ class Context:
     def cnn_dataset_reserve(self, capacity):
         check(lib().cup_cnn_dataset_reserve(self._p, capacity), self._p)
 
-    def cnn_dataset_add(self, r, e):
-        """One sample per block from device vectors r (residual) and e (error)."""
-        check(lib().cup_cnn_dataset_add(self._p, _dev_ptr(r), _dev_ptr(e)), self._p)
+    def cnn_dataset_add(self, r, e=None):
+        """One sample per block from the device residual r of a solver iterate
+        (target: the one-cell-overlap local solve's correction; e, the
+        iterate's error, is not used)."""
+        check(lib().cup_cnn_dataset_add(self._p, _dev_ptr(r), _dev_ptr(e) if e is not None else None), self._p)
 
     def cnn_dataset_size(self):
         return lib().cup_cnn_dataset_size(self._p)

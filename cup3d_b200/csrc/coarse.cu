@@ -119,15 +119,21 @@ __global__ void k_gj_extract(const double* __restrict__ G, int n, double* __rest
   }
 }
 
+// FP32 copy of a device array
+__global__ void k_to_float(const double* __restrict__ a, size_t n, float* __restrict__ out) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    out[i] = float(a[i]);
+}
+
 // y = Ainv x (n x n, row-major): one warp per row
-__global__ void __launch_bounds__(NT) k_coarse_gemv(const double* __restrict__ Ainv, const double* __restrict__ x,
+__global__ void __launch_bounds__(NT) k_coarse_gemv(const float* __restrict__ Ainv, const double* __restrict__ x,
                                                     int n, double* __restrict__ y) {
   const int lane = threadIdx.x & 31;
   const int warps = blockDim.x >> 5;
   for (int row = blockIdx.x * warps + (threadIdx.x >> 5); row < n; row += gridDim.x * warps) {
-    const double* a = Ainv + size_t(row) * n;
+    const float* a = Ainv + size_t(row) * n;
     double s = 0.0;
-    for (int j = lane; j < n; j += 32) s += a[j] * __ldg(x + j);
+    for (int j = lane; j < n; j += 32) s += double(a[j]) * __ldg(x + j);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) y[row] = s;
@@ -282,10 +288,21 @@ int coarse_build(cup_ctx* c) {
     }
   }
   // A_c^-1 by Gauss-Jordan on the device
+  // in FP64, kept in FP32: the two coarse corrections of an iteration read
+  // it whole (8 nb^2 bytes each in FP64, a large part of an iteration's
+  // traffic on meshes of a few thousand blocks)
   DevArena& A = C.arena;
-  if (int rc = A.alloc(&C.inv, size_t(nb) * nb)) return rc;
-  if (int rc = device_inverse(Ac.data(), nb, C.inv, c->num_sms, s))
-    return rc == CUP_ERR_MESH ? set_error(CUP_ERR_MESH, "two-level preconditioner: singular coarse operator") : rc;
+  {
+    DevArena tinv;
+    double* inv64 = nullptr;
+    if (int rc = tinv.alloc(&inv64, size_t(nb) * nb)) return rc;
+    if (int rc = device_inverse(Ac.data(), nb, inv64, c->num_sms, s))
+      return rc == CUP_ERR_MESH ? set_error(CUP_ERR_MESH, "two-level preconditioner: singular coarse operator") : rc;
+    if (int rc = A.alloc(&C.inv, size_t(nb) * nb)) return rc;
+    k_to_float<<<std::max(1, c->num_sms * 8), NT, 0, s>>>(inv64, size_t(nb) * nb, C.inv);
+    CUP_CUDA_TRY(cudaGetLastError());
+    CUP_CUDA_TRY(cudaStreamSynchronize(s));
+  }
   if (int rc = A.alloc(&C.rc, nb)) return rc;
   if (int rc = A.alloc(&C.yc, nb)) return rc;
   if (int rc = A.alloc(&C.rc2, nb)) return rc;

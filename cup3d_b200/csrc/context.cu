@@ -832,6 +832,9 @@ static int graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraph
   CUP_CUDA_TRY(stream_h2d(s, c->W.st_init, &init, sizeof(init)));
   DevMesh dmg = c->dm;
   dmg.case_dt = c->d_scalars + SC_GDT;
+  // the two-level solver's coarse space (built before the capture by graph_step)
+  const CoarseView cview = c->coarse.view();
+  const CoarseView* coarse = c->cfg.poisson_solver == CUP_POISSON_B200_TWOLEVEL ? &cview : nullptr;
   const int step_arg = use_pold ? c->cfg.step_2nd_start + 1 : 0;
   CUP_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   int rc = 0;
@@ -863,7 +866,8 @@ static int graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cudaGraph
     // event record nodes (external): the solve's device time, read after replay
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev0, s, cudaEventRecordExternal));
     SolveStats S{};
-    if (int r = poisson_bicgstab(c->dm, F.lhs, F.phi, P, c->W, S, s, c->h_pinned, nullptr)) return r;
+    if (int r = poisson_bicgstab(c->dm, F.lhs, F.phi, P, c->W, S, s, c->h_pinned, nullptr, coarse, c->num_sms))
+      return r;
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev1, s, cudaEventRecordExternal));
     if (int r = launch_weighted_sum(c->dm, F.phi, c->d_scalars + SC_SUMS, c->W, s)) return r;
     if (int r = launch_grad_update(dmg, F.vel[v], F.phi, pold, pnew, c->d_scalars + SC_SUMS, 0.0, step_arg,
@@ -895,6 +899,14 @@ static int graph_step(cup_ctx* c, int step, double* dt_used, cup_solve_stats* st
   Fields& F = c->F;
   const int use_pold = step > c->cfg.step_2nd_start ? 1 : 0;
   const int key = F.vcur | (F.pcur << 1) | (use_pold << 2);
+  if (c->cfg.poisson_solver == CUP_POISSON_B200_TWOLEVEL) {
+    // the captured steps hold the coarse space's buffers: a rebuilt one (a
+    // new mesh) needs new captures
+    const int before = c->coarse.mesh_version;
+    const float* inv = c->coarse.inv;
+    if (int rc = coarse_build(c)) return keep(c, rc);
+    if (c->coarse.mesh_version != before || c->coarse.inv != inv) graph_reset(c);
+  }
   if (!c->gexec[key])
     if (int rc = graph_capture(c, F.vcur, F.pcur, use_pold, &c->gexec[key])) return keep(c, rc);
   c->gio->cfl_fac = ctx_cfl_factor(c->cfg, step);
@@ -1069,7 +1081,9 @@ int cup_step(cup_ctx* c, int32_t step, double dt, double* dt_used, cup_solve_sta
   c->proj_open = 0;
   if (body_update_uinf(c)) graph_reset(c);  // CreateObstacles: the frame follows the body
   const bool moving = body_moves(c);
-  if (!(dt > 0) && c->cfg.step_graph && c->cfg.poisson_solver == CUP_POISSON_B200 && !c->prof.on && !moving) {
+  if (!(dt > 0) && c->cfg.step_graph &&
+      (c->cfg.poisson_solver == CUP_POISSON_B200 || c->cfg.poisson_solver == CUP_POISSON_B200_TWOLEVEL) &&
+      !c->prof.on && !moving) {
     const int rc = graph_step(c, step, dt_used, stats);
     if (rc >= 0) {
       body_coef_u(c, step, c->gio->dt);

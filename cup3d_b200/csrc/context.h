@@ -105,7 +105,7 @@ struct CoarseSpace {
   int nb = 0;                   // blocks it was built for (0: not built)
   int mesh_version = -1;        // cup_ctx::mesh_version it was built for
   int colours = 0;              // colours of the set-up
-  double* inv = nullptr;        // nb x nb, row-major
+  float* inv = nullptr;         // A_c^-1, nb x nb, row-major, FP32 (a preconditioner needs no more)
   double* rc = nullptr;         // nb: restricted vector
   double* rc2 = nullptr;        // nb: the second one of the persistent solver
   double* yc = nullptr;         // nb: coarse correction

@@ -366,7 +366,7 @@ struct KArgs {
   // two-level preconditioner (persistent solver): A_c^-1 (cnb x cnb, cnb = 0:
   // none), the restricted vectors of zv and zr and the blocks' 512 h^3
   int cnb;
-  const double* cinv;
+  const float* cinv;
   double* crc_v;
   double* crc_r;
   const double* cw;
@@ -902,9 +902,9 @@ __device__ __forceinline__ void coarse_restrict(const double c[8], double* rc, i
 template <class T>
 __device__ __forceinline__ double coarse_block(const KArgs<T>& A, const GroupIdx& G, int b, const double* rc, T* v,
                                                double* gsm) {
-  const double* row = A.cinv + size_t(b) * A.cnb;
+  const float* row = A.cinv + size_t(b) * A.cnb;
   double s[1] = {0.0};
-  for (int j = G.lane; j < A.cnb; j += GROUP) s[0] += row[j] * __ldcg(rc + j);
+  for (int j = G.lane; j < A.cnb; j += GROUP) s[0] += double(row[j]) * __ldcg(rc + j);
   group_reduce<1>(s, gsm, G);
   const double yc = s[0];
   double c[8];

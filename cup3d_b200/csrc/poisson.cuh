@@ -100,7 +100,7 @@ int launch_block_inverse(const DevMesh& M, const double* in, double* out, Poisso
 // the blocks' 512 h^3.  nb = 0: no coarse correction.
 struct CoarseView {
   int nb;
-  const double* inv;
+  const float* inv;  // FP32: the correction only has to be a fixed linear map
   double* rc;
   double* rc2;
   double* yc;

@@ -5,6 +5,9 @@
     python -m cup3d_b200.kernel_cases step    # 4 full time steps of the sphere workload
     python -m cup3d_b200.kernel_cases swarm   # 16 iterations of a batched solve over 8 swarm cases
 
+A second argument names the Poisson solver of the sphere cases (default
+b200; e.g. b200_twolevel).
+
 The sphere cases build the sphere mesh of cup3d_b200.workloads (2340
 blocks, 1.198M cells, ~0.3 GB of device memory); the swarm case batches the
 first 8 ellipsoid-swarm cases (10,879 blocks, 5.6M cells, ~2.5 GB).  Each exits
@@ -32,7 +35,8 @@ def main(argv):
         rc, st = batch.poisson_solve_dev(b, x)
         print(f"swarm ok: rc {rc}, {batch.nb} blocks, iterations {[s['iterations'] for s in st]}")
         return
-    ctx = make_sphere_ctx(0)
+    solver = argv[2] if len(argv) > 2 else "b200"
+    ctx = make_sphere_ctx(0, solver)
     n = ctx.nb * 512
     if case == "spmv":
         x = torch.tensor(np.random.default_rng(1).standard_normal(n), device="cuda")
@@ -43,7 +47,7 @@ def main(argv):
     elif case == "solve":
         b = torch.tensor(poisson_rhs(ctx), device="cuda")
         x = torch.zeros_like(b)
-        ctx.set_poisson("b200", 0.0, 1e-30, 16)
+        ctx.set_poisson(solver, 0.0, 1e-30, 16)
         rc, st = ctx.poisson_solve_dev(b, x)
         print(f"solve ok: rc {rc}, {st['iterations']} iterations")
     elif case == "step":

@@ -67,7 +67,8 @@ def test_coarse_apply_matches_dense_solve():
     ctx.coarse_apply(rd, zd)
     yc = np.linalg.solve(Ac, r.reshape(m.nb, 512).sum(axis=1))
     ref = np.repeat(yc, 512)
-    assert np.abs(zd.cpu().numpy() - ref).max() <= 1e-10 * np.abs(ref).max()
+    # A_c^-1 is kept in FP32
+    assert np.abs(zd.cpu().numpy() - ref).max() <= 1e-5 * np.abs(ref).max()
 
 
 def test_twolevel_solve_on_sphere_mesh():
@@ -91,3 +92,26 @@ def test_twolevel_solve_on_sphere_mesh():
         print(f"{solver}: {st['iterations']} iterations, {st['milliseconds']:.2f} ms, true residual {r_true:.2e}")
     print("iterations to 1e-6 on the sphere mesh", its)
     assert its["b200_twolevel"] * 3 <= its["b200"], its
+
+
+def test_captured_twolevel_step_equals_launched_step():
+    # the time step captured as a CUDA graph runs the two-level solver with
+    # the coarse space built before the capture: the same steps as launched
+    import cup3d_b200 as cup
+    from cup3d_b200.workloads import SPHERE_FLAGS, SPHERE_MESH, SPHERE_BODY
+    out = []
+    for g in (1, 0):
+        ctx = cup.Context(cup.config(SPHERE_FLAGS + f" -poissonSolver b200_twolevel -stepGraph {g}", device=0))
+        ctx.set_mesh_sphere_wake(**SPHERE_MESH)
+        ctx.obstacle_sphere(**SPHERE_BODY)
+        its = []
+        for step in range(4):
+            dt, rc, st = ctx.step(step)
+            assert rc == 0, st
+            its.append(st["iterations"])
+        out.append((ctx.download("vel"), ctx.download("pres"), its))
+    (v1, p1, i1), (v0, p0, i0) = out
+    print("two-level step iterations, captured / launched:", i1, i0)
+    assert i1 == i0
+    assert np.abs(v1 - v0).max() <= 1e-12 * np.abs(v0).max()
+    assert np.abs(p1 - p0).max() <= 1e-12 * np.abs(p0).max()
