@@ -404,6 +404,21 @@ class Context:
         """z = block inverse + folded network on r, the solver's path."""
         check(lib().cup_cnn_map_apply_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
 
+    FORCE_KEYS = ("surfForce", "presForce", "viscForce", "surfTorque")
+    FORCE_SCALARS = ("drag", "thrust", "Pout", "PoutBnd", "defPower", "defPowerBnd", "pLocom", "Pthrust", "Pdrag",
+                     "EffPDef", "EffPDefBnd")
+
+    def compute_forces(self):
+        """ComputeForces on the current velocity and pressure: dict of the
+        surface force, its pressure and viscous parts, the torque (arrays of 3)
+        and the scalar quantities of Obstacle::computeForces."""
+        out = np.zeros(23)
+        check(lib().cup_compute_forces(self._p, dptr(out)), self._p)
+        res = {k: out[3 * i:3 * i + 3].copy() for i, k in enumerate(self.FORCE_KEYS)}
+        res.update({k: float(out[12 + i]) for i, k in enumerate(self.FORCE_SCALARS)})
+        res["raw"] = out
+        return res
+
     def schwarz_apply(self, r, z):
         """z = block inverse + the one-cell-overlap local solve's correction on r."""
         check(lib().cup_schwarz_apply_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)

@@ -157,6 +157,7 @@ SIGNATURES = {
     "cup_cnn_precond_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_cnn_map_apply_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
     "cup_schwarz_apply_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "cup_compute_forces": (C.c_int, [_P, _D]),
     "cup_cnn_forward_host_noalloc": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32]),
     "cup_profile": (C.c_int, [_P, C.c_int32]),
     "cup_profile_read": (C.c_int, [_P, C.c_char_p, C.c_int32]),

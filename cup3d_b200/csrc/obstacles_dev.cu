@@ -405,6 +405,243 @@ void set_kinematics(Shape& s, const double* vel, const double* omega) {
   }
 }
 
+// ---- surface forces (ComputeForces, FluidSolidForces.cpp:14-229) ------------
+// Surface points of an obstacle block (KernelCharacteristicFunction's second
+// loop, ObstaclesCreate.cpp:83-117, and ObstacleBlock::write): cells where the
+// gradient of the block's own chi (central inside, one-sided second order at
+// the block's faces) is not zero and the smoothed delta
+//   Delta = (h^2 / 2) grad(chi) . grad(sdf) / |grad(sdf)|^2
+// exceeds machine epsilon; the point's normal is -Delta grad(sdf) (it carries
+// h^3).  One CTA per slot; nrm is component-major [3][nslots][512], zero
+// where a cell is no surface point.
+__global__ void __launch_bounds__(BN) k_obst_surface(const double* __restrict__ h_, const double* __restrict__ origin,
+                                                      Shape s, const int* __restrict__ block_of_slot,
+                                                      const double* __restrict__ chi, int nslots,
+                                                      double* __restrict__ nrm) {
+  const int slot = blockIdx.x, t = threadIdx.x;
+  const int b = block_of_slot[slot];
+  __shared__ double lab[10][10][10];
+  __shared__ double ch[8][8][8];
+  const double h = h_[b];
+  const double ox = origin[3 * b], oy = origin[3 * b + 1], oz = origin[3 * b + 2];
+  for (int i = t; i < 1000; i += BN) {
+    const int x = i % 10 - 1, y = (i / 10) % 10 - 1, z = i / 100 - 1;
+    lab[z + 1][y + 1][x + 1] = shape_sdf(s, ox + (x + 0.5) * h, oy + (y + 0.5) * h, oz + (z + 0.5) * h);
+  }
+  const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
+  ch[z][y][x] = chi[size_t(slot) * BN + t];
+  __syncthreads();
+  const double inv2h = 0.5 / h, fac1 = 0.5 * h * h;
+  const double dPx = lab[z + 1][y + 1][x + 2], dMx = lab[z + 1][y + 1][x];
+  const double dPy = lab[z + 1][y + 2][x + 1], dMy = lab[z + 1][y][x + 1];
+  const double dPz = lab[z + 2][y + 1][x + 1], dMz = lab[z][y + 1][x + 1];
+  const double gUX = inv2h * (dPx - dMx), gUY = inv2h * (dPy - dMy), gUZ = inv2h * (dPz - dMz);
+  const double gUSq = gUX * gUX + gUY * gUY + gUZ * gUZ + kEpsD;
+  // d/dx of chi along each axis: one-sided at the block's first and last cells
+  auto grad = [&](int i, double m2, double m1, double c0, double p1, double p2) {
+    return i == 0 ? 2.0 * (-0.5 * p2 + 2.0 * p1 - 1.5 * c0)
+                  : (i == 7 ? 2.0 * (1.5 * c0 - 2.0 * m1 + 0.5 * m2) : (p1 - m1));
+  };
+  const double c0 = ch[z][y][x];
+  const double gHX = grad(x, x > 1 ? ch[z][y][x - 2] : 0.0, x > 0 ? ch[z][y][x - 1] : 0.0, c0,
+                          x < 7 ? ch[z][y][x + 1] : 0.0, x < 6 ? ch[z][y][x + 2] : 0.0);
+  const double gHY = grad(y, y > 1 ? ch[z][y - 2][x] : 0.0, y > 0 ? ch[z][y - 1][x] : 0.0, c0,
+                          y < 7 ? ch[z][y + 1][x] : 0.0, y < 6 ? ch[z][y + 2][x] : 0.0);
+  const double gHZ = grad(z, z > 1 ? ch[z - 2][y][x] : 0.0, z > 0 ? ch[z - 1][y][x] : 0.0, c0,
+                          z < 7 ? ch[z + 1][y][x] : 0.0, z < 6 ? ch[z + 2][y][x] : 0.0);
+  double n3[3] = {0.0, 0.0, 0.0};
+  if (!(gHX * gHX + gHY * gHY + gHZ * gHZ < 1e-12)) {
+    const double numD = gHX * gUX + gHY * gUY + gHZ * gUZ;
+    const double delta = fac1 * numD / gUSq;
+    if (delta > kEpsD) {
+      n3[0] = -delta * gUX;
+      n3[1] = -delta * gUY;
+      n3[2] = -delta * gUZ;
+    }
+  }
+  for (int d = 0; d < 3; ++d) nrm[(size_t(d) * nslots + slot) * BN + t] = n3[d];
+}
+
+// Quantities summed over the surface points (Obstacle::computeForces order):
+// surface force (3), pressure force (3), viscous force (3), torque (3), drag,
+// thrust, Pout, PoutBnd, defPower, defPowerBnd, pLocom.
+constexpr int kForceQ = 19;
+constexpr int kFL = 16;  // force lab cells per side: -4 .. 11 around the block
+
+struct ForceArgs {
+  DevMesh M;
+  const double* vel;  // [3][n]
+  size_t n;
+  const double* pres;
+  const double* chi;  // grid chi
+  const double* origin;
+  const int* block_of_slot;
+  const double* nrm;   // [3][nslots][512]
+  const double* udef;  // [3][nslots][512]
+  int nslots;
+  double nu;
+  double cm[3], utrans[3], omega[3];
+  double* qslot;  // nslots * kForceQ
+  int* err;       // set when a surface point's stencil leaves the same-level neighbourhood
+};
+
+// KernelComputeForces::visit for one slot (one CTA, one thread per cell): the
+// velocity and chi labs over -4..11 from the block and its 26 neighbours at
+// the same level (through face neighbours x, then y, then z; cells of a
+// neighbour that is missing, coarser, finer or beyond a domain boundary are
+// NaN, and a surface point whose stencil reads one sets *err and adds
+// nothing), then the one-sided velocity gradients at the point moved along
+// the normal into the fluid, the pressure and viscous tractions and the sums.
+__global__ void __launch_bounds__(BN, 1) k_obst_forces(ForceArgs A) {
+  extern __shared__ double fl[];  // [4][kFL^3]: u, v, w, chi
+  __shared__ int nbr[27];
+  __shared__ double red[BN / 32][kForceQ];
+  const int slot = blockIdx.x, t = threadIdx.x;
+  const int b = A.block_of_slot[slot];
+  const DevMesh& M = A.M;
+  if (t < 27) {
+    const int off[3] = {t % 3 - 1, (t / 3) % 3 - 1, t / 9 - 1};
+    int cur = b;
+    for (int d = 0; d < 3 && cur >= 0; ++d) {
+      if (off[d] == 0) continue;
+      const int f = 2 * d + (off[d] > 0 ? 1 : 0);
+      cur = M.fkind[6 * cur + f] == K_SAME ? M.fnbr[24 * cur + 4 * f] : -1;
+    }
+    nbr[t] = cur;
+  }
+  __syncthreads();
+  constexpr int V = kFL * kFL * kFL;
+  for (int i = t; i < V; i += BN) {
+    const int x = i % kFL - 4, y = (i / kFL) % kFL - 4, z = i / (kFL * kFL) - 4;
+    const int ox = x < 0 ? -1 : (x >= 8 ? 1 : 0), oy = y < 0 ? -1 : (y >= 8 ? 1 : 0),
+              oz = z < 0 ? -1 : (z >= 8 ? 1 : 0);
+    const int nb = nbr[(ox + 1) + 3 * (oy + 1) + 9 * (oz + 1)];
+    const int cell = (x - 8 * ox) + 8 * (y - 8 * oy) + 64 * (z - 8 * oz);
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    for (int c = 0; c < 3; ++c) fl[c * V + i] = nb < 0 ? nan : A.vel[c * A.n + size_t(nb) * BN + cell];
+    fl[3 * V + i] = nb < 0 ? nan : A.chi[size_t(nb) * BN + cell];
+  }
+  __syncthreads();
+  auto at = [&](int c, int x, int y, int z) { return fl[c * V + (x + 4) + kFL * ((y + 4) + kFL * (z + 4))]; };
+  auto inrange = [](int i) { return i >= -4 && i < 12; };
+  double q[kForceQ];
+  for (int k = 0; k < kForceQ; ++k) q[k] = 0.0;
+  const int ix = t & 7, iy = (t >> 3) & 7, iz = t >> 6;
+  const double normX = A.nrm[(0 * size_t(A.nslots) + slot) * BN + t];
+  const double normY = A.nrm[(1 * size_t(A.nslots) + slot) * BN + t];
+  const double normZ = A.nrm[(2 * size_t(A.nslots) + slot) * BN + t];
+  if (normX != 0.0 || normY != 0.0 || normZ != 0.0) {
+    const double h = M.h[b], _1oH = A.nu / h;
+    const double p[3] = {A.origin[3 * b] + h * (ix + 0.5), A.origin[3 * b + 1] + h * (iy + 0.5),
+                         A.origin[3 * b + 2] + h * (iz + 0.5)};
+    const double norm = 1.0 / sqrt(normX * normX + normY * normY + normZ * normZ);
+    const double dx = normX * norm, dy = normY * norm, dz = normZ * norm;
+    // move up to four cells along the normal, out of the body
+    int x = ix, y = iy, z = iz;
+    for (int kk = 0; kk < 5; ++kk) {
+      const int dxi = int(round(kk * dx)), dyi = int(round(kk * dy)), dzi = int(round(kk * dz));
+      if (ix + dxi + 1 >= 12 || ix + dxi - 1 < -4) continue;
+      if (iy + dyi + 1 >= 12 || iy + dyi - 1 < -4) continue;
+      if (iz + dzi + 1 >= 12 || iz + dzi - 1 < -4) continue;
+      x = ix + dxi;
+      y = iy + dyi;
+      z = iz + dzi;
+      if (at(3, x, y, z) < 0.01) break;
+    }
+    const int sx = normX > 0 ? 1 : -1, sy = normY > 0 ? 1 : -1, sz = normZ > 0 ? 1 : -1;
+    constexpr double c0 = -137. / 60., c1 = 5., c2 = -5., c3 = 10. / 3., c4 = -5. / 4., c5 = 1. / 5.;
+    double g[3][3];  // g[c][d] = d u_c / d x_d at the point (ix, iy, iz)
+    for (int c = 0; c < 3; ++c) {
+      auto l = [&](int X, int Y, int Z) { return at(c, X, Y, Z); };
+      // first derivatives at (x, y, z): sixth-order one-sided, else second, else first order
+      auto d1 = [&](int d) {
+        const int sd = d == 0 ? sx : (d == 1 ? sy : sz);
+        const int e[3] = {d == 0, d == 1, d == 2};
+        const int pd = d == 0 ? x : (d == 1 ? y : z);
+        auto L = [&](int k) { return l(x + k * e[0], y + k * e[1], z + k * e[2]); };
+        if (inrange(pd + 5 * sd))
+          return sd * (c0 * L(0) + c1 * L(sd) + c2 * L(2 * sd) + c3 * L(3 * sd) + c4 * L(4 * sd) + c5 * L(5 * sd));
+        if (inrange(pd + 2 * sd)) return sd * (-1.5 * L(0) + 2.0 * L(sd) - 0.5 * L(2 * sd));
+        // the y branch of the reference multiplies by sx here (FluidSolidForces.cpp:127)
+        return (d == 1 ? sx : sd) * (L(sd) - L(0));
+      };
+      const double dvx = d1(0), dvy = d1(1), dvz = d1(2);
+      const double dxx = l(x - 1, y, z) - 2.0 * l(x, y, z) + l(x + 1, y, z);
+      const double dyy = l(x, y - 1, z) - 2.0 * l(x, y, z) + l(x, y + 1, z);
+      const double dzz = l(x, y, z - 1) - 2.0 * l(x, y, z) + l(x, y, z + 1);
+      double dxy, dyz, dxz;
+      if (inrange(x + 2 * sx) && inrange(y + 2 * sy))
+        dxy = sx * sy *
+              (-0.5 * (-1.5 * l(x + 2 * sx, y, z) + 2 * l(x + 2 * sx, y + sy, z) - 0.5 * l(x + 2 * sx, y + 2 * sy, z)) +
+               2 * (-1.5 * l(x + sx, y, z) + 2 * l(x + sx, y + sy, z) - 0.5 * l(x + sx, y + 2 * sy, z)) -
+               1.5 * (-1.5 * l(x, y, z) + 2 * l(x, y + sy, z) - 0.5 * l(x, y + 2 * sy, z)));
+      else
+        dxy = sx * sy * (l(x + sx, y + sy, z) - l(x + sx, y, z)) - (l(x, y + sy, z) - l(x, y, z));
+      if (inrange(y + 2 * sy) && inrange(z + 2 * sz))
+        dyz = sy * sz *
+              (-0.5 * (-1.5 * l(x, y + 2 * sy, z) + 2 * l(x, y + 2 * sy, z + sz) - 0.5 * l(x, y + 2 * sy, z + 2 * sz)) +
+               2 * (-1.5 * l(x, y + sy, z) + 2 * l(x, y + sy, z + sz) - 0.5 * l(x, y + sy, z + 2 * sz)) -
+               1.5 * (-1.5 * l(x, y, z) + 2 * l(x, y, z + sz) - 0.5 * l(x, y, z + 2 * sz)));
+      else
+        dyz = sy * sz * (l(x, y + sy, z + sz) - l(x, y + sy, z)) - (l(x, y, z + sz) - l(x, y, z));
+      if (inrange(x + 2 * sx) && inrange(z + 2 * sz))
+        dxz = sx * sz *
+              (-0.5 * (-1.5 * l(x, y, z + 2 * sz) + 2 * l(x + sx, y, z + 2 * sz) - 0.5 * l(x + 2 * sx, y, z + 2 * sz)) +
+               2 * (-1.5 * l(x, y, z + sz) + 2 * l(x + sx, y, z + sz) - 0.5 * l(x + 2 * sx, y, z + sz)) -
+               1.5 * (-1.5 * l(x, y, z) + 2 * l(x + sx, y, z) - 0.5 * l(x + 2 * sx, y, z)));
+      else
+        dxz = sx * sz * (l(x + sx, y, z + sz) - l(x, y, z + sz)) - (l(x + sx, y, z) - l(x, y, z));
+      // Taylor back from (x, y, z) to the surface point
+      g[c][0] = dvx + dxx * (ix - x) + dxy * (iy - y) + dxz * (iz - z);
+      g[c][1] = dvy + dyy * (iy - y) + dyz * (iz - z) + dxy * (ix - x);
+      g[c][2] = dvz + dzz * (iz - z) + dxz * (ix - x) + dyz * (iy - y);
+    }
+    const double P = A.pres[size_t(b) * BN + t];
+    const double fXV = _1oH * (g[0][0] * normX + g[0][1] * normY + g[0][2] * normZ);
+    const double fYV = _1oH * (g[1][0] * normX + g[1][1] * normY + g[1][2] * normZ);
+    const double fZV = _1oH * (g[2][0] * normX + g[2][1] * normY + g[2][2] * normZ);
+    const double fXP = -P * normX, fYP = -P * normY, fZP = -P * normZ;
+    const double fXT = fXV + fXP, fYT = fYV + fYP, fZT = fZV + fZP;
+    const double vX = at(0, ix, iy, iz), vY = at(1, ix, iy, iz), vZ = at(2, ix, iy, iz);
+    const size_t ud = size_t(slot) * BN + t, us = size_t(A.nslots) * BN;
+    const double uX = A.udef[ud], uY = A.udef[us + ud], uZ = A.udef[2 * us + ud];
+    double velUnit[3] = {0.0, 0.0, 0.0};
+    const double vn = sqrt(A.utrans[0] * A.utrans[0] + A.utrans[1] * A.utrans[1] + A.utrans[2] * A.utrans[2]);
+    if (vn > 1e-9)
+      for (int d = 0; d < 3; ++d) velUnit[d] = A.utrans[d] / vn;
+    const double forcePar = fXT * velUnit[0] + fYT * velUnit[1] + fZT * velUnit[2];
+    const double powOut = fXT * vX + fYT * vY + fZT * vZ;
+    const double powDef = fXT * uX + fYT * uY + fZT * uZ;
+    const double r[3] = {p[0] - A.cm[0], p[1] - A.cm[1], p[2] - A.cm[2]};
+    const double uS[3] = {A.utrans[0] + A.omega[1] * r[2] - r[1] * A.omega[2],
+                          A.utrans[1] + A.omega[2] * r[0] - r[2] * A.omega[0],
+                          A.utrans[2] + A.omega[0] * r[1] - r[0] * A.omega[1]};
+    const double v[kForceQ] = {fXT, fYT, fZT, fXP, fYP, fZP, fXV, fYV, fZV,
+                               r[1] * fZT - r[2] * fYT, r[2] * fXT - r[0] * fZT, r[0] * fYT - r[1] * fXT,
+                               -.5 * (forcePar - fabs(forcePar)), .5 * (forcePar + fabs(forcePar)), powOut,
+                               fmin(0.0, powOut), powDef, fmin(0.0, powDef),
+                               fXT * uS[0] + fYT * uS[1] + fZT * uS[2]};
+    bool finite = true;
+    for (int k = 0; k < kForceQ; ++k) finite &= isfinite(v[k]);
+    if (finite)
+      for (int k = 0; k < kForceQ; ++k) q[k] = v[k];
+    else
+      atomicExch(A.err, 1);
+  }
+  // CTA sums in a fixed order: warps, then the warps' partials
+  for (int k = 0; k < kForceQ; ++k) {
+    double a = q[k];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if ((t & 31) == 0) red[t >> 5][k] = a;
+  }
+  __syncthreads();
+  if (t < kForceQ) {
+    double a = 0.0;
+    for (int w = 0; w < BN / 32; ++w) a += red[w][t];
+    A.qslot[size_t(slot) * kForceQ + t] = a;
+  }
+}
+
 }  // namespace
 
 void body_record(cup_ctx* c, int kind, bool on_device, const double* ctr, const double* r, const double* q,
@@ -636,6 +873,93 @@ int ctx_obstacle_host_copies(cup_ctx* c) {
   return 0;
 }
 
+
+// The body's shape for the signed distance (sphere or ellipsoid).
+static int body_shape(const cup_ctx* c, Shape& s) {
+  const BodyState& B = c->body;
+  if (B.kind < 0) return set_error(CUP_ERR_STATE, "ComputeForces: the obstacle is no sphere or ellipsoid body");
+  s = Shape{};
+  s.kind = B.kind;
+  for (int d = 0; d < 3; ++d) s.c[d] = B.pos[d];
+  if (B.kind == 0) {
+    s.r = B.r;
+  } else {
+    quat_lab_to_body(B.quat, s.L);
+    for (int d = 0; d < 3; ++d) s.ax[d] = B.ax[d];
+  }
+  return 0;
+}
+
+// ComputeForces::operator() (FluidSolidForces.cpp:213-229) and the sums and
+// derived quantities of Obstacle::computeForces (Obstacle.cpp:271-300):
+// out[0..18] the kForceQ sums, out[19..22] Pthrust, Pdrag, EffPDef, EffPDefBnd.
+int compute_forces(cup_ctx* c, double out[23]) {
+  DevObstacle& o = c->ob;
+  for (int k = 0; k < 23; ++k) out[k] = 0.0;
+  if (o.nslots == 0) return 0;
+  Shape s{};
+  if (int rc = body_shape(c, s)) return rc;
+  const int ns = o.nslots, nb = c->mesh.nb;
+  cudaStream_t st = c->stream;
+  DevArena tmp;
+  double *origin = nullptr, *nrm = nullptr, *qslot = nullptr;
+  int* err = nullptr;
+  if (int rc = tmp.alloc(&origin, 3 * size_t(nb))) return rc;
+  if (int rc = tmp.alloc(&nrm, 3 * size_t(ns) * BN)) return rc;
+  if (int rc = tmp.alloc(&qslot, size_t(ns) * kForceQ)) return rc;
+  if (int rc = tmp.alloc(&err, 1)) return rc;
+  CUP_CUDA_TRY(stream_h2d(st, origin, c->mesh.origin.data(), 3 * size_t(nb) * sizeof(double)));
+  CUP_CUDA_TRY(stream_zero(st, err, sizeof(int)));
+  {
+    ProfScope ps("obstacle_surface", st);
+    k_obst_surface<<<ns, BN, 0, st>>>(c->dm.h, origin, s, o.block_of_slot, o.chi, ns, nrm);
+  }
+  ForceArgs A{};
+  A.M = c->dm;
+  A.vel = c->F.vel[c->F.vcur];
+  A.n = nbn(c);
+  A.pres = c->F.pres[c->F.pcur];
+  A.chi = c->F.chi;
+  A.origin = origin;
+  A.block_of_slot = o.block_of_slot;
+  A.nrm = nrm;
+  A.udef = o.udef;
+  A.nslots = ns;
+  A.nu = c->cfg.nu;
+  for (int d = 0; d < 3; ++d) {
+    A.cm[d] = o.kin[d];
+    A.utrans[d] = o.kin[3 + d];
+    A.omega[d] = o.kin[6 + d];
+  }
+  A.qslot = qslot;
+  A.err = err;
+  const size_t smem = 4 * size_t(kFL) * kFL * kFL * sizeof(double);
+  static unsigned long long attr = 0;
+  if (first_on_device(attr))
+    CUP_CUDA_TRY(cudaFuncSetAttribute(k_obst_forces, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  {
+    ProfScope ps("obstacle_forces", st);
+    k_obst_forces<<<ns, BN, smem, st>>>(A);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  std::vector<double> q(size_t(ns) * kForceQ);
+  int h_err = 0;
+  CUP_CUDA_TRY(stream_d2h(st, q.data(), qslot, q.size() * sizeof(double)));
+  CUP_CUDA_TRY(stream_d2h(st, &h_err, err, sizeof(int)));
+  if (h_err)
+    return set_error(CUP_ERR_MESH, "ComputeForces: a surface point's stencil reaches a block that is not a same-level "
+                                   "neighbour of the obstacle block (coarse-fine or domain boundary within 4 cells)");
+  for (int sl = 0; sl < ns; ++sl)  // slots in block order, as the reference's sum over blocks
+    for (int k = 0; k < kForceQ; ++k) out[k] += q[size_t(sl) * kForceQ + k];
+  const double eps = kEpsD;
+  const double vn = std::sqrt(o.kin[3] * o.kin[3] + o.kin[4] * o.kin[4] + o.kin[5] * o.kin[5]);
+  const double drag = out[12], thrust = out[13], defPower = out[16], defPowerBnd = out[17];
+  out[19] = thrust * vn;
+  out[20] = drag * vn;
+  out[21] = out[19] / (out[19] - std::min(defPower, 0.0) + eps);
+  out[22] = out[19] / (out[19] - defPowerBnd + eps);
+  return 0;
+}
 }  // namespace cup3d
 
 using namespace cup3d;
@@ -721,6 +1045,14 @@ int cup_obstacle_ellipsoid_dev(cup_ctx* c, const double* ctr, const double* ax, 
   set_kinematics(s, vel, omega);
   if (int rc = create_obstacle_dev(c, s)) return ctx_fail(c, rc, "cup_obstacle_ellipsoid_dev failed");
   body_record(c, 1, true, ctr, ax, q, vel, omega);
+  return 0;
+}
+
+int cup_compute_forces(cup_ctx* c, double* out) {
+  ProfBind pb_(c);
+  if (!c || !out || c->mesh.nb == 0 || c->host_only) return ctx_fail(c, CUP_ERR_ARG, "cup_compute_forces: bad arguments");
+  if (c->ncase > 1) return ctx_fail(c, CUP_ERR_STATE, "cup_compute_forces: not available on a batch of cases");
+  if (int rc = compute_forces(c, out)) return ctx_fail(c, rc, cup_last_error(nullptr));
   return 0;
 }
 

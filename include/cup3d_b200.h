@@ -329,6 +329,17 @@ int cup_set_poisson(cup_ctx* ctx, int32_t solver, double tol_abs, double tol_rel
  * the next solve starts afresh (the solution buffer holds partial results). */
 int cup_set_barrier_limit(cup_ctx* ctx, int64_t cycles);
 
+/* ComputeForces::operator() (FluidSolidForces.cpp:213-229, run by Simulation::advance after
+ * the projection, Simulation.cpp:214-215) with the sums and derived quantities of
+ * Obstacle::computeForces (Obstacle.cpp:271-300), for the context's sphere or ellipsoid body
+ * on the current velocity and pressure.  out[23]: surfForce[3], presForce[3], viscForce[3],
+ * surfTorque[3], drag, thrust, Pout, PoutBnd, defPower, defPowerBnd, pLocom, Pthrust, Pdrag,
+ * EffPDef, EffPDefBnd (all zero without a body).  The velocity stencil of a surface point
+ * reaches up to 4 cells beyond its block; these cells are read at the block's own level, so
+ * a point whose stencil reaches a coarser or finer block, or beyond a non-periodic domain
+ * boundary, returns CUP_ERR_MESH (bodies inside a region of uniform refinement satisfy it). */
+int cup_compute_forces(cup_ctx* ctx, double* out);
+
 /* ---- learned preconditioner (no counterpart in the reference: the new slot at
  * the preconditioner call sites PoissonSolverAMR.h:183-222, BiCGSTAB.cu:526-527).
  * z = P A_c^-1 P^T r + BJ(r) + (s/h) CNN(r_lab / s): the coarse correction, the exact

@@ -40,6 +40,8 @@ struct SimulationData {
   bool adapt = true;                   // adaptMesh on the reference's cadence in Simulation::advance
   bool meshChanged = false;            // set when an adaptation changed the mesh
   std::array<Real, 20> diagnostics{};  // its last values (the columns of diagnostics.dat)
+  bool computeForces = true;           // ComputeForces after the projection, as the reference does
+  std::array<Real, 23> forces{};       // its last values (cup_compute_forces' order)
 
   explicit SimulationData(const std::string& flags) {
     cup_config_default(&cfg);
@@ -160,6 +162,18 @@ class ComputeDissipation : public Operator {
   std::string getName() override { return "ComputeDissipation"; }
 };
 
+// ComputeForces (FluidSolidForces.cpp:213-229): the body's surface forces
+// after the projection (Simulation.cpp:214-215).
+class ComputeForces : public Operator {
+ public:
+  using Operator::Operator;
+  void operator()(Real) override {
+    if (!sim.computeForces || !sim.has_obstacle) return;
+    check(cup_compute_forces(sim.ctx, sim.forces.data()), sim.ctx);
+  }
+  std::string getName() override { return "ComputeForces"; }
+};
+
 // The time-step driver restricted to the hot path (Simulation.cpp:300-412),
 // with the reference's operator order (Simulation.cpp:186-215); mesh
 // adaptation stays with the caller.
@@ -174,6 +188,7 @@ class Simulation {
     pipeline.push_back(std::make_shared<UpdateObstacles>(sim));
     pipeline.push_back(std::make_shared<Penalization>(sim));
     pipeline.push_back(std::make_shared<PressureProjection>(sim));
+    pipeline.push_back(std::make_shared<ComputeForces>(sim));
     pipeline.push_back(std::make_shared<ComputeDissipation>(sim));
   }
   Real calcMaxTimestep() {

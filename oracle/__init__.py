@@ -51,6 +51,8 @@ SIG = {
     "orc_grad_update": (None, [C.c_void_p, _D, _D, C.c_double]),
     "orc_dissipation": (None, [C.c_void_p, _D, _D, _D, C.c_double, _D]),
     "orc_create_obstacle": (C.c_int, [C.c_void_p, C.c_int, _D, _D, _D, _I, _I, _D, _D, _D]),
+    "orc_obstacle_surface": (None, [C.c_void_p, C.c_int, _D, _D, _D, C.c_int, _I, _D, _D]),
+    "orc_compute_forces": (C.c_int, [C.c_void_p, _D, _D, _D, C.c_int, _I, _D, _D, C.c_double, _D, _D]),
     "orc_adapt_indicator": (None, [C.c_void_p, _D, _D, C.c_int, C.c_int, C.c_double, C.c_double, _D]),
     "orc_adapt_leaves": (C.c_int, [C.c_void_p, _D, C.c_double, C.c_double, _I, C.c_int]),
     "orc_adapt_transfer": (None, [C.c_void_p, C.c_void_p, _D, C.c_int, C.c_int, _D]),
@@ -251,6 +253,33 @@ class Mesh:
                                        _i(bos), _d(chi_o), _d(chi), _d(mom))
         return dict(slot=slot, block_of_slot=bos[:ns].copy(), chi_o=chi_o[:ns * 512].copy(), chi=chi,
                     mass=mom[3], com=mom[:3] / mom[3] if mom[3] > 0 else np.zeros(3))
+
+    def obstacle_surface(self, kind, centre, shape, block_of_slot, chi_o, quat=(1.0, 0.0, 0.0, 0.0)):
+        """Surface points of the obstacle blocks: normals [3][ns][512] (zero off
+        the surface), as ObstacleBlock::write records them (see oracle.cpp)."""
+        bos = np.ascontiguousarray(block_of_slot, np.int32)
+        ns = len(bos)
+        nrm = np.zeros(3 * ns * 512)
+        lib().orc_obstacle_surface(self._p, 0 if kind == "sphere" else 1,
+                                   _d(np.ascontiguousarray(centre, np.float64)),
+                                   _d(np.ascontiguousarray(np.atleast_1d(shape), np.float64)),
+                                   _d(np.ascontiguousarray(quat, np.float64)), ns, _i(bos),
+                                   _d(np.ascontiguousarray(chi_o, np.float64)), _d(nrm))
+        return nrm
+
+    def compute_forces(self, vel, pres, chi, block_of_slot, nrm, udef, nu, kin):
+        """ComputeForces' 19 sums (surface, pressure and viscous force, torque,
+        drag, thrust, Pout, PoutBnd, defPower, defPowerBnd, pLocom) and the
+        number of surface points whose stencil left the same-level cells."""
+        bos = np.ascontiguousarray(block_of_slot, np.int32)
+        q = np.zeros(19)
+        bad = lib().orc_compute_forces(self._p, _d(np.ascontiguousarray(vel, np.float64)),
+                                       _d(np.ascontiguousarray(pres, np.float64)),
+                                       _d(np.ascontiguousarray(chi, np.float64)), len(bos), _i(bos),
+                                       _d(np.ascontiguousarray(nrm, np.float64)),
+                                       _d(np.ascontiguousarray(udef, np.float64)), float(nu),
+                                       _d(np.ascontiguousarray(kin, np.float64)), _d(q))
+        return q, bad
 
     def adapt_indicator(self, vel, chi, level_max, level_max_vort, rtol, ctol):
         """Per-block refinement indicator of Simulation::adaptMesh (see oracle.cpp)."""

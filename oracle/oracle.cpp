@@ -1824,9 +1824,10 @@ struct Body {
 
 }  // namespace obst_orc
 
-extern "C" int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, const double* shape,
-                                   const double* q, int32_t* obst_slot, int32_t* block_of_slot, double* chi_o,
-                                   double* chi_grid, double* mom) {
+// The body of orc_create_obstacle's arguments (fill box with the reference's
+// safety margin of 3 finest cells; rotation from the quaternion).
+static obst_orc::Body orc_make_body(const orc_mesh* m, int kind, const double* centre, const double* shape,
+                                    const double* q) {
   using namespace obst_orc;
   Body B{};
   B.kind = kind;
@@ -1852,6 +1853,14 @@ extern "C" int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, 
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) B.R[i][j] = R[i][j];
   }
+  return B;
+}
+
+extern "C" int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, const double* shape,
+                                   const double* q, int32_t* obst_slot, int32_t* block_of_slot, double* chi_o,
+                                   double* chi_grid, double* mom) {
+  using namespace obst_orc;
+  const Body B = orc_make_body(m, kind, centre, shape, q);
   const int nb = m->nb;
   std::fill(chi_grid, chi_grid + size_t(nb) * BN, 0.0);
   int ns = 0;
@@ -1915,6 +1924,209 @@ extern "C" int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, 
     if (obst_slot[b] >= 0)
       for (int k = 0; k < 4; ++k) mom[k] += bm[4 * size_t(b) + k];
   return ns;
+}
+
+// ============================================================================
+// Surface forces (ComputeForces, FluidSolidForces.cpp:14-229).  Surface
+// points of each obstacle block (the second loop of
+// KernelCharacteristicFunction, ObstaclesCreate.cpp:83-117, and
+// ObstacleBlock::write): nrm[3][ns][512] = -Delta grad(sdf) where the block's
+// chi gradient is not zero and Delta > epsilon, else 0.
+// ============================================================================
+extern "C" void orc_obstacle_surface(orc_mesh* m, int kind, const double* centre, const double* shape,
+                                     const double* q, int ns, const int32_t* block_of_slot, const double* chi_o,
+                                     double* nrm) {
+  using namespace obst_orc;
+  const Body B = orc_make_body(m, kind, centre, shape, q);
+  for (int sl = 0; sl < ns; ++sl) {
+    const int b = block_of_slot[sl];
+    const double hb = m->h[b];
+    double org[3];
+    for (int d = 0; d < 3; ++d) org[d] = m->idx[b][d] * 8 * hb;
+    double lab[BS + 2][BS + 2][BS + 2];
+    for (int iz = -1; iz < BS + 1; ++iz)
+      for (int iy = -1; iy < BS + 1; ++iy)
+        for (int ix = -1; ix < BS + 1; ++ix)
+          lab[iz + 1][iy + 1][ix + 1] =
+              B.sdf(org[0] + hb * (ix + 0.5), org[1] + hb * (iy + 0.5), org[2] + hb * (iz + 0.5));
+    const double* CHI = chi_o + size_t(sl) * BN;
+    auto C = [&](int x, int y, int z) { return CHI[x + BS * y + BS * BS * z]; };
+    const double inv2h = .5 / hb, fac1 = .5 * hb * hb;
+    for (int z = 0; z < BS; ++z)
+      for (int y = 0; y < BS; ++y)
+        for (int x = 0; x < BS; ++x) {
+          const double gradUX = inv2h * (lab[z + 1][y + 1][x + 2] - lab[z + 1][y + 1][x]);
+          const double gradUY = inv2h * (lab[z + 1][y + 2][x + 1] - lab[z + 1][y][x + 1]);
+          const double gradUZ = inv2h * (lab[z + 2][y + 1][x + 1] - lab[z][y + 1][x + 1]);
+          const double gradUSq = gradUX * gradUX + gradUY * gradUY + gradUZ * gradUZ + EPS;
+          const double gradHX = x == 0 ? 2.0 * (-0.5 * C(x + 2, y, z) + 2.0 * C(x + 1, y, z) - 1.5 * C(x, y, z))
+                                : (x == BS - 1 ? 2.0 * (1.5 * C(x, y, z) - 2.0 * C(x - 1, y, z) + 0.5 * C(x - 2, y, z))
+                                               : (C(x + 1, y, z) - C(x - 1, y, z)));
+          const double gradHY = y == 0 ? 2.0 * (-0.5 * C(x, y + 2, z) + 2.0 * C(x, y + 1, z) - 1.5 * C(x, y, z))
+                                : (y == BS - 1 ? 2.0 * (1.5 * C(x, y, z) - 2.0 * C(x, y - 1, z) + 0.5 * C(x, y - 2, z))
+                                               : (C(x, y + 1, z) - C(x, y - 1, z)));
+          const double gradHZ = z == 0 ? 2.0 * (-0.5 * C(x, y, z + 2) + 2.0 * C(x, y, z + 1) - 1.5 * C(x, y, z))
+                                : (z == BS - 1 ? 2.0 * (1.5 * C(x, y, z) - 2.0 * C(x, y, z - 1) + 0.5 * C(x, y, z - 2))
+                                               : (C(x, y, z + 1) - C(x, y, z - 1)));
+          const int c = x + BS * y + BS * BS * z;
+          double n3[3] = {0, 0, 0};
+          if (!(gradHX * gradHX + gradHY * gradHY + gradHZ * gradHZ < 1e-12)) {
+            const double numD = gradHX * gradUX + gradHY * gradUY + gradHZ * gradUZ;
+            const double Delta = fac1 * numD / gradUSq;
+            if (Delta > EPS) {
+              n3[0] = -Delta * gradUX;
+              n3[1] = -Delta * gradUY;
+              n3[2] = -Delta * gradUZ;
+            }
+          }
+          for (int d = 0; d < 3; ++d) nrm[(size_t(d) * ns + sl) * BN + c] = n3[d];
+        }
+  }
+}
+
+// KernelComputeForces::visit over the slots (vel [3][n], udef [3][ns][512],
+// kin = centre of mass, translation and angular velocity); the lab is read
+// at the block's own level (periodic wrap; cells of no block at that level
+// are NaN).  qoi[19]: surface force, pressure force, viscous force, torque
+// (3 each), drag, thrust, Pout, PoutBnd, defPower, defPowerBnd, pLocom.
+// Returns the surface points whose result is not finite.
+extern "C" int orc_compute_forces(orc_mesh* m, const double* vel, const double* pres, const double* chi_grid, int ns,
+                                  const int32_t* block_of_slot, const double* nrm, const double* udef, double nu,
+                                  const double* kin, double* qoi) {
+  const size_t n = size_t(m->nb) * BN;
+  const double* CM = kin;
+  const double* uT = kin + 3;
+  const double* om = kin + 6;
+  double velUnit[3] = {0, 0, 0};
+  const double vn = std::sqrt(uT[0] * uT[0] + uT[1] * uT[1] + uT[2] * uT[2]);
+  if (vn > 1e-9)
+    for (int d = 0; d < 3; ++d) velUnit[d] = uT[d] / vn;
+  for (int k = 0; k < 19; ++k) qoi[k] = 0.0;
+  int bad = 0;
+  const double c0 = -137. / 60., c1 = 5., c2 = -5., c3 = 10. / 3., c4 = -5. / 4., c5 = 1. / 5.;
+  auto inrange = [](int i) { return i >= -4 && i < BS + 4; };
+  for (int sl = 0; sl < ns; ++sl) {
+    const int b = block_of_slot[sl], L = m->level[b];
+    const double h = m->h[b], _1oH = nu / h;
+    // field value at cell (x, y, z) of the block's frame, at its level
+    auto val = [&](const double* f, int x, int y, int z) {
+      int g[3] = {m->idx[b][0] * BS + x, m->idx[b][1] * BS + y, m->idx[b][2] * BS + z};
+      int bi[3];
+      for (int d = 0; d < 3; ++d) {
+        const int N = (m->bpd[d] << L) * BS;
+        if (g[d] < 0 || g[d] >= N) {
+          if (m->bc[d] != BC_PERIODIC) return std::numeric_limits<double>::quiet_NaN();
+          g[d] = ((g[d] % N) + N) % N;
+        }
+        bi[d] = g[d] / BS;
+      }
+      const int nbk = m->find(L, bi[0], bi[1], bi[2]);
+      if (nbk < 0) return std::numeric_limits<double>::quiet_NaN();
+      return f[size_t(nbk) * BN + (g[0] - bi[0] * BS) + BS * (g[1] - bi[1] * BS) + BS * BS * (g[2] - bi[2] * BS)];
+    };
+    for (int t = 0; t < BN; ++t) {
+      const double normX = nrm[(0 * size_t(ns) + sl) * BN + t], normY = nrm[(1 * size_t(ns) + sl) * BN + t],
+                   normZ = nrm[(2 * size_t(ns) + sl) * BN + t];
+      if (normX == 0.0 && normY == 0.0 && normZ == 0.0) continue;
+      const int ix = t % BS, iy = (t / BS) % BS, iz = t / (BS * BS);
+      const double p[3] = {m->idx[b][0] * 8 * h + h * (ix + 0.5), m->idx[b][1] * 8 * h + h * (iy + 0.5),
+                           m->idx[b][2] * 8 * h + h * (iz + 0.5)};
+      const double norm = 1.0 / std::sqrt(normX * normX + normY * normY + normZ * normZ);
+      const double dx = normX * norm, dy = normY * norm, dz = normZ * norm;
+      int x = ix, y = iy, z = iz;
+      for (int kk = 0; kk < 5; ++kk) {
+        const int dxi = int(std::round(kk * dx)), dyi = int(std::round(kk * dy)), dzi = int(std::round(kk * dz));
+        if (ix + dxi + 1 >= BS + 4 || ix + dxi - 1 < -4) continue;
+        if (iy + dyi + 1 >= BS + 4 || iy + dyi - 1 < -4) continue;
+        if (iz + dzi + 1 >= BS + 4 || iz + dzi - 1 < -4) continue;
+        x = ix + dxi;
+        y = iy + dyi;
+        z = iz + dzi;
+        if (val(chi_grid, x, y, z) < 0.01) break;
+      }
+      const int sx = normX > 0 ? +1 : -1, sy = normY > 0 ? +1 : -1, sz = normZ > 0 ? +1 : -1;
+      double G[3][3];
+      for (int c = 0; c < 3; ++c) {
+        const double* f = vel + c * n;
+        auto l = [&](int X, int Y, int Z) { return val(f, X, Y, Z); };
+        double dveldx, dveldy, dveldz;
+        if (inrange(x + 5 * sx))
+          dveldx = sx * (c0 * l(x, y, z) + c1 * l(x + sx, y, z) + c2 * l(x + 2 * sx, y, z) + c3 * l(x + 3 * sx, y, z) +
+                         c4 * l(x + 4 * sx, y, z) + c5 * l(x + 5 * sx, y, z));
+        else if (inrange(x + 2 * sx))
+          dveldx = sx * (-1.5 * l(x, y, z) + 2.0 * l(x + sx, y, z) - 0.5 * l(x + 2 * sx, y, z));
+        else
+          dveldx = sx * (l(x + sx, y, z) - l(x, y, z));
+        if (inrange(y + 5 * sy))
+          dveldy = sy * (c0 * l(x, y, z) + c1 * l(x, y + sy, z) + c2 * l(x, y + 2 * sy, z) + c3 * l(x, y + 3 * sy, z) +
+                         c4 * l(x, y + 4 * sy, z) + c5 * l(x, y + 5 * sy, z));
+        else if (inrange(y + 2 * sy))
+          dveldy = sy * (-1.5 * l(x, y, z) + 2.0 * l(x, y + sy, z) - 0.5 * l(x, y + 2 * sy, z));
+        else
+          dveldy = sx * (l(x, y + sy, z) - l(x, y, z));
+        if (inrange(z + 5 * sz))
+          dveldz = sz * (c0 * l(x, y, z) + c1 * l(x, y, z + sz) + c2 * l(x, y, z + 2 * sz) + c3 * l(x, y, z + 3 * sz) +
+                         c4 * l(x, y, z + 4 * sz) + c5 * l(x, y, z + 5 * sz));
+        else if (inrange(z + 2 * sz))
+          dveldz = sz * (-1.5 * l(x, y, z) + 2.0 * l(x, y, z + sz) - 0.5 * l(x, y, z + 2 * sz));
+        else
+          dveldz = sz * (l(x, y, z + sz) - l(x, y, z));
+        const double dveldx2 = l(x - 1, y, z) - 2.0 * l(x, y, z) + l(x + 1, y, z);
+        const double dveldy2 = l(x, y - 1, z) - 2.0 * l(x, y, z) + l(x, y + 1, z);
+        const double dveldz2 = l(x, y, z - 1) - 2.0 * l(x, y, z) + l(x, y, z + 1);
+        double dxy, dyz, dxz;
+        if (inrange(x + 2 * sx) && inrange(y + 2 * sy))
+          dxy = sx * sy * (-0.5 * (-1.5 * l(x + 2 * sx, y, z) + 2 * l(x + 2 * sx, y + sy, z) - 0.5 * l(x + 2 * sx, y + 2 * sy, z)) +
+                           2 * (-1.5 * l(x + sx, y, z) + 2 * l(x + sx, y + sy, z) - 0.5 * l(x + sx, y + 2 * sy, z)) -
+                           1.5 * (-1.5 * l(x, y, z) + 2 * l(x, y + sy, z) - 0.5 * l(x, y + 2 * sy, z)));
+        else
+          dxy = sx * sy * (l(x + sx, y + sy, z) - l(x + sx, y, z)) - (l(x, y + sy, z) - l(x, y, z));
+        if (inrange(y + 2 * sy) && inrange(z + 2 * sz))
+          dyz = sy * sz * (-0.5 * (-1.5 * l(x, y + 2 * sy, z) + 2 * l(x, y + 2 * sy, z + sz) - 0.5 * l(x, y + 2 * sy, z + 2 * sz)) +
+                           2 * (-1.5 * l(x, y + sy, z) + 2 * l(x, y + sy, z + sz) - 0.5 * l(x, y + sy, z + 2 * sz)) -
+                           1.5 * (-1.5 * l(x, y, z) + 2 * l(x, y, z + sz) - 0.5 * l(x, y, z + 2 * sz)));
+        else
+          dyz = sy * sz * (l(x, y + sy, z + sz) - l(x, y + sy, z)) - (l(x, y, z + sz) - l(x, y, z));
+        if (inrange(x + 2 * sx) && inrange(z + 2 * sz))
+          dxz = sx * sz * (-0.5 * (-1.5 * l(x, y, z + 2 * sz) + 2 * l(x + sx, y, z + 2 * sz) - 0.5 * l(x + 2 * sx, y, z + 2 * sz)) +
+                           2 * (-1.5 * l(x, y, z + sz) + 2 * l(x + sx, y, z + sz) - 0.5 * l(x + 2 * sx, y, z + sz)) -
+                           1.5 * (-1.5 * l(x, y, z) + 2 * l(x + sx, y, z) - 0.5 * l(x + 2 * sx, y, z)));
+        else
+          dxz = sx * sz * (l(x + sx, y, z + sz) - l(x, y, z + sz)) - (l(x + sx, y, z) - l(x, y, z));
+        G[c][0] = dveldx + dveldx2 * (ix - x) + dxy * (iy - y) + dxz * (iz - z);
+        G[c][1] = dveldy + dveldy2 * (iy - y) + dyz * (iz - z) + dxy * (ix - x);
+        G[c][2] = dveldz + dveldz2 * (iz - z) + dxz * (ix - x) + dyz * (iy - y);
+      }
+      const double P = pres[size_t(b) * BN + t];
+      const double fXV = _1oH * (G[0][0] * normX + G[0][1] * normY + G[0][2] * normZ);
+      const double fYV = _1oH * (G[1][0] * normX + G[1][1] * normY + G[1][2] * normZ);
+      const double fZV = _1oH * (G[2][0] * normX + G[2][1] * normY + G[2][2] * normZ);
+      const double fXP = -P * normX, fYP = -P * normY, fZP = -P * normZ;
+      const double fXT = fXV + fXP, fYT = fYV + fYP, fZT = fZV + fZP;
+      const double vX = vel[0 * n + size_t(b) * BN + t], vY = vel[1 * n + size_t(b) * BN + t],
+                   vZ = vel[2 * n + size_t(b) * BN + t];
+      const size_t us = size_t(ns) * BN, ud = size_t(sl) * BN + t;
+      const double forcePar = fXT * velUnit[0] + fYT * velUnit[1] + fZT * velUnit[2];
+      const double powOut = fXT * vX + fYT * vY + fZT * vZ;
+      const double powDef = fXT * udef[ud] + fYT * udef[us + ud] + fZT * udef[2 * us + ud];
+      const double r[3] = {p[0] - CM[0], p[1] - CM[1], p[2] - CM[2]};
+      const double uS[3] = {uT[0] + om[1] * r[2] - r[1] * om[2], uT[1] + om[2] * r[0] - r[2] * om[0],
+                            uT[2] + om[0] * r[1] - r[0] * om[1]};
+      const double v[19] = {fXT, fYT, fZT, fXP, fYP, fZP, fXV, fYV, fZV,
+                            r[1] * fZT - r[2] * fYT, r[2] * fXT - r[0] * fZT, r[0] * fYT - r[1] * fXT,
+                            -.5 * (forcePar - std::fabs(forcePar)), .5 * (forcePar + std::fabs(forcePar)), powOut,
+                            std::min(0.0, powOut), powDef, std::min(0.0, powDef),
+                            fXT * uS[0] + fYT * uS[1] + fZT * uS[2]};
+      bool finite = true;
+      for (int k = 0; k < 19; ++k) finite = finite && std::isfinite(v[k]);
+      if (!finite) {
+        ++bad;
+        continue;
+      }
+      for (int k = 0; k < 19; ++k) qoi[k] += v[k];
+    }
+  }
+  return bad;
 }
 
 // ============================================================================

@@ -105,6 +105,15 @@ int orc_create_obstacle(orc_mesh* m, int kind, const double* centre, const doubl
                         int32_t* obst_slot, int32_t* block_of_slot, double* chi_o, double* chi_grid,
                         double* mom);
 
+/* surface points of the obstacle blocks (normals [3][ns][512]) and the sums of
+ * ComputeForces (FluidSolidForces.cpp:14-229); returns the points whose result
+ * is not finite */
+void orc_obstacle_surface(orc_mesh* m, int kind, const double* centre, const double* shape, const double* q,
+                          int ns, const int32_t* block_of_slot, const double* chi_o, double* nrm);
+int orc_compute_forces(orc_mesh* m, const double* vel, const double* pres, const double* chi_grid, int ns,
+                       const int32_t* block_of_slot, const double* nrm, const double* udef, double nu,
+                       const double* kin, double* qoi);
+
 /* ---- learned preconditioner network (see oracle.cpp for the layout) ---- */
 int orc_cnn_nparam(int C);
 /* forward (out may be NULL), loss and gradient (target/grad may be NULL) */

@@ -102,5 +102,11 @@ int main() {
   double moved = 0;
   for (size_t i = 0; i < n; ++i) moved = std::max(moved, std::fabs(ca[i] - c0[i]));
   std::printf("moving sphere: 3 steps equal to cup_step, chi changed by %.3f\n", moved);
+  // ComputeForces ran after each projection (the pipeline's own operator)
+  std::printf("moving sphere: surface force %.6e %.6e %.6e, drag %.6e\n", A.sim.forces[0], A.sim.forces[1],
+              A.sim.forces[2], A.sim.forces[12]);
+  for (Real f : A.sim.forces)
+    if (!std::isfinite(f)) return 7;
+  if (A.sim.forces[0] == 0.0) return 8;
   return moved > 0.01 ? 0 : 6;
 }
