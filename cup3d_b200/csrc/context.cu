@@ -293,6 +293,7 @@ int cup_config_parse(cup_config* c, const char* args) {
       else if (v == "b200_learned_mixed") c->poisson_solver = CUP_POISSON_B200_LEARNED_MIXED;
       else if (v == "b200_twolevel") c->poisson_solver = CUP_POISSON_B200_TWOLEVEL;
       else if (v == "b200_schwarz") c->poisson_solver = CUP_POISSON_B200_SCHWARZ;
+      else if (v == "b200_pipelined") c->poisson_solver = CUP_POISSON_B200_PIPELINED;
       else return ctx_fail(nullptr, CUP_ERR_ARG, "Poisson solver: \"" + v + "\" unrecognized!");
     } else if (key == "device") {
       if (need_num()) return CUP_ERR_ARG;
@@ -556,6 +557,21 @@ int cup_block_inverse_dev(cup_ctx* c, const double* in, double* out) {
   return 0;
 }
 
+// The pipelined solver's 16 scratch vectors, allocated on its first use for
+// the current mesh size.
+static int pipelined_vectors(cup_ctx* c, double* vec[16]) {
+  const size_t n = nbn(c);
+  if (c->pipe_cap < n) {
+    c->pipe_arena.release();
+    c->pipe_cap = 0;
+    for (int i = 0; i < 16; ++i)
+      if (int rc = c->pipe_arena.alloc(&c->pipe_vec[i], n)) return rc;
+    c->pipe_cap = n;
+  }
+  for (int i = 0; i < 16; ++i) vec[i] = c->pipe_vec[i];
+  return 0;
+}
+
 // check_true: recompute ||b - A x||_2 in FP64 after the solve (stats.true_rel);
 // the time-step path skips it (-1) since the solvers already test their own
 // FP64 residual.
@@ -596,7 +612,11 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   if (learned) P.stall_window = 40;  // a stall hands over to block-Jacobi below
   const CoarseView cview = c->coarse.view();
   const CoarseView* coarse = twolevel ? &cview : nullptr;
-  if (solver == CUP_POISSON_B200_MIXED || solver == CUP_POISSON_B200_LEARNED_MIXED)
+  if (solver == CUP_POISSON_B200_PIPELINED) {
+    double* vec[16];
+    if (int rc2 = pipelined_vectors(c, vec)) return keep(c, rc2);
+    rc = poisson_pipelined(c->dm, b, x, P, c->W, vec, S, c->stream);
+  } else if (solver == CUP_POISSON_B200_MIXED || solver == CUP_POISSON_B200_LEARNED_MIXED)
     rc = poisson_mixed(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, lmap, coarse, c->num_sms);
   else
     rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, lmap, coarse, c->num_sms);

@@ -200,6 +200,10 @@ struct cup_ctx {
   // incremented whenever the mesh changes (keys what is built per mesh)
   int mesh_version = 0;
   cup3d::CoarseSpace coarse;
+  // scratch vectors of the pipelined solver (allocated on first use)
+  cup3d::DevArena pipe_arena;
+  double* pipe_vec[16] = {nullptr};
+  size_t pipe_cap = 0;
 };
 
 namespace cup3d {

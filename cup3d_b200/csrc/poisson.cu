@@ -2013,4 +2013,494 @@ int true_residual_norm(const DevMesh& M, const double* b, const double* x, int m
   return 0;
 }
 
+
+// ---- pipelined BiCGSTAB (PoissonSolverAMR::solve, PoissonSolverAMR.cpp:13-358) --
+// The reference's CPU solver: preconditioned pipelined BiCGSTAB (Cools and
+// Vanroose) with the exact block inverse, an explicit residual replacement
+// every 50 iterations, restarts on a serious breakdown of (r0, r) and the
+// best iterate kept.  One cooperative launch: every iteration is two phases
+// of the block groups and two grid barriers,
+//   1: t = A what; phat, s, shat, z, q, qhat, y; zhat = M z; (q,y), (y,y)
+//   2: v = A zhat; omega; x, r, rhat, w; what = M w; the six dot products,
+// with the sums sum(v h^3) that the next SpMV's mean-constraint row needs in
+// the same reductions.  Replacement iterations compute s, z, r and w from
+// their definitions (six phases), as the reference does.
+struct PState {
+  double alpha, beta, omega, r0r_prev, norm, init_norm, min_norm, eps, tol_abs, tol_rel;
+  double qy, yy, ms;  // last dots of phase 1, sum(v h^3) of the vector the next SpMV reads
+  int k, restarts, max_restarts, max_iter, converged, done, status, best_pending, use_xopt;
+};
+
+struct PArgs {
+  DevMesh M;
+  const double* b;
+  double* x;
+  double *xopt, *r0, *r, *rhat, *w, *what, *t, *phat, *s, *shat, *z, *zhat, *v, *q, *qhat, *y;
+  PState* st;
+  int mean_mode, zero_mean_row, ncache;
+};
+
+__global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_pbicg_persistent(PArgs A, GridSync Gs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* inv_eig = reinterpret_cast<double*>(smem_raw);
+  BlockInfo* cache = reinterpret_cast<BlockInfo*>(smem_raw + kSmemCache);
+  GroupTile* tiles = reinterpret_cast<GroupTile*>(smem_raw + kSmemTiles);
+  __shared__ double red[64];
+  __shared__ PState S;
+  __shared__ unsigned int epoch;
+  const GroupIdx G;
+  const DevMesh& M = A.M;
+  GroupTile& tile = tiles[G.g];
+  FdTile& ftile = reinterpret_cast<FdTile&>(tile);
+  fd_fill_inverse_eigen(inv_eig, c_lam);
+  for (int i = threadIdx.x; i < PGROUPS * KB_CACHE * 32; i += PNT) {
+    const int e = i >> 5, g = e / KB_CACHE, k = e % KB_CACHE;
+    const int slot = blockIdx.x * PGROUPS + g + k * gridDim.x * PGROUPS;
+    if (k < A.ncache && slot < M.nb) fill_block_info(M, M.order ? M.order[slot] : slot, cache[e], i & 31);
+  }
+  if (threadIdx.x == 0) {
+    S = *A.st;
+    epoch = 0u;
+  }
+  __syncthreads();
+  const double eps = S.eps;
+  // y = A v for the group's column of block bi (ms = sum(v h^3))
+  auto spmv = [&](const BlockInfo& bi, const double* vv, double ms, double out[8]) {
+    double col[8];
+    load_col(vv, bi.id, G, col);
+    spmv_group(bi, VecAt<double>{vv}, col, ms, A.mean_mode, tile, G, out);
+  };
+  auto precond = [&](const BlockInfo& bi, double c[8]) { block_inverse_group(c, ftile, G, bi.h, inv_eig); };
+  auto hsum = [&](const BlockInfo& bi, const double c[8]) {
+    double s = 0.0;
+#pragma unroll
+    for (int zz = 0; zz < 8; ++zz) s += c[zz];
+    return s * bi.h * bi.h * bi.h;
+  };
+  // the best iterate noted by the last reduction is x as it stands: copy it
+  // before x changes again
+  auto copy_best = [&](const BlockInfo& bi) {
+    if (!S.best_pending) return;
+    double c[8];
+    load_col(A.x, bi.id, G, c);
+    store_col(A.xopt, bi.id, G, c);
+  };
+  auto reduce = [&](auto& a) -> bool { return grid_allreduce(a, Gs, epoch, red); };
+  auto sync_state = [&]() { __syncthreads(); };
+  // w = A rhat, what = M w; (r0, r0), (r0, w), sum(what h^3): the scalars of a start or restart
+  auto start_phase = [&]() -> bool {
+    double a[3] = {0.0, 0.0, 0.0};
+    PERSISTENT_BLOCKS(bi) {
+      double w[8], r0[8];
+      spmv(bi, A.rhat, S.ms, w);
+      load_col(A.r0, bi.id, G, r0);
+      store_col(A.w, bi.id, G, w);
+#pragma unroll
+      for (int zz = 0; zz < 8; ++zz) {
+        a[0] += r0[zz] * r0[zz];
+        a[1] += r0[zz] * w[zz];
+      }
+      precond(bi, w);
+      store_col(A.what, bi.id, G, w);
+      a[2] += hsum(bi, w);
+    }
+    if (!reduce(a)) return false;
+    if (threadIdx.x == 0) {
+      S.alpha = a[0] / (a[1] + eps);
+      S.r0r_prev = a[0];
+      S.beta = 0.0;
+      S.omega = 0.0;
+      S.ms = a[2];
+    }
+    sync_state();
+    return true;
+  };
+  bool ok = true;
+  // ---- start: sum(x h^3); r0 = r = b - A x, rhat = M r0; then start_phase
+  {
+    double a[1] = {0.0};
+    PERSISTENT_BLOCKS(bi) {
+      double c[8];
+      load_col(A.x, bi.id, G, c);
+      a[0] += hsum(bi, c);
+    }
+    ok = reduce(a);
+    if (threadIdx.x == 0) S.ms = a[0];
+    sync_state();
+  }
+  if (ok) {
+    double a[1] = {0.0};
+    PERSISTENT_BLOCKS(bi) {
+      double ax[8], bc[8];
+      spmv(bi, A.x, S.ms, ax);
+      load_col(A.b, bi.id, G, bc);
+      if (A.zero_mean_row && bi.mean && G.lane == 0) bc[0] = 0.0;
+#pragma unroll
+      for (int zz = 0; zz < 8; ++zz) bc[zz] -= ax[zz];
+      store_col(A.r0, bi.id, G, bc);
+      store_col(A.r, bi.id, G, bc);
+      precond(bi, bc);
+      store_col(A.rhat, bi.id, G, bc);
+      a[0] += hsum(bi, bc);
+    }
+    ok = reduce(a);
+    if (threadIdx.x == 0) S.ms = a[0];
+    sync_state();
+  }
+  if (ok) {
+    double a[1] = {0.0};  // (r0, r0) again for the initial norm
+    ok = start_phase();
+    if (ok && threadIdx.x == 0) {
+      S.norm = S.init_norm = sqrt(S.r0r_prev);
+      S.min_norm = 1e50;
+      if (!(S.norm == S.norm)) {
+        S.done = 1;
+        S.status = SOLVE_NAN;
+      }
+    }
+    (void)a;
+    sync_state();
+  }
+  // ---- iterations
+  while (ok && !S.done && S.k < S.max_iter) {
+    const bool replace = S.k % 50 == 0;
+    const double al = S.alpha, be = S.beta, om = S.omega;
+    if (!replace) {
+      // phase 1
+      double a[3] = {0.0, 0.0, 0.0};
+      PERSISTENT_BLOCKS(bi) {
+        copy_best(bi);
+        double t[8], z[8];
+        spmv(bi, A.what, S.ms, t);
+        const size_t o0 = size_t(bi.id) * BN + G.gy * 8 + G.gx;
+#pragma unroll
+        for (int zz = 0; zz < 8; ++zz) {
+          const size_t o = o0 + zz * 64;
+          const double rh = A.rhat[o], sho = A.shat[o], w = A.w[o];
+          const double ph = rh + be * (A.phat[o] - om * sho);
+          const double sv = w + be * (A.s[o] - om * A.z[o]);
+          const double sh = A.what[o] + be * (sho - om * A.zhat[o]);
+          const double zn = t[zz] + be * (A.z[o] - om * A.v[o]);
+          const double q = A.r[o] - al * sv, qh = rh - al * sh, y = w - al * zn;
+          A.t[o] = t[zz];
+          A.phat[o] = ph;
+          A.s[o] = sv;
+          A.shat[o] = sh;
+          A.z[o] = zn;
+          A.q[o] = q;
+          A.qhat[o] = qh;
+          A.y[o] = y;
+          z[zz] = zn;
+          a[0] += q * y;
+          a[1] += y * y;
+        }
+        precond(bi, z);
+        store_col(A.zhat, bi.id, G, z);
+        a[2] += hsum(bi, z);
+      }
+      if (!(ok = reduce(a))) break;
+      if (threadIdx.x == 0) {
+        S.qy = a[0];
+        S.yy = a[1];
+        S.ms = a[2];
+        S.best_pending = 0;
+      }
+      sync_state();
+      // phase 2
+      const double omn = S.qy / (S.yy + eps);
+      double d[7] = {0, 0, 0, 0, 0, 0, 0};
+      PERSISTENT_BLOCKS(bi) {
+        double v[8], w[8];
+        spmv(bi, A.zhat, S.ms, v);
+        const size_t o0 = size_t(bi.id) * BN + G.gy * 8 + G.gx;
+#pragma unroll
+        for (int zz = 0; zz < 8; ++zz) {
+          const size_t o = o0 + zz * 64;
+          const double qh = A.qhat[o], y = A.y[o], r0 = A.r0[o];
+          const double x = A.x[o] + al * A.phat[o] + omn * qh;
+          const double r = A.q[o] - omn * y;
+          const double rh = qh - omn * (A.what[o] - al * A.zhat[o]);
+          const double wn = y - omn * (A.t[o] - al * v[zz]);
+          A.v[o] = v[zz];
+          A.x[o] = x;
+          A.r[o] = r;
+          A.rhat[o] = rh;
+          A.w[o] = wn;
+          w[zz] = wn;
+          d[0] += r0 * r;
+          d[1] += r0 * wn;
+          d[2] += r0 * A.s[o];
+          d[3] += r0 * A.z[o];
+          d[4] += r * r;
+          d[5] += r0 * r0;
+        }
+        precond(bi, w);
+        store_col(A.what, bi.id, G, w);
+        d[6] += hsum(bi, w);
+      }
+      if (!(ok = reduce(d))) break;
+      if (threadIdx.x == 0) {
+        S.omega = omn;
+        S.ms = d[6];
+        for (int i = 0; i < 6; ++i) red[32 + i] = d[i];
+      }
+      sync_state();
+    } else {
+      // replacement iteration: phat; s = A phat, shat = M s; z = A shat, ...
+      double a[1] = {0.0};
+      PERSISTENT_BLOCKS(bi) {
+        copy_best(bi);
+        double ph[8], rh[8], sh[8];
+        load_col(A.phat, bi.id, G, ph);
+        load_col(A.rhat, bi.id, G, rh);
+        load_col(A.shat, bi.id, G, sh);
+#pragma unroll
+        for (int zz = 0; zz < 8; ++zz) ph[zz] = rh[zz] + be * (ph[zz] - om * sh[zz]);
+        store_col(A.phat, bi.id, G, ph);
+        a[0] += hsum(bi, ph);
+      }
+      if (!(ok = reduce(a))) break;
+      if (threadIdx.x == 0) {
+        S.ms = a[0];
+        S.best_pending = 0;
+      }
+      sync_state();
+      a[0] = 0.0;
+      PERSISTENT_BLOCKS(bi) {
+        double s[8];
+        spmv(bi, A.phat, S.ms, s);
+        store_col(A.s, bi.id, G, s);
+        precond(bi, s);
+        store_col(A.shat, bi.id, G, s);
+        a[0] += hsum(bi, s);
+      }
+      if (!(ok = reduce(a))) break;
+      if (threadIdx.x == 0) S.ms = a[0];
+      sync_state();
+      double b3[3] = {0.0, 0.0, 0.0};
+      PERSISTENT_BLOCKS(bi) {
+        double z[8], r[8], s[8], rh[8], sh[8], w[8];
+        spmv(bi, A.shat, S.ms, z);
+        store_col(A.z, bi.id, G, z);
+        load_col(A.r, bi.id, G, r);
+        load_col(A.s, bi.id, G, s);
+        load_col(A.rhat, bi.id, G, rh);
+        load_col(A.shat, bi.id, G, sh);
+        load_col(A.w, bi.id, G, w);
+        double q[8], qh[8], y[8];
+#pragma unroll
+        for (int zz = 0; zz < 8; ++zz) {
+          q[zz] = r[zz] - al * s[zz];
+          qh[zz] = rh[zz] - al * sh[zz];
+          y[zz] = w[zz] - al * z[zz];
+          b3[0] += q[zz] * y[zz];
+          b3[1] += y[zz] * y[zz];
+        }
+        store_col(A.q, bi.id, G, q);
+        store_col(A.qhat, bi.id, G, qh);
+        store_col(A.y, bi.id, G, y);
+        precond(bi, z);
+        store_col(A.zhat, bi.id, G, z);
+        b3[2] += hsum(bi, z);
+      }
+      if (!(ok = reduce(b3))) break;
+      if (threadIdx.x == 0) S.ms = b3[2];
+      sync_state();
+      const double omn = b3[0] / (b3[1] + eps);
+      a[0] = 0.0;
+      PERSISTENT_BLOCKS(bi) {
+        double v[8], x[8], ph[8], qh[8];
+        spmv(bi, A.zhat, S.ms, v);
+        store_col(A.v, bi.id, G, v);
+        load_col(A.x, bi.id, G, x);
+        load_col(A.phat, bi.id, G, ph);
+        load_col(A.qhat, bi.id, G, qh);
+#pragma unroll
+        for (int zz = 0; zz < 8; ++zz) x[zz] = x[zz] + al * ph[zz] + omn * qh[zz];
+        store_col(A.x, bi.id, G, x);
+        a[0] += hsum(bi, x);
+      }
+      if (!(ok = reduce(a))) break;
+      if (threadIdx.x == 0) S.ms = a[0];
+      sync_state();
+      a[0] = 0.0;
+      PERSISTENT_BLOCKS(bi) {  // r = b - A x, rhat = M r
+        double ax[8], bc[8];
+        spmv(bi, A.x, S.ms, ax);
+        load_col(A.b, bi.id, G, bc);
+        if (A.zero_mean_row && bi.mean && G.lane == 0) bc[0] = 0.0;
+#pragma unroll
+        for (int zz = 0; zz < 8; ++zz) bc[zz] -= ax[zz];
+        store_col(A.r, bi.id, G, bc);
+        precond(bi, bc);
+        store_col(A.rhat, bi.id, G, bc);
+        a[0] += hsum(bi, bc);
+      }
+      if (!(ok = reduce(a))) break;
+      if (threadIdx.x == 0) S.ms = a[0];
+      sync_state();
+      double d[7] = {0, 0, 0, 0, 0, 0, 0};
+      PERSISTENT_BLOCKS(bi) {  // w = A rhat, what = M w; the dots
+        double w[8], r0[8], r[8], s[8], z[8];
+        spmv(bi, A.rhat, S.ms, w);
+        store_col(A.w, bi.id, G, w);
+        load_col(A.r0, bi.id, G, r0);
+        load_col(A.r, bi.id, G, r);
+        load_col(A.s, bi.id, G, s);
+        load_col(A.z, bi.id, G, z);
+#pragma unroll
+        for (int zz = 0; zz < 8; ++zz) {
+          d[0] += r0[zz] * r[zz];
+          d[1] += r0[zz] * w[zz];
+          d[2] += r0[zz] * s[zz];
+          d[3] += r0[zz] * z[zz];
+          d[4] += r[zz] * r[zz];
+          d[5] += r0[zz] * r0[zz];
+        }
+        precond(bi, w);
+        store_col(A.what, bi.id, G, w);
+        d[6] += hsum(bi, w);
+      }
+      if (!(ok = reduce(d))) break;
+      if (threadIdx.x == 0) {
+        S.omega = omn;
+        S.ms = d[6];
+        for (int i = 0; i < 6; ++i) red[32 + i] = d[i];
+      }
+      sync_state();
+    }
+    // scalars, restart, best iterate, stopping test (every CTA, its own copy)
+    if (threadIdx.x == 0) {
+      const double r0r = red[32], r0w = red[33], r0s = red[34], r0z = red[35], n1 = red[36], n2 = red[37];
+      const double omn = S.omega;
+      S.norm = sqrt(n1);
+      S.beta = S.alpha / (omn + eps) * r0r / (S.r0r_prev + eps);
+      double alpha = r0r / (r0w + S.beta * r0s - S.beta * omn * r0z);
+      double alphat = 1.0 / (omn + eps) + r0w / (r0r + eps) - S.beta * omn * r0z / (r0r + eps);
+      alphat = 1.0 / (alphat + eps);
+      if (fabs(alphat) < 10 * fabs(alpha)) alpha = alphat;
+      S.alpha = alpha;
+      S.r0r_prev = r0r;
+      S.best_pending = 0;
+      // restart on a serious breakdown (decided here, done below by all threads)
+      S.status = (r0r * r0r < 1e-16 * n1 * n2 && S.restarts < S.max_restarts) ? -1 : S.status;
+      if (S.norm < S.min_norm) {
+        S.use_xopt = 1;
+        S.min_norm = S.norm;
+        S.best_pending = 1;
+      }
+      if (!(S.norm == S.norm)) {
+        S.done = 1;
+        S.status = SOLVE_NAN;
+      } else if (S.norm < S.tol_abs || S.norm / (S.init_norm + eps) < S.tol_rel) {
+        S.done = 1;
+        S.converged = 1;
+        S.status = SOLVE_CONVERGED;
+      }
+      S.k += 1;
+    }
+    sync_state();
+    if (S.status == -1 && !S.done) {  // r0 = r; rhat = M r0; then as at the start
+      if (threadIdx.x == 0) {
+        S.status = SOLVE_RUNNING;
+        S.restarts += 1;
+      }
+      double a[1] = {0.0};
+      PERSISTENT_BLOCKS(bi) {
+        copy_best(bi);
+        double r[8];
+        load_col(A.r, bi.id, G, r);
+        store_col(A.r0, bi.id, G, r);
+        precond(bi, r);
+        store_col(A.rhat, bi.id, G, r);
+        a[0] += hsum(bi, r);
+      }
+      if (!(ok = reduce(a))) break;
+      if (threadIdx.x == 0) {
+        S.ms = a[0];
+        S.best_pending = 0;
+      }
+      sync_state();
+      if (!(ok = start_phase())) break;
+    } else if (S.status == -1 && threadIdx.x == 0) {
+      S.status = SOLVE_CONVERGED;
+    }
+    sync_state();
+  }
+  // the best iterate into x: x itself when the last reduction found it best
+  if (ok && S.use_xopt && !S.best_pending)
+    PERSISTENT_BLOCKS(bi) {
+      double c[8];
+      load_col(A.xopt, bi.id, G, c);
+      store_col(A.x, bi.id, G, c);
+    }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (!ok) {
+      S.done = 1;
+      S.status = SOLVE_BARRIER_TIMEOUT;
+    } else if (!S.done) {
+      S.status = SOLVE_MAXITER;
+    }
+    *A.st = S;
+  }
+}
+
+int poisson_pipelined(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
+                      double* const vec[16], SolveStats& out, cudaStream_t s) {
+  poisson_init_constants();
+  PState init{};
+  init.eps = 1e-100;
+  init.tol_abs = P.tol_abs;
+  init.tol_rel = P.tol_rel;
+  init.max_iter = P.max_iter;
+  init.max_restarts = 100;
+  init.status = SOLVE_RUNNING;
+  PState* st = reinterpret_cast<PState*>(W.st2);  // the refinement state's slot: unused by this solver
+  static_assert(sizeof(PState) <= sizeof(KrylovState), "PState fits the state slot");
+  CUP_CUDA_TRY(cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, s));
+  PArgs A{};
+  A.M = M;
+  A.b = b;
+  A.x = x;
+  double** dst[16] = {&A.xopt, &A.r0, &A.r, &A.rhat, &A.w, &A.what, &A.t, &A.phat,
+                      &A.s, &A.shat, &A.z, &A.zhat, &A.v, &A.q, &A.qhat, &A.y};
+  for (int i = 0; i < 16; ++i) *dst[i] = vec[i];
+  const size_t n = size_t(M.nb) * BN;
+  // the recurrences read phat, shat, s, z, zhat and v of "iteration -1": zero
+  for (int i = 7; i < 13; ++i) CUP_CUDA_TRY(cudaMemsetAsync(vec[i], 0, n * sizeof(double), s));
+  A.st = st;
+  A.mean_mode = P.mean_mode;
+  A.zero_mean_row = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
+  A.ncache = std::max(0, std::min(P.block_cache, KB_CACHE));
+  void (*kern)(PArgs, GridSync) = k_pbicg_persistent;
+  const size_t dyn = kPersistentSmem;
+  static unsigned long long attr = 0;
+  if (first_on_device(attr))
+    CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+  int per_sm = 0, dev = 0, sms = 0;
+  CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PNT, dyn));
+  CUP_CUDA_TRY(cudaGetDevice(&dev));
+  CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (per_sm < 1) return set_error(CUP_ERR_CUDA, "pipelined BiCGSTAB: kernel does not fit on an SM");
+  const int grid = std::max(1, std::min({per_sm * sms, (M.nb + PGROUPS - 1) / PGROUPS, std::max(W.grid, W.ggrid) / 2}));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
+  GridSync Gs{W.bar, W.partial, W.bar_error, W.barrier_cycles > 0 ? W.barrier_cycles : kBarrierClockLimit};
+  void* args[] = {(void*)&A, (void*)&Gs};
+  {
+    ProfScope ps("pbicg_persistent", s);
+    CUP_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)kern, dim3(grid), dim3(PNT), args, dyn, s));
+  }
+  PState fin{};
+  CUP_CUDA_TRY(cudaMemcpyAsync(&fin, st, sizeof(fin), cudaMemcpyDeviceToHost, s));
+  CUP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (fin.status == SOLVE_BARRIER_TIMEOUT) return set_error(CUP_ERR_CUDA, "pipelined BiCGSTAB: a grid barrier wait timed out");
+  out.iterations = fin.k;
+  out.restarts = fin.restarts;
+  out.status = fin.status;
+  out.err_init = fin.init_norm;
+  out.err_opt = fin.min_norm < 1e49 ? fin.min_norm : fin.init_norm;
+  return 0;
+}
+
 }  // namespace cup3d

@@ -126,6 +126,11 @@ int poisson_bicgstab(const DevMesh& M, const double* b, double* x, const SolvePa
 int poisson_mixed(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
                   SolveStats& out, cudaStream_t s, int* h_done_pinned, const LocalMap* lmap = nullptr,
                   const CoarseView* coarse = nullptr, int sms = 148);
+// The reference's pipelined BiCGSTAB with the exact block inverse
+// (PoissonSolverAMR.cpp:13-358), in one cooperative launch; vec: 16 vectors
+// of nb*512 doubles (scratch).
+int poisson_pipelined(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
+                      double* const vec[16], SolveStats& out, cudaStream_t s);
 // FP64 ||b - A x||_2 with the solvers' mean-row convention.
 int true_residual_norm(const DevMesh& M, const double* b, const double* x, int mean_mode, PoissonWork& W,
                        double* err_host, cudaStream_t s);

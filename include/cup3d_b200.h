@@ -49,6 +49,10 @@ extern "C" {
 #define CUP_POISSON_B200_TWOLEVEL 4 /* "b200_twolevel": BiCGSTAB, two-level preconditioner without
                                        the network (coarse correction + block inverse); the
                                        method the learned one is compared with */
+#define CUP_POISSON_B200_PIPELINED 6 /* "b200_pipelined": the reference CPU solver's pipelined BiCGSTAB
+                                       (PoissonSolverAMR.cpp:13-358: exact block inverse, residual
+                                       replacement every 50 iterations, restarts, best iterate), in
+                                       one persistent launch with two grid barriers per iteration */
 #define CUP_POISSON_B200_SCHWARZ 5  /* "b200_schwarz": the two-level preconditioner with the exact
                                        one-cell-overlap local solve of each block (restricted
                                        additive Schwarz) in place of the block inverse; the local

@@ -47,7 +47,7 @@ struct SimulationData {
     cup_config_default(&cfg);
     check(cup_config_parse(&cfg, flags.c_str()), nullptr);
     static const char* names[] = {"b200",          "b200_mixed",  "b200_learned", "b200_learned_mixed",
-                                  "b200_twolevel", "b200_schwarz"};
+                                  "b200_twolevel", "b200_schwarz", "b200_pipelined"};
     poissonSolver = names[cfg.poisson_solver];
     ctx = cup_create(&cfg);
     if (!ctx) throw std::runtime_error(std::string("cup3d_b200: ") + cup_last_error(nullptr));
@@ -129,7 +129,7 @@ class PoissonSolverB200 : public PoissonSolverBase {
 // reference's "iterative" / "cuda_iterative" select the plain FP64 solver.
 inline std::shared_ptr<PoissonSolverBase> makePoissonSolver(SimulationData& s) {
   static const char* known[] = {"b200",      "b200_mixed",     "b200_learned", "b200_learned_mixed",
-                                "b200_twolevel", "b200_schwarz", "iterative", "cuda_iterative"};
+                                "b200_twolevel", "b200_schwarz", "b200_pipelined", "iterative", "cuda_iterative"};
   for (const char* k : known)
     if (s.poissonSolver == k) return std::make_shared<PoissonSolverB200>(s);
   throw std::invalid_argument("Poisson solver: \"" + s.poissonSolver + "\" unrecognized!");
