@@ -59,6 +59,7 @@ class cup_config(C.Structure):
         ("ctol", C.c_double),
         ("level_max_vorticity", C.c_int32),
         ("level_start", C.c_int32),
+        ("poisson_persistent", C.c_int32),
     ]
 
 

@@ -220,6 +220,7 @@ void cup_config_default(cup_config* c) {
   c->ctol = 0.1;
   c->level_max_vorticity = -1;  // levelMax unless given
   c->level_start = -1;          // levelMax - 1 unless given (SimulationData.cpp:38)
+  c->poisson_persistent = 1;
 }
 
 static int parse_bc(const std::string& v) {
@@ -313,6 +314,9 @@ int cup_config_parse(cup_config* c, const char* args) {
     } else if (key == "levelStart") {
       if (need_num()) return CUP_ERR_ARG;
       c->level_start = int(dv);
+    } else if (key == "poissonPersistent") {
+      if (need_num()) return CUP_ERR_ARG;
+      c->poisson_persistent = int(dv) != 0 ? 1 : 0;
     } else if (key == "StaticObstacles") {
       if (need_num()) return CUP_ERR_ARG;
       c->static_obstacles = dv != 0 ? 1 : 0;
@@ -585,7 +589,7 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   P.mean_mode = c->cfg.mean_constraint;
   P.check_every = 8;
   P.stall_window = 0;
-  P.persistent = 1;
+  P.persistent = c->cfg.poisson_persistent;
   P.block_cache = c->cfg.poisson_block_cache;
   SolveStats S{};
   int rc = 0;

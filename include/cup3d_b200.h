@@ -103,6 +103,9 @@ typedef struct cup_config {
   double ctol;                 /* -Ctol: compress blocks whose indicators stay below it (default 0.1) */
   int32_t level_max_vorticity; /* -levelMaxVorticity (default levelMax) */
   int32_t level_start;         /* -levelStart: level of cup_set_mesh_uniform (default levelMax - 1) */
+  int32_t poisson_persistent;  /* -poissonPersistent: 1 (default) one cooperative launch per solve; 0 the
+                                  host-driven form, five kernels per iteration and a host check every 8
+                                  (plain, mixed and two-level solvers; for per-phase profiles) */
 } cup_config;
 
 typedef struct cup_solve_stats {

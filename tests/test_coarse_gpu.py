@@ -115,3 +115,25 @@ def test_captured_twolevel_step_equals_launched_step():
     assert i1 == i0
     assert np.abs(v1 - v0).max() <= 1e-12 * np.abs(v0).max()
     assert np.abs(p1 - p0).max() <= 1e-12 * np.abs(p0).max()
+
+
+@pytest.mark.parametrize("solver", ["b200", "b200_twolevel"])
+def test_host_driven_form_matches_persistent_solver(solver):
+    # -poissonPersistent 0: five kernels per iteration and a host check every
+    # 8 iterations (the coarse correction by its own kernels); the same method
+    # as the single cooperative launch, with other summation orders
+    sols = {}
+    for pers in (1, 0):
+        ctx = make_ctx("amr3_mixed", device=0, extra=f"-poissonPersistent {pers}")
+        m = oracle_mesh(ctx)
+        b = np.random.default_rng(11).standard_normal(m.n)
+        hh = np.repeat(m.h, 512)
+        b -= np.sum(b * hh ** 3) / np.sum(hh ** 3)
+        bd, xd = torch_dev(b), torch_dev(np.zeros(m.n))
+        ctx.set_poisson(solver, 0.0, 1e-8, 1000)
+        rc, st = ctx.poisson_solve_dev(bd, xd)
+        assert rc == 0 and st["status"] == 1 and st["true_rel"] <= 1.5e-8, (pers, st)
+        sols[pers] = (xd.cpu().numpy(), st["iterations"])
+    print(solver, "iterations persistent / host-driven:", sols[1][1], sols[0][1])
+    assert abs(sols[1][1] - sols[0][1]) <= max(2, sols[1][1] // 10)
+    assert np.linalg.norm(sols[1][0] - sols[0][0]) <= 1e-6 * np.linalg.norm(sols[1][0])
