@@ -208,18 +208,22 @@ def poisson_at_tolerance(ctx, stream, flush, rhs_list, reps=3):
     return res
 
 
-def swarm_batch(flush, steps=5):
+def swarm_batch(flush, steps=5, solver="b200"):
     """The 64-case ellipsoid swarm advanced as one batch (cup_batch_step: one
     set of launches and one Poisson launch per step for all cases), against
     the same cases stepped one by one; device time from CUDA events on the
     stepping streams, L2 flushed before every timed step.  Kernel by kernel
-    (-stepGraph 0) on both sides, so that no step pays a graph capture."""
+    (-stepGraph 0) on both sides, so that no step pays a graph capture.
+    solver: the Poisson solver of every case (b200_twolevel: each case's own
+    coarse space, built when the batch is created, timed apart)."""
     import torch
     import cup3d_b200 as cup
     from cup3d_b200.workloads import SWARM_WORKLOAD, make_swarm_ctx
     lib = cup._lib.lib()
-    ctxs = [make_swarm_ctx(i, torch.cuda.current_device(), "-stepGraph 0") for i in range(64)]
+    ctxs = [make_swarm_ctx(i, torch.cuda.current_device(), f"-stepGraph 0 -poissonSolver {solver}") for i in range(64)]
+    t0 = time.perf_counter()
     batch = cup.Batch(ctxs)
+    setup_s = time.perf_counter() - t0
     ncell = batch.nb * 512
 
     def timed(ctx, fn):
@@ -247,8 +251,9 @@ def swarm_batch(flush, steps=5):
         c.close()
     batch.close()
     return {
-        "workload": SWARM_WORKLOAD, "cases": 64, "cells": ncell,
-        "metric": "Mcell-steps/s (batched time steps of all cases, plain FP64)",
+        "workload": SWARM_WORKLOAD, "cases": 64, "cells": ncell, "solver": solver,
+        "batch_create_s": round(setup_s, 2),
+        "metric": "Mcell-steps/s (batched time steps of all cases, FP64)",
         "value": round(ncell * steps / (sum(ms) * 1e-3) / 1e6, 3), "steps": f"1..{steps} after step 0",
         "ms_per_step": [round(x, 2) for x in ms],
         "poisson_iterations_mean_max": [[round(sum(i) / len(i), 1), max(i)] for i in its],
@@ -482,7 +487,7 @@ def run_b200(args):
     if not args.no_poisson:
         line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush, rhs_list)
     if rank == 0 and not args.no_swarm:
-        line["swarm_batch"] = swarm_batch(flush)
+        line["swarm_batch"] = {s: swarm_batch(flush, solver=s) for s in ("b200", "b200_twolevel")}
     if rank == 0 and not args.no_obstacle:
         line["obstacle_creation"] = obstacle_creation()
     if rank == 0 and not args.no_cpu_baseline:

@@ -107,6 +107,49 @@ static int batch_setup(cup_ctx* c, const std::vector<Mesh>& cases) {
   return 0;
 }
 
+// The batch's two-level preconditioners, when built.
+static const BatchCoarse* batch_coarse(const cup_ctx* c) { return c->bcoarse.inv ? &c->bcoarse : nullptr; }
+
+// With the two-level solver configured: each case's coarse space, built on
+// the case's own context (its A_c, mean-constraint row included, and the
+// FP32 inverse), copied into one packed, block-diagonal array in case order.
+// No face joins two cases, so the batch's coarse operator is exactly that.
+static int batch_coarse_setup(cup_ctx* c, cup_ctx* const* cases) {
+  if (c->cfg.poisson_solver != CUP_POISSON_B200_TWOLEVEL) return 0;
+  std::vector<long long> off(c->ncase);
+  long long total = 0;
+  for (int k = 0; k < c->ncase; ++k) {
+    const long long n = c->case_first[k + 1] - c->case_first[k];
+    off[k] = total;
+    total += n * n;
+  }
+  DevArena& A = c->bcoarse_arena;
+  float* inv = nullptr;
+  long long* d_off = nullptr;
+  double *rc = nullptr, *rc2 = nullptr, *w = nullptr;
+  const int nb = c->mesh.nb;
+  if (int rc_ = A.alloc(&inv, size_t(total))) return rc_;
+  if (int rc_ = A.alloc(&d_off, size_t(c->ncase))) return rc_;
+  if (int rc_ = A.alloc(&rc, size_t(nb))) return rc_;
+  if (int rc_ = A.alloc(&rc2, size_t(nb))) return rc_;
+  if (int rc_ = A.alloc(&w, size_t(nb))) return rc_;
+  CUP_CUDA_TRY(stream_h2d(c->stream, d_off, off.data(), off.size() * sizeof(long long)));
+  std::vector<double> hw(nb);
+  for (int b = 0; b < nb; ++b) hw[b] = 512.0 * c->mesh.h[b] * c->mesh.h[b] * c->mesh.h[b];
+  CUP_CUDA_TRY(stream_h2d(c->stream, w, hw.data(), hw.size() * sizeof(double)));
+  for (int k = 0; k < c->ncase; ++k) {
+    cup_ctx* s = cases[k];
+    if (int rc_ = coarse_build(s)) return rc_;
+    const long long n = c->case_first[k + 1] - c->case_first[k];
+    if (s->coarse.nb != n) return set_error(CUP_ERR_STATE, "batch two-level: a case's coarse space does not match");
+    CUP_CUDA_TRY(cudaMemcpyAsync(inv + off[k], s->coarse.inv, size_t(n * n) * sizeof(float), cudaMemcpyDeviceToDevice,
+                                 s->stream));
+    CUP_CUDA_TRY(cudaStreamSynchronize(s->stream));
+  }
+  c->bcoarse = BatchCoarse{inv, d_off, rc, rc2, w};
+  return 0;
+}
+
 // The cases' current fields (velocity, pressure, grid chi) into the batch's.
 static int copy_case_fields(cup_ctx* c, const std::vector<const cup_ctx*>& cases) {
   const size_t N = size_t(c->mesh.nb) * BN;
@@ -268,7 +311,7 @@ static int batch_graph_capture(cup_ctx* c, int vcur, int pcur, int use_pold, cud
                                     F.phi, kgrid(c, TG_RHS), s))
       return r;
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev0, s, cudaEventRecordExternal));
-    if (int r = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, P, c->W, c->B, nullptr, s)) return r;
+    if (int r = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, P, c->W, c->B, nullptr, s, batch_coarse(c))) return r;
     CUP_CUDA_TRY(cudaEventRecordWithFlags(c->ev1, s, cudaEventRecordExternal));
     if (int r = launch_case_sums(c->dm, F.phi, T.bscratch, T.first, K, T.sums, grid, s)) return r;
     if (int r = launch_grad_update(c->dm, F.vel[v], F.phi, pold, pnew, nullptr, 0.0, step_arg,
@@ -359,6 +402,7 @@ cup_ctx* cup_batch_create(int32_t ncases, cup_ctx* const* cases) {
   int rc = batch_setup(c, meshes);
   if (rc == 0) rc = copy_case_fields(c, cs);
   if (rc == 0) rc = batch_step_setup(c, cs);
+  if (rc == 0) rc = batch_coarse_setup(c, cases);
   if (rc) {
     (void)rc;
     const std::string msg = "cup_batch_create: " + std::string(cup_last_error(nullptr));
@@ -391,7 +435,8 @@ int cup_batch_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solv
   const SolveParams P = batch_params(c);
   std::vector<SolveStats> S(c->ncase);
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
-  if (int rc = poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S.data(), c->stream)) return keep_err(c, rc);
+  if (int rc = poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S.data(), c->stream, batch_coarse(c)))
+    return keep_err(c, rc);
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   CUP_CUDA_TRY(cudaEventSynchronize(c->ev1));
   float ms = 0;
@@ -447,7 +492,8 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
     return keep_err(c, rc);
   std::vector<SolveStats> S(K);
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
-  if (int rc = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, batch_params(c), c->W, c->B, S.data(), c->stream))
+  if (int rc = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, batch_params(c), c->W, c->B, S.data(), c->stream,
+                                       batch_coarse(c)))
     return keep_err(c, rc);
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   if (int rc = launch_case_sums(c->dm, F.phi, T.bscratch, T.first, K, T.sums, grid, c->stream)) return keep_err(c, rc);

@@ -200,6 +200,9 @@ struct cup_ctx {
   // incremented whenever the mesh changes (keys what is built per mesh)
   int mesh_version = 0;
   cup3d::CoarseSpace coarse;
+  // a batch's two-level preconditioners (cup_batch_create with b200_twolevel)
+  cup3d::DevArena bcoarse_arena;
+  cup3d::BatchCoarse bcoarse;
   // scratch vectors of the pipelined solver (allocated on first use)
   cup3d::DevArena pipe_arena;
   double* pipe_vec[16] = {nullptr};

@@ -365,7 +365,8 @@ struct KArgs {
   int ncache;         // persistent solver: block entries staged per group at launch (<= KB_CACHE)
   // two-level preconditioner (persistent solver): A_c^-1 (cnb x cnb, cnb = 0:
   // none), the restricted vectors of zv and zr and the blocks' 512 h^3
-  int cnb;
+  int cnb;           // single case: blocks of A_c; batch: 1 when the cases carry coarse spaces
+  const long long* coff;  // batch: offset of each case's A_c^-1 (nb_c x nb_c) in cinv; null: one case
   const float* cinv;
   double* crc_v;
   double* crc_r;
@@ -899,12 +900,13 @@ __device__ __forceinline__ void coarse_restrict(const double c[8], double* rc, i
   if (G.lane == 0) rc[b] = s[0];
 }
 
+// row: block b's row of A_c^-1 (n entries), rc: the restriction of the
+// blocks that row spans.
 template <class T>
-__device__ __forceinline__ double coarse_block(const KArgs<T>& A, const GroupIdx& G, int b, const double* rc, T* v,
-                                               double* gsm) {
-  const float* row = A.cinv + size_t(b) * A.cnb;
+__device__ __forceinline__ double coarse_block_row(const KArgs<T>& A, const GroupIdx& G, int b, const float* row,
+                                                   const double* rc, int n, T* v, double* gsm) {
   double s[1] = {0.0};
-  for (int j = G.lane; j < A.cnb; j += GROUP) s[0] += double(row[j]) * __ldcg(rc + j);
+  for (int j = G.lane; j < n; j += GROUP) s[0] += double(row[j]) * __ldcg(rc + j);
   group_reduce<1>(s, gsm, G);
   const double yc = s[0];
   double c[8];
@@ -913,6 +915,20 @@ __device__ __forceinline__ double coarse_block(const KArgs<T>& A, const GroupIdx
   for (int z = 0; z < 8; ++z) c[z] = double(T(c[z] + yc));
   store_col(v, b, G, c);
   return G.lane == 0 ? yc * A.cw[b] : 0.0;  // summed over the CTA's threads by the grid reduction
+}
+
+template <class T>
+__device__ __forceinline__ double coarse_block(const KArgs<T>& A, const GroupIdx& G, int b, const double* rc, T* v,
+                                               double* gsm) {
+  return coarse_block_row(A, G, b, A.cinv + size_t(b) * A.cnb, rc, A.cnb, v, gsm);
+}
+
+// The same in a batch: block b of case c (blocks cf .. cf + n - 1), whose
+// A_c^-1 starts at coff[c] of the packed, block-diagonal cinv.
+template <class T>
+__device__ __forceinline__ double coarse_block_case(const KArgs<T>& A, const GroupIdx& G, int b, int cf, int n,
+                                                    long long off, const double* rc, T* v, double* gsm) {
+  return coarse_block_row(A, G, b, A.cinv + off + size_t(b - cf) * n, rc + cf, n, v, gsm);
 }
 
 // P0 (once): zr = M^-1 r for the initial residual; sum(zr h^3)
@@ -1406,6 +1422,21 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, G
   __syncthreads();
   // the case's first group writes its state and done flag
   auto lead = [&]() { return P.c >= 0 && gidx == gfirst[P.c] && G.lane == 0; };
+  // two-level preconditioner: the coarse correction of each running case on
+  // v (zr or zv) from its restriction rc, added by the case's groups; the
+  // case's added sum(v h^3) comes back to its groups (one more barrier)
+  auto coarse_phase = [&](const double* rc, T* v, bool active, double& added) -> bool {
+    double a[1] = {0.0};
+    if (active) {
+      const int cf = B.cfirst[P.c], n = B.cfirst[P.c + 1] - cf;
+      const long long off = A.coff[P.c];
+      BATCH_BLOCKS(bi) a[0] += coarse_block_case<T>(A, G, bi.id, cf, n, off, rc, v, gsm);
+    }
+    const bool okc = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, P.c, gfirst[max(P.c, 0)],
+                                               gfirst[max(P.c, 0) + 1], nullptr);
+    added = a[0];
+    return okc;
+  };
   bool ok = true;
   // PREP, INIT, P0: one barrier each
   {
@@ -1429,8 +1460,10 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, G
     if (P.c >= 0 && !S.done) BATCH_BLOCKS(bi) a[0] += p0_block<T>(A, G, tile, bi, inv_eig);
     ok = batch_allreduce<1, false>(a, B, Gs, epoch, gsm, G, gidx, P.c, gfirst[max(P.c, 0)], gfirst[max(P.c, 0) + 1],
                                    nullptr);
+    double cz = 0.0;
+    if (ok && A.cnb) ok = coarse_phase(A.crc_r, A.z1, P.c >= 0 && !S.done, cz);
     // q = 0 at the start, so z1 = zr
-    if (ok && P.c >= 0 && G.lane == 0) S.ms_zr = S.mean_sum = a[0];
+    if (ok && P.c >= 0 && G.lane == 0) S.ms_zr = S.mean_sum = a[0] + cz;
     if (ok && lead()) {
       A.st[P.c] = S;
       B.case_done[P.c] = S.done;
@@ -1492,6 +1525,12 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, G
       S.mean_sum = S.ms_zr - S.alpha * a[1];  // sum(z2 h^3)
     }
     __syncthreads();
+    if (A.cnb) {  // zv += the coarse correction of nu; sum(z2 h^3) with it
+      double cv = 0.0;
+      if (!(ok = coarse_phase(A.crc_v, A.z2, active, cv))) break;
+      if (active && G.lane == 0) S.mean_sum = S.ms_zr - S.alpha * (a[1] + cv);
+      __syncthreads();
+    }
     const int g0 = gfirst[max(P.c, 0)], g1 = gfirst[max(P.c, 0) + 1];
     double d[2] = {0.0, 0.0};
     if (active) BATCH_BLOCKS(bi) p2_block<T>(A, G, tile, bi, S.alpha, S.mean_sum, d);
@@ -1508,6 +1547,16 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_bicg_batched(KArgs<T> A, G
       fin_e(S, re);
       S.ms_zr = e[2];
       S.mean_sum = S.restart_pending ? e[2] : e[2] + S.beta * e[3];  // sum(z1 h^3) of the next P1
+    }
+    __syncthreads();
+    if (A.cnb) {  // zr += the coarse correction of r; the sums with it
+      double cr = 0.0;
+      if (!(ok = coarse_phase(A.crc_r, A.z1, active && !S.done, cr))) break;
+      if (active && !S.done && G.lane == 0) {
+        S.ms_zr = e[2] + cr;
+        S.mean_sum = S.restart_pending ? S.ms_zr : S.ms_zr + S.beta * e[3];
+      }
+      __syncthreads();
     }
     if (active && lead()) {
       A.st[P.c] = S;
@@ -1627,6 +1676,7 @@ static KArgs<T> make_args(const DevMesh& M, const T* b, T* x, T* const v[9], Poi
   A.ncache = 0;
   A.cnb = 0;
   A.cinv = nullptr;
+  A.coff = nullptr;
   A.crc_v = A.crc_r = nullptr;
   A.cw = nullptr;
   A.lw = nullptr;
@@ -1762,7 +1812,8 @@ int batch_solver_shape(int nb, int ncase, int* grid, int* groups) {
 }
 
 int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
-                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s) {
+                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s,
+                             const BatchCoarse* coarse) {
   poisson_init_constants();
   if (B.ncase < 1 || !B.st) return set_error(CUP_ERR_STATE, "batched BiCGSTAB: not a batch");
   double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
@@ -1779,6 +1830,14 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
   KArgs<double> A = make_args<double>(M, b, x, v, W, B.st, P.mean_mode, zmr, 0);
   A.ncache = KB_CACHE;
+  if (coarse && coarse->inv) {  // the cases' two-level preconditioners
+    A.cnb = 1;
+    A.cinv = coarse->inv;
+    A.coff = coarse->off;
+    A.crc_v = coarse->rc;
+    A.crc_r = coarse->rc2;
+    A.cw = coarse->w;
+  }
   GridSync Gs{W.bar, W.partial, W.bar_error, W.barrier_cycles > 0 ? W.barrier_cycles : kBarrierClockLimit};
   BatchArgs Ba{B.cfirst, B.cblocks, B.part, B.case_done, B.ncase, B.groups};
   void* args[] = {(void*)&A, (void*)&Gs, (void*)&Ba};

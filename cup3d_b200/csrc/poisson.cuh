@@ -73,6 +73,17 @@ struct BatchWork {
   KrylovState* st_init = nullptr;  // ncase: initial states of captured solves
 };
 
+// The cases' two-level preconditioners in a batch: each case's A_c^-1
+// (nb_c x nb_c, FP32, row-major) packed in case order (case c at off[c]),
+// the restriction buffers and 512 h^3 over the batch's blocks.
+struct BatchCoarse {
+  const float* inv = nullptr;
+  const long long* off = nullptr;
+  double* rc = nullptr;
+  double* rc2 = nullptr;
+  const double* w = nullptr;
+};
+
 struct SolveParams {
   double tol_abs, tol_rel;
   int max_iter, max_restarts, mean_mode;
@@ -162,6 +173,7 @@ int batch_solver_shape(int nb, int ncase, int* grid, int* groups);
 // One BiCGSTAB per case of the batch (x holds x0 on entry and each case's
 // best iterate on exit); out[c] per case.
 int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
-                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s);
+                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s,
+                             const BatchCoarse* coarse = nullptr);
 
 }  // namespace cup3d
