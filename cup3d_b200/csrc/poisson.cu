@@ -2459,7 +2459,11 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_pbicg_persistent(PArgs A, 
       S.k += 1;
     }
     sync_state();
-    if (S.status == -1 && !S.done) {  // r0 = r; rhat = M r0; then as at the start
+    // every thread reads the decision before thread 0 changes the state
+    const bool do_restart = S.status == -1 && !S.done;
+    const bool restart_at_end = S.status == -1 && S.done;
+    sync_state();
+    if (do_restart) {  // r0 = r; rhat = M r0; then as at the start
       if (threadIdx.x == 0) {
         S.status = SOLVE_RUNNING;
         S.restarts += 1;
@@ -2481,7 +2485,7 @@ __global__ void __launch_bounds__(PNT, 8 / PGROUPS) k_pbicg_persistent(PArgs A, 
       }
       sync_state();
       if (!(ok = start_phase())) break;
-    } else if (S.status == -1 && threadIdx.x == 0) {
+    } else if (restart_at_end && threadIdx.x == 0) {
       S.status = SOLVE_CONVERGED;
     }
     sync_state();
