@@ -4,19 +4,25 @@ Workload (N=1): flow past a fixed sphere at Re=300 -- domain 4x2x2, 4x2x2
 level-0 blocks of 8^3 cells, levelMax 4 (mesh frozen after refinement around
 the sphere and its wake: 2340 blocks, 1.198M cells), sphere radius 0.0625 at
 (1,1,1) moving at +0.1 in x with the frame following it (uinf = -0.1),
-nu = 0.1*0.125/300, WENO5, implicit penalization lambda=1e6, plain FP64
-BiCGSTAB with the exact block preconditioner, reference tolerances
-(-poissonTol 1e-6, -poissonTolRel 1e-4).  A "step" is one full time step:
-calcMaxTimestep, AdvectionDiffusion (3 RK stages), Penalization,
+nu = 0.1*0.125/300, WENO5, implicit penalization lambda=1e6, FP64 BiCGSTAB
+with the two-level preconditioner (block-constant coarse space + exact
+block inverse; --solver b200: the block inverse alone), reference
+tolerances (-poissonTol 1e-6, -poissonTolRel 1e-4).  A "step" is one full
+time step: calcMaxTimestep, AdvectionDiffusion (3 RK stages), Penalization,
 PressureProjection (RHS, Poisson solve, mean removal, gradient update).
+The timed steps follow the warm-up steps and --settle (50) more.
 
 `value`  Mcell-steps/s with the fields resident in HBM (device time, CUDA
          events on the context's stream), L2 flushed between timed steps.
 `e2e`    the same through the reference-facing C ABI with host buffers:
          per step velocity + pressure uploaded from pinned host memory, the
          step, velocity + pressure downloaded.
+`poisson_to_tolerance`  one solve of the seeded right-hand side to 1e-6 and
+         1e-10 (FP64 true residual) per solver; the learned network trained
+         in the run on the flow's own pressure right-hand sides.
 `swarm_batch`  64 independent penalized-ellipsoid cases (372-2659 blocks
-         each, 37.5M cells) advanced together by cup_batch_step, with step 0
+         each, 37.5M cells) advanced together by cup_batch_step: 200 steps
+         with the two-level solver, 5 with the block inverse alone; step 0
          also taken case by case for comparison.
 `--impl reference`  the reference's CPU path restated (oracle: upwind/WENO,
          penalization, projection with the pipelined BiCGSTAB + block CG of
@@ -255,8 +261,12 @@ def swarm_batch(flush, steps=5, solver="b200"):
         "batch_create_s": round(setup_s, 2),
         "metric": "Mcell-steps/s (batched time steps of all cases, FP64)",
         "value": round(ncell * steps / (sum(ms) * 1e-3) / 1e6, 3), "steps": f"1..{steps} after step 0",
-        "ms_per_step": [round(x, 2) for x in ms],
-        "poisson_iterations_mean_max": [[round(sum(i) / len(i), 1), max(i)] for i in its],
+        "ms_per_step": [round(x, 2) for x in ms] if len(ms) <= 10 else
+                       {"first5": [round(x, 2) for x in ms[:5]], "last5": [round(x, 2) for x in ms[-5:]],
+                        "mean": round(sum(ms) / len(ms), 2)},
+        "poisson_iterations_mean_max": [[round(sum(i) / len(i), 1), max(i)] for i in its] if len(its) <= 10 else
+                                       {"first": [round(sum(its[0]) / len(its[0]), 1), max(its[0])],
+                                        "last": [round(sum(its[-1]) / len(its[-1]), 1), max(its[-1])]},
         "step0": {"batch_ms": round(batch0_ms, 2), "one_by_one_ms": round(single_ms, 2),
                   "speedup": round(single_ms / batch0_ms, 3),
                   "poisson_iterations_mean_max": [round(sum(x["iterations"] for x in st0) / 64, 1),
@@ -487,7 +497,9 @@ def run_b200(args):
     if not args.no_poisson:
         line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush, rhs_list)
     if rank == 0 and not args.no_swarm:
-        line["swarm_batch"] = {s: swarm_batch(flush, solver=s) for s in ("b200", "b200_twolevel")}
+        # config 5's 200 steps with the two-level solver; 5 steps with the block
+        # inverse alone for comparison
+        line["swarm_batch"] = {s: swarm_batch(flush, steps=n, solver=s) for s, n in (("b200", 5), ("b200_twolevel", 200))}
     if rank == 0 and not args.no_obstacle:
         line["obstacle_creation"] = obstacle_creation()
     if rank == 0 and not args.no_cpu_baseline:

@@ -4,6 +4,7 @@
     python -m cup3d_b200.kernel_cases solve   # 16 BiCGSTAB iterations (sphere mesh, seeded RHS)
     python -m cup3d_b200.kernel_cases step    # 4 full time steps of the sphere workload
     python -m cup3d_b200.kernel_cases swarm   # 16 iterations of a batched solve over 8 swarm cases
+    python -m cup3d_b200.kernel_cases learned # 20 training steps, then 16 iterations of the learned solve
 
 A second argument names the Poisson solver of the sphere cases (default
 b200; e.g. b200_twolevel).
@@ -55,8 +56,32 @@ def main(argv):
             ctx.step(step)
         torch.cuda.synchronize()
         print(f"step ok: {ctx.nb} blocks")
+    elif case == "learned":
+        # samples from the residuals of plain iterates 0, 2, 4, 8 of the seeded
+        # right-hand side; 20 Adam steps (k_cnn_train); the learned solve
+        # (its map phases inside k_bicg_persistent), 16 iterations
+        b = torch.tensor(poisson_rhs(ctx), device="cuda")
+        level, index, _ = ctx.blocks()
+        mb = int(np.where((index == 0).all(axis=1))[0][0])
+        ctx.cnn_init(7)
+        ctx.cnn_dataset_reserve(ctx.nb * 4)
+        for k in (0, 2, 4, 8):
+            xk = torch.zeros_like(b)
+            if k:
+                ctx.set_poisson("b200", 0.0, 1e-30, k)
+                ctx.poisson_solve_dev(b, xk)
+            ax = torch.zeros_like(b)
+            ctx.poisson_apply(xk, ax)
+            r = b - ax
+            r[mb * 512] = -ax[mb * 512]
+            ctx.cnn_dataset_add(r.contiguous())
+        ctx.cnn_train(20, 128, 1e-3, 11)
+        x = torch.zeros_like(b)
+        ctx.set_poisson("b200_learned", 0.0, 1e-30, 16)
+        rc, st = ctx.poisson_solve_dev(b, x)
+        print(f"learned ok: rc {rc}, {st['iterations']} iterations, {ctx.cnn_dataset_size()} samples")
     else:
-        raise SystemExit(f"unknown case {case!r}: spmv | solve | step")
+        raise SystemExit(f"unknown case {case!r}: spmv | solve | step | learned | swarm")
 
 
 if __name__ == "__main__":
