@@ -24,6 +24,11 @@ The timed steps follow the warm-up steps and --settle (50) more.
          each, 37.5M cells) advanced together by cup_batch_step: 200 steps
          with the two-level solver, 5 with the block inverse alone; step 0
          also taken case by case for comparison.
+`mesh_adaptation`  from the settled state, three rounds of one adaptation
+         (vorticity tagging, refine/compress, field transfer), the two-level
+         coarse space of the new mesh, and 20 steps on it (the reference
+         adapts every 20 steps); timed apart from the steps, as the metric
+         leaves adaptation out.
 `--impl reference`  the reference's CPU path restated (oracle: upwind/WENO,
          penalization, projection with the pipelined BiCGSTAB + block CG of
          PoissonSolverAMR.cpp) on the host cores, one step per sample.
@@ -319,6 +324,66 @@ def obstacle_creation(reps=7):
     return out
 
 
+def mesh_adaptation(ctx, stream, step0, rounds=3, every=20):
+    """Mesh adaptation on the reference's cadence (Simulation.cpp:385: every
+    20 steps), timed apart from the steps, which the metric leaves it out of.
+    From the settled sphere state, `rounds` times: one adaptation
+    (cup_adapt_mesh: device vorticity indicator, host refine/compress with
+    2:1 balance, device field transfer, chi created again), the two-level
+    coarse space of the new mesh (A_c through the device operator, blocked
+    inverse; built by the first coarse application), then `every` steps on
+    the new mesh.  Wall time of the calls, device time of the steps.  Also
+    the dense inverse alone on the final mesh's A_c: the blocked form, and
+    the column-wise pivoted form (forced by a cyclic shift of the rows, so
+    its time includes the failed blocked attempt)."""
+    import torch
+    out = []
+    step = step0
+    for _ in range(rounds):
+        nb0 = ctx.nb
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        changed = ctx.adapt_mesh()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        r = torch.ones(ctx.nb * 512, dtype=torch.float64, device="cuda")
+        z = torch.zeros_like(r)
+        ctx.coarse_apply(r, z)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        its = []
+        e0.record(stream)
+        for _ in range(every):
+            _, rc, st = ctx.step(step)
+            step += 1
+            its.append(st["iterations"])
+        e1.record(stream)
+        e1.synchronize()
+        out.append({"changed": bool(changed), "blocks_before": nb0, "blocks_after": ctx.nb,
+                    "adapt_ms": round((t1 - t0) * 1e3, 3), "coarse_build_ms": round((t2 - t1) * 1e3, 3),
+                    "step_ms": round(e0.elapsed_time(e1) / every, 4),
+                    "poisson_iterations_mean": round(float(np.mean(its)), 2)})
+    Ac, _ = ctx.coarse_matrix()
+    level, index, _ = ctx.blocks()
+    mb = int(np.where((index == 0).all(axis=1))[0][0])
+    inv = {}
+    for name, mat, last in (("blocked", Ac, mb), ("column_pivoted", np.roll(Ac, 1, axis=0), -1)):
+        a = torch.tensor(mat, device="cuda")
+        ctx.dense_inverse(a.clone(), last)  # warm
+        ts = []
+        for _ in range(3):
+            b = a.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            piv = ctx.dense_inverse(b, last)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        inv[name] = {"ms": round(float(np.median(ts)), 3), "pivoted": bool(piv)}
+    amort = np.mean([o["adapt_ms"] + o["coarse_build_ms"] for o in out]) / every
+    return {"cadence_steps": every, "rounds": out, "amortized_ms_per_step": round(float(amort), 4),
+            "dense_inverse": dict(inv, n=int(len(Ac)))}
+
+
 def run_b200(args):
     import torch
     rank, world, local = dist_env()
@@ -504,6 +569,9 @@ def run_b200(args):
         line["obstacle_creation"] = obstacle_creation()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ctx, args, (vel0, pres0), first_step)
+    if rank == 0 and not args.no_adapt:
+        # last: it changes the context's mesh
+        line["mesh_adaptation"] = mesh_adaptation(ctx, stream, restore())
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -612,6 +680,7 @@ def main():
     ap.add_argument("--no-poisson", action="store_true", help="skip the Poisson-to-tolerance comparison")
     ap.add_argument("--no-swarm", action="store_true", help="skip the batched ellipsoid-swarm measurement")
     ap.add_argument("--no-obstacle", action="store_true", help="skip the obstacle-creation measurement")
+    ap.add_argument("--no-adapt", action="store_true", help="skip the mesh-adaptation measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

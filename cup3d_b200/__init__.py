@@ -322,6 +322,15 @@ class Context:
         """z = P A_c^-1 P^T r on torch CUDA float64 tensors."""
         check(lib().cup_coarse_apply_dev(self._p, _dev_ptr(r), _dev_ptr(z)), self._p)
 
+    def dense_inverse(self, a, last=-1):
+        """a <- a^-1 in place (torch CUDA float64, n x n, row-major), by the
+        coarse space's device inverse; True when the pivoted form ran."""
+        n = int(a.shape[0])
+        assert a.dtype.is_floating_point and a.element_size() == 8 and a.is_contiguous() and a.shape == (n, n)
+        piv = C.c_int32(0)
+        check(lib().cup_dense_inverse_dev(self._p, _dev_ptr(a), n, int(last), C.byref(piv)), self._p)
+        return bool(piv.value)
+
     def set_barrier_limit(self, cycles):
         """Wait limit of the persistent solvers' grid barriers (0: default)."""
         check(lib().cup_set_barrier_limit(self._p, int(cycles)), self._p)

@@ -143,6 +143,7 @@ SIGNATURES = {
     "cup_cnn_holdout": (C.c_int, [_P, C.c_int32]),
     "cup_cnn_eval": (C.c_int, [_P, C.POINTER(C.c_float)]),
     "cup_coarse_apply_dev": (C.c_int, [_P, C.c_void_p, C.c_void_p]),
+    "cup_dense_inverse_dev": (C.c_int, [_P, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]),
     "cup_set_poisson": (C.c_int, [_P, C.c_int32, C.c_double, C.c_double, C.c_int32]),
     "cup_cnn_num_params": (C.c_int32, []),
     "cup_cnn_init": (C.c_int, [_P, C.c_uint64]),

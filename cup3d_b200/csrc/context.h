@@ -110,7 +110,9 @@ struct CoarseSpace {
   double* rc2 = nullptr;        // nb: the second one of the persistent solver
   double* yc = nullptr;         // nb: coarse correction
   double* w = nullptr;          // nb: 512 h^3 of each block
-  std::vector<double> host_ac;  // A_c (row-major), for checks
+  std::vector<double> host_ac;  // A_c (row-major), for checks (kept when keep_host)
+  bool keep_host = false;
+  int pivoted = 0;              // A_c^-1 came from the column-wise pivoted Gauss-Jordan
   CoarseView view() const { return CoarseView{nb, inv, rc, rc2, yc, w}; }
 };
 
@@ -261,6 +263,9 @@ int adapt_mesh(cup_ctx* c, int* changed);
 int coarse_build(cup_ctx* c);
 // Inverse of an n x n host matrix (row-major) on the device (coarse.cu).
 int device_inverse(const double* a, int n, double* d_inv, int sms, cudaStream_t s);
+// The inverse in place of an n x n device matrix, index `last` (>= 0) last in
+// the pivot order; *fallback = 1 when the pivoted column-wise form ran.
+int device_inverse_dev(double* M, int n, int last, int sms, cudaStream_t s, int* fallback);
 // The learned map of the current weights for the solver (folds them when they
 // changed; the lab buffer for the current mesh).
 int lmap_prepare(cup_ctx* c, LocalMap* out);

@@ -417,9 +417,17 @@ int cup_cnn_forward_host_noalloc(cup_ctx* ctx, const float* in, float* out, int3
  * cup_coarse_matrix: builds it; out (may be NULL): A_c, nblocks^2 doubles,
  * row-major, blocks in cup_get_blocks order; *colours (may be NULL): the
  * colours of the set-up's block colouring.
- * cup_coarse_apply_dev: d_z = P A_c^-1 P^T d_r on device buffers. */
+ * cup_coarse_apply_dev: d_z = P A_c^-1 P^T d_r on device buffers.
+ * cup_dense_inverse_dev: the inverse that the coarse space uses, in place of
+ * the n x n row-major FP64 device matrix d_a: blocked Gauss-Jordan (panels of
+ * 32 pivots, no pivoting across panels) with index `last` (-1: none) moved to
+ * the end of the pivot order, checked by A^-1 (A v) = v to 1e-6 for a fixed
+ * probe v; when a pivot block is near-singular or the check fails, column-wise
+ * Gauss-Jordan with partial pivoting, and *pivoted (may be NULL) = 1.
+ * CUP_ERR_MESH for a singular matrix. */
 int cup_coarse_matrix(cup_ctx* ctx, double* out, int32_t* colours);
 int cup_coarse_apply_dev(cup_ctx* ctx, const double* d_r, double* d_z);
+int cup_dense_inverse_dev(cup_ctx* ctx, double* d_a, int32_t n, int32_t last, int32_t* pivoted);
 
 /* ---- profiling (the reference's DeviceProfiler, Utils/DeviceProfiler.cuh) ---- */
 /* Enables per-kernel CUDA-event timing (resets the counters). */

@@ -137,3 +137,58 @@ def test_host_driven_form_matches_persistent_solver(solver):
     print(solver, "iterations persistent / host-driven:", sols[1][1], sols[0][1])
     assert abs(sols[1][1] - sols[0][1]) <= max(2, sols[1][1] // 10)
     assert np.linalg.norm(sols[1][0] - sols[0][0]) <= 1e-6 * np.linalg.norm(sols[1][0])
+
+
+def test_dense_inverse_blocked_on_sphere_coarse_matrix():
+    # A_c of the benchmarked sphere mesh (2340 blocks, mean row of block mb
+    # last in the pivot order): the blocked form, to the FP64 accuracy of a
+    # dense inverse
+    import torch
+    from cup3d_b200.workloads import make_sphere_ctx
+    ctx = make_sphere_ctx(0)
+    Ac, _ = ctx.coarse_matrix()
+    level, index, _ = ctx.blocks()
+    mb = int(np.where((index == 0).all(axis=1))[0][0])
+    a = torch.tensor(Ac, device="cuda")
+    pivoted = ctx.dense_inverse(a, mb)
+    X = a.cpu().numpy()
+    ref = np.linalg.inv(Ac)
+    err = np.abs(X - ref).max() / np.abs(ref).max()
+    res = np.abs(X @ Ac - np.eye(len(Ac))).max()
+    print(f"sphere A_c ({len(Ac)} blocks): blocked inverse vs numpy {err:.2e}, |X A - I| {res:.2e}, pivoted {pivoted}")
+    assert not pivoted
+    assert err <= 1e-10 and res <= 1e-9
+
+
+@pytest.mark.parametrize("n", [1, 31, 33, 257])
+def test_dense_inverse_sizes_and_pivoted_form(n):
+    import torch
+    ctx = make_ctx("amr2_free", device=0)
+    rng = np.random.default_rng(n)
+    # diagonally dominant: the blocked form
+    A = rng.standard_normal((n, n)) + 2 * n * np.eye(n)
+    a = torch.tensor(A, device="cuda")
+    assert not ctx.dense_inverse(a, n // 2)
+    assert np.abs(a.cpu().numpy() @ A - np.eye(n)).max() <= 1e-13
+    if n < 2:
+        return
+    # a scaled cyclic shift (zero diagonal): one pivot block holds it all for
+    # n <= 32 (partial pivoting inside the block); beyond, the first pivot
+    # block has a zero row and the column-wise pivoted form runs
+    B = np.roll(np.diag(1.0 + rng.random(n)), 1, axis=0)
+    b = torch.tensor(B, device="cuda")
+    assert ctx.dense_inverse(b) == (n > 32)
+    assert np.abs(b.cpu().numpy() @ B - np.eye(n)).max() <= 1e-15
+
+
+def test_dense_inverse_singular_matrix_is_an_error():
+    import torch
+    ctx = make_ctx("amr2_free", device=0)
+    a = torch.zeros((40, 40), dtype=torch.float64, device="cuda")
+    with pytest.raises(cup.CupError):
+        ctx.dense_inverse(a)
+    # the context stays usable
+    A = np.eye(40) * 3.0
+    a = torch.tensor(A, device="cuda")
+    assert not ctx.dense_inverse(a)
+    assert np.abs(a.cpu().numpy() - np.eye(40) / 3.0).max() <= 1e-15
