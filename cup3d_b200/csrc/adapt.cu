@@ -211,45 +211,59 @@ int adapt_mesh(cup_ctx* c, int* changed) {
       }
     }
   }
-  // keep the old mesh tables and fields until the transfer has run
-  std::vector<void*> old_mesh, old_fields;
-  old_mesh.swap(c->mesh_arena.ptrs);
-  old_fields.swap(c->field_arena.ptrs);
-  auto free_old = [&]() {
-    cudaStreamSynchronize(c->stream);
-    for (void* q : old_mesh) cudaFree(q);
-    for (void* q : old_fields) cudaFree(q);
-    old_mesh.clear();
-    old_fields.clear();
-  };
+  // The new tables go into the table set not in use, so the transfer can
+  // still read the old mesh's; within the field arena's room the values move
+  // from each field's current buffer to its other one, otherwise into a new
+  // arena (the old one freed after the transfer).
   const DevMesh dm0 = c->dm;
   const Fields F0 = c->F;
   const int nb1 = m1.nb;
+  const int set1 = 1 - c->tab_cur;
   c->mesh = std::move(m1);
-  int rc = ctx_upload_mesh(c);
-  if (!rc) rc = ctx_alloc_fields(c);
-  if (rc) {
+  int rc = ctx_upload_mesh(c, set1);
+  if (rc) return rc;
+  std::vector<void*> old_fields;
+  const bool grow = nb1 > c->field_cap;
+  if (grow) {
+    old_fields.swap(c->field_arena.ptrs);  // F0's buffers stay valid until freed below
+    c->field_cap = 0;
+  }
+  auto free_old = [&]() {
+    if (old_fields.empty()) return;
+    cudaStreamSynchronize(c->stream);
+    for (void* q : old_fields) cudaFree(q);
+    old_fields.clear();
+  };
+  graph_reset(c);
+  c->obst_arena.release();
+  c->ob = DevObstacle();
+  c->proj_open = 0;
+  if ((rc = fields_reserve(c, nb1))) {
     free_old();
     return rc;
   }
-  DevArena tmp;
-  int* d_plan = nullptr;
-  if ((rc = tmp.alloc(&d_plan, plan.size()))) {
-    free_old();
-    return rc;
-  }
-  cudaError_t e = stream_h2d(c->stream, d_plan, plan.data(), plan.size() * sizeof(int32_t));
+  const int vdst = grow ? 0 : 1 - F0.vcur, pdst = grow ? 0 : 1 - F0.pcur;
+  int* d_plan = c->tabs[set1].plan;
+  cudaError_t e = cudaMemcpyAsync(d_plan, plan.data(), plan.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                                  c->stream);
   if (e == cudaSuccess) {
     ProfScope ps("adapt_transfer", c->stream);
     const int grid = std::max(1, std::min(nb1, c->num_sms * 8));
-    k_adapt_transfer<3><<<grid, NT, 0, c->stream>>>(dm0, F0.vel[F0.vcur], nb1, c->F.vel[0], d_plan, true);
-    k_adapt_transfer<1><<<grid, NT, 0, c->stream>>>(dm0, F0.pres[F0.pcur], nb1, c->F.pres[0], d_plan, false);
+    k_adapt_transfer<3><<<grid, NT, 0, c->stream>>>(dm0, F0.vel[F0.vcur], nb1, c->F.vel[vdst], d_plan, true);
+    k_adapt_transfer<1><<<grid, NT, 0, c->stream>>>(dm0, F0.pres[F0.pcur], nb1, c->F.pres[pdst], d_plan, false);
     e = cudaGetLastError();
   }
+  if (e != cudaSuccess) {
+    free_old();
+    return set_cuda_error(e, "adapt_transfer", __FILE__, __LINE__);
+  }
+  c->tab_cur = set1;
+  c->F.vcur = vdst;
+  c->F.pcur = pdst;
+  // the other buffers (the old values, after the transfer in stream order) and the rest zeroed
+  rc = fields_reset(c, true);
   free_old();
-  if (e != cudaSuccess) return set_cuda_error(e, "adapt_transfer", __FILE__, __LINE__);
-  c->F.vcur = 0;
-  c->F.pcur = 0;
+  if (rc) return rc;
   if ((rc = body_recreate(c))) return rc;
   *changed = 1;
   return 0;

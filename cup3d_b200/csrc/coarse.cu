@@ -454,18 +454,27 @@ __global__ void __launch_bounds__(NT) k_coarse_mean(int nb, const double* __rest
 // vector v; when a pivot block has a small pivot or the check fails, the
 // inverse is redone by column-wise Gauss-Jordan with partial pivoting
 // (*fallback = 1).  Returns CUP_ERR_MESH for a singular matrix.
-int device_inverse_dev(double* M, int n, int last, int sms, cudaStream_t s, int* fallback) {
+int device_inverse_dev(double* M, int n, int last, int sms, cudaStream_t s, int* fallback,
+                       InverseScratch* scratch) {
   if (fallback) *fallback = 0;
-  DevArena tmp;
-  double *M0 = nullptr, *Pinv = nullptr, *T = nullptr, *Cp = nullptr, *pv = nullptr;
-  int* flag = nullptr;
+  InverseScratch local;
+  InverseScratch& X = scratch ? *scratch : local;
+  if (X.cap < n) {
+    X.arena.release();
+    X.cap = 0;
+    const size_t cap = scratch ? size_t(n) + n / 4 : size_t(n);
+    if (int rc = X.arena.alloc(&X.M0, cap * cap)) return rc;
+    if (int rc = X.arena.alloc(&X.Pinv, GJB * GJB)) return rc;
+    if (int rc = X.arena.alloc(&X.T, size_t(GJB) * cap)) return rc;
+    if (int rc = X.arena.alloc(&X.Cp, size_t(GJB) * cap)) return rc;
+    if (int rc = X.arena.alloc(&X.pv, 3 * cap)) return rc;
+    if (int rc = X.arena.alloc(&X.flag, 2)) return rc;
+    X.cap = int(cap);
+  }
+  double *M0 = X.M0, *Pinv = X.Pinv, *T = X.T, *Cp = X.Cp, *pv = X.pv;
+  int* flag = X.flag;
   const size_t nn = size_t(n) * n;
-  if (int rc = tmp.alloc(&M0, nn)) return rc;
-  if (int rc = tmp.alloc(&Pinv, GJB * GJB)) return rc;
-  if (int rc = tmp.alloc(&T, size_t(GJB) * n)) return rc;
-  if (int rc = tmp.alloc(&Cp, size_t(GJB) * n)) return rc;
-  if (int rc = tmp.alloc(&pv, 3 * size_t(n))) return rc;
-  if (int rc = tmp.alloc(&flag, 2)) return rc;
+  DevArena tmp;  // the pivoted form's
   CUP_CUDA_TRY(cudaMemcpyAsync(M0, M, nn * sizeof(double), cudaMemcpyDeviceToDevice, s));
   CUP_CUDA_TRY(cudaMemsetAsync(flag, 0, 2 * sizeof(int), s));
   const int vg = std::max(1, std::min(sms * 8, (n + 7) / 8));
@@ -533,7 +542,6 @@ int coarse_build(cup_ctx* c) {
   if (C.nb == nb && C.mesh_version == c->mesh_version) return 0;
   if (nb > kCoarseMaxBlocks)
     return set_error(CUP_ERR_ARG, "two-level preconditioner: more blocks than the dense coarse solve takes (8192)");
-  C.arena.release();
   C.nb = 0;
   cudaStream_t s = c->stream;
   // block graph and its distance-2 colouring
@@ -581,17 +589,34 @@ int coarse_build(cup_ctx* c) {
     for (int j : adj[i])
       if (jmap[size_t(colour[j]) * nb + i] < 0) jmap[size_t(colour[j]) * nb + i] = j;
   }
-  DevArena& A = C.arena;
-  if (int rc = A.alloc(&C.w, nb)) return rc;
-  CUP_CUDA_TRY(stream_h2d(s, C.w, w.data(), nb * sizeof(double)));
-  DevArena tmp;
-  int *d_colour = nullptr, *d_jmap = nullptr;
-  double *d_sum = nullptr, *Ac = nullptr;
+  // storage with room for C.cap blocks, allocated again only to grow
   const size_t nn = size_t(nb) * nb;
-  if (int rc = tmp.alloc(&d_colour, nb)) return rc;
-  if (int rc = tmp.alloc(&d_jmap, jmap.size())) return rc;
-  if (int rc = tmp.alloc(&d_sum, nb)) return rc;
-  if (int rc = tmp.alloc(&Ac, nn)) return rc;
+  if (C.cap < nb) {
+    DevArena& A = C.arena;
+    A.release();
+    C.cap = 0;
+    const size_t cap = size_t(nb) + nb / 4;
+    if (int rc = A.alloc(&C.w, cap)) return rc;
+    if (int rc = A.alloc(&C.rc, cap)) return rc;
+    if (int rc = A.alloc(&C.yc, cap)) return rc;
+    if (int rc = A.alloc(&C.rc2, cap)) return rc;
+    if (int rc = A.alloc(&C.inv, cap * cap)) return rc;
+    if (int rc = A.alloc(&C.ac, cap * cap)) return rc;
+    if (int rc = A.alloc(&C.colour, cap)) return rc;
+    if (int rc = A.alloc(&C.sum, cap)) return rc;
+    C.cap = int(cap);
+  }
+  if (C.jcap < jmap.size()) {
+    C.jarena.release();
+    C.jcap = 0;
+    if (int rc = C.jarena.alloc(&C.jmap, jmap.size() + jmap.size() / 4)) return rc;
+    C.jcap = jmap.size() + jmap.size() / 4;
+  }
+  int* d_colour = C.colour;
+  int* d_jmap = C.jmap;
+  double* d_sum = C.sum;
+  double* Ac = C.ac;
+  CUP_CUDA_TRY(cudaMemcpyAsync(C.w, w.data(), nb * sizeof(double), cudaMemcpyHostToDevice, s));
   CUP_CUDA_TRY(cudaMemcpyAsync(d_colour, colour.data(), nb * sizeof(int), cudaMemcpyHostToDevice, s));
   CUP_CUDA_TRY(cudaMemcpyAsync(d_jmap, jmap.data(), jmap.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   CUP_CUDA_TRY(cudaMemsetAsync(Ac, 0, nn * sizeof(double), s));
@@ -624,17 +649,13 @@ int coarse_build(cup_ctx* c) {
   // thousand blocks)
   {
     int fb = 0;
-    if (int rc = device_inverse_dev(Ac, nb, mode == 1 ? mb : -1, c->num_sms, s, &fb))
+    if (int rc = device_inverse_dev(Ac, nb, mode == 1 ? mb : -1, c->num_sms, s, &fb, &C.iscratch))
       return rc == CUP_ERR_MESH ? set_error(CUP_ERR_MESH, "two-level preconditioner: singular coarse operator") : rc;
     C.pivoted = fb;
-    if (int rc = A.alloc(&C.inv, nn)) return rc;
     k_to_float<<<std::max(1, c->num_sms * 8), NT, 0, s>>>(Ac, nn, C.inv);
     CUP_CUDA_TRY(cudaGetLastError());
     CUP_CUDA_TRY(cudaStreamSynchronize(s));
   }
-  if (int rc = A.alloc(&C.rc, nb)) return rc;
-  if (int rc = A.alloc(&C.yc, nb)) return rc;
-  if (int rc = A.alloc(&C.rc2, nb)) return rc;
   C.nb = nb;
   C.mesh_version = c->mesh_version;
   C.colours = ncol;

@@ -55,34 +55,41 @@ static int keep(cup_ctx* c, int rc) {
   return rc;
 }
 
-int ctx_upload_mesh(cup_ctx* c) {
+int ctx_upload_mesh(cup_ctx* c, int set) {
   Mesh& m = c->mesh;
-  c->mesh_arena.release();
-  int *fk, *fn, *ix, *kerr;
-  double* h;
-  if (int rc = c->mesh_arena.alloc(&kerr, 1)) return rc;
-  CUP_CUDA_TRY(stream_zero(c->stream, kerr, sizeof(int)));
-  if (int rc = c->mesh_arena.alloc(&fk, 6 * size_t(m.nb))) return rc;
-  if (int rc = c->mesh_arena.alloc(&fn, 24 * size_t(m.nb))) return rc;
-  if (int rc = c->mesh_arena.alloc(&ix, 3 * size_t(m.nb))) return rc;
-  if (int rc = c->mesh_arena.alloc(&h, size_t(m.nb))) return rc;
-  CUP_CUDA_TRY(stream_h2d(c->stream, fk, m.face_kind.data(), 6 * size_t(m.nb) * 4));
-  CUP_CUDA_TRY(stream_h2d(c->stream, fn, m.face_nbr.data(), 24 * size_t(m.nb) * 4));
-  CUP_CUDA_TRY(stream_h2d(c->stream, ix, m.index.data(), 3 * size_t(m.nb) * 4));
-  CUP_CUDA_TRY(stream_h2d(c->stream, h, m.h.data(), size_t(m.nb) * 8));
+  if (set < 0) set = c->tab_cur;
+  MeshTables& T = c->tabs[set];
+  if (T.cap < m.nb) {
+    T.arena.release();
+    T.cap = 0;
+    const size_t cap = size_t(m.nb) + m.nb / 4;
+    if (int rc = T.arena.alloc(&T.kerr, 1)) return rc;
+    if (int rc = T.arena.alloc(&T.fk, 6 * cap)) return rc;
+    if (int rc = T.arena.alloc(&T.fn, 24 * cap)) return rc;
+    if (int rc = T.arena.alloc(&T.ix, 3 * cap)) return rc;
+    if (int rc = T.arena.alloc(&T.plan, 9 * cap)) return rc;
+    if (int rc = T.arena.alloc(&T.h, cap)) return rc;
+    T.cap = int(cap);
+  }
+  cudaStream_t s = c->stream;
+  CUP_CUDA_TRY(cudaMemsetAsync(T.kerr, 0, sizeof(int), s));
+  CUP_CUDA_TRY(cudaMemcpyAsync(T.fk, m.face_kind.data(), 6 * size_t(m.nb) * 4, cudaMemcpyHostToDevice, s));
+  CUP_CUDA_TRY(cudaMemcpyAsync(T.fn, m.face_nbr.data(), 24 * size_t(m.nb) * 4, cudaMemcpyHostToDevice, s));
+  CUP_CUDA_TRY(cudaMemcpyAsync(T.ix, m.index.data(), 3 * size_t(m.nb) * 4, cudaMemcpyHostToDevice, s));
+  CUP_CUDA_TRY(cudaMemcpyAsync(T.h, m.h.data(), size_t(m.nb) * 8, cudaMemcpyHostToDevice, s));
   c->dm.nb = m.nb;
   c->dm.mean_block = m.mean_block;
-  c->dm.fkind = fk;
-  c->dm.fnbr = fn;
-  c->dm.index = ix;
-  c->dm.h = h;
-  c->dm.order = nullptr;  // set by alloc_fields
+  c->dm.fkind = T.fk;
+  c->dm.fnbr = T.fn;
+  c->dm.index = T.ix;
+  c->dm.h = T.h;
+  c->dm.order = c->d_order;  // set again by fields_reset
   c->dm.bcase = nullptr;  // set for batches
   c->dm.case_mean = nullptr;
   c->dm.case_dt = nullptr;
   c->dm.case_sums = nullptr;
   c->dm.case_kin = nullptr;
-  c->dm.kerr = kerr;
+  c->dm.kerr = T.kerr;
   ++c->mesh_version;
   return 0;
 }
@@ -95,18 +102,18 @@ int ctx_check_kernels(cup_ctx* c) {
   return 0;
 }
 
-int ctx_alloc_fields(cup_ctx* c) {
+int fields_reserve(cup_ctx* c, int nb) {
+  if (c->field_cap >= nb) return 0;
   graph_reset(c);
   c->field_arena.release();
+  c->field_cap = 0;
   c->d_diag = nullptr;
   c->diag_cap = 0;
-  c->obst_arena.release();
-  c->ob = DevObstacle();
-  const size_t n = nbn(c);
+  c->d_order = nullptr;
+  const int cap = nb + nb / 4;
+  const size_t n = size_t(cap) * BN;
   DevArena& A = c->field_arena;
   Fields& F = c->F;
-  F = Fields();
-  c->proj_open = 0;
   for (int i = 0; i < 2; ++i) {
     if (int rc = A.alloc(&F.vel[i], 3 * n)) return rc;
     if (int rc = A.alloc(&F.pres[i], n)) return rc;
@@ -123,36 +130,57 @@ int ctx_alloc_fields(cup_ctx* c) {
   float** fvecs[] = {&W.fr, &W.frhat, &W.fp, &W.fnu, &W.ft, &W.fz1, &W.fz2, &W.fxs[0], &W.fxs[1], &W.fxs[2], &W.r32};
   for (float** v : fvecs)
     if (int rc = A.alloc(v, n)) return rc;
-  // grid: a few CTAs per SM, never more than blocks
-  W.grid = std::max(1, std::min(c->mesh.nb, c->num_sms * 8));
-  W.ggrid = std::max(1, std::min((c->mesh.nb + GROUPS_PER_CTA - 1) / GROUPS_PER_CTA, c->num_sms * 8));
-  if (int rc = A.alloc(&W.partial, size_t(std::max(W.grid, W.ggrid)) * 8)) return rc;
+  // partial sums for the largest grid of any mesh: a few CTAs per SM, and
+  // the penalization's 1184 CTAs
+  if (int rc = A.alloc(&W.partial, size_t(std::max(c->num_sms * 8, 1184)) * 8)) return rc;
   if (int rc = A.alloc(&W.counters, 32)) return rc;
   if (int rc = A.alloc(&W.bar, 1)) return rc;
   if (int rc = A.alloc(&W.bar_error, 1)) return rc;
   if (int rc = A.alloc(&W.st, 1)) return rc;
   if (int rc = A.alloc(&W.st2, 1)) return rc;
   if (int rc = A.alloc(&W.st_init, 1)) return rc;
-  CUP_CUDA_TRY(stream_zero(c->stream, W.counters, 32 * sizeof(unsigned int)));
-  CUP_CUDA_TRY(stream_zero(c->stream, W.bar, sizeof(unsigned int)));
-  CUP_CUDA_TRY(stream_zero(c->stream, W.bar_error, sizeof(int)));
+  if (int rc = A.alloc(&c->d_order, size_t(cap))) return rc;
+  c->field_cap = cap;
+  return 0;
+}
+
+int fields_reset(cup_ctx* c, bool keep_current) {
+  const size_t n = nbn(c);
+  cudaStream_t s = c->stream;
+  Fields& F = c->F;
+  PoissonWork& W = c->W;
   for (int i = 0; i < 2; ++i) {
-    CUP_CUDA_TRY(stream_zero(c->stream, F.vel[i], 3 * n * 8));
-    CUP_CUDA_TRY(stream_zero(c->stream, F.pres[i], n * 8));
+    if (!keep_current || i != F.vcur) CUP_CUDA_TRY(cudaMemsetAsync(F.vel[i], 0, 3 * n * 8, s));
+    if (!keep_current || i != F.pcur) CUP_CUDA_TRY(cudaMemsetAsync(F.pres[i], 0, n * 8, s));
   }
-  CUP_CUDA_TRY(stream_zero(c->stream, F.tmpV, 3 * n * 8));
-  CUP_CUDA_TRY(stream_zero(c->stream, F.lhs, n * 8));
-  CUP_CUDA_TRY(stream_zero(c->stream, F.chi, n * 8));
-  CUP_CUDA_TRY(stream_zero(c->stream, F.phi, n * 8));
+  CUP_CUDA_TRY(cudaMemsetAsync(F.tmpV, 0, 3 * n * 8, s));
+  CUP_CUDA_TRY(cudaMemsetAsync(F.lhs, 0, n * 8, s));
+  CUP_CUDA_TRY(cudaMemsetAsync(F.chi, 0, n * 8, s));
+  CUP_CUDA_TRY(cudaMemsetAsync(F.phi, 0, n * 8, s));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.counters, 0, 32 * sizeof(unsigned int), s));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
+  CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
+  // grid: a few CTAs per SM, never more than blocks
+  W.grid = std::max(1, std::min(c->mesh.nb, c->num_sms * 8));
+  W.ggrid = std::max(1, std::min((c->mesh.nb + GROUPS_PER_CTA - 1) / GROUPS_PER_CTA, c->num_sms * 8));
   // visit order of the block-group kernels, balanced for the persistent solver's groups
   int groups = 0;
   if (int rc = persistent_solver_groups(c->mesh.nb, W, &groups)) return rc;
   const std::vector<int32_t> order = mesh_visit_order(c->mesh, groups);
-  int* d_order = nullptr;
-  if (int rc = A.alloc(&d_order, order.size())) return rc;
-  CUP_CUDA_TRY(stream_h2d(c->stream, d_order, order.data(), order.size() * sizeof(int32_t)));
-  c->dm.order = d_order;
+  CUP_CUDA_TRY(cudaMemcpyAsync(c->d_order, order.data(), order.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+  c->dm.order = c->d_order;
   return 0;
+}
+
+int ctx_alloc_fields(cup_ctx* c) {
+  graph_reset(c);
+  c->obst_arena.release();
+  c->ob = DevObstacle();
+  c->proj_open = 0;
+  if (int rc = fields_reserve(c, c->mesh.nb)) return rc;
+  c->F.vcur = 0;
+  c->F.pcur = 0;
+  return fields_reset(c, false);
 }
 
 static int install_mesh(cup_ctx* c, const std::vector<std::array<int32_t, 4>>& leaves) {
@@ -367,7 +395,7 @@ cup_ctx* cup_create(const cup_config* cfg) {
 void cup_destroy(cup_ctx* c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  c->mesh_arena.release();
+  for (MeshTables& T : c->tabs) T.arena.release();
   c->field_arena.release();
   c->obst_arena.release();
   if (c->d_scalars) cudaFree(c->d_scalars);

@@ -100,8 +100,17 @@ struct BatchStep {
 
 // Coarse space of the two-level preconditioners (coarse.cu): A_c^-1 of the
 // Galerkin coarse operator (one unknown per block) and the apply buffers.
-struct CoarseSpace {
+// Scratch of the blocked dense inverse (coarse.cu), with room for cap x cap.
+struct InverseScratch {
   DevArena arena;
+  int cap = 0;
+  double *M0 = nullptr, *Pinv = nullptr, *T = nullptr, *Cp = nullptr, *pv = nullptr;
+  int* flag = nullptr;
+};
+
+struct CoarseSpace {
+  DevArena arena;               // the arrays below, with room for cap blocks
+  int cap = 0;
   int nb = 0;                   // blocks it was built for (0: not built)
   int mesh_version = -1;        // cup_ctx::mesh_version it was built for
   int colours = 0;              // colours of the set-up
@@ -110,6 +119,15 @@ struct CoarseSpace {
   double* rc2 = nullptr;        // nb: the second one of the persistent solver
   double* yc = nullptr;         // nb: coarse correction
   double* w = nullptr;          // nb: 512 h^3 of each block
+  // set-up scratch: A_c (FP64, then its inverse in place), colours, block sums,
+  // the per-colour neighbour map (jcap entries)
+  double* ac = nullptr;
+  int* colour = nullptr;
+  double* sum = nullptr;
+  DevArena jarena;
+  size_t jcap = 0;
+  int* jmap = nullptr;
+  InverseScratch iscratch;
   std::vector<double> host_ac;  // A_c (row-major), for checks (kept when keep_host)
   bool keep_host = false;
   int pivoted = 0;              // A_c^-1 came from the column-wise pivoted Gauss-Jordan
@@ -145,6 +163,17 @@ struct BodyState {
   int fix_frame[3] = {0, 0, 0};
 };
 
+// Device copies of a mesh's tables, with room for `cap` blocks; a context
+// keeps two sets, so that a mesh adaptation fills one while its field
+// transfer still reads the other.
+struct MeshTables {
+  DevArena arena;
+  int cap = 0;
+  int *fk = nullptr, *fn = nullptr, *ix = nullptr, *kerr = nullptr;
+  int* plan = nullptr;  // 9 per block: where an adapted mesh's block takes its values from
+  double* h = nullptr;
+};
+
 struct Fields {
   double* vel[2] = {nullptr, nullptr};  // ping-pong, 3*nb*512 each
   int vcur = 0;
@@ -162,7 +191,14 @@ struct cup_ctx {
   cup_config cfg;
   cup3d::Mesh mesh;
   cup3d::DevMesh dm{};
-  cup3d::DevArena mesh_arena, field_arena, obst_arena;
+  cup3d::DevArena field_arena, obst_arena;
+  // mesh tables in two sets (tabs[tab_cur] in use); the field arena holds
+  // room for field_cap blocks and is allocated again only to grow, so a mesh
+  // adaptation within that room allocates and frees nothing
+  cup3d::MeshTables tabs[2];
+  int tab_cur = 0;
+  int field_cap = 0;
+  int* d_order = nullptr;  // the block-group kernels' visit order (field arena)
   cup3d::Fields F;
   cup3d::PoissonWork W{};
   cup3d::DevObstacle ob;
@@ -222,12 +258,21 @@ struct ProfBind {
   ~ProfBind() { t_prof = prev; }  // nested API calls restore the caller's binding
 };
 int ctx_fail(cup_ctx* c, int code, const std::string& msg);
-// Uploads c->mesh and (re)allocates the fields and solver work for it.
-int ctx_upload_mesh(cup_ctx* c);
+// Uploads c->mesh into table set `set` (-1: the set in use) and points the
+// device mesh at it.
+int ctx_upload_mesh(cup_ctx* c, int set = -1);
 // CUP_ERR_CUDA with a message when a staged stencil kernel reported a timed-out
 // wait (call after synchronising the context's stream).
 int ctx_check_kernels(cup_ctx* c);
+// Room for the fields and solver work of c->mesh, all zeroed; the obstacle
+// data dropped.
 int ctx_alloc_fields(cup_ctx* c);
+// Room for nb blocks in the field arena (allocated again, a quarter larger,
+// only when nb exceeds it; then every field pointer changes).
+int fields_reserve(cup_ctx* c, int nb);
+// Zeroes the fields (but vel[vcur] and pres[pcur] when keep_current), sets
+// the launch grids and uploads the visit order of c->mesh.
+int fields_reset(cup_ctx* c, bool keep_current);
 // Installs an obstacle (nslots blocks with chi, udef and kinematics kin[9]).
 int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const double* chi, const double* udef,
                         const double* kin);
@@ -265,7 +310,9 @@ int coarse_build(cup_ctx* c);
 int device_inverse(const double* a, int n, double* d_inv, int sms, cudaStream_t s);
 // The inverse in place of an n x n device matrix, index `last` (>= 0) last in
 // the pivot order; *fallback = 1 when the pivoted column-wise form ran.
-int device_inverse_dev(double* M, int n, int last, int sms, cudaStream_t s, int* fallback);
+// Scratch from `scratch` when given (kept for the next call), else allocated for the call.
+int device_inverse_dev(double* M, int n, int last, int sms, cudaStream_t s, int* fallback,
+                       InverseScratch* scratch = nullptr);
 // The learned map of the current weights for the solver (folds them when they
 // changed; the lab buffer for the current mesh).
 int lmap_prepare(cup_ctx* c, LocalMap* out);

@@ -81,6 +81,39 @@ def test_adapt_mesh_matches_oracle():
     assert np.all(ctx.download("lhs") == 0.0)
 
 
+def test_consecutive_adaptations_match_oracle():
+    # the second and later adaptations move the fields within the storage the
+    # first one sized (each field's other buffer, the other table set) when
+    # the new mesh fits, and into new storage when it does not; both are
+    # compared with the oracle's transfer
+    probe = _setup(1.0, 0.1)
+    ind = probe.adapt_indicator()
+    vals = np.sort(ind[ind < 1e10])
+    rtol, ctol = float(vals[int(0.6 * len(vals))]), float(vals[int(0.4 * len(vals))])
+    ctx = _setup(rtol, ctol)
+    sizes = [ctx.nb]
+    for _ in range(3):
+        m0 = oracle_mesh(ctx)
+        vel0, pres0 = ctx.download("vel"), ctx.download("pres")
+        ref_leaves = m0.adapt_leaves(ctx.adapt_indicator(), rtol, ctol)
+        if not ctx.adapt_mesh():
+            break
+        got = _leaves(ctx)
+        assert sorted(map(tuple, got)) == sorted(map(tuple, ref_leaves))
+        m1 = oracle_mesh(ctx)
+        vref = m0.adapt_transfer(m1, vel0, 3, True)
+        pref = m0.adapt_transfer(m1, pres0, 1, False)
+        assert np.abs(ctx.download("vel") - vref).max() <= 1e-14 * np.abs(vref).max()
+        assert np.abs(ctx.download("pres") - pref).max() <= 1e-14 * np.abs(pref).max()
+        assert np.all(ctx.download("lhs") == 0.0)
+        sizes.append(ctx.nb)
+        # a step runs on the adapted mesh
+        dt, rc, st = ctx.step(len(sizes))
+        assert rc >= 0, st
+    print("blocks through the adaptations:", sizes)
+    assert len(sizes) >= 3
+
+
 def _sphere_run(steps):
     from cup3d_b200.workloads import SPHERE_BODY, SPHERE_FLAGS
     ctx = cup.Context(cup.config(SPHERE_FLAGS + " -levelStart 3 -Rtol 1 -Ctol 0.1 -stepGraph 0", device=0))
