@@ -20,10 +20,14 @@ The timed steps follow the warm-up steps and --settle (50) more.
 `poisson_to_tolerance`  one solve of the seeded right-hand side to 1e-6 and
          1e-10 (FP64 true residual) per solver; the learned network trained
          in the run on the flow's own pressure right-hand sides.
+`learned_re1000`  the network trained above, inside every solver on the
+         sphere at Re=1000, levelMax 5 (5000 blocks): one pressure
+         right-hand side of that flow solved to 1e-6.
 `swarm_batch`  64 independent penalized-ellipsoid cases (372-2659 blocks
          each, 37.5M cells) advanced together by cup_batch_step: 200 steps
-         with the two-level solver, 5 with the block inverse alone; step 0
-         also taken case by case for comparison.
+         with the two-level solver and the bodies moving, 5 with the block
+         inverse alone and the bodies held in place; step 0 also taken case
+         by case for comparison.
 `mesh_adaptation`  from the settled state, three rounds of one adaptation
          (vorticity tagging, refine/compress, field transfer), the two-level
          coarse space of the new mesh, and 20 steps on it (the reference
@@ -219,19 +223,74 @@ def poisson_at_tolerance(ctx, stream, flush, rhs_list, reps=3):
     return res
 
 
-def swarm_batch(flush, steps=5, solver="b200"):
+def learned_re1000(src, flush, settle=30, reps=3):
+    """The learned preconditioner's evaluation case: the network trained on
+    the Re=300 flow (src's weights) inside the solvers of the sphere at
+    Re=1000, levelMax 5 (5000 blocks, 2.56M cells).  That flow is stepped
+    `settle` steps from rest with the two-level solver; its last pressure
+    right-hand side is solved from zero to 1e-6 (FP64 true residual) by
+    every solver, device time, L2 flushed before each solve."""
+    import torch
+    import cup3d_b200 as cup
+    from cup3d_b200.workloads import SPHERE_RE1000_WORKLOAD, make_sphere_re1000_ctx
+    ctx = make_sphere_re1000_ctx(torch.cuda.current_device(), "b200_twolevel")
+    st_ = torch.cuda.ExternalStream(cup._lib.lib().cup_stream(ctx._p))
+    its = []
+    for k in range(settle):
+        _, _, st = ctx.step(k)
+        its.append(st["iterations"])
+    level, index, _ = ctx.blocks()
+    mb = int(np.where((index == 0).all(axis=1))[0][0])
+    b = torch.tensor(ctx.download("lhs"), device="cuda")
+    b[mb * 512] = 0.0  # the mean-constraint row
+    ctx.cnn_init(7)
+    ctx.cnn_set_params(src.cnn_get_params())
+    res = {"workload": SPHERE_RE1000_WORKLOAD, "blocks": ctx.nb, "cells": ctx.nb * 512,
+           "rhs": f"the pressure right-hand side of step {settle - 1} of the Re=1000 flow from rest; x0 = 0",
+           "network": "trained on the Re=300 levelMax 4 flow (poisson_to_tolerance.training), not retrained",
+           "settle_poisson_iterations": its[-5:]}
+    for solver in SOLVERS:
+        runs = []
+        for _ in range(reps):
+            x = torch.zeros_like(b)
+            ctx.set_poisson(solver, 0.0, 1e-6, 1000)
+            with torch.cuda.stream(st_):
+                flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st_)
+            rc, st = ctx.poisson_solve_dev(b, x)
+            e1.record(st_)
+            e1.synchronize()
+            runs.append((e0.elapsed_time(e1), rc, st))
+        runs.sort(key=lambda t: t[0])
+        ms, rc, st = runs[len(runs) // 2]
+        res[f"{solver}@1e-06"] = {"ms": round(ms, 3), "iterations": st["iterations"],
+                                  "true_rel": float(f"{st['true_rel']:.3e}"), "fallback": st["fallback"],
+                                  "status": st["status"], "rc": rc}
+    base = res["b200@1e-06"]["ms"]
+    res["speedup_vs_b200@1e-06"] = {k.split("@")[0]: round(base / v["ms"], 3)
+                                    for k, v in res.items() if k.endswith("@1e-06")}
+    ctx.close()
+    return res
+
+
+def swarm_batch(flush, steps=5, solver="b200", moving=False):
     """The 64-case ellipsoid swarm advanced as one batch (cup_batch_step: one
     set of launches and one Poisson launch per step for all cases), against
     the same cases stepped one by one; device time from CUDA events on the
     stepping streams, L2 flushed before every timed step.  Kernel by kernel
     (-stepGraph 0) on both sides, so that no step pays a graph capture.
     solver: the Poisson solver of every case (b200_twolevel: each case's own
-    coarse space, built when the batch is created, timed apart)."""
+    coarse space, built when the batch is created, timed apart).  moving:
+    every body moves with its velocity (each step advances the cases' poses
+    and creates their chi again inside the timed step), else the bodies are
+    held in place (-StaticObstacles 1)."""
     import torch
     import cup3d_b200 as cup
     from cup3d_b200.workloads import SWARM_WORKLOAD, make_swarm_ctx
     lib = cup._lib.lib()
-    ctxs = [make_swarm_ctx(i, torch.cuda.current_device(), f"-stepGraph 0 -poissonSolver {solver}") for i in range(64)]
+    extra = f"-stepGraph 0 -poissonSolver {solver}" + (" -StaticObstacles 0" if moving else "")
+    ctxs = [make_swarm_ctx(i, torch.cuda.current_device(), extra) for i in range(64)]
     t0 = time.perf_counter()
     batch = cup.Batch(ctxs)
     setup_s = time.perf_counter() - t0
@@ -263,6 +322,7 @@ def swarm_batch(flush, steps=5, solver="b200"):
     batch.close()
     return {
         "workload": SWARM_WORKLOAD, "cases": 64, "cells": ncell, "solver": solver,
+        "bodies": "moving (chi created again every step)" if moving else "held in place",
         "batch_create_s": round(setup_s, 2),
         "metric": "Mcell-steps/s (batched time steps of all cases, FP64)",
         "value": round(ncell * steps / (sum(ms) * 1e-3) / 1e6, 3), "steps": f"1..{steps} after step 0",
@@ -406,7 +466,7 @@ def run_b200(args):
     for k in range(args.warmup + args.settle):
         ctx.step(step)
         step += 1
-        if k % 8 == 7 and len(rhs_list) < 6:
+        if k % 4 == 3 and len(rhs_list) < 12:
             rhs_list.append(ctx.download("lhs"))
     # The timed pass, the per-kernel pass and the end-to-end pass all run the
     # same K steps from the same state (velocity and pressure are the whole
@@ -561,10 +621,13 @@ def run_b200(args):
     }
     if not args.no_poisson:
         line["poisson_to_tolerance"] = poisson_at_tolerance(ctx, stream, flush, rhs_list)
+        if rank == 0:
+            line["learned_re1000"] = learned_re1000(ctx, flush)
     if rank == 0 and not args.no_swarm:
-        # config 5's 200 steps with the two-level solver; 5 steps with the block
-        # inverse alone for comparison
-        line["swarm_batch"] = {s: swarm_batch(flush, steps=n, solver=s) for s, n in (("b200", 5), ("b200_twolevel", 200))}
+        # the swarm's 200 steps with the two-level solver and moving bodies;
+        # 5 steps with the block inverse alone (bodies in place) for comparison
+        line["swarm_batch"] = {s: swarm_batch(flush, steps=n, solver=s, moving=mv)
+                               for s, n, mv in (("b200", 5, False), ("b200_twolevel", 200, True))}
     if rank == 0 and not args.no_obstacle:
         line["obstacle_creation"] = obstacle_creation()
     if rank == 0 and not args.no_cpu_baseline:

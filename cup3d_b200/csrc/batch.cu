@@ -224,6 +224,40 @@ static int batch_step_setup(cup_ctx* c, const std::vector<const cup_ctx*>& cases
   return 0;
 }
 
+// Moving bodies (unless -StaticObstacles): when a case's body moves, every
+// case's pose is advanced and its chi created again at each launched step
+// (batch_bodies_advance), as cup_step does for one case; each case keeps its
+// own BDF2 history.  Free bodies and frames that follow a body stay with
+// single cases.
+static int batch_bodies_setup(cup_ctx* c, const std::vector<const cup_ctx*>& cases) {
+  if (c->cfg.static_obstacles) return 0;
+  bool any = false;
+  for (const cup_ctx* k : cases) any |= body_moves(k);
+  if (!any) return 0;
+  for (size_t k = 0; k < cases.size(); ++k) {
+    const BodyState& B = cases[k]->body;
+    bool frame = false;
+    for (int d = 0; d < 3; ++d) frame |= B.fix_frame[d] != 0;
+    if (body_free(cases[k]) || frame)
+      return set_error(CUP_ERR_ARG, ("batch of cases with moving bodies: case " + std::to_string(k) +
+                                     " has a free body or a frame that follows it (single cases only)").c_str());
+    if (B.kind < 0 && cases[k]->ob.nslots > 0)
+      return set_error(CUP_ERR_ARG, ("batch of cases with moving bodies: case " + std::to_string(k) +
+                                     " holds obstacle data that cannot be created again").c_str());
+  }
+  c->batch_moving = true;
+  c->case_body.clear();
+  c->case_coef.clear();
+  c->case_dt_prev.clear();
+  for (const cup_ctx* k : cases) {
+    c->case_body.push_back(k->body);
+    c->case_coef.push_back({k->coef_u[0], k->coef_u[1], k->coef_u[2]});
+    c->case_dt_prev.push_back(k->dt_prev);
+  }
+  // per-slot force sums for any slot count
+  return c->batch_arena.alloc(&c->T.slot_force, 6 * size_t(c->mesh.nb));
+}
+
 static ObstacleView batch_ob_view(const cup_ctx* c) {
   ObstacleView v;
   v.nslots = c->ob.nslots;
@@ -402,6 +436,7 @@ cup_ctx* cup_batch_create(int32_t ncases, cup_ctx* const* cases) {
   int rc = batch_setup(c, meshes);
   if (rc == 0) rc = copy_case_fields(c, cs);
   if (rc == 0) rc = batch_step_setup(c, cs);
+  if (rc == 0) rc = batch_bodies_setup(c, cs);
   if (rc == 0) rc = batch_coarse_setup(c, cases);
   if (rc) {
     (void)rc;
@@ -448,7 +483,8 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
                    cup_solve_stats* stats) {
   ProfBind pb_(c);
   if (!c || c->ncase < 2 || !dt_used) return ctx_fail(c, CUP_ERR_ARG, "cup_batch_step: not a batch or bad arguments");
-  if (!dt_in && c->cfg.step_graph && !c->prof.on) return batch_graph_step(c, step, dt_used, force, stats);
+  if (!dt_in && c->cfg.step_graph && !c->prof.on && !c->batch_moving)
+    return batch_graph_step(c, step, dt_used, force, stats);
   const int K = c->ncase;
   BatchStep& T = c->T;
   Fields& F = c->F;
@@ -469,6 +505,9 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
     dt_used[k] = dt[k];
   }
   CUP_CUDA_TRY(cudaMemcpyAsync(T.dt, dt.data(), K * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  // CreateObstacles: the cases' bodies at their new poses
+  if (c->batch_moving)
+    if (int rc = batch_bodies_advance(c, step, dt.data())) return keep_err(c, rc);
   // advection-diffusion, penalization, pressure projection: the single-case
   // kernels over all blocks, each block with its case's dt, kinematics and mean
   for (int st = 0; st < 3; ++st) {

@@ -1,6 +1,7 @@
 // Internal definition of cup_ctx (the C-ABI handle).
 #pragma once
 #include <string>
+#include <array>
 #include <vector>
 
 #include "../../include/cup3d_b200.h"
@@ -98,8 +99,6 @@ struct BatchStep {
   void* h_block = nullptr;      // the pinned allocation holding them
 };
 
-// Coarse space of the two-level preconditioners (coarse.cu): A_c^-1 of the
-// Galerkin coarse operator (one unknown per block) and the apply buffers.
 // Scratch of the blocked dense inverse (coarse.cu), with room for cap x cap.
 struct InverseScratch {
   DevArena arena;
@@ -108,6 +107,8 @@ struct InverseScratch {
   int* flag = nullptr;
 };
 
+// Coarse space of the two-level preconditioners (coarse.cu): A_c^-1 of the
+// Galerkin coarse operator (one unknown per block) and the apply buffers.
 struct CoarseSpace {
   DevArena arena;               // the arrays below, with room for cap blocks
   int cap = 0;
@@ -241,6 +242,13 @@ struct cup_ctx {
   // a batch's two-level preconditioners (cup_batch_create with b200_twolevel)
   cup3d::DevArena bcoarse_arena;
   cup3d::BatchCoarse bcoarse;
+  // moving bodies of a batch of cases (batch_bodies_advance): each case's
+  // body, BDF2 coefficients and previous dt; the shapes on the device
+  bool batch_moving = false;
+  std::vector<cup3d::BodyState> case_body;
+  std::vector<std::array<double, 3>> case_coef;
+  std::vector<double> case_dt_prev;
+  void* d_shapes = nullptr;
   // scratch vectors of the pipelined solver (allocated on first use)
   cup3d::DevArena pipe_arena;
   double* pipe_vec[16] = {nullptr};
@@ -299,6 +307,9 @@ int body_advance(cup_ctx* c, int step, double dt);
 // chi of the context's body at its current pose, by the path it was created
 // with, keeping its motion history (after a mesh change).
 int body_recreate(cup_ctx* c);
+// A batch's moving bodies: every case's pose advanced with its dt[k], then all
+// bodies created again on the flattened mesh (obstacles_dev.cu).
+int batch_bodies_advance(cup_ctx* c, int step, const double* dt);
 // Mesh adaptation (adapt.cu): the per-block refinement indicator, and one
 // adaptation of the mesh with the fields moved onto it (*changed = 0 when
 // the mesh stays as it is).

@@ -134,13 +134,14 @@ __device__ __forceinline__ double cta_sum512(double v, double* sm) {
   return s;
 }
 
-__global__ void __launch_bounds__(BN) k_obst_chi(const double* __restrict__ h_, const double* __restrict__ origin,
-                                                  Shape s, const int* __restrict__ slot_of_block,
-                                                  double* __restrict__ chi, double* __restrict__ udef,
-                                                  double* __restrict__ grid_chi, double* __restrict__ mom,
-                                                  const ObstResult* res) {
-  const int b = blockIdx.x, t = threadIdx.x;
-  const int slot = slot_of_block[b];
+// Block b's part of the body: its signed-distance lab, chi and udef = 0 of
+// its slot, the grid chi, the block's four moments (one CTA of 512 threads;
+// ns: the slot count, udef is component-major [3][ns][512]).
+__device__ __forceinline__ void obst_chi_block(int b, const double* __restrict__ h_, const double* __restrict__ origin,
+                                               const Shape& s, int slot, size_t ns, double* __restrict__ chi,
+                                               double* __restrict__ udef, double* __restrict__ grid_chi,
+                                               double* __restrict__ mom) {
+  const int t = threadIdx.x;
   if (slot < 0) {
     grid_chi[size_t(b) * BN + t] = 0.0;
     return;
@@ -172,7 +173,6 @@ __global__ void __launch_bounds__(BN) k_obst_chi(const double* __restrict__ h_, 
     c = (gIX * gUX + gIY * gUY + gIZ * gUZ) / gUSq;
   }
   chi[size_t(slot) * BN + t] = c;
-  const size_t ns = size_t(res->nslots);  // udef is component-major: [3][nslots][512]
   for (int d = 0; d < 3; ++d) udef[(d * ns + slot) * BN + t] = 0.0;
   grid_chi[size_t(b) * BN + t] = 0.0 < c ? c : 0.0;  // std::max(0, chi)
   const double px = ox + (x + 0.5) * h, py = oy + (y + 0.5) * h, pz = oz + (z + 0.5) * h;
@@ -185,6 +185,15 @@ __global__ void __launch_bounds__(BN) k_obst_chi(const double* __restrict__ h_, 
     mom[4 * slot + 2] = m2;
     mom[4 * slot + 3] = m3;
   }
+}
+
+__global__ void __launch_bounds__(BN) k_obst_chi(const double* __restrict__ h_, const double* __restrict__ origin,
+                                                  Shape s, const int* __restrict__ slot_of_block,
+                                                  double* __restrict__ chi, double* __restrict__ udef,
+                                                  double* __restrict__ grid_chi, double* __restrict__ mom,
+                                                  const ObstResult* res) {
+  const int b = blockIdx.x;
+  obst_chi_block(b, h_, origin, s, slot_of_block[b], size_t(res->nslots), chi, udef, grid_chi, mom);
 }
 
 __global__ void __launch_bounds__(BN) k_obst_kin(const double* __restrict__ mom, Shape s, ObstResult* res,
@@ -206,6 +215,84 @@ __global__ void __launch_bounds__(BN) k_obst_kin(const double* __restrict__ mom,
       res->kin[6 + d] = s.omega[d];
     }
     for (int i = 0; i < 9; ++i) kin_out[i] = res->kin[i];
+  }
+}
+
+// ---- moving bodies in a batch of cases -----------------------------------
+// Every case's body created again on the flattened mesh in one pass: the
+// slots of all cases in block order (case k's slots follow case k-1's, and
+// slot_first[k] is the slot count before the case's first block), each
+// block's chi from its case's shape by the single-case arithmetic, and per
+// case the kinematics from its own slots' moments in the single-case order.
+
+__global__ void __launch_bounds__(SLOT_THREADS) k_obst_slots_batch(
+    int nb, const double* __restrict__ h, const double* __restrict__ origin, const Shape* __restrict__ shapes,
+    const int* __restrict__ bcase, const int* __restrict__ first, int ncase, int* __restrict__ slot_of_block,
+    int* __restrict__ block_of_slot, int* __restrict__ slot_first, ObstResult* res) {
+  __shared__ int part[SLOT_THREADS];
+  const int t = threadIdx.x;
+  const int chunk = (nb + SLOT_THREADS - 1) / SLOT_THREADS;
+  const int b0 = min(nb, t * chunk), b1 = min(nb, b0 + chunk);
+  int cnt = 0;
+  for (int b = b0; b < b1; ++b) cnt += block_touches(shapes[bcase[b]], origin, h[b], b) ? 1 : 0;
+  part[t] = cnt;
+  __syncthreads();
+  for (int off = 1; off < SLOT_THREADS; off <<= 1) {
+    const int v = t >= off ? part[t - off] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int slot = part[t] - cnt;
+  for (int b = b0; b < b1; ++b) {
+    const int k = bcase[b];
+    if (b == first[k]) slot_first[k] = slot;
+    if (block_touches(shapes[k], origin, h[b], b)) {
+      slot_of_block[b] = slot;
+      block_of_slot[slot] = b;
+      ++slot;
+    } else {
+      slot_of_block[b] = -1;
+    }
+  }
+  if (t == SLOT_THREADS - 1) {
+    res->nslots = part[t];
+    slot_first[ncase] = part[t];
+  }
+}
+
+__global__ void __launch_bounds__(BN) k_obst_chi_batch(const double* __restrict__ h_, const double* __restrict__ origin,
+                                                        const Shape* __restrict__ shapes, const int* __restrict__ bcase,
+                                                        const int* __restrict__ slot_of_block, double* __restrict__ chi,
+                                                        double* __restrict__ udef, double* __restrict__ grid_chi,
+                                                        double* __restrict__ mom, const ObstResult* res) {
+  const int b = blockIdx.x;
+  const Shape s = shapes[bcase[b]];
+  obst_chi_block(b, h_, origin, s, slot_of_block[b], size_t(res->nslots), chi, udef, grid_chi, mom);
+}
+
+// One CTA per case: its centre of mass from its slots' moments, and its
+// velocities, as k_obst_kin does for one body (kin_out: 9 per case).
+__global__ void __launch_bounds__(BN) k_obst_kin_batch(const double* __restrict__ mom, const Shape* __restrict__ shapes,
+                                                        const int* __restrict__ slot_first,
+                                                        double* __restrict__ kin_out) {
+  __shared__ double sm[16];
+  const int k = blockIdx.x;
+  const int s0 = slot_first[k], n = slot_first[k + 1] - s0;
+  double a[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < n; i += BN)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a[q] += mom[4 * (s0 + i) + q];
+  double tot[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) tot[q] = cta_sum512(a[q], sm);
+  if (threadIdx.x == 0) {
+    double* kn = kin_out + 9 * k;
+    for (int d = 0; d < 3; ++d) {
+      kn[d] = tot[3] > 0 ? tot[d] / tot[3] : 0.0;
+      kn[3 + d] = shapes[k].vel[d];
+      kn[6 + d] = shapes[k].omega[d];
+    }
   }
 }
 
@@ -856,6 +943,88 @@ int body_recreate(cup_ctx* c) {
                      : cup_obstacle_ellipsoid(c, B.pos, B.ax, B.quat, B.vel, B.omega);
   c->body = keep_state;
   return rc;
+}
+
+// Moving bodies of a batch of cases (cup_batch_step): each case's pose
+// advanced by Obstacle::update with the case's own dt and BDF2 coefficients
+// (the order of cup_step: coefU, then the pose), then every body created
+// again on the flattened mesh; the per-case kinematics and slot offsets go
+// to the batch's step buffers.  A case without a body gets an empty box.
+int batch_bodies_advance(cup_ctx* c, int step, const double* dt) {
+  const int K = c->ncase;
+  std::vector<Shape> shapes(K);
+  for (int k = 0; k < K; ++k) {
+    BodyState& B = c->case_body[k];
+    double* cu = c->case_coef[k].data();
+    if (step > c->cfg.step_2nd_start && c->case_dt_prev[k] > 0) {  // Simulation.cpp:361-370
+      const double a = c->case_dt_prev[k], b = dt[k];
+      const double c1 = -(a + b) / (a * b);
+      const double c2 = b / (a + b) / a;
+      cu[0] = -b * (c1 + c2);
+      cu[1] = b * c1;
+      cu[2] = b * c2;
+    }
+    c->case_dt_prev[k] = dt[k];
+    Shape& sh = shapes[k];
+    sh = Shape{};
+    sh.kind = B.kind;
+    if (B.kind < 0) {
+      for (int d = 0; d < 3; ++d) {
+        sh.box[d][0] = 1.0;
+        sh.box[d][1] = 0.0;
+      }
+      continue;
+    }
+    body_update(B, c->cfg.uinf, step, c->cfg.step_2nd_start, cu, dt[k]);
+    const double hmin = c->case_mesh[k].spec.hmin;
+    for (int d = 0; d < 3; ++d) sh.c[d] = B.pos[d];
+    if (B.kind == 0) {
+      sphere_fill_box(B.pos, B.r, hmin, sh.box);
+      sh.r = B.r;
+    } else {
+      quat_lab_to_body(B.quat, sh.L);
+      for (int d = 0; d < 3; ++d) sh.ax[d] = B.ax[d];
+      ellipsoid_fill_box(B.pos, B.ax, hmin, sh.box);
+    }
+    set_kinematics(sh, B.vel, B.omega);
+  }
+  if (int rc = obst_dev_buffers(c)) return rc;
+  if (!c->d_shapes) {
+    unsigned char* p = nullptr;
+    if (int rc = c->batch_arena.alloc(&p, size_t(K) * sizeof(Shape))) return rc;
+    c->d_shapes = p;
+  }
+  Shape* d_shapes = static_cast<Shape*>(c->d_shapes);
+  DevObstacle& o = c->ob;
+  ObstResult* res = static_cast<ObstResult*>(o.d_result);
+  cudaStream_t st = c->stream;
+  const int nb = c->mesh.nb;
+  CUP_CUDA_TRY(cudaMemcpyAsync(d_shapes, shapes.data(), size_t(K) * sizeof(Shape), cudaMemcpyHostToDevice, st));
+  {
+    ProfScope ps("obstacle_slots", st);
+    k_obst_slots_batch<<<1, SLOT_THREADS, 0, st>>>(nb, c->dm.h, o.d_origin, d_shapes, c->dm.bcase, c->T.first, K,
+                                                  o.slot_of_block, o.block_of_slot, c->T.slot_first, res);
+  }
+  {
+    ProfScope ps("obstacle_near", st);
+    k_obst_near<<<std::max(1, std::min((nb + 255) / 256, c->num_sms * 4)), 256, 0, st>>>(c->dm, o.slot_of_block,
+                                                                                       o.near);
+  }
+  {
+    ProfScope ps("obstacle_chi", st);
+    k_obst_chi_batch<<<nb, BN, 0, st>>>(c->dm.h, o.d_origin, d_shapes, c->dm.bcase, o.slot_of_block, o.chi, o.udef,
+                                         c->F.chi, o.d_mom, res);
+  }
+  {
+    ProfScope ps("obstacle_kin", st);
+    k_obst_kin_batch<<<K, BN, 0, st>>>(o.d_mom, d_shapes, c->T.slot_first, c->T.kin);
+  }
+  CUP_CUDA_TRY(cudaGetLastError());
+  ObstResult h{};
+  CUP_CUDA_TRY(stream_d2h(st, &h, res, sizeof(h)));
+  o.nslots = h.nslots;
+  o.host_stale = true;
+  return 0;
 }
 
 // Host copies of a device-created obstacle (slot list, chi, udef), fetched

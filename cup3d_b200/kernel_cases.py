@@ -5,6 +5,7 @@
     python -m cup3d_b200.kernel_cases step    # 4 full time steps of the sphere workload
     python -m cup3d_b200.kernel_cases swarm   # 16 iterations of a batched solve over 8 swarm cases
     python -m cup3d_b200.kernel_cases learned # 20 training steps, then 16 iterations of the learned solve
+    python -m cup3d_b200.kernel_cases adapt   # 20 two-level steps, one mesh adaptation, the coarse rebuild, 1 step
 
 A second argument names the Poisson solver of the sphere cases (default
 b200; e.g. b200_twolevel).
@@ -80,8 +81,21 @@ def main(argv):
         ctx.set_poisson("b200_learned", 0.0, 1e-30, 16)
         rc, st = ctx.poisson_solve_dev(b, x)
         print(f"learned ok: rc {rc}, {st['iterations']} iterations, {ctx.cnn_dataset_size()} samples")
+    elif case == "adapt":
+        # the settled sphere flow adapted once (vorticity tagging), then the
+        # two-level coarse space of the new mesh (A_c by colours, the blocked
+        # inverse) built by the first coarse application, then one step
+        for step in range(20):
+            ctx.step(step)
+        changed = ctx.adapt_mesh()
+        r = torch.ones(ctx.nb * 512, dtype=torch.float64, device="cuda")
+        z = torch.zeros_like(r)
+        ctx.coarse_apply(r, z)
+        ctx.step(20)
+        torch.cuda.synchronize()
+        print(f"adapt ok: changed {changed}, {ctx.nb} blocks")
     else:
-        raise SystemExit(f"unknown case {case!r}: spmv | solve | step | learned | swarm")
+        raise SystemExit(f"unknown case {case!r}: spmv | solve | step | learned | adapt | swarm")
 
 
 if __name__ == "__main__":

@@ -114,6 +114,24 @@ def make_sphere_ctx(device, solver="b200"):
     return ctx
 
 
+# The learned preconditioner's evaluation case: the same sphere at Re=1000
+# (nu = 0.1*0.125/1000), levelMax 5, the mesh frozen after the same
+# refinement rule (5000 blocks, 2.56M cells).
+SPHERE_RE1000_FLAGS = (SPHERE_FLAGS.replace("-levelMax 4", "-levelMax 5")
+                       .replace("-nu 4.1666666666666667e-05", "-nu 1.25e-05"))
+SPHERE_RE1000_WORKLOAD = "sphere_re1000_amr_levelmax5_weno5_fp64"
+
+
+def make_sphere_re1000_ctx(device, solver="b200"):
+    """Context with the Re=1000, levelMax 5 sphere mesh and the sphere obstacle."""
+    import cup3d_b200 as cup
+    cfg = cup.config(SPHERE_RE1000_FLAGS + f" -poissonSolver {solver}", device=device)
+    ctx = cup.Context(cfg)
+    ctx.set_mesh_sphere_wake(**SPHERE_MESH)
+    ctx.obstacle_sphere(**SPHERE_BODY)
+    return ctx
+
+
 def poisson_rhs(ctx):
     """Seeded Poisson right-hand side on the context's mesh: N(0,1) white
     noise per cell plus 8 Gaussian sources (centres uniform in the sphere's

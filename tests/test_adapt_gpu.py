@@ -82,22 +82,26 @@ def test_adapt_mesh_matches_oracle():
 
 
 def test_consecutive_adaptations_match_oracle():
-    # the second and later adaptations move the fields within the storage the
-    # first one sized (each field's other buffer, the other table set) when
-    # the new mesh fits, and into new storage when it does not; both are
-    # compared with the oracle's transfer
-    probe = _setup(1.0, 0.1)
-    ind = probe.adapt_indicator()
-    vals = np.sort(ind[ind < 1e10])
+    # refine (new storage), compress with the flow scaled down (the storage
+    # the first adaptation sized: each field's other buffer, the other table
+    # set), refine again (within that storage); every transfer compared with
+    # the oracle's.  No body: its interface marks would keep blocks refined.
+    def setup(rtol, ctol):
+        ctx = make_ctx("amr2_free", device=0, extra=f"-Rtol {rtol} -Ctol {ctol}")
+        ctx.upload("vel", _flow(ctx))
+        xyz, _ = cell_centres(ctx)
+        ctx.upload("pres", np.cos(3 * xyz[:, 0]) * np.sin(2 * xyz[:, 2]))
+        return ctx
+    vals = np.sort(setup(1.0, 0.1).adapt_indicator())
     rtol, ctol = float(vals[int(0.6 * len(vals))]), float(vals[int(0.4 * len(vals))])
-    ctx = _setup(rtol, ctol)
+    ctx = setup(rtol, ctol)
     sizes = [ctx.nb]
-    for _ in range(3):
+    for scale in (1.0, 0.01, 1.0):
+        ctx.upload("vel", _flow(ctx) * scale)
         m0 = oracle_mesh(ctx)
         vel0, pres0 = ctx.download("vel"), ctx.download("pres")
         ref_leaves = m0.adapt_leaves(ctx.adapt_indicator(), rtol, ctol)
-        if not ctx.adapt_mesh():
-            break
+        assert ctx.adapt_mesh()
         got = _leaves(ctx)
         assert sorted(map(tuple, got)) == sorted(map(tuple, ref_leaves))
         m1 = oracle_mesh(ctx)
@@ -107,11 +111,11 @@ def test_consecutive_adaptations_match_oracle():
         assert np.abs(ctx.download("pres") - pref).max() <= 1e-14 * np.abs(pref).max()
         assert np.all(ctx.download("lhs") == 0.0)
         sizes.append(ctx.nb)
-        # a step runs on the adapted mesh
-        dt, rc, st = ctx.step(len(sizes))
-        assert rc >= 0, st
     print("blocks through the adaptations:", sizes)
-    assert len(sizes) >= 3
+    assert sizes[1] > sizes[0] and sizes[2] < sizes[1] and sizes[3] > sizes[2]
+    # a step on the last mesh
+    dt, rc, st = ctx.step(1)
+    assert rc >= 0, st
 
 
 def _sphere_run(steps):

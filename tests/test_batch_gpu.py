@@ -13,7 +13,9 @@
 * the single-case entry points refuse a batch;
 * time steps of a batch (own dt, obstacle, mean and solve per case) match
   the same cases stepped one by one, and replayed from a CUDA graph they
-  match the kernel-by-kernel batch step bit for bit.
+  match the kernel-by-kernel batch step bit for bit;
+* with moving bodies each case's pose and chi follow those of the case
+  stepped alone, chi bit for bit.
 """
 import numpy as np
 import pytest
@@ -134,8 +136,9 @@ def _smooth_velocity(ctx, phase):
                            0.3 * np.sin(y + z + phase)])
 
 
-def _step_cases(extra=""):
-    flags = "-poissonTol 0 -poissonTolRel 1e-11 -nu 0.01 -CFL 0.3 -rampup 0 -advection weno5 " + extra
+def _step_cases(extra="", static=True):
+    flags = ("-poissonTol 0 -poissonTolRel 1e-11 -nu 0.01 -CFL 0.3 -rampup 0 -advection weno5 "
+             f"-StaticObstacles {1 if static else 0} " + extra)
     a = make_ctx("tgv32", device=0, extra=flags)
     xyz, _ = a.cell_centres()
     x, y, z = xyz.T
@@ -192,6 +195,36 @@ def test_captured_batch_steps_match_launched_batch_steps():
         assert [s["iterations"] for s in st1] == [s["iterations"] for s in st0], step
         assert np.array_equal(batches[0].download("vel"), batches[1].download("vel")), step
         assert np.array_equal(batches[0].download("pres"), batches[1].download("pres")), step
+
+
+def test_moving_batch_matches_single_cases():
+    # bodies that move (-StaticObstacles 0): every batch step advances each
+    # case's pose with the case's own dt and BDF2 history and creates all
+    # bodies again on the flattened mesh; each case stepped alone by
+    # cup_step with the batch's dt moves its body the same way.  chi bit for
+    # bit at every step (the same creation arithmetic), velocity and
+    # pressure within the solver-order tolerances of the static comparison
+    singles = _step_cases("-stepGraph 0", static=False)
+    batch = cup.Batch(_step_cases(static=False))
+    chi0 = [batch.case_field("chi", k)[0].copy() for k in range(batch.ncase)]
+    for step in range(4):
+        rc, dts, forces, stats = batch.step(step)
+        assert rc == 0 and all(s["status"] == 1 for s in stats), (step, stats)
+        for k, s in enumerate(singles):
+            dt1, rc1, st1 = s.step(step, dt=dts[k])
+            assert rc1 == 0 and dt1 == dts[k]
+            assert np.array_equal(batch.case_field("chi", k)[0], s.download("chi")), (step, k)
+            u1 = s.download("vel").reshape(3, -1)
+            ub = batch.case_field("vel", k)
+            scale = np.abs(u1).max()
+            assert np.abs(ub - u1).max() <= 1e-8 * scale, (step, k, np.abs(ub - u1).max() / scale)
+            p1 = s.download("pres")
+            pb = batch.case_field("pres", k)[0]
+            assert np.abs(pb - p1).max() <= 1e-7 * np.abs(p1).max(), (step, k)
+    # the bodies moved: chi changed in the cases with a body
+    assert np.array_equal(batch.case_field("chi", 0)[0], chi0[0])
+    for k in (1, 2):
+        assert not np.array_equal(batch.case_field("chi", k)[0], chi0[k]), k
 
 
 def test_batch_with_a_single_block_case():
