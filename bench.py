@@ -307,7 +307,12 @@ def swarm_batch(flush, steps=5, solver="b200", moving=False):
         e1.synchronize()
         return e0.elapsed_time(e1), out
 
-    # step 0 of every case, one by one and as the batch, from the same state
+    # step 0 of every case, one by one and as the batch, from the same state;
+    # each case's coarse space built before (as the batch's is at creation)
+    if solver == "b200_twolevel":
+        for c in ctxs:
+            r = torch.ones(c.nb * 512, dtype=torch.float64, device="cuda")
+            c.coarse_apply(r, torch.zeros_like(r))
     single_ms = 0.0
     for c in ctxs:
         single_ms += timed(c, lambda: c.step(0))[0]

@@ -905,24 +905,8 @@ __device__ __forceinline__ void coarse_restrict(const double c[8], double* rc, i
 template <class T>
 __device__ __forceinline__ double coarse_block_row(const KArgs<T>& A, const GroupIdx& G, int b, const float* row,
                                                    const double* rc, int n, T* v, double* gsm) {
-  // the row in 16-byte loads with two partial sums where row and rc are
-  // 16-byte aligned (every row when n % 4 == 0), else one value at a time
-  double a0 = 0.0, a1 = 0.0;
-  int j0 = 0;
-  if (((reinterpret_cast<uintptr_t>(row) | reinterpret_cast<uintptr_t>(rc)) & 15) == 0) {
-    const int n4 = n >> 2;
-    const float4* r4 = reinterpret_cast<const float4*>(row);
-    const double2* c2 = reinterpret_cast<const double2*>(rc);
-    for (int j = G.lane; j < n4; j += GROUP) {
-      const float4 w = r4[j];
-      const double2 x0 = __ldcg(c2 + 2 * j), x1 = __ldcg(c2 + 2 * j + 1);
-      a0 = fma(double(w.y), x0.y, fma(double(w.x), x0.x, a0));
-      a1 = fma(double(w.w), x1.y, fma(double(w.z), x1.x, a1));
-    }
-    j0 = 4 * n4;
-  }
-  for (int j = j0 + G.lane; j < n; j += GROUP) a0 = fma(double(row[j]), __ldcg(rc + j), a0);
-  double s[1] = {a0 + a1};
+  double s[1] = {0.0};
+  for (int j = G.lane; j < n; j += GROUP) s[0] += double(row[j]) * __ldcg(rc + j);
   group_reduce<1>(s, gsm, G);
   const double yc = s[0];
   double c[8];

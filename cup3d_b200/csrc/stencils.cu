@@ -63,19 +63,6 @@ __device__ __forceinline__ double deriv(double U, double um3, double um2, double
   return (2 * up3 - 15 * up2 + 60 * up1 - 20 * u - 30 * um1 + 3 * um2) / 60.;
 }
 
-// The face value of deriv<1> at face k of a lab line (the lower face of the
-// line's cell k, upwind side p), its inputs read from the 3-layer star lab:
-// the line's cells at base + i stride, ghost layer l below at glo + (l-1) 64,
-// above at ghi + (l-1) 64.  For the rare faces where the upwind side flips.
-__device__ __noinline__ double weno_face_lab(const double* Lc, int base, int stride, int glo, int ghi, int k, bool p) {
-  double w[6];
-  for (int i = 0; i < 6; ++i) {
-    const int q = k - 3 + i;  // positions k-3 .. k+2
-    w[i] = Lc[q < 0 ? glo + (-q - 1) * 64 : (q >= BS ? ghi + (q - BS) * 64 : base + q * stride)];
-  }
-  return weno5_left(p ? w[0] : w[5], p ? w[1] : w[4], p ? w[2] : w[3], p ? w[3] : w[2], p ? w[4] : w[1]);
-}
-
 __device__ __forceinline__ bool has_finer(const DevMesh& M, int b) {
   bool r = false;
 #pragma unroll
@@ -149,91 +136,106 @@ __global__ void __launch_bounds__(NT, 3)
       }
     }
     if (SCHEME == 1) {
-      // WENO5 along lines.  Per direction d, one thread per (component c,
-      // line of 8 cells along d) loads the line's 14 values (its cells and
-      // three ghosts each side) and the cells' upwind sides, reconstructs the
-      // 9 face values of the line once each (face j is the upper face of
-      // cell j-1 with that cell's upwind side, face 0 the lower face of cell
-      // 0 with its side), and adds u_d (F_upper - F_lower) into adv[c][cell].
-      // A cell whose upwind side differs from the cell below it takes its
-      // lower face with its own side (read again from shared memory).  The
-      // face values are those of deriv<1>: the same reconstruction of the
-      // same inputs.  Meanwhile the other 64 threads add the diffusion of
-      // component d into corr (on top of the flux correction of a block with
-      // finer faces).
-      double* adv = corr + 3 * BN;  // 3 x 512: sum over d of u_d dF/dx_d
+      // WENO5: each face value is reconstructed once where the cells on both
+      // sides take the same upwind side.  Per direction: every cell
+      // reconstructs its upper face into fbuf; the lower faces of the first
+      // cells of the lines go to fstart; a cell then takes its lower face from
+      // the cell below, or reconstructs it itself where the upwind sign flips.
+      // The face values are those of deriv<1> (the same reconstruction of the
+      // same inputs), so the result does not change.
+      double* fbuf = corr + 3 * BN;   // 3 x 512: upper faces along the current direction
+      double* fstart = fbuf + 3 * BN; // 3 x 64: lower faces of the lines' first cells
+      auto L = [&](int c, int xx, int yy, int zz) { return lab[c * LG::V + LG::at(xx, yy, zz)]; };
+      double der[2][3][3];  // [cell slot][component][direction]
+      auto direction = [&](auto dconst) {
+        constexpr int d = decltype(dconst)::value;
+        constexpr int stride = d == 0 ? 1 : (d == 1 ? 8 : 64);
+        // reconstruction at the upper face of cell (p0, p1, p2) along d with
+        // the upwind side pos, as deriv<1>'s fp
+        auto face_up = [&](int c, int p0, int p1, int p2, bool pos) {
+          auto at = [&](int k) {
+            return L(c, p0 + (d == 0 ? k : 0), p1 + (d == 1 ? k : 0), p2 + (d == 2 ? k : 0));
+          };
+          const double um2 = at(-2), um1 = at(-1), u0 = at(0), up1 = at(1), up2 = at(2), up3 = at(3);
+          return weno5_left(pos ? um2 : up3, pos ? um1 : up2, pos ? u0 : up1, pos ? up1 : u0, pos ? up2 : um1);
+        };
 #pragma unroll 1
-      for (int d = 0; d < 3; ++d) {
+        for (int qq = 0; qq < 2; ++qq) {
+          const int cell = threadIdx.x + qq * NT;
+          const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+          const bool pos = L(d, x, y, z) + ui.v[d] > 0;
+#pragma unroll 1
+          for (int c = 0; c < 3; ++c) fbuf[c * BN + cell] = face_up(c, x, y, z, pos);
+        }
         if (threadIdx.x < 3 * 64) {
           const int c = threadIdx.x >> 6, line = threadIdx.x & 63;
-          const int a = line & 7, bb = line >> 3;
-          const int stride = d == 0 ? 1 : (d == 1 ? 8 : 64);
-          const int base = d == 0 ? 8 * a + 64 * bb : (d == 1 ? a + 64 * bb : a + 8 * bb);
-          // ghost layers l = 1..3 below and above (LabGeom's face order)
-          const int glo = BN + (2 * d) * 3 * 64 + line, ghi = BN + (2 * d + 1) * 3 * 64 + line;
-          const double* Lc = lab + c * LG::V;
-          const double* Ld = lab + d * LG::V;
-          double v[14];  // positions -3 .. 10 along the line
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            v[2 - k] = Lc[glo + k * 64];
-            v[11 + k] = Lc[ghi + k * 64];
-          }
-#pragma unroll
-          for (int k = 0; k < 8; ++k) v[3 + k] = Lc[base + k * stride];
-          double ua[8];
-          bool pos[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            ua[k] = Ld[base + k * stride] + ui.v[d];
-            pos[k] = ua[k] > 0;
-          }
-          // face j (positions j-3 .. j+2) with upwind side p, as deriv<1>'s fp
-          auto F = [&](int j, bool p) {
-            return weno5_left(p ? v[j] : v[j + 5], p ? v[j + 1] : v[j + 4], p ? v[j + 2] : v[j + 3],
-                              p ? v[j + 3] : v[j + 2], p ? v[j + 4] : v[j + 1]);
-          };
-          double fu[9];
-          fu[0] = F(0, pos[0]);
-#pragma unroll
-          for (int j = 1; j <= 8; ++j) fu[j] = F(j, pos[j - 1]);
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            double lower = fu[k];
-            if (k > 0 && pos[k - 1] != pos[k]) lower = weno_face_lab(Lc, base, stride, glo, ghi, k, pos[k]);
-            const double t = ua[k] * (fu[k + 1] - lower);
-            double& acc = adv[c * BN + base + k * stride];
-            acc = d == 0 ? t : acc + t;
-          }
-        } else {
-          auto L = [&](int xx, int yy, int zz) { return lab[d * LG::V + LG::at(xx, yy, zz)]; };
-          for (int cell = threadIdx.x - 3 * 64; cell < BN; cell += NT - 3 * 64) {
-            const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
-            const double sx = L(x + 1, y, z) + L(x - 1, y, z);
-            const double sy = L(x, y + 1, z) + L(x, y - 1, z);
-            const double sz = L(x, y, z + 1) + L(x, y, z - 1);
-            double dD;
-            if (d == 0)
-              dD = (sx + (sy + sz)) - 6 * L(x, y, z);
-            else if (d == 1)
-              dD = (sy + (sz + sx)) - 6 * L(x, y, z);
-            else
-              dD = (sz + (sx + sy)) - 6 * L(x, y, z);
-            double& cr = corr[d * BN + cell];
-            cr = (fix ? cr : 0.0) + facD * dD;
-          }
+          const int t1 = line & 7, t2 = line >> 3;
+          const int x = d == 0 ? 0 : t1, y = d == 1 ? 0 : (d == 0 ? t1 : t2), z = d == 2 ? 0 : t2;
+          const bool pos = L(d, x, y, z) + ui.v[d] > 0;  // the first cell's side
+          fstart[c * 64 + line] = face_up(c, x - (d == 0), y - (d == 1), z - (d == 2), pos);
         }
         __syncthreads();
-      }
+#pragma unroll
+        for (int qq = 0; qq < 2; ++qq) {
+          const int cell = threadIdx.x + qq * NT;
+          const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+          const int pd = d == 0 ? x : (d == 1 ? y : z);
+          const bool pos = L(d, x, y, z) + ui.v[d] > 0;
+          double fm[3];
+          if (pd == 0) {
+            const int line = d == 0 ? y + 8 * z : (d == 1 ? x + 8 * z : x + 8 * y);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) fm[c] = fstart[c * 64 + line];
+          } else {
+            const int xm = x - (d == 0), ym = y - (d == 1), zm = z - (d == 2);
+            const bool pos_m = L(d, xm, ym, zm) + ui.v[d] > 0;
+            if (pos_m == pos) {
+#pragma unroll
+              for (int c = 0; c < 3; ++c) fm[c] = fbuf[c * BN + cell - stride];
+            } else {  // the upwind side flips between the two cells
+#pragma unroll
+              for (int c = 0; c < 3; ++c) fm[c] = face_up(c, xm, ym, zm, pos);
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) der[qq][c][d] = fbuf[c * BN + cell] - fm[c];
+        }
+        __syncthreads();
+      };
+      direction(std::integral_constant<int, 0>{});
+      direction(std::integral_constant<int, 1>{});
+      direction(std::integral_constant<int, 2>{});
 #pragma unroll 1
       for (int qq = 0; qq < 2; ++qq) {
         const int cell = threadIdx.x + qq * NT;
+        const int x = cell & 7, y = (cell >> 3) & 7, z = cell >> 6;
+        const double uA[3] = {L(0, x, y, z) + ui.v[0], L(1, x, y, z) + ui.v[1], L(2, x, y, z) + ui.v[2]};
+        double out[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const double dx = der[qq][c][0], dy = der[qq][c][1], dz = der[qq][c][2];
+          const double sx = L(c, x + 1, y, z) + L(c, x - 1, y, z);
+          const double sy = L(c, x, y + 1, z) + L(c, x, y - 1, z);
+          const double sz = L(c, x, y, z + 1) + L(c, x, y, z - 1);
+          double dD, dA;
+          if (c == 0) {
+            dD = (sx + (sy + sz)) - 6 * L(0, x, y, z);
+            dA = uA[0] * dx + (uA[1] * dy + uA[2] * dz);
+          } else if (c == 1) {
+            dD = (sy + (sz + sx)) - 6 * L(1, x, y, z);
+            dA = uA[1] * dy + (uA[2] * dz + uA[0] * dx);
+          } else {
+            dD = (sz + (sx + sy)) - 6 * L(2, x, y, z);
+            dA = uA[2] * dz + (uA[0] * dx + uA[1] * dy);
+          }
+          out[c] = facA * dA + facD * dD;
+        }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const size_t gi = c * n + size_t(b) * BN + cell;
-          // advection, then diffusion and flux correction (corr)
-          const double tot = ((stage ? tmpV[gi] : 0.0) + facA * adv[c * BN + cell]) + corr[c * BN + cell];
-          vout[gi] = lab[c * LG::V + cell] + tot * (alpha / h3);
+          double tot = (stage ? tmpV[gi] : 0.0) + out[c];
+          if (fix) tot += corr[c * BN + cell];
+          vout[gi] = L(c, x, y, z) + tot * (alpha / h3);
           if (stage < 2) tmpV[gi] = tot * beta;
         }
       }
@@ -287,8 +289,8 @@ __global__ void __launch_bounds__(NT, 3)
 
 int launch_advect_stage(const DevMesh& M, const double* vin, double* vout, double* tmpV, double dt, double nu,
                         const double* uinf, int scheme, int stage, int grid, cudaStream_t s) {
-  // lab, flux correction (WENO5: and diffusion); WENO5 adds the advective sums (3 x 512)
-  const size_t smem = (3 * LabGeom<3>::V + 3 * BN + (scheme == 1 ? 3 * BN : 0)) * sizeof(double);
+  // lab, flux correction; WENO5 adds the face buffers (3 x 512 + 3 x 64)
+  const size_t smem = (3 * LabGeom<3>::V + 3 * BN + (scheme == 1 ? 3 * BN + 3 * 64 : 0)) * sizeof(double);
   static unsigned long long attr_set[2] = {0, 0};
   Vec3 ui{{uinf[0], uinf[1], uinf[2]}};
   if (scheme == 1) {

@@ -191,7 +191,7 @@ def make_swarm_ctx(i, device, extra=""):
     ctx = cup.Context(cfg)
     ctx.set_mesh_sphere_wake(p["center"], SWARM_AXES[0], 1, near_radius=0.6, wake_len=0.0, wake_radius=0.6)
     if device >= 0:
-        ctx.obstacle_ellipsoid(p["center"], SWARM_AXES, p["quat"], vel=p["vel"])
+        ctx.obstacle_ellipsoid(p["center"], SWARM_AXES, p["quat"], vel=p["vel"], on_device=True)
     return ctx
 
 
