@@ -200,8 +200,12 @@ int cup_batch_poisson_solve_dev(cup_ctx* batch, const double* d_b, double* d_x, 
  * the case's own max |u| and finest spacing).  dt_used[ncases]; force[6 ncases]
  * (penalization force and torque per case, may be NULL); stats[ncases] (may
  * be NULL).  The Poisson solves of all cases run in one device launch.
- * Bodies stay where the cases had them when the batch was made (as with
- * -StaticObstacles 1); moving bodies are stepped by cup_step on single cases. */
+ * Bodies move unless -StaticObstacles 1: when a case's sphere or ellipsoid
+ * moves, every step advances each case's pose with that case's dt
+ * (Obstacle::update, the case's own BDF2 history) and creates every body
+ * again at its new pose, as cup_step does for one case; such a batch steps
+ * kernel by kernel.  cup_batch_create refuses free bodies and frames that
+ * follow a body when bodies move. */
 int cup_batch_step(cup_ctx* batch, int32_t step, const double* dt_in, double* dt_used, double* force,
                    cup_solve_stats* stats);
 
