@@ -209,6 +209,7 @@ static int batch_step_setup(cup_ctx* c, const std::vector<const cup_ctx*>& cases
   std::vector<double> hmin(K);
   for (int k = 0; k < K; ++k) hmin[k] = c->case_mesh[k].spec.hmin;
   if (int rc = A.alloc(&T.hmin, size_t(K))) return rc;
+  if (int rc = A.alloc(&T.mixed, 2 * size_t(K))) return rc;
   CUP_CUDA_TRY(stream_h2d(c->stream, T.hmin, hmin.data(), K * sizeof(double)));
   if (int rc = A.alloc(&c->B.st_init, size_t(K))) return rc;
   // pinned host copies for captured steps
@@ -279,6 +280,22 @@ static SolveParams batch_params(const cup_ctx* c) {
   P.persistent = 1;
   P.block_cache = c->cfg.poisson_block_cache;
   return P;
+}
+
+// The batch's Poisson solve: FP64 (block inverse, or two-level when the
+// cases' coarse spaces were built), or mixed precision (-poissonSolver
+// b200_mixed: FP32 batched inner solves, FP64 refinement per case).  The
+// learned, Schwarz and pipelined solvers are single-case only.
+static int batch_solve(cup_ctx* c, const double* b, double* x, const SolveParams& P, SolveStats* S) {
+  const int sv = c->cfg.poisson_solver;
+  if (sv == CUP_POISSON_B200_LEARNED || sv == CUP_POISSON_B200_LEARNED_MIXED || sv == CUP_POISSON_B200_SCHWARZ ||
+      sv == CUP_POISSON_B200_PIPELINED)
+    return set_error(CUP_ERR_ARG, "batch of cases: the learned, Schwarz and pipelined solvers are single-case only "
+                                  "(b200, b200_mixed, b200_twolevel)");
+  if (sv == CUP_POISSON_B200_MIXED)
+    return poisson_mixed_batched(c->dm, b, x, P, c->W, c->B, S, c->stream, batch_coarse(c), c->T.first,
+                                 c->case_first.data(), c->T.bscratch, c->T.mixed);
+  return poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S, c->stream, batch_coarse(c));
 }
 
 // Worst outcome over the cases, stats per case.
@@ -470,8 +487,7 @@ int cup_batch_poisson_solve_dev(cup_ctx* c, const double* b, double* x, cup_solv
   const SolveParams P = batch_params(c);
   std::vector<SolveStats> S(c->ncase);
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
-  if (int rc = poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S.data(), c->stream, batch_coarse(c)))
-    return keep_err(c, rc);
+  if (int rc = batch_solve(c, b, x, P, S.data())) return keep_err(c, rc);
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   CUP_CUDA_TRY(cudaEventSynchronize(c->ev1));
   float ms = 0;
@@ -483,7 +499,8 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
                    cup_solve_stats* stats) {
   ProfBind pb_(c);
   if (!c || c->ncase < 2 || !dt_used) return ctx_fail(c, CUP_ERR_ARG, "cup_batch_step: not a batch or bad arguments");
-  if (!dt_in && c->cfg.step_graph && !c->prof.on && !c->batch_moving)
+  const bool fp64 = c->cfg.poisson_solver == CUP_POISSON_B200 || c->cfg.poisson_solver == CUP_POISSON_B200_TWOLEVEL;
+  if (!dt_in && c->cfg.step_graph && !c->prof.on && !c->batch_moving && fp64)
     return batch_graph_step(c, step, dt_used, force, stats);
   const int K = c->ncase;
   BatchStep& T = c->T;
@@ -531,9 +548,7 @@ int cup_batch_step(cup_ctx* c, int32_t step, const double* dt_in, double* dt_use
     return keep_err(c, rc);
   std::vector<SolveStats> S(K);
   CUP_CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
-  if (int rc = poisson_bicgstab_batched(c->dm, F.lhs, F.phi, batch_params(c), c->W, c->B, S.data(), c->stream,
-                                       batch_coarse(c)))
-    return keep_err(c, rc);
+  if (int rc = batch_solve(c, F.lhs, F.phi, batch_params(c), S.data())) return keep_err(c, rc);
   CUP_CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
   if (int rc = launch_case_sums(c->dm, F.phi, T.bscratch, T.first, K, T.sums, grid, c->stream)) return keep_err(c, rc);
   if (int rc = launch_grad_update(c->dm, F.vel[F.vcur], F.phi, pold, pnew, nullptr, 0.0, step,

@@ -91,6 +91,7 @@ struct BatchStep {
   double* bscratch = nullptr;   // 2 nb
   double* slot_force = nullptr; // 6 nslots
   double* hmin = nullptr;       // ncase: finest spacing of each case
+  double* mixed = nullptr;      // 2 ncase: the mixed-precision batch's per-case sums
   // pinned host copies filled by captured steps
   double* h_dt = nullptr;       // ncase
   double* h_force = nullptr;    // 6 ncase

@@ -1799,10 +1799,15 @@ static int launch_persistent(const KArgs<T>& A, PoissonWork& W, cudaStream_t s, 
 // group per block at most), the same shape as the single-case solver.
 int batch_solver_shape(int nb, int ncase, int* grid, int* groups) {
   const size_t dyn = batch_smem(ncase);
+  // every CTA resident for the FP64 solver and the FP32 inner solves alike
   void (*kern)(KArgs<double>, GridSync, BatchArgs) = k_bicg_batched<double>;
+  void (*kernf)(KArgs<float>, GridSync, BatchArgs) = k_bicg_batched<float>;
   CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
-  int per_sm = 0, dev = 0, sms = 0;
+  CUP_CUDA_TRY(cudaFuncSetAttribute(kernf, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
+  int per_sm = 0, per_sm_f = 0, dev = 0, sms = 0;
   CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, PNT, dyn));
+  CUP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, kernf, PNT, dyn));
+  per_sm = std::min(per_sm, per_sm_f);
   CUP_CUDA_TRY(cudaGetDevice(&dev));
   CUP_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) return set_error(CUP_ERR_CUDA, "batched BiCGSTAB: kernel does not fit on an SM");
@@ -1811,12 +1816,13 @@ int batch_solver_shape(int nb, int ncase, int* grid, int* groups) {
   return 0;
 }
 
-int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
-                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s,
-                             const BatchCoarse* coarse) {
+// The batched launch on vectors of type T: FP64 for the solver, FP32 for the
+// inner solves of the mixed-precision batch.
+template <class T>
+static int batched_launch(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, PoissonWork& W,
+                          BatchWork& B, SolveStats* out, cudaStream_t s, const BatchCoarse* coarse) {
   poisson_init_constants();
   if (B.ncase < 1 || !B.st) return set_error(CUP_ERR_STATE, "batched BiCGSTAB: not a batch");
-  double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
   const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
   if (P.graph) {  // captured: the initial states come from the device template
     CUP_CUDA_TRY(cudaMemcpyAsync(B.st, B.st_init, sizeof(KrylovState) * B.ncase, cudaMemcpyDeviceToDevice, s));
@@ -1828,7 +1834,7 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   CUP_CUDA_TRY(cudaMemsetAsync(B.case_done, 0, sizeof(int) * B.ncase, s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar, 0, sizeof(unsigned int), s));
   CUP_CUDA_TRY(cudaMemsetAsync(W.bar_error, 0, sizeof(int), s));
-  KArgs<double> A = make_args<double>(M, b, x, v, W, B.st, P.mean_mode, zmr, 0);
+  KArgs<T> A = make_args<T>(M, b, x, v, W, B.st, P.mean_mode, zmr, 0);
   A.ncache = KB_CACHE;
   if (coarse && coarse->inv) {  // the cases' two-level preconditioners
     A.cnb = 1;
@@ -1842,7 +1848,7 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
   BatchArgs Ba{B.cfirst, B.cblocks, B.part, B.case_done, B.ncase, B.groups};
   void* args[] = {(void*)&A, (void*)&Gs, (void*)&Ba};
   const size_t dyn = batch_smem(B.ncase);
-  void (*kern)(KArgs<double>, GridSync, BatchArgs) = k_bicg_batched<double>;
+  void (*kern)(KArgs<T>, GridSync, BatchArgs) = k_bicg_batched<T>;
   if (!P.graph) CUP_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
   {
     ProfScope ps("bicg_batched", s);
@@ -1862,6 +1868,187 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
     out[c].outer = 0;
     out[c].err_init = fin[c].err_init;
     out[c].err_opt = fin[c].err_opt;
+  }
+  return 0;
+}
+
+int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
+                             PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s,
+                             const BatchCoarse* coarse) {
+  double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
+  return batched_launch<double>(M, b, x, v, P, W, B, out, s, coarse);
+}
+
+// ---- mixed precision in a batch of cases ----------------------------------
+// FP32 batched inner solves (every case in one launch, with the batch's
+// coarse spaces when they are built) inside FP64 iterative refinement per
+// case, as poisson_mixed does for one case.  A case that has reached its
+// tolerance (or stopped) gets a zero inner right-hand side, which stops it
+// at once in the inner solve, so its x stays as it is.
+
+// Per block: x's mean-row entry zeroed (first call), e added, the block's
+// sum(x h^3) into bpart[b].
+__global__ void __launch_bounds__(NT) k_refine_update_batch(DevMesh M, double* x, const float* __restrict__ e,
+                                                            int zero_mean_row, double* __restrict__ bpart) {
+  __shared__ double red[64];
+  for (int b = blockIdx.x; b < M.nb; b += gridDim.x) {
+    const double h = M.h[b], h3 = h * h * h;
+    const int mb = M.case_mean[M.bcase[b]];
+    double s[1] = {0.0};
+    for (int c = threadIdx.x; c < BN; c += NT) {
+      const size_t i = size_t(b) * BN + c;
+      double v = x[i];
+      if (zero_mean_row && b == mb && c == 0) v = 0.0;
+      if (e) v += double(e[i]);
+      x[i] = v;
+      s[0] += v;
+    }
+    block_reduce<1>(s, red);
+    if (threadIdx.x == 0) bpart[b] = s[0] * h3;
+  }
+}
+
+// Per block: r = b - A x in FP32 into r32 (each case's operator with its own
+// mean row, case_ms[c] = sum(x h^3) of case c), |r|^2 of the block into bpart.
+__global__ void __launch_bounds__(NT) k_true_residual_batch(DevMesh M, const double* __restrict__ b,
+                                                            const double* __restrict__ x, float* __restrict__ r32,
+                                                            int mean_mode, int zero_mean_row,
+                                                            const double* __restrict__ case_ms,
+                                                            double* __restrict__ bpart) {
+  __shared__ GroupTile tiles[GROUPS];
+  __shared__ double gsm[2 * GROUPS];
+  const GroupIdx G;
+  GROUP_BLOCKS(blk) {
+    double col[8], y[8], bc[8];
+    load_col(x, blk, G, col);
+    fill_block_info(M, blk, tiles[G.g].bi, G.lane);
+    group_sync(G.g);
+    const int c = M.bcase[blk];
+    spmv_group(tiles[G.g].bi, VecAt<double>{x}, col, case_ms[c], mean_mode, tiles[G.g], G, y);
+    load_col(b, blk, G, bc);
+    if (zero_mean_row && blk == M.case_mean[c] && G.lane == 0) bc[0] = 0.0;
+    float* rb = r32 + size_t(blk) * BN + G.gy * 8 + G.gx;
+    double a[1] = {0.0};
+#pragma unroll
+    for (int z = 0; z < 8; ++z) {
+      const double ri = bc[z] - y[z];
+      rb[z * 64] = float(ri);
+      a[0] += ri * ri;
+    }
+    group_reduce<1>(a, &gsm[2 * G.g], G);
+    if (G.lane == 0) bpart[blk] = a[0];
+  }
+}
+
+// out[c] = the sum of part over case c's blocks (one CTA per case, fixed order)
+__global__ void __launch_bounds__(NT) k_case_total(const double* __restrict__ part, const int* __restrict__ first,
+                                                   double* __restrict__ out) {
+  __shared__ double red[64];
+  const int c = blockIdx.x;
+  double s[1] = {0.0};
+  for (int b = first[c] + threadIdx.x; b < first[c + 1]; b += NT) s[0] += part[b];
+  block_reduce<1>(s, red);
+  if (threadIdx.x == 0) out[c] = s[0];
+}
+
+int poisson_mixed_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
+                          BatchWork& B, SolveStats* out, cudaStream_t s, const BatchCoarse* coarse,
+                          const int* d_first, const int* first, double* bpart, double* d_case) {
+  const int K = B.ncase;
+  const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
+  float* const v[9] = {W.fr, W.frhat, W.fp, W.fnu, W.ft, W.fz1, W.fz2, W.fxs[1], W.fxs[2]};
+  float* e = W.fxs[0];
+  double* ms = d_case;     // K: each case's sum(x h^3)
+  double* rr = d_case + K; // K: each case's |b - A x|^2
+  const size_t n = size_t(M.nb) * BN;
+  std::vector<double> h_rr(K);
+  auto update = [&](const float* ee) -> int {
+    k_refine_update_batch<<<W.grid, NT, 0, s>>>(M, x, ee, ee ? 0 : zmr, bpart);
+    k_case_total<<<K, NT, 0, s>>>(bpart, d_first, ms);
+    CUP_CUDA_TRY(cudaGetLastError());
+    return 0;
+  };
+  auto residual = [&]() -> int {
+    {
+      ProfScope ps("refine_true_residual_fp64", s);
+      k_true_residual_batch<<<W.ggrid, NT, 0, s>>>(M, b, x, W.r32, P.mean_mode, zmr, ms, bpart);
+      k_case_total<<<K, NT, 0, s>>>(bpart, d_first, rr);
+    }
+    CUP_CUDA_TRY(cudaGetLastError());
+    CUP_CUDA_TRY(cudaMemcpyAsync(h_rr.data(), rr, K * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUP_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+  };
+  if (int rc = update(nullptr)) return rc;
+  if (int rc = residual()) return rc;
+  std::vector<double> err0(K), err(K);
+  std::vector<int> active(K, 1), total(K, 0), restarts(K, 0), outer_n(K, 0);
+  auto converged = [&](int k) { return err[k] <= P.tol_abs || err[k] / err0[k] <= P.tol_rel; };
+  for (int k = 0; k < K; ++k) {
+    err0[k] = err[k] = std::sqrt(h_rr[k]);
+    out[k] = SolveStats{};
+    out[k].err_init = err0[k];
+    out[k].status = SOLVE_MAXITER;
+    if (!(err0[k] == err0[k])) {
+      out[k].status = SOLVE_NAN;
+      active[k] = 0;
+    } else if (err0[k] <= P.tol_abs) {
+      out[k].status = SOLVE_CONVERGED;
+      active[k] = 0;
+    }
+  }
+  std::vector<SolveStats> in(K);
+  for (int outer = 0; outer < 40; ++outer) {
+    double q = 0.5;
+    int min_total = P.max_iter, nact = 0;
+    for (int k = 0; k < K; ++k) {
+      if (active[k] && converged(k)) {
+        out[k].status = SOLVE_CONVERGED;
+        active[k] = 0;
+      }
+      if (!active[k]) continue;
+      ++nact;
+      // the inner tolerance of the case that needs the most, within FP32 reach
+      const double want = std::max(P.tol_abs, P.tol_rel * err0[k]);
+      q = std::min(q, std::max(2e-5, 0.5 * want / err[k]));
+      min_total = std::min(min_total, total[k]);
+    }
+    if (nact == 0) break;
+    for (int k = 0; k < K; ++k)
+      if (!active[k])
+        CUP_CUDA_TRY(cudaMemsetAsync(W.r32 + size_t(first[k]) * BN, 0,
+                                     size_t(first[k + 1] - first[k]) * BN * sizeof(float), s));
+    SolveParams Q = P;
+    Q.tol_abs = 0.0;
+    Q.tol_rel = q;
+    Q.max_iter = std::max(1, P.max_iter - min_total);
+    CUP_CUDA_TRY(cudaMemsetAsync(e, 0, n * sizeof(float), s));
+    if (int rc = batched_launch<float>(M, W.r32, e, v, Q, W, B, in.data(), s, coarse)) return rc;
+    if (int rc = update(e)) return rc;
+    if (int rc = residual()) return rc;
+    for (int k = 0; k < K; ++k) {
+      if (!active[k]) continue;
+      total[k] += in[k].iterations;
+      restarts[k] += in[k].restarts;
+      outer_n[k] = outer + 1;
+      const double prev = err[k];
+      err[k] = std::sqrt(h_rr[k]);
+      if (!(err[k] == err[k]) || in[k].status == SOLVE_NAN) {
+        out[k].status = SOLVE_NAN;
+        active[k] = 0;
+      } else if (converged(k)) {
+        out[k].status = SOLVE_CONVERGED;
+        active[k] = 0;
+      } else if ((err[k] > 0.9 * prev && in[k].iterations > 0) || total[k] >= P.max_iter) {
+        active[k] = 0;  // refinement stagnated, or the iteration budget is spent
+      }
+    }
+  }
+  for (int k = 0; k < K; ++k) {
+    out[k].iterations = total[k];
+    out[k].restarts = restarts[k];
+    out[k].outer = outer_n[k];
+    out[k].err_opt = err[k];
   }
   return 0;
 }

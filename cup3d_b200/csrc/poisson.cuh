@@ -175,5 +175,11 @@ int batch_solver_shape(int nb, int ncase, int* grid, int* groups);
 int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P,
                              PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s,
                              const BatchCoarse* coarse = nullptr);
+// Mixed precision in a batch: FP32 batched inner solves inside per-case FP64
+// iterative refinement.  d_first / first: the cases' block offsets (device /
+// host, ncase + 1); bpart: nb doubles of scratch; d_case: 2 ncase doubles.
+int poisson_mixed_batched(const DevMesh& M, const double* b, double* x, const SolveParams& P, PoissonWork& W,
+                          BatchWork& B, SolveStats* out, cudaStream_t s, const BatchCoarse* coarse,
+                          const int* d_first, const int* first, double* bpart, double* d_case);
 
 }  // namespace cup3d

@@ -79,6 +79,38 @@ def test_batch_cases_match_oracle():
         batch.poisson_solve()
 
 
+def test_batch_mixed_precision_solve():
+    # -poissonSolver b200_mixed on a batch: FP32 inner solves of all cases in
+    # one launch inside FP64 refinement per case.  Each case reaches the FP64
+    # true residual on the oracle's operator, its solution agrees with the
+    # FP64 batched solve, and a case whose right-hand side is zero stays at
+    # x = 0 while the others refine.
+    names = ["tgv32", "amr2_free", "amr3_mixed"]
+    sols = {}
+    for solver in ("b200", "b200_mixed"):
+        ctxs = [make_ctx(n, device=0, extra=FLAGS + f" -poissonSolver {solver}") for n in names]
+        meshes = [oracle_mesh(c) for c in ctxs]
+        bs = [compatible_rhs(m, 40 + k) for k, m in enumerate(meshes)]
+        bs[1] = np.zeros_like(bs[1])
+        batch = cup.Batch(ctxs)
+        bd, xd = torch_dev(np.concatenate(bs)), torch_dev(np.zeros(sum(m.n for m in meshes)))
+        rc, stats = batch.poisson_solve_dev(bd, xd)
+        assert rc == 0, (solver, stats)
+        xs = split(batch, xd.cpu().numpy())
+        for k, (ctx, m, b, x, st) in enumerate(zip(ctxs, meshes, bs, xs, stats)):
+            assert st["status"] == 1, (solver, k, st)
+            bb = mean_row_zeroed(ctx, m, b)
+            res = np.linalg.norm(bb - m.apply(x, mean_constraint=ctx.cfg.mean_constraint))
+            assert res <= 1.05e-10 * max(np.linalg.norm(bb), 1e-300) or k == 1, (solver, k, res)
+        assert not np.any(xs[1]), solver
+        sols[solver] = (xs, stats)
+    print("iterations FP64 / mixed (inner):", [s["iterations"] for s in sols["b200"][1]],
+          [s["iterations"] for s in sols["b200_mixed"][1]])
+    for k in (0, 2):
+        x64, x32 = sols["b200"][0][k], sols["b200_mixed"][0][k]
+        assert np.linalg.norm(x32 - x64) <= 1e-8 * np.linalg.norm(x64), k
+
+
 def test_batch_zero_rhs_case_stops_at_once():
     ctxs = [make_ctx(n, device=0, extra=FLAGS) for n in ["amr2_free", "tgv32", "amr3_mixed"]]
     meshes = [oracle_mesh(c) for c in ctxs]
