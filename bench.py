@@ -26,8 +26,8 @@ The timed steps follow the warm-up steps and --settle (50) more.
 `swarm_batch`  64 independent penalized-ellipsoid cases (372-2659 blocks
          each, 37.5M cells) advanced together by cup_batch_step: 200 steps
          with the two-level solver and the bodies moving, 5 with the block
-         inverse alone and the bodies held in place; step 0 also taken case
-         by case for comparison.
+         inverse alone (FP64, and mixed precision) and the bodies held in
+         place; step 0 also taken case by case for comparison.
 `mesh_adaptation`  from the settled state, three rounds of one adaptation
          (vorticity tagging, refine/compress, field transfer), the two-level
          coarse space of the new mesh, and 20 steps on it (the reference
@@ -630,9 +630,11 @@ def run_b200(args):
             line["learned_re1000"] = learned_re1000(ctx, flush)
     if rank == 0 and not args.no_swarm:
         # the swarm's 200 steps with the two-level solver and moving bodies;
-        # 5 steps with the block inverse alone (bodies in place) for comparison
+        # 5 steps with the block inverse alone, FP64 and mixed precision (bodies
+        # in place), for comparison
         line["swarm_batch"] = {s: swarm_batch(flush, steps=n, solver=s, moving=mv)
-                               for s, n, mv in (("b200", 5, False), ("b200_twolevel", 200, True))}
+                               for s, n, mv in (("b200", 5, False), ("b200_mixed", 5, False),
+                                                ("b200_twolevel", 200, True))}
     if rank == 0 and not args.no_obstacle:
         line["obstacle_creation"] = obstacle_creation()
     if rank == 0 and not args.no_cpu_baseline:
