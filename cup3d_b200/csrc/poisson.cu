@@ -1818,12 +1818,15 @@ int batch_solver_shape(int nb, int ncase, int* grid, int* groups) {
 
 // The batched launch on vectors of type T: FP64 for the solver, FP32 for the
 // inner solves of the mixed-precision batch.
+// zero_mean_row: the mean-constraint row's right-hand side taken as zero
+// (the solver), or as given (the inner solves: it holds the row's residual).
 template <class T>
 static int batched_launch(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, PoissonWork& W,
-                          BatchWork& B, SolveStats* out, cudaStream_t s, const BatchCoarse* coarse) {
+                          BatchWork& B, SolveStats* out, cudaStream_t s, const BatchCoarse* coarse,
+                          int zero_mean_row) {
   poisson_init_constants();
   if (B.ncase < 1 || !B.st) return set_error(CUP_ERR_STATE, "batched BiCGSTAB: not a batch");
-  const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
+  const int zmr = zero_mean_row;
   if (P.graph) {  // captured: the initial states come from the device template
     CUP_CUDA_TRY(cudaMemcpyAsync(B.st, B.st_init, sizeof(KrylovState) * B.ncase, cudaMemcpyDeviceToDevice, s));
   } else {
@@ -1876,7 +1879,8 @@ int poisson_bicgstab_batched(const DevMesh& M, const double* b, double* x, const
                              PoissonWork& W, BatchWork& B, SolveStats* out, cudaStream_t s,
                              const BatchCoarse* coarse) {
   double* const v[9] = {W.r, W.rhat, W.p, W.nu, W.t, W.z1, W.z2, W.xs[1], W.xs[2]};
-  return batched_launch<double>(M, b, x, v, P, W, B, out, s, coarse);
+  const int zmr = (P.mean_mode == 1 || P.mean_mode == 3) ? 1 : 0;
+  return batched_launch<double>(M, b, x, v, P, W, B, out, s, coarse, zmr);
 }
 
 // ---- mixed precision in a batch of cases ----------------------------------
@@ -2023,7 +2027,7 @@ int poisson_mixed_batched(const DevMesh& M, const double* b, double* x, const So
     Q.tol_rel = q;
     Q.max_iter = std::max(1, P.max_iter - min_total);
     CUP_CUDA_TRY(cudaMemsetAsync(e, 0, n * sizeof(float), s));
-    if (int rc = batched_launch<float>(M, W.r32, e, v, Q, W, B, in.data(), s, coarse)) return rc;
+    if (int rc = batched_launch<float>(M, W.r32, e, v, Q, W, B, in.data(), s, coarse, 0)) return rc;
     if (int rc = update(e)) return rc;
     if (int rc = residual()) return rc;
     for (int k = 0; k < K; ++k) {
