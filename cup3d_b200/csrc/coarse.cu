@@ -173,7 +173,7 @@ constexpr int GJT = 64;  // update tile (GJT x GJT per CTA)
 // Pinv (GJB x GJB) = P^-1 by Gauss-Jordan with partial pivoting, one warp:
 // lane t owns columns t and t + GJB of the augmented block [P | I]; the pivot
 // search is a butterfly over the lanes (largest |entry|, the lower row on a
-// tie), so every lane holds the same pivot.  *flag = 1 when a pivot is not
+// tie), whose lane-0 result every lane takes.  *flag = 1 when a pivot is not
 // above 1e-13 of P's largest entry.
 __global__ void __launch_bounds__(32) k_bgj_block_inverse(const double* __restrict__ M, int n, int k0, int bk,
                                                           double* __restrict__ Pinv, int* flag) {
@@ -205,8 +205,13 @@ __global__ void __launch_bounds__(32) k_bgj_block_inverse(const double* __restri
         arg = oarg;
       }
     }
+    // lane 0's pair for every lane: it starts at row j and takes only a larger
+    // |entry| (or an equal one of a lower row), so it is always a row of the
+    // block, even when NaNs leave the lanes' pairs differing
+    a = __shfl_sync(0xffffffffu, a, 0);
+    arg = __shfl_sync(0xffffffffu, arg, 0);
     if (!(a > tiny)) bad = true;
-    const int p = arg;
+    const int p = min(max(arg, j), bk - 1);
     if (p != j) {
       double w = G[j][t];
       G[j][t] = G[p][t];
