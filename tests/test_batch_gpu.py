@@ -111,6 +111,22 @@ def test_batch_mixed_precision_solve():
         assert np.linalg.norm(x32 - x64) <= 1e-8 * np.linalg.norm(x64), k
 
 
+def test_batch_refuses_single_case_solvers():
+    # the learned, Schwarz and pipelined solvers are single-case only: a
+    # batch solve with one of them is an error, not a silent other solver
+    ctxs = [make_ctx(n, device=0, extra=FLAGS) for n in ("tgv32", "amr2_free")]
+    batch = cup.Batch(ctxs)
+    n = sum(c.nb * 512 for c in ctxs)
+    bd, xd = torch_dev(np.zeros(n)), torch_dev(np.zeros(n))
+    for solver in ("b200_learned", "b200_learned_mixed", "b200_schwarz", "b200_pipelined"):
+        batch.set_poisson(solver, 0.0, 1e-8, 100)
+        with pytest.raises(cup.CupError):
+            batch.poisson_solve_dev(bd, xd)
+    batch.set_poisson("b200", 0.0, 1e-8, 100)
+    rc, stats = batch.poisson_solve_dev(bd, xd)
+    assert rc == 0
+
+
 def test_batch_zero_rhs_case_stops_at_once():
     ctxs = [make_ctx(n, device=0, extra=FLAGS) for n in ["amr2_free", "tgv32", "amr3_mixed"]]
     meshes = [oracle_mesh(c) for c in ctxs]
