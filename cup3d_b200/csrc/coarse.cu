@@ -170,74 +170,74 @@ __global__ void k_gj_augment(const double* __restrict__ A, int n, double* __rest
 constexpr int GJB = 32;  // panel width
 constexpr int GJT = 64;  // update tile (GJT x GJT per CTA)
 
-// Pinv (GJB x GJB) = P^-1 by Gauss-Jordan with partial pivoting, one warp:
-// lane t owns columns t and t + GJB of the augmented block [P | I]; the pivot
-// search is a butterfly over the lanes (largest |entry|, the lower row on a
-// tie), whose lane-0 result every lane takes.  *flag = 1 when a pivot is not
-// above 1e-13 of P's largest entry.
-__global__ void __launch_bounds__(32) k_bgj_block_inverse(const double* __restrict__ M, int n, int k0, int bk,
+// Pinv (GJB x GJB) = P^-1 by Gauss-Jordan with partial pivoting, one CTA;
+// *flag = 1 when a pivot is not above 1e-13 of P's largest entry.
+__global__ void __launch_bounds__(256) k_bgj_block_inverse(const double* __restrict__ M, int n, int k0, int bk,
                                                           double* __restrict__ Pinv, int* flag) {
   __shared__ double G[GJB][2 * GJB + 1];
   __shared__ double fac[GJB];
+  __shared__ double red[8];
+  __shared__ int s_piv, s_bad;
   const int t = threadIdx.x;
   double amax = 0.0;
-  for (int r = 0; r < GJB; ++r) {
-    const double v = (r < bk && t < bk) ? M[size_t(k0 + r) * n + k0 + t] : (r == t ? 1.0 : 0.0);
-    G[r][t] = v;
-    G[r][GJB + t] = r == t ? 1.0 : 0.0;
-    if (r < bk && t < bk) amax = fmax(amax, fabs(v));
+  for (int e = t; e < GJB * 2 * GJB; e += blockDim.x) {
+    const int r = e / (2 * GJB), c = e % (2 * GJB);
+    double v;
+    if (c < GJB)
+      v = (r < bk && c < bk) ? M[size_t(k0 + r) * n + k0 + c] : (r == c ? 1.0 : 0.0);
+    else
+      v = c - GJB == r ? 1.0 : 0.0;
+    G[r][c] = v;
+    if (c < bk && r < bk) amax = fmax(amax, fabs(v));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-  __syncwarp();
+  if ((t & 31) == 0) red[t >> 5] = amax;
+  if (t == 0) s_bad = 0;
+  __syncthreads();
+  amax = 0.0;
+  for (int w = 0; w < int(blockDim.x >> 5); ++w) amax = fmax(amax, red[w]);
   const double tiny = 1e-13 * amax;
-  bool bad = false;
   for (int j = 0; j < bk; ++j) {
-    const int r0 = j + t;
-    double a = r0 < bk ? fabs(G[r0][j]) : -1.0;
-    int arg = r0;
+    if (t < 32) {
+      const int r = j + t;
+      double a = r < bk ? fabs(G[r][j]) : -1.0;
+      int arg = r;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double oa = __shfl_xor_sync(0xffffffffu, a, o);
-      const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
-      if (oa > a || (oa == a && oarg < arg)) {
-        a = oa;
-        arg = oarg;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double oa = __shfl_xor_sync(0xffffffffu, a, o);
+        const int oarg = __shfl_xor_sync(0xffffffffu, arg, o);
+        if (oa > a || (oa == a && oarg < arg)) {
+          a = oa;
+          arg = oarg;
+        }
+      }
+      if (t == 0) {
+        s_piv = arg;
+        if (!(a > tiny)) s_bad = 1;
       }
     }
-    // lane 0's pair for every lane: it starts at row j and takes only a larger
-    // |entry| (or an equal one of a lower row), so it is always a row of the
-    // block, even when NaNs leave the lanes' pairs differing
-    a = __shfl_sync(0xffffffffu, a, 0);
-    arg = __shfl_sync(0xffffffffu, arg, 0);
-    if (!(a > tiny)) bad = true;
-    const int p = min(max(arg, j), bk - 1);
-    if (p != j) {
-      double w = G[j][t];
+    __syncthreads();
+    const int p = s_piv;
+    if (p != j && t < 2 * GJB) {
+      const double a = G[j][t];
       G[j][t] = G[p][t];
-      G[p][t] = w;
-      w = G[j][GJB + t];
-      G[j][GJB + t] = G[p][GJB + t];
-      G[p][GJB + t] = w;
+      G[p][t] = a;
     }
-    __syncwarp();
+    __syncthreads();
     const double ip = 1.0 / G[j][j];
-    fac[t] = t == j ? 0.0 : G[t][j];
-    __syncwarp();
-    G[j][t] *= ip;
-    G[j][GJB + t] *= ip;
-    __syncwarp();
-    const double pj0 = G[j][t], pj1 = G[j][GJB + t];
-    for (int r = 0; r < GJB; ++r) {
-      if (r == j) continue;
-      const double f = fac[r];
-      G[r][t] -= f * pj0;
-      G[r][GJB + t] -= f * pj1;
+    if (t < GJB) fac[t] = t == j ? 0.0 : G[t][j];
+    __syncthreads();
+    if (t < 2 * GJB) G[j][t] *= ip;
+    __syncthreads();
+    for (int e = t; e < GJB * 2 * GJB; e += blockDim.x) {
+      const int r = e / (2 * GJB), c = e % (2 * GJB);
+      if (r != j) G[r][c] -= fac[r] * G[j][c];
     }
-    __syncwarp();
+    __syncthreads();
   }
-  for (int e = t; e < GJB * GJB; e += 32) Pinv[e] = G[e / GJB][GJB + e % GJB];
-  if (t == 0 && (bad || !(amax > 0.0) || !isfinite(amax))) *flag = 1;
+  for (int e = t; e < GJB * GJB; e += blockDim.x) Pinv[e] = G[e / GJB][GJB + e % GJB];
+  if (t == 0 && (s_bad || !(amax > 0.0) || !isfinite(amax))) *flag = 1;
 }
 
 // T' (GJB rows of n) and C (n rows of GJB) of the panel at k0
@@ -489,7 +489,7 @@ int device_inverse_dev(double* M, int n, int last, int sms, cudaStream_t s, int*
     const int pg = int(std::max<size_t>(1, std::min<size_t>(size_t(sms) * 8, (size_t(n) * (GJB + GJB / 8) + 255) / 256)));
     for (int k0 = 0; k0 < n; k0 += GJB) {
       const int bk = std::min(GJB, n - k0);
-      k_bgj_block_inverse<<<1, 32, 0, s>>>(M, n, k0, bk, Pinv, flag);
+      k_bgj_block_inverse<<<1, 256, 0, s>>>(M, n, k0, bk, Pinv, flag);
       k_bgj_panels<<<pg, 256, 0, s>>>(M, n, k0, bk, Pinv, T, Cp);
       k_bgj_update<<<dim3(tiles, tiles), 256, 0, s>>>(M, n, k0, bk, T, Cp);
     }
