@@ -4,6 +4,7 @@
     python -m cup3d_b200.kernel_cases solve   # 16 BiCGSTAB iterations (sphere mesh, seeded RHS)
     python -m cup3d_b200.kernel_cases step    # 4 full time steps of the sphere workload
     python -m cup3d_b200.kernel_cases swarm   # 16 iterations of a batched solve over 8 swarm cases
+    python -m cup3d_b200.kernel_cases swarm_step  # 3 batched two-level steps of 8 swarm cases, bodies moving
     python -m cup3d_b200.kernel_cases learned # 20 training steps, then 16 iterations of the learned solve
     python -m cup3d_b200.kernel_cases adapt   # 20 two-level steps, one mesh adaptation, the coarse rebuild, 1 step
 
@@ -27,6 +28,15 @@ def main(argv):
 
     from cup3d_b200.workloads import make_sphere_ctx, make_swarm_ctx, poisson_rhs, swarm_rhs
     case = argv[1] if len(argv) > 1 else "solve"
+    if case == "swarm_step":
+        import cup3d_b200 as cup
+        cases = [make_swarm_ctx(i, 0, "-stepGraph 0 -poissonSolver b200_twolevel -StaticObstacles 0") for i in range(8)]
+        batch = cup.Batch(cases)
+        for step in range(3):
+            rc, dts, forces, st = batch.step(step)
+        torch.cuda.synchronize()
+        print(f"swarm_step ok: rc {rc}, {batch.nb} blocks, iterations {[s['iterations'] for s in st]}")
+        return
     if case == "swarm":
         import cup3d_b200 as cup
         cases = [make_swarm_ctx(i, 0) for i in range(8)]
