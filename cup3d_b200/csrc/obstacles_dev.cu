@@ -148,18 +148,36 @@ __device__ __forceinline__ void obst_chi_block(int b, const double* __restrict__
   }
   __shared__ double lab[10][10][10];
   __shared__ double sm[16];
+  __shared__ double s_far;
   const double h = h_[b];
   const double ox = origin[3 * b], oy = origin[3 * b + 1], oz = origin[3 * b + 2];
-  for (int i = t; i < 1000; i += BN) {
-    const int x = i % 10 - 1, y = (i / 10) % 10 - 1, z = i / 100 - 1;
-    lab[z + 1][y + 1][x + 1] = shape_sdf(s, ox + (x + 0.5) * h, oy + (y + 0.5) * h, oz + (z + 0.5) * h);
+  // A block whose cells all lie more than one cell from the surface has chi
+  // 1 (inside) or 0 (outside) in every cell, which is what the lab below
+  // would give them: the signed distance is an exact distance (sphere, and
+  // the ellipsoid's closest-point solve), so no cell's value is farther than
+  // its distance to the block centre (at most 3.5 sqrt(3) h) from the
+  // centre's value.  Such blocks skip the lab (1e-6 h of margin for rounding).
+  if (t == 0) {
+    const double sc = shape_sdf(s, ox + 4.0 * h, oy + 4.0 * h, oz + 4.0 * h);
+    const double reach = 3.5 * 1.7320508075688772 * h + 1e-6 * h;
+    s_far = sc - reach > h ? 1.0 : (sc + reach < -h ? 0.0 : -1.0);
   }
   __syncthreads();
+  const bool far = s_far >= 0.0;
+  if (!far) {
+    for (int i = t; i < 1000; i += BN) {
+      const int x = i % 10 - 1, y = (i / 10) % 10 - 1, z = i / 100 - 1;
+      lab[z + 1][y + 1][x + 1] = shape_sdf(s, ox + (x + 0.5) * h, oy + (y + 0.5) * h, oz + (z + 0.5) * h);
+    }
+    __syncthreads();
+  }
   const int x = t & 7, y = (t >> 3) & 7, z = t >> 6;
   const double inv2h = 0.5 / h, vol = h * h * h;
-  const double s0 = lab[z + 1][y + 1][x + 1];
+  const double s0 = far ? 0.0 : lab[z + 1][y + 1][x + 1];
   double c;
-  if (s0 > h || s0 < -h) {
+  if (far) {
+    c = s_far;
+  } else if (s0 > h || s0 < -h) {
     c = s0 > 0 ? 1 : 0;
   } else {
     const double dPx = lab[z + 1][y + 1][x + 2], dMx = lab[z + 1][y + 1][x];
