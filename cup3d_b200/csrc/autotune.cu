@@ -58,7 +58,8 @@ int cup_autotune(cup_ctx* c, int32_t* choice, float* best_ms) {
   const double dt = 1e-4;
   const double* vel = F.vel[F.vcur];
   double* scratch = F.vel[1 - F.vcur];
-  const ObstacleView ob{c->ob.nslots, c->ob.slot_of_block, c->ob.near, c->ob.chi, c->ob.udef, c->ob.block_of_slot};
+  const ObstacleView ob{c->ob.nslots, c->ob.slot_of_block, c->ob.near, c->ob.chi, c->ob.udef, c->ob.block_of_slot,
+                       c->ob.udef_zero ? 1 : 0};
   std::function<int(int)> kernels[3] = {
       // one RK3 stage: writes the other velocity buffer and tmpV
       [&](int g) { return launch_advect_stage(c->dm, vel, scratch, F.tmpV, dt, c->cfg.nu, c->cfg.uinf,

@@ -267,6 +267,7 @@ static ObstacleView batch_ob_view(const cup_ctx* c) {
   v.chi = c->ob.chi;
   v.udef = c->ob.udef;
   v.blk = c->ob.block_of_slot;
+  v.udef_zero = c->ob.udef_zero ? 1 : 0;
   return v;
 }
 

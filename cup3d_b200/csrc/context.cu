@@ -1,6 +1,7 @@
 // C-ABI implementation: context, mesh, fields, Poisson entry points.
 #include <cmath>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <sstream>
 
@@ -725,6 +726,7 @@ static ObstacleView ob_view(const cup_ctx* c) {
   v.chi = c->ob.chi;
   v.udef = c->ob.udef;
   v.blk = c->ob.block_of_slot;
+  v.udef_zero = c->ob.udef_zero ? 1 : 0;
   return v;
 }
 
@@ -761,6 +763,7 @@ int ctx_upload_obstacle(cup_ctx* c, int nslots, const int32_t* blocks, const dou
   else
     o.h_udef.assign(3 * size_t(nslots) * BN, 0.0);
   for (int i = 0; i < 9; ++i) o.kin[i] = kin ? kin[i] : 0.0;
+  o.udef_zero = std::all_of(o.h_udef.begin(), o.h_udef.end(), [](double v) { return v == 0.0; });
   if (c->host_only) return 0;  // host copies only
   DevArena& A = c->obst_arena;
   if (int rc = A.alloc(&o.slot_of_block, m.nb)) return keep(c, rc);

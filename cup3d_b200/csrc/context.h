@@ -48,6 +48,7 @@ struct DevObstacle {
   // of the mesh, the host copies fetched when read
   int dev_cap = 0;
   bool host_stale = false;
+  bool udef_zero = false;  // every slot's udef is zero (bodies created by the library: rigid)
   double* d_mom = nullptr;        // 4 per slot: sum chi h^3 (x, y, z), sum chi h^3
   double* d_origin = nullptr;     // 3 nb block origins
   void* d_result = nullptr;       // slot count, mass, kinematics

@@ -490,6 +490,7 @@ int create_obstacle_dev(cup_ctx* c, Shape& s) {
   o.nslots = h.nslots;
   for (int i = 0; i < 9; ++i) o.kin[i] = h.kin[i];
   o.host_stale = true;
+  o.udef_zero = true;  // k_obst_chi writes udef = 0
   if (h.nslots == 0) {  // nothing of the body on the mesh: no obstacle
     c->obst_arena.release();
     c->ob = DevObstacle();
@@ -1042,6 +1043,7 @@ int batch_bodies_advance(cup_ctx* c, int step, const double* dt) {
   CUP_CUDA_TRY(stream_d2h(st, &h, res, sizeof(h)));
   o.nslots = h.nslots;
   o.host_stale = true;
+  o.udef_zero = true;  // k_obst_chi_batch writes udef = 0
   return 0;
 }
 

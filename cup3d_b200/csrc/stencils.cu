@@ -460,14 +460,19 @@ int launch_pressure_rhs(const DevMesh& M, const double* vel, const double* pold,
   int dev = 0;
   CUP_CUDA_TRY(cudaGetDevice(&dev));
   ProfScope ps("pressure_rhs", s);
+  // with udef = 0 in every slot the near-body terms (chi times the
+  // divergence of udef, with its flux correction) are exact zeros: no block
+  // needs the udef lab
+  ObstacleView o = ob;
+  if (o.udef_zero) o.near = nullptr;
   if (step > step_2nd_start) {
     if (int rc = resident_ctas(k_pressure_rhs<1>, rhs_smem<1>(), attr[1], resident[1])) return rc;
     grid = std::max(1, std::min({grid, resident[1][dev], M.nb}));
-    k_pressure_rhs<1><<<grid, NT, rhs_smem<1>(), s>>>(M, vel, pold, chi, ob, dt, lhs, phi);
+    k_pressure_rhs<1><<<grid, NT, rhs_smem<1>(), s>>>(M, vel, pold, chi, o, dt, lhs, phi);
   } else {
     if (int rc = resident_ctas(k_pressure_rhs<0>, rhs_smem<0>(), attr[0], resident[0])) return rc;
     grid = std::max(1, std::min({grid, resident[0][dev], M.nb}));
-    k_pressure_rhs<0><<<grid, NT, rhs_smem<0>(), s>>>(M, vel, pold, chi, ob, dt, lhs, phi);
+    k_pressure_rhs<0><<<grid, NT, rhs_smem<0>(), s>>>(M, vel, pold, chi, o, dt, lhs, phi);
   }
   CUP_CUDA_TRY(cudaGetLastError());
   return 0;

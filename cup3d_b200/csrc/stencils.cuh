@@ -12,6 +12,7 @@ struct ObstacleView {
   const double* chi;    // nslots*512 obstacle chi
   const double* udef;   // 3*nslots*512
   const int* blk;       // nslots: block of each slot
+  int udef_zero = 0;    // 1: every slot's udef is zero (rigid bodies)
 };
 
 // One RK3 stage (AdvectionDiffusion.cpp:286-320) fused with its update:
