@@ -183,7 +183,8 @@ def train_learned(ctx, rhs_list, iters=(0, 1, 2, 3, 5, 8, 12), steps=600, batch=
             "held_out_rel_loss": [round(float(before), 4), round(float(ctx.cnn_eval()), 4)]}
 
 
-SOLVERS = ("b200", "b200_mixed", "b200_twolevel", "b200_schwarz", "b200_learned", "b200_learned_mixed")
+SOLVERS = ("b200", "b200_mixed", "b200_twolevel", "b200_twolevel_mixed", "b200_schwarz", "b200_learned",
+           "b200_learned_mixed")
 
 
 def poisson_at_tolerance(ctx, stream, flush, rhs_list, reps=3):
@@ -309,7 +310,7 @@ def swarm_batch(flush, steps=5, solver="b200", moving=False):
 
     # step 0 of every case, one by one and as the batch, from the same state;
     # each case's coarse space built before (as the batch's is at creation)
-    if solver == "b200_twolevel":
+    if solver in ("b200_twolevel", "b200_twolevel_mixed"):
         for c in ctxs:
             r = torch.ones(c.nb * 512, dtype=torch.float64, device="cuda")
             c.coarse_apply(r, torch.zeros_like(r))
@@ -329,7 +330,9 @@ def swarm_batch(flush, steps=5, solver="b200", moving=False):
         "workload": SWARM_WORKLOAD, "cases": 64, "cells": ncell, "solver": solver,
         "bodies": "moving (chi created again every step)" if moving else "held in place",
         "batch_create_s": round(setup_s, 2),
-        "metric": "Mcell-steps/s (batched time steps of all cases, FP64)",
+        "metric": "Mcell-steps/s (batched time steps of all cases)",
+        "precision": ("FP32 inner Poisson solves in FP64 refinement, FP64 elsewhere" if solver.endswith("_mixed")
+                      else "FP64"),
         "value": round(ncell * steps / (sum(ms) * 1e-3) / 1e6, 3), "steps": f"1..{steps} after step 0",
         "ms_per_step": [round(x, 2) for x in ms] if len(ms) <= 10 else
                        {"first5": [round(x, 2) for x in ms[:5]], "last5": [round(x, 2) for x in ms[-5:]],
@@ -629,12 +632,13 @@ def run_b200(args):
         if rank == 0:
             line["learned_re1000"] = learned_re1000(ctx, flush)
     if rank == 0 and not args.no_swarm:
-        # the swarm's 200 steps with the two-level solver and moving bodies;
-        # 5 steps with the block inverse alone, FP64 and mixed precision (bodies
-        # in place), for comparison
+        # the swarm's 200 steps with moving bodies and the two-level solver,
+        # FP64 and mixed precision; 5 steps with the block inverse alone (FP64,
+        # mixed precision), bodies in place, for comparison
         line["swarm_batch"] = {s: swarm_batch(flush, steps=n, solver=s, moving=mv)
                                for s, n, mv in (("b200", 5, False), ("b200_mixed", 5, False),
-                                                ("b200_twolevel", 200, True))}
+                                                ("b200_twolevel", 200, True),
+                                                ("b200_twolevel_mixed", 200, True))}
     if rank == 0 and not args.no_obstacle:
         line["obstacle_creation"] = obstacle_creation()
     if rank == 0 and not args.no_cpu_baseline:

@@ -26,7 +26,8 @@ CNN_FORWARD_NOALLOC_MAX = 64  # CUP_CNN_FORWARD_NOALLOC_MAX
 
 BC = {"freespace": 0, "periodic": 1, "wall": 2}
 ADV = {"upwind5": 0, "upwind3": 0, "weno5": 1}
-SOLVER = {"b200": 0, "b200_mixed": 1, "b200_learned": 2, "b200_learned_mixed": 3, "b200_twolevel": 4, "b200_schwarz": 5, "b200_pipelined": 6}
+SOLVER = {"b200": 0, "b200_mixed": 1, "b200_learned": 2, "b200_learned_mixed": 3, "b200_twolevel": 4, "b200_schwarz": 5, "b200_pipelined": 6,
+          "b200_twolevel_mixed": 7}
 FIELD = {"vel": 0, "pres": 1, "chi": 2, "lhs": 3, "tmpV": 4}
 FIELD_NCOMP = {"vel": 3, "pres": 1, "chi": 1, "lhs": 1, "tmpV": 3}
 

@@ -115,7 +115,8 @@ static const BatchCoarse* batch_coarse(const cup_ctx* c) { return c->bcoarse.inv
 // FP32 inverse), copied into one packed, block-diagonal array in case order.
 // No face joins two cases, so the batch's coarse operator is exactly that.
 static int batch_coarse_setup(cup_ctx* c, cup_ctx* const* cases) {
-  if (c->cfg.poisson_solver != CUP_POISSON_B200_TWOLEVEL) return 0;
+  if (c->cfg.poisson_solver != CUP_POISSON_B200_TWOLEVEL && c->cfg.poisson_solver != CUP_POISSON_B200_TWOLEVEL_MIXED)
+    return 0;
   std::vector<long long> off(c->ncase);
   long long total = 0;
   for (int k = 0; k < c->ncase; ++k) {
@@ -285,15 +286,16 @@ static SolveParams batch_params(const cup_ctx* c) {
 
 // The batch's Poisson solve: FP64 (block inverse, or two-level when the
 // cases' coarse spaces were built), or mixed precision (-poissonSolver
-// b200_mixed: FP32 batched inner solves, FP64 refinement per case).  The
-// learned, Schwarz and pipelined solvers are single-case only.
+// b200_mixed, or b200_twolevel_mixed with the coarse spaces: FP32 batched
+// inner solves, FP64 refinement per case).  The learned, Schwarz and
+// pipelined solvers are single-case only.
 static int batch_solve(cup_ctx* c, const double* b, double* x, const SolveParams& P, SolveStats* S) {
   const int sv = c->cfg.poisson_solver;
   if (sv == CUP_POISSON_B200_LEARNED || sv == CUP_POISSON_B200_LEARNED_MIXED || sv == CUP_POISSON_B200_SCHWARZ ||
       sv == CUP_POISSON_B200_PIPELINED)
     return set_error(CUP_ERR_ARG, "batch of cases: the learned, Schwarz and pipelined solvers are single-case only "
-                                  "(b200, b200_mixed, b200_twolevel)");
-  if (sv == CUP_POISSON_B200_MIXED)
+                                  "(b200, b200_mixed, b200_twolevel, b200_twolevel_mixed)");
+  if (sv == CUP_POISSON_B200_MIXED || sv == CUP_POISSON_B200_TWOLEVEL_MIXED)
     return poisson_mixed_batched(c->dm, b, x, P, c->W, c->B, S, c->stream, batch_coarse(c), c->T.first,
                                  c->case_first.data(), c->T.bscratch, c->T.mixed);
   return poisson_bicgstab_batched(c->dm, b, x, P, c->W, c->B, S, c->stream, batch_coarse(c));

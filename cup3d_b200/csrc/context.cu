@@ -322,6 +322,7 @@ int cup_config_parse(cup_config* c, const char* args) {
       else if (v == "b200_learned") c->poisson_solver = CUP_POISSON_B200_LEARNED;
       else if (v == "b200_learned_mixed") c->poisson_solver = CUP_POISSON_B200_LEARNED_MIXED;
       else if (v == "b200_twolevel") c->poisson_solver = CUP_POISSON_B200_TWOLEVEL;
+      else if (v == "b200_twolevel_mixed") c->poisson_solver = CUP_POISSON_B200_TWOLEVEL_MIXED;
       else if (v == "b200_schwarz") c->poisson_solver = CUP_POISSON_B200_SCHWARZ;
       else if (v == "b200_pipelined") c->poisson_solver = CUP_POISSON_B200_PIPELINED;
       else return ctx_fail(nullptr, CUP_ERR_ARG, "Poisson solver: \"" + v + "\" unrecognized!");
@@ -627,7 +628,8 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
   // the two-level solvers: the coarse space of the mesh, built once per mesh
   // (outside the solve's timed region)
   const bool schwarz = solver == CUP_POISSON_B200_SCHWARZ;
-  const bool twolevel = learned || schwarz || solver == CUP_POISSON_B200_TWOLEVEL;
+  const bool twolevel =
+      learned || schwarz || solver == CUP_POISSON_B200_TWOLEVEL || solver == CUP_POISSON_B200_TWOLEVEL_MIXED;
   if (twolevel)
     if (int rc2 = coarse_build(c)) return keep(c, rc2);
   if (learned && !c->cnn.ready)
@@ -649,7 +651,8 @@ static int solve_impl(cup_ctx* c, const double* b, double* x, cup_solve_stats* s
     double* vec[16];
     if (int rc2 = pipelined_vectors(c, vec)) return keep(c, rc2);
     rc = poisson_pipelined(c->dm, b, x, P, c->W, vec, S, c->stream);
-  } else if (solver == CUP_POISSON_B200_MIXED || solver == CUP_POISSON_B200_LEARNED_MIXED)
+  } else if (solver == CUP_POISSON_B200_MIXED || solver == CUP_POISSON_B200_LEARNED_MIXED ||
+             solver == CUP_POISSON_B200_TWOLEVEL_MIXED)
     rc = poisson_mixed(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, lmap, coarse, c->num_sms);
   else
     rc = poisson_bicgstab(c->dm, b, x, P, c->W, S, c->stream, c->h_pinned, lmap, coarse, c->num_sms);

@@ -467,7 +467,7 @@ int cup_schwarz_apply_dev(cup_ctx* c, const double* d_r, double* d_z) {
 }
 
 int cup_set_poisson(cup_ctx* c, int32_t solver, double tol_abs, double tol_rel, int32_t max_iter) {
-  if (!c || solver < 0 || solver > CUP_POISSON_B200_PIPELINED || max_iter < 0)
+  if (!c || solver < 0 || solver > CUP_POISSON_B200_TWOLEVEL_MIXED || max_iter < 0)
     return ctx_fail(c, CUP_ERR_ARG, "cup_set_poisson: bad arguments");
   c->cfg.poisson_solver = solver;
   c->cfg.poisson_tol = tol_abs;

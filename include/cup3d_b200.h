@@ -57,6 +57,8 @@ extern "C" {
                                        one-cell-overlap local solve of each block (restricted
                                        additive Schwarz) in place of the block inverse; the local
                                        map the network is trained to reproduce */
+#define CUP_POISSON_B200_TWOLEVEL_MIXED 7 /* "b200_twolevel_mixed": the two-level preconditioner in
+                                       FP32 inner solves inside FP64 iterative refinement */
 
 /* field ids */
 #define CUP_FIELD_VEL 0   /* 3 components */

@@ -245,17 +245,20 @@ def test_captured_batch_steps_match_launched_batch_steps():
         assert np.array_equal(batches[0].download("pres"), batches[1].download("pres")), step
 
 
-def test_moving_batch_matches_single_cases():
+@pytest.mark.parametrize("solver", ["b200", "b200_twolevel_mixed"])
+def test_moving_batch_matches_single_cases(solver):
     # bodies that move (-StaticObstacles 0): every batch step advances each
     # case's pose with the case's own dt and BDF2 history and creates all
     # bodies again on the flattened mesh; each case stepped alone by
     # cup_step with the batch's dt moves its body the same way.  chi bit for
     # bit at every step (the same creation arithmetic), velocity within 1e-7
     # of max |u| and pressure within 1e-6 of max |p| (solves to 1e-10 that sum
-    # in other orders)
+    # in other orders), with the FP64 block inverse and with the two-level
+    # preconditioner in mixed precision
     # (a relative 1e-10: at 1e-11 a case's solve can stall on rounding)
-    singles = _step_cases("-stepGraph 0 -poissonTolRel 1e-10", static=False)
-    batch = cup.Batch(_step_cases("-poissonTolRel 1e-10", static=False))
+    flags = f"-poissonTolRel 1e-10 -poissonSolver {solver}"
+    singles = _step_cases("-stepGraph 0 " + flags, static=False)
+    batch = cup.Batch(_step_cases(flags, static=False))
     chi0 = [batch.case_field("chi", k)[0].copy() for k in range(batch.ncase)]
     # steps 0-2: Euler, then BDF2 poses
     for step in range(3):

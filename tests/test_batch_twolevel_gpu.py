@@ -66,3 +66,32 @@ def test_captured_batched_twolevel_steps_match_launched():
         assert [s["iterations"] for s in st1] == [s["iterations"] for s in st0], step
         assert np.array_equal(batches[0].download("vel"), batches[1].download("vel")), step
         assert np.array_equal(batches[0].download("pres"), batches[1].download("pres")), step
+
+
+def test_batched_twolevel_mixed_precision():
+    # -poissonSolver b200_twolevel_mixed on a batch: FP32 batched inner solves
+    # with each case's coarse correction, FP64 refinement per case.  Every case
+    # meets the FP64 tolerance on the oracle's operator, agrees with the FP64
+    # batched two-level solve, and needs fewer inner iterations than the
+    # batched block inverse in mixed precision.
+    sols = {}
+    for solver in ("b200_twolevel", "b200_twolevel_mixed", "b200_mixed"):
+        ctxs, batch = _batch(solver)
+        meshes = [oracle_mesh(c) for c in ctxs]
+        bs = [compatible_rhs(m, 40 + k) for k, m in enumerate(meshes)]
+        bd, xd = torch_dev(np.concatenate(bs)), torch_dev(np.zeros(sum(m.n for m in meshes)))
+        rc, stats = batch.poisson_solve_dev(bd, xd)
+        assert rc == 0, (solver, stats)
+        xs = split(batch, xd.cpu().numpy())
+        for k, (ctx, m, b, x, st) in enumerate(zip(ctxs, meshes, bs, xs, stats)):
+            assert st["status"] == 1, (solver, k, st)
+            bb = mean_row_zeroed(ctx, m, b)
+            res = np.linalg.norm(bb - m.apply(x, mean_constraint=ctx.cfg.mean_constraint))
+            assert res <= 1.05e-10 * np.linalg.norm(bb), (solver, k, res)
+        sols[solver] = (xs, [s["iterations"] for s in stats])
+    print("iterations two-level FP64 / two-level mixed / block inverse mixed:",
+          *(sols[s][1] for s in ("b200_twolevel", "b200_twolevel_mixed", "b200_mixed")))
+    for k in range(len(NAMES)):
+        x64, x32 = sols["b200_twolevel"][0][k], sols["b200_twolevel_mixed"][0][k]
+        assert np.linalg.norm(x32 - x64) <= 1e-8 * np.linalg.norm(x64), k
+    assert sum(sols["b200_twolevel_mixed"][1]) < sum(sols["b200_mixed"][1]), sols
