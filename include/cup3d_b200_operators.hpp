@@ -46,8 +46,10 @@ struct SimulationData {
   explicit SimulationData(const std::string& flags) {
     cup_config_default(&cfg);
     check(cup_config_parse(&cfg, flags.c_str()), nullptr);
-    static const char* names[] = {"b200",          "b200_mixed",  "b200_learned", "b200_learned_mixed",
-                                  "b200_twolevel", "b200_schwarz", "b200_pipelined"};
+    static const char* names[] = {"b200",          "b200_mixed",   "b200_learned",   "b200_learned_mixed",
+                                  "b200_twolevel", "b200_schwarz", "b200_pipelined", "b200_twolevel_mixed"};
+    if (cfg.poisson_solver < 0 || cfg.poisson_solver >= int(sizeof(names) / sizeof(names[0])))
+      throw std::runtime_error("cup3d_b200: Poisson solver id without a name");
     poissonSolver = names[cfg.poisson_solver];
     ctx = cup_create(&cfg);
     if (!ctx) throw std::runtime_error(std::string("cup3d_b200: ") + cup_last_error(nullptr));
@@ -114,7 +116,8 @@ class PoissonSolverBase {
   virtual void solve() = 0;
 };
 
-// "b200", "b200_mixed", "b200_learned", "b200_learned_mixed": RHS in
+// "b200", "b200_mixed", "b200_learned", "b200_learned_mixed", "b200_twolevel",
+// "b200_twolevel_mixed", "b200_schwarz", "b200_pipelined": RHS in
 // sim.lhs, initial guess and result in sim.pres (PoissonSolverAMR.cpp:20-21).
 // The variant is the context's -poissonSolver setting.
 class PoissonSolverB200 : public PoissonSolverBase {
@@ -128,8 +131,9 @@ class PoissonSolverB200 : public PoissonSolverBase {
 // PoissonSolverBase.cpp:10-32: the solver named by -poissonSolver.  The
 // reference's "iterative" / "cuda_iterative" select the plain FP64 solver.
 inline std::shared_ptr<PoissonSolverBase> makePoissonSolver(SimulationData& s) {
-  static const char* known[] = {"b200",      "b200_mixed",     "b200_learned", "b200_learned_mixed",
-                                "b200_twolevel", "b200_schwarz", "b200_pipelined", "iterative", "cuda_iterative"};
+  static const char* known[] = {"b200",           "b200_mixed",          "b200_learned", "b200_learned_mixed",
+                                "b200_twolevel",  "b200_twolevel_mixed", "b200_schwarz", "b200_pipelined",
+                                "iterative",      "cuda_iterative"};
   for (const char* k : known)
     if (s.poissonSolver == k) return std::make_shared<PoissonSolverB200>(s);
   throw std::invalid_argument("Poisson solver: \"" + s.poissonSolver + "\" unrecognized!");

@@ -48,10 +48,15 @@ int main() {
 
   // makePoissonSolver for every solver name: a Simulation is built with each
   // and steps, its projection calling pressureSolver->solve() in the middle
-  for (const char* name : {"b200", "b200_mixed", "b200_learned", "b200_learned_mixed", "iterative"}) {
+  for (const char* name : {"b200", "b200_mixed", "b200_learned", "b200_learned_mixed", "b200_twolevel",
+                           "b200_twolevel_mixed", "iterative"}) {
     Simulation T(std::string("-bpdx 4 -bpdy 4 -bpdz 4 -levelMax 1 -extent 6.283185307179586 -BC_x periodic "
                              "-BC_y periodic -BC_z periodic -nu 0.01 -CFL 0.3 -rampup 0 -poissonTolRel 1e-8 "
                              "-poissonTol 0 -poissonSolver ") + name);
+    if (T.sim.poissonSolver != (std::string(name) == "iterative" ? "b200" : name)) {
+      std::printf("solver %s: named %s\n", name, T.sim.poissonSolver.c_str());
+      return 10;
+    }
     check(cup_set_mesh_uniform(T.sim.ctx), T.sim.ctx);
     check(cup_upload_field(T.sim.ctx, CUP_FIELD_VEL, vel.data()), T.sim.ctx);
     if (T.sim.poissonSolver.find("learned") != std::string::npos) check(cup_cnn_init(T.sim.ctx, 5), T.sim.ctx);
