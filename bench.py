@@ -77,10 +77,13 @@ ALG_BYTES = {
 
 
 # DRAM bytes (read + write) per cell and iteration of the persistent solver,
-# measured by ncu (--set full) on 16 iterations of
-# `python -m cup3d_b200.kernel_cases solve`: 147.7 MB + 594.2 MB over 16
-# iterations of 1,198,080 cells; most of the 176 algorithmic bytes hit in L2.
-MEASURED_TRAFFIC_PER_CELL_ITER = {"bicg_persistent": 38.70}
+# measured by ncu (--set full) on 16 iterations of one solve on the sphere
+# mesh (1,198,080 cells), per solver:
+#   b200 (`python -m cup3d_b200.kernel_cases solve`): 147.7 MB + 594.2 MB,
+#     most of the 176 algorithmic bytes hit in L2;
+#   b200_twolevel (`... solve b200_twolevel`): 724.2 MB + 844.7 MB, the two
+#     reads of the 21.9 MB A_c^-1 an iteration most of the growth.
+MEASURED_TRAFFIC_PER_CELL_ITER = {("bicg_persistent", "b200"): 38.70, ("bicg_persistent", "b200_twolevel"): 81.8}
 
 
 def dist_env():
@@ -558,8 +561,8 @@ def run_b200(args):
         alg_bytes = ALG_BYTES.get(dom_name, 0) * ncell
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if alg_bytes else None
     traffic = None
-    if dom_name in MEASURED_TRAFFIC_PER_CELL_ITER and args.solver == "b200":
-        traffic = int(MEASURED_TRAFFIC_PER_CELL_ITER[dom_name] * ncell * sum(prof_iters) / max(dom_n, 1))
+    if (dom_name, args.solver) in MEASURED_TRAFFIC_PER_CELL_ITER:
+        traffic = int(MEASURED_TRAFFIC_PER_CELL_ITER[dom_name, args.solver] * ncell * sum(prof_iters) / max(dom_n, 1))
     # ---- e2e through the C ABI with host buffers: the same K steps, the state
     # uploaded from pinned host memory before and downloaded after every step
     step = restore()
