@@ -1820,10 +1820,12 @@ int batch_solver_shape(int nb, int ncase, int* grid, int* groups) {
 // inner solves of the mixed-precision batch.
 // zero_mean_row: the mean-constraint row's right-hand side taken as zero
 // (the solver), or as given (the inner solves: it holds the row's residual).
+// case_tol_rel (launched path only): each case's own relative tolerance in
+// place of P.tol_rel (each case's Krylov state carries its stopping test).
 template <class T>
 static int batched_launch(const DevMesh& M, const T* b, T* x, T* const v[9], const SolveParams& P, PoissonWork& W,
                           BatchWork& B, SolveStats* out, cudaStream_t s, const BatchCoarse* coarse,
-                          int zero_mean_row) {
+                          int zero_mean_row, const double* case_tol_rel = nullptr) {
   poisson_init_constants();
   if (B.ncase < 1 || !B.st) return set_error(CUP_ERR_STATE, "batched BiCGSTAB: not a batch");
   const int zmr = zero_mean_row;
@@ -1831,7 +1833,10 @@ static int batched_launch(const DevMesh& M, const T* b, T* x, T* const v[9], con
     CUP_CUDA_TRY(cudaMemcpyAsync(B.st, B.st_init, sizeof(KrylovState) * B.ncase, cudaMemcpyDeviceToDevice, s));
   } else {
     std::vector<KrylovState> init(B.ncase);
-    for (KrylovState& k : init) krylov_init_state(P, k);
+    for (int c = 0; c < B.ncase; ++c) {
+      krylov_init_state(P, init[c]);
+      if (case_tol_rel) init[c].tol_rel = case_tol_rel[c];
+    }
     CUP_CUDA_TRY(cudaMemcpyAsync(B.st, init.data(), sizeof(KrylovState) * B.ncase, cudaMemcpyHostToDevice, s));
   }
   CUP_CUDA_TRY(cudaMemsetAsync(B.case_done, 0, sizeof(int) * B.ncase, s));
@@ -2002,8 +2007,8 @@ int poisson_mixed_batched(const DevMesh& M, const double* b, double* x, const So
     }
   }
   std::vector<SolveStats> in(K);
+  std::vector<double> q(K, 0.5);
   for (int outer = 0; outer < 40; ++outer) {
-    double q = 0.5;
     int min_total = P.max_iter, nact = 0;
     for (int k = 0; k < K; ++k) {
       if (active[k] && converged(k)) {
@@ -2012,9 +2017,10 @@ int poisson_mixed_batched(const DevMesh& M, const double* b, double* x, const So
       }
       if (!active[k]) continue;
       ++nact;
-      // the inner tolerance of the case that needs the most, within FP32 reach
+      // each case's inner tolerance: the reduction it still needs, within
+      // FP32 reach, as for one case
       const double want = std::max(P.tol_abs, P.tol_rel * err0[k]);
-      q = std::min(q, std::max(2e-5, 0.5 * want / err[k]));
+      q[k] = std::min(0.5, std::max(2e-5, 0.5 * want / err[k]));
       min_total = std::min(min_total, total[k]);
     }
     if (nact == 0) break;
@@ -2024,10 +2030,10 @@ int poisson_mixed_batched(const DevMesh& M, const double* b, double* x, const So
                                      size_t(first[k + 1] - first[k]) * BN * sizeof(float), s));
     SolveParams Q = P;
     Q.tol_abs = 0.0;
-    Q.tol_rel = q;
+    Q.tol_rel = 0.5;
     Q.max_iter = std::max(1, P.max_iter - min_total);
     CUP_CUDA_TRY(cudaMemsetAsync(e, 0, n * sizeof(float), s));
-    if (int rc = batched_launch<float>(M, W.r32, e, v, Q, W, B, in.data(), s, coarse, 0)) return rc;
+    if (int rc = batched_launch<float>(M, W.r32, e, v, Q, W, B, in.data(), s, coarse, 0, q.data())) return rc;
     if (int rc = update(e)) return rc;
     if (int rc = residual()) return rc;
     for (int k = 0; k < K; ++k) {
