@@ -9,7 +9,8 @@
     python -m cup3d_b200.kernel_cases adapt   # 20 two-level steps, one mesh adaptation, the coarse rebuild, 1 step
 
 A second argument names the Poisson solver of the sphere cases (default
-b200; e.g. b200_twolevel).
+b200; e.g. b200_twolevel, or b200_twolevel_mixed, whose FP32 inner solve is
+the k_bicg_persistent<float> launch).
 
 The sphere cases build the sphere mesh of cup3d_b200.workloads (2340
 blocks, 1.198M cells, ~0.3 GB of device memory); the swarm case batches the
